@@ -1,0 +1,243 @@
+/*
+ * zmpm.h -- C ABI of the B200 implicit APIC MPM substep.
+ *
+ * This is the drop-in boundary for the implicit (backward-Euler) APIC MPM
+ * substep of ziran2019 (Lib/MPM over Lib/SPGrid).  The reference exposes that
+ * substep as C++ template classes with no FFI; every entry point below names the
+ * reference member function or plugin call it replaces (path:line inside the
+ * reference project).
+ *
+ * Conventions
+ *   - Every function returns an int status (ZMPM_OK == 0; negative values are
+ *     errors, positive values are informational outcomes of a substep).
+ *   - No C++ exception crosses this boundary.
+ *   - One context == one simulation on one CUDA device, driven from one host
+ *     thread (the reference is also single-caller, MpmSimulationBase.h:133-229).
+ *   - Host arrays are row-major: positions [n][3], matrices [n][3][3].
+ *   - Particles are addressed by the index they were added with; the library
+ *     reorders its device copy internally and never changes those indices.
+ */
+#ifndef ZMPM_H
+#define ZMPM_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- status -- */
+enum zmpm_status_code {
+    ZMPM_OK = 0,
+    /* a particle moved more than one cell in the substep; the reference throws
+       RestartException here (Lib/MPM/MpmSimulationBase.cpp:983-1002) */
+    ZMPM_CFL_VIOLATION = 1,
+    /* Newton stopped at max_iterations above tolerance; the reference only
+       returns false (Lib/Ziran/Math/Nonlinear/NewtonsMethod.h:65) */
+    ZMPM_NEWTON_NOT_CONVERGED = 2,
+    ZMPM_NAN_DETECTED = 3,
+    ZMPM_TIMEOUT = 4, /* a bounded device-side wait gave up */
+    ZMPM_BAD_ARG = -1,
+    ZMPM_OUT_OF_GRID = -2, /* a particle stencil leaves the configured grid */
+    ZMPM_CUDA_ERROR = -3,
+    ZMPM_NO_MEMORY = -4,
+    ZMPM_NOT_READY = -5, /* a test hook was called before zmpm_begin_implicit */
+    ZMPM_UNSUPPORTED = -6
+};
+
+/* ------------------------------------------------------------- enums -------- */
+enum zmpm_precision {
+    ZMPM_FP64 = 0, /* every array and every operation in double */
+    ZMPM_MIXED = 1 /* state, residuals, reductions FP64; Hessian-vector product FP32 */
+};
+
+/* SPGrid page shape.  GridState<double,3> is 128 B, so a 4 KiB page holds
+   2x4x4 nodes; GridState<float,3> is 64 B -> 4x4x4 nodes
+   (Lib/MPM/MpmGrid.h:14-43, Lib/SPGrid/Core/SPGrid_Mask.h:31-37). */
+enum zmpm_layout {
+    ZMPM_LAYOUT_AUTO = 0, /* FP64 -> 2x4x4, MIXED -> 4x4x4 */
+    ZMPM_LAYOUT_244 = 1,
+    ZMPM_LAYOUT_444 = 2
+};
+
+/* Constitutive models (F-based force helper plugins). */
+enum zmpm_model {
+    ZMPM_MODEL_NONE = 0,
+    /* NeoHookeanBorden: Lib/Ziran/Physics/ConstitutiveModel/NeoHookeanBorden.cpp:16-111 */
+    ZMPM_MODEL_NEOHOOKEAN_BORDEN = 1,
+    /* StvkWithHenckyIsotropic: Lib/Ziran/Physics/ConstitutiveModel/StvkWithHenckyIsotropic.h:114-173 */
+    ZMPM_MODEL_STVK_HENCKY_ISOTROPIC = 2,
+    /* Fixed corotated (Stomakhin et al. 2012).  Not present in the reference;
+       written in the reference's SVD-isotropic plugin form. */
+    ZMPM_MODEL_FIXED_COROTATED = 3
+};
+
+/* Plasticity return maps (PlasticityApplier plugins). */
+enum zmpm_plasticity {
+    ZMPM_PLASTIC_NONE = 0,
+    /* VonMisesStvkHencky::projectStrain, Lib/Ziran/Physics/PlasticityApplier.cpp:462-502 */
+    ZMPM_PLASTIC_VON_MISES = 1
+};
+
+/* Krylov solver of the Newton step (BackwardEuler.h:82-98). */
+enum zmpm_linear_solver { ZMPM_MINRES = 0, ZMPM_CG = 1 };
+
+/* Collision objects (AnalyticCollisionObject, CollisionObject.h:42-195). */
+enum zmpm_collider_shape { ZMPM_HALF_SPACE = 0, ZMPM_SPHERE = 1, ZMPM_BOX = 2 };
+enum zmpm_collider_type { ZMPM_STICKY = 1, ZMPM_SLIP = 2, ZMPM_SEPARATE = 3, ZMPM_GHOST = 4 };
+
+/* ----------------------------------------------------------- structs -------- */
+typedef struct zmpm_ctx zmpm_ctx;
+
+typedef struct zmpm_config {
+    int32_t precision;   /* zmpm_precision */
+    int32_t layout;      /* zmpm_layout */
+    int32_t grid_log2;   /* grid covers [0, 2^grid_log2)^3 nodes; <= 12 (SPGrid 4096^3) */
+    int32_t device;      /* CUDA device ordinal */
+    double dx;
+    double gravity[3];
+    double apic_rpic_ratio; /* 1 = APIC (reference default, MpmSimulationBase.cpp:36) */
+    double cfl;             /* only used for the half-cell statistic, as the reference */
+} zmpm_config;
+
+typedef struct zmpm_solver {
+    int32_t linear_solver;          /* zmpm_linear_solver */
+    int32_t newton_max_iterations;  /* reference default 3 (MpmSimulationBase.cpp:51) */
+    double newton_tolerance;        /* reference default 1e-5, mass-weighted norm */
+    int32_t krylov_max_iterations;  /* reference default 20 (BackwardEuler.h:56) */
+    int32_t pad0;
+    double krylov_tolerance;        /* absolute; MINRES default 1 (BackwardEuler.h:62) */
+    double linear_solve_tolerance_scale; /* NewtonsMethod.h:38, default 1 */
+} zmpm_solver;
+
+typedef struct zmpm_collider {
+    int32_t shape; /* zmpm_collider_shape */
+    int32_t type;  /* zmpm_collider_type */
+    double friction;
+    /* material-space level set: HALF_SPACE origin=a, outward normal=b;
+       SPHERE center=a, radius=radius; BOX min corner=a, max corner=b */
+    double a[3];
+    double b[3];
+    double radius;
+    /* rigid motion x = R s X + t (CollisionObject.cpp:340-400); the reference's
+       updateState callback is replaced by linear-in-time translation and scale:
+       t(time) = translation + time*translation_velocity, s = scale + time*scale_velocity */
+    double rotation[4]; /* quaternion w,x,y,z */
+    double angular_velocity[3];
+    double translation[3];
+    double translation_velocity[3];
+    double scale;
+    double scale_velocity;
+} zmpm_collider;
+
+typedef struct zmpm_stats {
+    int32_t newton_iterations;   /* Newton iterations that ran a linear solve */
+    int32_t krylov_iterations;   /* summed over Newton iterations */
+    int32_t hvp_count;           /* Hessian-vector products evaluated */
+    int32_t cfl_violation;       /* 1 if a particle moved more than dx */
+    int32_t newton_converged;    /* 1 if the Newton norm fell below tolerance */
+    int32_t status_flags;        /* bit 0: NaN seen, bit 1: bounded wait gave up */
+    int64_t num_particles;
+    int64_t num_groups;          /* particle groups (one per touched page) */
+    int64_t num_blocks;          /* pages in the page map */
+    int64_t num_nodes;           /* grid nodes with m != 0 */
+    int64_t num_collision_nodes;
+    double newton_residual_initial;
+    double newton_residual_final;
+    double ms_total;             /* device time of the substep */
+} zmpm_stats;
+
+/* Result of the binning pass (sortParticlesAndPolluteGrid,
+   Lib/MPM/MpmSimulationBase.cpp:1032-1103); caller-allocated arrays sized from
+   zmpm_bin_counts.  Any pointer may be NULL. */
+typedef struct zmpm_bin_result {
+    uint64_t* particle_sorter;       /* [P] sorted keys */
+    int32_t* particle_order;         /* [P] */
+    uint64_t* particle_base_offset;  /* [P] indexed by particle */
+    int32_t* particle_group;         /* [G][2] first,last (inclusive) */
+    uint64_t* block_offset;          /* [G] page index of each group */
+    uint64_t* page_offsets;          /* [B] page map blocks, first-touch order */
+} zmpm_bin_result;
+
+/* ------------------------------------------------------------ lifecycle ----- */
+/* replaces MpmSimulationBase ctor + initialize (MpmSimulationBase.cpp:33-144) */
+int zmpm_create(const zmpm_config* cfg, zmpm_ctx** out);
+int zmpm_destroy(zmpm_ctx* ctx);
+const char* zmpm_last_error(const zmpm_ctx* ctx);
+const char* zmpm_status_string(int status);
+
+/* ----------------------------------------------------- scene / plugin API --- */
+/* Appends particles (the sampling helpers' output, MpmInitializationHelper.h);
+   F = I, C = 0.  *lower receives the handle's first index
+   (MpmParticleHandleBase ctor, MpmParticleHandleBase.cpp:1-60). */
+int zmpm_add_particles(zmpm_ctx* ctx, int64_t count, const double* x, const double* v,
+    const double* mass, const double* volume, int64_t* lower);
+
+/* MpmParticleHandleBase::addFBasedMpmForce (MpmParticleHandleBase.cpp:77-90):
+   attaches a constitutive model built from (E, nu) to particles [lower, upper). */
+int zmpm_add_fbased_force(zmpm_ctx* ctx, int64_t lower, int64_t upper, int32_t model,
+    double youngs_modulus, double poisson_ratio);
+
+/* Per-particle Lame parameters (each reference particle owns its model copy,
+   MpmParticleHandleBase.cpp:470).  For NeoHookeanBorden lambda is converted to
+   kappa = 0.666666 mu + lambda as NeoHookeanBorden.cpp:20 does. */
+int zmpm_set_lame(zmpm_ctx* ctx, int64_t lower, int64_t upper, const double* mu,
+    const double* lambda);
+
+/* MpmParticleHandleBase::addPlasticity (MpmParticleHandleBase.cpp:331-348). */
+int zmpm_add_plasticity(zmpm_ctx* ctx, int64_t lower, int64_t upper, int32_t kind,
+    double yield_stress, double xi, double fail_stress);
+
+/* MpmSimulationBase::addCollisionObject (MpmSimulationBase.cpp:80-84). */
+int zmpm_add_collision_object(zmpm_ctx* ctx, const zmpm_collider* obj, int32_t* id);
+/* Replaces a collider description (the reference's updateState callback). */
+int zmpm_set_collision_object(zmpm_ctx* ctx, int32_t id, const zmpm_collider* obj);
+
+/* ---------------------------------------------------------- state I/O ------- */
+/* Copy particle state to/from host arrays in particle-index order.  Any pointer
+   may be NULL.  x,v: [P][3]; C,F: [P][3][3]. */
+int zmpm_get_particles(zmpm_ctx* ctx, double* x, double* v, double* C, double* F);
+int zmpm_set_particles(zmpm_ctx* ctx, const double* x, const double* v, const double* C,
+    const double* F);
+/* Plastic state per particle (VonMisesStvkHencky::yield_stress, broken). */
+int zmpm_get_plastic_state(zmpm_ctx* ctx, double* yield_stress, int32_t* broken);
+int64_t zmpm_num_particles(const zmpm_ctx* ctx);
+double zmpm_time(const zmpm_ctx* ctx);
+
+/* -------------------------------------------------------------- substep ----- */
+/* MpmSimulationBase::advanceOneTimeStep, implicit branch
+   (MpmSimulationBase.cpp:256-296): reinitialize (sort + page map) -> P2G ->
+   backward-Euler Newton (MINRES/CG, matrix-free Hessian) -> G2P ->
+   evolveStrain -> plasticity.  stats may be NULL. */
+int zmpm_substep(zmpm_ctx* ctx, double dt, const zmpm_solver* solver, zmpm_stats* stats);
+
+/* Default solver settings of the reference (MpmSimulationBase.cpp:51,
+   BackwardEuler.h:56-62, LinearSolver.h:24). */
+void zmpm_default_solver(zmpm_solver* s, int32_t linear_solver, int32_t precision);
+
+/* -------------------------------------------------------------- hooks ------- */
+/* Binning only (sortParticlesAndPolluteGrid).  counts: [P, G, B]. */
+int zmpm_bin(zmpm_ctx* ctx, int64_t* counts);
+int zmpm_bin_fetch(zmpm_ctx* ctx, zmpm_bin_result* out);
+
+/* Runs reinitialize + particlesToGrid + startBackwardEuler for time step dt
+   (MpmSimulationBase.cpp:610-633) and stops, so the hooks below can evaluate
+   the Newton objective.  num_nodes receives N. */
+int zmpm_begin_implicit(zmpm_ctx* ctx, double dt, int64_t* num_nodes);
+/* Grid after P2G in node-index order (getNumNodes numbering, MpmGrid.h:123-136):
+   m [N], v [N][3], coord [N][3]. */
+int zmpm_get_grid(zmpm_ctx* ctx, double* m, double* v, int32_t* coord);
+/* Initial Newton guess dv [N][3] and collision projection flags [N]. */
+int zmpm_get_initial_dv(zmpm_ctx* ctx, double* dv, int32_t* collided);
+/* BackwardEulerLagrangianForceObjective::updateState + computeResidual +
+   computeNorm (BackwardEuler.h:101-175): residual [N][3], norm may be NULL. */
+int zmpm_residual(zmpm_ctx* ctx, const double* dv, double* residual, double* norm);
+/* BackwardEulerLagrangianForceObjective::multiply (BackwardEuler.h:322-351),
+   matrix-free (M + dt^2 K) x at the state of the last zmpm_residual call.
+   fp32 != 0 evaluates the Hessian-vector product in FP32 (MIXED contexts). */
+int zmpm_multiply(zmpm_ctx* ctx, const double* x, double* b, int32_t fp32);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ZMPM_H */

@@ -1,0 +1,2102 @@
+// TEST INFRASTRUCTURE -- NOT PART OF THE PRODUCT.
+//
+// CPU oracle for the implicit (backward-Euler) APIC MPM substep of ziran2019
+// (Lib/MPM over Lib/SPGrid).  It restates the reference algorithm in plain
+// C++17 + OpenMP because the reference itself cannot be built here (it needs
+// Eigen3, TBB, OpenVDB and partio, none of which are present).  Only the test
+// suite, __graft_entry__.smoke() and bench.py's CPU-baseline leg load it, and
+// only as the checker / timed CPU baseline; the CUDA library never calls it.
+//
+// Parity pinning:
+//   * SPGrid addressing (Linear_Offset, Packed_Add, page map) is pinned against
+//     the reference's own SPGrid sources compiled into oracle/_ref (see
+//     oracle/ref_spgrid_driver.cpp and tests/golden/).
+//   * Everything Eigen-based (constitutive models, SVD, Krylov, transfers) is
+//     "parity unpinned" by reference outputs: the reference ships no tests or
+//     golden vectors, so it is pinned by analytic known-answer tests only
+//     (partition of unity, conservation, SVD reconstruction, FD checks of
+//     P/dP/HVP, return-map idempotence).
+//
+// The grid mirrors SPGrid: a MAP_NORESERVE virtual array of GridState structs
+// over the full 4096^3 domain, addressed by the SPGrid byte offset
+// (SPGrid_Utilities.cpp:103-109).  P2G runs the reference's 8-colour schedule,
+// so per-node summation order is the reference's (colour -> block -> sorted
+// particle).  Reductions use fixed 256-node chunks summed in order.
+
+#include "../include/zmpm.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <functional>
+#include <limits>
+#include <memory>
+#include <new>
+#include <string>
+#include <vector>
+
+#include <parallel/algorithm>
+#include <immintrin.h>
+#include <sys/mman.h>
+#include <omp.h>
+
+namespace zo {
+
+using u64 = uint64_t;
+
+// ------------------------------------------------------------------ SPGrid --
+// SPGrid_Mask<log2_struct, log2_field=log2_struct, 3, log2_page=12>,
+// Lib/SPGrid/Core/SPGrid_Mask.h:22-52 (masks), :150-157 (Linear_Offset),
+// :237-245 (Packed_Add); Bit_Spread/Bit_Pack are pdep/pext
+// (SPGrid_Utilities.h:80-359, SPGrid_Utilities.cpp:43-62).
+struct Mask {
+    int log2_struct = 0, block_bits = 0, xbits = 0, ybits = 0, zbits = 0;
+    u64 xmask = 0, ymask = 0, zmask = 0;
+
+    explicit Mask(int l2s)
+    {
+        log2_struct = l2s;
+        block_bits = 12 - l2s;
+        zbits = block_bits / 3 + (block_bits % 3 > 0);
+        ybits = block_bits / 3 + (block_bits % 3 > 1);
+        xbits = block_bits / 3;
+        const int sh = 3 - block_bits % 3;
+        const u64 hi = ~0ull << 12;
+        const u64 pz = (0x9249249249249249ull << sh) & hi;
+        const u64 py = (0x2492492492492492ull << sh) & hi;
+        const u64 px = (0x4924924924924924ull << sh) & hi;
+        const u64 ez = ((1ull << zbits) - 1) << l2s;
+        const u64 ey = ((1ull << ybits) - 1) << (l2s + zbits);
+        const u64 ex = ((1ull << xbits) - 1) << (l2s + zbits + ybits);
+        xmask = px | ex;
+        ymask = py | ey;
+        zmask = pz | ez;
+        init_stencil();
+    }
+    // BMI2 pdep/pext, the reference's HASWELL path (SPGrid_Utilities.cpp:23-41)
+    static u64 deposit(u64 data, u64 mask) { return _pdep_u64(data, mask); }
+    static u64 extract(u64 data, u64 mask) { return _pext_u64(data, mask); }
+    u64 stencil[27]; // Linear_Offset(i,j,k), i,j,k in {0,1,2}
+    void init_stencil()
+    {
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j)
+                for (int k = 0; k < 3; ++k) stencil[9 * i + 3 * j + k] = linear_offset(i, j, k);
+    }
+    u64 linear_offset(int i, int j, int k) const
+    {
+        return deposit((u64)(int64_t)i, xmask) | deposit((u64)(int64_t)j, ymask) | deposit((u64)(int64_t)k, zmask);
+    }
+    void coord(u64 off, int c[3]) const
+    {
+        c[0] = (int32_t)extract(off, xmask);
+        c[1] = (int32_t)extract(off, ymask);
+        c[2] = (int32_t)extract(off, zmask);
+    }
+    u64 packed_add(u64 a, u64 b) const
+    {
+        const u64 w = xmask | ymask | zmask;
+        const u64 rx = ((a | ~xmask) + (b & xmask)) & xmask;
+        const u64 ry = ((a | ~ymask) + (b & ymask)) & ymask;
+        const u64 rz = ((a | ~zmask) + (b & zmask)) & zmask;
+        const u64 rw = ((a | w) + (b & ~w)) & ~w;
+        return rx | ry | rz | rw;
+    }
+    int bx() const { return 1 << xbits; }
+    int by() const { return 1 << ybits; }
+    int bz() const { return 1 << zbits; }
+    int elements() const { return 1 << block_bits; }
+};
+
+// GridState<T,3>, Lib/MPM/MpmGrid.h:14-43 (field order must not change).
+template <class T>
+struct GridState {
+    T v[3];
+    T m;
+    T new_v[3];
+    typename std::conditional<std::is_same<T, float>::value, int32_t, int64_t>::type idx;
+    T padding[6];
+    T phase_field;
+    T phase_field_multiplier;
+};
+static_assert(sizeof(GridState<double>) == 128, "GridState<double,3> must be 128 B");
+static_assert(sizeof(GridState<float>) == 64, "GridState<float,3> must be 64 B");
+
+struct VMem {
+    void* p = nullptr;
+    size_t n = 0;
+    bool map(size_t bytes)
+    {
+        n = bytes;
+        p = mmap(nullptr, n, PROT_READ | PROT_WRITE, MAP_PRIVATE | MAP_ANONYMOUS | MAP_NORESERVE, -1, 0);
+        if (p == MAP_FAILED) {
+            p = nullptr;
+            return false;
+        }
+        return true;
+    }
+    void unmap()
+    {
+        if (p) munmap(p, n);
+        p = nullptr;
+    }
+};
+
+// ------------------------------------------------------------ 3x3 algebra --
+template <class T>
+struct M3 {
+    T a[3][3];
+    static M3 zero()
+    {
+        M3 m;
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j) m.a[i][j] = 0;
+        return m;
+    }
+    static M3 identity()
+    {
+        M3 m = zero();
+        m.a[0][0] = m.a[1][1] = m.a[2][2] = 1;
+        return m;
+    }
+    T& operator()(int i, int j) { return a[i][j]; }
+    const T& operator()(int i, int j) const { return a[i][j]; }
+};
+template <class T>
+static M3<T> mul(const M3<T>& A, const M3<T>& B)
+{
+    M3<T> C;
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) C.a[i][j] = A.a[i][0] * B.a[0][j] + A.a[i][1] * B.a[1][j] + A.a[i][2] * B.a[2][j];
+    return C;
+}
+template <class T>
+static M3<T> mulT(const M3<T>& A, const M3<T>& B) // A * B^T
+{
+    M3<T> C;
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) C.a[i][j] = A.a[i][0] * B.a[j][0] + A.a[i][1] * B.a[j][1] + A.a[i][2] * B.a[j][2];
+    return C;
+}
+template <class T>
+static M3<T> Tmul(const M3<T>& A, const M3<T>& B) // A^T * B
+{
+    M3<T> C;
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) C.a[i][j] = A.a[0][i] * B.a[0][j] + A.a[1][i] * B.a[1][j] + A.a[2][i] * B.a[2][j];
+    return C;
+}
+template <class T>
+static M3<T> transpose(const M3<T>& A)
+{
+    M3<T> C;
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) C.a[i][j] = A.a[j][i];
+    return C;
+}
+template <class T>
+static M3<T> scaled(const M3<T>& A, T s)
+{
+    M3<T> C;
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) C.a[i][j] = A.a[i][j] * s;
+    return C;
+}
+template <class T>
+static M3<T> add(const M3<T>& A, const M3<T>& B)
+{
+    M3<T> C;
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) C.a[i][j] = A.a[i][j] + B.a[i][j];
+    return C;
+}
+template <class T>
+static T contract(const M3<T>& A, const M3<T>& B)
+{
+    T s = 0;
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) s += A.a[i][j] * B.a[i][j];
+    return s;
+}
+template <class T>
+static T det(const M3<T>& m)
+{
+    return m.a[0][0] * (m.a[1][1] * m.a[2][2] - m.a[2][1] * m.a[1][2])
+        - m.a[1][0] * (m.a[0][1] * m.a[2][2] - m.a[2][1] * m.a[0][2])
+        + m.a[2][0] * (m.a[0][1] * m.a[1][2] - m.a[1][1] * m.a[0][2]);
+}
+// J F^{-T}, Lib/Ziran/Math/Linear/DenseExt.h:240-252
+template <class T>
+static M3<T> cofactor(const M3<T>& F)
+{
+    M3<T> A;
+    A.a[0][0] = F.a[1][1] * F.a[2][2] - F.a[1][2] * F.a[2][1];
+    A.a[0][1] = F.a[1][2] * F.a[2][0] - F.a[1][0] * F.a[2][2];
+    A.a[0][2] = F.a[1][0] * F.a[2][1] - F.a[1][1] * F.a[2][0];
+    A.a[1][0] = F.a[0][2] * F.a[2][1] - F.a[0][1] * F.a[2][2];
+    A.a[1][1] = F.a[0][0] * F.a[2][2] - F.a[0][2] * F.a[2][0];
+    A.a[1][2] = F.a[0][1] * F.a[2][0] - F.a[0][0] * F.a[2][1];
+    A.a[2][0] = F.a[0][1] * F.a[1][2] - F.a[0][2] * F.a[1][1];
+    A.a[2][1] = F.a[0][2] * F.a[1][0] - F.a[0][0] * F.a[1][2];
+    A.a[2][2] = F.a[0][0] * F.a[1][1] - F.a[0][1] * F.a[1][0];
+    return A;
+}
+template <class T>
+static M3<T> udiagvt(const M3<T>& U, const T d[3], const M3<T>& V) // U diag(d) V^T
+{
+    M3<T> C;
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) C.a[i][j] = U.a[i][0] * d[0] * V.a[j][0] + U.a[i][1] * d[1] * V.a[j][1] + U.a[i][2] * d[2] * V.a[j][2];
+    return C;
+}
+
+// ------------------------------------------------------------------ SVD ----
+// Implicit-shift QR SVD of 3x3 matrices (Gast et al.), as in
+// Lib/Ziran/Math/Linear/ImplicitQRSVD.h:219-532 and Givens.h:33-270.
+template <class T>
+struct Givens {
+    int i, k;
+    T c, s;
+    Givens(int i_, int k_) : i(i_), k(k_), c(1), s(0) {}
+    void compute(T a, T b)
+    {
+        T d = a * a + b * b;
+        c = 1;
+        s = 0;
+        T sd = std::sqrt(d);
+        if (sd) {
+            T t = 1 / sd;
+            c = a * t;
+            s = -b * t;
+        }
+    }
+    void computeUnconventional(T a, T b)
+    {
+        T d = a * a + b * b;
+        c = 0;
+        s = 1;
+        T sd = std::sqrt(d);
+        if (sd) {
+            T t = 1 / sd;
+            s = a * t;
+            c = b * t;
+        }
+    }
+    void rowRotation(M3<T>& A) const
+    {
+        for (int j = 0; j < 3; ++j) {
+            T t1 = A.a[i][j], t2 = A.a[k][j];
+            A.a[i][j] = c * t1 - s * t2;
+            A.a[k][j] = s * t1 + c * t2;
+        }
+    }
+    void columnRotation(M3<T>& A) const
+    {
+        for (int j = 0; j < 3; ++j) {
+            T t1 = A.a[j][i], t2 = A.a[j][k];
+            A.a[j][i] = c * t1 - s * t2;
+            A.a[j][k] = s * t1 + c * t2;
+        }
+    }
+};
+
+template <class T>
+static void zeroChase(M3<T>& H, M3<T>& U, M3<T>& V)
+{
+    Givens<T> r1(0, 1);
+    r1.compute(H.a[0][0], H.a[1][0]);
+    Givens<T> r2(1, 2);
+    if (H.a[1][0] != 0)
+        r2.compute(H.a[0][0] * H.a[0][1] + H.a[1][0] * H.a[1][1], H.a[0][0] * H.a[0][2] + H.a[1][0] * H.a[1][2]);
+    else
+        r2.compute(H.a[0][1], H.a[0][2]);
+    r1.rowRotation(H);
+    r2.columnRotation(H);
+    r2.columnRotation(V);
+    Givens<T> r3(1, 2);
+    r3.compute(H.a[1][1], H.a[2][1]);
+    r3.rowRotation(H);
+    r1.columnRotation(U);
+    r3.columnRotation(U);
+}
+
+template <class T>
+static void makeUpperBidiag(M3<T>& H, M3<T>& U, M3<T>& V)
+{
+    U = M3<T>::identity();
+    V = M3<T>::identity();
+    Givens<T> r(1, 2);
+    r.compute(H.a[1][0], H.a[2][0]);
+    r.rowRotation(H);
+    r.columnRotation(U);
+    zeroChase(H, U, V);
+}
+
+// 2x2 SVD of the block [[a00,a01],[a10,a11]] in Givens form (ImplicitQRSVD.h:95-160)
+template <class T>
+static void svd2(T a00, T a01, T a10, T a11, T& uc, T& us, T& s0, T& s1, T& vc, T& vs)
+{
+    // polar: R from x = (a00 + a11, a10 - a01)
+    T x0 = a00 + a11, x1 = a10 - a01;
+    T den = std::sqrt(x0 * x0 + x1 * x1);
+    uc = 1;
+    us = 0;
+    if (den != 0) {
+        uc = x0 / den;
+        us = -x1 / den;
+    }
+    // S = G A with G = [[c,-s],[s,c]] (rowRotation)
+    T S00 = uc * a00 - us * a10, S01 = uc * a01 - us * a11;
+    T S11 = us * a01 + uc * a11;
+    T cosine, sine;
+    T x = S00, y = S01, z = S11;
+    T y2 = y * y;
+    if (y2 == 0) {
+        cosine = 1;
+        sine = 0;
+        s0 = x;
+        s1 = z;
+    }
+    else {
+        T tau = T(0.5) * (x - z);
+        T w = std::sqrt(tau * tau + y2);
+        T t = (tau > 0) ? y / (tau + w) : y / (tau - w);
+        cosine = T(1) / std::sqrt(t * t + T(1));
+        sine = -t * cosine;
+        T c2 = cosine * cosine;
+        T csy = 2 * cosine * sine * y;
+        T s2 = sine * sine;
+        s0 = c2 * x - csy + s2 * z;
+        s1 = s2 * x + csy + c2 * z;
+    }
+    if (s0 < s1) {
+        std::swap(s0, s1);
+        vc = -sine;
+        vs = cosine;
+    }
+    else {
+        vc = cosine;
+        vs = sine;
+    }
+    // U *= V
+    T nc = uc * vc - us * vs;
+    T ns = us * vc + uc * vs;
+    uc = nc;
+    us = ns;
+}
+
+template <class T>
+static void process2(int t, M3<T>& B, M3<T>& U, T sigma[3], M3<T>& V)
+{
+    int other = (t == 1) ? 0 : 2;
+    sigma[other] = B.a[other][other];
+    Givens<T> u(t, t + 1), v(t, t + 1);
+    svd2(B.a[t][t], B.a[t][t + 1], B.a[t + 1][t], B.a[t + 1][t + 1], u.c, u.s, sigma[t], sigma[t + 1], v.c, v.s);
+    u.columnRotation(U);
+    v.columnRotation(V);
+}
+
+template <class T>
+static void flipSign(int i, M3<T>& U, T sigma[3])
+{
+    sigma[i] = -sigma[i];
+    for (int r = 0; r < 3; ++r) U.a[r][i] = -U.a[r][i];
+}
+template <class T>
+static void swapCol(M3<T>& A, int i, int j)
+{
+    for (int r = 0; r < 3; ++r) std::swap(A.a[r][i], A.a[r][j]);
+}
+template <class T>
+static void negCol(M3<T>& A, int i)
+{
+    for (int r = 0; r < 3; ++r) A.a[r][i] = -A.a[r][i];
+}
+
+template <class T>
+static void sort0(M3<T>& U, T sigma[3], M3<T>& V)
+{
+    if (std::fabs(sigma[1]) >= std::fabs(sigma[2])) {
+        if (sigma[1] < 0) {
+            flipSign(1, U, sigma);
+            flipSign(2, U, sigma);
+        }
+        return;
+    }
+    if (sigma[2] < 0) {
+        flipSign(1, U, sigma);
+        flipSign(2, U, sigma);
+    }
+    std::swap(sigma[1], sigma[2]);
+    swapCol(U, 1, 2);
+    swapCol(V, 1, 2);
+    if (sigma[1] > sigma[0]) {
+        std::swap(sigma[0], sigma[1]);
+        swapCol(U, 0, 1);
+        swapCol(V, 0, 1);
+    }
+    else {
+        negCol(U, 2);
+        negCol(V, 2);
+    }
+}
+
+template <class T>
+static void sort1(M3<T>& U, T sigma[3], M3<T>& V)
+{
+    if (std::fabs(sigma[0]) >= sigma[1]) {
+        if (sigma[0] < 0) {
+            flipSign(0, U, sigma);
+            flipSign(2, U, sigma);
+        }
+        return;
+    }
+    std::swap(sigma[0], sigma[1]);
+    swapCol(U, 0, 1);
+    swapCol(V, 0, 1);
+    if (std::fabs(sigma[1]) < std::fabs(sigma[2])) {
+        std::swap(sigma[1], sigma[2]);
+        swapCol(U, 1, 2);
+        swapCol(V, 1, 2);
+    }
+    else {
+        negCol(U, 1);
+        negCol(V, 1);
+    }
+    if (sigma[1] < 0) {
+        flipSign(1, U, sigma);
+        flipSign(2, U, sigma);
+    }
+}
+
+template <class T>
+static T wilkinsonShift(T a1, T b1, T a2)
+{
+    T d = T(0.5) * (a1 - a2);
+    T bs = b1 * b1;
+    return a2 - std::copysign(bs / (std::fabs(d) + std::sqrt(d * d + bs)), d);
+}
+
+template <class T>
+static T svd_tol();
+template <>
+double svd_tol<double>() { return 1024 * std::numeric_limits<double>::epsilon(); }
+template <>
+float svd_tol<float>() { return 128 * std::numeric_limits<float>::epsilon(); }
+
+template <class T>
+static int svd3(const M3<T>& A, M3<T>& U, T sigma[3], M3<T>& V)
+{
+    M3<T> B = A;
+    makeUpperBidiag(B, U, V);
+    int count = 0;
+    T tol = svd_tol<T>();
+    Givens<T> r(0, 1);
+    T alpha_1 = B.a[0][0], beta_1 = B.a[0][1], alpha_2 = B.a[1][1], alpha_3 = B.a[2][2], beta_2 = B.a[1][2];
+    T gamma_1 = alpha_1 * beta_1, gamma_2 = alpha_2 * beta_2;
+    tol *= std::max(T(0.5) * std::sqrt(alpha_1 * alpha_1 + alpha_2 * alpha_2 + alpha_3 * alpha_3 + beta_1 * beta_1 + beta_2 * beta_2), T(1));
+    // the reference loop has no cap; a cap keeps a pathological input from hanging a test
+    while (std::fabs(beta_2) > tol && std::fabs(beta_1) > tol && std::fabs(alpha_1) > tol && std::fabs(alpha_2) > tol
+        && std::fabs(alpha_3) > tol && count < 1000) {
+        T mu = wilkinsonShift(alpha_2 * alpha_2 + beta_1 * beta_1, gamma_2, alpha_3 * alpha_3 + beta_2 * beta_2);
+        r.compute(alpha_1 * alpha_1 - mu, gamma_1);
+        r.columnRotation(B);
+        r.columnRotation(V);
+        zeroChase(B, U, V);
+        alpha_1 = B.a[0][0];
+        beta_1 = B.a[0][1];
+        alpha_2 = B.a[1][1];
+        alpha_3 = B.a[2][2];
+        beta_2 = B.a[1][2];
+        gamma_1 = alpha_1 * beta_1;
+        gamma_2 = alpha_2 * beta_2;
+        count++;
+    }
+    if (std::fabs(beta_2) <= tol) {
+        process2(0, B, U, sigma, V);
+        sort0(U, sigma, V);
+    }
+    else if (std::fabs(beta_1) <= tol) {
+        process2(1, B, U, sigma, V);
+        sort1(U, sigma, V);
+    }
+    else if (std::fabs(alpha_2) <= tol) {
+        Givens<T> r1(1, 2);
+        r1.computeUnconventional(B.a[1][2], B.a[2][2]);
+        r1.rowRotation(B);
+        r1.columnRotation(U);
+        process2(0, B, U, sigma, V);
+        sort0(U, sigma, V);
+    }
+    else if (std::fabs(alpha_3) <= tol) {
+        Givens<T> r1(1, 2);
+        r1.compute(B.a[1][1], B.a[1][2]);
+        r1.columnRotation(B);
+        r1.columnRotation(V);
+        Givens<T> r2(0, 2);
+        r2.compute(B.a[0][0], B.a[0][2]);
+        r2.columnRotation(B);
+        r2.columnRotation(V);
+        process2(0, B, U, sigma, V);
+        sort0(U, sigma, V);
+    }
+    else if (std::fabs(alpha_1) <= tol) {
+        Givens<T> r1(0, 1);
+        r1.computeUnconventional(B.a[0][1], B.a[1][1]);
+        r1.rowRotation(B);
+        r1.columnRotation(U);
+        Givens<T> r2(0, 2);
+        r2.computeUnconventional(B.a[0][2], B.a[2][2]);
+        r2.rowRotation(B);
+        r2.columnRotation(U);
+        process2(1, B, U, sigma, V);
+        sort1(U, sigma, V);
+    }
+    return count;
+}
+
+// ------------------------------------------------------------ math tools ---
+// Lib/Ziran/Math/MathTools.h:163-262
+template <class T>
+static T clamp_small_magnitude(T x, T eps)
+{
+    if (x < -eps) return x;
+    if (x < 0) return -eps;
+    if (x < eps) return eps;
+    return x;
+}
+template <class T>
+static T log_1px_over_x(T x, T eps) { return std::fabs(x) < eps ? T(1) : std::log1p(x) / x; }
+template <class T>
+static T diff_log_over_diff(T x, T y, T eps) { return log_1px_over_x(x / y - 1, eps) / y; }
+template <class T>
+static T diff_interlock_log_over_diff(T x, T y, T logy, T eps) { return logy - y * diff_log_over_diff(x, y, eps); }
+
+// ---------------------------------------------------- constitutive models --
+template <class T>
+struct Model {
+    int32_t kind = ZMPM_MODEL_NONE;
+    T mu = 0, lambda = 0, kappa = 0, g = 1;
+};
+
+// Scratch of one particle.  SvdBasedIsotropicHelper<T,3> coefficients
+// (SvdBasedIsotropicHelper.h:97-162) for the SVD-based models.
+template <class T>
+struct Scratch {
+    M3<T> F, FinvT, U, V;
+    T J = 1, logJ = 0;
+    T sigma[3] = { 1, 1, 1 }, logS[3] = { 0, 0, 0 };
+    T psi[3], psi_d[3], psi_o[3]; // psi0..2, psi00/11/22, psi01/02/12
+    T m[3], p[3];                 // m01,m02,m12, p01,p02,p12
+};
+
+template <class T>
+static void isotropicContract(const Scratch<T>& s, const M3<T>& A, M3<T>& B)
+{
+    // B = dPdF(Sigma) : A, SvdBasedIsotropicHelper.h:151-162
+    B.a[0][0] = s.psi_d[0] * A.a[0][0] + s.psi_o[0] * A.a[1][1] + s.psi_o[1] * A.a[2][2];
+    B.a[1][1] = s.psi_o[0] * A.a[0][0] + s.psi_d[1] * A.a[1][1] + s.psi_o[2] * A.a[2][2];
+    B.a[2][2] = s.psi_o[1] * A.a[0][0] + s.psi_o[2] * A.a[1][1] + s.psi_d[2] * A.a[2][2];
+    B.a[0][1] = ((s.m[0] + s.p[0]) * A.a[0][1] + (s.m[0] - s.p[0]) * A.a[1][0]) / 2;
+    B.a[1][0] = ((s.m[0] - s.p[0]) * A.a[0][1] + (s.m[0] + s.p[0]) * A.a[1][0]) / 2;
+    B.a[0][2] = ((s.m[1] + s.p[1]) * A.a[0][2] + (s.m[1] - s.p[1]) * A.a[2][0]) / 2;
+    B.a[2][0] = ((s.m[1] - s.p[1]) * A.a[0][2] + (s.m[1] + s.p[1]) * A.a[2][0]) / 2;
+    B.a[1][2] = ((s.m[2] + s.p[2]) * A.a[1][2] + (s.m[2] - s.p[2]) * A.a[2][1]) / 2;
+    B.a[2][1] = ((s.m[2] - s.p[2]) * A.a[1][2] + (s.m[2] + s.p[2]) * A.a[2][1]) / 2;
+}
+
+template <class T>
+static void updateScratch(const Model<T>& c, const M3<T>& F, Scratch<T>& s)
+{
+    s.F = F;
+    if (c.kind == ZMPM_MODEL_NEOHOOKEAN_BORDEN) {
+        // NeoHookeanBorden::updateScratch, NeoHookeanBorden.cpp:24-35
+        s.J = det(F);
+        M3<T> JFinvT = cofactor(F);
+        s.FinvT = scaled(JFinvT, T(1) / s.J);
+        s.logJ = std::log(s.J);
+        return;
+    }
+    if (c.kind != ZMPM_MODEL_STVK_HENCKY_ISOTROPIC && c.kind != ZMPM_MODEL_FIXED_COROTATED) return;
+    svd3(F, s.U, s.sigma, s.V);
+    const T eps = T(1e-6);
+    const T mu = c.mu, lambda = c.lambda;
+    const T* sg = s.sigma;
+    if (c.kind == ZMPM_MODEL_STVK_HENCKY_ISOTROPIC) {
+        // StvkWithHenckyIsotropic::updateScratch (3D), StvkWithHenckyIsotropic.h:114-143
+        for (int d = 0; d < 3; ++d) s.logS[d] = std::log(std::fabs(sg[d]));
+        const T* L = s.logS;
+        T g = 2 * mu + lambda;
+        T sum_log = L[0] + L[1] + L[2];
+        T prod01 = sg[0] * sg[1], prod02 = sg[0] * sg[2], prod12 = sg[1] * sg[2];
+        s.psi[0] = (2 * mu * L[0] + lambda * sum_log) / sg[0];
+        s.psi[1] = (2 * mu * L[1] + lambda * sum_log) / sg[1];
+        s.psi[2] = (2 * mu * L[2] + lambda * sum_log) / sg[2];
+        s.psi_d[0] = (g * (1 - L[0]) - lambda * (L[1] + L[2])) / (sg[0] * sg[0]);
+        s.psi_d[1] = (g * (1 - L[1]) - lambda * (L[0] + L[2])) / (sg[1] * sg[1]);
+        s.psi_d[2] = (g * (1 - L[2]) - lambda * (L[0] + L[1])) / (sg[2] * sg[2]);
+        s.psi_o[0] = lambda / (sg[0] * sg[1]);
+        s.psi_o[1] = lambda / (sg[0] * sg[2]);
+        s.psi_o[2] = lambda / (sg[1] * sg[2]);
+        s.m[0] = -(lambda * sum_log + 2 * mu * diff_interlock_log_over_diff(sg[0], sg[1], L[1], eps)) / prod01;
+        s.m[1] = -(lambda * sum_log + 2 * mu * diff_interlock_log_over_diff(sg[0], sg[2], L[2], eps)) / prod02;
+        s.m[2] = -(lambda * sum_log + 2 * mu * diff_interlock_log_over_diff(sg[1], sg[2], L[2], eps)) / prod12;
+    }
+    else {
+        // Fixed corotated, psi = mu sum (s_i-1)^2 + lambda/2 (J-1)^2 written in
+        // the same SVD-isotropic form (derivatives of psi-hat in sigma).
+        T J = sg[0] * sg[1] * sg[2];
+        T c0 = sg[1] * sg[2], c1 = sg[0] * sg[2], c2 = sg[0] * sg[1];
+        s.J = J;
+        s.psi[0] = 2 * mu * (sg[0] - 1) + lambda * (J - 1) * c0;
+        s.psi[1] = 2 * mu * (sg[1] - 1) + lambda * (J - 1) * c1;
+        s.psi[2] = 2 * mu * (sg[2] - 1) + lambda * (J - 1) * c2;
+        s.psi_d[0] = 2 * mu + lambda * c0 * c0;
+        s.psi_d[1] = 2 * mu + lambda * c1 * c1;
+        s.psi_d[2] = 2 * mu + lambda * c2 * c2;
+        s.psi_o[0] = lambda * sg[2] * (2 * J - 1);
+        s.psi_o[1] = lambda * sg[1] * (2 * J - 1);
+        s.psi_o[2] = lambda * sg[0] * (2 * J - 1);
+        s.m[0] = 2 * mu - lambda * (J - 1) * sg[2];
+        s.m[1] = 2 * mu - lambda * (J - 1) * sg[1];
+        s.m[2] = 2 * mu - lambda * (J - 1) * sg[0];
+    }
+    s.p[0] = (s.psi[0] + s.psi[1]) / clamp_small_magnitude(sg[0] + sg[1], eps);
+    s.p[1] = (s.psi[0] + s.psi[2]) / clamp_small_magnitude(sg[0] + sg[2], eps);
+    s.p[2] = (s.psi[1] + s.psi[2]) / clamp_small_magnitude(sg[1] + sg[2], eps);
+}
+
+template <class T>
+static T psi(const Model<T>& c, const Scratch<T>& s)
+{
+    if (c.kind == ZMPM_MODEL_NEOHOOKEAN_BORDEN) {
+        // NeoHookeanBorden::psi, NeoHookeanBorden.cpp:37-52
+        M3<T> JaF = scaled(s.F, std::pow(s.J, -T(1) / T(3)));
+        T psi_dev = c.mu / 2 * (contract(JaF, JaF) - 3);
+        T psi_vol = c.kappa / 2 * ((s.J * s.J - 1) / 2 - std::log(s.J));
+        T psi_pos = (s.J >= 1) ? (psi_vol + psi_dev) : psi_dev;
+        T psi_neg = (s.J >= 1) ? T(0) : psi_vol;
+        return c.g * psi_pos + psi_neg;
+    }
+    if (c.kind == ZMPM_MODEL_STVK_HENCKY_ISOTROPIC) {
+        T tr = s.logS[0] + s.logS[1] + s.logS[2];
+        return c.mu * (s.logS[0] * s.logS[0] + s.logS[1] * s.logS[1] + s.logS[2] * s.logS[2]) + T(0.5) * c.lambda * tr * tr;
+    }
+    if (c.kind == ZMPM_MODEL_FIXED_COROTATED) {
+        T a = s.sigma[0] - 1, b = s.sigma[1] - 1, d = s.sigma[2] - 1, J = s.sigma[0] * s.sigma[1] * s.sigma[2];
+        return c.mu * (a * a + b * b + d * d) + T(0.5) * c.lambda * (J - 1) * (J - 1);
+    }
+    return 0;
+}
+
+template <class T>
+static M3<T> firstPiola(const Model<T>& c, const Scratch<T>& s)
+{
+    if (c.kind == ZMPM_MODEL_NEOHOOKEAN_BORDEN) {
+        // kirchhoff (NeoHookeanBorden.cpp:67-83), then P = tau F^{-T}
+        // (HyperelasticConstitutiveModel.h:85-90)
+        M3<T> B = mulT(s.F, s.F);
+        T tr = B.a[0][0] + B.a[1][1] + B.a[2][2];
+        M3<T> devB = B;
+        for (int d = 0; d < 3; ++d) devB.a[d][d] = B.a[d][d] - T(1) / 3 * tr;
+        M3<T> tau_dev = scaled(devB, c.mu * std::pow(s.J, -T(2) / T(3)));
+        T prime = c.kappa / 2 * (s.J - 1 / s.J);
+        T vol = s.J * prime;
+        M3<T> tau;
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j) {
+                T tv = (i == j) ? vol : T(0);
+                tau.a[i][j] = (s.J >= 1) ? c.g * (tau_dev.a[i][j] + tv) : c.g * tau_dev.a[i][j] + tv;
+            }
+        return mul(tau, s.FinvT);
+    }
+    if (c.kind == ZMPM_MODEL_STVK_HENCKY_ISOTROPIC || c.kind == ZMPM_MODEL_FIXED_COROTATED)
+        return udiagvt(s.U, s.psi, s.V);
+    return M3<T>::zero();
+}
+
+template <class T>
+static M3<T> firstPiolaDifferential(const Model<T>& c, const Scratch<T>& s, const M3<T>& dF)
+{
+    if (c.kind == ZMPM_MODEL_NEOHOOKEAN_BORDEN) {
+        // NeoHookeanBorden::firstPiolaDifferential, NeoHookeanBorden.cpp:85-111
+        T FinvT_dF = contract(s.FinvT, dF);
+        T deltaJ = s.J * FinvT_dF;
+        T FcontractF = contract(s.F, s.F);
+        M3<T> deltaFinvT = scaled(mul(mul(s.FinvT, transpose(dF)), s.FinvT), T(-1));
+        T a = -T(1) / 3;
+        T muJ2a = c.mu * std::pow(s.J, T(2) * a);
+        T prime = c.kappa / 2 * (s.J - T(1) / s.J);
+        T prime2 = c.kappa / 2 * (T(1) + T(1) / (s.J * s.J));
+        T F_dF = contract(s.F, dF);
+        M3<T> dP;
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j) {
+                T dev = 2 * a * muJ2a * FinvT_dF * (a * FcontractF * s.FinvT.a[i][j] + s.F.a[i][j]);
+                dev += muJ2a * (2 * a * F_dF * s.FinvT.a[i][j] + a * FcontractF * deltaFinvT.a[i][j] + dF.a[i][j]);
+                T vol = deltaJ * prime * s.FinvT.a[i][j] + s.J * deltaJ * prime2 * s.FinvT.a[i][j] + s.J * prime * deltaFinvT.a[i][j];
+                dP.a[i][j] = (s.J >= 1) ? c.g * (dev + vol) : c.g * dev + vol;
+            }
+        return dP;
+    }
+    if (c.kind == ZMPM_MODEL_STVK_HENCKY_ISOTROPIC || c.kind == ZMPM_MODEL_FIXED_COROTATED) {
+        // StvkWithHenckyIsotropic::firstPiolaDifferential, StvkWithHenckyIsotropic.h:164-170
+        M3<T> D = mul(Tmul(s.U, dF), s.V);
+        M3<T> K;
+        isotropicContract(s, D, K);
+        return mulT(mul(s.U, K), s.V);
+    }
+    return M3<T>::zero();
+}
+
+// ------------------------------------------------------------ plasticity --
+template <class T>
+struct Plastic {
+    int32_t kind = ZMPM_PLASTIC_NONE;
+    T yield_stress = 0, xi = 0, fail_stress = 0;
+    int32_t broken = 0;
+    T crack_normal[3] = { 0, 0, 0 };
+};
+
+// VonMisesStvkHencky::projectStrain, PlasticityApplier.cpp:462-502
+template <class T>
+static void vonMisesProject(const Model<T>& c, Plastic<T>& p, M3<T>& F)
+{
+    M3<T> U, V;
+    T sigma[3];
+    svd3(F, U, sigma, V);
+    T eps[3];
+    for (int d = 0; d < 3; ++d) eps[d] = std::log(std::max(sigma[d], T(1e-4)));
+    T tr = eps[0] + eps[1] + eps[2];
+    T hat[3];
+    for (int d = 0; d < 3; ++d) hat[d] = eps[d] - (tr / T(3)) * T(1);
+    T hat2 = hat[0] * hat[0] + hat[1] * hat[1] + hat[2] * hat[2];
+    T hat_norm = std::sqrt(hat2);
+    T delta_gamma = hat_norm - p.yield_stress / (2 * c.mu);
+    if (delta_gamma <= 0) return;
+    p.yield_stress -= p.xi * delta_gamma;
+    T H[3], expH[3];
+    for (int d = 0; d < 3; ++d) H[d] = eps[d] - (delta_gamma / hat_norm) * hat[d];
+    T tau_0 = 2 * c.mu * H[0] + c.lambda * (H[0] + H[1] + H[2]);
+    for (int d = 0; d < 3; ++d) expH[d] = std::exp(H[d]);
+    F = udiagvt(U, expH, V);
+    if (tau_0 >= p.fail_stress) {
+        p.broken = 1;
+        for (int d = 0; d < 3; ++d) p.crack_normal[d] = V.a[d][0];
+    }
+}
+
+// ------------------------------------------------------------- colliders --
+template <class T>
+struct Collider {
+    zmpm_collider d;
+    // state at the current time (updateState)
+    T R[3][3];
+    T omega[3];
+    T b[3], dbdt[3];
+    T s = 1, dsdt = 0;
+
+    void setRotation()
+    {
+        T w = (T)d.rotation[0], x = (T)d.rotation[1], y = (T)d.rotation[2], z = (T)d.rotation[3];
+        T n = std::sqrt(w * w + x * x + y * y + z * z);
+        if (n == 0) {
+            w = 1;
+            x = y = z = 0;
+            n = 1;
+        }
+        w /= n;
+        x /= n;
+        y /= n;
+        z /= n;
+        R[0][0] = 1 - 2 * (y * y + z * z);
+        R[0][1] = 2 * (x * y - w * z);
+        R[0][2] = 2 * (x * z + w * y);
+        R[1][0] = 2 * (x * y + w * z);
+        R[1][1] = 1 - 2 * (x * x + z * z);
+        R[1][2] = 2 * (y * z - w * x);
+        R[2][0] = 2 * (x * z - w * y);
+        R[2][1] = 2 * (y * z + w * x);
+        R[2][2] = 1 - 2 * (x * x + y * y);
+    }
+    void update(double time)
+    {
+        setRotation();
+        for (int i = 0; i < 3; ++i) {
+            omega[i] = (T)d.angular_velocity[i];
+            b[i] = (T)(d.translation[i] + time * d.translation_velocity[i]);
+            dbdt[i] = (T)d.translation_velocity[i];
+        }
+        s = (T)(d.scale + time * d.scale_velocity);
+        dsdt = (T)d.scale_velocity;
+    }
+    // AnalyticLevelSet::queryInside for the three shapes (AnalyticLevelSet.cpp:111-119, 272-287, 435-451, 504-539)
+    bool queryInside(const T X[3], T N[3]) const
+    {
+        if (d.shape == ZMPM_HALF_SPACE) {
+            T n[3] = { (T)d.b[0], (T)d.b[1], (T)d.b[2] };
+            T nn = std::sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
+            for (int i = 0; i < 3; ++i) n[i] /= nn;
+            T phi = n[0] * (X[0] - (T)d.a[0]) + n[1] * (X[1] - (T)d.a[1]) + n[2] * (X[2] - (T)d.a[2]);
+            if (phi <= 0) {
+                for (int i = 0; i < 3; ++i) N[i] = n[i];
+                return true;
+            }
+            return false;
+        }
+        if (d.shape == ZMPM_SPHERE) {
+            T tc[3] = { X[0] - (T)d.a[0], X[1] - (T)d.a[1], X[2] - (T)d.a[2] };
+            T d2 = tc[0] * tc[0] + tc[1] * tc[1] + tc[2] * tc[2];
+            T r = (T)d.radius;
+            if (d2 < r * r) {
+                T dist = std::sqrt(d2);
+                if (dist < T(1e-7)) {
+                    N[0] = 1;
+                    N[1] = N[2] = 0;
+                }
+                else
+                    for (int i = 0; i < 3; ++i) N[i] = (1 / dist) * tc[i];
+                return true;
+            }
+            return false;
+        }
+        // axis-aligned box: half edges h, centre c, signed distance
+        // min(max_i d_i, 0) + |max(d, 0)| with d_i = |X_i - c_i| - h_i
+        T h[3], ctr[3], xp[3], dd[3];
+        for (int i = 0; i < 3; ++i) {
+            h[i] = ((T)d.b[i] - (T)d.a[i]) / T(2);
+            ctr[i] = ((T)d.a[i] + (T)d.b[i]) / T(2);
+            xp[i] = X[i] - ctr[i];
+            dd[i] = std::fabs(xp[i]) - h[i];
+        }
+        int imax = 0;
+        for (int i = 1; i < 3; ++i)
+            if (dd[i] > dd[imax]) imax = i;
+        T q2 = 0;
+        for (int i = 0; i < 3; ++i) {
+            T q = dd[i] > 0 ? dd[i] : T(0);
+            q2 += q * q;
+        }
+        T phi = std::min(dd[imax], T(0)) + std::sqrt(q2);
+        if (phi > 0) return false;
+        for (int i = 0; i < 3; ++i) N[i] = 0;
+        N[imax] = xp[imax] >= 0 ? T(1) : T(-1);
+        return true;
+    }
+    // AnalyticCollisionObject::detectAndResolveCollision, CollisionObject.cpp:340-400
+    bool detectAndResolve(const T x[3], T v[3], T n[3]) const
+    {
+        if (d.type == ZMPM_GHOST) return false;
+        T xb[3] = { x[0] - b[0], x[1] - b[1], x[2] - b[2] };
+        T one_over_s = 1 / s;
+        T X[3];
+        for (int i = 0; i < 3; ++i) X[i] = (R[0][i] * xb[0] + R[1][i] * xb[1] + R[2][i] * xb[2]) * one_over_s;
+        T N[3];
+        if (!queryInside(X, N)) return false;
+        T vo[3];
+        vo[0] = omega[1] * xb[2] - omega[2] * xb[1];
+        vo[1] = omega[2] * xb[0] - omega[0] * xb[2];
+        vo[2] = omega[0] * xb[1] - omega[1] * xb[0];
+        for (int i = 0; i < 3; ++i) vo[i] += (dsdt * one_over_s) * xb[i] + dbdt[i];
+        for (int i = 0; i < 3; ++i) v[i] -= vo[i];
+        if (d.type == ZMPM_STICKY) {
+            v[0] = v[1] = v[2] = 0;
+        }
+        else {
+            for (int i = 0; i < 3; ++i) n[i] = R[i][0] * N[0] + R[i][1] * N[1] + R[i][2] * N[2];
+            T dot = v[0] * n[0] + v[1] * n[1] + v[2] * n[2];
+            if (d.type == ZMPM_SLIP || dot < 0) {
+                for (int i = 0; i < 3; ++i) v[i] -= n[i] * dot;
+                T fr = (T)d.friction;
+                if (fr != 0 && dot < 0) {
+                    T vn = std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+                    if (-dot * fr < vn)
+                        for (int i = 0; i < 3; ++i) v[i] += v[i] / vn * dot * fr;
+                    else
+                        v[0] = v[1] = v[2] = 0;
+                }
+            }
+        }
+        for (int i = 0; i < 3; ++i) v[i] += vo[i];
+        return true;
+    }
+};
+
+// AnalyticCollisionObject::multiObjectCollision, CollisionObject.cpp:66-105
+template <class T>
+static bool multiObjectCollision(const std::vector<Collider<T>>& objs, const T x[3], T v[3], M3<T>& K)
+{
+    bool any = false;
+    int slip = 0;
+    K = M3<T>::zero();
+    for (const auto& o : objs) {
+        if (o.d.type == ZMPM_GHOST) continue;
+        T n[3] = { 0, 0, 0 };
+        bool col = o.detectAndResolve(x, v, n);
+        any = col || any;
+        if (!col) continue;
+        if (o.d.type == ZMPM_STICKY) {
+            K = M3<T>::identity();
+            break;
+        }
+        for (int c = 0; c < slip; ++c) {
+            T dot = K.a[0][c] * n[0] + K.a[1][c] * n[1] + K.a[2][c] * n[2];
+            for (int i = 0; i < 3; ++i) n[i] -= dot * K.a[i][c];
+        }
+        T len = std::sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
+        if (len) {
+            for (int i = 0; i < 3; ++i) K.a[i][slip] = n[i] / len;
+            if (++slip == 3) break;
+        }
+    }
+    return any;
+}
+
+// ---------------------------------------------------------------- B-spline --
+// Quadratic B-spline, BSplines.h:16-29,55-81, MathTools.h:15-25; the stencil
+// loop order and products of MpmGrid::iterateKernel (MpmGrid.h:220-271).
+static inline int int_floor(double x)
+{
+    int i = (int)x;
+    return i - (i > x);
+}
+static inline int int_floor(float x)
+{
+    int i = (int)x;
+    return i - (i > x);
+}
+template <class T>
+struct Spline {
+    T w[3][3], dw[3][3];
+    int base[3];
+    T one_over_dx;
+    Spline(const T X[3], T dx)
+    {
+        one_over_dx = 1 / dx;
+        for (int d = 0; d < 3; ++d) {
+            T x = one_over_dx * X[d];
+            base[d] = int_floor(x - T(0.5));
+            T d0 = x - base[d];
+            T z = T(1.5) - d0;
+            w[d][0] = T(0.5) * z * z;
+            T d1 = d0 - 1;
+            w[d][1] = T(0.75) - d1 * d1;
+            T d2 = 1 - d1;
+            T zz = T(1.5) - d2;
+            w[d][2] = T(0.5) * zz * zz;
+            dw[d][0] = -z;
+            dw[d][1] = -T(2) * d1;
+            dw[d][2] = zz;
+        }
+    }
+};
+
+// ----------------------------------------------------------------- sim ----
+template <class T>
+struct Sim {
+    using G = GridState<T>;
+    Mask mask;
+    double dx_d;
+    T dx, gravity[3], apic_rpic_ratio, cfl;
+    double time = 0;
+
+    // particles, in the order they were added
+    int64_t P = 0;
+    std::vector<T> X, V, Cm, F, Fn, mass, vol;
+    std::vector<Model<T>> model;
+    std::vector<Plastic<T>> plastic;
+    std::vector<Scratch<T>> scratch;
+    std::vector<M3<T>> gradV, stress;
+    std::vector<Collider<T>> colliders;
+
+    // binning
+    std::vector<u64> sorter, base_offset;
+    std::vector<int32_t> order;
+    std::vector<std::pair<int, int>> group;
+    std::vector<u64> block_offset;
+    std::vector<u64> blocks;
+    VMem grid, pagemap;
+    size_t pagemap_bytes = 0;
+    int64_t N = 0;
+
+    // Newton objective
+    T dt = 0;
+    std::vector<T> mvec, dv, vn; // [N], [N*3], [N*3]
+    std::vector<uint8_t> collided;
+    std::vector<M3<T>> proj;
+    bool implicit_ready = false;
+    std::string err;
+
+    explicit Sim(int l2s) : mask(l2s) {}
+    ~Sim()
+    {
+        grid.unmap();
+        pagemap.unmap();
+    }
+
+    bool init(const zmpm_config& c)
+    {
+        dx_d = c.dx;
+        dx = (T)c.dx;
+        for (int d = 0; d < 3; ++d) gravity[d] = (T)c.gravity[d];
+        apic_rpic_ratio = (T)c.apic_rpic_ratio;
+        cfl = (T)c.cfl;
+        // SPGrid allocator over 4096^3 nodes (MpmGrid.h:83-111)
+        size_t elems = (size_t)1 << 36;
+        if (!grid.map(elems * sizeof(G))) return false;
+        pagemap_bytes = ((elems >> mask.block_bits) + 63) / 64 * 8;
+        return pagemap.map(pagemap_bytes);
+    }
+
+    G& at(u64 offset) const { return *reinterpret_cast<G*>(reinterpret_cast<char*>(grid.p) + offset); }
+
+    template <class F_>
+    void iterateKernel(const Spline<T>& sp, u64 base, F_&& f) const
+    {
+        for (int i = 0; i < 3; ++i) {
+            T wi = sp.w[0][i];
+            T dwidxi = sp.one_over_dx * sp.dw[0][i];
+            for (int j = 0; j < 3; ++j) {
+                T wj = sp.w[1][j];
+                T wij = wi * wj;
+                T dwijdxi = dwidxi * wj;
+                T dwijdxj = wi * sp.one_over_dx * sp.dw[1][j];
+                for (int k = 0; k < 3; ++k) {
+                    T wk = sp.w[2][k];
+                    T wijk = wij * wk;
+                    T dw[3] = { dwijdxi * wk, dwijdxj * wk, wij * sp.one_over_dx * sp.dw[2][k] };
+                    int node[3] = { sp.base[0] + i, sp.base[1] + j, sp.base[2] + k };
+                    G& g = at(mask.packed_add(base, mask.stencil[9 * i + 3 * j + k]));
+                    f(node, wijk, dw, g);
+                }
+            }
+        }
+    }
+
+    // iterateGrid / iterateTouchedGrid, MpmGrid.h:139-218
+    template <class F_>
+    void iterateBlocks(bool active_only, F_&& f)
+    {
+        const int bxn = mask.bx(), byn = mask.by(), bzn = mask.bz();
+#pragma omp parallel for schedule(static)
+        for (int64_t b = 0; b < (int64_t)blocks.size(); ++b) {
+            u64 base = blocks[b];
+            int bc[3];
+            mask.coord(base, bc);
+            for (int i = 0; i < bxn; ++i)
+                for (int j = 0; j < byn; ++j)
+                    for (int k = 0; k < bzn; ++k) {
+                        G& g = at(mask.packed_add(base, mask.linear_offset(i, j, k)));
+                        if (active_only && g.idx < 0) continue;
+                        int node[3] = { bc[0] + i, bc[1] + j, bc[2] + k };
+                        f(node, g);
+                    }
+        }
+    }
+
+    // --------------------------------------------------------- binning --
+    // MpmSimulationBase::sortParticlesAndPolluteGrid, MpmSimulationBase.cpp:1032-1103
+    int sortParticlesAndPolluteGrid()
+    {
+        const int index_bits = 32 - mask.block_bits;
+        if (P >= ((int64_t)1 << index_bits)) {
+            err = "too many particles for the key encoding";
+            return ZMPM_BAD_ARG;
+        }
+        sorter.resize(P);
+        base_offset.resize(P);
+        order.resize(P);
+        T one_over_dx = T(1) / dx;
+        int bad = 0;
+#pragma omp parallel for reduction(| : bad)
+        for (int64_t i = 0; i < P; ++i) {
+            int b[3];
+            for (int d = 0; d < 3; ++d) b[d] = int_floor(X[3 * i + d] * one_over_dx - T(0.5));
+            for (int d = 0; d < 3; ++d) bad |= (b[d] < 0 || b[d] > 4096 - 16);
+            u64 off = mask.linear_offset(b[0], b[1], b[2]);
+            sorter[i] = ((off >> mask.log2_struct) << index_bits) + (u64)i;
+        }
+        if (bad) {
+            err = "particle outside the SPGrid domain";
+            return ZMPM_OUT_OF_GRID;
+        }
+        __gnu_parallel::sort(sorter.begin(), sorter.end());
+        group.clear();
+        block_offset.clear();
+        int last = 0;
+        for (int64_t i = 0; i < P; ++i)
+            if (i == P - 1 || (sorter[i] >> 32) != (sorter[i + 1] >> 32)) {
+                group.emplace_back(last, (int)i);
+                block_offset.push_back(sorter[i] >> 32);
+                last = (int)i + 1;
+            }
+        // page map: Clear re-maps the bitmap (SPGrid_Page_Map.h:38-43)
+        pagemap.unmap();
+        if (!pagemap.map(pagemap_bytes)) return ZMPM_NO_MEMORY;
+        blocks.clear();
+        u64* pm = static_cast<u64*>(pagemap.p);
+        auto set_page = [&](u64 off) { // Set_Page, SPGrid_Page_Map.h:61-70
+            u64 m = 1ull << ((off >> 12) & 0x3f);
+            u64& e = pm[off >> 18];
+            if (m & ~e) {
+                e |= m;
+                blocks.push_back((off >> 12) << 12);
+            }
+        };
+        const int bxn = mask.bx(), byn = mask.by(), bzn = mask.bz();
+        for (int64_t i = 0; i < P; ++i) {
+            order[i] = (int32_t)(sorter[i] & ((1ull << index_bits) - 1));
+            u64 off = (sorter[i] >> index_bits) << mask.log2_struct;
+            base_offset[order[i]] = off;
+            if (i == P - 1 || (sorter[i] >> 32) != (sorter[i + 1] >> 32)) {
+                set_page(off);
+                for (int a = 0; a < 2; ++a)
+                    for (int b = 0; b < 2; ++b)
+                        for (int c = 0; c < 2; ++c) set_page(mask.packed_add(off, mask.linear_offset(bxn * a, byn * b, bzn * c)));
+            }
+        }
+        const int epb = mask.elements();
+#pragma omp parallel for schedule(static)
+        for (int64_t b = 0; b < (int64_t)blocks.size(); ++b) {
+            G* g = &at(blocks[b]);
+            std::memset(g, 0, 4096);
+            for (int e = 0; e < epb; ++e) g[e].idx = -1;
+        }
+        return ZMPM_OK;
+    }
+
+    // MpmGrid::getNumNodes, MpmGrid.h:123-136
+    int64_t getNumNodes()
+    {
+        int64_t n = 0;
+        const int epb = mask.elements();
+        for (size_t b = 0; b < blocks.size(); ++b) {
+            G* g = &at(blocks[b]);
+            for (int e = 0; e < epb; ++e)
+                if (g[e].m != 0) g[e].idx = n++;
+        }
+        return n;
+    }
+
+    template <class F_>
+    void coloredGroups(F_&& f)
+    {
+        for (u64 color = 0; color < 8; ++color) {
+#pragma omp parallel for schedule(dynamic, 1)
+            for (int64_t gi = 0; gi < (int64_t)group.size(); ++gi) {
+                if ((block_offset[gi] & 7) != color) continue;
+                for (int idx = group[gi].first; idx <= group[gi].second; ++idx) f(order[idx]);
+            }
+        }
+    }
+
+    // ------------------------------------------------------------- P2G --
+    // particlesToGridHelper<APIC,deg2>, MpmSimulationBase.cpp:563-608, and the
+    // normalisation of particlesToGrid, :474-485
+    void particlesToGrid()
+    {
+        coloredGroups([&](int i) {
+            const T* Xp = &X[3 * i];
+            T m = mass[i];
+            T mom[3] = { m * V[3 * i], m * V[3 * i + 1], m * V[3 * i + 2] };
+            T C[3][3];
+            for (int r = 0; r < 3; ++r)
+                for (int c = 0; c < 3; ++c) C[r][c] = m * Cm[9 * i + 3 * r + c];
+            Spline<T> sp(Xp, dx);
+            iterateKernel(sp, base_offset[i], [&](const int node[3], T w, const T*, G& g) {
+                T xi[3];
+                for (int d = 0; d < 3; ++d) xi[d] = node[d] * dx - Xp[d];
+                for (int r = 0; r < 3; ++r) g.v[r] += (C[r][0] * xi[0] + C[r][1] * xi[1] + C[r][2] * xi[2] + mom[r]) * w;
+                g.m += m * w;
+            });
+        });
+        N = getNumNodes();
+        iterateBlocks(true, [&](const int*, G& g) {
+            for (int d = 0; d < 3; ++d) g.v[d] /= g.m;
+        });
+    }
+
+    // ----------------------------------------------------- Newton setup --
+    // startBackwardEuler + buildMassMatrix + buildInitialDvAndVnForNewton,
+    // MpmSimulationBase.cpp:610-633, 793-802, 1105-1136
+    void startBackwardEuler()
+    {
+        mvec.assign(N, 0);
+        dv.assign(3 * N, 0);
+        vn.assign(3 * N, 0);
+        collided.assign(N, 0);
+        proj.assign(N, M3<T>::identity());
+        for (auto& c : colliders) c.update(time);
+        iterateBlocks(true, [&](const int node[3], G& g) {
+            int64_t id = g.idx;
+            mvec[id] = g.m;
+            T vi[3] = { g.v[0], g.v[1], g.v[2] };
+            T xi[3] = { node[0] * dx, node[1] * dx, node[2] * dx };
+            M3<T> K;
+            bool any = multiObjectCollision(colliders, xi, vi, K);
+            if (any) {
+                collided[id] = 1;
+                M3<T> P = M3<T>::identity();
+                M3<T> KK = mulT(K, K);
+                for (int r = 0; r < 3; ++r)
+                    for (int c = 0; c < 3; ++c) P.a[r][c] -= KK.a[r][c];
+                proj[id] = P;
+                for (int d = 0; d < 3; ++d) dv[3 * id + d] = vi[d] - g.v[d];
+            }
+            else
+                for (int d = 0; d < 3; ++d) dv[3 * id + d] = gravity[d] * dt;
+            for (int d = 0; d < 3; ++d) vn[3 * id + d] = g.v[d];
+        });
+        Fn = F; // backupStrain
+        implicit_ready = true;
+    }
+
+    void project(std::vector<T>& v) const
+    {
+#pragma omp parallel for schedule(static)
+        for (int64_t i = 0; i < N; ++i) {
+            if (!collided[i]) continue;
+            const M3<T>& Pm = proj[i];
+            T a = v[3 * i], b = v[3 * i + 1], c = v[3 * i + 2];
+            for (int r = 0; r < 3; ++r) v[3 * i + r] = Pm.a[r][0] * a + Pm.a[r][1] * b + Pm.a[r][2] * c;
+        }
+    }
+
+    // evalInterpolantAndGradient, MpmForceBase.cpp:213-244 (gradient only;
+    // the interpolated value is not used on the implicit path)
+    void evalGradient(const std::vector<T>& field, bool add_vn, std::vector<M3<T>>& grad)
+    {
+        iterateBlocks(false, [&](const int*, G& g) {
+            g.new_v[0] = g.new_v[1] = g.new_v[2] = 0;
+        });
+        iterateBlocks(true, [&](const int*, G& g) {
+            int64_t id = g.idx;
+            for (int d = 0; d < 3; ++d) g.new_v[d] = (add_vn ? vn[3 * id + d] : T(0)) + field[3 * id + d];
+        });
+        grad.resize(P);
+#pragma omp parallel for schedule(static)
+        for (int64_t i = 0; i < P; ++i) {
+            M3<T> gr = M3<T>::zero();
+            Spline<T> sp(&X[3 * i], dx);
+            iterateKernel(sp, base_offset[i], [&](const int*, T, const T* dw, G& g) {
+                for (int r = 0; r < 3; ++r)
+                    for (int c = 0; c < 3; ++c) gr.a[r][c] += g.new_v[r] * dw[c];
+            });
+            grad[i] = gr;
+        }
+    }
+
+    // rasterizeForceToTVStack<false>, MpmForceBase.cpp:102-152
+    void rasterize(T scale, const std::vector<M3<T>>& S, std::vector<T>& out)
+    {
+        iterateBlocks(true, [&](const int*, G& g) {
+            g.new_v[0] = g.new_v[1] = g.new_v[2] = 0;
+        });
+        coloredGroups([&](int i) {
+            const M3<T>& s = S[i];
+            Spline<T> sp(&X[3 * i], dx);
+            iterateKernel(sp, base_offset[i], [&](const int*, T, const T* dw, G& g) {
+                for (int r = 0; r < 3; ++r) {
+                    T delta = s.a[r][0] * dw[0] + s.a[r][1] * dw[1] + s.a[r][2] * dw[2];
+                    g.new_v[r] -= scale * delta;
+                }
+            });
+        });
+        iterateBlocks(true, [&](const int*, G& g) {
+            for (int d = 0; d < 3; ++d) out[3 * g.idx + d] += g.new_v[d];
+        });
+    }
+
+    // updateState -> MpmForceBase::updatePositionBasedState, MpmForceBase.cpp:306-344
+    // (G2P of vn+dv, F=(I+dt gradV)Fn, scratch, stress V0 P Fn^T)
+    void updateState(const std::vector<T>& dvin)
+    {
+        evalGradient(dvin, true, gradV);
+        stress.resize(P);
+        scratch.resize(P);
+#pragma omp parallel for schedule(static)
+        for (int64_t i = 0; i < P; ++i) {
+            M3<T> Fnp = load9(Fn, i);
+            M3<T> A = M3<T>::identity();
+            for (int r = 0; r < 3; ++r)
+                for (int c = 0; c < 3; ++c) A.a[r][c] += dt * gradV[i].a[r][c];
+            M3<T> Fp = mul(A, Fnp);
+            store9(F, i, Fp);
+            if (model[i].kind == ZMPM_MODEL_NONE) {
+                stress[i] = M3<T>::zero();
+                continue;
+            }
+            updateScratch(model[i], Fp, scratch[i]);
+            M3<T> Pp = firstPiola(model[i], scratch[i]);
+            stress[i] = mulT(scaled(Pp, vol[i]), Fnp);
+        }
+    }
+
+    // computeResidual + computeNorm, BackwardEuler.h:101-140
+    T computeResidual(std::vector<T>& r)
+    {
+        r.assign(3 * N, 0);
+        for (int64_t i = 0; i < N; ++i)
+            for (int d = 0; d < 3; ++d) r[3 * i + d] = dt * gravity[d] * mvec[i];
+        rasterize(dt, stress, r);
+        for (int64_t i = 0; i < N; ++i) // MassLumpedInertia::addScaledForces, Inertia.cpp:32-41
+            for (int d = 0; d < 3; ++d) r[3 * i + d] -= (dt / dt) * mvec[i] * dv[3 * i + d];
+        project(r);
+        return computeNorm(r);
+    }
+
+    T reduce(const std::function<T(int64_t)>& term) const
+    {
+        const int64_t chunk = 256;
+        int64_t nch = (N + chunk - 1) / chunk;
+        std::vector<T> part(nch, 0);
+#pragma omp parallel for schedule(static)
+        for (int64_t c = 0; c < nch; ++c) {
+            T s = 0;
+            for (int64_t i = c * chunk; i < std::min(N, (c + 1) * chunk); ++i) s += term(i);
+            part[c] = s;
+        }
+        T s = 0;
+        for (T v : part) s += v;
+        return s;
+    }
+    T computeNorm(const std::vector<T>& r) const
+    {
+        return std::sqrt(reduce([&](int64_t i) {
+            return (r[3 * i] * r[3 * i] + r[3 * i + 1] * r[3 * i + 1] + r[3 * i + 2] * r[3 * i + 2]) / mvec[i];
+        }));
+    }
+    T dot(const std::vector<T>& a, const std::vector<T>& b) const
+    {
+        return reduce([&](int64_t i) { return a[3 * i] * b[3 * i] + a[3 * i + 1] * b[3 * i + 1] + a[3 * i + 2] * b[3 * i + 2]; });
+    }
+
+    // multiply, BackwardEuler.h:322-351: b = M x + dt^2 sum dS grad w
+    int64_t hvp_count = 0;
+    void multiply(const std::vector<T>& x, std::vector<T>& b)
+    {
+        hvp_count++;
+        b.assign(3 * N, 0);
+        T scale = -(dt * dt);
+        T iscale = scale / (dt * dt);
+        for (int64_t i = 0; i < N; ++i)
+            for (int d = 0; d < 3; ++d) b[3 * i + d] -= iscale * mvec[i] * x[3 * i + d];
+        std::vector<M3<T>> gdv;
+        evalGradient(x, false, gdv);
+        std::vector<M3<T>> dS(P);
+#pragma omp parallel for schedule(static)
+        for (int64_t i = 0; i < P; ++i) {
+            if (model[i].kind == ZMPM_MODEL_NONE) {
+                dS[i] = M3<T>::zero();
+                continue;
+            }
+            M3<T> Fnp = load9(Fn, i);
+            M3<T> dP = firstPiolaDifferential(model[i], scratch[i], mul(gdv[i], Fnp));
+            dS[i] = mulT(scaled(dP, vol[i]), Fnp);
+        }
+        rasterize(scale, dS, b);
+    }
+    void precondition(const std::vector<T>& in, std::vector<T>& out) const
+    {
+        out.resize(3 * N);
+        for (int64_t i = 0; i < N; ++i)
+            for (int d = 0; d < 3; ++d) out[3 * i + d] = in[3 * i + d] / mvec[i];
+    }
+
+    // Minres::solve, Minres.h:69-149 (x starts at zero, so A x = 0 is not evaluated)
+    int minres(std::vector<T>& x, const std::vector<T>& b, T rel_tol, T abs_tol, int max_it)
+    {
+        std::vector<T> mk(3 * N, 0), mkm1(3 * N, 0), mkm2(3 * N, 0), z(3 * N, 0), qkm1(3 * N, 0), qk(3 * N, 0), qkp1;
+        T g_c[3] = { 1, 1, 1 }, g_s[3] = { 0, 0, 0 }; // Gk, Gkm1, Gkm2
+        T gamma = 0, delta = 0, epsilon = 0, beta_kp1 = 0, alpha_k = 0, beta_k = 0, tk = 0;
+        qkp1 = b;
+        project(qkp1);
+        precondition(qkp1, z);
+        T rnorm = std::sqrt(dot(z, qkp1));
+        beta_kp1 = rnorm;
+        T local_tol = std::min(rel_tol * rnorm, abs_tol);
+        if (rnorm < local_tol) return 0;
+        if (rnorm > 0)
+            for (int64_t i = 0; i < 3 * N; ++i) {
+                qkp1[i] /= beta_kp1;
+                z[i] /= beta_kp1;
+            }
+        T rhs0 = rnorm, rhs1 = 0;
+        for (int k = 0; k < max_it; ++k) {
+            if (rnorm < local_tol) return k;
+            mkm2.swap(mkm1);
+            mkm1.swap(mk);
+            mk = z;
+            beta_k = beta_kp1;
+            qkm1.swap(qkp1);
+            qkm1.swap(qk);
+            multiply(mk, qkp1);
+            project(qkp1);
+            alpha_k = dot(mk, qkp1);
+            for (int64_t i = 0; i < 3 * N; ++i) qkp1[i] -= alpha_k * qk[i];
+            for (int64_t i = 0; i < 3 * N; ++i) qkp1[i] -= beta_k * qkm1[i];
+            precondition(qkp1, z);
+            beta_kp1 = std::sqrt(std::max(T(0), dot(z, qkp1)));
+            if (beta_kp1 > 0)
+                for (int64_t i = 0; i < 3 * N; ++i) {
+                    qkp1[i] /= beta_kp1;
+                    z[i] /= beta_kp1;
+                }
+            // applyAllPreviousGivensRotationsAndDetermineNewGivens, Minres.h:151-175
+            g_c[2] = g_c[1];
+            g_s[2] = g_s[1];
+            g_c[1] = g_c[0];
+            g_s[1] = g_s[0];
+            T e0 = 0, e1 = beta_k; // Gkm2 row rotation of (0, beta_k)
+            {
+                T t1 = e0, t2 = e1;
+                e0 = g_c[2] * t1 - g_s[2] * t2;
+                e1 = g_s[2] * t1 + g_c[2] * t2;
+            }
+            epsilon = e0;
+            T d0 = e1, d1 = alpha_k;
+            {
+                T t1 = d0, t2 = d1;
+                d0 = g_c[1] * t1 - g_s[1] * t2;
+                d1 = g_s[1] * t1 + g_c[1] * t2;
+            }
+            delta = d0;
+            T t0 = d1, tt1 = beta_kp1;
+            {
+                Givens<T> G(0, 1);
+                G.compute(t0, tt1);
+                g_c[0] = G.c;
+                g_s[0] = G.s;
+            }
+            {
+                T a1 = t0, a2 = tt1;
+                t0 = g_c[0] * a1 - g_s[0] * a2;
+            }
+            gamma = t0;
+            {
+                T a1 = rhs0, a2 = rhs1;
+                rhs0 = g_c[0] * a1 - g_s[0] * a2;
+                rhs1 = g_s[0] * a1 + g_c[0] * a2;
+            }
+            tk = rhs0;
+            T residual = rhs1;
+            rhs0 = residual;
+            rhs1 = 0;
+            rnorm = residual < 0 ? -residual : residual;
+            for (int64_t i = 0; i < 3 * N; ++i) mk[i] = (mk[i] - delta * mkm1[i] - epsilon * mkm2[i]) / gamma;
+            for (int64_t i = 0; i < 3 * N; ++i) x[i] += tk * mk[i];
+        }
+        return max_it;
+    }
+
+    // ConjugateGradient::solve, ConjugateGradient.h:99-147 (x starts at zero)
+    int cg(std::vector<T>& x, const std::vector<T>& b, T rel_tol, T abs_tol, int max_it)
+    {
+        std::vector<T> r = b, q, p, temp;
+        project(r);
+        precondition(r, q);
+        p = q;
+        T zTrk = dot(r, q);
+        T rnorm = std::sqrt(zTrk);
+        T local_tol = std::min(rel_tol * rnorm, abs_tol);
+        for (int cnt = 0; cnt < max_it; ++cnt) {
+            if (rnorm < local_tol) return cnt;
+            multiply(p, temp);
+            project(temp);
+            T alpha = zTrk / dot(temp, p);
+            for (int64_t i = 0; i < 3 * N; ++i) {
+                x[i] += p[i] * alpha;
+                r[i] -= temp[i] * alpha;
+            }
+            precondition(r, q);
+            T zTrk_last = zTrk;
+            zTrk = dot(q, r);
+            T beta = zTrk / zTrk_last;
+            for (int64_t i = 0; i < 3 * N; ++i) p[i] = q[i] + beta * p[i];
+            rnorm = std::sqrt(zTrk);
+        }
+        return max_it;
+    }
+
+    // NewtonsMethod::solve, NewtonsMethod.h:42-66
+    bool newton(const zmpm_solver& s, zmpm_stats& st)
+    {
+        std::vector<T> r, step;
+        bool first = true;
+        for (int it = 0; it < s.newton_max_iterations; ++it) {
+            updateState(dv);
+            T rn = computeResidual(r);
+            if (first) st.newton_residual_initial = (double)rn;
+            first = false;
+            st.newton_residual_final = (double)rn;
+            if (!(rn == rn)) st.status_flags |= 1;
+            if (rn < (T)s.newton_tolerance) return true;
+            T rel = std::min(T(0.5), (T)s.linear_solve_tolerance_scale * std::sqrt(std::max(rn, (T)s.newton_tolerance)));
+            step.assign(3 * N, 0);
+            int k = (s.linear_solver == ZMPM_CG)
+                ? cg(step, r, rel, (T)s.krylov_tolerance, s.krylov_max_iterations)
+                : minres(step, r, rel, (T)s.krylov_tolerance, s.krylov_max_iterations);
+            st.krylov_iterations += k;
+            st.newton_iterations += 1;
+            for (int64_t i = 0; i < 3 * N; ++i) dv[i] += step[i];
+        }
+        return false;
+    }
+
+    // ------------------------------------------------------------- G2P --
+    // constructNewVelocityFromNewtonResult + gridToParticlesHelper<APIC,deg2,!MLS>
+    // + evolveStrain + applyPlasticity, MpmSimulationBase.cpp:867-877, 906-1030
+    int gridToParticles()
+    {
+        iterateBlocks(false, [&](const int*, G& g) {
+            g.new_v[0] = g.new_v[1] = g.new_v[2] = 0;
+        });
+        iterateBlocks(true, [&](const int*, G& g) {
+            for (int d = 0; d < 3; ++d) g.new_v[d] = g.v[d] + dv[3 * g.idx + d];
+        });
+        T D_inverse = 4 / (dx * dx);
+        int too_fast = 0;
+        gradV.resize(P);
+#pragma omp parallel for schedule(static) reduction(| : too_fast)
+        for (int64_t i = 0; i < P; ++i) {
+            T* Xp = &X[3 * i];
+            T picV[3] = { 0, 0, 0 };
+            M3<T> Bp = M3<T>::zero(), gr = M3<T>::zero();
+            Spline<T> sp(Xp, dx);
+            iterateKernel(sp, base_offset[i], [&](const int node[3], T w, const T* dw, G& g) {
+                T xi[3];
+                for (int d = 0; d < 3; ++d) xi[d] = node[d] * dx - Xp[d];
+                for (int r = 0; r < 3; ++r) {
+                    picV[r] += w * g.new_v[r];
+                    for (int c = 0; c < 3; ++c) {
+                        Bp.a[r][c] += w * g.new_v[r] * xi[c];
+                        gr.a[r][c] += g.new_v[r] * dw[c];
+                    }
+                }
+            });
+            gradV[i] = gr;
+            for (int d = 0; d < 3; ++d) V[3 * i + d] = picV[d];
+            T a = (apic_rpic_ratio + 1) * T(0.5), bcoef = (apic_rpic_ratio - 1) * T(0.5);
+            for (int r = 0; r < 3; ++r)
+                for (int c = 0; c < 3; ++c) Cm[9 * i + 3 * r + c] = a * (Bp.a[r][c] * D_inverse) + bcoef * (Bp.a[c][r] * D_inverse);
+            T inc2 = 0;
+            for (int d = 0; d < 3; ++d) {
+                T inc = (T)dt * picV[d];
+                Xp[d] += inc;
+                inc2 += inc * inc;
+            }
+            too_fast |= (inc2 > dx * dx);
+        }
+        // evolveStrain with the G2P velocity gradient, FBasedMpmForceHelper.cpp:95-109
+#pragma omp parallel for schedule(static)
+        for (int64_t i = 0; i < P; ++i) {
+            if (model[i].kind == ZMPM_MODEL_NONE) continue;
+            M3<T> A = M3<T>::identity();
+            for (int r = 0; r < 3; ++r)
+                for (int c = 0; c < 3; ++c) A.a[r][c] += (T)dt * gradV[i].a[r][c];
+            M3<T> Fp = mul(A, load9(F, i));
+            if (plastic[i].kind == ZMPM_PLASTIC_VON_MISES) vonMisesProject(model[i], plastic[i], Fp);
+            store9(F, i, Fp);
+        }
+        return too_fast;
+    }
+
+    static M3<T> load9(const std::vector<T>& a, int64_t i)
+    {
+        M3<T> m;
+        for (int r = 0; r < 3; ++r)
+            for (int c = 0; c < 3; ++c) m.a[r][c] = a[9 * i + 3 * r + c];
+        return m;
+    }
+    static void store9(std::vector<T>& a, int64_t i, const M3<T>& m)
+    {
+        for (int r = 0; r < 3; ++r)
+            for (int c = 0; c < 3; ++c) a[9 * i + 3 * r + c] = m.a[r][c];
+    }
+
+    int beginImplicit(double dt_in)
+    {
+        dt = (T)dt_in;
+        implicit_ready = false;
+        int st = sortParticlesAndPolluteGrid();
+        if (st != ZMPM_OK) return st;
+        particlesToGrid();
+        startBackwardEuler();
+        return ZMPM_OK;
+    }
+
+    // MpmSimulationBase::advanceOneTimeStep (implicit), MpmSimulationBase.cpp:256-296
+    int substep(double dt_in, const zmpm_solver& s, zmpm_stats& st)
+    {
+        std::memset(&st, 0, sizeof(st));
+        hvp_count = 0;
+        int rc = beginImplicit(dt_in);
+        if (rc != ZMPM_OK) return rc;
+        bool conv = newton(s, st);
+        F = Fn; // restoreStrain
+        int too_fast = gridToParticles();
+        time += dt_in;
+        implicit_ready = false;
+        st.newton_converged = conv ? 1 : 0;
+        st.cfl_violation = too_fast;
+        st.hvp_count = (int32_t)hvp_count;
+        st.num_particles = P;
+        st.num_groups = (int64_t)group.size();
+        st.num_blocks = (int64_t)blocks.size();
+        st.num_nodes = N;
+        int64_t nc = 0;
+        for (auto c : collided) nc += c;
+        st.num_collision_nodes = nc;
+        if (st.status_flags & 1) return ZMPM_NAN_DETECTED;
+        return too_fast ? ZMPM_CFL_VIOLATION : ZMPM_OK;
+    }
+};
+
+// Type-erased handle over the float / double instantiations.
+struct Ctx {
+    zmpm_config cfg;
+    bool is_double = true;
+    std::unique_ptr<Sim<double>> d;
+    std::unique_ptr<Sim<float>> f;
+    std::string err;
+};
+
+} // namespace zo
+
+using zo::Ctx;
+
+#define DISPATCH(ctx, ...)               \
+    do {                                 \
+        if ((ctx)->is_double) {          \
+            auto& S = *(ctx)->d;         \
+            __VA_ARGS__;                 \
+        }                                \
+        else {                           \
+            auto& S = *(ctx)->f;         \
+            __VA_ARGS__;                 \
+        }                                \
+    } while (0)
+
+template <class SimT>
+static void add_particles_impl(SimT& S, int64_t n, const double* x, const double* v, const double* m, const double* vol)
+{
+    using T = typename std::remove_reference<decltype(S.dx)>::type;
+    for (int64_t i = 0; i < n; ++i) {
+        for (int d = 0; d < 3; ++d) {
+            S.X.push_back((T)x[3 * i + d]);
+            S.V.push_back(v ? (T)v[3 * i + d] : T(0));
+        }
+        for (int k = 0; k < 9; ++k) {
+            S.Cm.push_back(T(0));
+            S.F.push_back((k % 4 == 0) ? T(1) : T(0));
+        }
+        S.mass.push_back((T)m[i]);
+        S.vol.push_back((T)vol[i]);
+        S.model.emplace_back();
+        S.plastic.emplace_back();
+    }
+    S.P += n;
+    S.Fn = S.F;
+}
+
+extern "C" {
+
+// The oracle exports the same interface as include/zmpm.h with the prefix
+// zoracle_.  The config's precision picks the instantiation: ZMPM_FP64 ->
+// double with GridState<double> (2x4x4 pages); anything else -> float with
+// GridState<float> (4x4x4 pages), the reference's T=float build.
+int zoracle_create(const zmpm_config* cfg, Ctx** out)
+{
+    if (!cfg || !out || !(cfg->dx > 0)) return ZMPM_BAD_ARG;
+    auto* c = new (std::nothrow) Ctx();
+    if (!c) return ZMPM_NO_MEMORY;
+    c->cfg = *cfg;
+    c->is_double = (cfg->precision == ZMPM_FP64);
+    bool ok;
+    if (c->is_double) {
+        c->d.reset(new zo::Sim<double>(7));
+        ok = c->d->init(*cfg);
+    }
+    else {
+        c->f.reset(new zo::Sim<float>(6));
+        ok = c->f->init(*cfg);
+    }
+    if (!ok) {
+        delete c;
+        return ZMPM_NO_MEMORY;
+    }
+    *out = c;
+    return ZMPM_OK;
+}
+
+int zoracle_destroy(Ctx* c)
+{
+    delete c;
+    return ZMPM_OK;
+}
+
+const char* zoracle_last_error(const Ctx* c)
+{
+    if (!c) return "null context";
+    if (c->is_double) return c->d->err.c_str();
+    return c->f->err.c_str();
+}
+
+int zoracle_add_particles(Ctx* c, int64_t n, const double* x, const double* v, const double* m, const double* vol, int64_t* lower)
+{
+    if (!c || n < 0 || (n && (!x || !m || !vol))) return ZMPM_BAD_ARG;
+    DISPATCH(c, {
+        if (lower) *lower = S.P;
+        add_particles_impl(S, n, x, v, m, vol);
+    });
+    return ZMPM_OK;
+}
+
+int zoracle_add_fbased_force(Ctx* c, int64_t lo, int64_t hi, int32_t kind, double E, double nu)
+{
+    if (!c) return ZMPM_BAD_ARG;
+    DISPATCH(c, {
+        using T = typename std::remove_reference<decltype(S.dx)>::type;
+        if (lo < 0 || hi > S.P || lo > hi) return ZMPM_BAD_ARG;
+        T Et = (T)E, nut = (T)nu;
+        T lambda = Et * nut / ((T(1) + nut) * (T(1) - T(2) * nut));
+        T mu = Et / (T(2) * (T(1) + nut));
+        for (int64_t i = lo; i < hi; ++i) {
+            S.model[i].kind = kind;
+            S.model[i].mu = mu;
+            S.model[i].lambda = lambda;
+            S.model[i].kappa = (T)0.666666 * mu + lambda;
+            S.model[i].g = 1;
+        }
+    });
+    return ZMPM_OK;
+}
+
+int zoracle_set_lame(Ctx* c, int64_t lo, int64_t hi, const double* mu, const double* lambda)
+{
+    if (!c || !mu || !lambda) return ZMPM_BAD_ARG;
+    DISPATCH(c, {
+        using T = typename std::remove_reference<decltype(S.dx)>::type;
+        if (lo < 0 || hi > S.P || lo > hi) return ZMPM_BAD_ARG;
+        for (int64_t i = lo; i < hi; ++i) {
+            S.model[i].mu = (T)mu[i - lo];
+            S.model[i].lambda = (T)lambda[i - lo];
+            S.model[i].kappa = (T)0.666666 * S.model[i].mu + S.model[i].lambda;
+        }
+    });
+    return ZMPM_OK;
+}
+
+int zoracle_add_plasticity(Ctx* c, int64_t lo, int64_t hi, int32_t kind, double ys, double xi, double fs)
+{
+    if (!c) return ZMPM_BAD_ARG;
+    DISPATCH(c, {
+        using T = typename std::remove_reference<decltype(S.dx)>::type;
+        if (lo < 0 || hi > S.P || lo > hi) return ZMPM_BAD_ARG;
+        for (int64_t i = lo; i < hi; ++i) {
+            S.plastic[i].kind = kind;
+            S.plastic[i].yield_stress = (T)ys;
+            S.plastic[i].xi = (T)xi;
+            S.plastic[i].fail_stress = (T)fs;
+        }
+    });
+    return ZMPM_OK;
+}
+
+int zoracle_add_collision_object(Ctx* c, const zmpm_collider* o, int32_t* id)
+{
+    if (!c || !o) return ZMPM_BAD_ARG;
+    DISPATCH(c, {
+        using T = typename std::remove_reference<decltype(S.dx)>::type;
+        zo::Collider<T> col;
+        col.d = *o;
+        col.update(S.time);
+        if (id) *id = (int32_t)S.colliders.size();
+        S.colliders.push_back(col);
+    });
+    return ZMPM_OK;
+}
+
+int zoracle_set_collision_object(Ctx* c, int32_t id, const zmpm_collider* o)
+{
+    if (!c || !o) return ZMPM_BAD_ARG;
+    DISPATCH(c, {
+        if (id < 0 || id >= (int32_t)S.colliders.size()) return ZMPM_BAD_ARG;
+        S.colliders[id].d = *o;
+    });
+    return ZMPM_OK;
+}
+
+int zoracle_get_particles(Ctx* c, double* x, double* v, double* C, double* F)
+{
+    if (!c) return ZMPM_BAD_ARG;
+    DISPATCH(c, {
+        for (int64_t i = 0; i < 3 * S.P; ++i) {
+            if (x) x[i] = S.X[i];
+            if (v) v[i] = S.V[i];
+        }
+        for (int64_t i = 0; i < 9 * S.P; ++i) {
+            if (C) C[i] = S.Cm[i];
+            if (F) F[i] = S.F[i];
+        }
+    });
+    return ZMPM_OK;
+}
+
+int zoracle_set_particles(Ctx* c, const double* x, const double* v, const double* C, const double* F)
+{
+    if (!c) return ZMPM_BAD_ARG;
+    DISPATCH(c, {
+        using T = typename std::remove_reference<decltype(S.dx)>::type;
+        for (int64_t i = 0; i < 3 * S.P; ++i) {
+            if (x) S.X[i] = (T)x[i];
+            if (v) S.V[i] = (T)v[i];
+        }
+        for (int64_t i = 0; i < 9 * S.P; ++i) {
+            if (C) S.Cm[i] = (T)C[i];
+            if (F) S.F[i] = (T)F[i];
+        }
+    });
+    return ZMPM_OK;
+}
+
+int zoracle_get_plastic_state(Ctx* c, double* ys, int32_t* broken)
+{
+    if (!c) return ZMPM_BAD_ARG;
+    DISPATCH(c, {
+        for (int64_t i = 0; i < S.P; ++i) {
+            if (ys) ys[i] = S.plastic[i].yield_stress;
+            if (broken) broken[i] = S.plastic[i].broken;
+        }
+    });
+    return ZMPM_OK;
+}
+
+int64_t zoracle_num_particles(const Ctx* c)
+{
+    if (!c) return -1;
+    return c->is_double ? c->d->P : c->f->P;
+}
+
+double zoracle_time(const Ctx* c)
+{
+    if (!c) return 0;
+    return c->is_double ? c->d->time : c->f->time;
+}
+
+int zoracle_substep(Ctx* c, double dt, const zmpm_solver* s, zmpm_stats* st)
+{
+    if (!c || !s || !(dt > 0)) return ZMPM_BAD_ARG;
+    zmpm_stats local;
+    if (!st) st = &local;
+    int rc;
+    double t0 = omp_get_wtime();
+    DISPATCH(c, { rc = S.substep(dt, *s, *st); });
+    st->ms_total = (omp_get_wtime() - t0) * 1e3;
+    return rc;
+}
+
+int zoracle_bin(Ctx* c, int64_t* counts)
+{
+    if (!c) return ZMPM_BAD_ARG;
+    int rc;
+    DISPATCH(c, {
+        rc = S.sortParticlesAndPolluteGrid();
+        if (counts) {
+            counts[0] = S.P;
+            counts[1] = (int64_t)S.group.size();
+            counts[2] = (int64_t)S.blocks.size();
+        }
+    });
+    return rc;
+}
+
+int zoracle_bin_fetch(Ctx* c, zmpm_bin_result* out)
+{
+    if (!c || !out) return ZMPM_BAD_ARG;
+    DISPATCH(c, {
+        for (int64_t i = 0; i < S.P; ++i) {
+            if (out->particle_sorter) out->particle_sorter[i] = S.sorter[i];
+            if (out->particle_order) out->particle_order[i] = S.order[i];
+            if (out->particle_base_offset) out->particle_base_offset[i] = S.base_offset[i];
+        }
+        for (size_t g = 0; g < S.group.size(); ++g) {
+            if (out->particle_group) {
+                out->particle_group[2 * g] = S.group[g].first;
+                out->particle_group[2 * g + 1] = S.group[g].second;
+            }
+            if (out->block_offset) out->block_offset[g] = S.block_offset[g];
+        }
+        for (size_t b = 0; b < S.blocks.size(); ++b)
+            if (out->page_offsets) out->page_offsets[b] = S.blocks[b];
+    });
+    return ZMPM_OK;
+}
+
+int zoracle_begin_implicit(Ctx* c, double dt, int64_t* n)
+{
+    if (!c || !(dt > 0)) return ZMPM_BAD_ARG;
+    int rc;
+    DISPATCH(c, {
+        rc = S.beginImplicit(dt);
+        if (n) *n = S.N;
+    });
+    return rc;
+}
+
+int zoracle_get_grid(Ctx* c, double* m, double* v, int32_t* coord)
+{
+    if (!c) return ZMPM_BAD_ARG;
+    DISPATCH(c, {
+        if (!S.implicit_ready) return ZMPM_NOT_READY;
+        S.iterateBlocks(true, [&](const int node[3], decltype(S.at(0))& g) {
+            int64_t id = g.idx;
+            if (m) m[id] = g.m;
+            for (int d = 0; d < 3; ++d) {
+                if (v) v[3 * id + d] = g.v[d];
+                if (coord) coord[3 * id + d] = node[d];
+            }
+        });
+    });
+    return ZMPM_OK;
+}
+
+int zoracle_get_initial_dv(Ctx* c, double* dv, int32_t* col)
+{
+    if (!c) return ZMPM_BAD_ARG;
+    DISPATCH(c, {
+        if (!S.implicit_ready) return ZMPM_NOT_READY;
+        for (int64_t i = 0; i < S.N; ++i) {
+            for (int d = 0; d < 3; ++d)
+                if (dv) dv[3 * i + d] = S.dv[3 * i + d];
+            if (col) col[i] = S.collided[i];
+        }
+    });
+    return ZMPM_OK;
+}
+
+int zoracle_residual(Ctx* c, const double* dvin, double* r, double* norm)
+{
+    if (!c || !dvin) return ZMPM_BAD_ARG;
+    DISPATCH(c, {
+        using T = typename std::remove_reference<decltype(S.dx)>::type;
+        if (!S.implicit_ready) return ZMPM_NOT_READY;
+        for (int64_t i = 0; i < 3 * S.N; ++i) S.dv[i] = (T)dvin[i];
+        S.updateState(S.dv);
+        std::vector<T> res;
+        T nr = S.computeResidual(res);
+        if (r)
+            for (int64_t i = 0; i < 3 * S.N; ++i) r[i] = res[i];
+        if (norm) *norm = nr;
+    });
+    return ZMPM_OK;
+}
+
+int zoracle_multiply(Ctx* c, const double* x, double* b, int32_t fp32)
+{
+    (void)fp32;
+    if (!c || !x || !b) return ZMPM_BAD_ARG;
+    DISPATCH(c, {
+        using T = typename std::remove_reference<decltype(S.dx)>::type;
+        if (!S.implicit_ready || S.scratch.size() != (size_t)S.P) return ZMPM_NOT_READY;
+        std::vector<T> xi(3 * S.N), bo;
+        for (int64_t i = 0; i < 3 * S.N; ++i) xi[i] = (T)x[i];
+        S.multiply(xi, bo);
+        for (int64_t i = 0; i < 3 * S.N; ++i) b[i] = bo[i];
+    });
+    return ZMPM_OK;
+}
+
+// Single-particle model evaluation for known-answer and FD tests:
+// given F (row-major), returns psi, P and dP:dF.
+int zoracle_model_eval(int32_t kind, double E, double nu, const double* F, const double* dF, double* psi_out, double* P_out, double* dP_out)
+{
+    zo::Model<double> c;
+    c.kind = kind;
+    c.lambda = E * nu / ((1 + nu) * (1 - 2 * nu));
+    c.mu = E / (2 * (1 + nu));
+    c.kappa = 0.666666 * c.mu + c.lambda;
+    zo::M3<double> Fm, dFm;
+    for (int r = 0; r < 3; ++r)
+        for (int k = 0; k < 3; ++k) {
+            Fm.a[r][k] = F[3 * r + k];
+            dFm.a[r][k] = dF ? dF[3 * r + k] : 0;
+        }
+    zo::Scratch<double> s;
+    zo::updateScratch(c, Fm, s);
+    if (psi_out) *psi_out = zo::psi(c, s);
+    zo::M3<double> P = zo::firstPiola(c, s), dP = zo::firstPiolaDifferential(c, s, dFm);
+    for (int r = 0; r < 3; ++r)
+        for (int k = 0; k < 3; ++k) {
+            if (P_out) P_out[3 * r + k] = P.a[r][k];
+            if (dP_out) dP_out[3 * r + k] = dP.a[r][k];
+        }
+    return ZMPM_OK;
+}
+
+// 3x3 SVD of the oracle (F = U diag(sigma) V^T), double or float.
+int zoracle_svd3(const double* F, double* U, double* sigma, double* V, int32_t fp32)
+{
+    if (fp32) {
+        zo::M3<float> A, Uf, Vf;
+        float s[3];
+        for (int i = 0; i < 9; ++i) A.a[i / 3][i % 3] = (float)F[i];
+        int it = zo::svd3(A, Uf, s, Vf);
+        for (int i = 0; i < 9; ++i) {
+            U[i] = Uf.a[i / 3][i % 3];
+            V[i] = Vf.a[i / 3][i % 3];
+        }
+        for (int d = 0; d < 3; ++d) sigma[d] = s[d];
+        return it;
+    }
+    zo::M3<double> A, Ud, Vd;
+    double s[3];
+    for (int i = 0; i < 9; ++i) A.a[i / 3][i % 3] = F[i];
+    int it = zo::svd3(A, Ud, s, Vd);
+    for (int i = 0; i < 9; ++i) {
+        U[i] = Ud.a[i / 3][i % 3];
+        V[i] = Vd.a[i / 3][i % 3];
+    }
+    for (int d = 0; d < 3; ++d) sigma[d] = s[d];
+    return it;
+}
+
+// Von Mises return map on one F (row-major, in place); returns the new yield stress.
+int zoracle_von_mises(int32_t kind, double E, double nu, double yield_stress, double xi, double* F, double* ys_out)
+{
+    zo::Model<double> c;
+    c.kind = kind;
+    c.lambda = E * nu / ((1 + nu) * (1 - 2 * nu));
+    c.mu = E / (2 * (1 + nu));
+    zo::Plastic<double> p;
+    p.kind = ZMPM_PLASTIC_VON_MISES;
+    p.yield_stress = yield_stress;
+    p.xi = xi;
+    p.fail_stress = 1e300;
+    zo::M3<double> Fm;
+    for (int i = 0; i < 9; ++i) Fm.a[i / 3][i % 3] = F[i];
+    zo::vonMisesProject(c, p, Fm);
+    for (int i = 0; i < 9; ++i) F[i] = Fm.a[i / 3][i % 3];
+    if (ys_out) *ys_out = p.yield_stress;
+    return ZMPM_OK;
+}
+
+// SPGrid helpers for the golden-vector tests.
+uint64_t zoracle_linear_offset(int32_t log2_struct, int32_t i, int32_t j, int32_t k)
+{
+    return zo::Mask(log2_struct).linear_offset(i, j, k);
+}
+uint64_t zoracle_packed_add(int32_t log2_struct, uint64_t a, uint64_t b)
+{
+    return zo::Mask(log2_struct).packed_add(a, b);
+}
+void zoracle_masks(int32_t log2_struct, uint64_t* xyz)
+{
+    zo::Mask m(log2_struct);
+    xyz[0] = m.xmask;
+    xyz[1] = m.ymask;
+    xyz[2] = m.zmask;
+}
+
+} // extern "C"

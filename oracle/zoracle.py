@@ -1,0 +1,44 @@
+"""TEST INFRASTRUCTURE: ctypes binding of the CPU oracle (oracle/build/libzmpm_oracle.so).
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU baseline use this.  The
+oracle exports the zmpm C ABI under the prefix ``zoracle_`` plus a few
+single-kernel helpers (SVD, model evaluation, return map, SPGrid masks).
+"""
+import ctypes as C
+import os
+import subprocess
+
+from ziran2019_b200 import abi
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "build", "libzmpm_oracle.so")
+_lib = None
+
+
+def build():
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        L = abi.Lib(LIB_PATH, "zoracle_", product=False)
+        d = L.dll
+        d.zoracle_model_eval.restype = C.c_int
+        d.zoracle_model_eval.argtypes = [C.c_int32, C.c_double, C.c_double, abi.c_double_p, abi.c_double_p,
+                                         abi.c_double_p, abi.c_double_p, abi.c_double_p]
+        d.zoracle_svd3.restype = C.c_int
+        d.zoracle_svd3.argtypes = [abi.c_double_p, abi.c_double_p, abi.c_double_p, abi.c_double_p, C.c_int32]
+        d.zoracle_von_mises.restype = C.c_int
+        d.zoracle_von_mises.argtypes = [C.c_int32, C.c_double, C.c_double, C.c_double, C.c_double,
+                                        abi.c_double_p, abi.c_double_p]
+        d.zoracle_linear_offset.restype = C.c_uint64
+        d.zoracle_linear_offset.argtypes = [C.c_int32, C.c_int32, C.c_int32, C.c_int32]
+        d.zoracle_packed_add.restype = C.c_uint64
+        d.zoracle_packed_add.argtypes = [C.c_int32, C.c_uint64, C.c_uint64]
+        d.zoracle_masks.restype = None
+        d.zoracle_masks.argtypes = [C.c_int32, abi.c_uint64_p]
+        _lib = L
+    return _lib

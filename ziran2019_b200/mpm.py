@@ -1,0 +1,366 @@
+"""Host-side mirror of the reference's MPM scene / plugin API over the C ABI.
+
+Names follow the reference so that scene code reads the same:
+
+* `MpmSimulation`      <- MpmSimulationBase<T,3> (Lib/MPM/MpmSimulationBase.h:133-229)
+* `MpmParticleHandle`  <- MpmParticleHandleBase<T,3> (Lib/MPM/MpmParticleHandleBase.h:53-107)
+* `NeoHookeanBorden`, `StvkWithHenckyIsotropic`, `FixedCorotated`
+                        <- constitutive model plugins (Lib/Ziran/Physics/ConstitutiveModel)
+* `VonMisesStvkHencky` <- plasticity plugin (Lib/Ziran/Physics/PlasticityApplier.h:187-281)
+* `HalfSpace`, `Sphere`, `AxisAlignedAnalyticBox`, `AnalyticCollisionObject`
+                        <- collision plugins (Lib/Ziran/Math/Geometry)
+
+Every call goes through the CUDA library (`abi.product_lib()`); a missing
+library raises instead of falling back to anything else.
+"""
+import numpy as np
+
+from . import abi
+from .abi import ptr
+
+
+# ------------------------------------------------------------------ models --
+class _Model:
+    kind = abi.MODEL_NONE
+
+    def __init__(self, E=1.0, nu=0.3):
+        self.E = float(E)
+        self.nu = float(nu)
+        self.lam = self.E * self.nu / ((1 + self.nu) * (1 - 2 * self.nu))
+        self.mu = self.E / (2 * (1 + self.nu))
+
+
+class NeoHookeanBorden(_Model):
+    """NeoHookeanBorden(E, nu), NeoHookeanBorden.cpp:10-21."""
+    kind = abi.MODEL_NEOHOOKEAN_BORDEN
+
+
+class StvkWithHenckyIsotropic(_Model):
+    """StvkWithHenckyIsotropic(E, nu), StvkWithHenckyIsotropic.h:60-70."""
+    kind = abi.MODEL_STVK_HENCKY_ISOTROPIC
+
+
+class FixedCorotated(_Model):
+    """Fixed corotated elasticity (Stomakhin et al. 2012); no reference counterpart."""
+    kind = abi.MODEL_FIXED_COROTATED
+
+
+class VonMisesStvkHencky:
+    """VonMisesStvkHencky(yield_stress, fail_stress, xi), PlasticityApplier.cpp:443-450."""
+    kind = abi.PLASTIC_VON_MISES
+
+    def __init__(self, yield_stress, fail_stress=0.0, xi=0.0):
+        self.yield_stress = float(yield_stress)
+        self.fail_stress = float(fail_stress)
+        self.xi = float(xi)
+
+
+# -------------------------------------------------------------- colliders --
+class HalfSpace:
+    """HalfSpace(origin, outward_normal), AnalyticLevelSet.cpp:259-304."""
+
+    def __init__(self, origin, normal):
+        self.shape = abi.HALF_SPACE
+        self.a = tuple(float(v) for v in origin)
+        self.b = tuple(float(v) for v in normal)
+        self.radius = 0.0
+
+
+class Sphere:
+    """Sphere(center, radius), AnalyticLevelSet.cpp:388-451."""
+
+    def __init__(self, center, radius):
+        self.shape = abi.SPHERE
+        self.a = tuple(float(v) for v in center)
+        self.b = (0.0, 0.0, 0.0)
+        self.radius = float(radius)
+
+
+class AxisAlignedAnalyticBox:
+    """AxisAlignedAnalyticBox(min_corner, max_corner), AnalyticLevelSet.cpp:353-386."""
+
+    def __init__(self, min_corner, max_corner):
+        self.shape = abi.BOX
+        self.a = tuple(float(v) for v in min_corner)
+        self.b = tuple(float(v) for v in max_corner)
+        self.radius = 0.0
+
+
+class AnalyticCollisionObject:
+    """AnalyticCollisionObject(level_set, type) with the rigid motion x = R s X + t.
+
+    The reference's `updateState(time, object)` callback is expressed as a
+    linear-in-time translation and scale (CollisionObject.h:63-71,146-170).
+    """
+    STICKY, SLIP, SEPARATE, GHOST = abi.STICKY, abi.SLIP, abi.SEPARATE, abi.GHOST
+
+    def __init__(self, level_set, type_, friction=0.0):
+        self.ls = level_set
+        self.type = int(type_)
+        self.friction = float(friction)
+        self.rotation = (1.0, 0.0, 0.0, 0.0)
+        self.angular_velocity = (0.0, 0.0, 0.0)
+        self.translation = (0.0, 0.0, 0.0)
+        self.translation_velocity = (0.0, 0.0, 0.0)
+        self.scale = 1.0
+        self.scale_velocity = 0.0
+
+    def setFriction(self, f):
+        self.friction = float(f)
+
+    def setTranslation(self, b, dbdt=(0.0, 0.0, 0.0)):
+        self.translation = tuple(float(v) for v in b)
+        self.translation_velocity = tuple(float(v) for v in dbdt)
+
+    def setRotation(self, q):
+        self.rotation = tuple(float(v) for v in q)
+
+    def setAngularVelocity(self, w):
+        self.angular_velocity = tuple(float(v) for v in w)
+
+    def setScaling(self, s, dsdt=0.0):
+        self.scale = float(s)
+        self.scale_velocity = float(dsdt)
+
+    def to_struct(self):
+        c = abi.Collider()
+        c.shape = self.ls.shape
+        c.type = self.type
+        c.friction = self.friction
+        c.a[:] = self.ls.a
+        c.b[:] = self.ls.b
+        c.radius = self.ls.radius
+        c.rotation[:] = self.rotation
+        c.angular_velocity[:] = self.angular_velocity
+        c.translation[:] = self.translation
+        c.translation_velocity[:] = self.translation_velocity
+        c.scale = self.scale
+        c.scale_velocity = self.scale_velocity
+        return c
+
+
+def add_all_walls_in_domain(sim, max_domain_boundary, offset, type_):
+    """MpmInitializationHelper::addAllWallsInDomain (MpmInitializationHelper.h:614-629)."""
+    ids = []
+    for d in range(3):
+        for s in (-1, 1):
+            o = [0.0, 0.0, 0.0]
+            n = [0.0, 0.0, 0.0]
+            o[d] = offset if s == 1 else max_domain_boundary - offset
+            n[d] = float(s)
+            ids.append(sim.addCollisionObject(AnalyticCollisionObject(HalfSpace(o, n), type_)))
+    return ids
+
+
+# --------------------------------------------------------------- handles --
+class MpmParticleHandle:
+    """Particle range [lower, upper) of one MpmSimulation (MpmParticleHandleBase)."""
+
+    def __init__(self, sim, lower, upper):
+        self.sim = sim
+        self.lower = lower
+        self.upper = upper
+
+    def addFBasedMpmForce(self, model):
+        self.sim._call("add_fbased_force", self.lower, self.upper, model.kind, model.E, model.nu)
+
+    def setLame(self, mu, lam):
+        mu = np.ascontiguousarray(mu, dtype=np.float64)
+        lam = np.ascontiguousarray(lam, dtype=np.float64)
+        self.sim._call("set_lame", self.lower, self.upper, ptr(mu), ptr(lam))
+
+    def addPlasticity(self, model, plasticity):
+        del model  # the model is the one attached with addFBasedMpmForce
+        self.sim._call("add_plasticity", self.lower, self.upper, plasticity.kind,
+                       plasticity.yield_stress, plasticity.xi, plasticity.fail_stress)
+
+
+# ------------------------------------------------------------ simulation --
+class MpmSimulation:
+    """Implicit APIC MPM on one GPU (MpmSimulationBase<T,3>, symplectic = false).
+
+    precision: "fp64" or "mixed".  `newton_tolerance`, `newton_max_iterations`
+    and the Krylov settings mirror `sim.newton` and `sim.objective` of the
+    reference (MpmSimulationBase.cpp:51, BackwardEuler.h:51-98).
+    """
+
+    def __init__(self, dx, gravity=(0.0, 0.0, 0.0), precision="fp64", layout="auto",
+                 grid_log2=10, apic_rpic_ratio=1.0, cfl=0.6, device=0, lib=None):
+        self.lib = lib if lib is not None else abi.product_lib()
+        cfg = abi.Config()
+        cfg.precision = {"fp64": abi.FP64, "mixed": abi.MIXED}[precision]
+        cfg.layout = {"auto": abi.LAYOUT_AUTO, "244": abi.LAYOUT_244, "444": abi.LAYOUT_444}[layout]
+        cfg.grid_log2 = int(grid_log2)
+        cfg.device = int(device)
+        cfg.dx = float(dx)
+        cfg.gravity[:] = [float(g) for g in gravity]
+        cfg.apic_rpic_ratio = float(apic_rpic_ratio)
+        cfg.cfl = float(cfl)
+        self.cfg = cfg
+        self.precision = precision
+        h = abi.C.c_void_p()
+        self.lib.check(self.lib.create(abi.C.byref(cfg), abi.C.byref(h)), "create")
+        self.ctx = h
+        self.linear_solver = abi.MINRES
+        self.newton_tolerance = 1e-5
+        self.newton_max_iterations = 3
+        self.krylov_max_iterations = 20
+        self.krylov_tolerance = 1.0
+        self.linear_solve_tolerance_scale = 1.0
+        self.last_stats = None
+
+    # lifecycle
+    def close(self):
+        if self.ctx:
+            self.lib.destroy(self.ctx)
+            self.ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:  # noqa: BLE001 - interpreter shutdown
+            pass
+
+    def _call(self, name, *args):
+        return self.lib.check(getattr(self.lib, name)(self.ctx, *args), name, self.ctx)
+
+    # scene
+    def addParticles(self, x, v=None, mass=None, volume=None):
+        x = np.ascontiguousarray(x, dtype=np.float64).reshape(-1, 3)
+        n = x.shape[0]
+        v = np.zeros_like(x) if v is None else np.ascontiguousarray(v, dtype=np.float64).reshape(-1, 3)
+        mass = np.ascontiguousarray(np.broadcast_to(mass, (n,)), dtype=np.float64)
+        volume = np.ascontiguousarray(np.broadcast_to(volume, (n,)), dtype=np.float64)
+        lower = abi.C.c_int64()
+        self._call("add_particles", n, ptr(x), ptr(v), ptr(mass), ptr(volume), abi.C.byref(lower))
+        return MpmParticleHandle(self, lower.value, lower.value + n)
+
+    def addCollisionObject(self, obj):
+        cid = abi.C.c_int32()
+        s = obj.to_struct()
+        self._call("add_collision_object", abi.C.byref(s), abi.C.byref(cid))
+        return cid.value
+
+    def setCollisionObject(self, cid, obj):
+        s = obj.to_struct()
+        self._call("set_collision_object", int(cid), abi.C.byref(s))
+
+    def switchLinearSolver(self, kind):
+        """BackwardEulerLagrangianForceObjective::switchLinearSolver (BackwardEuler.h:82-98):
+        a fresh solver keeps max 20 iterations and the LinearSolver default
+        tolerance 16 eps(T) (LinearSolver.h:24)."""
+        self.linear_solver = kind
+        self.krylov_max_iterations = 20
+        eps = np.finfo(np.float64 if self.precision == "fp64" else np.float32).eps
+        self.krylov_tolerance = 16 * float(eps)
+
+    def solver(self):
+        s = abi.Solver()
+        s.linear_solver = self.linear_solver
+        s.newton_max_iterations = self.newton_max_iterations
+        s.newton_tolerance = self.newton_tolerance
+        s.krylov_max_iterations = self.krylov_max_iterations
+        s.krylov_tolerance = self.krylov_tolerance
+        s.linear_solve_tolerance_scale = self.linear_solve_tolerance_scale
+        return s
+
+    # stepping
+    def advanceOneTimeStep(self, dt):
+        st = abi.Stats()
+        s = self.solver()
+        rc = self._call("substep", float(dt), abi.C.byref(s), abi.C.byref(st))
+        self.last_stats = st.as_dict()
+        self.last_status = rc
+        return rc
+
+    # state
+    @property
+    def count(self):
+        return int(self.lib.num_particles(self.ctx))
+
+    @property
+    def time(self):
+        return float(self.lib.time(self.ctx))
+
+    def getParticles(self):
+        n = self.count
+        x = np.empty((n, 3))
+        v = np.empty((n, 3))
+        Cm = np.empty((n, 3, 3))
+        F = np.empty((n, 3, 3))
+        self._call("get_particles", ptr(x), ptr(v), ptr(Cm), ptr(F))
+        return {"X": x, "V": v, "C": Cm, "F": F}
+
+    def setParticles(self, X=None, V=None, C=None, F=None):
+        def p(a, shape):
+            if a is None:
+                return None, None
+            a = np.ascontiguousarray(a, dtype=np.float64).reshape(shape)
+            return a, ptr(a)
+        n = self.count
+        keep = [p(X, (n, 3)), p(V, (n, 3)), p(C, (n, 3, 3)), p(F, (n, 3, 3))]
+        self._call("set_particles", *[k[1] for k in keep])
+
+    def getPlasticState(self):
+        n = self.count
+        ys = np.empty(n)
+        broken = np.empty(n, dtype=np.int32)
+        self._call("get_plastic_state", ptr(ys), ptr(broken, abi.C.c_int32))
+        return ys, broken
+
+    # hooks on the implicit objective (tests / adjoints)
+    def binParticles(self):
+        counts = np.zeros(3, dtype=np.int64)
+        self._call("bin", ptr(counts, abi.C.c_int64))
+        P, G, B = (int(c) for c in counts)
+        out = {
+            "particle_sorter": np.empty(P, dtype=np.uint64),
+            "particle_order": np.empty(P, dtype=np.int32),
+            "particle_base_offset": np.empty(P, dtype=np.uint64),
+            "particle_group": np.empty((G, 2), dtype=np.int32),
+            "block_offset": np.empty(G, dtype=np.uint64),
+            "page_offsets": np.empty(B, dtype=np.uint64),
+        }
+        r = abi.BinResult()
+        r.particle_sorter = ptr(out["particle_sorter"], abi.C.c_uint64)
+        r.particle_order = ptr(out["particle_order"], abi.C.c_int32)
+        r.particle_base_offset = ptr(out["particle_base_offset"], abi.C.c_uint64)
+        r.particle_group = ptr(out["particle_group"], abi.C.c_int32)
+        r.block_offset = ptr(out["block_offset"], abi.C.c_uint64)
+        r.page_offsets = ptr(out["page_offsets"], abi.C.c_uint64)
+        self._call("bin_fetch", abi.C.byref(r))
+        return out
+
+    def beginImplicit(self, dt):
+        n = abi.C.c_int64()
+        self._call("begin_implicit", float(dt), abi.C.byref(n))
+        self.num_nodes = int(n.value)
+        return self.num_nodes
+
+    def getGrid(self):
+        n = self.num_nodes
+        m = np.empty(n)
+        v = np.empty((n, 3))
+        coord = np.empty((n, 3), dtype=np.int32)
+        self._call("get_grid", ptr(m), ptr(v), ptr(coord, abi.C.c_int32))
+        return m, v, coord
+
+    def getInitialDv(self):
+        n = self.num_nodes
+        dv = np.empty((n, 3))
+        col = np.empty(n, dtype=np.int32)
+        self._call("get_initial_dv", ptr(dv), ptr(col, abi.C.c_int32))
+        return dv, col
+
+    def residual(self, dv):
+        dv = np.ascontiguousarray(dv, dtype=np.float64).reshape(-1, 3)
+        r = np.empty_like(dv)
+        norm = abi.C.c_double()
+        self._call("residual", ptr(dv), ptr(r), abi.C.byref(norm))
+        return r, norm.value
+
+    def multiply(self, x, fp32=False):
+        x = np.ascontiguousarray(x, dtype=np.float64).reshape(-1, 3)
+        b = np.empty_like(x)
+        self._call("multiply", ptr(x), ptr(b), 1 if fp32 else 0)
+        return b
