@@ -1,0 +1,338 @@
+#!/usr/bin/env python
+"""Benchmark of the implicit APIC MPM substep on the 1M-particle elastoplastic
+workload: four jittered boxes of 25x25x50 cells x 8 particles (250,000 each),
+dx = 1/256, dt = 5e-4, StvkWithHenckyIsotropic E = 5e4, nu = 0.35 with the
+von Mises return map (yield stress 150 Pa), gravity, sticky walls 3 dx inside
+the unit cube, reference solver settings (MINRES, 3 Newton x 20 Krylov).
+
+A step is one substep of the whole scene.  `value` is mixed-precision substeps/s
+(device time, CUDA events on the library's stream); the FP64 substep is timed on
+the same scene for the speed-up and the position error between the two.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Multi-GPU runs are independent replicas (the substep has no data-path
+collective); rank 0 prints one JSON line.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+DX = 1.0 / 256
+DT = 5e-4
+CELLS = (25, 25, 50)
+PPC = 8
+RHO = 1000.0
+E, NU, YIELD = 5e4, 0.35, 150.0
+METRIC = "implicit MPM substeps/sec at 1M particles, mixed vs FP64 GPU, at <=1e-6 rel err"
+HVP_WORDS = 22  # compulsory words per particle of one Hessian-vector product: X(3), Fn(9), F(9), V0(1)
+
+
+def scene(n_boxes=4, seed_pos=1, seed_vel=2, seed_jit=0, velocity="particle"):
+    """Seeded synthetic scene (the benchmark has no dataset; shapes follow the workload).
+
+    velocity="particle": every particle draws its velocity uniformly from [-1,1]^3,
+    so the Newton solve works from the first substep.  velocity="box": one rigid
+    velocity per box; the boxes then fly undeformed (Newton converges at its first
+    residual check, no Hessian products) until they reach a wall."""
+    size = np.array(CELLS) * DX
+    rng = np.random.default_rng(seed_pos)
+    corners = []
+    while len(corners) < 4:
+        c = rng.uniform(4 * DX, 1 - size - 4 * DX)
+        if all(np.any((c + size + 2 * DX <= o) | (o + size + 2 * DX <= c)) for o in corners):
+            corners.append(c)
+    vel = np.random.default_rng(seed_vel).uniform(-1, 1, size=(4, 3))
+    jr = np.random.default_rng(seed_jit)
+    grid = np.stack(np.meshgrid(*[np.arange(c) for c in CELLS], indexing="ij"), -1).reshape(-1, 3)
+    xs, vs = [], []
+    for b in range(n_boxes):
+        x = (np.repeat(grid, PPC, 0) + jr.random((grid.shape[0] * PPC, 3))) * DX + corners[b]
+        xs.append(x)
+        vs.append(np.tile(vel[b], (x.shape[0], 1)))
+    x, v = np.concatenate(xs), np.concatenate(vs)
+    if velocity == "particle":
+        v = np.random.default_rng(seed_vel).uniform(-1, 1, size=x.shape)
+    return x, v
+
+
+def make_sim(x, v, precision, lib=None, model="hencky"):
+    from ziran2019_b200 import abi, mpm
+
+    sim = mpm.MpmSimulation(DX, gravity=(0, -9.8, 0), precision=precision, grid_log2=9,
+                            device=int(os.environ.get("LOCAL_RANK", "0")) if lib is None else 0, lib=lib)
+    V0 = DX ** 3 / PPC
+    h = sim.addParticles(x, v, RHO * V0, V0)
+    m = mpm.StvkWithHenckyIsotropic(E, NU) if model == "hencky" else mpm.NeoHookeanBorden(E, NU)
+    h.addFBasedMpmForce(m)
+    h.addPlasticity(m, mpm.VonMisesStvkHencky(YIELD, 1e30, 0.0))
+    mpm.add_all_walls_in_domain(sim, 1.0, 3 * DX, abi.STICKY)
+    return sim
+
+
+class Clocks:
+    """nvidia-smi samples during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def start(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                       "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        self.p.wait()
+        self.f.flush()
+        rows = [r.split(",") for r in open(self.f.name).read().strip().splitlines() if r.strip()]
+        os.unlink(self.f.name)
+        sm = [float(r[1]) for r in rows if len(r) >= 9 and r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if len(r) >= 9 and r[2].strip().replace(".", "").isdigit()]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            if len(r) < 9:
+                continue
+            for k, n in enumerate(names):
+                if r[5 + k].strip().lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(rows)}
+
+
+def dist_setup():
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    return world, rank
+
+
+def barrier_max(value, world):
+    """Barrier and max over ranks."""
+    if world == 1:
+        return value
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def timed_steps(sim, steps, world, profile=False):
+    """Runs `steps` substeps between CUDA events on the library stream; returns ms and stats."""
+    import ctypes
+
+    import torch
+
+    from ziran2019_b200 import abi
+    sptr = ctypes.c_void_p()
+    sim.lib.check(sim.lib.get_stream(sim.ctx, ctypes.byref(sptr)), "get_stream")
+    stream = torch.cuda.ExternalStream(sptr.value or 0)
+    sim.lib.set_profiling(sim.ctx, 1 if profile else 0)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    barrier_max(0.0, world)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    stats = []
+    for _ in range(steps):
+        rc = sim.advanceOneTimeStep(DT)
+        if rc not in (abi.OK, abi.CFL_VIOLATION):
+            raise RuntimeError(f"substep status {rc}")
+        stats.append(sim.last_stats)
+    e1.record(stream)
+    e1.synchronize()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    sim.lib.set_profiling(sim.ctx, 0)
+    return barrier_max(ms, world), stats
+
+
+def cpu_oracle_rate(steps, warmup, velocity="particle"):
+    """The oracle (CPU restatement of the reference substep) on one 250k-particle
+    box of the same scene, all host threads; returns 1M-equivalent substeps/s."""
+    from oracle import zoracle
+    x, v = scene(n_boxes=1, velocity=velocity)
+    sim = make_sim(x, v, "fp64", lib=zoracle.lib())
+    for _ in range(warmup):
+        sim.advanceOneTimeStep(DT)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        sim.advanceOneTimeStep(DT)
+    dt = time.perf_counter() - t0
+    P = x.shape[0]
+    return steps / dt * P / 1_000_000, P, dt
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return
+    cores = os.cpu_count()
+    rate, P, secs = cpu_oracle_rate(args.steps, args.warmup, args.velocity)
+    sample = f"{args.steps} substeps of one {P}-particle box of the workload (oracle port, {cores} threads), scaled by {P}/1e6"
+    line = {"metric": METRIC, "value": rate, "unit": "substeps/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * secs / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "impl": "reference",
+            "config": {"workload": "config1-elastoplastic-4boxes", "particles": 1_000_000, "sample_particles": P},
+            "cpu_baseline": {"value": rate, "unit": "substeps/s", "cores": cores, "kind": "port", "sample": sample},
+            "e2e": {"value": rate, "unit": "substeps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--accuracy-steps", type=int, default=100)
+    ap.add_argument("--cpu-steps", type=int, default=1)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--model", default="hencky", choices=["hencky", "nh"])
+    ap.add_argument("--velocity", default="particle", choices=["particle", "box"])
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    world, rank = dist_setup()
+    if args.impl == "reference":
+        run_reference(args, world, rank)
+        return
+
+    import torch
+
+    from ziran2019_b200 import build
+    build.build()
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    x, v = scene(velocity=args.velocity)
+    P = x.shape[0]
+    sims = {p: make_sim(x, v, p, model=args.model) for p in ("fp64", "mixed")}
+    for p in ("fp64", "mixed"):
+        for _ in range(args.warmup):
+            sims[p].advanceOneTimeStep(DT)
+    ms64, st64 = timed_steps(sims["fp64"], args.steps, world)
+    clocks = Clocks(dev)
+    clocks.start()
+    ms_mx, st_mx = timed_steps(sims["mixed"], args.steps, world, profile=True)
+    clk = clocks.stop()
+    value = world * args.steps / (ms_mx / 1e3)
+    fp64_value = world * args.steps / (ms64 / 1e3)
+
+    # position error of the mixed substep against the FP64 substep after
+    # `accuracy-steps` substeps from the same initial state
+    done = args.warmup + args.steps
+    for p in ("fp64", "mixed"):
+        for _ in range(max(0, args.accuracy_steps - done)):
+            sims[p].advanceOneTimeStep(DT)
+    x64 = sims["fp64"].getParticles()["X"]
+    xmx = sims["mixed"].getParticles()["X"]
+    rel_err = float(np.linalg.norm(xmx - x64) / np.linalg.norm(x64))
+    max_abs_dx = float(np.abs(xmx - x64).max() / DX)
+
+    # dominant kernel: the Hessian-vector product
+    hvp_ms = sum(s["ms_hvp"] for s in st_mx)
+    hvp_n = sum(s["hvp_timed"] for s in st_mx)
+    nodes = st_mx[-1]["num_blocks"] * 64
+    hvp_bytes = P * HVP_WORDS * 4 + nodes * 3 * 8 * 2
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except OSError:
+        pass
+    peak = float(peaks.get("hbm_gbs", 6650.0))
+    achieved = hvp_bytes / (hvp_ms / hvp_n / 1e3) / 1e9 if hvp_n else None
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak if achieved else None, "traffic": None,
+                "kernel": "k_hvp (FP32 Hessian-vector product)", "bytes_per_launch": hvp_bytes,
+                "avg_launch_ms": hvp_ms / hvp_n if hvp_n else None, "peak_source": "measured" if peaks else "fallback"}
+
+    e2e = None
+    if not args.no_e2e:
+        sim = sims["mixed"]
+        pin = {k: torch.empty(s, dtype=torch.float64, pin_memory=True) for k, s in (("X", (P, 3)), ("V", (P, 3)), ("C", (P, 3, 3)), ("F", (P, 3, 3)))}
+        cur = sim.getParticles()
+        for k in pin:
+            pin[k].numpy()[...] = cur[k]
+        import ctypes
+        sptr = ctypes.c_void_p()
+        sim.lib.get_stream(sim.ctx, ctypes.byref(sptr))
+        stream = torch.cuda.ExternalStream(sptr.value or 0)
+        arrs = {k: t.numpy() for k, t in pin.items()}
+        from ziran2019_b200.abi import ptr
+
+        def e2e_step():
+            sim._call("set_particles", ptr(arrs["X"]), ptr(arrs["V"]), ptr(arrs["C"]), ptr(arrs["F"]))
+            sim.advanceOneTimeStep(DT)
+            sim._call("get_particles", ptr(arrs["X"]), ptr(arrs["V"]), ptr(arrs["C"]), ptr(arrs["F"]))
+        for _ in range(args.warmup):
+            e2e_step()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        barrier_max(0.0, world)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(args.steps):
+            e2e_step()
+        e1.record(stream)
+        e1.synchronize()
+        ms_e2e = barrier_max(e0.elapsed_time(e1), world)
+        e2e = {"value": world * args.steps / (ms_e2e / 1e3), "unit": "substeps/s", "h2d_bytes_per_step": P * 24 * 8,
+               "d2h_bytes_per_step": P * 24 * 8}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        rate, Pc, secs = cpu_oracle_rate(args.cpu_steps, 0, args.velocity)
+        cpu = {"value": rate, "unit": "substeps/s", "cores": os.cpu_count(), "kind": "port",
+               "sample": f"{args.cpu_steps} substep(s) of one {Pc}-particle box of the workload, oracle port, {secs:.1f} s, scaled by {Pc}/1e6"}
+
+    launches = sum(s["kernel_launches"] for s in st_mx)
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "substeps/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms_mx / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "fp32 Hessian products, fp64 state/residual/reductions", "data": "synthetic",
+            "config": {"workload": "config1-elastoplastic-4boxes", "particles": P, "dx": DX, "dt": DT,
+                       "model": f"{args.model}+von Mises", "velocity": args.velocity, "solver": "MINRES, Newton 3 x Krylov 20 (reference defaults)",
+                       "parallelism": f"replicas x{world}", "l2": "inputs larger than L2 (particle state ~300 MB)"},
+            "particles_substeps_per_s": value * P,
+            "fp64_value": fp64_value, "mixed_over_fp64": value / fp64_value,
+            "rel_pos_err_vs_fp64": rel_err, "max_abs_err_over_dx": max_abs_dx, "accuracy_steps": max(args.accuracy_steps, done),
+            "newton_krylov_per_step": [st_mx[-1]["newton_iterations"], st_mx[-1]["krylov_iterations"]],
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+    for s in sims.values():
+        s.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -145,6 +145,10 @@ typedef struct zmpm_stats {
     double newton_residual_initial;
     double newton_residual_final;
     double ms_total;             /* device time of the substep */
+    double ms_hvp;               /* summed device time of the Hessian-vector products that ran
+                                    (only with zmpm_set_profiling on) */
+    int32_t hvp_timed;           /* number of products in ms_hvp */
+    int32_t kernel_launches;     /* CUDA kernels this library launched for the substep */
 } zmpm_stats;
 
 /* Result of the binning pass (sortParticlesAndPolluteGrid,
@@ -210,6 +214,14 @@ double zmpm_time(const zmpm_ctx* ctx);
    backward-Euler Newton (MINRES/CG, matrix-free Hessian) -> G2P ->
    evolveStrain -> plasticity.  stats may be NULL. */
 int zmpm_substep(zmpm_ctx* ctx, double dt, const zmpm_solver* solver, zmpm_stats* stats);
+
+/* The CUDA stream (cudaStream_t) every kernel of this context runs on, so a
+   caller can order its own work or CUDA events against the substep. */
+int zmpm_get_stream(zmpm_ctx* ctx, void** stream);
+/* on != 0: bracket each Hessian-vector product with CUDA events and report
+   their summed device time in zmpm_stats.ms_hvp (the reference's ZIRAN_TIMER
+   scopes, Lib/Ziran/CS/Util/Timer.h:34-58, as device timers). */
+int zmpm_set_profiling(zmpm_ctx* ctx, int32_t on);
 
 /* Default solver settings of the reference (MpmSimulationBase.cpp:51,
    BackwardEuler.h:56-62, LinearSolver.h:24). */

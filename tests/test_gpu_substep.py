@@ -1,0 +1,115 @@
+"""Full implicit substeps of the CUDA library against the oracle (same seeded
+scenes, same solver settings), plus status codes and edge cases."""
+import numpy as np
+import pytest
+
+from ziran2019_b200 import abi, mpm
+from tests.scenes import build_scene, jittered_box
+
+pytestmark = pytest.mark.gpu
+
+
+def run_pair(oracle, kind, solver, steps, plastic=None, precision="fp64", tol=1e-7, newton_max=8, kmax=40, walls=False, seed=0):
+    dx = 1.0 / 64
+    sims = [mpm.MpmSimulation(dx, gravity=(0, -9.8, 0), precision=precision, grid_log2=8),
+            mpm.MpmSimulation(dx, gravity=(0, -9.8, 0), precision="fp64", lib=oracle)]
+    for s in sims:
+        build_scene(s, kind=kind, n=6, dx=dx, plastic=plastic, walls=walls, seed=seed)
+        if solver == "cg":
+            s.switchLinearSolver(abi.CG)
+        s.newton_tolerance = tol
+        s.newton_max_iterations = newton_max
+        s.krylov_max_iterations = kmax
+    stats = [[], []]
+    for _ in range(steps):
+        for k, s in enumerate(sims):
+            rc = s.advanceOneTimeStep(1e-3)
+            assert rc == abi.OK, (k, rc, s.last_stats)
+            stats[k].append(s.last_stats)
+    return sims, stats
+
+
+def rel(a, b):
+    return np.abs(a - b).max() / max(np.abs(b).max(), 1e-300)
+
+
+@pytest.mark.parametrize("kind,plastic", [("fcr", None), ("nh", None), ("hencky", 150.0)])
+@pytest.mark.parametrize("solver", ["minres", "cg"])
+def test_substeps_match_oracle_fp64(cuda_lib, oracle, kind, plastic, solver):
+    (g, o), (sg, so) = run_pair(oracle, kind, solver, steps=5, plastic=plastic)
+    for a, b in zip(sg, so):
+        assert a["num_nodes"] == b["num_nodes"] and a["num_blocks"] == b["num_blocks"]
+        assert a["num_groups"] == b["num_groups"]
+        assert abs(a["newton_iterations"] - b["newton_iterations"]) <= 1
+        assert a["newton_converged"] == b["newton_converged"]
+    pg, po = g.getParticles(), o.getParticles()
+    # FP64 vs FP64 differ only by summation order (atomics vs colour order)
+    assert rel(pg["X"], po["X"]) < 1e-10
+    assert rel(pg["V"], po["V"]) < 1e-6
+    assert rel(pg["F"], po["F"]) < 1e-8
+    assert rel(pg["C"], po["C"]) < 1e-5
+    if plastic:
+        yg, _ = g.getPlasticState()
+        yo, _ = o.getPlasticState()
+        np.testing.assert_allclose(yg, yo, rtol=1e-9)
+
+
+@pytest.mark.parametrize("kind", ["fcr", "hencky"])
+def test_mixed_precision_tracks_fp64_oracle(cuda_lib, oracle, kind):
+    """MIXED: FP64 state and residuals, FP32 Hessian products; a converged Newton
+    solve lands on the FP64 solution up to the Newton tolerance."""
+    (g, o), (sg, so) = run_pair(oracle, kind, "cg", steps=5, precision="mixed", tol=1e-9, newton_max=12, kmax=60)
+    pg, po = g.getParticles(), o.getParticles()
+    assert rel(pg["X"], po["X"]) < 1e-8
+    assert rel(pg["V"], po["V"]) < 1e-4
+
+
+def test_walls_and_free_particles(cuda_lib, oracle):
+    dx = 1.0 / 64
+    sims = [mpm.MpmSimulation(dx, gravity=(0, -9.8, 0), precision="fp64", grid_log2=8),
+            mpm.MpmSimulation(dx, gravity=(0, -9.8, 0), precision="fp64", lib=oracle)]
+    rng = np.random.default_rng(9)
+    x_free = rng.uniform(0.6, 0.7, size=(300, 3))
+    for s in sims:
+        build_scene(s, kind="nh", n=5, dx=dx, walls=True, ground=None, v0=(2.0, -3.0, 1.0))
+        s.addParticles(x_free, rng.standard_normal((300, 3)) * 0 + np.array([0.5, 0.0, -0.5]), 0.01, 1e-6)
+        s.addCollisionObject(mpm.AnalyticCollisionObject(mpm.Sphere((0.55, 0.3, 0.5), 0.08), abi.SLIP, 0.3))
+        box = mpm.AnalyticCollisionObject(mpm.AxisAlignedAnalyticBox((0.35, 0.0, 0.3), (0.45, 0.12, 0.7)), abi.SEPARATE, 0.2)
+        box.setTranslation((0.0, 0.0, 0.0), (0.0, 0.5, 0.0))
+        s.addCollisionObject(box)
+        s.newton_tolerance = 1e-8
+        s.newton_max_iterations = 10
+        s.krylov_max_iterations = 40
+    for _ in range(6):
+        for s in sims:
+            assert s.advanceOneTimeStep(1e-3) == abi.OK
+    pg, po = sims[0].getParticles(), sims[1].getParticles()
+    assert rel(pg["X"], po["X"]) < 1e-10
+    assert rel(pg["V"], po["V"]) < 1e-6
+
+
+def test_cfl_violation_status(cuda_lib):
+    dx = 1.0 / 64
+    sim = mpm.MpmSimulation(dx, precision="fp64", grid_log2=8)
+    x = jittered_box(3, dx, (0.5, 0.5, 0.5), 8)
+    sim.addParticles(x, np.tile([40.0, 0.0, 0.0], (x.shape[0], 1)), 1.0, 1e-6)
+    assert sim.advanceOneTimeStep(1e-3) == abi.CFL_VIOLATION
+    assert sim.last_stats["cfl_violation"] == 1
+
+
+def test_empty_scene_substep(cuda_lib):
+    sim = mpm.MpmSimulation(1.0 / 64, precision="fp64", grid_log2=8)
+    assert sim.advanceOneTimeStep(1e-3) == abi.OK
+    assert sim.last_stats["num_particles"] == 0
+
+
+def test_free_fall_is_exact(cuda_lib):
+    dx = 1.0 / 64
+    for prec in ("fp64", "mixed"):
+        sim = mpm.MpmSimulation(dx, gravity=(0, -9.8, 0), precision=prec, grid_log2=8)
+        build_scene(sim, kind="fcr", n=4, dx=dx, ground=None, v0=(0, 0, 0))
+        for _ in range(4):
+            assert sim.advanceOneTimeStep(1e-3) == abi.OK
+        p = sim.getParticles()
+        np.testing.assert_allclose(p["V"][:, 1], -9.8 * 4e-3, rtol=1e-12)
+        np.testing.assert_allclose(p["F"], np.broadcast_to(np.eye(3), p["F"].shape), atol=1e-12)

@@ -93,6 +93,9 @@ class Stats(C.Structure):
         ("newton_residual_initial", C.c_double),
         ("newton_residual_final", C.c_double),
         ("ms_total", C.c_double),
+        ("ms_hvp", C.c_double),
+        ("hvp_timed", C.c_int32),
+        ("kernel_launches", C.c_int32),
     ]
 
     def as_dict(self):
@@ -137,6 +140,8 @@ _SIGS = {
 
 # entry points exported by the product library only
 _PRODUCT_ONLY = {
+    "get_stream": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
+    "set_profiling": (C.c_int, [C.c_void_p, C.c_int32]),
     "status_string": (C.c_char_p, [C.c_int]),
     "default_solver": (None, [C.POINTER(Solver), C.c_int32, C.c_int32]),
 }

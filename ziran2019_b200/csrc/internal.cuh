@@ -1,0 +1,180 @@
+// Context and launch interface shared by the library's translation units.
+#pragma once
+
+#include <cstdint>
+#include <cstdio>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/zmpm.h"
+#include "common.cuh"
+
+namespace zmpm {
+
+// Kernels launched by this library on the calling host thread (reported per
+// substep in zmpm_stats.kernel_launches).
+extern thread_local int64_t g_kernel_launches;
+
+// ------------------------------------------------------------ primitives --
+int64_t scan_scratch_elems(int64_t n);
+template <class T>
+void exclusive_scan(const T* in, T* out, int64_t n, T* total, T* scratch, cudaStream_t st);
+int64_t radix_scratch_elems(int64_t n);
+uint64_t* radix_sort(uint64_t* keys, uint64_t* alt, int64_t n, int lo_bit, int nbits, int32_t* scratch, cudaStream_t st);
+
+// ---------------------------------------------------------- device buffer --
+struct DBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    template <class T>
+    T* as() const { return static_cast<T*>(p); }
+    cudaError_t ensure(size_t n)
+    {
+        if (n <= bytes) return cudaSuccess;
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+        size_t want = n + n / 4 + 256;
+        cudaError_t e = cudaMalloc(&p, want);
+        if (e == cudaSuccess) bytes = want;
+        return e;
+    }
+    void release()
+    {
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+    }
+};
+
+// Counters the device writes and the host reads once per substep.
+struct DevCounters {
+    int64_t G, B, N;           // groups, pages, active nodes
+    int32_t flags;             // FLAG_*
+    int32_t pad;
+};
+
+// Scalar state of the Newton / Krylov loop, kept on the device so no host
+// round trip is needed inside a solve.  Double-buffered where a kernel's CTAs
+// read the previous value while CTA 0 writes the next one.
+struct SolverScalars {
+    int32_t newton_done;       // 1 once the Newton norm fell below tolerance (or NaN)
+    int32_t krylov_active;     // 1 while the current linear solve iterates
+    int32_t newton_iters;      // linear solves run
+    int32_t krylov_iters;      // summed Krylov iterations
+    int32_t hvp_count;
+    int32_t converged;
+    int32_t pad[2];
+    int32_t kcount[64];        // Krylov iterations of each Newton iteration
+    double res_initial, res_final;
+    double rel_tol, local_tol;
+    double rnorm;              // current preconditioned residual norm of the linear solve
+    // CG
+    double zTrk;
+    // MINRES (Minres.h:16-24), double buffered by iteration parity
+    double mr[2][12];
+};
+enum MinresSlot { MR_GC0, MR_GS0, MR_GC1, MR_GS1, MR_GC2, MR_GS2, MR_RHS0, MR_RHS1, MR_BETA_KP1, MR_TK, MR_DELTA, MR_EPS };
+
+// Field indices of the particle pools.
+enum PdField { PD_X = 0, PD_V = 3, PD_C = 6, PD_F = 15, PD_M = 24, PD_VOL = 25, PD_MU = 26, PD_LAM = 27, PD_KAPPA = 28,
+    PD_G = 29, PD_YS = 30, PD_XI = 31, PD_FS = 32, PD_CRACK = 33, PD_FIELDS = 36 };
+enum PiField { PI_KIND = 0, PI_PKIND = 1, PI_BROKEN = 2, PI_ID = 3, PI_FIELDS = 4 };
+
+// Reduction slots: per-CTA partial sums written by node kernels.
+constexpr int RED_MAX_CTAS = 1024;
+enum RedSlot { RED_A = 0, RED_B = 1, RED_C = 2, RED_N = 3 };
+
+struct Ctx {
+    zmpm_config cfg;
+    int layout = 1;            // 1: 2x4x4 pages, 2: 4x4x4 pages
+    bool mixed = false;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    std::string err;
+    double time = 0;
+
+    // grid extent
+    int grid_log2 = 10;
+    int pages[3] = { 0, 0, 0 }; // pages per axis
+    int64_t table_size = 0;
+    int key_bits = 0;           // significant key bits above the particle index
+
+    // host copy of the scene until the first upload
+    int64_t P = 0;
+    bool uploaded = false;
+    std::vector<double> hx, hv, hC, hF, hcrack, hm, hvol, hmu, hlam, hkappa, hg, hys, hxi, hfs;
+    std::vector<uint8_t> hkind, hpkind;
+    std::vector<int32_t> hbroken;
+    std::vector<zmpm_collider> colliders;
+
+    // particles in slot order, structure of arrays (capacity Pcap).  The
+    // double fields live in one pool [PD_FIELDS][Pcap] and the integer fields
+    // in another, so the binning permutation moves all state in one kernel.
+    int64_t Pcap = 0;
+    DBuf pd, pd_alt, pi, pi_alt;
+    DBuf slot_of_id;   // particle index -> slot
+    DBuf base_by_id;   // short4 base node per particle index (binning)
+    DBuf base;         // short4 base node per slot
+    DBuf Fn;           // [9][Pcap] F at the start of the Newton solve
+    DBuf scratch;      // Hessian scratch [NS][Pcap] in the HVP precision
+    DBuf frac;         // [3][Pcap] fractional offsets in cells (FP32 HVP)
+    double* pdf(int f) const { return pd.as<double>() + (int64_t)f * Pcap; }
+    int32_t* pif(int f) const { return pi.as<int32_t>() + (int64_t)f * Pcap; }
+
+    // binning
+    DBuf keys, keys_alt, flags_i32, scan_i32, scan_scr, radix_scr;
+    DBuf group_start, group_page, group_nbr, emit_flag, emit_scan;
+    DBuf page_first, page_block;          // dense page tables
+    DBuf block_page, block_index;         // per page: packed coords, page index
+    int64_t G = 0, B = 0, N = 0;
+    bool binned = false;
+
+    // grid, block-dense: scalars [B][NPB], vectors [B][3][NPB]
+    DBuf gm, gmv, vn, dv, vstar, facc, res, proj, collided, node_idx;
+    // Krylov vectors
+    DBuf kv[10];
+    DBuf red;                             // reduction partials [4][RED_MAX_CTAS]
+    DBuf scal;                            // SolverScalars
+    DBuf counters;                        // DevCounters
+    DBuf dcolliders;
+    DevCounters hcounters;
+    bool implicit_ready = false;
+    bool scratch_valid = false;
+    bool profiling = false;
+    std::vector<cudaEvent_t> hvp_ev;      // [newton][krylov][2] when profiling
+    int prof_newton = 0, prof_krylov = 0;
+    DBuf stage;                           // host <-> device particle transfers
+    double dt = 0;
+
+    int npb() const { return layout == 1 ? 32 : 64; }
+};
+
+#define ZMPM_CUDA(expr)                                                                            \
+    do {                                                                                           \
+        cudaError_t _e = (expr);                                                                   \
+        if (_e != cudaSuccess) {                                                                   \
+            ctx->err = std::string(#expr) + ": " + cudaGetErrorString(_e);                         \
+            return ZMPM_CUDA_ERROR;                                                                \
+        }                                                                                          \
+    } while (0)
+
+// ---------------------------------------------------------------- passes --
+int run_binning(Ctx* ctx);
+int run_p2g(Ctx* ctx);                                 // P2G + grid normalisation + Newton setup
+int run_newton(Ctx* ctx, const zmpm_solver& s);       // backward-Euler Newton
+int run_g2p(Ctx* ctx);                                 // G2P + evolveStrain + plasticity
+int upload_colliders(Ctx* ctx, double time);
+int launch_update(Ctx* ctx);                           // G2P(vn+dv) -> stress -> force P2G
+int launch_residual(Ctx* ctx);                         // r = dt m g + dt f - m dv (projected), norm partials
+int launch_hvp(Ctx* ctx, const double* x, double* out, bool fp32); // out += dt^2 K x (no inertia)
+int finalize_multiply(Ctx* ctx, const double* x, double* q); // q = project(m x + q)
+int ensure_node_buffers(Ctx* ctx);
+int compute_node_indices(Ctx* ctx);                    // getNumNodes numbering (hooks)
+
+} // namespace zmpm
+
+struct zmpm_ctx : zmpm::Ctx {};

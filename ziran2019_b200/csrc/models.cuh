@@ -1,0 +1,264 @@
+// Constitutive models, their Hessian-vector scratch, and return maps, per
+// particle in registers.
+//
+// update(): F -> stress S = V0 P(F) Fn^T (FBasedMpmForceHelper::updateImplicitState,
+//           Lib/MPM/Force/FBasedMpmForceHelper.cpp:68-92) and the scratch the
+//           Hessian-vector product needs.
+// hvp():    grad(dv) -> dS = V0 dP(grad(dv) Fn) Fn^T
+//           (FBasedMpmForceHelper::computeStressDifferential, :132-154).
+//
+// Scratch slots (NS = 34, stored [slot][particle] in the HVP precision):
+//   SVD-isotropic models (StvkWithHenckyIsotropic, fixed corotated):
+//     0-8 U, 9-17 W = Fn V, 18-29 the SvdBasedIsotropicHelper coefficients
+//     (psi00,psi11,psi22, psi01,psi02,psi12, m01,m02,m12, p01,p02,p12)
+//     pre-multiplied by V0, so dS = U K(U^T grad(dv) W) W^T.
+//   NeoHookeanBorden: 0-8 F, 9-17 F^{-T}, 18-26 Fn, 27 J, 28 mu J^{-2/3},
+//     29 kappa/2 (J - 1/J), 30 kappa/2 (1 + 1/J^2), 31 g, 32 V0, 33 F:F.
+#pragma once
+#include "svd3.cuh"
+#include "../../include/zmpm.h"
+
+namespace zmpm {
+
+constexpr int NS = 34;
+
+template <class T>
+ZMPM_HD T clamp_small_magnitude(T x, T eps)
+{
+    if (x < -eps) return x;
+    if (x < T(0)) return -eps;
+    if (x < eps) return eps;
+    return x;
+}
+// (x log y - y log x)/(x - y) evaluated as MathTools.h:247-252 does
+template <class T>
+ZMPM_HD T diff_interlock_log_over_diff(T x, T y, T logy, T eps)
+{
+    T p = x / y - T(1);
+    T l1p = (fabs(p) < eps) ? T(1) : log1p(p) / p;
+    return logy - y * (l1p / y);
+}
+
+// SvdBasedIsotropicHelper::dPdFOfSigmaContract (SvdBasedIsotropicHelper.h:151-162)
+// with coefficients c = (psi00,psi11,psi22, psi01,psi02,psi12, m01,m02,m12, p01,p02,p12)
+template <class T>
+ZMPM_HD M3<T> iso_contract(const T c[12], const M3<T>& A)
+{
+    M3<T> B;
+    B(0, 0) = c[0] * A(0, 0) + c[3] * A(1, 1) + c[4] * A(2, 2);
+    B(1, 1) = c[3] * A(0, 0) + c[1] * A(1, 1) + c[5] * A(2, 2);
+    B(2, 2) = c[4] * A(0, 0) + c[5] * A(1, 1) + c[2] * A(2, 2);
+    B(0, 1) = ((c[6] + c[9]) * A(0, 1) + (c[6] - c[9]) * A(1, 0)) / T(2);
+    B(1, 0) = ((c[6] - c[9]) * A(0, 1) + (c[6] + c[9]) * A(1, 0)) / T(2);
+    B(0, 2) = ((c[7] + c[10]) * A(0, 2) + (c[7] - c[10]) * A(2, 0)) / T(2);
+    B(2, 0) = ((c[7] - c[10]) * A(0, 2) + (c[7] + c[10]) * A(2, 0)) / T(2);
+    B(1, 2) = ((c[8] + c[11]) * A(1, 2) + (c[8] - c[11]) * A(2, 1)) / T(2);
+    B(2, 1) = ((c[8] - c[11]) * A(1, 2) + (c[8] + c[11]) * A(2, 1)) / T(2);
+    return B;
+}
+
+// Derivatives of psi-hat(sigma) for the SVD-isotropic models.
+// psi[3] = d psi / d sigma_i; c[12] = second-order coefficients.
+template <class T>
+ZMPM_HD void iso_coefficients(int kind, T mu, T lambda, const T sg[3], T psi[3], T c[12])
+{
+    const T eps = T(1e-6);
+    if (kind == ZMPM_MODEL_STVK_HENCKY_ISOTROPIC) {
+        // StvkWithHenckyIsotropic::updateScratch (3D), StvkWithHenckyIsotropic.h:114-143
+        T L0 = log(fabs(sg[0])), L1 = log(fabs(sg[1])), L2 = log(fabs(sg[2]));
+        T g = T(2) * mu + lambda;
+        T sum_log = L0 + L1 + L2;
+        psi[0] = (T(2) * mu * L0 + lambda * sum_log) / sg[0];
+        psi[1] = (T(2) * mu * L1 + lambda * sum_log) / sg[1];
+        psi[2] = (T(2) * mu * L2 + lambda * sum_log) / sg[2];
+        c[0] = (g * (T(1) - L0) - lambda * (L1 + L2)) / (sg[0] * sg[0]);
+        c[1] = (g * (T(1) - L1) - lambda * (L0 + L2)) / (sg[1] * sg[1]);
+        c[2] = (g * (T(1) - L2) - lambda * (L0 + L1)) / (sg[2] * sg[2]);
+        c[3] = lambda / (sg[0] * sg[1]);
+        c[4] = lambda / (sg[0] * sg[2]);
+        c[5] = lambda / (sg[1] * sg[2]);
+        c[6] = -(lambda * sum_log + T(2) * mu * diff_interlock_log_over_diff(sg[0], sg[1], L1, eps)) / (sg[0] * sg[1]);
+        c[7] = -(lambda * sum_log + T(2) * mu * diff_interlock_log_over_diff(sg[0], sg[2], L2, eps)) / (sg[0] * sg[2]);
+        c[8] = -(lambda * sum_log + T(2) * mu * diff_interlock_log_over_diff(sg[1], sg[2], L2, eps)) / (sg[1] * sg[2]);
+    }
+    else {
+        // fixed corotated: psi-hat = mu sum (s_i - 1)^2 + lambda/2 (J - 1)^2
+        T J = sg[0] * sg[1] * sg[2];
+        T c0 = sg[1] * sg[2], c1 = sg[0] * sg[2], c2 = sg[0] * sg[1];
+        psi[0] = T(2) * mu * (sg[0] - T(1)) + lambda * (J - T(1)) * c0;
+        psi[1] = T(2) * mu * (sg[1] - T(1)) + lambda * (J - T(1)) * c1;
+        psi[2] = T(2) * mu * (sg[2] - T(1)) + lambda * (J - T(1)) * c2;
+        c[0] = T(2) * mu + lambda * c0 * c0;
+        c[1] = T(2) * mu + lambda * c1 * c1;
+        c[2] = T(2) * mu + lambda * c2 * c2;
+        c[3] = lambda * sg[2] * (T(2) * J - T(1));
+        c[4] = lambda * sg[1] * (T(2) * J - T(1));
+        c[5] = lambda * sg[0] * (T(2) * J - T(1));
+        c[6] = T(2) * mu - lambda * (J - T(1)) * sg[2];
+        c[7] = T(2) * mu - lambda * (J - T(1)) * sg[1];
+        c[8] = T(2) * mu - lambda * (J - T(1)) * sg[0];
+    }
+    c[9] = (psi[0] + psi[1]) / clamp_small_magnitude(sg[0] + sg[1], eps);
+    c[10] = (psi[0] + psi[2]) / clamp_small_magnitude(sg[0] + sg[2], eps);
+    c[11] = (psi[1] + psi[2]) / clamp_small_magnitude(sg[1] + sg[2], eps);
+}
+
+// Kirchhoff stress of NeoHookeanBorden (NeoHookeanBorden.cpp:67-83) and
+// P = tau F^{-T} (HyperelasticConstitutiveModel.h:85-90).
+template <class T>
+ZMPM_HD M3<T> nh_first_piola(T mu, T kappa, T g, T J, const M3<T>& F, const M3<T>& FinvT)
+{
+    M3<T> B = m3_mulT(F, F);
+    T tr = B(0, 0) + B(1, 1) + B(2, 2);
+    T sdev = mu * pow(J, -T(2) / T(3));
+    T vol = J * (kappa / T(2) * (J - T(1) / J));
+    M3<T> tau;
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            T dv = (i == j) ? B(i, j) - T(1) / T(3) * tr : B(i, j);
+            T td = sdev * dv;
+            T tv = (i == j) ? vol : T(0);
+            tau(i, j) = (J >= T(1)) ? g * (td + tv) : g * td + tv;
+        }
+    return m3_mul(tau, FinvT);
+}
+
+// Computes S = V0 P(F) Fn^T and writes the Hessian scratch of particle p.
+template <class T, class TH>
+ZMPM_D M3<T> model_update(int kind, const ModelParams& mp, T V0, const M3<T>& F, const M3<T>& Fn, TH* __restrict__ scr,
+    int64_t stride, int64_t p)
+{
+    if (kind == ZMPM_MODEL_NEOHOOKEAN_BORDEN) {
+        T J = m3_det(F);
+        M3<T> FinvT = m3_cofactor(F);
+#pragma unroll
+        for (int i = 0; i < 9; ++i) FinvT.a[i] *= T(1) / J;
+        T mu = (T)mp.mu, kappa = (T)mp.kappa, g = (T)mp.g;
+        M3<T> P = nh_first_piola(mu, kappa, g, J, F, FinvT);
+#pragma unroll
+        for (int i = 0; i < 9; ++i) {
+            scr[i * stride + p] = (TH)F.a[i];
+            scr[(9 + i) * stride + p] = (TH)FinvT.a[i];
+            scr[(18 + i) * stride + p] = (TH)Fn.a[i];
+        }
+        scr[27 * stride + p] = (TH)J;
+        scr[28 * stride + p] = (TH)(mu * pow(J, T(2) * (-T(1) / T(3))));
+        scr[29 * stride + p] = (TH)(kappa / T(2) * (J - T(1) / J));
+        scr[30 * stride + p] = (TH)(kappa / T(2) * (T(1) + T(1) / (J * J)));
+        scr[31 * stride + p] = (TH)g;
+        scr[32 * stride + p] = (TH)V0;
+        scr[33 * stride + p] = (TH)m3_contract(F, F);
+        M3<T> VP = P;
+#pragma unroll
+        for (int i = 0; i < 9; ++i) VP.a[i] *= V0;
+        return m3_mulT(VP, Fn);
+    }
+    if (kind == ZMPM_MODEL_STVK_HENCKY_ISOTROPIC || kind == ZMPM_MODEL_FIXED_COROTATED) {
+        M3<T> U, V;
+        T sg[3];
+        svd3(F, U, sg, V);
+        T psi[3], c[12];
+        iso_coefficients(kind, (T)mp.mu, (T)mp.lambda, sg, psi, c);
+        M3<T> P = m3_udvt(U, psi, V);
+        M3<T> W = m3_mul(Fn, V);
+#pragma unroll
+        for (int i = 0; i < 9; ++i) {
+            scr[i * stride + p] = (TH)U.a[i];
+            scr[(9 + i) * stride + p] = (TH)W.a[i];
+        }
+#pragma unroll
+        for (int i = 0; i < 12; ++i) scr[(18 + i) * stride + p] = (TH)(c[i] * V0);
+        M3<T> VP = P;
+#pragma unroll
+        for (int i = 0; i < 9; ++i) VP.a[i] *= V0;
+        return m3_mulT(VP, Fn);
+    }
+    return m3_zero<T>();
+}
+
+// dS = V0 dP(G Fn) Fn^T from the stored scratch; G = grad(dv) at the particle.
+template <class TH>
+ZMPM_D M3<TH> model_hvp(int kind, const TH* __restrict__ scr, int64_t stride, int64_t p, const M3<TH>& G)
+{
+    if (kind == ZMPM_MODEL_NEOHOOKEAN_BORDEN) {
+        M3<TH> F, FinvT, Fn;
+#pragma unroll
+        for (int i = 0; i < 9; ++i) {
+            F.a[i] = scr[i * stride + p];
+            FinvT.a[i] = scr[(9 + i) * stride + p];
+            Fn.a[i] = scr[(18 + i) * stride + p];
+        }
+        TH J = scr[27 * stride + p], muJ2a = scr[28 * stride + p], prime = scr[29 * stride + p];
+        TH prime2 = scr[30 * stride + p], g = scr[31 * stride + p], V0 = scr[32 * stride + p];
+        TH FcF = scr[33 * stride + p];
+        M3<TH> dF = m3_mul(G, Fn);
+        // NeoHookeanBorden::firstPiolaDifferential, NeoHookeanBorden.cpp:85-111
+        TH FinvT_dF = m3_contract(FinvT, dF);
+        TH deltaJ = J * FinvT_dF;
+        M3<TH> dFinvT = m3_mul(m3_mulT(FinvT, dF), FinvT); // F^{-T} dF^T F^{-T}
+        TH a = -TH(1) / TH(3);
+        TH F_dF = m3_contract(F, dF);
+        M3<TH> dP;
+#pragma unroll
+        for (int i = 0; i < 9; ++i) {
+            TH dfi = -dFinvT.a[i];
+            TH dev = TH(2) * a * muJ2a * FinvT_dF * (a * FcF * FinvT.a[i] + F.a[i]);
+            dev += muJ2a * (TH(2) * a * F_dF * FinvT.a[i] + a * FcF * dfi + dF.a[i]);
+            TH vol = deltaJ * prime * FinvT.a[i] + J * deltaJ * prime2 * FinvT.a[i] + J * prime * dfi;
+            dP.a[i] = ((J >= TH(1)) ? g * (dev + vol) : g * dev + vol) * V0;
+        }
+        return m3_mulT(dP, Fn);
+    }
+    if (kind == ZMPM_MODEL_STVK_HENCKY_ISOTROPIC || kind == ZMPM_MODEL_FIXED_COROTATED) {
+        M3<TH> U, W;
+        TH c[12];
+#pragma unroll
+        for (int i = 0; i < 9; ++i) {
+            U.a[i] = scr[i * stride + p];
+            W.a[i] = scr[(9 + i) * stride + p];
+        }
+#pragma unroll
+        for (int i = 0; i < 12; ++i) c[i] = scr[(18 + i) * stride + p];
+        M3<TH> D = m3_mul(m3_Tmul(U, G), W);
+        M3<TH> K = iso_contract(c, D);
+        return m3_mulT(m3_mul(U, K), W);
+    }
+    return m3_zero<TH>();
+}
+
+// VonMisesStvkHencky::projectStrain, Lib/Ziran/Physics/PlasticityApplier.cpp:462-502.
+// Returns true when the state changed; updates yield stress and the broken flag.
+template <class T>
+ZMPM_D void von_mises_project(T mu, T lambda, T& yield_stress, T xi, T fail_stress, int& broken, T crack[3], M3<T>& F)
+{
+    M3<T> U, V;
+    T sg[3];
+    svd3(F, U, sg, V);
+    T e[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) e[d] = log(sg[d] > T(1e-4) ? sg[d] : T(1e-4));
+    T tr = e[0] + e[1] + e[2];
+    T h[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) h[d] = e[d] - (tr / T(3));
+    T hn = sqrt(h[0] * h[0] + h[1] * h[1] + h[2] * h[2]);
+    T dg = hn - yield_stress / (T(2) * mu);
+    if (dg <= T(0)) return;
+    yield_stress -= xi * dg;
+    T H[3], eH[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) H[d] = e[d] - (dg / hn) * h[d];
+    T tau0 = T(2) * mu * H[0] + lambda * (H[0] + H[1] + H[2]);
+#pragma unroll
+    for (int d = 0; d < 3; ++d) eH[d] = exp(H[d]);
+    F = m3_udvt(U, eH, V);
+    if (tau0 >= fail_stress) {
+        broken = 1;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) crack[d] = V(d, 0);
+    }
+}
+
+} // namespace zmpm

@@ -1,0 +1,491 @@
+// Particle <-> grid transfers of the implicit substep.
+//
+// Work unit: one CTA per particle group (the particles whose base node lies in
+// one SPGrid page, MpmSimulationBase.cpp:1055-1063).  Every stencil node of
+// those particles lies in the 2x2x2 pages starting at the group's page, whose
+// block indices binning stored in group_nbr[8g..8g+7].
+//
+//  gather  : the 8 page slabs of a grid vector ([3][NPB] contiguous per page)
+//            are staged into shared memory with cp.async.bulk (TMA bulk copy)
+//            completing on an mbarrier; particles read their 27 nodes there.
+//  scatter : particles accumulate into a shared [8][C][NPB] window with shared
+//            atomics; the window is flushed with coalesced global atomics.
+//
+// Kernels
+//  k_p2g     particlesToGridHelper<APIC> (MpmSimulationBase.cpp:563-608)
+//  k_update  MpmForceBase::updatePositionBasedState + rasterizeForceToTVStack
+//            (MpmForceBase.cpp:306-344, 102-152) fused: G2P of grad(vn+dv),
+//            F = (I + dt grad v) Fn, stress and Hessian scratch, force P2G
+//  k_hvp     MpmForceBase::addScaledForceDifferential (MpmForceBase.cpp:259-302)
+//            fused: G2P of grad(dv), dS = V0 dP Fn^T, P2G of dS grad w
+//  k_g2p     gridToParticlesHelper<APIC> (MpmSimulationBase.cpp:906-1016) +
+//            evolveStrain + applyPlasticity (:1018-1030)
+#include "internal.cuh"
+#include "models.cuh"
+
+namespace zmpm {
+
+constexpr int XF_THREADS = 128;
+constexpr long long STAGE_WAIT_LIMIT = 1ll << 22;
+
+// ------------------------------------------------------------ TMA staging --
+__device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, int count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(smem_addr(dst)), "l"(src),
+        "r"(bytes), "r"(smem_addr(bar))
+        : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_addr(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Bounded wait: gives up after STAGE_WAIT_LIMIT polls and raises FLAG_TIMEOUT.
+__device__ __forceinline__ void mbar_wait_bounded(uint64_t* bar, uint32_t parity, int32_t* flags)
+{
+    long long it = 0;
+    while (!mbar_try_wait(bar, parity)) {
+        if (++it > STAGE_WAIT_LIMIT) {
+            atomicOr(flags, (int32_t)FLAG_TIMEOUT);
+            return;
+        }
+    }
+}
+
+// Stages the 8 page slabs ([3][NPB] doubles each) of vector `vec` into win.
+// Must be called by all threads of the CTA; nbr is in shared memory.
+template <int NPB>
+__device__ __forceinline__ void stage_window(double* win, const double* __restrict__ vec, const int32_t* nbr, uint64_t* bar, int32_t* flags)
+{
+    constexpr uint32_t SLAB = 3 * NPB * sizeof(double);
+    if (threadIdx.x == 0) {
+        mbar_init(bar, 1);
+        mbar_expect_tx(bar, 8 * SLAB);
+#pragma unroll
+        for (int t = 0; t < 8; ++t) bulk_g2s(win + t * 3 * NPB, vec + (int64_t)nbr[t] * 3 * NPB, SLAB, bar);
+    }
+    __syncthreads();
+    mbar_wait_bounded(bar, 0, flags);
+}
+
+// ------------------------------------------------------------ B-spline ----
+// Quadratic B-spline weights of one axis from d0 = x/dx - base (BSplines.h:55-81).
+template <class T>
+__device__ __forceinline__ void bspline(T d0, T w[3], T dw[3])
+{
+    T z = T(1.5) - d0;
+    w[0] = T(0.5) * z * z;
+    T d1 = d0 - T(1);
+    w[1] = T(0.75) - d1 * d1;
+    T d2 = T(1) - d1;
+    T zz = T(1.5) - d2;
+    w[2] = T(0.5) * zz * zz;
+    dw[0] = -z;
+    dw[1] = -T(2) * d1;
+    dw[2] = zz;
+}
+
+// Window slot of stencil node (lx+i, ly+j, lz+k): page t in the 2x2x2
+// neighbourhood, element e inside it.
+template <class L>
+__device__ __forceinline__ int win_slot(int wx, int wy, int wz, int& e)
+{
+    int t = ((wx >= L::BX) << 2) | ((wy >= L::BY) << 1) | (wz >= L::BZ);
+    e = L::elem(wx & (L::BX - 1), wy & (L::BY - 1), wz & (L::BZ - 1));
+    return t;
+}
+
+// Iterates the 27 stencil nodes in the order and with the products of
+// MpmGrid::iterateKernel (MpmGrid.h:247-269).  f(t, e, node_offset_ijk, w, dw[3]).
+template <class L, class T, class Fn>
+__device__ __forceinline__ void for_stencil(int lx, int ly, int lz, const T w[3][3], const T dwr[3][3], T inv_dx, Fn&& f)
+{
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        T wi = w[0][i];
+        T dwidxi = inv_dx * dwr[0][i];
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            T wj = w[1][j];
+            T wij = wi * wj;
+            T dwijdxi = dwidxi * wj;
+            T dwijdxj = wi * inv_dx * dwr[1][j];
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                T wk = w[2][k];
+                T wijk = wij * wk;
+                T dw[3] = { dwijdxi * wk, dwijdxj * wk, wij * inv_dx * dwr[2][k] };
+                int e;
+                int t = win_slot<L>(lx + i, ly + j, lz + k, e);
+                f(t, e, i, j, k, wijk, dw);
+            }
+        }
+    }
+}
+
+template <int NC, int NPB, class TA>
+__device__ __forceinline__ void zero_window(TA* acc)
+{
+    for (int i = threadIdx.x; i < 8 * NC * NPB; i += blockDim.x) acc[i] = TA(0);
+}
+// Adds window [8][NC][NPB] into global block-dense arrays.  Component c < NC0
+// goes to `a` ([B][NC0][NPB]), the rest to `b` ([B][NC-NC0][NPB]).
+template <int NC, int NC0, int NPB, class TA>
+__device__ __forceinline__ void flush_window(const TA* acc, const int32_t* nbr, double* __restrict__ a, double* __restrict__ b)
+{
+    for (int i = threadIdx.x; i < 8 * NC * NPB; i += blockDim.x) {
+        TA v = acc[i];
+        if (v == TA(0)) continue;
+        int t = i / (NC * NPB);
+        int r = i - t * NC * NPB;
+        int c = r / NPB;
+        int e = r - c * NPB;
+        int64_t blk = nbr[t];
+        if (c < NC0)
+            atomicAdd(&a[(blk * NC0 + c) * NPB + e], (double)v);
+        else
+            atomicAdd(&b[(blk * (NC - NC0) + (c - NC0)) * NPB + e], (double)v);
+    }
+}
+
+// ------------------------------------------------------------------ P2G ----
+// Also writes each particle's fractional cell offsets (frac) for the FP32 HVP.
+template <class L, class TH>
+__global__ void __launch_bounds__(XF_THREADS) k_p2g(const int32_t* __restrict__ group_start, const int32_t* __restrict__ group_nbr,
+    const double* __restrict__ pd, int64_t cap, const short4* __restrict__ base, double dx, double* __restrict__ gm, double* __restrict__ gmv,
+    TH* __restrict__ frac)
+{
+    constexpr int NPB = L::NPB;
+    __shared__ __align__(16) double acc[8 * 4 * NPB];
+    __shared__ int32_t nbr[8];
+    const int g = blockIdx.x;
+    if (threadIdx.x < 8) nbr[threadIdx.x] = group_nbr[8 * g + threadIdx.x];
+    zero_window<4, NPB>(acc);
+    __syncthreads();
+    const double inv_dx = 1.0 / dx;
+    const int s0 = group_start[g], s1 = group_start[g + 1];
+    for (int s = s0 + threadIdx.x; s < s1; s += blockDim.x) {
+        const short4 b = base[s];
+        double xp[3], w[3][3], dwr[3][3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            xp[d] = pd[(PD_X + d) * cap + s];
+            double d0 = inv_dx * xp[d] - (double)((&b.x)[d]);
+            frac[d * cap + s] = (TH)d0;
+            bspline(d0, w[d], dwr[d]);
+        }
+        const double mass = pd[PD_M * cap + s];
+        double mom[3], Cm[9];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) mom[d] = mass * pd[(PD_V + d) * cap + s];
+#pragma unroll
+        for (int q = 0; q < 9; ++q) Cm[q] = mass * pd[(PD_C + q) * cap + s];
+        const int lx = b.x & (L::BX - 1), ly = b.y & (L::BY - 1), lz = b.z & (L::BZ - 1);
+        for_stencil<L>(lx, ly, lz, w, dwr, inv_dx, [&](int t, int e, int i, int j, int k, double wijk, const double*) {
+            double xi[3] = { (b.x + i) * dx - xp[0], (b.y + j) * dx - xp[1], (b.z + k) * dx - xp[2] };
+            double* a = acc + t * 4 * NPB + e;
+            atomicAdd(a, mass * wijk);
+#pragma unroll
+            for (int r = 0; r < 3; ++r)
+                atomicAdd(a + (1 + r) * NPB, (Cm[3 * r] * xi[0] + Cm[3 * r + 1] * xi[1] + Cm[3 * r + 2] * xi[2] + mom[r]) * wijk);
+        });
+    }
+    __syncthreads();
+    flush_window<4, 1, NPB>(acc, nbr, gm, gmv);
+}
+
+// --------------------------------------------------------------- update ----
+// grad v at the particle from vstar = vn + dv, F = (I + dt grad v) Fn,
+// S = V0 P(F) Fn^T, Hessian scratch, and facc -= sum_p S grad w.
+template <class L, class TH>
+__global__ void __launch_bounds__(XF_THREADS) k_update(const int32_t* __restrict__ group_start, const int32_t* __restrict__ group_nbr,
+    const double* __restrict__ pd, const int32_t* __restrict__ pi, int64_t cap, const short4* __restrict__ base, double dx, double dt,
+    const double* __restrict__ vstar, double* __restrict__ facc, TH* __restrict__ scr, const SolverScalars* __restrict__ sc,
+    int32_t* __restrict__ flags)
+{
+    if (sc && sc->newton_done) return;
+    constexpr int NPB = L::NPB;
+    __shared__ __align__(128) double win[8 * 3 * NPB];
+    __shared__ __align__(16) double acc[8 * 3 * NPB];
+    __shared__ int32_t nbr[8];
+    __shared__ __align__(8) uint64_t bar;
+    const int g = blockIdx.x;
+    if (threadIdx.x < 8) nbr[threadIdx.x] = group_nbr[8 * g + threadIdx.x];
+    zero_window<3, NPB>(acc);
+    __syncthreads();
+    stage_window<NPB>(win, vstar, nbr, &bar, flags);
+    const double inv_dx = 1.0 / dx;
+    const int s0 = group_start[g], s1 = group_start[g + 1];
+    for (int s = s0 + threadIdx.x; s < s1; s += blockDim.x) {
+        const short4 b = base[s];
+        double w[3][3], dwr[3][3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            double d0 = inv_dx * pd[(PD_X + d) * cap + s] - (double)((&b.x)[d]);
+            bspline(d0, w[d], dwr[d]);
+        }
+        const int lx = b.x & (L::BX - 1), ly = b.y & (L::BY - 1), lz = b.z & (L::BZ - 1);
+        M3<double> gv = m3_zero<double>();
+        for_stencil<L>(lx, ly, lz, w, dwr, inv_dx, [&](int t, int e, int, int, int, double, const double* dw) {
+            const double* vv = win + t * 3 * NPB + e;
+#pragma unroll
+            for (int r = 0; r < 3; ++r) {
+                double vr = vv[r * NPB];
+#pragma unroll
+                for (int c = 0; c < 3; ++c) gv(r, c) += vr * dw[c];
+            }
+        });
+        const int kind = pi[PI_KIND * cap + s];
+        if (kind == ZMPM_MODEL_NONE) continue;
+        M3<double> Fn, A = m3_identity<double>();
+#pragma unroll
+        for (int q = 0; q < 9; ++q) {
+            Fn.a[q] = pd[(PD_F + q) * cap + s];
+            A.a[q] += dt * gv.a[q];
+        }
+        M3<double> F = m3_mul(A, Fn);
+        ModelParams mp{ pd[PD_MU * cap + s], pd[PD_LAM * cap + s], pd[PD_KAPPA * cap + s], pd[PD_G * cap + s] };
+        M3<double> S = model_update<double, TH>(kind, mp, pd[PD_VOL * cap + s], F, Fn, scr, cap, s);
+        for_stencil<L>(lx, ly, lz, w, dwr, inv_dx, [&](int t, int e, int, int, int, double, const double* dw) {
+            double* a = acc + t * 3 * NPB + e;
+#pragma unroll
+            for (int r = 0; r < 3; ++r) atomicAdd(a + r * NPB, -(S(r, 0) * dw[0] + S(r, 1) * dw[1] + S(r, 2) * dw[2]));
+        });
+    }
+    __syncthreads();
+    flush_window<3, 3, NPB>(acc, nbr, facc, nullptr);
+}
+
+// ------------------------------------------------------------------ HVP ----
+// out += sum_p dS_p grad w_ip with dS = V0 dP(grad(x) Fn) Fn^T; TH is the
+// arithmetic precision (float in mixed runs).  Skipped when the linear solve
+// is inactive.
+template <class L, class TH>
+__global__ void __launch_bounds__(XF_THREADS) k_hvp(const int32_t* __restrict__ group_start, const int32_t* __restrict__ group_nbr,
+    const int32_t* __restrict__ pi, int64_t cap, const short4* __restrict__ base, double dx, const TH* __restrict__ frac,
+    const TH* __restrict__ scr, const double* __restrict__ x, double* __restrict__ out, const SolverScalars* __restrict__ sc,
+    int32_t* __restrict__ flags)
+{
+    if (sc && (sc->newton_done || !sc->krylov_active)) return;
+    constexpr int NPB = L::NPB;
+    __shared__ __align__(128) double win[8 * 3 * NPB];
+    __shared__ __align__(16) TH acc[8 * 3 * NPB];
+    __shared__ int32_t nbr[8];
+    __shared__ __align__(8) uint64_t bar;
+    const int g = blockIdx.x;
+    if (threadIdx.x < 8) nbr[threadIdx.x] = group_nbr[8 * g + threadIdx.x];
+    zero_window<3, NPB>(acc);
+    __syncthreads();
+    stage_window<NPB>(win, x, nbr, &bar, flags);
+    const TH inv_dx = TH(1.0 / dx);
+    const int s0 = group_start[g], s1 = group_start[g + 1];
+    for (int s = s0 + threadIdx.x; s < s1; s += blockDim.x) {
+        const int kind = pi[PI_KIND * cap + s];
+        if (kind == ZMPM_MODEL_NONE) continue;
+        const short4 b = base[s];
+        TH w[3][3], dwr[3][3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) bspline(frac[d * cap + s], w[d], dwr[d]);
+        const int lx = b.x & (L::BX - 1), ly = b.y & (L::BY - 1), lz = b.z & (L::BZ - 1);
+        M3<TH> G = m3_zero<TH>();
+        for_stencil<L>(lx, ly, lz, w, dwr, inv_dx, [&](int t, int e, int, int, int, TH, const TH* dw) {
+            const double* vv = win + t * 3 * NPB + e;
+#pragma unroll
+            for (int r = 0; r < 3; ++r) {
+                TH vr = (TH)vv[r * NPB];
+#pragma unroll
+                for (int c = 0; c < 3; ++c) G(r, c) += vr * dw[c];
+            }
+        });
+        M3<TH> dS = model_hvp<TH>(kind, scr, cap, s, G);
+        for_stencil<L>(lx, ly, lz, w, dwr, inv_dx, [&](int t, int e, int, int, int, TH, const TH* dw) {
+            TH* a = acc + t * 3 * NPB + e;
+#pragma unroll
+            for (int r = 0; r < 3; ++r) atomicAdd(a + r * NPB, dS(r, 0) * dw[0] + dS(r, 1) * dw[1] + dS(r, 2) * dw[2]);
+        });
+    }
+    __syncthreads();
+    flush_window<3, 3, NPB>(acc, nbr, out, nullptr);
+}
+
+// ------------------------------------------------------------------ G2P ----
+template <class L>
+__global__ void __launch_bounds__(XF_THREADS) k_g2p(const int32_t* __restrict__ group_start, const int32_t* __restrict__ group_nbr,
+    double* __restrict__ pd, int32_t* __restrict__ pi, int64_t cap, const short4* __restrict__ base, double dx, double dt,
+    double apic_rpic_ratio, const double* __restrict__ vnew, int32_t* __restrict__ flags)
+{
+    constexpr int NPB = L::NPB;
+    __shared__ __align__(128) double win[8 * 3 * NPB];
+    __shared__ int32_t nbr[8];
+    __shared__ __align__(8) uint64_t bar;
+    const int g = blockIdx.x;
+    if (threadIdx.x < 8) nbr[threadIdx.x] = group_nbr[8 * g + threadIdx.x];
+    __syncthreads();
+    stage_window<NPB>(win, vnew, nbr, &bar, flags);
+    const double inv_dx = 1.0 / dx;
+    const double D_inverse = 4.0 / (dx * dx);
+    const double ca = (apic_rpic_ratio + 1) * 0.5, cb = (apic_rpic_ratio - 1) * 0.5;
+    int too_fast = 0;
+    const int s0 = group_start[g], s1 = group_start[g + 1];
+    for (int s = s0 + threadIdx.x; s < s1; s += blockDim.x) {
+        const short4 b = base[s];
+        double xp[3], w[3][3], dwr[3][3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            xp[d] = pd[(PD_X + d) * cap + s];
+            bspline(inv_dx * xp[d] - (double)((&b.x)[d]), w[d], dwr[d]);
+        }
+        const int lx = b.x & (L::BX - 1), ly = b.y & (L::BY - 1), lz = b.z & (L::BZ - 1);
+        double pv[3] = { 0, 0, 0 };
+        M3<double> Bp = m3_zero<double>(), gv = m3_zero<double>();
+        for_stencil<L>(lx, ly, lz, w, dwr, inv_dx, [&](int t, int e, int i, int j, int k, double wijk, const double* dw) {
+            const double* vv = win + t * 3 * NPB + e;
+            double xi[3] = { (b.x + i) * dx - xp[0], (b.y + j) * dx - xp[1], (b.z + k) * dx - xp[2] };
+#pragma unroll
+            for (int r = 0; r < 3; ++r) {
+                double vr = vv[r * NPB];
+                pv[r] += wijk * vr;
+#pragma unroll
+                for (int c = 0; c < 3; ++c) {
+                    Bp(r, c) += wijk * vr * xi[c];
+                    gv(r, c) += vr * dw[c];
+                }
+            }
+        });
+        double inc2 = 0;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            pd[(PD_V + d) * cap + s] = pv[d];
+            double inc = dt * pv[d];
+            pd[(PD_X + d) * cap + s] = xp[d] + inc;
+            inc2 += inc * inc;
+        }
+        too_fast |= (inc2 > dx * dx);
+#pragma unroll
+        for (int r = 0; r < 3; ++r)
+#pragma unroll
+            for (int c = 0; c < 3; ++c) pd[(PD_C + 3 * r + c) * cap + s] = ca * (Bp(r, c) * D_inverse) + cb * (Bp(c, r) * D_inverse);
+        const int kind = pi[PI_KIND * cap + s];
+        if (kind == ZMPM_MODEL_NONE) continue;
+        // evolveStrain (FBasedMpmForceHelper.cpp:95-109) on the restored F = Fn
+        M3<double> F0, A = m3_identity<double>();
+#pragma unroll
+        for (int q = 0; q < 9; ++q) {
+            F0.a[q] = pd[(PD_F + q) * cap + s];
+            A.a[q] += dt * gv.a[q];
+        }
+        M3<double> F = m3_mul(A, F0);
+        if (pi[PI_PKIND * cap + s] == ZMPM_PLASTIC_VON_MISES) {
+            double ys = pd[PD_YS * cap + s];
+            int broken = pi[PI_BROKEN * cap + s];
+            double crack[3] = { pd[(PD_CRACK + 0) * cap + s], pd[(PD_CRACK + 1) * cap + s], pd[(PD_CRACK + 2) * cap + s] };
+            von_mises_project<double>(pd[PD_MU * cap + s], pd[PD_LAM * cap + s], ys, pd[PD_XI * cap + s], pd[PD_FS * cap + s], broken, crack, F);
+            pd[PD_YS * cap + s] = ys;
+            pi[PI_BROKEN * cap + s] = broken;
+#pragma unroll
+            for (int d = 0; d < 3; ++d) pd[(PD_CRACK + d) * cap + s] = crack[d];
+        }
+#pragma unroll
+        for (int q = 0; q < 9; ++q) pd[(PD_F + q) * cap + s] = F.a[q];
+    }
+    if (__syncthreads_or(too_fast) && threadIdx.x == 0) atomicOr(flags, (int32_t)FLAG_CFL);
+}
+
+// ------------------------------------------------------------- launchers --
+template <class L>
+static int p2g_impl(Ctx* ctx)
+{
+    const int64_t G = ctx->G;
+    if (G == 0) return ZMPM_OK;
+    if (ctx->mixed)
+        k_p2g<L, float><<<(unsigned)G, XF_THREADS, 0, ctx->stream>>>(ctx->group_start.as<int32_t>(), ctx->group_nbr.as<int32_t>(), ctx->pd.as<double>(),
+            ctx->Pcap, ctx->base.as<short4>(), ctx->cfg.dx, ctx->gm.as<double>(), ctx->gmv.as<double>(), ctx->frac.as<float>());
+    else
+        k_p2g<L, double><<<(unsigned)G, XF_THREADS, 0, ctx->stream>>>(ctx->group_start.as<int32_t>(), ctx->group_nbr.as<int32_t>(), ctx->pd.as<double>(),
+            ctx->Pcap, ctx->base.as<short4>(), ctx->cfg.dx, ctx->gm.as<double>(), ctx->gmv.as<double>(), ctx->frac.as<double>());
+    ++g_kernel_launches;
+    return ZMPM_OK;
+}
+int launch_p2g(Ctx* ctx) { return ctx->layout == 1 ? p2g_impl<Layout244>(ctx) : p2g_impl<Layout444>(ctx); }
+
+template <class L>
+static int update_impl(Ctx* ctx)
+{
+    const int64_t G = ctx->G;
+    if (G == 0) return ZMPM_OK;
+    DevCounters* dc = ctx->counters.as<DevCounters>();
+    const SolverScalars* sc = ctx->scal.as<SolverScalars>();
+    if (ctx->mixed)
+        k_update<L, float><<<(unsigned)G, XF_THREADS, 0, ctx->stream>>>(ctx->group_start.as<int32_t>(), ctx->group_nbr.as<int32_t>(),
+            ctx->pd.as<double>(), ctx->pi.as<int32_t>(), ctx->Pcap, ctx->base.as<short4>(), ctx->cfg.dx, ctx->dt, ctx->vstar.as<double>(),
+            ctx->facc.as<double>(), ctx->scratch.as<float>(), sc, &dc->flags);
+    else
+        k_update<L, double><<<(unsigned)G, XF_THREADS, 0, ctx->stream>>>(ctx->group_start.as<int32_t>(), ctx->group_nbr.as<int32_t>(),
+            ctx->pd.as<double>(), ctx->pi.as<int32_t>(), ctx->Pcap, ctx->base.as<short4>(), ctx->cfg.dx, ctx->dt, ctx->vstar.as<double>(),
+            ctx->facc.as<double>(), ctx->scratch.as<double>(), sc, &dc->flags);
+    ++g_kernel_launches;
+    return ZMPM_OK;
+}
+int launch_update(Ctx* ctx) { return ctx->layout == 1 ? update_impl<Layout244>(ctx) : update_impl<Layout444>(ctx); }
+
+template <class L>
+static int hvp_impl(Ctx* ctx, const double* x, double* out, bool fp32, bool gated)
+{
+    const int64_t G = ctx->G;
+    if (G == 0) return ZMPM_OK;
+    DevCounters* dc = ctx->counters.as<DevCounters>();
+    const SolverScalars* sc = gated ? ctx->scal.as<SolverScalars>() : nullptr;
+    if (fp32)
+        k_hvp<L, float><<<(unsigned)G, XF_THREADS, 0, ctx->stream>>>(ctx->group_start.as<int32_t>(), ctx->group_nbr.as<int32_t>(),
+            ctx->pi.as<int32_t>(), ctx->Pcap, ctx->base.as<short4>(), ctx->cfg.dx, ctx->frac.as<float>(), ctx->scratch.as<float>(), x, out, sc,
+            &dc->flags);
+    else
+        k_hvp<L, double><<<(unsigned)G, XF_THREADS, 0, ctx->stream>>>(ctx->group_start.as<int32_t>(), ctx->group_nbr.as<int32_t>(),
+            ctx->pi.as<int32_t>(), ctx->Pcap, ctx->base.as<short4>(), ctx->cfg.dx, ctx->frac.as<double>(), ctx->scratch.as<double>(), x, out, sc,
+            &dc->flags);
+    ++g_kernel_launches;
+    return ZMPM_OK;
+}
+int launch_hvp_gated(Ctx* ctx, const double* x, double* out, bool gated)
+{
+    bool fp32 = ctx->mixed;
+    return ctx->layout == 1 ? hvp_impl<Layout244>(ctx, x, out, fp32, gated) : hvp_impl<Layout444>(ctx, x, out, fp32, gated);
+}
+int launch_hvp(Ctx* ctx, const double* x, double* out, bool fp32)
+{
+    if (fp32 && !ctx->mixed) return ZMPM_UNSUPPORTED;
+    return ctx->layout == 1 ? hvp_impl<Layout244>(ctx, x, out, ctx->mixed, false) : hvp_impl<Layout444>(ctx, x, out, ctx->mixed, false);
+}
+
+template <class L>
+static int g2p_impl(Ctx* ctx)
+{
+    const int64_t G = ctx->G;
+    if (G == 0) return ZMPM_OK;
+    DevCounters* dc = ctx->counters.as<DevCounters>();
+    k_g2p<L><<<(unsigned)G, XF_THREADS, 0, ctx->stream>>>(ctx->group_start.as<int32_t>(), ctx->group_nbr.as<int32_t>(), ctx->pd.as<double>(),
+        ctx->pi.as<int32_t>(), ctx->Pcap, ctx->base.as<short4>(), ctx->cfg.dx, ctx->dt, ctx->cfg.apic_rpic_ratio, ctx->vstar.as<double>(), &dc->flags);
+    ++g_kernel_launches;
+    return ZMPM_OK;
+}
+int launch_g2p(Ctx* ctx) { return ctx->layout == 1 ? g2p_impl<Layout244>(ctx) : g2p_impl<Layout444>(ctx); }
+
+} // namespace zmpm
