@@ -66,10 +66,10 @@ def scene(n_boxes=4, seed_pos=1, seed_vel=2, seed_jit=0, velocity="particle"):
     return x, v
 
 
-def make_sim(x, v, precision, lib=None, model="hencky"):
+def make_sim(x, v, precision, lib=None, model="hencky", layout="auto"):
     from ziran2019_b200 import abi, mpm
 
-    sim = mpm.MpmSimulation(DX, gravity=(0, -9.8, 0), precision=precision, grid_log2=9,
+    sim = mpm.MpmSimulation(DX, gravity=(0, -9.8, 0), precision=precision, grid_log2=9, layout=layout,
                             device=int(os.environ.get("LOCAL_RANK", "0")) if lib is None else 0, lib=lib)
     V0 = DX ** 3 / PPC
     h = sim.addParticles(x, v, RHO * V0, V0)
@@ -217,6 +217,10 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--model", default="hencky", choices=["hencky", "nh"])
     ap.add_argument("--velocity", default="particle", choices=["particle", "box"])
+    ap.add_argument("--only", default=None, choices=["fp64", "mixed"], help="time one precision (profiling runs)")
+    ap.add_argument("--boxes", type=int, default=4, help="boxes of 250k particles (profiling runs use fewer)")
+    ap.add_argument("--fp64-layout", default="444", choices=["444", "auto"],
+                    help="page layout of the FP64 substep: 444 = same as the mixed run (only precision differs)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -230,12 +234,21 @@ def main():
     from ziran2019_b200 import build
     build.build()
     dev = int(os.environ.get("LOCAL_RANK", "0"))
-    x, v = scene(velocity=args.velocity)
+    x, v = scene(n_boxes=args.boxes, velocity=args.velocity)
     P = x.shape[0]
-    sims = {p: make_sim(x, v, p, model=args.model) for p in ("fp64", "mixed")}
-    for p in ("fp64", "mixed"):
+    precs = [args.only] if args.only else ["fp64", "mixed"]
+    sims = {p: make_sim(x, v, p, model=args.model, layout=args.fp64_layout if p == "fp64" else "auto") for p in precs}
+    for p in precs:
         for _ in range(args.warmup):
             sims[p].advanceOneTimeStep(DT)
+    if args.only:
+        ms, st = timed_steps(sims[args.only], args.steps, world, profile=True)
+        if rank == 0:
+            print(json.dumps({"only": args.only, "particles": P, "ms_per_step": ms / args.steps,
+                              "hvp_ms": sum(s["ms_hvp"] for s in st) / max(1, sum(s["hvp_timed"] for s in st)),
+                              "launches_per_step": st[-1]["kernel_launches"], "newton_krylov": [st[-1]["newton_iterations"], st[-1]["krylov_iterations"]]}),
+                  flush=True)
+        return
     ms64, st64 = timed_steps(sims["fp64"], args.steps, world)
     clocks = Clocks(dev)
     clocks.start()
@@ -318,7 +331,7 @@ def main():
             "ms_per_step": ms_mx / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "fp32 Hessian products, fp64 state/residual/reductions", "data": "synthetic",
             "config": {"workload": "config1-elastoplastic-4boxes", "particles": P, "dx": DX, "dt": DT,
-                       "model": f"{args.model}+von Mises", "velocity": args.velocity, "solver": "MINRES, Newton 3 x Krylov 20 (reference defaults)",
+                       "model": f"{args.model}+von Mises", "velocity": args.velocity, "fp64_layout": args.fp64_layout, "solver": "MINRES, Newton 3 x Krylov 20 (reference defaults)",
                        "parallelism": f"replicas x{world}", "l2": "inputs larger than L2 (particle state ~300 MB)"},
             "particles_substeps_per_s": value * P,
             "fp64_value": fp64_value, "mixed_over_fp64": value / fp64_value,

@@ -4,6 +4,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <cstdlib>
 #include <new>
 
 #include "internal.cuh"
@@ -51,6 +52,8 @@ int upload(Ctx* ctx)
     ZMPM_CUDA(ctx->base.ensure(cap * sizeof(short4)));
     ZMPM_CUDA(ctx->scratch.ensure(NS * cap * TH));
     ZMPM_CUDA(ctx->frac.ensure(3 * cap * TH));
+    ZMPM_CUDA(ctx->stress.ensure(9 * cap * sizeof(double)));
+    ZMPM_CUDA(ctx->dstress.ensure(9 * cap * TH));
     std::vector<double> hpd((size_t)PD_FIELDS * cap, 0.0);
     std::vector<int32_t> hpi((size_t)PI_FIELDS * cap, 0), sid(cap);
     for (int64_t i = 0; i < P; ++i) {
@@ -335,6 +338,10 @@ int zmpm_create(const zmpm_config* cfg, zmpm_ctx** out)
     }
     ctx->device = cfg->device;
     ctx->grid_log2 = cfg->grid_log2;
+    {
+        const char* f = getenv("ZMPM_HVP_FUSED");
+        ctx->hvp_fused = f && f[0] == '1';
+    }
     auto fail = [&](cudaError_t e) {
         ctx->err = cudaGetErrorString(e);
         delete ctx;
@@ -378,7 +385,7 @@ int zmpm_destroy(zmpm_ctx* ctx)
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     DBuf* bufs[] = { &ctx->pd, &ctx->pd_alt, &ctx->pi, &ctx->pi_alt, &ctx->slot_of_id, &ctx->base_by_id, &ctx->base, &ctx->Fn, &ctx->scratch,
-        &ctx->frac, &ctx->keys, &ctx->keys_alt, &ctx->flags_i32, &ctx->scan_i32, &ctx->scan_scr, &ctx->radix_scr, &ctx->group_start,
+        &ctx->frac, &ctx->stress, &ctx->dstress, &ctx->keys, &ctx->keys_alt, &ctx->flags_i32, &ctx->scan_i32, &ctx->scan_scr, &ctx->radix_scr, &ctx->group_start,
         &ctx->group_page, &ctx->group_nbr, &ctx->emit_flag, &ctx->emit_scan, &ctx->page_first, &ctx->page_block, &ctx->block_page,
         &ctx->block_index, &ctx->gm, &ctx->gmv, &ctx->vn, &ctx->dv, &ctx->vstar, &ctx->facc, &ctx->res, &ctx->proj, &ctx->collided,
         &ctx->node_idx, &ctx->red, &ctx->scal, &ctx->counters, &ctx->dcolliders };

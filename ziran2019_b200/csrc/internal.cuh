@@ -61,7 +61,8 @@ struct DevCounters {
 // read the previous value while CTA 0 writes the next one.
 struct SolverScalars {
     int32_t newton_done;       // 1 once the Newton norm fell below tolerance (or NaN)
-    int32_t krylov_active;     // 1 while the current linear solve iterates
+    int32_t stop_at;           // Krylov iterations it >= stop_at are skipped (latched by the
+                               // iteration that converged; read only by later kernels)
     int32_t newton_iters;      // linear solves run
     int32_t krylov_iters;      // summed Krylov iterations
     int32_t hvp_count;
@@ -121,6 +122,9 @@ struct Ctx {
     DBuf base;         // short4 base node per slot
     DBuf Fn;           // [9][Pcap] F at the start of the Newton solve
     DBuf scratch;      // Hessian scratch [NS][Pcap] in the HVP precision
+    DBuf stress;       // [9][Pcap] V0 P(F) Fn^T of the current Newton iterate
+    DBuf dstress;      // [9][Pcap] dS of one Hessian-vector product (HVP precision)
+    bool hvp_fused = false; // one fused HVP kernel instead of stress + scatter
     DBuf frac;         // [3][Pcap] fractional offsets in cells (FP32 HVP)
     double* pdf(int f) const { return pd.as<double>() + (int64_t)f * Pcap; }
     int32_t* pif(int f) const { return pi.as<int32_t>() + (int64_t)f * Pcap; }

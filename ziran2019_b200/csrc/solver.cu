@@ -26,7 +26,7 @@ constexpr int ND_THREADS = 256;
 
 int launch_p2g(Ctx* ctx);
 int launch_g2p(Ctx* ctx);
-int launch_hvp_gated(Ctx* ctx, const double* x, double* out, bool gated);
+int launch_hvp_gated(Ctx* ctx, const double* x, double* out, bool gated, int it);
 
 // ------------------------------------------------------------ reductions --
 __device__ __forceinline__ double warp_sum(double v)
@@ -317,7 +317,7 @@ __global__ void __launch_bounds__(ND_THREADS) k_newton_check(NodeGeom ng, const 
         if (done) {
             sc->newton_done = 1;
             sc->converged = (norm == norm) ? 1 : 0;
-            sc->krylov_active = 0;
+            sc->stop_at = 0;
         }
         else {
             double mx = norm > np.tol ? norm : np.tol;
@@ -369,7 +369,7 @@ __global__ void __launch_bounds__(ND_THREADS) k_krylov_start(NodeGeom ng, Krylov
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         sc->rnorm = rnorm;
         sc->local_tol = lt;
-        sc->krylov_active = active ? 1 : 0;
+        sc->stop_at = active ? 0x7fffffff : 0;
         if (np.minres) {
             double* mr = sc->mr[0];
             mr[MR_GC0] = mr[MR_GC1] = mr[MR_GC2] = 1;
@@ -396,9 +396,9 @@ __global__ void __launch_bounds__(ND_THREADS) k_krylov_start(NodeGeom ng, Krylov
 template <int NPB>
 __global__ void __launch_bounds__(ND_THREADS) k_apply_A(NodeGeom ng, const double* __restrict__ gm, const int8_t* __restrict__ col,
     const double* __restrict__ P6, double dt2, const double* __restrict__ xin, double* __restrict__ hacc, double* __restrict__ out,
-    double* __restrict__ part, const SolverScalars* __restrict__ sc, int gated, int project)
+    double* __restrict__ part, const SolverScalars* __restrict__ sc, int gated, int project, int it)
 {
-    if (gated && (sc->newton_done || !sc->krylov_active)) return;
+    if (gated && (sc->newton_done || it >= sc->stop_at)) return;
     double acc = 0;
     for (int64_t n = (int64_t)blockIdx.x * ND_THREADS + threadIdx.x; n < ng.nn; n += (int64_t)gridDim.x * ND_THREADS) {
         const double m = gm[n];
@@ -427,7 +427,7 @@ template <int NPB>
 __global__ void __launch_bounds__(ND_THREADS) k_cg_b(NodeGeom ng, const double* __restrict__ gm, KrylovBufs kb, const double* __restrict__ part_in,
     double* __restrict__ part_out, const SolverScalars* __restrict__ sc, int it)
 {
-    if (sc->newton_done || !sc->krylov_active) return;
+    if (sc->newton_done || it >= sc->stop_at) return;
     const double alpha = sc->mr[it & 1][0] / reduce_partials(part_in, ng.parts);
     double acc = 0;
     for (int64_t n = (int64_t)blockIdx.x * ND_THREADS + threadIdx.x; n < ng.nn; n += (int64_t)gridDim.x * ND_THREADS) {
@@ -451,7 +451,7 @@ template <int NPB>
 __global__ void __launch_bounds__(ND_THREADS) k_cg_c(NodeGeom ng, KrylovBufs kb, const double* __restrict__ part_in, SolverScalars* __restrict__ sc, int it,
     int nit)
 {
-    if (sc->newton_done || !sc->krylov_active) return;
+    if (sc->newton_done || it >= sc->stop_at) return;
     const double zTrk = reduce_partials(part_in, ng.parts);
     const double beta = zTrk / sc->mr[it & 1][0];
     const double rnorm = sqrt(zTrk);
@@ -462,6 +462,7 @@ __global__ void __launch_bounds__(ND_THREADS) k_cg_c(NodeGeom ng, KrylovBufs kb,
         sc->krylov_iters += 1;
         sc->hvp_count += 1;
         if (nit < 64) sc->kcount[nit] += 1;
+        if (rnorm < sc->local_tol) sc->stop_at = it + 1; // the reference tests at the next loop top
     }
     for (int64_t n = (int64_t)blockIdx.x * ND_THREADS + threadIdx.x; n < ng.nn; n += (int64_t)gridDim.x * ND_THREADS)
         for (int k = 0; k < 3; ++k) {
@@ -477,7 +478,7 @@ __global__ void __launch_bounds__(ND_THREADS) k_mr_b(NodeGeom ng, const double* 
     const double* __restrict__ qk, const double* __restrict__ qkm1, double* __restrict__ zout, const double* __restrict__ part_in,
     double* __restrict__ part_out, const SolverScalars* __restrict__ sc, int it)
 {
-    if (sc->newton_done || !sc->krylov_active) return;
+    if (sc->newton_done || it >= sc->stop_at) return;
     const double alpha = reduce_partials(part_in, ng.parts);
     const double beta_k = sc->mr[it & 1][MR_BETA_KP1];
     double acc = 0;
@@ -508,7 +509,7 @@ __global__ void __launch_bounds__(ND_THREADS) k_mr_c(NodeGeom ng, double* __rest
     const double* __restrict__ zin, const double* __restrict__ mkm1, const double* __restrict__ mkm2, double* __restrict__ mk_out,
     double* __restrict__ x, const double* __restrict__ part_in, SolverScalars* __restrict__ sc, int it, int nit)
 {
-    if (sc->newton_done || !sc->krylov_active) return;
+    if (sc->newton_done || it >= sc->stop_at) return;
     const double dz = reduce_partials(part_in, ng.parts);
     const double* cur = sc->mr[it & 1];
     const double alpha_k = sc->mr[(it + 1) & 1][MR_TK];
@@ -552,6 +553,7 @@ __global__ void __launch_bounds__(ND_THREADS) k_mr_c(NodeGeom ng, double* __rest
         sc->krylov_iters += 1;
         sc->hvp_count += 1;
         if (nit < 64) sc->kcount[nit] += 1;
+        if (rnorm < sc->local_tol) sc->stop_at = it + 1; // the reference tests at the next loop top
     }
     const bool norm = beta_kp1 > 0;
     for (int64_t n = (int64_t)blockIdx.x * ND_THREADS + threadIdx.x; n < ng.nn; n += (int64_t)gridDim.x * ND_THREADS)
@@ -567,15 +569,6 @@ __global__ void __launch_bounds__(ND_THREADS) k_mr_c(NodeGeom ng, double* __rest
         }
 }
 
-// Convergence test of the linear solve, run as its own kernel after the
-// iteration's last node kernel (the reference tests at the loop top).  Clearing
-// krylov_active inside that node kernel would let later CTAs of the same
-// launch skip their share of the update.
-__global__ void k_krylov_check(SolverScalars* __restrict__ sc)
-{
-    if (sc->newton_done || !sc->krylov_active) return;
-    if (sc->rnorm < sc->local_tol) sc->krylov_active = 0;
-}
 
 // dv += step; vstar = vn + dv on active nodes.
 template <int NPB>
@@ -680,10 +673,10 @@ int finalize_multiply(Ctx* ctx, const double* x, double* q)
     const double dt2 = ctx->dt * ctx->dt;
     if (ctx->layout == 1)
         k_apply_A<32><<<ng.parts, ND_THREADS, 0, ctx->stream>>>(ng, ctx->gm.as<double>(), ctx->collided.as<int8_t>(), ctx->proj.as<double>(), dt2, x,
-            ctx->kv[9].as<double>(), q, nullptr, nullptr, 0, 0);
+            ctx->kv[9].as<double>(), q, nullptr, nullptr, 0, 0, 0);
     else
         k_apply_A<64><<<ng.parts, ND_THREADS, 0, ctx->stream>>>(ng, ctx->gm.as<double>(), ctx->collided.as<int8_t>(), ctx->proj.as<double>(), dt2, x,
-            ctx->kv[9].as<double>(), q, nullptr, nullptr, 0, 0);
+            ctx->kv[9].as<double>(), q, nullptr, nullptr, 0, 0, 0);
     ++g_kernel_launches;
     return ZMPM_OK;
 }
@@ -749,30 +742,26 @@ static int newton_impl(Ctx* ctx, const zmpm_solver& s)
                 double* mkm1 = kb.M[(k + 2) % 3];
                 double* mkm2 = kb.M[(k + 1) % 3];
                 if (prof) ZMPM_CUDA(cudaEventRecord(ctx->hvp_ev[2 * (it * s.krylov_max_iterations + k)], st));
-                launch_hvp_gated(ctx, zin, kb.hacc, true);
+                launch_hvp_gated(ctx, zin, kb.hacc, true, k);
                 if (prof) ZMPM_CUDA(cudaEventRecord(ctx->hvp_ev[2 * (it * s.krylov_max_iterations + k) + 1], st));
                 k_apply_A<NPB><<<nb, ND_THREADS, 0, st>>>(ng, ctx->gm.as<double>(), ctx->collided.as<int8_t>(), ctx->proj.as<double>(), dt2, zin,
-                    kb.hacc, qkp1, pA, sc, 1, 1);
+                    kb.hacc, qkp1, pA, sc, 1, 1, k);
                 ++g_kernel_launches;
                 k_mr_b<NPB><<<nb, ND_THREADS, 0, st>>>(ng, ctx->gm.as<double>(), qkp1, qk, qkm1, zout, pA, pC, sc, k);
                 ++g_kernel_launches;
                 k_mr_c<NPB><<<nb, ND_THREADS, 0, st>>>(ng, qkp1, zout, zin, mkm1, mkm2, mk, kb.x, pC, sc, k, it);
                 ++g_kernel_launches;
-                k_krylov_check<<<1, 1, 0, st>>>(sc);
-                ++g_kernel_launches;
             }
             else {
                 if (prof) ZMPM_CUDA(cudaEventRecord(ctx->hvp_ev[2 * (it * s.krylov_max_iterations + k)], st));
-                launch_hvp_gated(ctx, kb.p, kb.hacc, true);
+                launch_hvp_gated(ctx, kb.p, kb.hacc, true, k);
                 if (prof) ZMPM_CUDA(cudaEventRecord(ctx->hvp_ev[2 * (it * s.krylov_max_iterations + k) + 1], st));
                 k_apply_A<NPB><<<nb, ND_THREADS, 0, st>>>(ng, ctx->gm.as<double>(), ctx->collided.as<int8_t>(), ctx->proj.as<double>(), dt2, kb.p,
-                    kb.hacc, kb.tmp, pA, sc, 1, 1);
+                    kb.hacc, kb.tmp, pA, sc, 1, 1, k);
                 ++g_kernel_launches;
                 k_cg_b<NPB><<<nb, ND_THREADS, 0, st>>>(ng, ctx->gm.as<double>(), kb, pA, pC, sc, k);
                 ++g_kernel_launches;
                 k_cg_c<NPB><<<nb, ND_THREADS, 0, st>>>(ng, kb, pC, sc, k, it);
-                ++g_kernel_launches;
-                k_krylov_check<<<1, 1, 0, st>>>(sc);
                 ++g_kernel_launches;
             }
         }

@@ -166,6 +166,63 @@ __device__ __forceinline__ void flush_window(const TA* acc, const int32_t* nbr, 
     }
 }
 
+
+// ------------------------------------------------------ scatter ordering --
+// Particles of a group are sorted by cell (element) then index.  Shared-memory
+// scatters are issued in "layers": thread q handles the r-th particle (r = q /
+// NPB) of cell e = q % NPB, so the 32 lanes of a warp hold particles of 32
+// different cells and a warp-wide atomic at a fixed stencil offset never hits
+// the same node twice.  A page holds NPB cells; cnt/start are per-cell counts
+// and first slots inside the group.
+template <class L>
+struct CellLayout {
+    int cnt[L::NPB];
+    int start[L::NPB];
+    int layers;
+};
+
+template <class L>
+__device__ __forceinline__ void build_cell_layout(CellLayout<L>& cl, const short4* __restrict__ base, int s0, int s1)
+{
+    for (int e = threadIdx.x; e < L::NPB; e += blockDim.x) cl.cnt[e] = 0;
+    __syncthreads();
+    for (int s = s0 + threadIdx.x; s < s1; s += blockDim.x) {
+        const short4 b = base[s];
+        atomicAdd(&cl.cnt[L::elem(b.x & (L::BX - 1), b.y & (L::BY - 1), b.z & (L::BZ - 1))], 1);
+    }
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        constexpr int PER = L::NPB / 32;
+        const int lane = threadIdx.x;
+        int c[PER], local = 0, mx = 0;
+#pragma unroll
+        for (int k = 0; k < PER; ++k) {
+            c[k] = cl.cnt[lane * PER + k];
+            local += c[k];
+            mx = c[k] > mx ? c[k] : mx;
+        }
+        int incl = local;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            int n = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += n;
+        }
+        int run = incl - local;
+#pragma unroll
+        for (int k = 0; k < PER; ++k) {
+            cl.start[lane * PER + k] = run;
+            run += c[k];
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            int n = __shfl_xor_sync(0xffffffffu, mx, o);
+            mx = n > mx ? n : mx;
+        }
+        if (lane == 0) cl.layers = mx;
+    }
+    __syncthreads();
+}
+
 // ------------------------------------------------------------------ P2G ----
 // Also writes each particle's fractional cell offsets (frac) for the FP32 HVP.
 template <class L, class TH>
@@ -176,13 +233,17 @@ __global__ void __launch_bounds__(XF_THREADS) k_p2g(const int32_t* __restrict__ 
     constexpr int NPB = L::NPB;
     __shared__ __align__(16) double acc[8 * 4 * NPB];
     __shared__ int32_t nbr[8];
+    __shared__ CellLayout<L> cl;
     const int g = blockIdx.x;
     if (threadIdx.x < 8) nbr[threadIdx.x] = group_nbr[8 * g + threadIdx.x];
     zero_window<4, NPB>(acc);
-    __syncthreads();
     const double inv_dx = 1.0 / dx;
     const int s0 = group_start[g], s1 = group_start[g + 1];
-    for (int s = s0 + threadIdx.x; s < s1; s += blockDim.x) {
+    build_cell_layout<L>(cl, base, s0, s1);
+    for (int q = threadIdx.x; q < cl.layers * NPB; q += blockDim.x) {
+        const int r = q / NPB, ce = q % NPB;
+        if (r >= cl.cnt[ce]) continue;
+        const int s = s0 + cl.start[ce] + r;
         const short4 b = base[s];
         double xp[3], w[3][3], dwr[3][3];
 #pragma unroll
@@ -213,28 +274,36 @@ __global__ void __launch_bounds__(XF_THREADS) k_p2g(const int32_t* __restrict__ 
 }
 
 // --------------------------------------------------------------- update ----
-// grad v at the particle from vstar = vn + dv, F = (I + dt grad v) Fn,
-// S = V0 P(F) Fn^T, Hessian scratch, and facc -= sum_p S grad w.
+// Two kernels per Newton iteration (MpmForceBase::updatePositionBasedState then
+// rasterizeForceToTVStack, MpmForceBase.cpp:306-344, 102-152):
+//  k_stress: grad v at the particle from vstar = vn + dv, F = (I + dt grad v) Fn,
+//            S = V0 P(F) Fn^T (to `stress`) and the Hessian scratch; particles in
+//            slot order so every particle array is read coalesced.
+//  k_force : facc -= sum_p S_p grad w_ip, layered conflict-free scatter.
 template <class L, class TH>
-__global__ void __launch_bounds__(XF_THREADS) k_update(const int32_t* __restrict__ group_start, const int32_t* __restrict__ group_nbr,
+__global__ void __launch_bounds__(XF_THREADS) k_stress(const int32_t* __restrict__ group_start, const int32_t* __restrict__ group_nbr,
     const double* __restrict__ pd, const int32_t* __restrict__ pi, int64_t cap, const short4* __restrict__ base, double dx, double dt,
-    const double* __restrict__ vstar, double* __restrict__ facc, TH* __restrict__ scr, const SolverScalars* __restrict__ sc,
+    const double* __restrict__ vstar, double* __restrict__ stress, TH* __restrict__ scr, const SolverScalars* __restrict__ sc,
     int32_t* __restrict__ flags)
 {
     if (sc && sc->newton_done) return;
     constexpr int NPB = L::NPB;
     __shared__ __align__(128) double win[8 * 3 * NPB];
-    __shared__ __align__(16) double acc[8 * 3 * NPB];
     __shared__ int32_t nbr[8];
     __shared__ __align__(8) uint64_t bar;
     const int g = blockIdx.x;
     if (threadIdx.x < 8) nbr[threadIdx.x] = group_nbr[8 * g + threadIdx.x];
-    zero_window<3, NPB>(acc);
     __syncthreads();
     stage_window<NPB>(win, vstar, nbr, &bar, flags);
     const double inv_dx = 1.0 / dx;
     const int s0 = group_start[g], s1 = group_start[g + 1];
     for (int s = s0 + threadIdx.x; s < s1; s += blockDim.x) {
+        const int kind = pi[PI_KIND * cap + s];
+        if (kind == ZMPM_MODEL_NONE) {
+#pragma unroll
+            for (int q = 0; q < 9; ++q) stress[q * cap + s] = 0.0;
+            continue;
+        }
         const short4 b = base[s];
         double w[3][3], dwr[3][3];
 #pragma unroll
@@ -253,8 +322,6 @@ __global__ void __launch_bounds__(XF_THREADS) k_update(const int32_t* __restrict
                 for (int c = 0; c < 3; ++c) gv(r, c) += vr * dw[c];
             }
         });
-        const int kind = pi[PI_KIND * cap + s];
-        if (kind == ZMPM_MODEL_NONE) continue;
         M3<double> Fn, A = m3_identity<double>();
 #pragma unroll
         for (int q = 0; q < 9; ++q) {
@@ -264,10 +331,46 @@ __global__ void __launch_bounds__(XF_THREADS) k_update(const int32_t* __restrict
         M3<double> F = m3_mul(A, Fn);
         ModelParams mp{ pd[PD_MU * cap + s], pd[PD_LAM * cap + s], pd[PD_KAPPA * cap + s], pd[PD_G * cap + s] };
         M3<double> S = model_update<double, TH>(kind, mp, pd[PD_VOL * cap + s], F, Fn, scr, cap, s);
+#pragma unroll
+        for (int q = 0; q < 9; ++q) stress[q * cap + s] = S.a[q];
+    }
+}
+
+template <class L>
+__global__ void __launch_bounds__(XF_THREADS) k_force(const int32_t* __restrict__ group_start, const int32_t* __restrict__ group_nbr,
+    const double* __restrict__ pd, int64_t cap, const short4* __restrict__ base, double dx, const double* __restrict__ stress,
+    double* __restrict__ facc, const SolverScalars* __restrict__ sc)
+{
+    if (sc && sc->newton_done) return;
+    constexpr int NPB = L::NPB;
+    __shared__ __align__(16) double acc[8 * 3 * NPB];
+    __shared__ int32_t nbr[8];
+    __shared__ CellLayout<L> cl;
+    const int g = blockIdx.x;
+    if (threadIdx.x < 8) nbr[threadIdx.x] = group_nbr[8 * g + threadIdx.x];
+    zero_window<3, NPB>(acc);
+    const double inv_dx = 1.0 / dx;
+    const int s0 = group_start[g], s1 = group_start[g + 1];
+    build_cell_layout<L>(cl, base, s0, s1);
+    for (int q = threadIdx.x; q < cl.layers * NPB; q += blockDim.x) {
+        const int r = q / NPB, ce = q % NPB;
+        if (r >= cl.cnt[ce]) continue;
+        const int s = s0 + cl.start[ce] + r;
+        const short4 b = base[s];
+        double w[3][3], dwr[3][3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            double d0 = inv_dx * pd[(PD_X + d) * cap + s] - (double)((&b.x)[d]);
+            bspline(d0, w[d], dwr[d]);
+        }
+        M3<double> S;
+#pragma unroll
+        for (int q2 = 0; q2 < 9; ++q2) S.a[q2] = stress[q2 * cap + s];
+        const int lx = b.x & (L::BX - 1), ly = b.y & (L::BY - 1), lz = b.z & (L::BZ - 1);
         for_stencil<L>(lx, ly, lz, w, dwr, inv_dx, [&](int t, int e, int, int, int, double, const double* dw) {
             double* a = acc + t * 3 * NPB + e;
 #pragma unroll
-            for (int r = 0; r < 3; ++r) atomicAdd(a + r * NPB, -(S(r, 0) * dw[0] + S(r, 1) * dw[1] + S(r, 2) * dw[2]));
+            for (int c = 0; c < 3; ++c) atomicAdd(a + c * NPB, -(S(c, 0) * dw[0] + S(c, 1) * dw[1] + S(c, 2) * dw[2]));
         });
     }
     __syncthreads();
@@ -279,17 +382,18 @@ __global__ void __launch_bounds__(XF_THREADS) k_update(const int32_t* __restrict
 // arithmetic precision (float in mixed runs).  Skipped when the linear solve
 // is inactive.
 template <class L, class TH>
-__global__ void __launch_bounds__(XF_THREADS) k_hvp(const int32_t* __restrict__ group_start, const int32_t* __restrict__ group_nbr,
+__global__ void __launch_bounds__(XF_THREADS, sizeof(TH) == 4 ? 4 : 2) k_hvp(const int32_t* __restrict__ group_start, const int32_t* __restrict__ group_nbr,
     const int32_t* __restrict__ pi, int64_t cap, const short4* __restrict__ base, double dx, const TH* __restrict__ frac,
     const TH* __restrict__ scr, const double* __restrict__ x, double* __restrict__ out, const SolverScalars* __restrict__ sc,
-    int32_t* __restrict__ flags)
+    int32_t* __restrict__ flags, int it)
 {
-    if (sc && (sc->newton_done || !sc->krylov_active)) return;
+    if (sc && (sc->newton_done || it >= sc->stop_at)) return;
     constexpr int NPB = L::NPB;
     __shared__ __align__(128) double win[8 * 3 * NPB];
     __shared__ __align__(16) TH acc[8 * 3 * NPB];
     __shared__ int32_t nbr[8];
     __shared__ __align__(8) uint64_t bar;
+    __shared__ CellLayout<L> cl;
     const int g = blockIdx.x;
     if (threadIdx.x < 8) nbr[threadIdx.x] = group_nbr[8 * g + threadIdx.x];
     zero_window<3, NPB>(acc);
@@ -297,7 +401,11 @@ __global__ void __launch_bounds__(XF_THREADS) k_hvp(const int32_t* __restrict__ 
     stage_window<NPB>(win, x, nbr, &bar, flags);
     const TH inv_dx = TH(1.0 / dx);
     const int s0 = group_start[g], s1 = group_start[g + 1];
-    for (int s = s0 + threadIdx.x; s < s1; s += blockDim.x) {
+    build_cell_layout<L>(cl, base, s0, s1);
+    for (int q = threadIdx.x; q < cl.layers * NPB; q += blockDim.x) {
+        const int r = q / NPB, ce = q % NPB;
+        if (r >= cl.cnt[ce]) continue;
+        const int s = s0 + cl.start[ce] + r;
         const int kind = pi[PI_KIND * cap + s];
         if (kind == ZMPM_MODEL_NONE) continue;
         const short4 b = base[s];
@@ -316,10 +424,100 @@ __global__ void __launch_bounds__(XF_THREADS) k_hvp(const int32_t* __restrict__ 
             }
         });
         M3<TH> dS = model_hvp<TH>(kind, scr, cap, s, G);
+        // recomputed rather than kept live across the constitutive step
+#pragma unroll
+        for (int d = 0; d < 3; ++d) bspline(frac[d * cap + s], w[d], dwr[d]);
         for_stencil<L>(lx, ly, lz, w, dwr, inv_dx, [&](int t, int e, int, int, int, TH, const TH* dw) {
             TH* a = acc + t * 3 * NPB + e;
 #pragma unroll
             for (int r = 0; r < 3; ++r) atomicAdd(a + r * NPB, dS(r, 0) * dw[0] + dS(r, 1) * dw[1] + dS(r, 2) * dw[2]);
+        });
+    }
+    __syncthreads();
+    flush_window<3, 3, NPB>(acc, nbr, out, nullptr);
+}
+
+// Split form of the same product (two kernels, dS round-trips through HBM in
+// the HVP precision): k_hvp_stress gathers grad(x) and evaluates dS in slot
+// order; k_hvp_scatter adds dS grad w with the layered scatter.  Each half
+// holds far fewer live registers than the fused kernel.
+template <class L, class TH>
+__global__ void __launch_bounds__(XF_THREADS) k_hvp_stress(const int32_t* __restrict__ group_start, const int32_t* __restrict__ group_nbr,
+    const int32_t* __restrict__ pi, int64_t cap, const short4* __restrict__ base, double dx, const TH* __restrict__ frac,
+    const TH* __restrict__ scr, const double* __restrict__ x, TH* __restrict__ dstress, const SolverScalars* __restrict__ sc,
+    int32_t* __restrict__ flags, int it)
+{
+    if (sc && (sc->newton_done || it >= sc->stop_at)) return;
+    constexpr int NPB = L::NPB;
+    __shared__ __align__(128) double win[8 * 3 * NPB];
+    __shared__ int32_t nbr[8];
+    __shared__ __align__(8) uint64_t bar;
+    const int g = blockIdx.x;
+    if (threadIdx.x < 8) nbr[threadIdx.x] = group_nbr[8 * g + threadIdx.x];
+    __syncthreads();
+    stage_window<NPB>(win, x, nbr, &bar, flags);
+    const TH inv_dx = TH(1.0 / dx);
+    const int s0 = group_start[g], s1 = group_start[g + 1];
+    for (int s = s0 + threadIdx.x; s < s1; s += blockDim.x) {
+        const int kind = pi[PI_KIND * cap + s];
+        if (kind == ZMPM_MODEL_NONE) {
+#pragma unroll
+            for (int q = 0; q < 9; ++q) dstress[q * cap + s] = TH(0);
+            continue;
+        }
+        const short4 b = base[s];
+        TH w[3][3], dwr[3][3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) bspline(frac[d * cap + s], w[d], dwr[d]);
+        const int lx = b.x & (L::BX - 1), ly = b.y & (L::BY - 1), lz = b.z & (L::BZ - 1);
+        M3<TH> G = m3_zero<TH>();
+        for_stencil<L>(lx, ly, lz, w, dwr, inv_dx, [&](int t, int e, int, int, int, TH, const TH* dw) {
+            const double* vv = win + t * 3 * NPB + e;
+#pragma unroll
+            for (int r = 0; r < 3; ++r) {
+                TH vr = (TH)vv[r * NPB];
+#pragma unroll
+                for (int c = 0; c < 3; ++c) G(r, c) += vr * dw[c];
+            }
+        });
+        M3<TH> dS = model_hvp<TH>(kind, scr, cap, s, G);
+#pragma unroll
+        for (int q = 0; q < 9; ++q) dstress[q * cap + s] = dS.a[q];
+    }
+}
+
+template <class L, class TH>
+__global__ void __launch_bounds__(XF_THREADS) k_hvp_scatter(const int32_t* __restrict__ group_start, const int32_t* __restrict__ group_nbr,
+    int64_t cap, const short4* __restrict__ base, double dx, const TH* __restrict__ frac, const TH* __restrict__ dstress,
+    double* __restrict__ out, const SolverScalars* __restrict__ sc, int it)
+{
+    if (sc && (sc->newton_done || it >= sc->stop_at)) return;
+    constexpr int NPB = L::NPB;
+    __shared__ __align__(16) TH acc[8 * 3 * NPB];
+    __shared__ int32_t nbr[8];
+    __shared__ CellLayout<L> cl;
+    const int g = blockIdx.x;
+    if (threadIdx.x < 8) nbr[threadIdx.x] = group_nbr[8 * g + threadIdx.x];
+    zero_window<3, NPB>(acc);
+    const TH inv_dx = TH(1.0 / dx);
+    const int s0 = group_start[g], s1 = group_start[g + 1];
+    build_cell_layout<L>(cl, base, s0, s1);
+    for (int q = threadIdx.x; q < cl.layers * NPB; q += blockDim.x) {
+        const int r = q / NPB, ce = q % NPB;
+        if (r >= cl.cnt[ce]) continue;
+        const int s = s0 + cl.start[ce] + r;
+        const short4 b = base[s];
+        TH w[3][3], dwr[3][3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) bspline(frac[d * cap + s], w[d], dwr[d]);
+        M3<TH> dS;
+#pragma unroll
+        for (int q2 = 0; q2 < 9; ++q2) dS.a[q2] = dstress[q2 * cap + s];
+        const int lx = b.x & (L::BX - 1), ly = b.y & (L::BY - 1), lz = b.z & (L::BZ - 1);
+        for_stencil<L>(lx, ly, lz, w, dwr, inv_dx, [&](int t, int e, int, int, int, TH, const TH* dw) {
+            TH* a = acc + t * 3 * NPB + e;
+#pragma unroll
+            for (int c = 0; c < 3; ++c) atomicAdd(a + c * NPB, dS(c, 0) * dw[0] + dS(c, 1) * dw[1] + dS(c, 2) * dw[2]);
         });
     }
     __syncthreads();
@@ -434,45 +632,62 @@ static int update_impl(Ctx* ctx)
     DevCounters* dc = ctx->counters.as<DevCounters>();
     const SolverScalars* sc = ctx->scal.as<SolverScalars>();
     if (ctx->mixed)
-        k_update<L, float><<<(unsigned)G, XF_THREADS, 0, ctx->stream>>>(ctx->group_start.as<int32_t>(), ctx->group_nbr.as<int32_t>(),
+        k_stress<L, float><<<(unsigned)G, XF_THREADS, 0, ctx->stream>>>(ctx->group_start.as<int32_t>(), ctx->group_nbr.as<int32_t>(),
             ctx->pd.as<double>(), ctx->pi.as<int32_t>(), ctx->Pcap, ctx->base.as<short4>(), ctx->cfg.dx, ctx->dt, ctx->vstar.as<double>(),
-            ctx->facc.as<double>(), ctx->scratch.as<float>(), sc, &dc->flags);
+            ctx->stress.as<double>(), ctx->scratch.as<float>(), sc, &dc->flags);
     else
-        k_update<L, double><<<(unsigned)G, XF_THREADS, 0, ctx->stream>>>(ctx->group_start.as<int32_t>(), ctx->group_nbr.as<int32_t>(),
+        k_stress<L, double><<<(unsigned)G, XF_THREADS, 0, ctx->stream>>>(ctx->group_start.as<int32_t>(), ctx->group_nbr.as<int32_t>(),
             ctx->pd.as<double>(), ctx->pi.as<int32_t>(), ctx->Pcap, ctx->base.as<short4>(), ctx->cfg.dx, ctx->dt, ctx->vstar.as<double>(),
-            ctx->facc.as<double>(), ctx->scratch.as<double>(), sc, &dc->flags);
+            ctx->stress.as<double>(), ctx->scratch.as<double>(), sc, &dc->flags);
+    ++g_kernel_launches;
+    k_force<L><<<(unsigned)G, XF_THREADS, 0, ctx->stream>>>(ctx->group_start.as<int32_t>(), ctx->group_nbr.as<int32_t>(), ctx->pd.as<double>(),
+        ctx->Pcap, ctx->base.as<short4>(), ctx->cfg.dx, ctx->stress.as<double>(), ctx->facc.as<double>(), sc);
     ++g_kernel_launches;
     return ZMPM_OK;
 }
 int launch_update(Ctx* ctx) { return ctx->layout == 1 ? update_impl<Layout244>(ctx) : update_impl<Layout444>(ctx); }
 
-template <class L>
-static int hvp_impl(Ctx* ctx, const double* x, double* out, bool fp32, bool gated)
+template <class L, class TH>
+static void hvp_launch(Ctx* ctx, const double* x, double* out, const SolverScalars* sc, int it)
 {
     const int64_t G = ctx->G;
-    if (G == 0) return ZMPM_OK;
     DevCounters* dc = ctx->counters.as<DevCounters>();
+    if (ctx->hvp_fused) {
+        k_hvp<L, TH><<<(unsigned)G, XF_THREADS, 0, ctx->stream>>>(ctx->group_start.as<int32_t>(), ctx->group_nbr.as<int32_t>(),
+            ctx->pi.as<int32_t>(), ctx->Pcap, ctx->base.as<short4>(), ctx->cfg.dx, ctx->frac.as<TH>(), ctx->scratch.as<TH>(), x, out, sc,
+            &dc->flags, it);
+        ++g_kernel_launches;
+        return;
+    }
+    k_hvp_stress<L, TH><<<(unsigned)G, XF_THREADS, 0, ctx->stream>>>(ctx->group_start.as<int32_t>(), ctx->group_nbr.as<int32_t>(),
+        ctx->pi.as<int32_t>(), ctx->Pcap, ctx->base.as<short4>(), ctx->cfg.dx, ctx->frac.as<TH>(), ctx->scratch.as<TH>(), x,
+        ctx->dstress.as<TH>(), sc, &dc->flags, it);
+    ++g_kernel_launches;
+    k_hvp_scatter<L, TH><<<(unsigned)G, XF_THREADS, 0, ctx->stream>>>(ctx->group_start.as<int32_t>(), ctx->group_nbr.as<int32_t>(), ctx->Pcap,
+        ctx->base.as<short4>(), ctx->cfg.dx, ctx->frac.as<TH>(), ctx->dstress.as<TH>(), out, sc, it);
+    ++g_kernel_launches;
+}
+
+template <class L>
+static int hvp_impl(Ctx* ctx, const double* x, double* out, bool fp32, bool gated, int it)
+{
+    if (ctx->G == 0) return ZMPM_OK;
     const SolverScalars* sc = gated ? ctx->scal.as<SolverScalars>() : nullptr;
     if (fp32)
-        k_hvp<L, float><<<(unsigned)G, XF_THREADS, 0, ctx->stream>>>(ctx->group_start.as<int32_t>(), ctx->group_nbr.as<int32_t>(),
-            ctx->pi.as<int32_t>(), ctx->Pcap, ctx->base.as<short4>(), ctx->cfg.dx, ctx->frac.as<float>(), ctx->scratch.as<float>(), x, out, sc,
-            &dc->flags);
+        hvp_launch<L, float>(ctx, x, out, sc, it);
     else
-        k_hvp<L, double><<<(unsigned)G, XF_THREADS, 0, ctx->stream>>>(ctx->group_start.as<int32_t>(), ctx->group_nbr.as<int32_t>(),
-            ctx->pi.as<int32_t>(), ctx->Pcap, ctx->base.as<short4>(), ctx->cfg.dx, ctx->frac.as<double>(), ctx->scratch.as<double>(), x, out, sc,
-            &dc->flags);
-    ++g_kernel_launches;
+        hvp_launch<L, double>(ctx, x, out, sc, it);
     return ZMPM_OK;
 }
-int launch_hvp_gated(Ctx* ctx, const double* x, double* out, bool gated)
+int launch_hvp_gated(Ctx* ctx, const double* x, double* out, bool gated, int it)
 {
     bool fp32 = ctx->mixed;
-    return ctx->layout == 1 ? hvp_impl<Layout244>(ctx, x, out, fp32, gated) : hvp_impl<Layout444>(ctx, x, out, fp32, gated);
+    return ctx->layout == 1 ? hvp_impl<Layout244>(ctx, x, out, fp32, gated, it) : hvp_impl<Layout444>(ctx, x, out, fp32, gated, it);
 }
 int launch_hvp(Ctx* ctx, const double* x, double* out, bool fp32)
 {
     if (fp32 && !ctx->mixed) return ZMPM_UNSUPPORTED;
-    return ctx->layout == 1 ? hvp_impl<Layout244>(ctx, x, out, ctx->mixed, false) : hvp_impl<Layout444>(ctx, x, out, ctx->mixed, false);
+    return ctx->layout == 1 ? hvp_impl<Layout244>(ctx, x, out, ctx->mixed, false, 0) : hvp_impl<Layout444>(ctx, x, out, ctx->mixed, false, 0);
 }
 
 template <class L>
