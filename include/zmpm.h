@@ -249,6 +249,31 @@ int zmpm_residual(zmpm_ctx* ctx, const double* dv, double* residual, double* nor
    fp32 != 0 evaluates the Hessian-vector product in FP32 (MIXED contexts). */
 int zmpm_multiply(zmpm_ctx* ctx, const double* x, double* b, int32_t fp32);
 
+/* --------------------------------------------------- allocation-free ----- */
+/* Largest particle count zmpm_sort_keys_noalloc accepts. */
+#define ZMPM_NOALLOC_MAX_PARTICLES 262144
+
+/* This entry point has no counterpart in the reference.  It is for callers that
+   cannot call cudaMalloc (a host that owns all device memory and forbids new
+   allocations, or a loop that cannot take cudaMalloc's implicit device
+   synchronisation): it computes the particle keys of the binning pass
+   (sortParticlesAndPolluteGrid's key and sort) for n particles and sorts them,
+   allocating nothing.
+     x      device array [n][3] of positions (row-major, like the host arrays)
+     keys   device array [n]; receives the sorted keys, bit-identical to
+            zmpm_bin_result.particle_sorter of a context with the same
+            precision, layout, grid_log2 and dx
+     stream cudaStream_t to run on (NULL = the default stream)
+   Scratch memory is one fixed device array inside the library (about 2.2 MB on
+   every GPU that loads it, kept until exit); n above
+   ZMPM_NOALLOC_MAX_PARTICLES is rejected with ZMPM_BAD_ARG.  The first call
+   on each device looks up that array's device address, so make it before any
+   stream capture.  Calls share the array: calls that overlap on the GPU race.
+   Returns ZMPM_OUT_OF_GRID if a particle's stencil leaves the grid.  The call
+   synchronises `stream` before it returns. */
+int zmpm_sort_keys_noalloc(const double* x, int64_t n, double dx, int32_t precision, int32_t layout, int32_t grid_log2,
+    uint64_t* keys, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

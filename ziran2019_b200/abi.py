@@ -27,6 +27,7 @@ UNSUPPORTED = -6
 
 FP64 = 0
 MIXED = 1
+NOALLOC_MAX_PARTICLES = 262144
 LAYOUT_AUTO, LAYOUT_244, LAYOUT_444 = 0, 1, 2
 MODEL_NONE, MODEL_NEOHOOKEAN_BORDEN, MODEL_STVK_HENCKY_ISOTROPIC, MODEL_FIXED_COROTATED = 0, 1, 2, 3
 PLASTIC_NONE, PLASTIC_VON_MISES = 0, 1
@@ -143,6 +144,7 @@ _PRODUCT_ONLY = {
     "get_stream": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
     "set_profiling": (C.c_int, [C.c_void_p, C.c_int32]),
     "status_string": (C.c_char_p, [C.c_int]),
+    "sort_keys_noalloc": (C.c_int, [C.c_void_p, C.c_int64, C.c_double, C.c_int32, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p]),
     "default_solver": (None, [C.POINTER(Solver), C.c_int32, C.c_int32]),
 }
 

@@ -12,7 +12,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT_DIR = os.path.join(HERE, "lib")
 OUT = os.path.join(OUT_DIR, "libzmpm.so")
-SOURCES = ["api.cu", "bin.cu", "prims.cu", "solver.cu", "transfer.cu"]
+SOURCES = ["api.cu", "bin.cu", "noalloc.cu", "prims.cu", "solver.cu", "transfer.cu"]
 HEADERS = ["common.cuh", "internal.cuh", "mat3.cuh", "models.cuh", "svd3.cuh"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = [
