@@ -56,12 +56,13 @@ def test_substeps_match_oracle_fp64(cuda_lib, oracle, kind, plastic, solver):
 
 @pytest.mark.parametrize("kind", ["fcr", "hencky"])
 def test_mixed_precision_tracks_fp64_oracle(cuda_lib, oracle, kind):
-    """MIXED: FP64 state and residuals, FP32 Hessian products; a converged Newton
-    solve lands on the FP64 solution up to the Newton tolerance."""
-    (g, o), (sg, so) = run_pair(oracle, kind, "cg", steps=5, precision="mixed", tol=1e-9, newton_max=12, kmax=60)
+    """MIXED: FP64 state, vectors, residual assembly and reductions; FP32 particle
+    constitutive arithmetic and Hessian products.  A converged Newton solve lands
+    on the FP64 solution up to the FP32 noise floor of the force."""
+    (g, o), (sg, so) = run_pair(oracle, kind, "cg", steps=5, precision="mixed", tol=1e-7, newton_max=12, kmax=60)
     pg, po = g.getParticles(), o.getParticles()
-    assert rel(pg["X"], po["X"]) < 1e-8
-    assert rel(pg["V"], po["V"]) < 1e-4
+    assert rel(pg["X"], po["X"]) < 1e-7
+    assert rel(pg["V"], po["V"]) < 1e-3
 
 
 def test_walls_and_free_particles(cuda_lib, oracle):

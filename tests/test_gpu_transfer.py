@@ -85,8 +85,10 @@ def test_hvp_fp32_mixed_matches_fp64_oracle(cuda_lib, oracle, kind):
     dv_o[oo] = dv_sorted
     rg, ng = g.residual(dv_g)
     ro, no = o.residual(dv_o)
-    # the residual is FP64 in MIXED runs
-    np.testing.assert_allclose(rg[og], ro[oo], rtol=0, atol=1e-10 * np.abs(ro).max())
+    # MIXED: particle stress in FP32 (FP64 for near-degenerate SVDs), force sums and
+    # residual assembly in FP64; bound 1e-5 of the largest entry
+    np.testing.assert_allclose(rg[og], ro[oo], rtol=0, atol=1e-5 * np.abs(ro).max())
+    assert abs(ng - no) <= 1e-5 * no
     x_sorted = rng.standard_normal((N, 3))
     xg = np.empty_like(x_sorted)
     xo = np.empty_like(x_sorted)

@@ -341,6 +341,8 @@ int zmpm_create(const zmpm_config* cfg, zmpm_ctx** out)
     {
         const char* f = getenv("ZMPM_HVP_FUSED");
         ctx->hvp_fused = f && f[0] == '1';
+        const char* ng = getenv("ZMPM_NO_GRAPH");
+        ctx->no_graph = ng && ng[0] == '1';
     }
     auto fail = [&](cudaError_t e) {
         ctx->err = cudaGetErrorString(e);
@@ -393,6 +395,7 @@ int zmpm_destroy(zmpm_ctx* ctx)
     for (auto& b : ctx->kv) b.release();
     ctx->stage.release();
     for (cudaEvent_t e : ctx->hvp_ev) cudaEventDestroy(e);
+    if (ctx->graph_exec) cudaGraphExecDestroy(ctx->graph_exec);
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);
     if (ctx->ev1) cudaEventDestroy(ctx->ev1);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -600,6 +603,10 @@ int zmpm_substep(zmpm_ctx* ctx, double dt, const zmpm_solver* s, zmpm_stats* st)
     ZMPM_CUDA(cudaMemcpyAsync(&hs, ctx->scal.p, sizeof(hs), cudaMemcpyDeviceToHost, ctx->stream));
     ZMPM_CUDA(cudaMemcpyAsync(&hc, ctx->counters.p, sizeof(hc), cudaMemcpyDeviceToHost, ctx->stream));
     ZMPM_CUDA(cudaStreamSynchronize(ctx->stream));
+    if (ctx->graph_exec) {
+        cudaGraphExecDestroy(ctx->graph_exec);
+        ctx->graph_exec = nullptr;
+    }
     float ms = 0;
     cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
     ctx->time += dt;
@@ -617,6 +624,8 @@ int zmpm_substep(zmpm_ctx* ctx, double dt, const zmpm_solver* s, zmpm_stats* st)
     st->num_blocks = ctx->B;
     st->num_nodes = hc.N;
     st->ms_total = ms;
+    if (ctx->graph_used) // Newton body: stress, force, residual, check, start, step, advance
+        g_kernel_launches += 7 * (int64_t)hs.nit + (ctx->hvp_fused ? 5 : 6) * (int64_t)hs.krylov_bodies;
     st->kernel_launches = (int32_t)(g_kernel_launches - launches0);
     ctx->N = hc.N;
     if (ctx->prof_newton > 0) {

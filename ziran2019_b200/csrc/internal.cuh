@@ -61,13 +61,15 @@ struct DevCounters {
 // read the previous value while CTA 0 writes the next one.
 struct SolverScalars {
     int32_t newton_done;       // 1 once the Newton norm fell below tolerance (or NaN)
-    int32_t stop_at;           // Krylov iterations it >= stop_at are skipped (latched by the
-                               // iteration that converged; read only by later kernels)
+    int32_t kactive;           // 1 while the current linear solve iterates
+    int32_t kit;               // Krylov iteration index of the current linear solve
+    int32_t nit;               // Newton iteration index (= Newton loop bodies run)
+    int32_t krylov_bodies;     // Krylov loop bodies run (graph launch accounting)
+    int32_t pad0;
     int32_t newton_iters;      // linear solves run
     int32_t krylov_iters;      // summed Krylov iterations
     int32_t hvp_count;
     int32_t converged;
-    int32_t pad[2];
     int32_t kcount[64];        // Krylov iterations of each Newton iteration
     double res_initial, res_final;
     double rel_tol, local_tol;
@@ -125,6 +127,9 @@ struct Ctx {
     DBuf stress;       // [9][Pcap] V0 P(F) Fn^T of the current Newton iterate
     DBuf dstress;      // [9][Pcap] dS of one Hessian-vector product (HVP precision)
     bool hvp_fused = false; // one fused HVP kernel instead of stress + scatter
+    bool no_graph = false;  // host-driven Newton loop instead of the conditional graph
+    cudaGraphExec_t graph_exec = nullptr; // last Newton graph, released after the next sync
+    bool graph_used = false;              // the last Newton solve ran as a graph
     DBuf frac;         // [3][Pcap] fractional offsets in cells (FP32 HVP)
     double* pdf(int f) const { return pd.as<double>() + (int64_t)f * Pcap; }
     int32_t* pif(int f) const { return pi.as<int32_t>() + (int64_t)f * Pcap; }

@@ -126,9 +126,13 @@ ZMPM_HD M3<T> nh_first_piola(T mu, T kappa, T g, T J, const M3<T>& F, const M3<T
 }
 
 // Computes S = V0 P(F) Fn^T and writes the Hessian scratch of particle p.
+// With `degenerate` set (FP32 evaluation), SVD-based models stop after the
+// SVD and report whether the singular values are too close to inversion
+// (|sigma2| <= 0.2) or too stretched (sigma0 >= 5) for FP32; the caller then
+// re-evaluates the particle in FP64.
 template <class T, class TH>
 ZMPM_D M3<T> model_update(int kind, const ModelParams& mp, T V0, const M3<T>& F, const M3<T>& Fn, TH* __restrict__ scr,
-    int64_t stride, int64_t p)
+    int64_t stride, int64_t p, bool* degenerate = nullptr)
 {
     if (kind == ZMPM_MODEL_NEOHOOKEAN_BORDEN) {
         T J = m3_det(F);
@@ -159,6 +163,11 @@ ZMPM_D M3<T> model_update(int kind, const ModelParams& mp, T V0, const M3<T>& F,
         M3<T> U, V;
         T sg[3];
         svd3(F, U, sg, V);
+        if (degenerate) {
+            const bool bad = !(fabs(sg[2]) > T(0.2) && sg[0] < T(5));
+            *degenerate = bad;
+            if (bad) return m3_zero<T>();
+        }
         T psi[3], c[12];
         iso_coefficients(kind, (T)mp.mu, (T)mp.lambda, sg, psi, c);
         M3<T> P = m3_udvt(U, psi, V);

@@ -26,7 +26,7 @@ constexpr int ND_THREADS = 256;
 
 int launch_p2g(Ctx* ctx);
 int launch_g2p(Ctx* ctx);
-int launch_hvp_gated(Ctx* ctx, const double* x, double* out, bool gated, int it);
+int launch_hvp_krylov(Ctx* ctx, const double* x0, const double* x1, bool alt, double* out);
 
 // ------------------------------------------------------------ reductions --
 __device__ __forceinline__ double warp_sum(double v)
@@ -289,7 +289,10 @@ __global__ void __launch_bounds__(ND_THREADS) k_residual(NodeGeom ng, const doub
     if (threadIdx.x == 0) part[blockIdx.x] = s;
 }
 
-// Solver buffers of one linear solve.
+// Solver buffers of one linear solve.  MINRES rotates its three Lanczos
+// vectors Q, three search directions M and two preconditioned vectors Z by the
+// iteration index k read from device memory, so the same kernels (and the same
+// graph body) serve every iteration.
 struct KrylovBufs {
     double *x, *r, *p, *q, *tmp;      // CG
     double *Q[3], *M[3], *Z[2];       // MINRES
@@ -297,27 +300,34 @@ struct KrylovBufs {
 };
 
 struct NewtonParams {
-    int32_t minres;
+    int32_t minres, kmax, nmax, pad;
     double tol, abs_tol, tol_scale, dt;
 };
+
+__device__ __forceinline__ bool krylov_off(const SolverScalars* sc) { return sc->newton_done || !sc->kactive; }
+
+// Role selection by iteration index without indexing the parameter arrays at
+// run time (which would copy the kernel parameters to local memory).
+__device__ __forceinline__ double* sel3(double* const (&a)[3], int i) { return i == 0 ? a[0] : (i == 1 ? a[1] : a[2]); }
+__device__ __forceinline__ double* sel2(double* const (&a)[2], int i) { return i == 0 ? a[0] : a[1]; }
 
 // Newton check (NewtonsMethod.h:48-61) + start of the linear solve: x = 0,
 // CG: r = res, q = r/m, p = q, partial r.q;  MINRES: Q0 = res, Z0 = res/m,
 // Q1 = Q2 = M* = 0, partial z.q.
 template <int NPB>
 __global__ void __launch_bounds__(ND_THREADS) k_newton_check(NodeGeom ng, const double* __restrict__ gm, const double* __restrict__ res,
-    KrylovBufs kb, NewtonParams np, double* __restrict__ part_in, double* __restrict__ part_out, SolverScalars* __restrict__ sc, int first)
+    KrylovBufs kb, NewtonParams np, double* __restrict__ part_in, double* __restrict__ part_out, SolverScalars* __restrict__ sc)
 {
     if (sc->newton_done) return;
     const double norm = sqrt(reduce_partials(part_in, ng.parts));
     const bool done = (norm < np.tol) || !(norm == norm);
     if (blockIdx.x == 0 && threadIdx.x == 0) {
-        if (first) sc->res_initial = norm;
+        if (sc->nit == 0) sc->res_initial = norm;
         sc->res_final = norm;
         if (done) {
             sc->newton_done = 1;
             sc->converged = (norm == norm) ? 1 : 0;
-            sc->stop_at = 0;
+            sc->kactive = 0;
         }
         else {
             double mx = norm > np.tol ? norm : np.tol;
@@ -355,21 +365,27 @@ __global__ void __launch_bounds__(ND_THREADS) k_newton_check(NodeGeom ng, const 
     if (threadIdx.x == 0) part_out[blockIdx.x] = s;
 }
 
-// Initial preconditioned norm and local tolerance; MINRES normalises Q0, Z0.
+// Initial preconditioned norm and local tolerance (Minres.h:73-98,
+// ConjugateGradient.h:108-117); MINRES normalises Q0, Z0.  Sets the Krylov
+// loop condition when running as a graph.
 template <int NPB>
 __global__ void __launch_bounds__(ND_THREADS) k_krylov_start(NodeGeom ng, KrylovBufs kb, NewtonParams np, const double* __restrict__ part_in,
-    SolverScalars* __restrict__ sc)
+    SolverScalars* __restrict__ sc, cudaGraphConditionalHandle hK, int use_graph)
 {
-    if (sc->newton_done) return;
+    if (sc->newton_done) {
+        if (use_graph && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(hK, 0u);
+        return;
+    }
     const double dotv = reduce_partials(part_in, ng.parts);
     const double rnorm = sqrt(dotv);
     const double rel = sc->rel_tol;
     const double lt = fmin(rel * rnorm, np.abs_tol);
-    const bool active = !(rnorm < lt);
+    const bool active = !(rnorm < lt) && np.kmax > 0;
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         sc->rnorm = rnorm;
         sc->local_tol = lt;
-        sc->stop_at = active ? 0x7fffffff : 0;
+        sc->kit = 0;
+        sc->kactive = active ? 1 : 0;
         if (np.minres) {
             double* mr = sc->mr[0];
             mr[MR_GC0] = mr[MR_GC1] = mr[MR_GC2] = 1;
@@ -378,10 +394,9 @@ __global__ void __launch_bounds__(ND_THREADS) k_krylov_start(NodeGeom ng, Krylov
             mr[MR_RHS1] = 0;
             mr[MR_BETA_KP1] = rnorm;
         }
-        else {
-            sc->zTrk = dotv;
+        else
             sc->mr[0][0] = dotv; // CG keeps zTrk double-buffered in mr[parity][0]
-        }
+        if (use_graph) cudaGraphSetConditional(hK, active ? 1u : 0u);
     }
     if (!np.minres || !active || !(rnorm > 0)) return;
     for (int64_t n = (int64_t)blockIdx.x * ND_THREADS + threadIdx.x; n < ng.nn; n += (int64_t)gridDim.x * ND_THREADS)
@@ -392,13 +407,13 @@ __global__ void __launch_bounds__(ND_THREADS) k_krylov_start(NodeGeom ng, Krylov
         }
 }
 
-// out = project(m x + dt^2 hacc), zero hacc, partial dot(out, w).
+// out = project(m x + dt^2 hacc) (BackwardEuler.h:322-351 then Minres.h:116);
+// zeroes hacc; partial dot(out, x) when part != null.
 template <int NPB>
-__global__ void __launch_bounds__(ND_THREADS) k_apply_A(NodeGeom ng, const double* __restrict__ gm, const int8_t* __restrict__ col,
+__device__ __forceinline__ void apply_A_body(NodeGeom ng, const double* __restrict__ gm, const int8_t* __restrict__ col,
     const double* __restrict__ P6, double dt2, const double* __restrict__ xin, double* __restrict__ hacc, double* __restrict__ out,
-    double* __restrict__ part, const SolverScalars* __restrict__ sc, int gated, int project, int it)
+    double* __restrict__ part, int project)
 {
-    if (gated && (sc->newton_done || it >= sc->stop_at)) return;
     double acc = 0;
     for (int64_t n = (int64_t)blockIdx.x * ND_THREADS + threadIdx.x; n < ng.nn; n += (int64_t)gridDim.x * ND_THREADS) {
         const double m = gm[n];
@@ -421,13 +436,36 @@ __global__ void __launch_bounds__(ND_THREADS) k_apply_A(NodeGeom ng, const doubl
     }
 }
 
+// The reference's multiply without projection (test hooks).
+template <int NPB>
+__global__ void __launch_bounds__(ND_THREADS) k_apply_A(NodeGeom ng, const double* __restrict__ gm, const int8_t* __restrict__ col,
+    const double* __restrict__ P6, double dt2, const double* __restrict__ xin, double* __restrict__ hacc, double* __restrict__ out)
+{
+    apply_A_body<NPB>(ng, gm, col, P6, dt2, xin, hacc, out, nullptr, 0);
+}
+
+// Krylov form: MINRES qkp1 = project(A mk) with mk = Z[k&1], alpha partial
+// mk . qkp1; CG tmp = project(A p), partial tmp . p.
+template <int NPB>
+__global__ void __launch_bounds__(ND_THREADS) k_apply_A_krylov(NodeGeom ng, const double* __restrict__ gm, const int8_t* __restrict__ col,
+    const double* __restrict__ P6, double dt2, KrylovBufs kb, int minres, double* __restrict__ part, const SolverScalars* __restrict__ sc)
+{
+    if (krylov_off(sc)) return;
+    const int k = sc->kit;
+    if (minres)
+        apply_A_body<NPB>(ng, gm, col, P6, dt2, sel2(kb.Z, k & 1), kb.hacc, sel3(kb.Q, (k + 1) % 3), part, 1);
+    else
+        apply_A_body<NPB>(ng, gm, col, P6, dt2, kb.p, kb.hacc, kb.tmp, part, 1);
+}
+
 // ---------------------------------------------------------------- CG ------
 // x += alpha p; r -= alpha tmp; q = r/m; partial q.r
 template <int NPB>
 __global__ void __launch_bounds__(ND_THREADS) k_cg_b(NodeGeom ng, const double* __restrict__ gm, KrylovBufs kb, const double* __restrict__ part_in,
-    double* __restrict__ part_out, const SolverScalars* __restrict__ sc, int it)
+    double* __restrict__ part_out, const SolverScalars* __restrict__ sc)
 {
-    if (sc->newton_done || it >= sc->stop_at) return;
+    if (krylov_off(sc)) return;
+    const int it = sc->kit;
     const double alpha = sc->mr[it & 1][0] / reduce_partials(part_in, ng.parts);
     double acc = 0;
     for (int64_t n = (int64_t)blockIdx.x * ND_THREADS + threadIdx.x; n < ng.nn; n += (int64_t)gridDim.x * ND_THREADS) {
@@ -446,12 +484,12 @@ __global__ void __launch_bounds__(ND_THREADS) k_cg_b(NodeGeom ng, const double* 
     if (threadIdx.x == 0) part_out[blockIdx.x] = s;
 }
 
-// beta, p = q + beta p, convergence
+// beta, p = q + beta p, residual norm
 template <int NPB>
-__global__ void __launch_bounds__(ND_THREADS) k_cg_c(NodeGeom ng, KrylovBufs kb, const double* __restrict__ part_in, SolverScalars* __restrict__ sc, int it,
-    int nit)
+__global__ void __launch_bounds__(ND_THREADS) k_cg_c(NodeGeom ng, KrylovBufs kb, const double* __restrict__ part_in, SolverScalars* __restrict__ sc)
 {
-    if (sc->newton_done || it >= sc->stop_at) return;
+    if (krylov_off(sc)) return;
+    const int it = sc->kit, nit = sc->nit;
     const double zTrk = reduce_partials(part_in, ng.parts);
     const double beta = zTrk / sc->mr[it & 1][0];
     const double rnorm = sqrt(zTrk);
@@ -462,7 +500,6 @@ __global__ void __launch_bounds__(ND_THREADS) k_cg_c(NodeGeom ng, KrylovBufs kb,
         sc->krylov_iters += 1;
         sc->hvp_count += 1;
         if (nit < 64) sc->kcount[nit] += 1;
-        if (rnorm < sc->local_tol) sc->stop_at = it + 1; // the reference tests at the next loop top
     }
     for (int64_t n = (int64_t)blockIdx.x * ND_THREADS + threadIdx.x; n < ng.nn; n += (int64_t)gridDim.x * ND_THREADS)
         for (int k = 0; k < 3; ++k) {
@@ -474,11 +511,15 @@ __global__ void __launch_bounds__(ND_THREADS) k_cg_c(NodeGeom ng, KrylovBufs kb,
 // ------------------------------------------------------------- MINRES -----
 // qkp1 -= alpha qk + beta_k qkm1; z = qkp1/m; partial z.qkp1
 template <int NPB>
-__global__ void __launch_bounds__(ND_THREADS) k_mr_b(NodeGeom ng, const double* __restrict__ gm, double* __restrict__ qkp1,
-    const double* __restrict__ qk, const double* __restrict__ qkm1, double* __restrict__ zout, const double* __restrict__ part_in,
-    double* __restrict__ part_out, const SolverScalars* __restrict__ sc, int it)
+__global__ void __launch_bounds__(ND_THREADS) k_mr_b(NodeGeom ng, const double* __restrict__ gm, KrylovBufs kb, const double* __restrict__ part_in,
+    double* __restrict__ part_out, SolverScalars* __restrict__ sc)
 {
-    if (sc->newton_done || it >= sc->stop_at) return;
+    if (krylov_off(sc)) return;
+    const int it = sc->kit;
+    double* __restrict__ qkp1 = sel3(kb.Q, (it + 1) % 3);
+    const double* __restrict__ qk = sel3(kb.Q, it % 3);
+    const double* __restrict__ qkm1 = sel3(kb.Q, (it + 2) % 3);
+    double* __restrict__ zout = sel2(kb.Z, (it + 1) & 1);
     const double alpha = reduce_partials(part_in, ng.parts);
     const double beta_k = sc->mr[it & 1][MR_BETA_KP1];
     double acc = 0;
@@ -497,19 +538,23 @@ __global__ void __launch_bounds__(ND_THREADS) k_mr_b(NodeGeom ng, const double* 
     }
     double s = block_sum(acc);
     if (threadIdx.x == 0) part_out[blockIdx.x] = s;
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        // alpha of this iteration is needed by the Givens update in k_mr_c
-        const_cast<SolverScalars*>(sc)->mr[(it + 1) & 1][MR_TK] = alpha;
-    }
+    // alpha of this iteration, for the Givens update in k_mr_c
+    if (blockIdx.x == 0 && threadIdx.x == 0) sc->mr[(it + 1) & 1][MR_TK] = alpha;
 }
 
 // Givens update (Minres.h:151-175), normalisation, search direction and x.
 template <int NPB>
-__global__ void __launch_bounds__(ND_THREADS) k_mr_c(NodeGeom ng, double* __restrict__ qkp1, double* __restrict__ zout,
-    const double* __restrict__ zin, const double* __restrict__ mkm1, const double* __restrict__ mkm2, double* __restrict__ mk_out,
-    double* __restrict__ x, const double* __restrict__ part_in, SolverScalars* __restrict__ sc, int it, int nit)
+__global__ void __launch_bounds__(ND_THREADS) k_mr_c(NodeGeom ng, KrylovBufs kb, const double* __restrict__ part_in, SolverScalars* __restrict__ sc)
 {
-    if (sc->newton_done || it >= sc->stop_at) return;
+    if (krylov_off(sc)) return;
+    const int it = sc->kit, nit = sc->nit;
+    double* __restrict__ qkp1 = sel3(kb.Q, (it + 1) % 3);
+    double* __restrict__ zout = sel2(kb.Z, (it + 1) & 1);
+    const double* __restrict__ zin = sel2(kb.Z, it & 1);
+    const double* __restrict__ mkm1 = sel3(kb.M, (it + 2) % 3);
+    const double* __restrict__ mkm2 = sel3(kb.M, (it + 1) % 3);
+    double* __restrict__ mk_out = sel3(kb.M, it % 3);
+    double* __restrict__ x = kb.x;
     const double dz = reduce_partials(part_in, ng.parts);
     const double* cur = sc->mr[it & 1];
     const double alpha_k = sc->mr[(it + 1) & 1][MR_TK];
@@ -553,7 +598,6 @@ __global__ void __launch_bounds__(ND_THREADS) k_mr_c(NodeGeom ng, double* __rest
         sc->krylov_iters += 1;
         sc->hvp_count += 1;
         if (nit < 64) sc->kcount[nit] += 1;
-        if (rnorm < sc->local_tol) sc->stop_at = it + 1; // the reference tests at the next loop top
     }
     const bool norm = beta_kp1 > 0;
     for (int64_t n = (int64_t)blockIdx.x * ND_THREADS + threadIdx.x; n < ng.nn; n += (int64_t)gridDim.x * ND_THREADS)
@@ -569,14 +613,27 @@ __global__ void __launch_bounds__(ND_THREADS) k_mr_c(NodeGeom ng, double* __rest
         }
 }
 
+// Ends a Krylov iteration: advances k and applies the convergence test of the
+// next loop top (Minres.h:100, ConjugateGradient.h:118); as a graph, sets the
+// loop condition.  A separate one-thread kernel so that no kernel both reads
+// and updates k.
+__global__ void k_krylov_advance(SolverScalars* __restrict__ sc, int kmax, cudaGraphConditionalHandle hK, int use_graph)
+{
+    sc->krylov_bodies += 1;
+    if (!sc->newton_done && sc->kactive) {
+        const int k = sc->kit + 1;
+        sc->kit = k;
+        if (sc->rnorm < sc->local_tol || k >= kmax) sc->kactive = 0;
+    }
+    if (use_graph) cudaGraphSetConditional(hK, (!sc->newton_done && sc->kactive) ? 1u : 0u);
+}
 
 // dv += step; vstar = vn + dv on active nodes.
 template <int NPB>
 __global__ void __launch_bounds__(ND_THREADS) k_newton_step(NodeGeom ng, const double* __restrict__ gm, const double* __restrict__ step,
-    const double* __restrict__ vn, double* __restrict__ dv, double* __restrict__ vstar, SolverScalars* __restrict__ sc)
+    const double* __restrict__ vn, double* __restrict__ dv, double* __restrict__ vstar, const SolverScalars* __restrict__ sc)
 {
     if (sc->newton_done) return;
-    if (blockIdx.x == 0 && threadIdx.x == 0) sc->newton_iters += 1;
     for (int64_t n = (int64_t)blockIdx.x * ND_THREADS + threadIdx.x; n < ng.nn; n += (int64_t)gridDim.x * ND_THREADS) {
         const bool act = gm[n] != 0;
         for (int k = 0; k < 3; ++k) {
@@ -586,6 +643,16 @@ __global__ void __launch_bounds__(ND_THREADS) k_newton_step(NodeGeom ng, const d
             vstar[i] = act ? vn[i] + d : 0.0;
         }
     }
+}
+
+// Ends a Newton iteration (NewtonsMethod.h:46 loop); as a graph, sets the
+// Newton loop condition.
+__global__ void k_newton_advance(SolverScalars* __restrict__ sc, int nmax, cudaGraphConditionalHandle hN, int use_graph)
+{
+    if (!sc->newton_done) sc->newton_iters += 1;
+    const int n = sc->nit + 1;
+    sc->nit = n;
+    if (use_graph) cudaGraphSetConditional(hN, (!sc->newton_done && n < nmax) ? 1u : 0u);
 }
 
 // ------------------------------------------------------------ host side --
@@ -673,45 +740,219 @@ int finalize_multiply(Ctx* ctx, const double* x, double* q)
     const double dt2 = ctx->dt * ctx->dt;
     if (ctx->layout == 1)
         k_apply_A<32><<<ng.parts, ND_THREADS, 0, ctx->stream>>>(ng, ctx->gm.as<double>(), ctx->collided.as<int8_t>(), ctx->proj.as<double>(), dt2, x,
-            ctx->kv[9].as<double>(), q, nullptr, nullptr, 0, 0, 0);
+            ctx->kv[9].as<double>(), q);
     else
         k_apply_A<64><<<ng.parts, ND_THREADS, 0, ctx->stream>>>(ng, ctx->gm.as<double>(), ctx->collided.as<int8_t>(), ctx->proj.as<double>(), dt2, x,
-            ctx->kv[9].as<double>(), q, nullptr, nullptr, 0, 0, 0);
+            ctx->kv[9].as<double>(), q);
+    ++g_kernel_launches;
+    return ZMPM_OK;
+}
+
+namespace {
+
+struct NewtonLaunch {
+    Ctx* ctx;
+    NodeGeom ng;
+    KrylovBufs kb;
+    NewtonParams np;
+    SolverScalars* sc;
+    double *pA, *pB, *pC;
+    double dt2;
+    int nb;
+};
+
+// First part of a Newton iteration: update, residual, check, Krylov start.
+template <int NPB>
+int launch_newton_head(const NewtonLaunch& L, cudaStream_t st, cudaGraphConditionalHandle hK, int use_graph)
+{
+    Ctx* ctx = L.ctx;
+    int rc = launch_update(ctx);
+    if (rc) return rc;
+    rc = launch_residual(ctx);
+    if (rc) return rc;
+    k_newton_check<NPB><<<L.nb, ND_THREADS, 0, st>>>(L.ng, ctx->gm.as<double>(), ctx->res.as<double>(), L.kb, L.np, L.pA, L.pB, L.sc);
+    ++g_kernel_launches;
+    k_krylov_start<NPB><<<L.nb, ND_THREADS, 0, st>>>(L.ng, L.kb, L.np, L.pB, L.sc, hK, use_graph);
+    ++g_kernel_launches;
+    return ZMPM_OK;
+}
+
+// One Krylov iteration: Hessian-vector product, A x, and the solver updates.
+template <int NPB>
+int launch_krylov_iteration(const NewtonLaunch& L, cudaStream_t st, cudaGraphConditionalHandle hK, int use_graph, cudaEvent_t e0, cudaEvent_t e1)
+{
+    Ctx* ctx = L.ctx;
+    if (e0) ZMPM_CUDA(cudaEventRecord(e0, st));
+    if (L.np.minres)
+        launch_hvp_krylov(ctx, L.kb.Z[0], L.kb.Z[1], true, L.kb.hacc);
+    else
+        launch_hvp_krylov(ctx, L.kb.p, L.kb.p, false, L.kb.hacc);
+    if (e1) ZMPM_CUDA(cudaEventRecord(e1, st));
+    k_apply_A_krylov<NPB><<<L.nb, ND_THREADS, 0, st>>>(L.ng, ctx->gm.as<double>(), ctx->collided.as<int8_t>(), ctx->proj.as<double>(), L.dt2, L.kb,
+        L.np.minres, L.pA, L.sc);
+    ++g_kernel_launches;
+    if (L.np.minres) {
+        k_mr_b<NPB><<<L.nb, ND_THREADS, 0, st>>>(L.ng, ctx->gm.as<double>(), L.kb, L.pA, L.pC, L.sc);
+        k_mr_c<NPB><<<L.nb, ND_THREADS, 0, st>>>(L.ng, L.kb, L.pC, L.sc);
+    }
+    else {
+        k_cg_b<NPB><<<L.nb, ND_THREADS, 0, st>>>(L.ng, ctx->gm.as<double>(), L.kb, L.pA, L.pC, L.sc);
+        k_cg_c<NPB><<<L.nb, ND_THREADS, 0, st>>>(L.ng, L.kb, L.pC, L.sc);
+    }
+    g_kernel_launches += 2;
+    k_krylov_advance<<<1, 1, 0, st>>>(L.sc, L.np.kmax, hK, use_graph);
     ++g_kernel_launches;
     return ZMPM_OK;
 }
 
 template <int NPB>
+int launch_newton_tail(const NewtonLaunch& L, cudaStream_t st, cudaGraphConditionalHandle hN, int use_graph)
+{
+    Ctx* ctx = L.ctx;
+    k_newton_step<NPB><<<L.nb, ND_THREADS, 0, st>>>(L.ng, ctx->gm.as<double>(), L.kb.x, ctx->vn.as<double>(), ctx->dv.as<double>(),
+        ctx->vstar.as<double>(), L.sc);
+    k_newton_advance<<<1, 1, 0, st>>>(L.sc, L.np.nmax, hN, use_graph);
+    g_kernel_launches += 2;
+    return ZMPM_OK;
+}
+
+#define ZMPM_CAP(expr)                                                                                                 \
+    do {                                                                                                               \
+        cudaError_t _e = (expr);                                                                                       \
+        if (_e != cudaSuccess) {                                                                                       \
+            ctx->err = std::string(#expr) + ": " + cudaGetErrorString(_e);                                             \
+            cudaStreamCaptureStatus _cs;                                                                               \
+            if (cudaStreamIsCapturing(st, &_cs) == cudaSuccess && _cs != cudaStreamCaptureStatusNone) {               \
+                cudaGraph_t _g;                                                                                        \
+                cudaStreamEndCapture(st, &_g);                                                                         \
+            }                                                                                                          \
+            if (g) cudaGraphDestroy(g);                                                                                \
+            return ZMPM_CUDA_ERROR;                                                                                    \
+        }                                                                                                              \
+    } while (0)
+
+// The Newton solve as one CUDA graph: WHILE(Newton){ head; WHILE(Krylov){
+// iteration }; tail }.  Both loop conditions are set on the device, so the
+// host launches the whole solve once and no Krylov slot is launched idle.
+template <int NPB>
+int newton_graph(const NewtonLaunch& L, cudaGraphExec_t* exec_out)
+{
+    Ctx* ctx = L.ctx;
+    cudaStream_t st = ctx->stream;
+    cudaGraph_t g = nullptr;
+    ZMPM_CAP(cudaGraphCreate(&g, 0));
+    cudaGraphConditionalHandle hN, hK;
+    ZMPM_CAP(cudaGraphConditionalHandleCreate(&hN, g, 1, cudaGraphCondAssignDefault));
+    ZMPM_CAP(cudaGraphConditionalHandleCreate(&hK, g, 0, cudaGraphCondAssignDefault));
+    cudaGraphNodeParams pN = {};
+    pN.type = cudaGraphNodeTypeConditional;
+    pN.conditional.handle = hN;
+    pN.conditional.type = cudaGraphCondTypeWhile;
+    pN.conditional.size = 1;
+    cudaGraphNode_t nN;
+    ZMPM_CAP(cudaGraphAddNode(&nN, g, nullptr, 0, &pN));
+    cudaGraph_t bodyN = pN.conditional.phGraph_out[0];
+
+    ZMPM_CAP(cudaStreamBeginCaptureToGraph(st, bodyN, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    int rc = launch_newton_head<NPB>(L, st, hK, 1);
+    if (rc) {
+        cudaGraph_t tmp;
+        cudaStreamEndCapture(st, &tmp);
+        cudaGraphDestroy(g);
+        return rc;
+    }
+    cudaStreamCaptureStatus cst;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t ndeps = 0;
+    cudaGraph_t capg = nullptr;
+    ZMPM_CAP(cudaStreamGetCaptureInfo(st, &cst, nullptr, &capg, &deps, &ndeps));
+    cudaGraphNodeParams pK = {};
+    pK.type = cudaGraphNodeTypeConditional;
+    pK.conditional.handle = hK;
+    pK.conditional.type = cudaGraphCondTypeWhile;
+    pK.conditional.size = 1;
+    cudaGraphNode_t nK;
+    ZMPM_CAP(cudaGraphAddNode(&nK, capg, deps, ndeps, &pK));
+    ZMPM_CAP(cudaStreamUpdateCaptureDependencies(st, &nK, 1, cudaStreamSetCaptureDependencies));
+    cudaGraph_t bodyK = pK.conditional.phGraph_out[0];
+    rc = launch_newton_tail<NPB>(L, st, hN, 1);
+    cudaGraph_t tmp = nullptr;
+    ZMPM_CAP(cudaStreamEndCapture(st, &tmp));
+    if (rc) {
+        cudaGraphDestroy(g);
+        return rc;
+    }
+    ZMPM_CAP(cudaStreamBeginCaptureToGraph(st, bodyK, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    rc = launch_krylov_iteration<NPB>(L, st, hK, 1, nullptr, nullptr);
+    ZMPM_CAP(cudaStreamEndCapture(st, &tmp));
+    if (rc) {
+        cudaGraphDestroy(g);
+        return rc;
+    }
+    ZMPM_CAP(cudaGraphInstantiate(exec_out, g, 0));
+    cudaGraphDestroy(g);
+    return ZMPM_OK;
+}
+
+} // namespace
+
+template <int NPB>
 static int newton_impl(Ctx* ctx, const zmpm_solver& s)
 {
     cudaStream_t st = ctx->stream;
-    NodeGeom ng = node_geom(ctx);
-    SolverScalars* sc = ctx->scal.as<SolverScalars>();
+    NewtonLaunch L;
+    L.ctx = ctx;
+    L.ng = node_geom(ctx);
+    L.sc = ctx->scal.as<SolverScalars>();
     double* part = ctx->red.as<double>();
-    double *pA = part + RED_A * RED_MAX_CTAS, *pB = part + RED_B * RED_MAX_CTAS, *pC = part + RED_C * RED_MAX_CTAS;
-    KrylovBufs kb;
-    double** v = reinterpret_cast<double**>(ctx->kv);
-    (void)v;
-    kb.x = ctx->kv[0].as<double>();
-    kb.r = ctx->kv[1].as<double>();
-    kb.p = ctx->kv[2].as<double>();
-    kb.q = ctx->kv[3].as<double>();
-    kb.tmp = ctx->kv[4].as<double>();
-    kb.Q[0] = ctx->kv[1].as<double>();
-    kb.Q[1] = ctx->kv[2].as<double>();
-    kb.Q[2] = ctx->kv[3].as<double>();
-    kb.M[0] = ctx->kv[4].as<double>();
-    kb.M[1] = ctx->kv[5].as<double>();
-    kb.M[2] = ctx->kv[6].as<double>();
-    kb.Z[0] = ctx->kv[7].as<double>();
-    kb.Z[1] = ctx->kv[8].as<double>();
-    kb.hacc = ctx->kv[9].as<double>();
-    NewtonParams np{ s.linear_solver == ZMPM_MINRES ? 1 : 0, s.newton_tolerance, s.krylov_tolerance, s.linear_solve_tolerance_scale, ctx->dt };
-    const double dt2 = ctx->dt * ctx->dt;
-    ZMPM_CUDA(cudaMemsetAsync(sc, 0, sizeof(SolverScalars), st));
-    if (ng.nn == 0) return ZMPM_OK;
-    const int nb = ng.parts;
+    L.pA = part + RED_A * RED_MAX_CTAS;
+    L.pB = part + RED_B * RED_MAX_CTAS;
+    L.pC = part + RED_C * RED_MAX_CTAS;
+    L.kb.x = ctx->kv[0].as<double>();
+    L.kb.r = ctx->kv[1].as<double>();
+    L.kb.p = ctx->kv[2].as<double>();
+    L.kb.q = ctx->kv[3].as<double>();
+    L.kb.tmp = ctx->kv[4].as<double>();
+    L.kb.Q[0] = ctx->kv[1].as<double>();
+    L.kb.Q[1] = ctx->kv[2].as<double>();
+    L.kb.Q[2] = ctx->kv[3].as<double>();
+    L.kb.M[0] = ctx->kv[4].as<double>();
+    L.kb.M[1] = ctx->kv[5].as<double>();
+    L.kb.M[2] = ctx->kv[6].as<double>();
+    L.kb.Z[0] = ctx->kv[7].as<double>();
+    L.kb.Z[1] = ctx->kv[8].as<double>();
+    L.kb.hacc = ctx->kv[9].as<double>();
+    L.np.minres = s.linear_solver == ZMPM_MINRES ? 1 : 0;
+    L.np.kmax = s.krylov_max_iterations;
+    L.np.nmax = s.newton_max_iterations;
+    L.np.tol = s.newton_tolerance;
+    L.np.abs_tol = s.krylov_tolerance;
+    L.np.tol_scale = s.linear_solve_tolerance_scale;
+    L.np.dt = ctx->dt;
+    L.dt2 = ctx->dt * ctx->dt;
+    L.nb = L.ng.parts;
+    ZMPM_CUDA(cudaMemsetAsync(L.sc, 0, sizeof(SolverScalars), st));
+    ctx->prof_newton = 0;
+    ctx->graph_used = false;
+    if (L.ng.nn == 0 || s.newton_max_iterations == 0) return ZMPM_OK;
     const bool prof = ctx->profiling && s.newton_max_iterations <= 64;
+    if (!prof && !ctx->no_graph) {
+        // whole solve as one graph with device-side loop conditions
+        cudaGraphExec_t exec = nullptr;
+        const int64_t launches0 = g_kernel_launches;
+        int rc = newton_graph<NPB>(L, &exec);
+        if (rc) return rc;
+        cudaError_t e = cudaGraphLaunch(exec, st);
+        // kernels inside the graph are counted per executed loop body after the
+        // substep (see zmpm_substep), not once at capture
+        g_kernel_launches = launches0;
+        ctx->graph_used = true;
+        if (ctx->graph_exec) cudaGraphExecDestroy(ctx->graph_exec);
+        ctx->graph_exec = exec; // released after the next synchronisation
+        ZMPM_CUDA(e);
+        return ZMPM_OK;
+    }
+    // host-driven loop (profiling: each product bracketed by events)
     ctx->prof_newton = prof ? s.newton_max_iterations : 0;
     ctx->prof_krylov = s.krylov_max_iterations;
     if (prof) {
@@ -723,55 +964,18 @@ static int newton_impl(Ctx* ctx, const zmpm_solver& s)
         }
     }
     for (int it = 0; it < s.newton_max_iterations; ++it) {
-        int rc = launch_update(ctx);
+        int rc = launch_newton_head<NPB>(L, st, 0, 0);
         if (rc) return rc;
-        rc = launch_residual(ctx);
-        if (rc) return rc;
-        k_newton_check<NPB><<<nb, ND_THREADS, 0, st>>>(ng, ctx->gm.as<double>(), ctx->res.as<double>(), kb, np, pA, pB, sc, it == 0 ? 1 : 0);
-        ++g_kernel_launches;
-        k_krylov_start<NPB><<<nb, ND_THREADS, 0, st>>>(ng, kb, np, pB, sc);
-        ++g_kernel_launches;
         for (int k = 0; k < s.krylov_max_iterations; ++k) {
-            if (np.minres) {
-                double* zin = kb.Z[k & 1];
-                double* zout = kb.Z[(k + 1) & 1];
-                double* qk = kb.Q[k % 3];
-                double* qkm1 = kb.Q[(k + 2) % 3];
-                double* qkp1 = kb.Q[(k + 1) % 3];
-                double* mk = kb.M[k % 3];
-                double* mkm1 = kb.M[(k + 2) % 3];
-                double* mkm2 = kb.M[(k + 1) % 3];
-                if (prof) ZMPM_CUDA(cudaEventRecord(ctx->hvp_ev[2 * (it * s.krylov_max_iterations + k)], st));
-                launch_hvp_gated(ctx, zin, kb.hacc, true, k);
-                if (prof) ZMPM_CUDA(cudaEventRecord(ctx->hvp_ev[2 * (it * s.krylov_max_iterations + k) + 1], st));
-                k_apply_A<NPB><<<nb, ND_THREADS, 0, st>>>(ng, ctx->gm.as<double>(), ctx->collided.as<int8_t>(), ctx->proj.as<double>(), dt2, zin,
-                    kb.hacc, qkp1, pA, sc, 1, 1, k);
-                ++g_kernel_launches;
-                k_mr_b<NPB><<<nb, ND_THREADS, 0, st>>>(ng, ctx->gm.as<double>(), qkp1, qk, qkm1, zout, pA, pC, sc, k);
-                ++g_kernel_launches;
-                k_mr_c<NPB><<<nb, ND_THREADS, 0, st>>>(ng, qkp1, zout, zin, mkm1, mkm2, mk, kb.x, pC, sc, k, it);
-                ++g_kernel_launches;
-            }
-            else {
-                if (prof) ZMPM_CUDA(cudaEventRecord(ctx->hvp_ev[2 * (it * s.krylov_max_iterations + k)], st));
-                launch_hvp_gated(ctx, kb.p, kb.hacc, true, k);
-                if (prof) ZMPM_CUDA(cudaEventRecord(ctx->hvp_ev[2 * (it * s.krylov_max_iterations + k) + 1], st));
-                k_apply_A<NPB><<<nb, ND_THREADS, 0, st>>>(ng, ctx->gm.as<double>(), ctx->collided.as<int8_t>(), ctx->proj.as<double>(), dt2, kb.p,
-                    kb.hacc, kb.tmp, pA, sc, 1, 1, k);
-                ++g_kernel_launches;
-                k_cg_b<NPB><<<nb, ND_THREADS, 0, st>>>(ng, ctx->gm.as<double>(), kb, pA, pC, sc, k);
-                ++g_kernel_launches;
-                k_cg_c<NPB><<<nb, ND_THREADS, 0, st>>>(ng, kb, pC, sc, k, it);
-                ++g_kernel_launches;
-            }
+            cudaEvent_t e0 = prof ? ctx->hvp_ev[2 * (it * s.krylov_max_iterations + k)] : nullptr;
+            cudaEvent_t e1 = prof ? ctx->hvp_ev[2 * (it * s.krylov_max_iterations + k) + 1] : nullptr;
+            rc = launch_krylov_iteration<NPB>(L, st, 0, 0, e0, e1);
+            if (rc) return rc;
         }
-        k_newton_step<NPB><<<nb, ND_THREADS, 0, st>>>(ng, ctx->gm.as<double>(), kb.x, ctx->vn.as<double>(), ctx->dv.as<double>(),
-            ctx->vstar.as<double>(), sc);
-        ++g_kernel_launches;
+        rc = launch_newton_tail<NPB>(L, st, 0, 0);
+        if (rc) return rc;
         ZMPM_CUDA(cudaGetLastError());
     }
-    // the reference evaluates the residual once more only at the top of the
-    // next Newton iteration; vstar already holds vn + dv of the last step.
     return ZMPM_OK;
 }
 

@@ -280,11 +280,11 @@ __global__ void __launch_bounds__(XF_THREADS) k_p2g(const int32_t* __restrict__ 
 //            S = V0 P(F) Fn^T (to `stress`) and the Hessian scratch; particles in
 //            slot order so every particle array is read coalesced.
 //  k_force : facc -= sum_p S_p grad w_ip, layered conflict-free scatter.
-template <class L, class TH>
+template <class L, class TS, class TH>
 __global__ void __launch_bounds__(XF_THREADS) k_stress(const int32_t* __restrict__ group_start, const int32_t* __restrict__ group_nbr,
     const double* __restrict__ pd, const int32_t* __restrict__ pi, int64_t cap, const short4* __restrict__ base, double dx, double dt,
-    const double* __restrict__ vstar, double* __restrict__ stress, TH* __restrict__ scr, const SolverScalars* __restrict__ sc,
-    int32_t* __restrict__ flags)
+    const TH* __restrict__ frac, const double* __restrict__ vstar, TS* __restrict__ stress, TH* __restrict__ scr,
+    const SolverScalars* __restrict__ sc, int32_t* __restrict__ flags)
 {
     if (sc && sc->newton_done) return;
     constexpr int NPB = L::NPB;
@@ -295,83 +295,116 @@ __global__ void __launch_bounds__(XF_THREADS) k_stress(const int32_t* __restrict
     if (threadIdx.x < 8) nbr[threadIdx.x] = group_nbr[8 * g + threadIdx.x];
     __syncthreads();
     stage_window<NPB>(win, vstar, nbr, &bar, flags);
-    const double inv_dx = 1.0 / dx;
+    const TS inv_dx = TS(1.0 / dx);
+    const TS tdt = TS(dt);
     const int s0 = group_start[g], s1 = group_start[g + 1];
     for (int s = s0 + threadIdx.x; s < s1; s += blockDim.x) {
         const int kind = pi[PI_KIND * cap + s];
         if (kind == ZMPM_MODEL_NONE) {
 #pragma unroll
-            for (int q = 0; q < 9; ++q) stress[q * cap + s] = 0.0;
+            for (int q = 0; q < 9; ++q) stress[q * cap + s] = TS(0);
             continue;
         }
         const short4 b = base[s];
-        double w[3][3], dwr[3][3];
+        TS w[3][3], dwr[3][3];
 #pragma unroll
-        for (int d = 0; d < 3; ++d) {
-            double d0 = inv_dx * pd[(PD_X + d) * cap + s] - (double)((&b.x)[d]);
-            bspline(d0, w[d], dwr[d]);
-        }
+        for (int d = 0; d < 3; ++d) bspline((TS)frac[d * cap + s], w[d], dwr[d]);
         const int lx = b.x & (L::BX - 1), ly = b.y & (L::BY - 1), lz = b.z & (L::BZ - 1);
-        M3<double> gv = m3_zero<double>();
-        for_stencil<L>(lx, ly, lz, w, dwr, inv_dx, [&](int t, int e, int, int, int, double, const double* dw) {
+        M3<TS> gv = m3_zero<TS>();
+        for_stencil<L>(lx, ly, lz, w, dwr, inv_dx, [&](int t, int e, int, int, int, TS, const TS* dw) {
             const double* vv = win + t * 3 * NPB + e;
 #pragma unroll
             for (int r = 0; r < 3; ++r) {
-                double vr = vv[r * NPB];
+                TS vr = (TS)vv[r * NPB];
 #pragma unroll
                 for (int c = 0; c < 3; ++c) gv(r, c) += vr * dw[c];
             }
         });
-        M3<double> Fn, A = m3_identity<double>();
+        M3<TS> Fn, A = m3_identity<TS>();
 #pragma unroll
         for (int q = 0; q < 9; ++q) {
-            Fn.a[q] = pd[(PD_F + q) * cap + s];
-            A.a[q] += dt * gv.a[q];
+            Fn.a[q] = (TS)pd[(PD_F + q) * cap + s];
+            A.a[q] += tdt * gv.a[q];
         }
-        M3<double> F = m3_mul(A, Fn);
+        M3<TS> F = m3_mul(A, Fn);
         ModelParams mp{ pd[PD_MU * cap + s], pd[PD_LAM * cap + s], pd[PD_KAPPA * cap + s], pd[PD_G * cap + s] };
-        M3<double> S = model_update<double, TH>(kind, mp, pd[PD_VOL * cap + s], F, Fn, scr, cap, s);
+        const double V0 = pd[PD_VOL * cap + s];
+        bool degenerate = false;
+        M3<TS> S = model_update<TS, TH>(kind, mp, (TS)V0, F, Fn, scr, cap, s, sizeof(TS) == 4 ? &degenerate : nullptr);
+        if constexpr (sizeof(TS) == 4) {
+            if (degenerate) { // FP64 re-evaluation of near-degenerate particles
+                M3<double> Fnd, Ad = m3_identity<double>();
+#pragma unroll
+                for (int q = 0; q < 9; ++q) {
+                    Fnd.a[q] = pd[(PD_F + q) * cap + s];
+                    Ad.a[q] += dt * (double)gv.a[q];
+                }
+                S = m3_cast<TS>(model_update<double, TH>(kind, mp, V0, m3_mul(Ad, Fnd), Fnd, scr, cap, s, nullptr));
+            }
+        }
 #pragma unroll
         for (int q = 0; q < 9; ++q) stress[q * cap + s] = S.a[q];
     }
 }
 
-template <class L>
+template <class L, class TS, class TH>
 __global__ void __launch_bounds__(XF_THREADS) k_force(const int32_t* __restrict__ group_start, const int32_t* __restrict__ group_nbr,
-    const double* __restrict__ pd, int64_t cap, const short4* __restrict__ base, double dx, const double* __restrict__ stress,
+    int64_t cap, const short4* __restrict__ base, double dx, const TH* __restrict__ frac, const TS* __restrict__ stress,
     double* __restrict__ facc, const SolverScalars* __restrict__ sc)
 {
     if (sc && sc->newton_done) return;
     constexpr int NPB = L::NPB;
-    __shared__ __align__(16) double acc[8 * 3 * NPB];
+    __shared__ __align__(16) TS acc[8 * 3 * NPB];
     __shared__ int32_t nbr[8];
     __shared__ CellLayout<L> cl;
     const int g = blockIdx.x;
     if (threadIdx.x < 8) nbr[threadIdx.x] = group_nbr[8 * g + threadIdx.x];
     zero_window<3, NPB>(acc);
-    const double inv_dx = 1.0 / dx;
+    const TS inv_dx = TS(1.0 / dx);
     const int s0 = group_start[g], s1 = group_start[g + 1];
     build_cell_layout<L>(cl, base, s0, s1);
-    for (int q = threadIdx.x; q < cl.layers * NPB; q += blockDim.x) {
-        const int r = q / NPB, ce = q % NPB;
-        if (r >= cl.cnt[ce]) continue;
-        const int s = s0 + cl.start[ce] + r;
-        const short4 b = base[s];
-        double w[3][3], dwr[3][3];
+    // One cell per thread (see k_hvp_scatter): FP32 keeps all 81 sums in
+    // registers, FP64 one force component per pass.
+    const int ce = threadIdx.x % NPB;
+    const int lx = ce >> (L::YB + L::ZB), ly = (ce >> L::ZB) & (L::BY - 1), lz = ce & (L::BZ - 1);
+    const int cnt = cl.cnt[ce], first = s0 + cl.start[ce];
+    constexpr int NCP = sizeof(TS) == 4 ? 3 : 1;
+#pragma unroll 1
+    for (int c0 = 0; c0 < 3; c0 += NCP) {
+        TS a[27][NCP];
 #pragma unroll
-        for (int d = 0; d < 3; ++d) {
-            double d0 = inv_dx * pd[(PD_X + d) * cap + s] - (double)((&b.x)[d]);
-            bspline(d0, w[d], dwr[d]);
+        for (int n = 0; n < 27; ++n)
+#pragma unroll
+            for (int c = 0; c < NCP; ++c) a[n][c] = TS(0);
+        for (int r = threadIdx.x / NPB; r < cnt; r += blockDim.x / NPB) {
+            const int s = first + r;
+            TS w[3][3], dwr[3][3];
+#pragma unroll
+            for (int d = 0; d < 3; ++d) bspline((TS)frac[d * cap + s], w[d], dwr[d]);
+            TS row[NCP][3];
+#pragma unroll
+            for (int c = 0; c < NCP; ++c)
+#pragma unroll
+                for (int q2 = 0; q2 < 3; ++q2) row[c][q2] = stress[(3 * (c0 + c) + q2) * cap + s];
+            for_stencil<L>(lx, ly, lz, w, dwr, inv_dx, [&](int, int, int i, int j, int k, TS, const TS* dw) {
+                const int n = 9 * i + 3 * j + k;
+#pragma unroll
+                for (int c = 0; c < NCP; ++c) a[n][c] -= row[c][0] * dw[0] + row[c][1] * dw[1] + row[c][2] * dw[2];
+            });
         }
-        M3<double> S;
+        if (threadIdx.x / NPB < cnt) {
 #pragma unroll
-        for (int q2 = 0; q2 < 9; ++q2) S.a[q2] = stress[q2 * cap + s];
-        const int lx = b.x & (L::BX - 1), ly = b.y & (L::BY - 1), lz = b.z & (L::BZ - 1);
-        for_stencil<L>(lx, ly, lz, w, dwr, inv_dx, [&](int t, int e, int, int, int, double, const double* dw) {
-            double* a = acc + t * 3 * NPB + e;
+            for (int i = 0; i < 3; ++i)
 #pragma unroll
-            for (int c = 0; c < 3; ++c) atomicAdd(a + c * NPB, -(S(c, 0) * dw[0] + S(c, 1) * dw[1] + S(c, 2) * dw[2]));
-        });
+                for (int j = 0; j < 3; ++j)
+#pragma unroll
+                    for (int k = 0; k < 3; ++k) {
+                        int e;
+                        const int t = win_slot<L>(lx + i, ly + j, lz + k, e);
+#pragma unroll
+                        for (int c = 0; c < NCP; ++c) atomicAdd(acc + t * 3 * NPB + (c0 + c) * NPB + e, a[9 * i + 3 * j + k][c]);
+                    }
+        }
     }
     __syncthreads();
     flush_window<3, 3, NPB>(acc, nbr, facc, nullptr);
@@ -384,10 +417,10 @@ __global__ void __launch_bounds__(XF_THREADS) k_force(const int32_t* __restrict_
 template <class L, class TH>
 __global__ void __launch_bounds__(XF_THREADS, sizeof(TH) == 4 ? 4 : 2) k_hvp(const int32_t* __restrict__ group_start, const int32_t* __restrict__ group_nbr,
     const int32_t* __restrict__ pi, int64_t cap, const short4* __restrict__ base, double dx, const TH* __restrict__ frac,
-    const TH* __restrict__ scr, const double* __restrict__ x, double* __restrict__ out, const SolverScalars* __restrict__ sc,
-    int32_t* __restrict__ flags, int it)
+    const TH* __restrict__ scr, const double* __restrict__ x0, const double* __restrict__ x1, int alt, double* __restrict__ out,
+    const SolverScalars* __restrict__ sc, int32_t* __restrict__ flags)
 {
-    if (sc && (sc->newton_done || it >= sc->stop_at)) return;
+    if (sc && (sc->newton_done || !sc->kactive)) return;
     constexpr int NPB = L::NPB;
     __shared__ __align__(128) double win[8 * 3 * NPB];
     __shared__ __align__(16) TH acc[8 * 3 * NPB];
@@ -398,6 +431,8 @@ __global__ void __launch_bounds__(XF_THREADS, sizeof(TH) == 4 ? 4 : 2) k_hvp(con
     if (threadIdx.x < 8) nbr[threadIdx.x] = group_nbr[8 * g + threadIdx.x];
     zero_window<3, NPB>(acc);
     __syncthreads();
+    // the input alternates between x0 and x1 with the Krylov iteration (MINRES)
+    const double* x = (alt && sc && (sc->kit & 1)) ? x1 : x0;
     stage_window<NPB>(win, x, nbr, &bar, flags);
     const TH inv_dx = TH(1.0 / dx);
     const int s0 = group_start[g], s1 = group_start[g + 1];
@@ -444,10 +479,10 @@ __global__ void __launch_bounds__(XF_THREADS, sizeof(TH) == 4 ? 4 : 2) k_hvp(con
 template <class L, class TH>
 __global__ void __launch_bounds__(XF_THREADS) k_hvp_stress(const int32_t* __restrict__ group_start, const int32_t* __restrict__ group_nbr,
     const int32_t* __restrict__ pi, int64_t cap, const short4* __restrict__ base, double dx, const TH* __restrict__ frac,
-    const TH* __restrict__ scr, const double* __restrict__ x, TH* __restrict__ dstress, const SolverScalars* __restrict__ sc,
-    int32_t* __restrict__ flags, int it)
+    const TH* __restrict__ scr, const double* __restrict__ x0, const double* __restrict__ x1, int alt, TH* __restrict__ dstress,
+    const SolverScalars* __restrict__ sc, int32_t* __restrict__ flags)
 {
-    if (sc && (sc->newton_done || it >= sc->stop_at)) return;
+    if (sc && (sc->newton_done || !sc->kactive)) return;
     constexpr int NPB = L::NPB;
     __shared__ __align__(128) double win[8 * 3 * NPB];
     __shared__ int32_t nbr[8];
@@ -455,6 +490,8 @@ __global__ void __launch_bounds__(XF_THREADS) k_hvp_stress(const int32_t* __rest
     const int g = blockIdx.x;
     if (threadIdx.x < 8) nbr[threadIdx.x] = group_nbr[8 * g + threadIdx.x];
     __syncthreads();
+    // the input alternates between x0 and x1 with the Krylov iteration (MINRES)
+    const double* x = (alt && sc && (sc->kit & 1)) ? x1 : x0;
     stage_window<NPB>(win, x, nbr, &bar, flags);
     const TH inv_dx = TH(1.0 / dx);
     const int s0 = group_start[g], s1 = group_start[g + 1];
@@ -489,9 +526,9 @@ __global__ void __launch_bounds__(XF_THREADS) k_hvp_stress(const int32_t* __rest
 template <class L, class TH>
 __global__ void __launch_bounds__(XF_THREADS) k_hvp_scatter(const int32_t* __restrict__ group_start, const int32_t* __restrict__ group_nbr,
     int64_t cap, const short4* __restrict__ base, double dx, const TH* __restrict__ frac, const TH* __restrict__ dstress,
-    double* __restrict__ out, const SolverScalars* __restrict__ sc, int it)
+    double* __restrict__ out, const SolverScalars* __restrict__ sc)
 {
-    if (sc && (sc->newton_done || it >= sc->stop_at)) return;
+    if (sc && (sc->newton_done || !sc->kactive)) return;
     constexpr int NPB = L::NPB;
     __shared__ __align__(16) TH acc[8 * 3 * NPB];
     __shared__ int32_t nbr[8];
@@ -502,23 +539,51 @@ __global__ void __launch_bounds__(XF_THREADS) k_hvp_scatter(const int32_t* __res
     const TH inv_dx = TH(1.0 / dx);
     const int s0 = group_start[g], s1 = group_start[g + 1];
     build_cell_layout<L>(cl, base, s0, s1);
-    for (int q = threadIdx.x; q < cl.layers * NPB; q += blockDim.x) {
-        const int r = q / NPB, ce = q % NPB;
-        if (r >= cl.cnt[ce]) continue;
-        const int s = s0 + cl.start[ce] + r;
-        const short4 b = base[s];
-        TH w[3][3], dwr[3][3];
+    // Thread -> one cell (ce) and every (blockDim/NPB)-th particle of it: all of
+    // its particles share the cell's 27 nodes, so their contributions are summed
+    // in registers and added to the window once.
+    const int ce = threadIdx.x % NPB;
+    const int lx = ce >> (L::YB + L::ZB), ly = (ce >> L::ZB) & (L::BY - 1), lz = ce & (L::BZ - 1);
+    const int cnt = cl.cnt[ce], first = s0 + cl.start[ce];
+    // FP32 keeps all 81 sums in registers (one pass); FP64 one component per pass.
+    constexpr int NCP = sizeof(TH) == 4 ? 3 : 1;
+#pragma unroll 1
+    for (int c0 = 0; c0 < 3; c0 += NCP) {
+        TH a[27][NCP];
 #pragma unroll
-        for (int d = 0; d < 3; ++d) bspline(frac[d * cap + s], w[d], dwr[d]);
-        M3<TH> dS;
+        for (int n = 0; n < 27; ++n)
 #pragma unroll
-        for (int q2 = 0; q2 < 9; ++q2) dS.a[q2] = dstress[q2 * cap + s];
-        const int lx = b.x & (L::BX - 1), ly = b.y & (L::BY - 1), lz = b.z & (L::BZ - 1);
-        for_stencil<L>(lx, ly, lz, w, dwr, inv_dx, [&](int t, int e, int, int, int, TH, const TH* dw) {
-            TH* a = acc + t * 3 * NPB + e;
+            for (int c = 0; c < NCP; ++c) a[n][c] = TH(0);
+        for (int r = threadIdx.x / NPB; r < cnt; r += blockDim.x / NPB) {
+            const int s = first + r;
+            TH w[3][3], dwr[3][3];
 #pragma unroll
-            for (int c = 0; c < 3; ++c) atomicAdd(a + c * NPB, dS(c, 0) * dw[0] + dS(c, 1) * dw[1] + dS(c, 2) * dw[2]);
-        });
+            for (int d = 0; d < 3; ++d) bspline(frac[d * cap + s], w[d], dwr[d]);
+            TH row[NCP][3];
+#pragma unroll
+            for (int c = 0; c < NCP; ++c)
+#pragma unroll
+                for (int q2 = 0; q2 < 3; ++q2) row[c][q2] = dstress[(3 * (c0 + c) + q2) * cap + s];
+            for_stencil<L>(lx, ly, lz, w, dwr, inv_dx, [&](int, int, int i, int j, int k, TH, const TH* dw) {
+                const int n = 9 * i + 3 * j + k;
+#pragma unroll
+                for (int c = 0; c < NCP; ++c) a[n][c] += row[c][0] * dw[0] + row[c][1] * dw[1] + row[c][2] * dw[2];
+            });
+        }
+        if (threadIdx.x / NPB < cnt) {
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+#pragma unroll
+                for (int j = 0; j < 3; ++j)
+#pragma unroll
+                    for (int k = 0; k < 3; ++k) {
+                        int e;
+                        const int t = win_slot<L>(lx + i, ly + j, lz + k, e);
+                        TH* dst = acc + t * 3 * NPB + e;
+#pragma unroll
+                        for (int c = 0; c < NCP; ++c) atomicAdd(dst + (c0 + c) * NPB, a[9 * i + 3 * j + k][c]);
+                    }
+        }
     }
     __syncthreads();
     flush_window<3, 3, NPB>(acc, nbr, out, nullptr);
@@ -631,63 +696,73 @@ static int update_impl(Ctx* ctx)
     if (G == 0) return ZMPM_OK;
     DevCounters* dc = ctx->counters.as<DevCounters>();
     const SolverScalars* sc = ctx->scal.as<SolverScalars>();
-    if (ctx->mixed)
-        k_stress<L, float><<<(unsigned)G, XF_THREADS, 0, ctx->stream>>>(ctx->group_start.as<int32_t>(), ctx->group_nbr.as<int32_t>(),
-            ctx->pd.as<double>(), ctx->pi.as<int32_t>(), ctx->Pcap, ctx->base.as<short4>(), ctx->cfg.dx, ctx->dt, ctx->vstar.as<double>(),
-            ctx->stress.as<double>(), ctx->scratch.as<float>(), sc, &dc->flags);
-    else
-        k_stress<L, double><<<(unsigned)G, XF_THREADS, 0, ctx->stream>>>(ctx->group_start.as<int32_t>(), ctx->group_nbr.as<int32_t>(),
-            ctx->pd.as<double>(), ctx->pi.as<int32_t>(), ctx->Pcap, ctx->base.as<short4>(), ctx->cfg.dx, ctx->dt, ctx->vstar.as<double>(),
-            ctx->stress.as<double>(), ctx->scratch.as<double>(), sc, &dc->flags);
-    ++g_kernel_launches;
-    k_force<L><<<(unsigned)G, XF_THREADS, 0, ctx->stream>>>(ctx->group_start.as<int32_t>(), ctx->group_nbr.as<int32_t>(), ctx->pd.as<double>(),
-        ctx->Pcap, ctx->base.as<short4>(), ctx->cfg.dx, ctx->stress.as<double>(), ctx->facc.as<double>(), sc);
-    ++g_kernel_launches;
+    if (ctx->mixed) {
+        k_stress<L, float, float><<<(unsigned)G, XF_THREADS, 0, ctx->stream>>>(ctx->group_start.as<int32_t>(), ctx->group_nbr.as<int32_t>(),
+            ctx->pd.as<double>(), ctx->pi.as<int32_t>(), ctx->Pcap, ctx->base.as<short4>(), ctx->cfg.dx, ctx->dt, ctx->frac.as<float>(),
+            ctx->vstar.as<double>(), ctx->stress.as<float>(), ctx->scratch.as<float>(), sc, &dc->flags);
+        ++g_kernel_launches;
+        k_force<L, float, float><<<(unsigned)G, XF_THREADS, 0, ctx->stream>>>(ctx->group_start.as<int32_t>(), ctx->group_nbr.as<int32_t>(),
+            ctx->Pcap, ctx->base.as<short4>(), ctx->cfg.dx, ctx->frac.as<float>(), ctx->stress.as<float>(), ctx->facc.as<double>(), sc);
+        ++g_kernel_launches;
+    }
+    else {
+        k_stress<L, double, double><<<(unsigned)G, XF_THREADS, 0, ctx->stream>>>(ctx->group_start.as<int32_t>(), ctx->group_nbr.as<int32_t>(),
+            ctx->pd.as<double>(), ctx->pi.as<int32_t>(), ctx->Pcap, ctx->base.as<short4>(), ctx->cfg.dx, ctx->dt, ctx->frac.as<double>(),
+            ctx->vstar.as<double>(), ctx->stress.as<double>(), ctx->scratch.as<double>(), sc, &dc->flags);
+        ++g_kernel_launches;
+        k_force<L, double, double><<<(unsigned)G, XF_THREADS, 0, ctx->stream>>>(ctx->group_start.as<int32_t>(), ctx->group_nbr.as<int32_t>(),
+            ctx->Pcap, ctx->base.as<short4>(), ctx->cfg.dx, ctx->frac.as<double>(), ctx->stress.as<double>(), ctx->facc.as<double>(), sc);
+        ++g_kernel_launches;
+    }
     return ZMPM_OK;
 }
 int launch_update(Ctx* ctx) { return ctx->layout == 1 ? update_impl<Layout244>(ctx) : update_impl<Layout444>(ctx); }
 
 template <class L, class TH>
-static void hvp_launch(Ctx* ctx, const double* x, double* out, const SolverScalars* sc, int it)
+static void hvp_launch(Ctx* ctx, const double* x0, const double* x1, int alt, double* out, const SolverScalars* sc)
 {
     const int64_t G = ctx->G;
     DevCounters* dc = ctx->counters.as<DevCounters>();
     if (ctx->hvp_fused) {
         k_hvp<L, TH><<<(unsigned)G, XF_THREADS, 0, ctx->stream>>>(ctx->group_start.as<int32_t>(), ctx->group_nbr.as<int32_t>(),
-            ctx->pi.as<int32_t>(), ctx->Pcap, ctx->base.as<short4>(), ctx->cfg.dx, ctx->frac.as<TH>(), ctx->scratch.as<TH>(), x, out, sc,
-            &dc->flags, it);
+            ctx->pi.as<int32_t>(), ctx->Pcap, ctx->base.as<short4>(), ctx->cfg.dx, ctx->frac.as<TH>(), ctx->scratch.as<TH>(), x0, x1, alt, out,
+            sc, &dc->flags);
         ++g_kernel_launches;
         return;
     }
     k_hvp_stress<L, TH><<<(unsigned)G, XF_THREADS, 0, ctx->stream>>>(ctx->group_start.as<int32_t>(), ctx->group_nbr.as<int32_t>(),
-        ctx->pi.as<int32_t>(), ctx->Pcap, ctx->base.as<short4>(), ctx->cfg.dx, ctx->frac.as<TH>(), ctx->scratch.as<TH>(), x,
-        ctx->dstress.as<TH>(), sc, &dc->flags, it);
+        ctx->pi.as<int32_t>(), ctx->Pcap, ctx->base.as<short4>(), ctx->cfg.dx, ctx->frac.as<TH>(), ctx->scratch.as<TH>(), x0, x1, alt,
+        ctx->dstress.as<TH>(), sc, &dc->flags);
     ++g_kernel_launches;
     k_hvp_scatter<L, TH><<<(unsigned)G, XF_THREADS, 0, ctx->stream>>>(ctx->group_start.as<int32_t>(), ctx->group_nbr.as<int32_t>(), ctx->Pcap,
-        ctx->base.as<short4>(), ctx->cfg.dx, ctx->frac.as<TH>(), ctx->dstress.as<TH>(), out, sc, it);
+        ctx->base.as<short4>(), ctx->cfg.dx, ctx->frac.as<TH>(), ctx->dstress.as<TH>(), out, sc);
     ++g_kernel_launches;
 }
 
 template <class L>
-static int hvp_impl(Ctx* ctx, const double* x, double* out, bool fp32, bool gated, int it)
+static int hvp_impl(Ctx* ctx, const double* x0, const double* x1, int alt, double* out, bool fp32, const SolverScalars* sc)
 {
     if (ctx->G == 0) return ZMPM_OK;
-    const SolverScalars* sc = gated ? ctx->scal.as<SolverScalars>() : nullptr;
     if (fp32)
-        hvp_launch<L, float>(ctx, x, out, sc, it);
+        hvp_launch<L, float>(ctx, x0, x1, alt, out, sc);
     else
-        hvp_launch<L, double>(ctx, x, out, sc, it);
+        hvp_launch<L, double>(ctx, x0, x1, alt, out, sc);
     return ZMPM_OK;
 }
-int launch_hvp_gated(Ctx* ctx, const double* x, double* out, bool gated, int it)
+
+// Product inside the Newton solve: gated by the solver scalars; with alt the
+// input is x0 on even and x1 on odd Krylov iterations.
+int launch_hvp_krylov(Ctx* ctx, const double* x0, const double* x1, bool alt, double* out)
 {
-    bool fp32 = ctx->mixed;
-    return ctx->layout == 1 ? hvp_impl<Layout244>(ctx, x, out, fp32, gated, it) : hvp_impl<Layout444>(ctx, x, out, fp32, gated, it);
+    const SolverScalars* sc = ctx->scal.as<SolverScalars>();
+    return ctx->layout == 1 ? hvp_impl<Layout244>(ctx, x0, x1, alt ? 1 : 0, out, ctx->mixed, sc)
+                            : hvp_impl<Layout444>(ctx, x0, x1, alt ? 1 : 0, out, ctx->mixed, sc);
 }
+
 int launch_hvp(Ctx* ctx, const double* x, double* out, bool fp32)
 {
     if (fp32 && !ctx->mixed) return ZMPM_UNSUPPORTED;
-    return ctx->layout == 1 ? hvp_impl<Layout244>(ctx, x, out, ctx->mixed, false, 0) : hvp_impl<Layout444>(ctx, x, out, ctx->mixed, false, 0);
+    return ctx->layout == 1 ? hvp_impl<Layout244>(ctx, x, x, 0, out, ctx->mixed, nullptr) : hvp_impl<Layout444>(ctx, x, x, 0, out, ctx->mixed, nullptr);
 }
 
 template <class L>
