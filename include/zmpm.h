@@ -79,6 +79,19 @@ enum zmpm_plasticity {
     ZMPM_PLASTIC_VON_MISES = 1
 };
 
+/* Damage models applied after P2G (FractureSimulation::particlesToGrid,
+   Projects/fracture/FractureSimulation.h:149-160). */
+enum zmpm_damage {
+    ZMPM_DAMAGE_NONE = 0,
+    /* Rankine ("naive") damage, FractureSimulation::solvePhaseFieldSystemNaive
+       (FractureSimulation.h:509-554): principal Cauchy stress of the undegraded
+       NeoHookeanBorden stress, c <- min(c, sigma_F / sigma_max) when
+       sigma_max > sigma_F, g = c^2 (1 - k) + k.  sigma_max is the largest
+       principal stress (the reference takes the first eigenvalue in the order
+       of Eigen's general eigen-solver). */
+    ZMPM_DAMAGE_RANKINE = 1
+};
+
 /* Krylov solver of the Newton step (BackwardEuler.h:82-98). */
 enum zmpm_linear_solver { ZMPM_MINRES = 0, ZMPM_CG = 1 };
 
@@ -191,6 +204,14 @@ int zmpm_set_lame(zmpm_ctx* ctx, int64_t lower, int64_t upper, const double* mu,
 /* MpmParticleHandleBase::addPlasticity (MpmParticleHandleBase.cpp:331-348). */
 int zmpm_add_plasticity(zmpm_ctx* ctx, int64_t lower, int64_t upper, int32_t kind,
     double yield_stress, double xi, double fail_stress);
+
+/* Damage on particles [lower, upper) that use NeoHookeanBorden: the phase
+   field of MpmParticleHandleBase::addFBasedMpmForceWithPhaseField
+   (MpmParticleHandleBase.cpp:92-118: c = 1, residual_phase) and
+   FractureSimulation::sigmaF (FractureSimulation.h:52). */
+int zmpm_add_damage(zmpm_ctx* ctx, int64_t lower, int64_t upper, int32_t kind, double sigma_f, double residual_phase);
+/* Phase-field value c per particle (1 undamaged, 0 fully damaged). */
+int zmpm_get_damage(zmpm_ctx* ctx, double* c);
 
 /* MpmSimulationBase::addCollisionObject (MpmSimulationBase.cpp:80-84). */
 int zmpm_add_collision_object(zmpm_ctx* ctx, const zmpm_collider* obj, int32_t* id);

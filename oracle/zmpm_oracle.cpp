@@ -5,7 +5,8 @@
 // C++17 + OpenMP because the reference itself cannot be built here (it needs
 // Eigen3, TBB, OpenVDB and partio, none of which are present).  Only the test
 // suite, __graft_entry__.smoke() and bench.py's CPU-baseline leg load it, and
-// only as the checker / timed CPU baseline; the CUDA library never calls it.
+// only to check results and as the timed CPU baseline; the CUDA library never
+// calls it.
 //
 // Parity pinning:
 //   * SPGrid addressing (Linear_Offset, Packed_Add, page map) is pinned against
@@ -787,6 +788,65 @@ static void vonMisesProject(const Model<T>& c, Plastic<T>& p, M3<T>& F)
     }
 }
 
+// ---------------------------------------------------------------- damage --
+template <class T>
+struct Damage {
+    int32_t kind = ZMPM_DAMAGE_NONE;
+    T c = 1, k = T(0.001), sigma_f = 0;
+};
+
+// Largest eigenvalue of a symmetric 3x3 matrix by cyclic Jacobi rotations
+// (Golub & Van Loan, Matrix Computations, 8.5.2).
+template <class T>
+static T sym3_max_eig_jacobi(M3<T> A)
+{
+    for (int sweep = 0; sweep < 50; ++sweep) {
+        T off = A.a[0][1] * A.a[0][1] + A.a[0][2] * A.a[0][2] + A.a[1][2] * A.a[1][2];
+        if (off == 0) break;
+        for (int p = 0; p < 2; ++p)
+            for (int q = p + 1; q < 3; ++q) {
+                if (A.a[p][q] == 0) continue;
+                T theta = (A.a[q][q] - A.a[p][p]) / (2 * A.a[p][q]);
+                T t = (theta >= 0 ? T(1) : T(-1)) / (std::fabs(theta) + std::sqrt(theta * theta + 1));
+                T c = 1 / std::sqrt(t * t + 1), s = t * c;
+                for (int k = 0; k < 3; ++k) { // A <- J^T A J
+                    T akp = A.a[k][p], akq = A.a[k][q];
+                    A.a[k][p] = c * akp - s * akq;
+                    A.a[k][q] = s * akp + c * akq;
+                }
+                for (int k = 0; k < 3; ++k) {
+                    T apk = A.a[p][k], aqk = A.a[q][k];
+                    A.a[p][k] = c * apk - s * aqk;
+                    A.a[q][k] = s * apk + c * aqk;
+                }
+            }
+    }
+    return std::max(A.a[0][0], std::max(A.a[1][1], A.a[2][2]));
+}
+
+// FractureSimulation::solvePhaseFieldSystemNaive, FractureSimulation.h:509-554
+// (largest principal Cauchy stress of the undegraded NeoHookeanBorden stress).
+template <class T>
+static void rankineUpdate(Model<T>& c, Damage<T>& d, const M3<T>& F)
+{
+    T J = det(F);
+    M3<T> B = mulT(F, F);
+    T tr = B.a[0][0] + B.a[1][1] + B.a[2][2];
+    T sdev = c.mu * std::pow(J, -T(2) / T(3));
+    T vol = J * (c.kappa / 2 * (J - 1 / J));
+    M3<T> cauchy;
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) {
+            T dv = (i == j) ? B.a[i][j] - T(1) / 3 * tr : B.a[i][j];
+            cauchy.a[i][j] = ((i == j) ? sdev * dv + vol : sdev * dv) / J;
+        }
+    T smax = sym3_max_eig_jacobi(cauchy);
+    T newC = d.c;
+    if (smax > d.sigma_f) newC = std::min(d.c, d.sigma_f / smax);
+    d.c = newC;
+    c.g = newC * newC * (1 - d.k) + d.k;
+}
+
 // ------------------------------------------------------------- colliders --
 template <class T>
 struct Collider {
@@ -1006,6 +1066,7 @@ struct Sim {
     std::vector<T> X, V, Cm, F, Fn, mass, vol;
     std::vector<Model<T>> model;
     std::vector<Plastic<T>> plastic;
+    std::vector<Damage<T>> damage;
     std::vector<Scratch<T>> scratch;
     std::vector<M3<T>> gradV, stress;
     std::vector<Collider<T>> colliders;
@@ -1622,6 +1683,11 @@ struct Sim {
         int st = sortParticlesAndPolluteGrid();
         if (st != ZMPM_OK) return st;
         particlesToGrid();
+        // FractureSimulation::particlesToGrid runs the damage update after P2G
+#pragma omp parallel for schedule(static)
+        for (int64_t i = 0; i < P; ++i)
+            if (damage[i].kind == ZMPM_DAMAGE_RANKINE && model[i].kind == ZMPM_MODEL_NEOHOOKEAN_BORDEN)
+                rankineUpdate(model[i], damage[i], load9(F, i));
         startBackwardEuler();
         return ZMPM_OK;
     }
@@ -1695,6 +1761,7 @@ static void add_particles_impl(SimT& S, int64_t n, const double* x, const double
         S.vol.push_back((T)vol[i]);
         S.model.emplace_back();
         S.plastic.emplace_back();
+        S.damage.emplace_back();
     }
     S.P += n;
     S.Fn = S.F;
@@ -1800,6 +1867,31 @@ int zoracle_add_plasticity(Ctx* c, int64_t lo, int64_t hi, int32_t kind, double 
             S.plastic[i].xi = (T)xi;
             S.plastic[i].fail_stress = (T)fs;
         }
+    });
+    return ZMPM_OK;
+}
+
+int zoracle_add_damage(Ctx* c, int64_t lo, int64_t hi, int32_t kind, double sigma_f, double residual_phase)
+{
+    if (!c) return ZMPM_BAD_ARG;
+    DISPATCH(c, {
+        using T = typename std::remove_reference<decltype(S.dx)>::type;
+        if (lo < 0 || hi > S.P || lo > hi) return ZMPM_BAD_ARG;
+        for (int64_t i = lo; i < hi; ++i) {
+            S.damage[i].kind = kind;
+            S.damage[i].sigma_f = (T)sigma_f;
+            S.damage[i].k = (T)residual_phase;
+            S.damage[i].c = 1;
+        }
+    });
+    return ZMPM_OK;
+}
+
+int zoracle_get_damage(Ctx* c, double* out)
+{
+    if (!c || !out) return ZMPM_BAD_ARG;
+    DISPATCH(c, {
+        for (int64_t i = 0; i < S.P; ++i) out[i] = S.damage[i].c;
     });
     return ZMPM_OK;
 }

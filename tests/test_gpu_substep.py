@@ -114,3 +114,41 @@ def test_free_fall_is_exact(cuda_lib):
         p = sim.getParticles()
         np.testing.assert_allclose(p["V"][:, 1], -9.8 * 4e-3, rtol=1e-12)
         np.testing.assert_allclose(p["F"], np.broadcast_to(np.eye(3), p["F"].shape), atol=1e-12)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_rankine_damage_matches_oracle(cuda_lib, oracle, precision):
+    """NeoHookeanBorden with naive Rankine damage (FractureSimulation.h:509-554):
+    a pre-stretched block softens where its principal stress passed sigma_F;
+    phase field c and the degraded dynamics follow the oracle."""
+    dx = 1.0 / 64
+    sims = [mpm.MpmSimulation(dx, gravity=(0, -9.8, 0), precision=precision, grid_log2=8),
+            mpm.MpmSimulation(dx, gravity=(0, -9.8, 0), precision="fp64", lib=oracle)]
+    rng = np.random.default_rng(11)
+    for s in sims:
+        h, x = build_scene(s, kind="nh", n=6, dx=dx, seed=2)
+        n = x.shape[0]
+        stretch = 1.0 + 0.2 * (x[:, 0] - x[:, 0].min()) / np.ptp(x[:, 0])
+        F = np.zeros((n, 3, 3))
+        F[:, 0, 0] = stretch
+        F[:, 1, 1] = F[:, 2, 2] = 1.0
+        s.setParticles(F=F)
+        h.addRankineDamage(2000.0, residual_phase=0.01)
+        s.newton_tolerance = 1e-7
+        s.newton_max_iterations = 12
+        s.krylov_max_iterations = 60
+    for _ in range(4):
+        for k, s in enumerate(sims):
+            rc = s.advanceOneTimeStep(1e-3)
+            assert rc == abi.OK, (k, rc, s.last_stats)
+    cg, co = sims[0].getDamage(), sims[1].getDamage()
+    assert (co < 1).sum() > 0 and (co == 1).sum() > 0
+    pg, po = sims[0].getParticles(), sims[1].getParticles()
+    if precision == "fp64":
+        np.testing.assert_allclose(cg, co, rtol=1e-9, atol=0)
+        assert rel(pg["X"], po["X"]) < 1e-10
+        assert rel(pg["V"], po["V"]) < 1e-6
+    else:
+        np.testing.assert_allclose(cg, co, rtol=1e-4, atol=0)
+        assert rel(pg["X"], po["X"]) < 1e-7
+        assert rel(pg["V"], po["V"]) < 1e-3

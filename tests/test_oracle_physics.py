@@ -144,3 +144,48 @@ def test_newton_converges_on_colliding_cube(oracle):
         assert rc == abi.OK
         assert sim.last_stats["newton_converged"] == 1
         assert sim.last_stats["num_collision_nodes"] > 0
+
+
+def _nh_uniaxial_cauchy_max(s, E, nu):
+    """Largest principal Cauchy stress of NeoHookeanBorden (g = 1) under F = R diag(s, 1, 1):
+    tau = mu J^(-2/3) dev(F F^T) + J kappa/2 (J - 1/J) I (NeoHookeanBorden.cpp:67-83)."""
+    mu = E / (2 * (1 + nu))
+    lam = E * nu / ((1 + nu) * (1 - 2 * nu))
+    kappa = 0.666666 * mu + lam
+    J = s
+    dev = np.array([s * s, 1.0, 1.0]) - (s * s + 2) / 3
+    tau = mu * J ** (-2.0 / 3.0) * dev + J * kappa / 2 * (J - 1 / J)
+    return (tau / J).max()
+
+
+def test_rankine_damage_known_answer(oracle):
+    """Naive Rankine damage (FractureSimulation.h:509-554): after P2G each
+    NeoHookeanBorden particle takes c = min(c, sigma_F / sigma_max) once its
+    largest principal Cauchy stress passes sigma_F, and g = c^2 (1 - k) + k.
+    Particles of another model are untouched."""
+    E, nu, dx = 1e4, 0.3, 1.0 / 64
+    sim = mpm.MpmSimulation(dx, gravity=(0, 0, 0), precision="fp64", lib=oracle)
+    x = jittered_box(4, dx, (0.4, 0.4, 0.4), 8, seed=3)
+    n = x.shape[0]
+    h_nh = sim.addParticles(x[: n // 2], np.zeros((n // 2, 3)), 1e-3, dx ** 3 / 8)
+    h_hk = sim.addParticles(x[n // 2:], np.zeros((n - n // 2, 3)), 1e-3, dx ** 3 / 8)
+    h_nh.addFBasedMpmForce(mpm.NeoHookeanBorden(E, nu))
+    h_hk.addFBasedMpmForce(mpm.StvkWithHenckyIsotropic(E, nu))
+    rng = np.random.default_rng(5)
+    stretch = rng.uniform(0.9, 1.3, n)
+    F = np.empty((n, 3, 3))
+    for i in range(n):
+        q, _ = np.linalg.qr(rng.standard_normal((3, 3)))
+        F[i] = q @ np.diag([stretch[i], 1.0, 1.0]) @ q.T
+    sim.setParticles(F=F)
+    smax = np.array([_nh_uniaxial_cauchy_max(s, E, nu) for s in stretch])
+    sigma_f = float(np.median(smax[: n // 2]))
+    h_nh.addRankineDamage(sigma_f, residual_phase=0.001)
+    h_hk.addRankineDamage(sigma_f, residual_phase=0.001)
+    assert np.all(sim.getDamage() == 1.0)
+    assert sim.advanceOneTimeStep(1e-4) == abi.OK
+    c = sim.getDamage()
+    want = np.where(smax > sigma_f, np.minimum(1.0, sigma_f / smax), 1.0)
+    np.testing.assert_allclose(c[: n // 2], want[: n // 2], rtol=1e-12)
+    assert (c[: n // 2] < 1).sum() > n // 8
+    assert np.all(c[n // 2:] == 1.0)

@@ -31,6 +31,7 @@ NOALLOC_MAX_PARTICLES = 262144
 LAYOUT_AUTO, LAYOUT_244, LAYOUT_444 = 0, 1, 2
 MODEL_NONE, MODEL_NEOHOOKEAN_BORDEN, MODEL_STVK_HENCKY_ISOTROPIC, MODEL_FIXED_COROTATED = 0, 1, 2, 3
 PLASTIC_NONE, PLASTIC_VON_MISES = 0, 1
+DAMAGE_NONE, DAMAGE_RANKINE = 0, 1
 MINRES, CG = 0, 1
 HALF_SPACE, SPHERE, BOX = 0, 1, 2
 STICKY, SLIP, SEPARATE, GHOST = 1, 2, 3, 4
@@ -122,6 +123,8 @@ _SIGS = {
     "add_fbased_force": (C.c_int, [C.c_void_p, C.c_int64, C.c_int64, C.c_int32, C.c_double, C.c_double]),
     "set_lame": (C.c_int, [C.c_void_p, C.c_int64, C.c_int64, c_double_p, c_double_p]),
     "add_plasticity": (C.c_int, [C.c_void_p, C.c_int64, C.c_int64, C.c_int32, C.c_double, C.c_double, C.c_double]),
+    "add_damage": (C.c_int, [C.c_void_p, C.c_int64, C.c_int64, C.c_int32, C.c_double, C.c_double]),
+    "get_damage": (C.c_int, [C.c_void_p, c_double_p]),
     "add_collision_object": (C.c_int, [C.c_void_p, C.POINTER(Collider), c_int32_p]),
     "set_collision_object": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(Collider)]),
     "get_particles": (C.c_int, [C.c_void_p, c_double_p, c_double_p, c_double_p, c_double_p]),

@@ -75,6 +75,10 @@ int upload(Ctx* ctx)
         hpd[PD_XI * cap + i] = ctx->hxi[i];
         hpd[PD_FS * cap + i] = ctx->hfs[i];
         for (int d = 0; d < 3; ++d) hpd[(PD_CRACK + d) * cap + i] = ctx->hcrack[3 * i + d];
+        hpd[PD_PF_C * cap + i] = ctx->hpfc[i];
+        hpd[PD_PF_K * cap + i] = ctx->hpfk[i];
+        hpd[PD_SIGMA_F * cap + i] = ctx->hsigf[i];
+        hpi[PI_DAMAGE * cap + i] = ctx->hdamage[i];
         hpi[PI_KIND * cap + i] = ctx->hkind[i];
         hpi[PI_PKIND * cap + i] = ctx->hpkind[i];
         hpi[PI_BROKEN * cap + i] = ctx->hbroken[i];
@@ -84,6 +88,8 @@ int upload(Ctx* ctx)
     ZMPM_CUDA(cudaMemcpy(ctx->pd.p, hpd.data(), hpd.size() * sizeof(double), cudaMemcpyHostToDevice));
     ZMPM_CUDA(cudaMemcpy(ctx->pi.p, hpi.data(), hpi.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
     ZMPM_CUDA(cudaMemcpy(ctx->slot_of_id.p, sid.data(), sid.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
+    ctx->has_damage = false;
+    for (int64_t i = 0; i < P; ++i) ctx->has_damage |= ctx->hdamage[i] != ZMPM_DAMAGE_NONE;
     ctx->uploaded = true;
     ctx->binned = false;
     ctx->implicit_ready = false;
@@ -120,6 +126,10 @@ int download(Ctx* ctx)
         ctx->hys[i] = hpd[PD_YS * cap + s];
         ctx->hxi[i] = hpd[PD_XI * cap + s];
         ctx->hfs[i] = hpd[PD_FS * cap + s];
+        ctx->hpfc[i] = hpd[PD_PF_C * cap + s];
+        ctx->hpfk[i] = hpd[PD_PF_K * cap + s];
+        ctx->hsigf[i] = hpd[PD_SIGMA_F * cap + s];
+        ctx->hdamage[i] = (uint8_t)hpi[PI_DAMAGE * cap + s];
         ctx->hkind[i] = (uint8_t)hpi[PI_KIND * cap + s];
         ctx->hpkind[i] = (uint8_t)hpi[PI_PKIND * cap + s];
         ctx->hbroken[i] = hpi[PI_BROKEN * cap + s];
@@ -439,6 +449,10 @@ int zmpm_add_particles(zmpm_ctx* ctx, int64_t n, const double* x, const double* 
         ctx->hys.push_back(0);
         ctx->hxi.push_back(0);
         ctx->hfs.push_back(0);
+        ctx->hpfc.push_back(1.0);
+        ctx->hpfk.push_back(0.001);
+        ctx->hsigf.push_back(0.0);
+        ctx->hdamage.push_back(ZMPM_DAMAGE_NONE);
         ctx->hkind.push_back(ZMPM_MODEL_NONE);
         ctx->hpkind.push_back(ZMPM_PLASTIC_NONE);
         ctx->hbroken.push_back(0);
@@ -494,6 +508,32 @@ int zmpm_add_plasticity(zmpm_ctx* ctx, int64_t lo, int64_t hi, int32_t kind, dou
         ctx->hxi[i] = xi;
         ctx->hfs[i] = fs;
     }
+    return ZMPM_OK;
+}
+
+int zmpm_add_damage(zmpm_ctx* ctx, int64_t lo, int64_t hi, int32_t kind, double sigma_f, double residual_phase)
+{
+    if (!ctx || lo < 0 || hi > ctx->P || lo > hi) return ZMPM_BAD_ARG;
+    if (kind != ZMPM_DAMAGE_NONE && kind != ZMPM_DAMAGE_RANKINE) return ZMPM_BAD_ARG;
+    cudaSetDevice(ctx->device);
+    int rc = begin_edit(ctx);
+    if (rc) return rc;
+    for (int64_t i = lo; i < hi; ++i) {
+        ctx->hdamage[i] = (uint8_t)kind;
+        ctx->hsigf[i] = sigma_f;
+        ctx->hpfk[i] = residual_phase;
+        ctx->hpfc[i] = 1.0;
+    }
+    return ZMPM_OK;
+}
+
+int zmpm_get_damage(zmpm_ctx* ctx, double* c)
+{
+    if (!ctx || !c) return ZMPM_BAD_ARG;
+    cudaSetDevice(ctx->device);
+    int rc = download(ctx);
+    if (rc) return rc;
+    for (int64_t i = 0; i < ctx->P; ++i) c[i] = ctx->hpfc[i];
     return ZMPM_OK;
 }
 

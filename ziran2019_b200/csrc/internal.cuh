@@ -83,8 +83,8 @@ enum MinresSlot { MR_GC0, MR_GS0, MR_GC1, MR_GS1, MR_GC2, MR_GS2, MR_RHS0, MR_RH
 
 // Field indices of the particle pools.
 enum PdField { PD_X = 0, PD_V = 3, PD_C = 6, PD_F = 15, PD_M = 24, PD_VOL = 25, PD_MU = 26, PD_LAM = 27, PD_KAPPA = 28,
-    PD_G = 29, PD_YS = 30, PD_XI = 31, PD_FS = 32, PD_CRACK = 33, PD_FIELDS = 36 };
-enum PiField { PI_KIND = 0, PI_PKIND = 1, PI_BROKEN = 2, PI_ID = 3, PI_FIELDS = 4 };
+    PD_G = 29, PD_YS = 30, PD_XI = 31, PD_FS = 32, PD_CRACK = 33, PD_PF_C = 36, PD_PF_K = 37, PD_SIGMA_F = 38, PD_FIELDS = 39 };
+enum PiField { PI_KIND = 0, PI_PKIND = 1, PI_BROKEN = 2, PI_ID = 3, PI_DAMAGE = 4, PI_FIELDS = 5 };
 
 // Reduction slots: per-CTA partial sums written by node kernels.
 constexpr int RED_MAX_CTAS = 1024;
@@ -109,9 +109,10 @@ struct Ctx {
     // host copy of the scene until the first upload
     int64_t P = 0;
     bool uploaded = false;
-    std::vector<double> hx, hv, hC, hF, hcrack, hm, hvol, hmu, hlam, hkappa, hg, hys, hxi, hfs;
-    std::vector<uint8_t> hkind, hpkind;
+    std::vector<double> hx, hv, hC, hF, hcrack, hm, hvol, hmu, hlam, hkappa, hg, hys, hxi, hfs, hpfc, hpfk, hsigf;
+    std::vector<uint8_t> hkind, hpkind, hdamage;
     std::vector<int32_t> hbroken;
+    bool has_damage = false;
     std::vector<zmpm_collider> colliders;
 
     // particles in slot order, structure of arrays (capacity Pcap).  The
@@ -180,6 +181,7 @@ int upload_colliders(Ctx* ctx, double time);
 int launch_update(Ctx* ctx);                           // G2P(vn+dv) -> stress -> force P2G
 int launch_residual(Ctx* ctx);                         // r = dt m g + dt f - m dv (projected), norm partials
 int launch_hvp(Ctx* ctx, const double* x, double* out, bool fp32); // out += dt^2 K x (no inertia)
+int launch_damage(Ctx* ctx);                           // Rankine damage after P2G
 int finalize_multiply(Ctx* ctx, const double* x, double* q); // q = project(m x + q)
 int ensure_node_buffers(Ctx* ctx);
 int compute_node_indices(Ctx* ctx);                    // getNumNodes numbering (hooks)

@@ -694,6 +694,8 @@ int run_p2g(Ctx* ctx)
     ZMPM_CUDA(cudaMemsetAsync(ctx->kv[9].p, 0, 3 * nn * sizeof(double), st)); // Hessian accumulator
     rc = launch_p2g(ctx);
     if (rc) return rc;
+    rc = launch_damage(ctx); // the fracture hook runs after particlesToGrid
+    if (rc) return rc;
     rc = upload_colliders(ctx, ctx->time);
     if (rc) return rc;
     NodeGeom ng = node_geom(ctx);

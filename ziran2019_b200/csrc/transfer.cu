@@ -273,6 +273,74 @@ __global__ void __launch_bounds__(XF_THREADS) k_p2g(const int32_t* __restrict__ 
     flush_window<4, 1, NPB>(acc, nbr, gm, gmv);
 }
 
+// -------------------------------------------------------------- damage -----
+// Largest eigenvalue of a symmetric 3x3 matrix by the trigonometric solution
+// of the characteristic cubic (O. K. Smith, "Eigenvalues of a symmetric 3x3
+// matrix", CACM 4(4), 1961).
+__device__ __forceinline__ double sym3_max_eig(const M3<double>& A)
+{
+    const double p1 = A(0, 1) * A(0, 1) + A(0, 2) * A(0, 2) + A(1, 2) * A(1, 2);
+    const double q = (A(0, 0) + A(1, 1) + A(2, 2)) / 3.0;
+    const double a = A(0, 0) - q, b = A(1, 1) - q, c = A(2, 2) - q;
+    const double p2 = a * a + b * b + c * c + 2.0 * p1;
+    if (p2 == 0.0) return q;
+    const double p = sqrt(p2 / 6.0);
+    M3<double> B = A;
+    B(0, 0) = a;
+    B(1, 1) = b;
+    B(2, 2) = c;
+#pragma unroll
+    for (int i = 0; i < 9; ++i) B.a[i] /= p;
+    double r = m3_det(B) / 2.0;
+    r = r < -1.0 ? -1.0 : (r > 1.0 ? 1.0 : r);
+    const double phi = acos(r) / 3.0;
+    return q + 2.0 * p * cos(phi);
+}
+
+// FractureSimulation::solvePhaseFieldSystemNaive (FractureSimulation.h:509-554)
+// for particles with Rankine damage and NeoHookeanBorden: Cauchy stress of the
+// undegraded (g = 1) Kirchhoff stress, c <- min(c, sigma_F / sigma_max) when
+// sigma_max > sigma_F, g = c^2 (1 - k) + k.
+__global__ void k_rankine(double* __restrict__ pd, const int32_t* __restrict__ pi, int64_t cap, int64_t P)
+{
+    const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= P) return;
+    if (pi[PI_DAMAGE * cap + s] != ZMPM_DAMAGE_RANKINE || pi[PI_KIND * cap + s] != ZMPM_MODEL_NEOHOOKEAN_BORDEN) return;
+    M3<double> F;
+#pragma unroll
+    for (int q = 0; q < 9; ++q) F.a[q] = pd[(PD_F + q) * cap + s];
+    const double J = m3_det(F);
+    const double mu = pd[PD_MU * cap + s], kappa = pd[PD_KAPPA * cap + s];
+    // NeoHookeanBorden::kirchhoff with g = 1 (NeoHookeanBorden.cpp:67-83)
+    M3<double> B = m3_mulT(F, F);
+    const double tr = B(0, 0) + B(1, 1) + B(2, 2);
+    const double sdev = mu * pow(J, -2.0 / 3.0);
+    const double vol = J * (kappa / 2 * (J - 1 / J));
+    M3<double> cauchy;
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            const double dv = (i == j) ? B(i, j) - 1.0 / 3.0 * tr : B(i, j);
+            cauchy(i, j) = ((i == j) ? sdev * dv + vol : sdev * dv) / J;
+        }
+    const double sigma_max = sym3_max_eig(cauchy);
+    const double sigma_f = pd[PD_SIGMA_F * cap + s];
+    double c = pd[PD_PF_C * cap + s];
+    const double k = pd[PD_PF_K * cap + s];
+    if (sigma_max > sigma_f) c = fmin(c, sigma_f / sigma_max);
+    pd[PD_PF_C * cap + s] = c;
+    pd[PD_G * cap + s] = c * c * (1 - k) + k;
+}
+
+int launch_damage(Ctx* ctx)
+{
+    if (!ctx->has_damage || ctx->P == 0) return ZMPM_OK;
+    k_rankine<<<(unsigned)((ctx->P + 255) / 256), 256, 0, ctx->stream>>>(ctx->pd.as<double>(), ctx->pi.as<int32_t>(), ctx->Pcap, ctx->P);
+    ++g_kernel_launches;
+    return ZMPM_OK;
+}
+
 // --------------------------------------------------------------- update ----
 // Two kernels per Newton iteration (MpmForceBase::updatePositionBasedState then
 // rasterizeForceToTVStack, MpmForceBase.cpp:306-344, 102-152):

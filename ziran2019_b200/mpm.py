@@ -169,6 +169,11 @@ class MpmParticleHandle:
         lam = np.ascontiguousarray(lam, dtype=np.float64)
         self.sim._call("set_lame", self.lower, self.upper, ptr(mu), ptr(lam))
 
+    def addRankineDamage(self, sigma_f, residual_phase=0.001):
+        """Phase field + Rankine damage (addFBasedMpmForceWithPhaseField with
+        FractureSimulation::useNaiveDamage and sigmaF); needs NeoHookeanBorden."""
+        self.sim._call("add_damage", self.lower, self.upper, abi.DAMAGE_RANKINE, float(sigma_f), float(residual_phase))
+
     def addPlasticity(self, model, plasticity):
         del model  # the model is the one attached with addFBasedMpmForce
         self.sim._call("add_plasticity", self.lower, self.upper, plasticity.kind,
@@ -300,6 +305,11 @@ class MpmSimulation:
         n = self.count
         keep = [p(X, (n, 3)), p(V, (n, 3)), p(C, (n, 3, 3)), p(F, (n, 3, 3))]
         self._call("set_particles", *[k[1] for k in keep])
+
+    def getDamage(self):
+        c = np.empty(self.count)
+        self._call("get_damage", ptr(c))
+        return c
 
     def getPlasticState(self):
         n = self.count
