@@ -95,6 +95,12 @@ enum zmpm_damage {
 /* Krylov solver of the Newton step (BackwardEuler.h:82-98). */
 enum zmpm_linear_solver { ZMPM_MINRES = 0, ZMPM_CG = 1 };
 
+/* Implicit integrator of a substep.  NEWTON: MpmSimulationBase::backwardEulerStep
+   (MpmSimulationBase.cpp:610-657).  ADMM: AdmmSimulation::admmStep
+   (Projects/admm/AdmmSimulationFoam.h:766-801), the local (per-particle F),
+   global (MINRES on the grid) and dual steps of "Silly Rubber". */
+enum zmpm_integrator { ZMPM_NEWTON = 0, ZMPM_ADMM = 1 };
+
 /* Collision objects (AnalyticCollisionObject, CollisionObject.h:42-195). */
 enum zmpm_collider_shape { ZMPM_HALF_SPACE = 0, ZMPM_SPHERE = 1, ZMPM_BOX = 2 };
 enum zmpm_collider_type { ZMPM_STICKY = 1, ZMPM_SLIP = 2, ZMPM_SEPARATE = 3, ZMPM_GHOST = 4 };
@@ -121,6 +127,14 @@ typedef struct zmpm_solver {
     int32_t pad0;
     double krylov_tolerance;        /* absolute; MINRES default 1 (BackwardEuler.h:62) */
     double linear_solve_tolerance_scale; /* NewtonsMethod.h:38, default 1 */
+    /* ADMM (integrator = ZMPM_ADMM); AdmmSimulationFoam.h:47-70 */
+    int32_t integrator;             /* zmpm_integrator, default NEWTON */
+    int32_t admm_iterations;        /* admm_max_iterations (class default 100; scenes 15-40) */
+    double admm_rho_scale;          /* rho_scale, default 0.5 */
+    double admm_local_tolerance;    /* local_tolerance of the per-particle Newton, default 1e-8 */
+    double admm_global_tolerance;   /* global_tolerance: absolute MINRES tolerance, default 1e-6 */
+    int32_t admm_global_max_iterations; /* global_max_iteration, default 10000 */
+    int32_t pad1;
 } zmpm_solver;
 
 typedef struct zmpm_collider {
@@ -212,6 +226,22 @@ int zmpm_add_plasticity(zmpm_ctx* ctx, int64_t lower, int64_t upper, int32_t kin
 int zmpm_add_damage(zmpm_ctx* ctx, int64_t lower, int64_t upper, int32_t kind, double sigma_f, double residual_phase);
 /* Phase-field value c per particle (1 undamaged, 0 fully damaged). */
 int zmpm_get_damage(zmpm_ctx* ctx, double* c);
+
+/* MpmParticleHandleBase::addFElasticNonequilibratedBasedMpmForce
+   (MpmParticleHandleBase.cpp:468-478) with the reference's only instantiated
+   model, StvkWithHencky(E, nu) (StvkWithHencky.cpp:10-20): a second elastic
+   strain Fe ("Fe_Nonequilibrated", starts at I) that G2P advects and relaxes by
+   the viscous return map of FElasticNonequilibratedBasedMpmForceHelper::
+   evolveStrain (FElasticNonequilibratedBasedMpmForceHelper.h:62-87).  Its
+   energy enters the ADMM local step (AdmmSimulationFoam.h:575-612).  Every
+   particle in [lower, upper) must already carry StvkWithHenckyIsotropic;
+   StvkWithHencky has no stress differential (StvkWithHencky.cpp:185-190), so a
+   Newton substep over such particles returns ZMPM_BAD_ARG. */
+int zmpm_add_viscoelastic(zmpm_ctx* ctx, int64_t lower, int64_t upper, double youngs_modulus, double poisson_ratio,
+    double viscosity_d, double viscosity_v);
+/* Fe per particle, [P][3][3] in particle-index order (I where none is attached). */
+int zmpm_get_viscoelastic_strain(zmpm_ctx* ctx, double* Fe);
+int zmpm_set_viscoelastic_strain(zmpm_ctx* ctx, const double* Fe);
 
 /* MpmSimulationBase::addCollisionObject (MpmSimulationBase.cpp:80-84). */
 int zmpm_add_collision_object(zmpm_ctx* ctx, const zmpm_collider* obj, int32_t* id);

@@ -847,6 +847,264 @@ static void rankineUpdate(Model<T>& c, Damage<T>& d, const M3<T>& F)
     c.g = newC * newC * (1 - d.k) + d.k;
 }
 
+// ------------------------------------------------------- viscoelastic --
+// Second elastic strain Fe ("Fe_Nonequilibrated") with the reference's only
+// instantiated model StvkWithHencky (MpmParticlesHandle3d.cpp:9).
+template <class T>
+struct Visco {
+    int32_t on = 0;
+    T mu = 0, lambda = 0, vd = 1, vv = 1; // StvkWithHencky(E, nu), viscosity_d, viscosity_v
+};
+
+// FElasticNonequilibratedBasedMpmForceHelper::evolveStrain,
+// FElasticNonequilibratedBasedMpmForceHelper.h:62-87: backward-Euler relaxation
+// of the Hencky strain of Fe (deviatoric rate alpha, volumetric rate alpha + 3 beta).
+template <class T>
+static void viscousCoefficients(const Visco<T>& v, T dt, T& a, T& b)
+{
+    T alpha = T(2.0) * v.mu / v.vd;
+    T beta = T(2.0) * (T(2.0) * v.mu + v.lambda * 3) / (T(9.0) * v.vv) - T(2.0) * v.mu / (v.vd * 3);
+    a = T(1.0) / (T(1.0) + dt * alpha);
+    b = dt * beta / (T(1.0) + dt * (alpha + 3 * beta));
+}
+
+template <class T>
+static void viscousReturn(const Visco<T>& v, T dt, M3<T>& Fe)
+{
+    M3<T> U, V;
+    T sigma[3];
+    svd3(Fe, U, sigma, V);
+    T a, b;
+    viscousCoefficients(v, dt, a, b);
+    T et[3];
+    for (int d = 0; d < 3; ++d) et[d] = std::log(std::fabs(sigma[d]));
+    // `epsilon_trial.trace()` of a 3-vector: Eigen's trace of a 3x1 matrix is
+    // its single diagonal coefficient, epsilon_trial(0)
+    T tr = et[0];
+    T ex[3];
+    for (int d = 0; d < 3; ++d) ex[d] = std::exp(a * (et[d] - b * tr));
+    Fe = udiagvt(U, ex, V);
+}
+
+// ------------------------------------------------------------------ ADMM --
+// Diagonal (singular-value space) derivatives of psi = mu |log S|^2 +
+// lambda/2 tr(log S)^2, StvkWithHenckyIsotropic.h:218-269 (identical in
+// StvkWithHencky.cpp:154-183).
+template <class T>
+static void henckyDiagonal(T mu, T lambda, const T s[3], T dE[3], T ddE[3][3])
+{
+    T L[3];
+    for (int d = 0; d < 3; ++d) L[d] = std::log(std::fabs(s[d]));
+    T sum_log = L[0] + L[1] + L[2];
+    T g = 2 * mu + lambda;
+    for (int d = 0; d < 3; ++d) dE[d] = (2 * mu * L[d] + lambda * sum_log) / s[d];
+    ddE[0][0] = (g * (1 - L[0]) - lambda * (L[1] + L[2])) / (s[0] * s[0]);
+    ddE[1][1] = (g * (1 - L[1]) - lambda * (L[0] + L[2])) / (s[1] * s[1]);
+    ddE[2][2] = (g * (1 - L[2]) - lambda * (L[0] + L[1])) / (s[2] * s[2]);
+    ddE[0][1] = ddE[1][0] = lambda / (s[0] * s[1]);
+    ddE[0][2] = ddE[2][0] = lambda / (s[0] * s[2]);
+    ddE[1][2] = ddE[2][1] = lambda / (s[1] * s[2]);
+}
+
+// Eigenvalues of a symmetric 3x3 matrix by cyclic Jacobi rotations.
+template <class T>
+static void sym3EigJacobi(M3<T> A, T ev[3])
+{
+    for (int sweep = 0; sweep < 50; ++sweep) {
+        T off = A.a[0][1] * A.a[0][1] + A.a[0][2] * A.a[0][2] + A.a[1][2] * A.a[1][2];
+        if (off == 0) break;
+        for (int p = 0; p < 2; ++p)
+            for (int q = p + 1; q < 3; ++q) {
+                if (A.a[p][q] == 0) continue;
+                T theta = (A.a[q][q] - A.a[p][p]) / (2 * A.a[p][q]);
+                T t = (theta >= 0 ? T(1) : T(-1)) / (std::fabs(theta) + std::sqrt(theta * theta + 1));
+                T c = 1 / std::sqrt(t * t + 1), s = t * c;
+                for (int k = 0; k < 3; ++k) {
+                    T akp = A.a[k][p], akq = A.a[k][q];
+                    A.a[k][p] = c * akp - s * akq;
+                    A.a[k][q] = s * akp + c * akq;
+                }
+                for (int k = 0; k < 3; ++k) {
+                    T apk = A.a[p][k], aqk = A.a[q][k];
+                    A.a[p][k] = c * apk - s * aqk;
+                    A.a[q][k] = s * apk + c * aqk;
+                }
+            }
+    }
+    for (int d = 0; d < 3; ++d) ev[d] = A.a[d][d];
+}
+
+// Squared Frobenius norms of makePD / makePD2D (AdmmFormula.h:12-35): the
+// eigenvalues clamped at zero.
+template <class T>
+static T makePDNorm2(const M3<T>& A)
+{
+    T ev[3];
+    sym3EigJacobi(A, ev);
+    T s = 0;
+    for (int d = 0; d < 3; ++d) s += ev[d] > 0 ? ev[d] * ev[d] : T(0);
+    return s;
+}
+template <class T>
+static T makePD2DNorm2(T a, T b, T d)
+{
+    T m = (a + d) / 2, r = std::sqrt((a - d) * (a - d) / 4 + b * b);
+    T l0 = m - r, l1 = m + r;
+    return (l0 > 0 ? l0 * l0 : T(0)) + (l1 > 0 ? l1 * l1 : T(0));
+}
+
+// StvkWithHenckyIsotropic::Bij (3D), StvkWithHenckyIsotropic.h:180-216:
+// [[P+M, M-P], [M-P, P+M]] with P = B_Pij, M = B_Mij.
+template <class T>
+static void henckyBij(T mu, T lambda, const T s[3], int i, int j, T clamp, T& P, T& M)
+{
+    auto clampMag = [&](T x) {
+        T mag = x > 0 ? x : -x;
+        T sign = x > 0 ? T(1) : T(-1);
+        return (mag > clamp ? mag : clamp) * sign;
+    };
+    T dE[3], ddE[3][3];
+    henckyDiagonal(mu, lambda, s, dE, ddE);
+    P = T(0.5) * (dE[i] + dE[j]) / clampMag(s[i] + s[j]);
+    T L[3];
+    for (int d = 0; d < 3; ++d) L[d] = std::log(std::fabs(s[d]));
+    T sum_log = L[0] + L[1] + L[2];
+    M = T(-0.5) * (lambda * sum_log + 2 * mu * diff_interlock_log_over_diff(s[i], s[j], L[j], T(1e-8))) / (s[i] * s[j]);
+}
+
+// VonMisesStvkHencky::projectSigma / projectSigmaAndDerivative,
+// PlasticityApplier.cpp:526-602.
+template <class T>
+static bool vmProjectSigma(T mu, T ys, const T s[3], T out[3], T D[3][3])
+{
+    T eps[3];
+    for (int d = 0; d < 3; ++d) eps[d] = std::log(std::max(s[d], T(1e-4)));
+    T tr = eps[0] + eps[1] + eps[2];
+    T hat[3];
+    for (int d = 0; d < 3; ++d) hat[d] = eps[d] - (tr / T(3)) * T(1);
+    T hat_norm = std::sqrt(hat[0] * hat[0] + hat[1] * hat[1] + hat[2] * hat[2]);
+    T delta_gamma = hat_norm - ys / (2 * mu);
+    if (delta_gamma <= 0) {
+        for (int r = 0; r < 3; ++r) {
+            out[r] = s[r];
+            for (int c = 0; c < 3; ++c) D[r][c] = r == c ? T(1) : T(0);
+        }
+        return false;
+    }
+    T w[3];
+    for (int d = 0; d < 3; ++d) w[d] = 1 / s[d];
+    T sv[3];
+    for (int d = 0; d < 3; ++d) sv[d] = eps[d] - tr / 3 * T(1);
+    T snorm = std::sqrt(sv[0] * sv[0] + sv[1] * sv[1] + sv[2] * sv[2]);
+    T sh[3];
+    for (int d = 0; d < 3; ++d) sh[d] = sv[d] / snorm;
+    for (int d = 0; d < 3; ++d) out[d] = std::exp(eps[d] - (delta_gamma / hat_norm) * hat[d]);
+    T k1 = T(1) - ys / (2 * mu * snorm), k2 = ys / (2 * mu * snorm);
+    for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c) {
+            T Iw = r == c ? w[c] : T(0);
+            D[r][c] = out[r] * (Iw - k1 * (Iw - w[c] / T(3)) - k2 * sh[r] * sh[c] * w[c]);
+        }
+    return true;
+}
+
+// The viscous map in singular-value space and its derivative,
+// AdmmSimulationFoam.h:583-595.
+template <class T>
+static void viscousSigma(const Visco<T>& v, T dt, const T zi[3], T zp[3], T D[3][3])
+{
+    T a, b;
+    viscousCoefficients(v, dt, a, b);
+    T et[3];
+    for (int d = 0; d < 3; ++d) et[d] = std::log(std::fabs(zi[d]));
+    T tr = et[0]; // epsilon_trial.trace() of a 3-vector, as in viscousReturn
+    for (int d = 0; d < 3; ++d) zp[d] = std::exp(a * (et[d] - b * tr));
+    for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c) D[r][c] = zp[r] * a * ((r == c ? 1 / zi[c] : T(0)) - b * (1 / zi[c]));
+}
+
+template <class T>
+static M3<T> inverse3(const M3<T>& A)
+{
+    M3<T> C = cofactor(A);
+    T det = A.a[0][0] * C.a[0][0] + A.a[0][1] * C.a[0][1] + A.a[0][2] * C.a[0][2];
+    M3<T> inv;
+    for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c) inv.a[r][c] = C.a[c][r] / det;
+    return inv;
+}
+
+// One strain of AdmmSimulation::FStepSolve (AdmmSimulationFoam.h:507-615):
+// SVD of the target FDb, then a Newton solve in singular values for
+// argmin vol psi(P(z)) + coeff/2 |z - sigma|^2 starting from the current F.
+// mode 0: elastic, 1: von Mises projection, 2: viscous map.
+template <class T>
+static M3<T> admmLocalSolve(const M3<T>& FDb, const M3<T>& Fcur, T vol, T coeff, T mu, T lambda, int mode, T ys, const Visco<T>& vis,
+    T dt, int iters, T tol)
+{
+    M3<T> U, V;
+    T sigma[3];
+    svd3(FDb, U, sigma, V);
+    M3<T> W = Tmul(U, mul(Fcur, V));
+    T zi[3] = { W.a[0][0], W.a[1][1], W.a[2][2] };
+    for (int j = 0; j < iters; ++j) {
+        T zp[3], D[3][3];
+        if (mode == 1)
+            vmProjectSigma(mu, ys, zi, zp, D);
+        else if (mode == 2)
+            viscousSigma(vis, dt, zi, zp, D);
+        else
+            for (int r = 0; r < 3; ++r) {
+                zp[r] = zi[r];
+                for (int c = 0; c < 3; ++c) D[r][c] = r == c ? T(1) : T(0);
+            }
+        T dE[3], ddE[3][3];
+        henckyDiagonal(mu, lambda, zp, dE, ddE);
+        T g[3];
+        for (int d = 0; d < 3; ++d) g[d] = vol * dE[d] + coeff * (zi[d] - sigma[d]);
+        M3<T> Pm;
+        for (int r = 0; r < 3; ++r)
+            for (int c = 0; c < 3; ++c) {
+                T acc = ddE[r][0] * D[0][c] + ddE[r][1] * D[1][c] + ddE[r][2] * D[2][c];
+                Pm.a[r][c] = vol * acc + (r == c ? coeff : T(0));
+            }
+        M3<T> inv = inverse3(Pm);
+        T step[3];
+        for (int r = 0; r < 3; ++r) step[r] = inv.a[r][0] * (-g[0]) + inv.a[r][1] * (-g[1]) + inv.a[r][2] * (-g[2]);
+        for (int d = 0; d < 3; ++d) zi[d] += step[d];
+        if (std::sqrt(step[0] * step[0] + step[1] * step[1] + step[2] * step[2]) < tol) break;
+    }
+    return udiagvt(U, zi, V);
+}
+
+// initOmega for one strain, AdmmSimulationFoam.h:236-270:
+// omega = sqrt(vol sqrt(|makePD(d2E)|^2 + sum_ij |makePD2D(B_ij)|^2)).
+template <class T>
+static T admmOmega(const M3<T>& Fa, T vol, T mu, T lambda, bool vm, T ys)
+{
+    M3<T> U, V;
+    T sigma[3];
+    svd3(Fa, U, sigma, V);
+    T dE[3], ddE[3][3];
+    henckyDiagonal(mu, lambda, sigma, dE, ddE);
+    M3<T> A;
+    for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c) A.a[r][c] = ddE[r][c];
+    T total = makePDNorm2(A);
+    if (vm) {
+        T sp[3], D[3][3];
+        vmProjectSigma(mu, ys, sigma, sp, D);
+        for (int d = 0; d < 3; ++d) sigma[d] = sp[d];
+    }
+    const int pairs[3][2] = { { 0, 1 }, { 0, 2 }, { 1, 2 } };
+    for (auto& pr : pairs) {
+        T P, M;
+        henckyBij(mu, lambda, sigma, pr[0], pr[1], T(1e-6), P, M);
+        total += makePD2DNorm2(P + M, M - P, P + M);
+    }
+    return std::sqrt(vol * std::sqrt(total));
+}
+
 // ------------------------------------------------------------- colliders --
 template <class T>
 struct Collider {
@@ -944,6 +1202,24 @@ struct Collider {
         N[imax] = xp[imax] >= 0 ? T(1) : T(-1);
         return true;
     }
+    // AnalyticCollisionObject::getBoundaryVelocityAndNormal, CollisionObject.cpp:313-338
+    bool boundaryVelocityAndNormal(const T x[3], T vb[3], T n[3]) const
+    {
+        if (d.type == ZMPM_GHOST) return false;
+        T xb[3] = { x[0] - b[0], x[1] - b[1], x[2] - b[2] };
+        T one_over_s = 1 / s;
+        T X[3];
+        for (int i = 0; i < 3; ++i) X[i] = (R[0][i] * xb[0] + R[1][i] * xb[1] + R[2][i] * xb[2]) * one_over_s;
+        T N[3];
+        if (!queryInside(X, N)) return false;
+        vb[0] = omega[1] * xb[2] - omega[2] * xb[1];
+        vb[1] = omega[2] * xb[0] - omega[0] * xb[2];
+        vb[2] = omega[0] * xb[1] - omega[1] * xb[0];
+        for (int i = 0; i < 3; ++i) vb[i] += (dsdt * one_over_s) * xb[i] + dbdt[i];
+        for (int i = 0; i < 3; ++i) n[i] = R[i][0] * N[0] + R[i][1] * N[1] + R[i][2] * N[2];
+        return true;
+    }
+
     // AnalyticCollisionObject::detectAndResolveCollision, CollisionObject.cpp:340-400
     bool detectAndResolve(const T x[3], T v[3], T n[3]) const
     {
@@ -1067,6 +1343,9 @@ struct Sim {
     std::vector<Model<T>> model;
     std::vector<Plastic<T>> plastic;
     std::vector<Damage<T>> damage;
+    std::vector<Visco<T>> visco;
+    std::vector<T> Fe;                                   // Fe_Nonequilibrated [P][9]
+    std::vector<T> admm_y, admm_omega, admm_last_dv;     // ADMM state carried across substeps: [P][18], [P][2], [P][3]
     std::vector<Scratch<T>> scratch;
     std::vector<M3<T>> gradV, stress;
     std::vector<Collider<T>> colliders;
@@ -1435,8 +1714,13 @@ struct Sim {
 
     // multiply, BackwardEuler.h:322-351: b = M x + dt^2 sum dS grad w
     int64_t hvp_count = 0;
+    bool admm_mode = false;
     void multiply(const std::vector<T>& x, std::vector<T>& b)
     {
+        if (admm_mode) {
+            admmMultiply(x, b);
+            return;
+        }
         hvp_count++;
         b.assign(3 * N, 0);
         T scale = -(dt * dt);
@@ -1460,18 +1744,25 @@ struct Sim {
     }
     void precondition(const std::vector<T>& in, std::vector<T>& out) const
     {
+        const std::vector<T>& pre = admm_mode ? admm_pre : mvec;
         out.resize(3 * N);
         for (int64_t i = 0; i < N; ++i)
-            for (int d = 0; d < 3; ++d) out[3 * i + d] = in[3 * i + d] / mvec[i];
+            for (int d = 0; d < 3; ++d) out[3 * i + d] = in[3 * i + d] / pre[i];
     }
 
-    // Minres::solve, Minres.h:69-149 (x starts at zero, so A x = 0 is not evaluated)
-    int minres(std::vector<T>& x, const std::vector<T>& b, T rel_tol, T abs_tol, int max_it)
+    // Minres::solve, Minres.h:69-149.  Newton's solves start from x = 0, so
+    // A x = 0 is not evaluated; `warm` starts from the given x (ADMM's dvStep).
+    int minres(std::vector<T>& x, const std::vector<T>& b, T rel_tol, T abs_tol, int max_it, bool warm = false)
     {
         std::vector<T> mk(3 * N, 0), mkm1(3 * N, 0), mkm2(3 * N, 0), z(3 * N, 0), qkm1(3 * N, 0), qk(3 * N, 0), qkp1;
         T g_c[3] = { 1, 1, 1 }, g_s[3] = { 0, 0, 0 }; // Gk, Gkm1, Gkm2
         T gamma = 0, delta = 0, epsilon = 0, beta_kp1 = 0, alpha_k = 0, beta_k = 0, tk = 0;
-        qkp1 = b;
+        if (warm) {
+            multiply(x, qkp1);
+            for (int64_t i = 0; i < 3 * N; ++i) qkp1[i] = b[i] - qkp1[i];
+        }
+        else
+            qkp1 = b;
         project(qkp1);
         precondition(qkp1, z);
         T rnorm = std::sqrt(dot(z, qkp1));
@@ -1605,6 +1896,319 @@ struct Sim {
         return false;
     }
 
+    // ------------------------------------------------------------ ADMM --
+    // AdmmSimulation (Projects/admm/AdmmSimulationFoam.h).  Strain slot 0 is F
+    // with the particle's Hencky model (and von Mises projection if it has
+    // one), slot 1 is Fe with its StvkWithHencky model (viscoelastic particles).
+    std::vector<T> admm_pre;              // preconditioner per node
+    std::vector<T> admm_val;              // assembled 125-entry stencil [N][125]
+    std::vector<int32_t> admm_idx;        // its column node ids
+    std::vector<M3<T>> admm_F[2];         // local variables F (AdmmSimulation::F)
+    std::vector<M3<T>> admm_gvn;          // grad vn at particles (for bFu)
+
+    bool isHencky(int64_t i) const { return model[i].kind == ZMPM_MODEL_STVK_HENCKY_ISOTROPIC; }
+    M3<T> strainN(int k, int64_t i) const { return k == 0 ? load9(Fn, i) : load9(Fe, i); }
+    T& omegaOf(int k, int64_t i) { return admm_omega[2 * i + k]; }
+    M3<T> yOf(int k, int64_t i) const
+    {
+        M3<T> m;
+        for (int q = 0; q < 9; ++q) m.a[q / 3][q % 3] = admm_y[18 * i + 9 * k + q];
+        return m;
+    }
+    void setY(int k, int64_t i, const M3<T>& m)
+    {
+        for (int q = 0; q < 9; ++q) admm_y[18 * i + 9 * k + q] = m.a[q / 3][q % 3];
+    }
+
+    // AnalyticCollisionObject::multiObjectCollisionWithFakeSeparate,
+    // CollisionObject.cpp:108-156: a SEPARATE object whose boundary the node
+    // already leaves does not collide.
+    static bool multiObjectCollisionFakeSeparate(const std::vector<Collider<T>>& objs, const T x[3], T v[3], M3<T>& K)
+    {
+        bool any = false;
+        int slip = 0;
+        K = M3<T>::zero();
+        for (const auto& o : objs) {
+            if (o.d.type == ZMPM_GHOST) continue;
+            T n[3] = { 0, 0, 0 };
+            T old[3] = { v[0], v[1], v[2] };
+            bool col = o.detectAndResolve(x, v, n);
+            if (col && o.d.type == ZMPM_SEPARATE) {
+                T vb[3] = { 0, 0, 0 }, nb[3] = { 0, 0, 0 };
+                o.boundaryVelocityAndNormal(x, vb, nb);
+                T dot = (old[0] - vb[0]) * nb[0] + (old[1] - vb[1]) * nb[1] + (old[2] - vb[2]) * nb[2];
+                if (dot > 0) {
+                    for (int d = 0; d < 3; ++d) v[d] = old[d];
+                    col = false;
+                }
+            }
+            any = col || any;
+            if (!col) continue;
+            if (o.d.type == ZMPM_STICKY) {
+                K = M3<T>::identity();
+                break;
+            }
+            for (int c = 0; c < slip; ++c) {
+                T dot = K.a[0][c] * n[0] + K.a[1][c] * n[1] + K.a[2][c] * n[2];
+                for (int i = 0; i < 3; ++i) n[i] -= dot * K.a[i][c];
+            }
+            T len = std::sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
+            if (len) {
+                for (int i = 0; i < 3; ++i) K.a[i][slip] = n[i] / len;
+                if (++slip == 3) break;
+            }
+        }
+        return any;
+    }
+
+    // updateCollisionNodes, AdmmSimulationFoam.h:276-293
+    void admmUpdateCollisionNodes()
+    {
+        collided.assign(N, 0);
+        proj.assign(N, M3<T>::identity());
+        iterateBlocks(true, [&](const int node[3], G& g) {
+            int64_t id = g.idx;
+            T vi[3], xi[3];
+            for (int d = 0; d < 3; ++d) {
+                vi[d] = dv[3 * id + d] + vn[3 * id + d];
+                xi[d] = node[d] * dx;
+            }
+            M3<T> K;
+            if (multiObjectCollisionFakeSeparate(colliders, xi, vi, K)) {
+                collided[id] = 1;
+                M3<T> Pm = M3<T>::identity();
+                M3<T> KK = mulT(K, K);
+                for (int r = 0; r < 3; ++r)
+                    for (int c = 0; c < 3; ++c) Pm.a[r][c] -= KK.a[r][c];
+                proj[id] = Pm;
+                for (int d = 0; d < 3; ++d) dv[3 * id + d] = vi[d] - vn[3 * id + d];
+            }
+        });
+    }
+
+    // initStep (AdmmSimulationFoam.h:297-403) and initMultiplierAndPreconditioner (:407-505)
+    void admmInit(T rho)
+    {
+        for (auto& c : colliders) c.update(time);
+        mvec.assign(N, 0);
+        vn.assign(3 * N, 0);
+        dv.assign(3 * N, 0);
+        iterateBlocks(true, [&](const int*, G& g) {
+            int64_t id = g.idx;
+            mvec[id] = g.m;
+            for (int d = 0; d < 3; ++d) vn[3 * id + d] = g.v[d];
+        });
+        Fn = F; // backupStrain
+        // dv from the previous substep's particle dv (:304-320)
+        std::vector<T> dvw(N, 0);
+        coloredGroups([&](int i) {
+            Spline<T> sp(&X[3 * i], dx);
+            iterateKernel(sp, base_offset[i], [&](const int*, T w, const T*, G& g) {
+                if (g.idx < 0) return;
+                for (int d = 0; d < 3; ++d) dv[3 * g.idx + d] += admm_last_dv[3 * i + d] * w;
+                dvw[g.idx] += w;
+            });
+        });
+        for (int64_t id = 0; id < N; ++id)
+            for (int d = 0; d < 3; ++d) dv[3 * id + d] = dv[3 * id + d] * dt / dvw[id];
+        admmUpdateCollisionNodes();
+        // initial local variables F = (I + dt grad(vn + dv)) Fn (:329-339)
+        std::vector<M3<T>> grad;
+        evalGradient(dv, true, grad);
+        evalGradient(std::vector<T>(3 * N, 0), true, admm_gvn);
+        for (int k = 0; k < 2; ++k) admm_F[k].assign(P, M3<T>::identity());
+#pragma omp parallel for schedule(static)
+        for (int64_t i = 0; i < P; ++i) {
+            for (int k = 0; k < 2; ++k) {
+                if (k == 1 && !visco[i].on) continue;
+                M3<T> Sn = strainN(k, i);
+                M3<T> Fa = Sn;
+                M3<T> t = mul(grad[i], Sn);
+                for (int r = 0; r < 3; ++r)
+                    for (int c = 0; c < 3; ++c) Fa.a[r][c] += dt * t.a[r][c];
+                admm_F[k][i] = Fa;
+            }
+            // initOmega (:222-274) and the rescaled dual variables (:355-371)
+            if (!isHencky(i)) continue;
+            T om0 = admm_omega[2 * i], om1 = admm_omega[2 * i + 1];
+            bool vm = plastic[i].kind == ZMPM_PLASTIC_VON_MISES;
+            admm_omega[2 * i] = admmOmega(admm_F[0][i], vol[i], model[i].mu, model[i].lambda, vm, plastic[i].yield_stress);
+            if (visco[i].on) admm_omega[2 * i + 1] = admmOmega(admm_F[1][i], vol[i], visco[i].mu, visco[i].lambda, false, T(0));
+            for (int q = 0; q < 9; ++q) {
+                admm_y[18 * i + q] = admm_y[18 * i + q] * om0 / admm_omega[2 * i];
+                admm_y[18 * i + 9 + q] = admm_y[18 * i + 9 + q] * om1 / admm_omega[2 * i + 1];
+            }
+        }
+        // assembled global matrix M + sum_p rho omega^2 dt^2 (Fn^T grad w)(Fn^T grad w)^T
+        // per node pair, and its diagonal as preconditioner
+        admm_val.assign((size_t)N * 125, 0);
+        admm_idx.assign((size_t)N * 125, 0);
+        admm_pre = mvec;
+        coloredGroups([&](int i) {
+            Spline<T> sp(&X[3 * i], dx);
+            int nodes[27][3], ids[27], cnt = 0;
+            T ftdw[2][27][3];
+            iterateKernel(sp, base_offset[i], [&](const int node[3], T, const T* dw, G& g) {
+                if (g.idx < 0) return;
+                for (int d = 0; d < 3; ++d) nodes[cnt][d] = node[d];
+                ids[cnt] = (int)g.idx;
+                for (int k = 0; k < 2; ++k) {
+                    if (k == 1 && !visco[i].on) continue;
+                    M3<T> Sn = strainN(k, i);
+                    for (int c = 0; c < 3; ++c) ftdw[k][cnt][c] = Sn.a[0][c] * dw[0] + Sn.a[1][c] * dw[1] + Sn.a[2][c] * dw[2];
+                }
+                ++cnt;
+            });
+            for (int k = 0; k < 2; ++k) {
+                if (k == 1 && !visco[i].on) continue;
+                T om = admm_omega[2 * i + k];
+                T coeff = rho * om * om * dt * dt;
+                for (int p = 0; p < cnt; ++p) {
+                    for (int q = 0; q < cnt; ++q) {
+                        int off = 25 * (nodes[q][0] - nodes[p][0] + 2) + 5 * (nodes[q][1] - nodes[p][1] + 2) + nodes[q][2] - nodes[p][2] + 2;
+                        size_t e = (size_t)ids[p] * 125 + off;
+                        admm_idx[e] = ids[q];
+                        admm_val[e] += coeff * (ftdw[k][p][0] * ftdw[k][q][0] + ftdw[k][p][1] * ftdw[k][q][1] + ftdw[k][p][2] * ftdw[k][q][2]);
+                    }
+                    admm_pre[ids[p]] += coeff * (ftdw[k][p][0] * ftdw[k][p][0] + ftdw[k][p][1] * ftdw[k][p][1] + ftdw[k][p][2] * ftdw[k][p][2]);
+                }
+            }
+        });
+    }
+
+    // GlobalSystem multiplier, AdmmSimulationFoam.h:127-143
+    void admmMultiply(const std::vector<T>& x, std::vector<T>& b)
+    {
+        hvp_count++;
+        b.assign(3 * N, 0);
+#pragma omp parallel for schedule(static)
+        for (int64_t n = 0; n < N; ++n) {
+            T r[3] = { mvec[n] * x[3 * n], mvec[n] * x[3 * n + 1], mvec[n] * x[3 * n + 2] };
+            const T* val = &admm_val[(size_t)n * 125];
+            const int32_t* idx = &admm_idx[(size_t)n * 125];
+            for (int k = 0; k < 125; ++k)
+                for (int d = 0; d < 3; ++d) r[d] += x[3 * idx[k] + d] * val[k];
+            for (int d = 0; d < 3; ++d) b[3 * n + d] = r[d];
+        }
+    }
+
+    // FStep + FStepSolve, AdmmSimulationFoam.h:507-636
+    void admmFStep(T rho, T local_tol)
+    {
+        std::vector<M3<T>> grad;
+        evalGradient(dv, true, grad);
+#pragma omp parallel for schedule(static)
+        for (int64_t i = 0; i < P; ++i) {
+            if (!isHencky(i)) continue;
+            for (int k = 0; k < 2; ++k) {
+                if (k == 1 && !visco[i].on) continue;
+                M3<T> Sn = strainN(k, i);
+                T om = admm_omega[2 * i + k];
+                M3<T> y = yOf(k, i);
+                M3<T> FDb = Sn;
+                M3<T> t = mul(grad[i], Sn);
+                for (int r = 0; r < 3; ++r)
+                    for (int c = 0; c < 3; ++c) FDb.a[r][c] = (Sn.a[r][c] + (-y.a[r][c] / (om * rho))) + dt * t.a[r][c];
+                T coeff = rho * om * om;
+                if (k == 0) {
+                    int mode = plastic[i].kind == ZMPM_PLASTIC_VON_MISES ? 1 : 0;
+                    admm_F[0][i] = admmLocalSolve(FDb, admm_F[0][i], vol[i], coeff, model[i].mu, model[i].lambda, mode,
+                        plastic[i].yield_stress, visco[i], dt, 5, local_tol);
+                }
+                else
+                    admm_F[1][i] = admmLocalSolve(FDb, admm_F[1][i], vol[i], coeff, visco[i].mu, visco[i].lambda, 2, T(0), visco[i], dt, 20,
+                        local_tol);
+            }
+        }
+    }
+
+    // dvStep, AdmmSimulationFoam.h:163-220: rhs = dt M g + sum_p dt rho omega^2
+    // bFu Fn^T grad w with bFu = F - Fn + y/(omega rho) - dt grad(vn) Fn; MINRES
+    // from the current dv.
+    int admmDvStep(T rho, T tol, T rel_tol, int max_it)
+    {
+        std::vector<T> rhs(3 * N);
+        for (int64_t n = 0; n < N; ++n)
+            for (int d = 0; d < 3; ++d) rhs[3 * n + d] = dt * mvec[n] * gravity[d];
+        std::vector<M3<T>> R(P);
+#pragma omp parallel for schedule(static)
+        for (int64_t i = 0; i < P; ++i) {
+            M3<T> acc = M3<T>::zero();
+            for (int k = 0; k < 2; ++k) {
+                if (k == 1 && !visco[i].on) continue;
+                M3<T> Sn = strainN(k, i);
+                T om = admm_omega[2 * i + k];
+                M3<T> y = yOf(k, i);
+                M3<T> t = mul(admm_gvn[i], Sn);
+                M3<T> bFu;
+                for (int r = 0; r < 3; ++r)
+                    for (int c = 0; c < 3; ++c)
+                        bFu.a[r][c] = admm_F[k][i].a[r][c] - Sn.a[r][c] + y.a[r][c] / (om * rho) - dt * t.a[r][c];
+                M3<T> Rk = mulT(scaled(bFu, dt * rho * om * om), Sn);
+                acc = add(acc, Rk);
+            }
+            R[i] = acc;
+        }
+        rasterize(T(-1), R, rhs);
+        admm_mode = true;
+        int k = minres(dv, rhs, rel_tol, tol, max_it, true);
+        admm_mode = false;
+        return k;
+    }
+
+    // uStep, AdmmSimulationFoam.h:638-671: y += rho omega (F - (I + dt grad(vn + dv)) Fn)
+    void admmUStep(T rho)
+    {
+        std::vector<M3<T>> grad;
+        evalGradient(dv, true, grad);
+#pragma omp parallel for schedule(static)
+        for (int64_t i = 0; i < P; ++i) {
+            for (int k = 0; k < 2; ++k) {
+                if (k == 1 && !visco[i].on) continue;
+                M3<T> Sn = strainN(k, i);
+                T om = admm_omega[2 * i + k];
+                M3<T> y = yOf(k, i);
+                M3<T> t = mul(grad[i], Sn);
+                for (int r = 0; r < 3; ++r)
+                    for (int c = 0; c < 3; ++c) {
+                        T tmp = admm_F[k][i].a[r][c] - Sn.a[r][c] - dt * t.a[r][c];
+                        y.a[r][c] += rho * om * tmp;
+                    }
+                setY(k, i, y);
+            }
+        }
+    }
+
+    // admmStep, AdmmSimulationFoam.h:766-801
+    int admmStep(const zmpm_solver& s, zmpm_stats& st)
+    {
+        const T rho = (T)s.admm_rho_scale;
+        admmInit(rho);
+        // residual_current is 1 (its computation is commented out, :779-780), so
+        // the MINRES relative tolerance is min(0.5, sqrt(max(1, 1e-6))) = 0.5
+        const T rel = std::min(T(0.5), T(1) * std::sqrt(std::max(T(1), T(1e-6))));
+        for (int it = 0; it < s.admm_iterations; ++it) {
+            admmUpdateCollisionNodes();
+            admmFStep(rho, (T)s.admm_local_tolerance);
+            st.krylov_iterations += admmDvStep(rho, (T)s.admm_global_tolerance, rel, s.admm_global_max_iterations);
+            admmUStep(rho);
+            st.newton_iterations += 1;
+        }
+        // last_dv = sum_i dv_i w_ip / (dt sum_i w_ip) (:788-800)
+#pragma omp parallel for schedule(static)
+        for (int64_t i = 0; i < P; ++i) {
+            T acc[3] = { 0, 0, 0 }, wsum = 0;
+            Spline<T> sp(&X[3 * i], dx);
+            iterateKernel(sp, base_offset[i], [&](const int*, T w, const T*, G& g) {
+                if (g.idx < 0) return;
+                for (int d = 0; d < 3; ++d) acc[d] += dv[3 * g.idx + d] * w;
+                wsum += w;
+            });
+            for (int d = 0; d < 3; ++d) admm_last_dv[3 * i + d] = acc[d] / (wsum * dt);
+        }
+        return ZMPM_OK;
+    }
+
     // ------------------------------------------------------------- G2P --
     // constructNewVelocityFromNewtonResult + gridToParticlesHelper<APIC,deg2,!MLS>
     // + evolveStrain + applyPlasticity, MpmSimulationBase.cpp:867-877, 906-1030
@@ -1659,6 +2263,11 @@ struct Sim {
             M3<T> Fp = mul(A, load9(F, i));
             if (plastic[i].kind == ZMPM_PLASTIC_VON_MISES) vonMisesProject(model[i], plastic[i], Fp);
             store9(F, i, Fp);
+            if (visco[i].on) {
+                M3<T> Fep = mul(A, load9(Fe, i));
+                viscousReturn(visco[i], (T)dt, Fep);
+                store9(Fe, i, Fep);
+            }
         }
         return too_fast;
     }
@@ -1697,10 +2306,35 @@ struct Sim {
     {
         std::memset(&st, 0, sizeof(st));
         hvp_count = 0;
-        int rc = beginImplicit(dt_in);
-        if (rc != ZMPM_OK) return rc;
-        bool conv = newton(s, st);
-        F = Fn; // restoreStrain
+        bool any_visco = false, all_models = true;
+        for (int64_t i = 0; i < P; ++i) {
+            any_visco = any_visco || visco[i].on;
+            all_models = all_models && model[i].kind != ZMPM_MODEL_NONE;
+        }
+        bool conv = true;
+        if (s.integrator == ZMPM_ADMM) {
+            // AdmmSimulation::advanceOneTimeStep, AdmmSimulationFoam.h:816-837
+            if (!all_models) {
+                err = "ADMM needs an F-based model on every particle";
+                return ZMPM_BAD_ARG;
+            }
+            dt = (T)dt_in;
+            implicit_ready = false;
+            int rc = sortParticlesAndPolluteGrid();
+            if (rc != ZMPM_OK) return rc;
+            particlesToGrid();
+            admmStep(s, st);
+        }
+        else {
+            if (any_visco) {
+                err = "viscoelastic particles need the ADMM integrator (StvkWithHencky has no stress differential)";
+                return ZMPM_BAD_ARG;
+            }
+            int rc = beginImplicit(dt_in);
+            if (rc != ZMPM_OK) return rc;
+            conv = newton(s, st);
+            F = Fn; // restoreStrain
+        }
         int too_fast = gridToParticles();
         time += dt_in;
         implicit_ready = false;
@@ -1762,6 +2396,12 @@ static void add_particles_impl(SimT& S, int64_t n, const double* x, const double
         S.model.emplace_back();
         S.plastic.emplace_back();
         S.damage.emplace_back();
+        S.visco.emplace_back();
+        for (int k = 0; k < 9; ++k) S.Fe.push_back((k % 4 == 0) ? T(1) : T(0));
+        for (int k = 0; k < 18; ++k) S.admm_y.push_back(T(0));
+        S.admm_omega.push_back(T(1));
+        S.admm_omega.push_back(T(1));
+        for (int k = 0; k < 3; ++k) S.admm_last_dv.push_back(T(0));
     }
     S.P += n;
     S.Fn = S.F;
@@ -1893,6 +2533,62 @@ int zoracle_get_damage(Ctx* c, double* out)
     DISPATCH(c, {
         for (int64_t i = 0; i < S.P; ++i) out[i] = S.damage[i].c;
     });
+    return ZMPM_OK;
+}
+
+int zoracle_add_viscoelastic(Ctx* c, int64_t lo, int64_t hi, double E, double nu, double vd, double vv)
+{
+    if (!c || !(vd > 0) || !(vv > 0)) return ZMPM_BAD_ARG;
+    DISPATCH(c, {
+        using T = typename std::remove_reference<decltype(S.dx)>::type;
+        if (lo < 0 || hi > S.P || lo > hi) return ZMPM_BAD_ARG;
+        for (int64_t i = lo; i < hi; ++i)
+            if (S.model[i].kind != ZMPM_MODEL_STVK_HENCKY_ISOTROPIC) return ZMPM_BAD_ARG;
+        T Et = (T)E, nut = (T)nu;
+        for (int64_t i = lo; i < hi; ++i) {
+            auto& v = S.visco[i];
+            v.on = 1;
+            v.lambda = Et * nut / ((T(1) + nut) * (T(1) - T(2) * nut)); // StvkWithHencky.cpp:16-20
+            v.mu = Et / (T(2) * (T(1) + nut));
+            v.vd = (T)vd;
+            v.vv = (T)vv;
+            for (int q = 0; q < 9; ++q) S.Fe[9 * i + q] = (q % 4 == 0) ? T(1) : T(0);
+        }
+    });
+    return ZMPM_OK;
+}
+
+int zoracle_get_viscoelastic_strain(Ctx* c, double* Fe)
+{
+    if (!c || !Fe) return ZMPM_BAD_ARG;
+    DISPATCH(c, {
+        for (int64_t i = 0; i < 9 * S.P; ++i) Fe[i] = S.Fe[i];
+    });
+    return ZMPM_OK;
+}
+
+int zoracle_set_viscoelastic_strain(Ctx* c, const double* Fe)
+{
+    if (!c || !Fe) return ZMPM_BAD_ARG;
+    DISPATCH(c, {
+        using T = typename std::remove_reference<decltype(S.dx)>::type;
+        for (int64_t i = 0; i < 9 * S.P; ++i) S.Fe[i] = (T)Fe[i];
+    });
+    return ZMPM_OK;
+}
+
+// The viscous return map alone on one strain (test hook).
+int zoracle_viscous_return(double E, double nu, double vd, double vv, double dt, double* F)
+{
+    zo::Visco<double> v;
+    v.lambda = E * nu / ((1 + nu) * (1 - 2 * nu));
+    v.mu = E / (2 * (1 + nu));
+    v.vd = vd;
+    v.vv = vv;
+    zo::M3<double> m;
+    for (int q = 0; q < 9; ++q) m.a[q / 3][q % 3] = F[q];
+    zo::viscousReturn(v, dt, m);
+    for (int q = 0; q < 9; ++q) F[q] = m.a[q / 3][q % 3];
     return ZMPM_OK;
 }
 

@@ -189,3 +189,87 @@ def test_rankine_damage_known_answer(oracle):
     np.testing.assert_allclose(c[: n // 2], want[: n // 2], rtol=1e-12)
     assert (c[: n // 2] < 1).sum() > n // 8
     assert np.all(c[n // 2:] == 1.0)
+
+
+def _admm_scene(lib, integrator, visco=False, iters=20, precision="fp64", E=2e4, nu=0.4, dx=1.0 / 64, seed=3,
+                grid_log2=None):
+    """Slab dropped on a sticky sphere over a sticky ground (the ADMM benchmark's
+    shape, scaled down)."""
+    kw = {} if grid_log2 is None else {"grid_log2": grid_log2}
+    s = mpm.MpmSimulation(dx, gravity=(0, -9.8, 0), precision=precision, lib=lib, **kw)
+    x = jittered_box((12, 4, 12), dx, (0.3, 0.55, 0.3), 8, seed)
+    V0 = dx ** 3 / 8
+    h = s.addParticles(x, np.tile([0.0, -1.0, 0.0], (len(x), 1)), 1000 * V0, V0)
+    h.addFBasedMpmForce(mpm.StvkWithHenckyIsotropic(E, nu))
+    if visco:
+        mu = E / (2 * (1 + nu))
+        nv = 2 * mu * 0.05  # relaxation time 0.05 s: alpha = 2 mu / nu_d = 1 / 0.05
+        h.addFElasticNonequilibratedBasedMpmForce(mpm.StvkWithHencky(E, nu), nv, nv)
+    s.addCollisionObject(mpm.AnalyticCollisionObject(mpm.Sphere((0.5, 0.35, 0.5), 0.2), abi.STICKY))
+    s.addCollisionObject(mpm.AnalyticCollisionObject(mpm.HalfSpace((0, 0.1, 0), (0, 1, 0)), abi.STICKY))
+    if integrator == "admm":
+        s.useAdmm(admm_max_iterations=iters, rho_scale=0.8, global_tolerance=1e-8)
+    else:
+        s.switchLinearSolver(abi.CG)
+        s.newton_tolerance = 1e-9
+        s.newton_max_iterations = 30
+        s.krylov_max_iterations = 500
+    return s
+
+
+def test_admm_converges_to_the_newton_solution(oracle):
+    """ADMM (AdmmSimulationFoam.h:766-801) minimises the same backward-Euler
+    objective as Newton: with enough iterations both restatements land on the
+    same velocities."""
+    out = {}
+    for integ, iters in (("newton", 0), ("admm", 20), ("admm", 100)):
+        s = _admm_scene(oracle, integ, iters=iters)
+        for _ in range(3):
+            assert s.advanceOneTimeStep(2e-3) == abi.OK
+        out[iters] = s.getParticles()["V"]
+    scale = np.abs(out[0]).max()
+    assert np.abs(out[20] - out[0]).max() / scale < 1e-3
+    assert np.abs(out[100] - out[0]).max() / scale < 1e-9
+
+
+def test_viscous_return_map_known_answer(oracle):
+    """FElasticNonequilibratedBasedMpmForceHelper::evolveStrain (h:62-87):
+    eps = (eps_trial - dt beta / (1 + dt (alpha + 3 beta)) t) / (1 + dt alpha),
+    Fe = U exp(eps) V^T, with alpha = 2 mu / nu_d, beta = 2 (2 mu + 3 lambda) /
+    (9 nu_v) - 2 mu / (3 nu_d).  t is `epsilon_trial.trace()` of a 3-vector,
+    which Eigen evaluates as its first coefficient."""
+    rng = np.random.default_rng(4)
+    E, nu, vd, vv, dt = 2e4, 0.4, 700.0, 500.0, 2e-3
+    mu, lam = E / (2 * (1 + nu)), E * nu / ((1 + nu) * (1 - 2 * nu))
+    alpha = 2 * mu / vd
+    beta = 2 * (2 * mu + 3 * lam) / (9 * vv) - 2 * mu / (3 * vd)
+    for _ in range(20):
+        s = np.sort(rng.uniform(0.7, 1.4, 3))[::-1]
+        U, _ = np.linalg.qr(rng.standard_normal((3, 3)))
+        V, _ = np.linalg.qr(rng.standard_normal((3, 3)))
+        U *= np.sign(np.linalg.det(U))
+        V *= np.sign(np.linalg.det(V))
+        F = U @ np.diag(s) @ V.T
+        out = np.ascontiguousarray(F.ravel())
+        oracle.dll.zoracle_viscous_return(C.c_double(E), C.c_double(nu), C.c_double(vd), C.c_double(vv), C.c_double(dt), P(out))
+        et = np.log(s)
+        eps = (et - dt * beta / (1 + dt * (alpha + 3 * beta)) * et[0]) / (1 + dt * alpha)
+        np.testing.assert_allclose(out.reshape(3, 3), U @ np.diag(np.exp(eps)) @ V.T, rtol=0, atol=1e-12)
+    # infinite viscosities leave Fe unchanged
+    out = np.ascontiguousarray(F.ravel())
+    oracle.dll.zoracle_viscous_return(C.c_double(E), C.c_double(nu), C.c_double(1e300), C.c_double(1e300), C.c_double(dt), P(out))
+    np.testing.assert_allclose(out.reshape(3, 3), F, atol=1e-12)
+
+
+def test_admm_viscoelastic_substeps(oracle):
+    """Viscoelastic slab (config 2 shape): Fe deviates from I under load and the
+    substep status is clean; Newton refuses viscoelastic particles like the
+    reference's StvkWithHencky, which has no stress differential."""
+    s = _admm_scene(oracle, "admm", visco=True)
+    for _ in range(3):
+        assert s.advanceOneTimeStep(2e-3) == abi.OK
+    Fe = s.getViscoelasticStrain()
+    assert np.abs(Fe - np.eye(3)).max() > 1e-3
+    assert np.all(np.isfinite(Fe))
+    s.integrator = abi.NEWTON
+    assert s.lib.substep(s.ctx, 2e-3, C.byref(s.solver()), None) == abi.BAD_ARG

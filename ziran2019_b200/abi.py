@@ -32,6 +32,7 @@ LAYOUT_AUTO, LAYOUT_244, LAYOUT_444 = 0, 1, 2
 MODEL_NONE, MODEL_NEOHOOKEAN_BORDEN, MODEL_STVK_HENCKY_ISOTROPIC, MODEL_FIXED_COROTATED = 0, 1, 2, 3
 PLASTIC_NONE, PLASTIC_VON_MISES = 0, 1
 DAMAGE_NONE, DAMAGE_RANKINE = 0, 1
+NEWTON, ADMM = 0, 1
 MINRES, CG = 0, 1
 HALF_SPACE, SPHERE, BOX = 0, 1, 2
 STICKY, SLIP, SEPARATE, GHOST = 1, 2, 3, 4
@@ -59,6 +60,13 @@ class Solver(C.Structure):
         ("pad0", C.c_int32),
         ("krylov_tolerance", C.c_double),
         ("linear_solve_tolerance_scale", C.c_double),
+        ("integrator", C.c_int32),
+        ("admm_iterations", C.c_int32),
+        ("admm_rho_scale", C.c_double),
+        ("admm_local_tolerance", C.c_double),
+        ("admm_global_tolerance", C.c_double),
+        ("admm_global_max_iterations", C.c_int32),
+        ("pad1", C.c_int32),
     ]
 
 
@@ -125,6 +133,9 @@ _SIGS = {
     "add_plasticity": (C.c_int, [C.c_void_p, C.c_int64, C.c_int64, C.c_int32, C.c_double, C.c_double, C.c_double]),
     "add_damage": (C.c_int, [C.c_void_p, C.c_int64, C.c_int64, C.c_int32, C.c_double, C.c_double]),
     "get_damage": (C.c_int, [C.c_void_p, c_double_p]),
+    "add_viscoelastic": (C.c_int, [C.c_void_p, C.c_int64, C.c_int64, C.c_double, C.c_double, C.c_double, C.c_double]),
+    "get_viscoelastic_strain": (C.c_int, [C.c_void_p, c_double_p]),
+    "set_viscoelastic_strain": (C.c_int, [C.c_void_p, c_double_p]),
     "add_collision_object": (C.c_int, [C.c_void_p, C.POINTER(Collider), c_int32_p]),
     "set_collision_object": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(Collider)]),
     "get_particles": (C.c_int, [C.c_void_p, c_double_p, c_double_p, c_double_p, c_double_p]),

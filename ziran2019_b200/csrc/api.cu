@@ -83,13 +83,28 @@ int upload(Ctx* ctx)
         hpi[PI_PKIND * cap + i] = ctx->hpkind[i];
         hpi[PI_BROKEN * cap + i] = ctx->hbroken[i];
         hpi[PI_ID * cap + i] = (int32_t)i;
+        hpi[PI_VISCO * cap + i] = ctx->hvisco[i];
+        for (int q = 0; q < 9; ++q) hpd[(PD_FE + q) * cap + i] = ctx->hFe[9 * i + q];
+        hpd[PD_VMU * cap + i] = ctx->hvmu[i];
+        hpd[PD_VLAM * cap + i] = ctx->hvlam[i];
+        hpd[PD_VD * cap + i] = ctx->hvd[i];
+        hpd[PD_VV * cap + i] = ctx->hvv[i];
+        for (int q = 0; q < 18; ++q) hpd[(PD_Y + q) * cap + i] = ctx->hy[18 * i + q];
+        for (int k = 0; k < 2; ++k) hpd[(PD_OMEGA + k) * cap + i] = ctx->homega[2 * i + k];
+        for (int d = 0; d < 3; ++d) hpd[(PD_LASTDV + d) * cap + i] = ctx->hlastdv[3 * i + d];
         sid[i] = (int32_t)i;
     }
     ZMPM_CUDA(cudaMemcpy(ctx->pd.p, hpd.data(), hpd.size() * sizeof(double), cudaMemcpyHostToDevice));
     ZMPM_CUDA(cudaMemcpy(ctx->pi.p, hpi.data(), hpi.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
     ZMPM_CUDA(cudaMemcpy(ctx->slot_of_id.p, sid.data(), sid.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
     ctx->has_damage = false;
-    for (int64_t i = 0; i < P; ++i) ctx->has_damage |= ctx->hdamage[i] != ZMPM_DAMAGE_NONE;
+    ctx->has_visco = false;
+    ctx->all_models = true;
+    for (int64_t i = 0; i < P; ++i) {
+        ctx->has_damage |= ctx->hdamage[i] != ZMPM_DAMAGE_NONE;
+        ctx->has_visco |= ctx->hvisco[i] != 0;
+        ctx->all_models &= ctx->hkind[i] != ZMPM_MODEL_NONE;
+    }
     ctx->uploaded = true;
     ctx->binned = false;
     ctx->implicit_ready = false;
@@ -101,7 +116,9 @@ int download(Ctx* ctx)
 {
     if (!ctx->uploaded) return ZMPM_OK;
     const int64_t P = ctx->P, cap = ctx->Pcap;
-    std::vector<double> hpd((size_t)PD_FIELDS * cap);
+    // fields past pd_active were not moved by the permutation: the host copy stays
+    const bool ext = ctx->pd_active == PD_FIELDS;
+    std::vector<double> hpd((size_t)ctx->pd_active * cap);
     std::vector<int32_t> hpi((size_t)PI_FIELDS * cap);
     ZMPM_CUDA(cudaStreamSynchronize(ctx->stream));
     ZMPM_CUDA(cudaMemcpy(hpd.data(), ctx->pd.p, hpd.size() * sizeof(double), cudaMemcpyDeviceToHost));
@@ -133,6 +150,16 @@ int download(Ctx* ctx)
         ctx->hkind[i] = (uint8_t)hpi[PI_KIND * cap + s];
         ctx->hpkind[i] = (uint8_t)hpi[PI_PKIND * cap + s];
         ctx->hbroken[i] = hpi[PI_BROKEN * cap + s];
+        ctx->hvisco[i] = (uint8_t)hpi[PI_VISCO * cap + s];
+        if (!ext) continue;
+        for (int q = 0; q < 9; ++q) ctx->hFe[9 * i + q] = hpd[(PD_FE + q) * cap + s];
+        ctx->hvmu[i] = hpd[PD_VMU * cap + s];
+        ctx->hvlam[i] = hpd[PD_VLAM * cap + s];
+        ctx->hvd[i] = hpd[PD_VD * cap + s];
+        ctx->hvv[i] = hpd[PD_VV * cap + s];
+        for (int q = 0; q < 18; ++q) ctx->hy[18 * i + q] = hpd[(PD_Y + q) * cap + s];
+        for (int k = 0; k < 2; ++k) ctx->homega[2 * i + k] = hpd[(PD_OMEGA + k) * cap + s];
+        for (int d = 0; d < 3; ++d) ctx->hlastdv[3 * i + d] = hpd[(PD_LASTDV + d) * cap + s];
     }
     return ZMPM_OK;
 }
@@ -326,6 +353,12 @@ void zmpm_default_solver(zmpm_solver* s, int32_t linear_solver, int32_t precisio
     s->newton_tolerance = 1e-5;
     s->krylov_max_iterations = 20;
     s->linear_solve_tolerance_scale = 1;
+    s->integrator = ZMPM_NEWTON;
+    s->admm_iterations = 100; // AdmmSimulationFoam.h:65-70
+    s->admm_rho_scale = 0.5;
+    s->admm_local_tolerance = 1e-8;
+    s->admm_global_tolerance = 1e-6;
+    s->admm_global_max_iterations = 10000;
     if (linear_solver == ZMPM_MINRES)
         s->krylov_tolerance = 1;
     else
@@ -456,6 +489,16 @@ int zmpm_add_particles(zmpm_ctx* ctx, int64_t n, const double* x, const double* 
         ctx->hkind.push_back(ZMPM_MODEL_NONE);
         ctx->hpkind.push_back(ZMPM_PLASTIC_NONE);
         ctx->hbroken.push_back(0);
+        ctx->hvisco.push_back(0);
+        for (int q = 0; q < 9; ++q) ctx->hFe.push_back((q % 4 == 0) ? 1.0 : 0.0);
+        ctx->hvmu.push_back(0);
+        ctx->hvlam.push_back(0);
+        ctx->hvd.push_back(1);
+        ctx->hvv.push_back(1);
+        for (int q = 0; q < 18; ++q) ctx->hy.push_back(0.0);
+        ctx->homega.push_back(1.0);
+        ctx->homega.push_back(1.0);
+        for (int d = 0; d < 3; ++d) ctx->hlastdv.push_back(0.0);
     }
     ctx->P += n;
     return ZMPM_OK;
@@ -537,6 +580,52 @@ int zmpm_get_damage(zmpm_ctx* ctx, double* c)
     return ZMPM_OK;
 }
 
+int zmpm_add_viscoelastic(zmpm_ctx* ctx, int64_t lo, int64_t hi, double E, double nu, double vd, double vv)
+{
+    if (!ctx || lo < 0 || hi > ctx->P || lo > hi || !(vd > 0) || !(vv > 0)) return ZMPM_BAD_ARG;
+    for (int64_t i = lo; i < hi; ++i)
+        if (ctx->hkind[i] != ZMPM_MODEL_STVK_HENCKY_ISOTROPIC) {
+            ctx->err = "viscoelastic particles must use StvkWithHenckyIsotropic";
+            return ZMPM_BAD_ARG;
+        }
+    cudaSetDevice(ctx->device);
+    int rc = begin_edit(ctx);
+    if (rc) return rc;
+    // StvkWithHencky::setLameParameters, StvkWithHencky.cpp:16-20
+    const double lambda = E * nu / ((1 + nu) * (1 - 2 * nu)), mu = E / (2 * (1 + nu));
+    for (int64_t i = lo; i < hi; ++i) {
+        ctx->hvisco[i] = 1;
+        ctx->hvmu[i] = mu;
+        ctx->hvlam[i] = lambda;
+        ctx->hvd[i] = vd;
+        ctx->hvv[i] = vv;
+        for (int q = 0; q < 9; ++q) ctx->hFe[9 * i + q] = (q % 4 == 0) ? 1.0 : 0.0;
+    }
+    if (hi > lo) ctx->has_visco = true;
+    ctx->pd_active = PD_FIELDS;
+    return ZMPM_OK;
+}
+
+int zmpm_get_viscoelastic_strain(zmpm_ctx* ctx, double* Fe)
+{
+    if (!ctx || !Fe) return ZMPM_BAD_ARG;
+    cudaSetDevice(ctx->device);
+    int rc = download(ctx);
+    if (rc) return rc;
+    std::memcpy(Fe, ctx->hFe.data(), 9 * ctx->P * sizeof(double));
+    return ZMPM_OK;
+}
+
+int zmpm_set_viscoelastic_strain(zmpm_ctx* ctx, const double* Fe)
+{
+    if (!ctx || !Fe) return ZMPM_BAD_ARG;
+    cudaSetDevice(ctx->device);
+    int rc = begin_edit(ctx);
+    if (rc) return rc;
+    std::memcpy(ctx->hFe.data(), Fe, 9 * ctx->P * sizeof(double));
+    return ZMPM_OK;
+}
+
 int zmpm_add_collision_object(zmpm_ctx* ctx, const zmpm_collider* o, int32_t* id)
 {
     if (!ctx || !o) return ZMPM_BAD_ARG;
@@ -608,7 +697,7 @@ int zmpm_get_plastic_state(zmpm_ctx* ctx, double* ys, int32_t* broken)
 }
 
 // ---------------------------------------------------------------- substep --
-static int begin_implicit_impl(zmpm_ctx* ctx, double dt)
+static int begin_implicit_impl(zmpm_ctx* ctx, double dt, bool damage = true)
 {
     int rc = upload(ctx);
     if (rc) return rc;
@@ -616,7 +705,7 @@ static int begin_implicit_impl(zmpm_ctx* ctx, double dt)
     ctx->implicit_ready = false;
     rc = run_binning(ctx);
     if (rc) return rc;
-    rc = run_p2g(ctx);
+    rc = run_p2g(ctx, damage);
     if (rc) return rc;
     ctx->implicit_ready = true;
     return ZMPM_OK;
@@ -625,15 +714,36 @@ static int begin_implicit_impl(zmpm_ctx* ctx, double dt)
 int zmpm_substep(zmpm_ctx* ctx, double dt, const zmpm_solver* s, zmpm_stats* st)
 {
     if (!ctx || !s || !(dt > 0) || s->newton_max_iterations < 0 || s->krylov_max_iterations < 0) return ZMPM_BAD_ARG;
+    const bool admm = s->integrator == ZMPM_ADMM;
+    if (!admm && s->integrator != ZMPM_NEWTON) return ZMPM_BAD_ARG;
+    if (admm && (s->admm_iterations < 0 || s->admm_global_max_iterations < 0 || !(s->admm_rho_scale > 0))) return ZMPM_BAD_ARG;
     cudaSetDevice(ctx->device);
+    if (admm) {
+        // AdmmSimulation indexes F (and Fe) by particle, so every particle needs an F-based model
+        int rc = upload(ctx);
+        if (rc) return rc;
+        if (!ctx->all_models) {
+            ctx->err = "ADMM needs an F-based model on every particle";
+            return ZMPM_BAD_ARG;
+        }
+        if (ctx->pd_active != PD_FIELDS) { // ADMM state moves with the particles from now on
+            int rc = begin_edit(ctx);
+            if (rc) return rc;
+            ctx->pd_active = PD_FIELDS;
+        }
+    }
+    else if (ctx->has_visco) {
+        ctx->err = "viscoelastic particles need the ADMM integrator (StvkWithHencky has no stress differential)";
+        return ZMPM_BAD_ARG;
+    }
     zmpm_stats local;
     if (!st) st = &local;
     std::memset(st, 0, sizeof(*st));
     const int64_t launches0 = g_kernel_launches;
     ZMPM_CUDA(cudaEventRecord(ctx->ev0, ctx->stream));
-    int rc = begin_implicit_impl(ctx, dt);
+    int rc = begin_implicit_impl(ctx, dt, !admm);
     if (rc) return rc;
-    rc = run_newton(ctx, *s);
+    rc = admm ? run_admm(ctx, *s) : run_newton(ctx, *s);
     if (rc) return rc;
     rc = run_g2p(ctx);
     if (rc) return rc;
@@ -664,7 +774,9 @@ int zmpm_substep(zmpm_ctx* ctx, double dt, const zmpm_solver* s, zmpm_stats* st)
     st->num_blocks = ctx->B;
     st->num_nodes = hc.N;
     st->ms_total = ms;
-    if (ctx->graph_used) // Newton body: stress, force, residual, check, start, step, advance
+    if (ctx->graph_used && admm) // ADMM iteration: 7 head + 3 tail kernels; Krylov body: 6
+        g_kernel_launches += 10 * (int64_t)hs.nit + 6 * (int64_t)hs.krylov_bodies;
+    else if (ctx->graph_used) // Newton body: stress, force, residual, check, start, step, advance
         g_kernel_launches += 7 * (int64_t)hs.nit + (ctx->hvp_fused ? 5 : 6) * (int64_t)hs.krylov_bodies;
     st->kernel_launches = (int32_t)(g_kernel_launches - launches0);
     ctx->N = hc.N;

@@ -82,7 +82,7 @@ __global__ void k_group_heads(const uint64_t* __restrict__ keys, int64_t P, int3
 // New slot i receives particle keys[i] & idmask: gather every field from its
 // old slot.  Also writes group starts and each group's page coordinates.
 template <class L>
-__global__ void k_permute(const uint64_t* __restrict__ keys, int64_t P, int64_t cap, const double* __restrict__ pd_src,
+__global__ void k_permute(const uint64_t* __restrict__ keys, int64_t P, int64_t cap, int npd, const double* __restrict__ pd_src,
     double* __restrict__ pd_dst, const int32_t* __restrict__ pi_src, int32_t* __restrict__ pi_dst, int32_t* __restrict__ slot_of_id,
     const short4* __restrict__ base_by_id, short4* __restrict__ base, const int32_t* __restrict__ head, const int32_t* __restrict__ gidx,
     int32_t* __restrict__ group_start, int4* __restrict__ group_page)
@@ -93,7 +93,7 @@ __global__ void k_permute(const uint64_t* __restrict__ keys, int64_t P, int64_t 
     const int32_t id = (int32_t)(k & ((1ull << L::INDEX_BITS) - 1));
     const int32_t old = slot_of_id[id];
 #pragma unroll 4
-    for (int f = 0; f < PD_FIELDS; ++f) pd_dst[f * cap + i] = pd_src[f * cap + old];
+    for (int f = 0; f < npd; ++f) pd_dst[f * cap + i] = pd_src[f * cap + old];
 #pragma unroll
     for (int f = 0; f < PI_FIELDS; ++f) pi_dst[f * cap + i] = pi_src[f * cap + old];
     pi_dst[PI_ID * cap + i] = id;
@@ -198,7 +198,7 @@ static int binning_impl(Ctx* ctx)
     k_group_heads<<<nblk(P), BIN_THREADS, 0, st>>>(keys, P, head);
     ++g_kernel_launches;
     exclusive_scan<int32_t>(head, gidx, P, tot, sscr, st);
-    k_permute<L><<<nblk(P), BIN_THREADS, 0, st>>>(keys, P, cap, ctx->pd.as<double>(), ctx->pd_alt.as<double>(), ctx->pi.as<int32_t>(),
+    k_permute<L><<<nblk(P), BIN_THREADS, 0, st>>>(keys, P, cap, ctx->pd_active, ctx->pd.as<double>(), ctx->pd_alt.as<double>(), ctx->pi.as<int32_t>(),
         ctx->pi_alt.as<int32_t>(), ctx->slot_of_id.as<int32_t>(), ctx->base_by_id.as<short4>(), ctx->base.as<short4>(), head, gidx,
         ctx->group_start.as<int32_t>(), ctx->group_page.as<int4>());
     ++g_kernel_launches;

@@ -82,9 +82,12 @@ struct SolverScalars {
 enum MinresSlot { MR_GC0, MR_GS0, MR_GC1, MR_GS1, MR_GC2, MR_GS2, MR_RHS0, MR_RHS1, MR_BETA_KP1, MR_TK, MR_DELTA, MR_EPS };
 
 // Field indices of the particle pools.
+// Fields from PD_CORE on (viscoelastic strain, ADMM state) are moved by the
+// binning permutation only once a context uses them (Ctx::pd_active).
 enum PdField { PD_X = 0, PD_V = 3, PD_C = 6, PD_F = 15, PD_M = 24, PD_VOL = 25, PD_MU = 26, PD_LAM = 27, PD_KAPPA = 28,
-    PD_G = 29, PD_YS = 30, PD_XI = 31, PD_FS = 32, PD_CRACK = 33, PD_PF_C = 36, PD_PF_K = 37, PD_SIGMA_F = 38, PD_FIELDS = 39 };
-enum PiField { PI_KIND = 0, PI_PKIND = 1, PI_BROKEN = 2, PI_ID = 3, PI_DAMAGE = 4, PI_FIELDS = 5 };
+    PD_G = 29, PD_YS = 30, PD_XI = 31, PD_FS = 32, PD_CRACK = 33, PD_PF_C = 36, PD_PF_K = 37, PD_SIGMA_F = 38, PD_CORE = 39,
+    PD_FE = 39, PD_VMU = 48, PD_VLAM = 49, PD_VD = 50, PD_VV = 51, PD_Y = 52, PD_OMEGA = 70, PD_LASTDV = 72, PD_FIELDS = 75 };
+enum PiField { PI_KIND = 0, PI_PKIND = 1, PI_BROKEN = 2, PI_ID = 3, PI_DAMAGE = 4, PI_VISCO = 5, PI_FIELDS = 6 };
 
 // Reduction slots: per-CTA partial sums written by node kernels.
 constexpr int RED_MAX_CTAS = 1024;
@@ -110,9 +113,13 @@ struct Ctx {
     int64_t P = 0;
     bool uploaded = false;
     std::vector<double> hx, hv, hC, hF, hcrack, hm, hvol, hmu, hlam, hkappa, hg, hys, hxi, hfs, hpfc, hpfk, hsigf;
-    std::vector<uint8_t> hkind, hpkind, hdamage;
+    std::vector<uint8_t> hkind, hpkind, hdamage, hvisco;
     std::vector<int32_t> hbroken;
+    std::vector<double> hFe, hvmu, hvlam, hvd, hvv, hy, homega, hlastdv; // viscoelastic + ADMM state
     bool has_damage = false;
+    bool has_visco = false;
+    bool all_models = true;               // every particle has an F-based model
+    int pd_active = PD_CORE;              // pd fields the binning permutation moves
     std::vector<zmpm_collider> colliders;
 
     // particles in slot order, structure of arrays (capacity Pcap).  The
@@ -160,6 +167,13 @@ struct Ctx {
     DBuf stage;                           // host <-> device particle transfers
     double dt = 0;
 
+    // ADMM (per substep): local variables F, Fe [18][Pcap]; grad vn [9][Pcap];
+    // global-operator coefficients B [6][Pcap] (HVP precision); node
+    // preconditioner, right-hand side and transfer weights
+    DBuf adm_F, adm_gvn, adm_B, adm_pre, adm_rhs, adm_w;
+    bool admm_used = false;               // the last substep ran ADMM (launch accounting)
+    int admm_iters = 0;
+
     int npb() const { return layout == 1 ? 32 : 64; }
 };
 
@@ -174,7 +188,7 @@ struct Ctx {
 
 // ---------------------------------------------------------------- passes --
 int run_binning(Ctx* ctx);
-int run_p2g(Ctx* ctx);                                 // P2G + grid normalisation + Newton setup
+int run_p2g(Ctx* ctx, bool damage = true);            // P2G (+ damage hook) + grid normalisation + Newton setup
 int run_newton(Ctx* ctx, const zmpm_solver& s);       // backward-Euler Newton
 int run_g2p(Ctx* ctx);                                 // G2P + evolveStrain + plasticity
 int upload_colliders(Ctx* ctx, double time);
@@ -182,6 +196,17 @@ int launch_update(Ctx* ctx);                           // G2P(vn+dv) -> stress -
 int launch_residual(Ctx* ctx);                         // r = dt m g + dt f - m dv (projected), norm partials
 int launch_hvp(Ctx* ctx, const double* x, double* out, bool fp32); // out += dt^2 K x (no inertia)
 int launch_damage(Ctx* ctx);                           // Rankine damage after P2G
+int run_admm(Ctx* ctx, const zmpm_solver& s);         // AdmmSimulation::admmStep
+// particle kernels of the ADMM substep (admm.cu)
+int launch_admm_dvinit(Ctx* ctx);                      // scatter last_dv w and w
+int launch_admm_init(Ctx* ctx, double rho);            // local variables, omega, y rescale, B
+int launch_admm_pre(Ctx* ctx);                         // preconditioner += grad w^T B grad w
+int launch_admm_local(Ctx* ctx, double rho, double local_tol); // F step + rhs stress
+int launch_admm_op(Ctx* ctx, const double* x0, const double* x1, bool alt, double* out, bool gated); // out += sum (grad x B) grad w
+int launch_admm_dual(Ctx* ctx, double rho);            // y += rho omega (F - (I + dt grad v) Fn)
+int launch_admm_lastdv(Ctx* ctx);                      // last_dv = sum dv w / (dt sum w)
+int launch_force_scatter(Ctx* ctx, double* out);       // out -= sum_p stress_p grad w_ip (stress buffer)
+int launch_hvp_scatter(Ctx* ctx, double* out, bool gated); // out += sum_p dstress_p grad w_ip
 int finalize_multiply(Ctx* ctx, const double* x, double* q); // q = project(m x + q)
 int ensure_node_buffers(Ctx* ctx);
 int compute_node_indices(Ctx* ctx);                    // getNumNodes numbering (hooks)

@@ -17,6 +17,8 @@
 // MINRES follows Minres.h:69-175, CG follows ConjugateGradient.h:99-147
 // (the working `solve`), both with the 1/m preconditioner
 // (MpmSimulationBase.cpp:617-623) and the collision projection.
+#include <algorithm>
+
 #include "internal.cuh"
 #include "mat3.cuh"
 
@@ -173,6 +175,79 @@ __device__ bool collider_resolve(const DevCollider& c, const double x[3], double
     return true;
 }
 
+// AnalyticCollisionObject::getBoundaryVelocityAndNormal (CollisionObject.cpp:313-338)
+__device__ bool collider_boundary(const DevCollider& c, const double x[3], double vb[3], double n[3])
+{
+    if (c.type == ZMPM_GHOST) return false;
+    double xb[3] = { x[0] - c.t[0], x[1] - c.t[1], x[2] - c.t[2] };
+    double ios = 1 / c.s;
+    double X[3];
+    for (int i = 0; i < 3; ++i) X[i] = (c.R[i] * xb[0] + c.R[3 + i] * xb[1] + c.R[6 + i] * xb[2]) * ios;
+    double N[3];
+    if (!collider_inside(c, X, N)) return false;
+    vb[0] = c.omega[1] * xb[2] - c.omega[2] * xb[1];
+    vb[1] = c.omega[2] * xb[0] - c.omega[0] * xb[2];
+    vb[2] = c.omega[0] * xb[1] - c.omega[1] * xb[0];
+    for (int i = 0; i < 3; ++i) vb[i] += (c.dsdt * ios) * xb[i] + c.dtdt[i];
+    for (int i = 0; i < 3; ++i) n[i] = c.R[3 * i] * N[0] + c.R[3 * i + 1] * N[1] + c.R[3 * i + 2] * N[2];
+    return true;
+}
+
+// AnalyticCollisionObject::multiObjectCollision (CollisionObject.cpp:66-105), or
+// with fake_separate multiObjectCollisionWithFakeSeparate (:108-156), where a
+// SEPARATE object the node already leaves does not collide.  Returns whether
+// any object collided; vi is resolved and P6 = I - K K^T (xx, xy, xz, yy, yz, zz).
+__device__ bool multi_collide(const DevCollider* __restrict__ cols, int ncols, const double xi[3], double vi[3], double P6[6], bool fake_separate)
+{
+    bool any = false;
+    int slip = 0;
+    double K[3][3] = { { 0, 0, 0 }, { 0, 0, 0 }, { 0, 0, 0 } };
+    for (int o = 0; o < ncols; ++o) {
+        if (cols[o].type == ZMPM_GHOST) continue;
+        double nrm[3] = { 0, 0, 0 };
+        const double old[3] = { vi[0], vi[1], vi[2] };
+        bool hit = collider_resolve(cols[o], xi, vi, nrm);
+        if (hit && fake_separate && cols[o].type == ZMPM_SEPARATE) {
+            double vb[3] = { 0, 0, 0 }, nb[3] = { 0, 0, 0 };
+            collider_boundary(cols[o], xi, vb, nb);
+            if ((old[0] - vb[0]) * nb[0] + (old[1] - vb[1]) * nb[1] + (old[2] - vb[2]) * nb[2] > 0) {
+                vi[0] = old[0];
+                vi[1] = old[1];
+                vi[2] = old[2];
+                hit = false;
+            }
+        }
+        any = hit || any;
+        if (!hit) continue;
+        if (cols[o].type == ZMPM_STICKY) {
+            for (int r = 0; r < 3; ++r)
+                for (int q = 0; q < 3; ++q) K[r][q] = (r == q) ? 1.0 : 0.0;
+            break;
+        }
+        for (int q = 0; q < slip; ++q) {
+            double dd = K[0][q] * nrm[0] + K[1][q] * nrm[1] + K[2][q] * nrm[2];
+            for (int r = 0; r < 3; ++r) nrm[r] -= dd * K[r][q];
+        }
+        double len = sqrt(nrm[0] * nrm[0] + nrm[1] * nrm[1] + nrm[2] * nrm[2]);
+        if (len != 0) {
+            for (int r = 0; r < 3; ++r) K[r][slip] = nrm[r] / len;
+            if (++slip == 3) break;
+        }
+    }
+    double KK[3][3];
+    for (int r = 0; r < 3; ++r)
+        for (int q = 0; q < 3; ++q) KK[r][q] = K[r][0] * K[q][0] + K[r][1] * K[q][1] + K[r][2] * K[q][2];
+    if (any) {
+        P6[0] = 1 - KK[0][0];
+        P6[1] = -KK[0][1];
+        P6[2] = -KK[0][2];
+        P6[3] = 1 - KK[1][1];
+        P6[4] = -KK[1][2];
+        P6[5] = 1 - KK[2][2];
+    }
+    return any;
+}
+
 // ------------------------------------------------------------- grid init --
 // particlesToGrid normalisation (MpmSimulationBase.cpp:474-485) +
 // buildInitialDvAndVnForNewton (:1105-1136): vn, dv, vstar = vn + dv,
@@ -199,42 +274,8 @@ __global__ void __launch_bounds__(ND_THREADS) k_grid_init(NodeGeom ng, const dou
             const int lx = e >> (L::YB + L::ZB), ly = (e >> L::ZB) & (L::BY - 1), lz = e & (L::BZ - 1);
             double xi[3] = { (bp.x * L::BX + lx) * dx, (bp.y * L::BY + ly) * dx, (bp.z * L::BZ + lz) * dx };
             double vi[3] = { v[0], v[1], v[2] };
-            // AnalyticCollisionObject::multiObjectCollision (CollisionObject.cpp:66-105)
-            bool any = false;
-            int slip = 0;
-            double K[3][3] = { { 0, 0, 0 }, { 0, 0, 0 }, { 0, 0, 0 } };
-            for (int o = 0; o < ncols; ++o) {
-                if (cols[o].type == ZMPM_GHOST) continue;
-                double nrm[3] = { 0, 0, 0 };
-                bool hit = collider_resolve(cols[o], xi, vi, nrm);
-                any = hit || any;
-                if (!hit) continue;
-                if (cols[o].type == ZMPM_STICKY) {
-                    for (int r = 0; r < 3; ++r)
-                        for (int q = 0; q < 3; ++q) K[r][q] = (r == q) ? 1.0 : 0.0;
-                    break;
-                }
-                for (int q = 0; q < slip; ++q) {
-                    double dd = K[0][q] * nrm[0] + K[1][q] * nrm[1] + K[2][q] * nrm[2];
-                    for (int r = 0; r < 3; ++r) nrm[r] -= dd * K[r][q];
-                }
-                double len = sqrt(nrm[0] * nrm[0] + nrm[1] * nrm[1] + nrm[2] * nrm[2]);
-                if (len != 0) {
-                    for (int r = 0; r < 3; ++r) K[r][slip] = nrm[r] / len;
-                    if (++slip == 3) break;
-                }
-            }
-            if (any) {
+            if (multi_collide(cols, ncols, xi, vi, P, false)) {
                 c = 1;
-                double KK[3][3];
-                for (int r = 0; r < 3; ++r)
-                    for (int q = 0; q < 3; ++q) KK[r][q] = K[r][0] * K[q][0] + K[r][1] * K[q][1] + K[r][2] * K[q][2];
-                P[0] = 1 - KK[0][0];
-                P[1] = -KK[0][1];
-                P[2] = -KK[0][2];
-                P[3] = 1 - KK[1][1];
-                P[4] = -KK[1][2];
-                P[5] = 1 - KK[2][2];
                 for (int k = 0; k < 3; ++k) d[k] = vi[k] - v[k];
             }
             else {
@@ -297,6 +338,7 @@ struct KrylovBufs {
     double *x, *r, *p, *q, *tmp;      // CG
     double *Q[3], *M[3], *Z[2];       // MINRES
     double* hacc;                     // Hessian accumulator
+    const double* pre;                // diagonal preconditioner per node (the mass for Newton)
 };
 
 struct NewtonParams {
@@ -342,7 +384,7 @@ __global__ void __launch_bounds__(ND_THREADS) k_newton_check(NodeGeom ng, const 
         for (int k = 0; k < 3; ++k) {
             int64_t i = vidx<NPB>(n, k);
             double rv = res[i];
-            double z = (m != 0) ? rv / m : 0.0;
+            double z = (m != 0) ? rv / kb.pre[n] : 0.0;
             kb.x[i] = 0;
             if (np.minres) {
                 kb.Q[0][i] = rv;
@@ -475,7 +517,7 @@ __global__ void __launch_bounds__(ND_THREADS) k_cg_b(NodeGeom ng, const double* 
             kb.x[i] += kb.p[i] * alpha;
             double r = kb.r[i] - kb.tmp[i] * alpha;
             kb.r[i] = r;
-            double q = (m != 0) ? r / m : 0.0;
+            double q = (m != 0) ? r / kb.pre[n] : 0.0;
             kb.q[i] = q;
             acc += q * r;
         }
@@ -531,7 +573,7 @@ __global__ void __launch_bounds__(ND_THREADS) k_mr_b(NodeGeom ng, const double* 
             q -= alpha * qk[i];
             q -= beta_k * qkm1[i];
             qkp1[i] = q;
-            double z = (m != 0) ? q / m : 0.0;
+            double z = (m != 0) ? q / kb.pre[n] : 0.0;
             zout[i] = z;
             acc += z * q;
         }
@@ -655,6 +697,120 @@ __global__ void k_newton_advance(SolverScalars* __restrict__ sc, int nmax, cudaG
     if (use_graph) cudaGraphSetConditional(hN, (!sc->newton_done && n < nmax) ? 1u : 0u);
 }
 
+// ------------------------------------------------------------------ ADMM --
+// updateCollisionNodes (AdmmSimulationFoam.h:276-293) on vi = dv + vn with the
+// fake-separate rule, vstar = vn + dv and the right-hand side's dt m g (dvStep,
+// :167-170).  With wsum (initStep, :304-320) dv is first replaced by
+// dv dt / sum_p w_ip.
+template <class L>
+__global__ void __launch_bounds__(ND_THREADS) k_admm_collide(NodeGeom ng, const double* __restrict__ gm, const int4* __restrict__ block_page,
+    double dx, double gx, double gy, double gz, double dt, const DevCollider* __restrict__ cols, int ncols, const double* __restrict__ vn,
+    double* __restrict__ dv, double* __restrict__ vstar, int8_t* __restrict__ col, double* __restrict__ P6, double* __restrict__ rhs,
+    const double* __restrict__ wsum)
+{
+    constexpr int NPB = L::NPB;
+    const double g[3] = { gx, gy, gz };
+    for (int64_t n = (int64_t)blockIdx.x * ND_THREADS + threadIdx.x; n < ng.nn; n += (int64_t)gridDim.x * ND_THREADS) {
+        const int64_t b = n / NPB;
+        const int e = (int)(n - b * NPB);
+        const double m = gm[n];
+        double v[3], d[3];
+        for (int k = 0; k < 3; ++k) {
+            v[k] = vn[vidx<NPB>(n, k)];
+            d[k] = dv[vidx<NPB>(n, k)];
+        }
+        int8_t c = 0;
+        double P[6] = { 1, 0, 0, 1, 0, 1 };
+        if (m != 0) {
+            if (wsum)
+                for (int k = 0; k < 3; ++k) d[k] = d[k] * dt / wsum[n];
+            const int4 bp = block_page[b];
+            const int lx = e >> (L::YB + L::ZB), ly = (e >> L::ZB) & (L::BY - 1), lz = e & (L::BZ - 1);
+            const double xi[3] = { (bp.x * L::BX + lx) * dx, (bp.y * L::BY + ly) * dx, (bp.z * L::BZ + lz) * dx };
+            double vi[3] = { d[0] + v[0], d[1] + v[1], d[2] + v[2] };
+            if (multi_collide(cols, ncols, xi, vi, P, true)) {
+                c = 1;
+                for (int k = 0; k < 3; ++k) d[k] = vi[k] - v[k];
+            }
+        }
+        else
+            d[0] = d[1] = d[2] = 0;
+        for (int k = 0; k < 3; ++k) {
+            const int64_t i = vidx<NPB>(n, k);
+            dv[i] = d[k];
+            vstar[i] = (m != 0) ? v[k] + d[k] : 0.0;
+            rhs[i] = (m != 0) ? dt * m * g[k] : 0.0;
+        }
+        col[n] = c;
+        for (int k = 0; k < 6; ++k) P6[k * ng.nn + n] = P[k];
+    }
+}
+
+// Start of dvStep's MINRES from the current dv (Minres.h:73-98): r =
+// project(rhs - (m dv + hacc)), zeroes hacc; Q0 = r, Z0 = r / pre, the other
+// Lanczos vectors and search directions 0, the correction x = 0; partial z.r.
+// The relative tolerance is min(0.5, sqrt(max(residual, 1e-6))) with the
+// reference's constant residual 1 (AdmmSimulationFoam.h:779-782): 0.5.
+template <int NPB>
+__global__ void __launch_bounds__(ND_THREADS) k_admm_start(NodeGeom ng, const double* __restrict__ gm, const int8_t* __restrict__ col,
+    const double* __restrict__ P6, const double* __restrict__ rhs, const double* __restrict__ dv, KrylovBufs kb, double* __restrict__ part,
+    SolverScalars* __restrict__ sc)
+{
+    if (blockIdx.x == 0 && threadIdx.x == 0) sc->rel_tol = 0.5;
+    double acc = 0;
+    for (int64_t n = (int64_t)blockIdx.x * ND_THREADS + threadIdx.x; n < ng.nn; n += (int64_t)gridDim.x * ND_THREADS) {
+        const double m = gm[n];
+        double r[3];
+        for (int k = 0; k < 3; ++k) {
+            const int64_t i = vidx<NPB>(n, k);
+            r[k] = (m != 0) ? rhs[i] - (m * dv[i] + kb.hacc[i]) : 0.0;
+            kb.hacc[i] = 0;
+        }
+        if (m != 0) project3(col, P6, ng.nn, n, r);
+        for (int k = 0; k < 3; ++k) {
+            const int64_t i = vidx<NPB>(n, k);
+            const double z = (m != 0) ? r[k] / kb.pre[n] : 0.0;
+            kb.x[i] = 0;
+            kb.Q[0][i] = r[k];
+            kb.Q[1][i] = 0;
+            kb.Q[2][i] = 0;
+            kb.M[0][i] = 0;
+            kb.M[1][i] = 0;
+            kb.M[2][i] = 0;
+            kb.Z[0][i] = z;
+            acc += z * r[k];
+        }
+    }
+    double t = block_sum(acc);
+    if (threadIdx.x == 0) part[blockIdx.x] = t;
+}
+
+// dv += x (the MINRES correction); vstar = vn + dv on active nodes.
+template <int NPB>
+__global__ void __launch_bounds__(ND_THREADS) k_admm_dv_update(NodeGeom ng, const double* __restrict__ gm, const double* __restrict__ x,
+    const double* __restrict__ vn, double* __restrict__ dv, double* __restrict__ vstar)
+{
+    for (int64_t n = (int64_t)blockIdx.x * ND_THREADS + threadIdx.x; n < ng.nn; n += (int64_t)gridDim.x * ND_THREADS) {
+        const bool act = gm[n] != 0;
+        for (int k = 0; k < 3; ++k) {
+            const int64_t i = vidx<NPB>(n, k);
+            const double d = dv[i] + x[i];
+            dv[i] = d;
+            vstar[i] = act ? vn[i] + d : 0.0;
+        }
+    }
+}
+
+// Ends an ADMM iteration (admmStep loop, AdmmSimulationFoam.h:776-784).
+__global__ void k_admm_advance(SolverScalars* __restrict__ sc, int nmax, cudaGraphConditionalHandle hN, int use_graph)
+{
+    sc->newton_iters += 1;
+    const int n = sc->nit + 1;
+    sc->nit = n;
+    if (n >= nmax) sc->converged = 1;
+    if (use_graph) cudaGraphSetConditional(hN, n < nmax ? 1u : 0u);
+}
+
 // ------------------------------------------------------------ host side --
 static NodeGeom node_geom(const Ctx* ctx)
 {
@@ -682,7 +838,7 @@ int ensure_node_buffers(Ctx* ctx)
     return ZMPM_OK;
 }
 
-int run_p2g(Ctx* ctx)
+int run_p2g(Ctx* ctx, bool damage)
 {
     cudaStream_t st = ctx->stream;
     const int64_t nn = ctx->B * ctx->npb();
@@ -694,8 +850,10 @@ int run_p2g(Ctx* ctx)
     ZMPM_CUDA(cudaMemsetAsync(ctx->kv[9].p, 0, 3 * nn * sizeof(double), st)); // Hessian accumulator
     rc = launch_p2g(ctx);
     if (rc) return rc;
-    rc = launch_damage(ctx); // the fracture hook runs after particlesToGrid
-    if (rc) return rc;
+    if (damage) {
+        rc = launch_damage(ctx); // the fracture hook runs after particlesToGrid
+        if (rc) return rc;
+    }
     rc = upload_colliders(ctx, ctx->time);
     if (rc) return rc;
     NodeGeom ng = node_geom(ctx);
@@ -833,13 +991,13 @@ int launch_newton_tail(const NewtonLaunch& L, cudaStream_t st, cudaGraphConditio
         }                                                                                                              \
     } while (0)
 
-// The Newton solve as one CUDA graph: WHILE(Newton){ head; WHILE(Krylov){
-// iteration }; tail }.  Both loop conditions are set on the device, so the
-// host launches the whole solve once and no Krylov slot is launched idle.
-template <int NPB>
-int newton_graph(const NewtonLaunch& L, cudaGraphExec_t* exec_out)
+// An outer solver loop as one CUDA graph: WHILE(outer){ head; WHILE(Krylov){
+// body }; tail }.  Both loop conditions are set on the device, so the host
+// launches the whole solve once and no Krylov slot is launched idle.
+// head(st, hK), body(st, hK) and tail(st, hN) launch with use_graph = 1.
+template <class Head, class Body, class Tail>
+int loop_graph(Ctx* ctx, Head&& head, Body&& body, Tail&& tail, cudaGraphExec_t* exec_out)
 {
-    Ctx* ctx = L.ctx;
     cudaStream_t st = ctx->stream;
     cudaGraph_t g = nullptr;
     ZMPM_CAP(cudaGraphCreate(&g, 0));
@@ -856,7 +1014,7 @@ int newton_graph(const NewtonLaunch& L, cudaGraphExec_t* exec_out)
     cudaGraph_t bodyN = pN.conditional.phGraph_out[0];
 
     ZMPM_CAP(cudaStreamBeginCaptureToGraph(st, bodyN, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
-    int rc = launch_newton_head<NPB>(L, st, hK, 1);
+    int rc = head(st, hK);
     if (rc) {
         cudaGraph_t tmp;
         cudaStreamEndCapture(st, &tmp);
@@ -877,7 +1035,7 @@ int newton_graph(const NewtonLaunch& L, cudaGraphExec_t* exec_out)
     ZMPM_CAP(cudaGraphAddNode(&nK, capg, deps, ndeps, &pK));
     ZMPM_CAP(cudaStreamUpdateCaptureDependencies(st, &nK, 1, cudaStreamSetCaptureDependencies));
     cudaGraph_t bodyK = pK.conditional.phGraph_out[0];
-    rc = launch_newton_tail<NPB>(L, st, hN, 1);
+    rc = tail(st, hN);
     cudaGraph_t tmp = nullptr;
     ZMPM_CAP(cudaStreamEndCapture(st, &tmp));
     if (rc) {
@@ -885,7 +1043,7 @@ int newton_graph(const NewtonLaunch& L, cudaGraphExec_t* exec_out)
         return rc;
     }
     ZMPM_CAP(cudaStreamBeginCaptureToGraph(st, bodyK, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
-    rc = launch_krylov_iteration<NPB>(L, st, hK, 1, nullptr, nullptr);
+    rc = body(st, hK);
     ZMPM_CAP(cudaStreamEndCapture(st, &tmp));
     if (rc) {
         cudaGraphDestroy(g);
@@ -894,6 +1052,16 @@ int newton_graph(const NewtonLaunch& L, cudaGraphExec_t* exec_out)
     ZMPM_CAP(cudaGraphInstantiate(exec_out, g, 0));
     cudaGraphDestroy(g);
     return ZMPM_OK;
+}
+
+// The Newton solve as one graph.
+template <int NPB>
+int newton_graph(const NewtonLaunch& L, cudaGraphExec_t* exec_out)
+{
+    return loop_graph(
+        L.ctx, [&](cudaStream_t st, cudaGraphConditionalHandle hK) { return launch_newton_head<NPB>(L, st, hK, 1); },
+        [&](cudaStream_t st, cudaGraphConditionalHandle hK) { return launch_krylov_iteration<NPB>(L, st, hK, 1, nullptr, nullptr); },
+        [&](cudaStream_t st, cudaGraphConditionalHandle hN) { return launch_newton_tail<NPB>(L, st, hN, 1); }, exec_out);
 }
 
 } // namespace
@@ -924,6 +1092,7 @@ static int newton_impl(Ctx* ctx, const zmpm_solver& s)
     L.kb.Z[0] = ctx->kv[7].as<double>();
     L.kb.Z[1] = ctx->kv[8].as<double>();
     L.kb.hacc = ctx->kv[9].as<double>();
+    L.kb.pre = ctx->gm.as<double>();
     L.np.minres = s.linear_solver == ZMPM_MINRES ? 1 : 0;
     L.np.kmax = s.krylov_max_iterations;
     L.np.nmax = s.newton_max_iterations;
@@ -984,6 +1153,167 @@ static int newton_impl(Ctx* ctx, const zmpm_solver& s)
 int run_newton(Ctx* ctx, const zmpm_solver& s)
 {
     return ctx->layout == 1 ? newton_impl<32>(ctx, s) : newton_impl<64>(ctx, s);
+}
+
+// AdmmSimulation::admmStep (AdmmSimulationFoam.h:766-801) after P2G: initStep,
+// the global operator's preconditioner, then per iteration the collision
+// update, F step (+ dvStep right-hand side), dvStep's MINRES and the dual
+// update; finally last_dv.  The iteration loop runs as one conditional graph
+// like the Newton solve (host-driven when profiling or without graphs).
+template <class L>
+static int admm_impl(Ctx* ctx, const zmpm_solver& s)
+{
+    constexpr int NPB = L::NPB;
+    cudaStream_t st = ctx->stream;
+    const int64_t nn = ctx->B * NPB, cap = ctx->Pcap;
+    const size_t TH = ctx->mixed ? sizeof(float) : sizeof(double);
+    ZMPM_CUDA(ctx->adm_F.ensure(18 * cap * sizeof(double)));
+    ZMPM_CUDA(ctx->adm_gvn.ensure(9 * cap * sizeof(double)));
+    ZMPM_CUDA(ctx->adm_B.ensure(6 * cap * TH));
+    ZMPM_CUDA(ctx->adm_pre.ensure(std::max<int64_t>(nn, 1) * sizeof(double)));
+    ZMPM_CUDA(ctx->adm_rhs.ensure(std::max<int64_t>(3 * nn, 1) * sizeof(double)));
+    ZMPM_CUDA(ctx->adm_w.ensure(std::max<int64_t>(nn, 1) * sizeof(double)));
+    NewtonLaunch Lc;
+    Lc.ctx = ctx;
+    Lc.ng = node_geom(ctx);
+    Lc.sc = ctx->scal.as<SolverScalars>();
+    double* part = ctx->red.as<double>();
+    Lc.pA = part + RED_A * RED_MAX_CTAS;
+    Lc.pB = part + RED_B * RED_MAX_CTAS;
+    Lc.pC = part + RED_C * RED_MAX_CTAS;
+    KrylovBufs& kb = Lc.kb;
+    kb.x = ctx->kv[0].as<double>();
+    kb.r = kb.p = kb.q = kb.tmp = nullptr;
+    kb.Q[0] = ctx->kv[1].as<double>();
+    kb.Q[1] = ctx->kv[2].as<double>();
+    kb.Q[2] = ctx->kv[3].as<double>();
+    kb.M[0] = ctx->kv[4].as<double>();
+    kb.M[1] = ctx->kv[5].as<double>();
+    kb.M[2] = ctx->kv[6].as<double>();
+    kb.Z[0] = ctx->kv[7].as<double>();
+    kb.Z[1] = ctx->kv[8].as<double>();
+    kb.hacc = ctx->kv[9].as<double>();
+    kb.pre = ctx->adm_pre.as<double>();
+    Lc.np.minres = 1;
+    Lc.np.kmax = s.admm_global_max_iterations;
+    Lc.np.nmax = s.admm_iterations;
+    Lc.np.tol = 0;
+    Lc.np.abs_tol = s.admm_global_tolerance;
+    Lc.np.tol_scale = 1;
+    Lc.np.dt = ctx->dt;
+    Lc.dt2 = 1.0;
+    Lc.nb = Lc.ng.parts;
+    const double rho = s.admm_rho_scale, local_tol = s.admm_local_tolerance;
+    ZMPM_CUDA(cudaMemsetAsync(Lc.sc, 0, sizeof(SolverScalars), st));
+    ctx->prof_newton = 0;
+    ctx->graph_used = false;
+    ctx->admm_iters = 0;
+    if (nn == 0) return ZMPM_OK;
+    const double* g = ctx->cfg.gravity;
+    const int ncols = (int)ctx->colliders.size();
+    const DevCollider* cols = ctx->dcolliders.as<DevCollider>();
+    auto collide = [&](cudaStream_t sm, const double* wsum) {
+        k_admm_collide<L><<<Lc.nb, ND_THREADS, 0, sm>>>(Lc.ng, ctx->gm.as<double>(), ctx->block_page.as<int4>(), ctx->cfg.dx, g[0], g[1], g[2],
+            ctx->dt, cols, ncols, ctx->vn.as<double>(), ctx->dv.as<double>(), ctx->vstar.as<double>(), ctx->collided.as<int8_t>(),
+            ctx->proj.as<double>(), ctx->adm_rhs.as<double>(), wsum);
+        ++g_kernel_launches;
+    };
+
+    // initStep + initMultiplierAndPreconditioner
+    ZMPM_CUDA(cudaMemsetAsync(ctx->dv.p, 0, 3 * nn * sizeof(double), st));
+    ZMPM_CUDA(cudaMemsetAsync(ctx->adm_w.p, 0, nn * sizeof(double), st));
+    int rc = launch_admm_dvinit(ctx);
+    if (rc) return rc;
+    collide(st, ctx->adm_w.as<double>());
+    rc = launch_admm_init(ctx, rho);
+    if (rc) return rc;
+    ZMPM_CUDA(cudaMemcpyAsync(ctx->adm_pre.p, ctx->gm.p, nn * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    rc = launch_admm_pre(ctx);
+    if (rc) return rc;
+
+    auto head = [&](cudaStream_t sm, cudaGraphConditionalHandle hK, int ug) {
+        collide(sm, nullptr);
+        int r = launch_admm_local(ctx, rho, local_tol);
+        if (r) return r;
+        r = launch_force_scatter(ctx, ctx->adm_rhs.as<double>());
+        if (r) return r;
+        r = launch_admm_op(ctx, ctx->dv.as<double>(), ctx->dv.as<double>(), false, kb.hacc, false);
+        if (r) return r;
+        k_admm_start<NPB><<<Lc.nb, ND_THREADS, 0, sm>>>(Lc.ng, ctx->gm.as<double>(), ctx->collided.as<int8_t>(), ctx->proj.as<double>(),
+            ctx->adm_rhs.as<double>(), ctx->dv.as<double>(), kb, Lc.pB, Lc.sc);
+        k_krylov_start<NPB><<<Lc.nb, ND_THREADS, 0, sm>>>(Lc.ng, kb, Lc.np, Lc.pB, Lc.sc, hK, ug);
+        g_kernel_launches += 2;
+        return (int)ZMPM_OK;
+    };
+    auto body = [&](cudaStream_t sm, cudaGraphConditionalHandle hK, int ug) {
+        int r = launch_admm_op(ctx, kb.Z[0], kb.Z[1], true, kb.hacc, true);
+        if (r) return r;
+        k_apply_A_krylov<NPB><<<Lc.nb, ND_THREADS, 0, sm>>>(Lc.ng, ctx->gm.as<double>(), ctx->collided.as<int8_t>(), ctx->proj.as<double>(),
+            1.0, kb, 1, Lc.pA, Lc.sc);
+        k_mr_b<NPB><<<Lc.nb, ND_THREADS, 0, sm>>>(Lc.ng, ctx->gm.as<double>(), kb, Lc.pA, Lc.pC, Lc.sc);
+        k_mr_c<NPB><<<Lc.nb, ND_THREADS, 0, sm>>>(Lc.ng, kb, Lc.pC, Lc.sc);
+        k_krylov_advance<<<1, 1, 0, sm>>>(Lc.sc, Lc.np.kmax, hK, ug);
+        g_kernel_launches += 4;
+        return (int)ZMPM_OK;
+    };
+    auto tail = [&](cudaStream_t sm, cudaGraphConditionalHandle hN, int ug) {
+        k_admm_dv_update<NPB><<<Lc.nb, ND_THREADS, 0, sm>>>(Lc.ng, ctx->gm.as<double>(), kb.x, ctx->vn.as<double>(), ctx->dv.as<double>(),
+            ctx->vstar.as<double>());
+        ++g_kernel_launches;
+        int r = launch_admm_dual(ctx, rho);
+        if (r) return r;
+        k_admm_advance<<<1, 1, 0, sm>>>(Lc.sc, Lc.np.nmax, hN, ug);
+        ++g_kernel_launches;
+        return (int)ZMPM_OK;
+    };
+
+    if (s.admm_iterations > 0) {
+        if (!ctx->profiling && !ctx->no_graph) {
+            cudaGraphExec_t exec = nullptr;
+            const int64_t launches0 = g_kernel_launches;
+            rc = loop_graph(
+                ctx, [&](cudaStream_t sm, cudaGraphConditionalHandle hK) { return head(sm, hK, 1); },
+                [&](cudaStream_t sm, cudaGraphConditionalHandle hK) { return body(sm, hK, 1); },
+                [&](cudaStream_t sm, cudaGraphConditionalHandle hN) { return tail(sm, hN, 1); }, &exec);
+            if (rc) return rc;
+            cudaError_t e = cudaGraphLaunch(exec, st);
+            g_kernel_launches = launches0; // counted per executed body after the substep
+            ctx->graph_used = true;
+            if (ctx->graph_exec) cudaGraphExecDestroy(ctx->graph_exec);
+            ctx->graph_exec = exec;
+            ZMPM_CUDA(e);
+        }
+        else {
+            // host-driven: the Krylov loop polls the active flag every 8 iterations
+            for (int it = 0; it < s.admm_iterations; ++it) {
+                rc = head(st, 0, 0);
+                if (rc) return rc;
+                for (int k = 0; k < Lc.np.kmax; k += 8) {
+                    for (int j = 0; j < 8 && k + j < Lc.np.kmax; ++j) {
+                        rc = body(st, 0, 0);
+                        if (rc) return rc;
+                    }
+                    SolverScalars hs;
+                    ZMPM_CUDA(cudaMemcpyAsync(&hs, Lc.sc, sizeof(hs), cudaMemcpyDeviceToHost, st));
+                    ZMPM_CUDA(cudaStreamSynchronize(st));
+                    if (!hs.kactive) break;
+                }
+                rc = tail(st, 0, 0);
+                if (rc) return rc;
+                ZMPM_CUDA(cudaGetLastError());
+            }
+        }
+    }
+    ctx->admm_iters = s.admm_iterations;
+    rc = launch_admm_lastdv(ctx);
+    if (rc) return rc;
+    ZMPM_CUDA(cudaGetLastError());
+    return ZMPM_OK;
+}
+
+int run_admm(Ctx* ctx, const zmpm_solver& s)
+{
+    return ctx->layout == 1 ? admm_impl<Layout244>(ctx, s) : admm_impl<Layout444>(ctx, s);
 }
 
 int run_g2p(Ctx* ctx)

@@ -40,6 +40,12 @@ class StvkWithHenckyIsotropic(_Model):
     kind = abi.MODEL_STVK_HENCKY_ISOTROPIC
 
 
+class StvkWithHencky(_Model):
+    """StvkWithHencky(E, nu), StvkWithHencky.cpp:10-20: the model of the
+    non-equilibrated (viscous) strain; same energy as StvkWithHenckyIsotropic."""
+    kind = abi.MODEL_STVK_HENCKY_ISOTROPIC
+
+
 class FixedCorotated(_Model):
     """Fixed corotated elasticity (Stomakhin et al. 2012); no reference counterpart."""
     kind = abi.MODEL_FIXED_COROTATED
@@ -174,6 +180,12 @@ class MpmParticleHandle:
         FractureSimulation::useNaiveDamage and sigmaF); needs NeoHookeanBorden."""
         self.sim._call("add_damage", self.lower, self.upper, abi.DAMAGE_RANKINE, float(sigma_f), float(residual_phase))
 
+    def addFElasticNonequilibratedBasedMpmForce(self, model, viscosity_d, viscosity_v):
+        """MpmParticleHandleBase::addFElasticNonequilibratedBasedMpmForce
+        (MpmParticleHandleBase.cpp:468-478): Fe starts at I, relaxes by the
+        viscous return map; the particles must already use StvkWithHenckyIsotropic."""
+        self.sim._call("add_viscoelastic", self.lower, self.upper, model.E, model.nu, float(viscosity_d), float(viscosity_v))
+
     def addPlasticity(self, model, plasticity):
         del model  # the model is the one attached with addFBasedMpmForce
         self.sim._call("add_plasticity", self.lower, self.upper, plasticity.kind,
@@ -212,6 +224,13 @@ class MpmSimulation:
         self.krylov_max_iterations = 20
         self.krylov_tolerance = 1.0
         self.linear_solve_tolerance_scale = 1.0
+        # ADMM integrator (AdmmSimulation members, AdmmSimulationFoam.h:47-70)
+        self.integrator = abi.NEWTON
+        self.admm_max_iterations = 100
+        self.rho_scale = 0.5
+        self.local_tolerance = 1e-8
+        self.global_tolerance = 1e-6
+        self.global_max_iteration = 10000
         self.last_stats = None
 
     # lifecycle
@@ -267,7 +286,23 @@ class MpmSimulation:
         s.krylov_max_iterations = self.krylov_max_iterations
         s.krylov_tolerance = self.krylov_tolerance
         s.linear_solve_tolerance_scale = self.linear_solve_tolerance_scale
+        s.integrator = self.integrator
+        s.admm_iterations = self.admm_max_iterations
+        s.admm_rho_scale = self.rho_scale
+        s.admm_local_tolerance = self.local_tolerance
+        s.admm_global_tolerance = self.global_tolerance
+        s.admm_global_max_iterations = self.global_max_iteration
         return s
+
+    def useAdmm(self, admm_max_iterations=None, rho_scale=None, local_tolerance=None, global_tolerance=None,
+                global_max_iteration=None):
+        """Substep with AdmmSimulation::admmStep instead of Newton."""
+        self.integrator = abi.ADMM
+        for k, v in (("admm_max_iterations", admm_max_iterations), ("rho_scale", rho_scale),
+                     ("local_tolerance", local_tolerance), ("global_tolerance", global_tolerance),
+                     ("global_max_iteration", global_max_iteration)):
+            if v is not None:
+                setattr(self, k, v)
 
     # stepping
     def advanceOneTimeStep(self, dt):
@@ -310,6 +345,15 @@ class MpmSimulation:
         c = np.empty(self.count)
         self._call("get_damage", ptr(c))
         return c
+
+    def getViscoelasticStrain(self):
+        Fe = np.empty((self.count, 3, 3))
+        self._call("get_viscoelastic_strain", ptr(Fe))
+        return Fe
+
+    def setViscoelasticStrain(self, Fe):
+        Fe = np.ascontiguousarray(Fe, dtype=np.float64).reshape(self.count, 3, 3)
+        self._call("set_viscoelastic_strain", ptr(Fe))
 
     def getPlasticState(self):
         n = self.count
