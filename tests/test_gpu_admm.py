@@ -66,6 +66,8 @@ def test_admm_mixed_precision_tracks_fp64_oracle(cuda_lib, oracle):
     """MIXED: FP32 operator coefficients and products in the global MINRES,
     FP64 local solves, state and reductions."""
     sims = [slab(None, precision="mixed", visco=True, grid_log2=8), slab(oracle, visco=True)]
+    for s in sims:
+        s.global_tolerance = 1e-9
     run(sims, 4)
     pg, po = sims[0].getParticles(), sims[1].getParticles()
     assert rel(pg["X"], po["X"]) < 1e-7
