@@ -84,6 +84,150 @@ def make_sim(x, v, precision, lib=None, model="hencky", layout="auto"):
     return sim
 
 
+# ----------------------------------------------------------------------------
+# Secondary workloads (the other benchmark configurations; `--workload`).  Each
+# prints its own JSON line; the default workload is the headline above.
+def _jitter_box(cells, dx, lo, ppc, seed):
+    rng = np.random.default_rng(seed)
+    grid = np.stack(np.meshgrid(*[np.arange(c) for c in cells], indexing="ij"), -1).reshape(-1, 3)
+    return (np.repeat(grid, ppc, 0) + rng.random((grid.shape[0] * ppc, 3))) * dx + np.asarray(lo, dtype=np.float64)
+
+
+def wl_cube32k(precision, lib=None, layout="auto", scale=1):
+    """Elastic cube: 16^3 cells x 8 ppc = 32,768 particles (seed 0), dx = 1/64,
+    min corner (0.375, 0.125, 0.375), fixed corotated E = 1e4, nu = 0.3,
+    rho = 1000, gravity, sticky ground y = 0.1, Newton-CG rel. tol 1e-7, dt = 1e-3."""
+    from ziran2019_b200 import abi, mpm
+    dx = 1.0 / 64
+    x = _jitter_box((16, 16, 16), dx, (0.375, 0.125, 0.375), 8, 0)
+    sim = mpm.MpmSimulation(dx, gravity=(0, -9.8, 0), precision=precision, grid_log2=7, layout=layout, lib=lib)
+    V0 = dx ** 3 / 8
+    h = sim.addParticles(x, np.zeros_like(x), 1000.0 * V0, V0)
+    h.addFBasedMpmForce(mpm.FixedCorotated(1e4, 0.3))
+    sim.addCollisionObject(mpm.AnalyticCollisionObject(mpm.HalfSpace((0, 0.1, 0), (0, 1, 0)), abi.STICKY))
+    sim.switchLinearSolver(abi.CG)
+    sim.newton_tolerance = 1e-7
+    sim.newton_max_iterations = 10
+    sim.krylov_max_iterations = 100
+    return sim, 1e-3, x.shape[0], {"workload": "config0-elastic-cube-32k", "model": "fixed corotated", "solver": "Newton-CG tol 1e-7"}
+
+
+def wl_admm500k(precision, lib=None, layout="auto", scale=1):
+    """Viscoelastic ADMM slab: 0.6 x 0.1 x 0.6 at dx = 1/120, 72 x 12 x 72 cells x 8
+    ppc = 497,664 particles (seed 3) over a static sticky sphere of radius 0.2;
+    StvkWithHenckyIsotropic E = 2e4, nu = 0.4 plus the non-equilibrated
+    StvkWithHencky with nu_d = nu_v = 2 mu tau, tau = 0.05 s; 20 ADMM
+    iterations, rho_scale 0.8, dt = 2e-3.  The slab starts touching the sphere
+    with the speed of a 0.3 m drop (sqrt(2 g 0.3) = 2.42 m/s) so every timed
+    substep deforms it.  scale > 1 takes every scale-th cell column in x and z
+    (CPU samples)."""
+    from ziran2019_b200 import abi, mpm
+    dx = 1.0 / 120
+    nx = 72 // scale
+    x = _jitter_box((nx, 12, nx), dx, (0.5 - nx * dx / 2, 0.5 + 2 * dx, 0.5 - nx * dx / 2), 8, 3)
+    sim = mpm.MpmSimulation(dx, gravity=(0, -9.8, 0), precision=precision, grid_log2=8, layout=layout, lib=lib)
+    V0 = dx ** 3 / 8
+    v = np.tile([0.0, -np.sqrt(2 * 9.8 * 0.3), 0.0], (x.shape[0], 1))
+    h = sim.addParticles(x, v, 1000.0 * V0, V0)
+    E, nu, tau = 2e4, 0.4, 0.05
+    h.addFBasedMpmForce(mpm.StvkWithHenckyIsotropic(E, nu))
+    nvis = 2 * E / (2 * (1 + nu)) * tau
+    h.addFElasticNonequilibratedBasedMpmForce(mpm.StvkWithHencky(E, nu), nvis, nvis)
+    sim.addCollisionObject(mpm.AnalyticCollisionObject(mpm.Sphere((0.5, 0.3, 0.5), 0.2), abi.STICKY))
+    sim.addCollisionObject(mpm.AnalyticCollisionObject(mpm.HalfSpace((0, 3 * dx, 0), (0, 1, 0)), abi.STICKY))
+    sim.useAdmm(admm_max_iterations=20, rho_scale=0.8, global_tolerance=1e-8, local_tolerance=1e-8)
+    return sim, 2e-3, x.shape[0], {"workload": "config2-viscoelastic-admm-500k", "model": "hencky + viscoelastic Fe",
+                                   "solver": "ADMM 20 iterations, MINRES abs tol 1e-8"}
+
+
+def wl_damage2m(precision, lib=None, layout="auto", scale=1):
+    """Notched slab 1.0 x 0.25 x 0.1 with a 0.1-long, one-cell-wide edge notch at
+    mid-length, 8 ppc at dx = 1/216 (216 x 54 x 22 cells, about 2.05M
+    particles, seed 4); the end faces are held by sticky boxes moving apart at
+    +-0.5 m/s; NeoHookeanBorden E = 1e5, nu = 0.3 with Rankine damage sigma_F =
+    1e3 Pa, k = 1e-3; dt = 2e-4, no gravity.  scale > 1 keeps every scale-th
+    cell layer in z (CPU samples)."""
+    from ziran2019_b200 import abi, mpm
+    dx = 1.0 / 216
+    nx, ny, nz = 216, 54, max(1, 22 // scale)
+    lo = np.array([0.25, 0.5, 0.5])
+    x = _jitter_box((nx, ny, nz), dx, lo, 8, 4)
+    rel = (x - lo) / dx
+    notch = (np.abs(rel[:, 0] - nx / 2) < 0.5) & (rel[:, 1] < 0.1 / dx)
+    x = x[~notch]
+    sim = mpm.MpmSimulation(dx, gravity=(0, 0, 0), precision=precision, grid_log2=9, layout=layout, lib=lib)
+    V0 = dx ** 3 / 8
+    h = sim.addParticles(x, np.zeros_like(x), 1000.0 * V0, V0)
+    h.addFBasedMpmForce(mpm.NeoHookeanBorden(1e5, 0.3))
+    h.addRankineDamage(1e3, residual_phase=1e-3)
+    hi = lo + np.array([nx, ny, nz]) * dx
+    grip = 3 * dx
+    for side, vel in ((0, -0.5), (1, 0.5)):
+        a = [lo[0] - 4 * dx if side == 0 else hi[0] - grip, lo[1] - 4 * dx, lo[2] - 4 * dx]
+        b = [lo[0] + grip if side == 0 else hi[0] + 4 * dx, hi[1] + 4 * dx, hi[2] + 4 * dx]
+        box = mpm.AnalyticCollisionObject(mpm.AxisAlignedAnalyticBox(a, b), abi.STICKY)
+        box.setTranslation((0.0, 0.0, 0.0), (vel, 0.0, 0.0))
+        sim.addCollisionObject(box)
+    return sim, 2e-4, x.shape[0], {"workload": "config3-rankine-notched-slab-2m", "model": "neo-Hookean + Rankine damage",
+                                   "solver": "MINRES, Newton 3 x Krylov 20 (reference defaults)"}
+
+
+WORKLOADS = {"cube32k": wl_cube32k, "admm500k": wl_admm500k, "damage2m": wl_damage2m}
+
+
+def run_workload(args, world, rank):
+    """One secondary workload: mixed and FP64 GPU substeps/s, position error
+    of mixed against FP64 after the timed steps, and the oracle on a sample."""
+    import torch
+
+    from ziran2019_b200 import build
+    build.build()
+    fn = WORKLOADS[args.workload]
+    sims, meta = {}, None
+    for p in ("fp64", "mixed"):
+        sims[p], dt, P, meta = fn(p, layout="444")
+    for p in sims:
+        for _ in range(args.warmup):
+            rc = sims[p].advanceOneTimeStep(dt)
+            assert rc == 0, (p, rc, sims[p].last_stats)
+    ms64, st64 = timed_steps(sims["fp64"], args.steps, world, dt=dt)
+    clocks = Clocks(int(os.environ.get("LOCAL_RANK", "0")))
+    clocks.start()
+    ms_mx, st_mx = timed_steps(sims["mixed"], args.steps, world, dt=dt)
+    clk = clocks.stop()
+    x64 = sims["fp64"].getParticles()["X"]
+    xmx = sims["mixed"].getParticles()["X"]
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        from oracle import zoracle
+        scale = {"cube32k": 1, "admm500k": 4, "damage2m": 11}[args.workload]
+        osim, _, Pc, _ = fn("fp64", lib=zoracle.lib(), scale=scale)
+        for _ in range(args.warmup):
+            osim.advanceOneTimeStep(dt)
+        t0 = time.perf_counter()
+        for _ in range(args.cpu_steps):
+            osim.advanceOneTimeStep(dt)
+        secs = time.perf_counter() - t0
+        cpu = {"value": args.cpu_steps / secs * Pc / P, "unit": "substeps/s", "cores": os.cpu_count(), "kind": "port",
+               "sample": f"{args.cpu_steps} substep(s) of a {Pc}-particle cut of the workload after {args.warmup} warm-up, oracle port, "
+                         f"{secs:.1f} s, scaled by {Pc}/{P}"}
+    if rank == 0:
+        value = world * args.steps / (ms_mx / 1e3)
+        fp64_value = world * args.steps / (ms64 / 1e3)
+        line = {"metric": f"implicit MPM substeps/sec, {meta['workload']}", "value": value, "unit": "substeps/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_mx / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "mixed (fp32 operator, fp64 state)", "data": "synthetic",
+                "config": dict(meta, particles=P, dt=dt), "particles_substeps_per_s": value * P,
+                "fp64_value": fp64_value, "mixed_over_fp64": value / fp64_value,
+                "rel_pos_err_vs_fp64": float(np.linalg.norm(xmx - x64) / np.linalg.norm(x64)),
+                "accuracy_steps": args.warmup + args.steps,
+                "iterations_per_step": [st_mx[-1]["newton_iterations"], st_mx[-1]["krylov_iterations"]],
+                "gpu_launches": sum(s["kernel_launches"] for s in st_mx), "cpu_baseline": cpu, "clocks": clk}
+        print(json.dumps(line), flush=True)
+    for s in sims.values():
+        s.close()
+
+
 class Clocks:
     """nvidia-smi samples during the timed region."""
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
@@ -138,17 +282,18 @@ def dist_setup():
 
 
 def barrier_max(value, world):
-    """Barrier and max over ranks."""
+    """Barrier and max over ranks (the slowest replica's time)."""
     if world == 1:
         return value
     import torch
     import torch.distributed as dist
-    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([value], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
 
-def timed_steps(sim, steps, world, profile=False):
+def timed_steps(sim, steps, world, profile=False, dt=None):
     """Runs `steps` substeps between CUDA events on the library stream; returns ms and stats."""
     import ctypes
 
@@ -166,7 +311,7 @@ def timed_steps(sim, steps, world, profile=False):
     e0.record(stream)
     stats = []
     for _ in range(steps):
-        rc = sim.advanceOneTimeStep(DT)
+        rc = sim.advanceOneTimeStep(DT if dt is None else dt)
         if rc not in (abi.OK, abi.CFL_VIOLATION):
             raise RuntimeError(f"substep status {rc}")
         stats.append(sim.last_stats)
@@ -225,12 +370,17 @@ def main():
     ap.add_argument("--boxes", type=int, default=4, help="boxes of 250k particles (profiling runs use fewer)")
     ap.add_argument("--fp64-layout", default="444", choices=["444", "auto"],
                     help="page layout of the FP64 substep: 444 = same as the mixed run (only precision differs)")
+    ap.add_argument("--workload", default="config1", choices=["config1"] + sorted(WORKLOADS),
+                    help="config1: the headline 1M-particle workload; others print their own line")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     world, rank = dist_setup()
     if args.impl == "reference":
         run_reference(args, world, rank)
+        return
+    if args.workload != "config1":
+        run_workload(args, world, rank)
         return
 
     import torch

@@ -274,6 +274,29 @@ int zmpm_get_stream(zmpm_ctx* ctx, void** stream);
    scopes, Lib/Ziran/CS/Util/Timer.h:34-58, as device timers). */
 int zmpm_set_profiling(zmpm_ctx* ctx, int32_t on);
 
+/* ------------------------------------------------------------ adjoint ------ */
+/* Reverse mode of one implicit substep (no reference counterpart: ziran2019 has
+   no differentiation).  The context holds the state s_n; the call runs the
+   substep forward from s_n (the context then holds s_{n+1}) and maps the
+   gradients of a scalar loss with respect to s_{n+1} to gradients with respect
+   to s_n in place: gx, gv [P][3], gC, gF [P][3][3] in particle-index order
+   (NULL means zero).  gE [P] accumulates dL/dE_p, the Young's modulus at fixed
+   Poisson ratio (mu and lambda scale with E).  The derivative is the hand-written
+   adjoint of P2G, of the converged Newton solution through the implicit
+   function theorem, and of G2P (quadratic B-spline weights, their gradients and
+   Hessians): the adjoint system (M + dt^2 K) lambda = g uses the substep's own
+   symmetric Hessian, solved in FP64 by CG to the relative `adjoint_tolerance`.
+   Binning is held fixed (piecewise constant in x).  Returns ZMPM_UNSUPPORTED
+   for plasticity, damage, viscoelastic particles or the ADMM integrator. */
+int zmpm_adjoint_substep(zmpm_ctx* ctx, double dt, const zmpm_solver* s, double adjoint_tolerance, double* gx, double* gv, double* gC,
+    double* gF, double* gE, zmpm_stats* stats);
+
+/* Device-resident checkpoints of the full particle state and time (for
+   checkpointed adjoint rollouts).  slot >= 0; a slot is allocated on first
+   save and kept until zmpm_destroy. */
+int zmpm_checkpoint_save(zmpm_ctx* ctx, int32_t slot);
+int zmpm_checkpoint_load(zmpm_ctx* ctx, int32_t slot);
+
 /* Default solver settings of the reference (MpmSimulationBase.cpp:51,
    BackwardEuler.h:56-62, LinearSolver.h:24). */
 void zmpm_default_solver(zmpm_solver* s, int32_t linear_solver, int32_t precision);

@@ -35,6 +35,7 @@
 #include <memory>
 #include <new>
 #include <string>
+#include <map>
 #include <vector>
 
 #include <parallel/algorithm>
@@ -1348,6 +1349,14 @@ struct Sim {
     std::vector<T> admm_y, admm_omega, admm_last_dv;     // ADMM state carried across substeps: [P][18], [P][2], [P][3]
     std::vector<Scratch<T>> scratch;
     std::vector<M3<T>> gradV, stress;
+    struct Checkpoint {
+        std::vector<T> X, V, Cm, F, Fe, y, omega, lastdv;
+        std::vector<Model<T>> model;
+        std::vector<Plastic<T>> plastic;
+        std::vector<Damage<T>> damage;
+        double time = 0;
+    };
+    std::map<int, Checkpoint> checkpoints;
     std::vector<Collider<T>> colliders;
 
     // binning
@@ -1894,6 +1903,227 @@ struct Sim {
             for (int64_t i = 0; i < 3 * N; ++i) dv[i] += step[i];
         }
         return false;
+    }
+
+    // --------------------------------------------------------- adjoint --
+    // Reverse mode of one implicit substep (no reference counterpart).  With
+    // v* = vn + dv the converged Newton solution of
+    //   G(v*) = M v* - q - dt M g + dt sum_p V0 P(F_p) Fn_p^T grad w_ip = 0 (free nodes),
+    //   F_p = (I + dt sum_j v*_j grad w_jp^T) Fn_p,  q_i = sum_p w_ip m_p (v_p + C_p (x_i - x_p)),
+    // the implicit function theorem gives dL/dtheta = -lambda^T dG/dtheta with
+    // (M + dt^2 K) lambda = P dL/dv* (the Newton Hessian, projected).  Binning
+    // (base nodes) is held fixed.
+
+    // Weights, gradients and Hessians of the quadratic B-spline stencil.
+    template <class F_>
+    void iterateKernel2(const Spline<T>& sp, u64 base, F_&& f) const
+    {
+        const T idx = sp.one_over_dx, idx2 = sp.one_over_dx * sp.one_over_dx;
+        const T dd[3] = { T(1), T(-2), T(1) };
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j)
+                for (int k = 0; k < 3; ++k) {
+                    T Nx = sp.w[0][i], Ny = sp.w[1][j], Nz = sp.w[2][k];
+                    T Dx = sp.dw[0][i], Dy = sp.dw[1][j], Dz = sp.dw[2][k];
+                    T w = Nx * Ny * Nz;
+                    T dw[3] = { Dx * Ny * Nz * idx, Nx * Dy * Nz * idx, Nx * Ny * Dz * idx };
+                    T H[3][3];
+                    H[0][0] = dd[i] * Ny * Nz * idx2;
+                    H[1][1] = Nx * dd[j] * Nz * idx2;
+                    H[2][2] = Nx * Ny * dd[k] * idx2;
+                    H[0][1] = H[1][0] = Dx * Dy * Nz * idx2;
+                    H[0][2] = H[2][0] = Dx * Ny * Dz * idx2;
+                    H[1][2] = H[2][1] = Nx * Dy * Dz * idx2;
+                    int node[3] = { sp.base[0] + i, sp.base[1] + j, sp.base[2] + k };
+                    G& g = at(mask.packed_add(base, mask.stencil[9 * i + 3 * j + k]));
+                    f(node, w, dw, H, g);
+                }
+    }
+
+    static T youngsModulus(const Model<T>& c)
+    {
+        if (c.kind == ZMPM_MODEL_NEOHOOKEAN_BORDEN) {
+            T lam = c.kappa - T(0.666666) * c.mu;
+            return c.mu * (3 * lam + 2 * c.mu) / (lam + c.mu);
+        }
+        return c.mu * (3 * c.lambda + 2 * c.mu) / (c.lambda + c.mu);
+    }
+
+    int adjointSubstep(double dt_in, const zmpm_solver& s, double tol, double* gx, double* gv, double* gC, double* gF, double* gE,
+        zmpm_stats& st)
+    {
+        for (int64_t i = 0; i < P; ++i)
+            if (plastic[i].kind != ZMPM_PLASTIC_NONE || damage[i].kind != ZMPM_DAMAGE_NONE || visco[i].on) {
+                err = "the adjoint supports elastic particles only";
+                return ZMPM_UNSUPPORTED;
+            }
+        if (s.integrator != ZMPM_NEWTON) {
+            err = "the adjoint differentiates the Newton substep";
+            return ZMPM_UNSUPPORTED;
+        }
+        const std::vector<T> X0 = X, V0v = V, C0 = Cm, F0 = F;
+        int rc = substep(dt_in, s, st);
+        if (rc != ZMPM_OK && rc != ZMPM_CFL_VIOLATION) return rc;
+        // the operators below evaluate at the pre-substep positions; keep s_{n+1}
+        const std::vector<T> X1 = X, F1 = F;
+        X = X0;
+        // the Hessian and stresses at the converged solution
+        updateState(dv);
+        const T dtt = dt;
+        std::vector<T> vstar(3 * N);
+        for (int64_t n = 0; n < N; ++n)
+            for (int d = 0; d < 3; ++d) vstar[3 * n + d] = vn[3 * n + d] + dv[3 * n + d];
+        auto in3 = [&](const double* a, int64_t i, int d) { return a ? (T)a[3 * i + d] : T(0); };
+        auto in9 = [&](const double* a, int64_t i) {
+            M3<T> m = M3<T>::zero();
+            if (a)
+                for (int q = 0; q < 9; ++q) m.a[q / 3][q % 3] = (T)a[9 * i + q];
+            return m;
+        };
+        const T D_inv = 4 / (dx * dx);
+        std::vector<T> xbar(3 * P), vbar(3 * P, 0), Cbar(9 * P, 0), Fbar(9 * P, 0);
+        // (1) G2P: v_p' = sum w v*, C_p' = D^-1 sum w v* (x_i - x_p)^T,
+        //     F_p' = (I + dt grad v*) Fn, x_p' = x_p + dt v_p'
+        std::vector<T> vsbar(3 * N, 0);
+        coloredGroups([&](int i) {
+            const T* xp = &X0[3 * i];
+            T vt[3], xb[3];
+            for (int d = 0; d < 3; ++d) {
+                vt[d] = in3(gv, i, d) + dtt * in3(gx, i, d);
+                xb[d] = in3(gx, i, d);
+            }
+            M3<T> Cb = in9(gC, i), Fb = in9(gF, i), Fn_ = load9(F0, i);
+            M3<T> FnFbT = mulT(Fn_, Fb); // Fn gF^T
+            M3<T> gvs = M3<T>::zero();
+            Spline<T> sp(xp, dx);
+            iterateKernel2(sp, base_offset[i], [&](const int node[3], T w, const T* dw, const T H[3][3], G& g) {
+                const int64_t id = g.idx;
+                if (id < 0) return;
+                const T* v = &vstar[3 * id];
+                T xi[3];
+                for (int d = 0; d < 3; ++d) xi[d] = node[d] * dx - xp[d];
+                // Fb Fn^T grad w
+                T fd[3], cx[3];
+                for (int r = 0; r < 3; ++r) {
+                    fd[r] = 0;
+                    cx[r] = 0;
+                    for (int c = 0; c < 3; ++c) {
+                        T FbFnT = Fb.a[r][0] * Fn_.a[c][0] + Fb.a[r][1] * Fn_.a[c][1] + Fb.a[r][2] * Fn_.a[c][2];
+                        fd[r] += FbFnT * dw[c];
+                        cx[r] += Cb.a[r][c] * xi[c];
+                    }
+                }
+                for (int d = 0; d < 3; ++d) vsbar[3 * id + d] += w * vt[d] + D_inv * w * cx[d] + dtt * fd[d];
+                T vdot = v[0] * vt[0] + v[1] * vt[1] + v[2] * vt[2];
+                T vCx = v[0] * cx[0] + v[1] * cx[1] + v[2] * cx[2];
+                T CTv[3], q[3];
+                for (int c = 0; c < 3; ++c) CTv[c] = Cb.a[0][c] * v[0] + Cb.a[1][c] * v[1] + Cb.a[2][c] * v[2];
+                for (int r = 0; r < 3; ++r) q[r] = FnFbT.a[r][0] * v[0] + FnFbT.a[r][1] * v[1] + FnFbT.a[r][2] * v[2];
+                for (int d = 0; d < 3; ++d) {
+                    xb[d] += vdot * dw[d] + D_inv * (vCx * dw[d] - w * CTv[d]);
+                    xb[d] += dtt * (H[d][0] * q[0] + H[d][1] * q[1] + H[d][2] * q[2]);
+                }
+                for (int r = 0; r < 3; ++r)
+                    for (int c = 0; c < 3; ++c) gvs.a[r][c] += v[r] * dw[c];
+            });
+            M3<T> A = M3<T>::identity();
+            for (int r = 0; r < 3; ++r)
+                for (int c = 0; c < 3; ++c) A.a[r][c] += dtt * gvs.a[r][c];
+            store9(Fbar, i, Tmul(A, Fb));
+            for (int d = 0; d < 3; ++d) xbar[3 * i + d] = xb[d];
+        });
+        // (2) adjoint solve (M + dt^2 K) lambda = P vsbar, CG with the Newton operator
+        project(vsbar);
+        std::vector<T> lam(3 * N, 0);
+        int kit = cg(lam, vsbar, (T)tol, T(1e300), 100000);
+        st.krylov_iterations += kit;
+        // (3) grid adjoints: qbar = lambda, mbar = -lambda . (v* - dt g)
+        std::vector<T> mbar(N);
+        for (int64_t n = 0; n < N; ++n) {
+            T a = 0;
+            for (int d = 0; d < 3; ++d) a += lam[3 * n + d] * (vstar[3 * n + d] - dtt * gravity[d]);
+            mbar[n] = -a;
+        }
+        // (4) particle adjoints of the force term, of P2G and of E
+#pragma omp parallel for schedule(static)
+        for (int64_t i = 0; i < P; ++i) {
+            const T* xp = &X0[3 * i];
+            Spline<T> sp(xp, dx);
+            M3<T> Lam = M3<T>::zero(), Vs = M3<T>::zero();
+            iterateKernel2(sp, base_offset[i], [&](const int*, T, const T* dw, const T (*)[3], G& g) {
+                if (g.idx < 0) return;
+                for (int r = 0; r < 3; ++r)
+                    for (int c = 0; c < 3; ++c) {
+                        Lam.a[r][c] += lam[3 * g.idx + r] * dw[c];
+                        Vs.a[r][c] += vstar[3 * g.idx + r] * dw[c];
+                    }
+            });
+            M3<T> Fn_ = load9(F0, i);
+            M3<T> Fb = load9(Fbar, i);
+            T xb[3] = { xbar[3 * i], xbar[3 * i + 1], xbar[3 * i + 2] };
+            T vb[3] = { 0, 0, 0 };
+            M3<T> Cb = M3<T>::zero();
+            if (model[i].kind != ZMPM_MODEL_NONE) {
+                M3<T> A = M3<T>::identity();
+                for (int r = 0; r < 3; ++r)
+                    for (int c = 0; c < 3; ++c) A.a[r][c] += dtt * Vs.a[r][c];
+                M3<T> Fp = mul(A, Fn_);
+                Scratch<T> sc;
+                updateScratch(model[i], Fp, sc);
+                M3<T> Pp = firstPiola(model[i], sc);
+                M3<T> LF = mul(Lam, Fn_);
+                M3<T> dPL = firstPiolaDifferential(model[i], sc, LF);
+                T c0 = dtt * vol[i];
+                M3<T> t1 = Tmul(A, dPL), t2 = Tmul(Lam, Pp);
+                for (int r = 0; r < 3; ++r)
+                    for (int c = 0; c < 3; ++c) Fb.a[r][c] -= c0 * (t1.a[r][c] + t2.a[r][c]);
+                if (gE) gE[i] -= (double)(c0 * contract(Pp, LF) / youngsModulus(model[i]));
+                M3<T> Q1 = mulT(dPL, Fn_), Q2 = mulT(Pp, Fn_);
+                iterateKernel2(sp, base_offset[i], [&](const int*, T, const T*, const T H[3][3], G& g) {
+                    if (g.idx < 0) return;
+                    const T* v = &vstar[3 * g.idx];
+                    const T* l = &lam[3 * g.idx];
+                    T a[3], b[3];
+                    for (int c = 0; c < 3; ++c) {
+                        a[c] = Q1.a[0][c] * v[0] + Q1.a[1][c] * v[1] + Q1.a[2][c] * v[2];
+                        b[c] = Q2.a[0][c] * l[0] + Q2.a[1][c] * l[1] + Q2.a[2][c] * l[2];
+                    }
+                    for (int d = 0; d < 3; ++d)
+                        xb[d] -= c0 * (dtt * (H[d][0] * a[0] + H[d][1] * a[1] + H[d][2] * a[2]) + (H[d][0] * b[0] + H[d][1] * b[1] + H[d][2] * b[2]));
+                });
+            }
+            // P2G: q_i = sum w m (v + C (x_i - x_p)), m_i = sum w m
+            const T mp = mass[i];
+            M3<T> Cp = load9(C0, i);
+            const T* vp = &V0v[3 * i];
+            iterateKernel2(sp, base_offset[i], [&](const int node[3], T w, const T* dw, const T (*)[3], G& g) {
+                if (g.idx < 0) return;
+                const T* l = &lam[3 * g.idx];
+                T xi[3];
+                for (int d = 0; d < 3; ++d) xi[d] = node[d] * dx - xp[d];
+                T u[3];
+                for (int r = 0; r < 3; ++r) u[r] = vp[r] + Cp.a[r][0] * xi[0] + Cp.a[r][1] * xi[1] + Cp.a[r][2] * xi[2];
+                T lu = l[0] * u[0] + l[1] * u[1] + l[2] * u[2];
+                for (int d = 0; d < 3; ++d) {
+                    vb[d] += w * mp * l[d];
+                    T CTl = Cp.a[0][d] * l[0] + Cp.a[1][d] * l[1] + Cp.a[2][d] * l[2];
+                    xb[d] += mp * lu * dw[d] - w * mp * CTl + mbar[g.idx] * mp * dw[d];
+                }
+                for (int r = 0; r < 3; ++r)
+                    for (int c = 0; c < 3; ++c) Cb.a[r][c] += w * mp * l[r] * xi[c];
+            });
+            for (int d = 0; d < 3; ++d) {
+                if (gx) gx[3 * i + d] = (double)xb[d];
+                if (gv) gv[3 * i + d] = (double)vb[d];
+            }
+            for (int q = 0; q < 9; ++q) {
+                if (gC) gC[9 * i + q] = (double)Cb.a[q / 3][q % 3];
+                if (gF) gF[9 * i + q] = (double)Fb.a[q / 3][q % 3];
+            }
+        }
+        X = X1;
+        F = F1;
+        return rc;
     }
 
     // ------------------------------------------------------------ ADMM --
@@ -2589,6 +2819,61 @@ int zoracle_viscous_return(double E, double nu, double vd, double vv, double dt,
     for (int q = 0; q < 9; ++q) m.a[q / 3][q % 3] = F[q];
     zo::viscousReturn(v, dt, m);
     for (int q = 0; q < 9; ++q) F[q] = m.a[q / 3][q % 3];
+    return ZMPM_OK;
+}
+
+int zoracle_adjoint_substep(Ctx* c, double dt, const zmpm_solver* s, double tol, double* gx, double* gv, double* gC, double* gF,
+    double* gE, zmpm_stats* st)
+{
+    if (!c || !s || !(dt > 0)) return ZMPM_BAD_ARG;
+    zmpm_stats local;
+    if (!st) st = &local;
+    int rc;
+    DISPATCH(c, { rc = S.adjointSubstep(dt, *s, tol, gx, gv, gC, gF, gE, *st); });
+    return rc;
+}
+
+int zoracle_checkpoint_save(Ctx* c, int32_t slot)
+{
+    if (!c || slot < 0) return ZMPM_BAD_ARG;
+    DISPATCH(c, {
+        auto& k = S.checkpoints[slot];
+        k.X = S.X;
+        k.V = S.V;
+        k.Cm = S.Cm;
+        k.F = S.F;
+        k.Fe = S.Fe;
+        k.y = S.admm_y;
+        k.omega = S.admm_omega;
+        k.lastdv = S.admm_last_dv;
+        k.model = S.model;
+        k.plastic = S.plastic;
+        k.damage = S.damage;
+        k.time = S.time;
+    });
+    return ZMPM_OK;
+}
+
+int zoracle_checkpoint_load(Ctx* c, int32_t slot)
+{
+    if (!c) return ZMPM_BAD_ARG;
+    DISPATCH(c, {
+        auto it = S.checkpoints.find(slot);
+        if (it == S.checkpoints.end() || it->second.X.size() != S.X.size()) return ZMPM_BAD_ARG;
+        auto& k = it->second;
+        S.X = k.X;
+        S.V = k.V;
+        S.Cm = k.Cm;
+        S.F = k.F;
+        S.Fe = k.Fe;
+        S.admm_y = k.y;
+        S.admm_omega = k.omega;
+        S.admm_last_dv = k.lastdv;
+        S.model = k.model;
+        S.plastic = k.plastic;
+        S.damage = k.damage;
+        S.time = k.time;
+    });
     return ZMPM_OK;
 }
 

@@ -151,6 +151,10 @@ _SIGS = {
     "get_initial_dv": (C.c_int, [C.c_void_p, c_double_p, c_int32_p]),
     "residual": (C.c_int, [C.c_void_p, c_double_p, c_double_p, c_double_p]),
     "multiply": (C.c_int, [C.c_void_p, c_double_p, c_double_p, C.c_int32]),
+    "adjoint_substep": (C.c_int, [C.c_void_p, C.c_double, C.POINTER(Solver), C.c_double, c_double_p, c_double_p, c_double_p,
+                                  c_double_p, c_double_p, C.POINTER(Stats)]),
+    "checkpoint_save": (C.c_int, [C.c_void_p, C.c_int32]),
+    "checkpoint_load": (C.c_int, [C.c_void_p, C.c_int32]),
 }
 
 # entry points exported by the product library only

@@ -433,9 +433,12 @@ int zmpm_destroy(zmpm_ctx* ctx)
         &ctx->frac, &ctx->stress, &ctx->dstress, &ctx->keys, &ctx->keys_alt, &ctx->flags_i32, &ctx->scan_i32, &ctx->scan_scr, &ctx->radix_scr, &ctx->group_start,
         &ctx->group_page, &ctx->group_nbr, &ctx->emit_flag, &ctx->emit_scan, &ctx->page_first, &ctx->page_block, &ctx->block_page,
         &ctx->block_index, &ctx->gm, &ctx->gmv, &ctx->vn, &ctx->dv, &ctx->vstar, &ctx->facc, &ctx->res, &ctx->proj, &ctx->collided,
-        &ctx->node_idx, &ctx->red, &ctx->scal, &ctx->counters, &ctx->dcolliders };
+        &ctx->node_idx, &ctx->red, &ctx->scal, &ctx->counters, &ctx->dcolliders, &ctx->adm_F, &ctx->adm_gvn, &ctx->adm_B, &ctx->adm_pre,
+        &ctx->adm_rhs, &ctx->adm_w, &ctx->adj };
     for (DBuf* b : bufs) b->release();
     for (auto& b : ctx->kv) b.release();
+    for (auto* v : { &ctx->ckpt_pd, &ctx->ckpt_pi, &ctx->ckpt_sid })
+        for (auto& b : *v) b.release();
     ctx->stage.release();
     for (cudaEvent_t e : ctx->hvp_ev) cudaEventDestroy(e);
     if (ctx->graph_exec) cudaGraphExecDestroy(ctx->graph_exec);
@@ -801,6 +804,175 @@ int zmpm_substep(zmpm_ctx* ctx, double dt, const zmpm_solver* s, zmpm_stats* st)
     }
     if (st->status_flags & 1) return ZMPM_NAN_DETECTED;
     return st->cfl_violation ? ZMPM_CFL_VIOLATION : ZMPM_OK;
+}
+
+// ---------------------------------------------------------------- adjoint --
+int zmpm_adjoint_substep(zmpm_ctx* ctx, double dt, const zmpm_solver* s, double tol, double* gx, double* gv, double* gC, double* gF,
+    double* gE, zmpm_stats* st)
+{
+    if (!ctx || !s || !(dt > 0) || !(tol > 0) || s->newton_max_iterations < 0 || s->krylov_max_iterations < 0) return ZMPM_BAD_ARG;
+    if (s->integrator != ZMPM_NEWTON) {
+        ctx->err = "the adjoint differentiates the Newton substep";
+        return ZMPM_UNSUPPORTED;
+    }
+    for (int64_t i = 0; i < ctx->P; ++i)
+        if (ctx->hpkind[i] != ZMPM_PLASTIC_NONE || ctx->hdamage[i] != ZMPM_DAMAGE_NONE || ctx->hvisco[i]) {
+            ctx->err = "the adjoint supports elastic particles only";
+            return ZMPM_UNSUPPORTED;
+        }
+    cudaSetDevice(ctx->device);
+    zmpm_stats local;
+    if (!st) st = &local;
+    std::memset(st, 0, sizeof(*st));
+    const int64_t launches0 = g_kernel_launches;
+    int rc = upload(ctx);
+    if (rc) return rc;
+    ctx->dt = dt;
+    ctx->implicit_ready = false;
+    rc = run_binning(ctx);
+    if (rc) return rc;
+    const int64_t P = ctx->P, cap = ctx->Pcap;
+    cudaStream_t sm = ctx->stream;
+    ZMPM_CUDA(ctx->adj.ensure((size_t)AJ_FIELDS * cap * sizeof(double)));
+    double* aj = ctx->adj.as<double>();
+    // the state before the substep (pool fields x, v, C, F are the first 24) in slot order
+    ZMPM_CUDA(cudaMemcpyAsync(aj, ctx->pd.p, 24 * cap * sizeof(double), cudaMemcpyDeviceToDevice, sm));
+    ZMPM_CUDA(cudaMemsetAsync(aj + AJ_GX * cap, 0, 24 * cap * sizeof(double), sm));
+    if (P) {
+        ZMPM_CUDA(ctx->stage.ensure(25 * P * sizeof(double))); // 24 gradient components + dL/dE
+        double* stg = ctx->stage.as<double>();
+        const double* src[4] = { gx, gv, gC, gF };
+        const int nc[4] = { 3, 3, 9, 9 }, fld[4] = { AJ_GX, AJ_GV, AJ_GC, AJ_GF };
+        int64_t off = 0;
+        for (int a = 0; a < 4; ++a) {
+            if (!src[a]) continue;
+            ZMPM_CUDA(cudaMemcpyAsync(stg + off, src[a], nc[a] * P * sizeof(double), cudaMemcpyHostToDevice, sm));
+            k_fields_from_host<<<(unsigned)((P + 255) / 256), 256, 0, sm>>>(stg + off, nc[a], P, cap, ctx->slot_of_id.as<int32_t>(),
+                aj + (int64_t)fld[a] * cap);
+            ++g_kernel_launches;
+            off += nc[a] * P;
+        }
+    }
+    // forward: P2G, Newton, the Hessian at the converged solution, G2P
+    rc = run_p2g(ctx, true);
+    if (rc) return rc;
+    rc = run_newton(ctx, *s);
+    if (rc) return rc;
+    rc = launch_update(ctx, false);
+    if (rc) return rc;
+    rc = run_g2p(ctx);
+    if (rc) return rc;
+    SolverScalars hs;
+    ZMPM_CUDA(cudaMemcpyAsync(&hs, ctx->scal.p, sizeof(hs), cudaMemcpyDeviceToHost, sm));
+    ZMPM_CUDA(cudaStreamSynchronize(sm));
+    if (ctx->graph_exec) {
+        cudaGraphExecDestroy(ctx->graph_exec);
+        ctx->graph_exec = nullptr;
+    }
+    if (ctx->graph_used) g_kernel_launches += 7 * (int64_t)hs.nit + (ctx->hvp_fused ? 5 : 6) * (int64_t)hs.krylov_bodies;
+    st->newton_iterations = hs.newton_iters;
+    st->newton_converged = hs.converged;
+    st->newton_residual_initial = hs.res_initial;
+    st->newton_residual_final = hs.res_final;
+    // reverse: G2P, the adjoint solve, force / P2G / E
+    const int64_t nn = ctx->B * ctx->npb();
+    ZMPM_CUDA(cudaMemsetAsync(ctx->res.p, 0, 3 * nn * sizeof(double), sm));
+    rc = launch_adj_g2p(ctx, ctx->res.as<double>());
+    if (rc) return rc;
+    rc = run_adjoint_solve(ctx, tol, 100000);
+    if (rc) return rc;
+    rc = launch_adj_particle(ctx, ctx->kv[0].as<double>());
+    if (rc) return rc;
+    SolverScalars ha;
+    ZMPM_CUDA(cudaMemcpyAsync(&ha, ctx->scal.p, sizeof(ha), cudaMemcpyDeviceToHost, sm));
+    // gradients back to particle-index order
+    if (P) {
+        double* stg = ctx->stage.as<double>();
+        double* dst[4] = { gx, gv, gC, gF };
+        const int nc[4] = { 3, 3, 9, 9 }, fld[4] = { AJ_OX, AJ_OV, AJ_OC, AJ_OF };
+        int64_t off = 0;
+        for (int a = 0; a < 4; ++a) {
+            if (!dst[a]) continue;
+            k_fields_to_host<<<(unsigned)((P + 255) / 256), 256, 0, sm>>>(stg + off, nc[a], P, cap, ctx->slot_of_id.as<int32_t>(),
+                aj + (int64_t)fld[a] * cap);
+            ++g_kernel_launches;
+            ZMPM_CUDA(cudaMemcpyAsync(dst[a], stg + off, nc[a] * P * sizeof(double), cudaMemcpyDeviceToHost, sm));
+            off += nc[a] * P;
+        }
+        if (gE) {
+            std::vector<double> e(P);
+            k_fields_to_host<<<(unsigned)((P + 255) / 256), 256, 0, sm>>>(stg + off, 1, P, cap, ctx->slot_of_id.as<int32_t>(), aj + AJ_OE * cap);
+            ++g_kernel_launches;
+            ZMPM_CUDA(cudaMemcpyAsync(e.data(), stg + off, P * sizeof(double), cudaMemcpyDeviceToHost, sm));
+            ZMPM_CUDA(cudaStreamSynchronize(sm));
+            for (int64_t i = 0; i < P; ++i) gE[i] += e[i];
+        }
+    }
+    ZMPM_CUDA(cudaStreamSynchronize(sm));
+    DevCounters hc;
+    ZMPM_CUDA(cudaMemcpy(&hc, ctx->counters.p, sizeof(hc), cudaMemcpyDeviceToHost));
+    st->krylov_iterations = ha.krylov_iters;
+    st->hvp_count = ha.hvp_count;
+    st->cfl_violation = (hc.flags & FLAG_CFL) ? 1 : 0;
+    st->status_flags = (hc.flags & FLAG_NAN ? 1 : 0) | (hc.flags & FLAG_TIMEOUT ? 2 : 0);
+    st->num_particles = P;
+    st->num_groups = ctx->G;
+    st->num_blocks = ctx->B;
+    st->num_nodes = hc.N;
+    st->kernel_launches = (int32_t)(g_kernel_launches - launches0);
+    ctx->time += dt;
+    if (hc.flags & FLAG_TIMEOUT) {
+        ctx->err = "a bounded device wait gave up";
+        return ZMPM_TIMEOUT;
+    }
+    return st->cfl_violation ? ZMPM_CFL_VIOLATION : ZMPM_OK;
+}
+
+// ------------------------------------------------------------ checkpoints --
+int zmpm_checkpoint_save(zmpm_ctx* ctx, int32_t slot)
+{
+    if (!ctx || slot < 0 || slot > 4096) return ZMPM_BAD_ARG;
+    cudaSetDevice(ctx->device);
+    int rc = upload(ctx);
+    if (rc) return rc;
+    const size_t n = (size_t)slot + 1;
+    if (ctx->ckpt_pd.size() < n) {
+        ctx->ckpt_pd.resize(n);
+        ctx->ckpt_pi.resize(n);
+        ctx->ckpt_sid.resize(n);
+        ctx->ckpt_time.resize(n, 0.0);
+        ctx->ckpt_P.resize(n, -1);
+    }
+    const int64_t cap = ctx->Pcap;
+    ZMPM_CUDA(ctx->ckpt_pd[slot].ensure((size_t)PD_FIELDS * cap * sizeof(double)));
+    ZMPM_CUDA(ctx->ckpt_pi[slot].ensure((size_t)PI_FIELDS * cap * sizeof(int32_t)));
+    ZMPM_CUDA(ctx->ckpt_sid[slot].ensure((size_t)cap * sizeof(int32_t)));
+    ZMPM_CUDA(cudaMemcpyAsync(ctx->ckpt_pd[slot].p, ctx->pd.p, (size_t)ctx->pd_active * cap * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+    ZMPM_CUDA(cudaMemcpyAsync(ctx->ckpt_pi[slot].p, ctx->pi.p, (size_t)PI_FIELDS * cap * sizeof(int32_t), cudaMemcpyDeviceToDevice, ctx->stream));
+    ZMPM_CUDA(cudaMemcpyAsync(ctx->ckpt_sid[slot].p, ctx->slot_of_id.p, (size_t)cap * sizeof(int32_t), cudaMemcpyDeviceToDevice, ctx->stream));
+    ZMPM_CUDA(cudaStreamSynchronize(ctx->stream));
+    ctx->ckpt_time[slot] = ctx->time;
+    ctx->ckpt_P[slot] = ctx->P * 1000 + ctx->pd_active; // particle count and active fields of the saved pool
+    return ZMPM_OK;
+}
+
+int zmpm_checkpoint_load(zmpm_ctx* ctx, int32_t slot)
+{
+    if (!ctx || slot < 0 || (size_t)slot >= ctx->ckpt_pd.size() || ctx->ckpt_P[slot] < 0) return ZMPM_BAD_ARG;
+    if (ctx->ckpt_P[slot] != ctx->P * 1000 + ctx->pd_active || !ctx->uploaded) {
+        ctx->err = "the checkpoint was saved with a different particle set";
+        return ZMPM_BAD_ARG;
+    }
+    cudaSetDevice(ctx->device);
+    const int64_t cap = ctx->Pcap;
+    ZMPM_CUDA(cudaMemcpyAsync(ctx->pd.p, ctx->ckpt_pd[slot].p, (size_t)ctx->pd_active * cap * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+    ZMPM_CUDA(cudaMemcpyAsync(ctx->pi.p, ctx->ckpt_pi[slot].p, (size_t)PI_FIELDS * cap * sizeof(int32_t), cudaMemcpyDeviceToDevice, ctx->stream));
+    ZMPM_CUDA(cudaMemcpyAsync(ctx->slot_of_id.p, ctx->ckpt_sid[slot].p, (size_t)cap * sizeof(int32_t), cudaMemcpyDeviceToDevice, ctx->stream));
+    ZMPM_CUDA(cudaStreamSynchronize(ctx->stream));
+    ctx->time = ctx->ckpt_time[slot];
+    ctx->binned = false;
+    ctx->implicit_ready = false;
+    return ZMPM_OK;
 }
 
 // ------------------------------------------------------------------ hooks --

@@ -89,6 +89,12 @@ enum PdField { PD_X = 0, PD_V = 3, PD_C = 6, PD_F = 15, PD_M = 24, PD_VOL = 25, 
     PD_FE = 39, PD_VMU = 48, PD_VLAM = 49, PD_VD = 50, PD_VV = 51, PD_Y = 52, PD_OMEGA = 70, PD_LASTDV = 72, PD_FIELDS = 75 };
 enum PiField { PI_KIND = 0, PI_PKIND = 1, PI_BROKEN = 2, PI_ID = 3, PI_DAMAGE = 4, PI_VISCO = 5, PI_FIELDS = 6 };
 
+// Adjoint particle arrays [AJ_FIELDS][Pcap] (FP64, slot order): the state
+// before the substep (same field order as the pool's first 24 fields), the
+// incoming gradients and the outgoing ones.
+enum AdjField { AJ_X0 = 0, AJ_V0 = 3, AJ_C0 = 6, AJ_F0 = 15, AJ_GX = 24, AJ_GV = 27, AJ_GC = 30, AJ_GF = 39, AJ_OX = 48, AJ_OV = 51,
+    AJ_OC = 54, AJ_OF = 63, AJ_OE = 72, AJ_FIELDS = 73 };
+
 // Reduction slots: per-CTA partial sums written by node kernels.
 constexpr int RED_MAX_CTAS = 1024;
 enum RedSlot { RED_A = 0, RED_B = 1, RED_C = 2, RED_N = 3 };
@@ -171,6 +177,10 @@ struct Ctx {
     // global-operator coefficients B [6][Pcap] (HVP precision); node
     // preconditioner, right-hand side and transfer weights
     DBuf adm_F, adm_gvn, adm_B, adm_pre, adm_rhs, adm_w;
+    DBuf adj;                             // adjoint particle arrays [AJ_FIELDS][Pcap]
+    std::vector<DBuf> ckpt_pd, ckpt_pi, ckpt_sid; // device checkpoints
+    std::vector<double> ckpt_time;
+    std::vector<int64_t> ckpt_P;
     bool admm_used = false;               // the last substep ran ADMM (launch accounting)
     int admm_iters = 0;
 
@@ -192,7 +202,10 @@ int run_p2g(Ctx* ctx, bool damage = true);            // P2G (+ damage hook) + g
 int run_newton(Ctx* ctx, const zmpm_solver& s);       // backward-Euler Newton
 int run_g2p(Ctx* ctx);                                 // G2P + evolveStrain + plasticity
 int upload_colliders(Ctx* ctx, double time);
-int launch_update(Ctx* ctx);                           // G2P(vn+dv) -> stress -> force P2G
+int launch_update(Ctx* ctx, bool gated = true);       // G2P(vn+dv) -> stress -> force P2G
+int launch_adj_g2p(Ctx* ctx, double* vsbar);           // adjoint of G2P (adjoint.cu)
+int launch_adj_particle(Ctx* ctx, const double* lam);  // adjoint of the force term, P2G and E
+int run_adjoint_solve(Ctx* ctx, double tol, int max_iterations); // (M + dt^2 K) lambda = P dL/dv*
 int launch_residual(Ctx* ctx);                         // r = dt m g + dt f - m dv (projected), norm partials
 int launch_hvp(Ctx* ctx, const double* x, double* out, bool fp32); // out += dt^2 K x (no inertia)
 int launch_damage(Ctx* ctx);                           // Rankine damage after P2G

@@ -811,6 +811,43 @@ __global__ void k_admm_advance(SolverScalars* __restrict__ sc, int nmax, cudaGra
     if (use_graph) cudaGraphSetConditional(hN, n < nmax ? 1u : 0u);
 }
 
+// ---------------------------------------------------------------- adjoint --
+// Start of the adjoint CG solve (ConjugateGradient.h:99-117 with x = 0):
+// r = project(g), q = r / m, p = q, partial r.q; relative tolerance `tol`.
+template <int NPB>
+__global__ void __launch_bounds__(ND_THREADS) k_adj_cg_init(NodeGeom ng, const double* __restrict__ gm, const int8_t* __restrict__ col,
+    const double* __restrict__ P6, const double* __restrict__ g, KrylovBufs kb, double tol, double* __restrict__ part,
+    SolverScalars* __restrict__ sc)
+{
+    if (blockIdx.x == 0 && threadIdx.x == 0) sc->rel_tol = tol;
+    double acc = 0;
+    for (int64_t n = (int64_t)blockIdx.x * ND_THREADS + threadIdx.x; n < ng.nn; n += (int64_t)gridDim.x * ND_THREADS) {
+        const double m = gm[n];
+        double r[3];
+        for (int k = 0; k < 3; ++k) r[k] = (m != 0) ? g[vidx<NPB>(n, k)] : 0.0;
+        if (m != 0) project3(col, P6, ng.nn, n, r);
+        for (int k = 0; k < 3; ++k) {
+            const int64_t i = vidx<NPB>(n, k);
+            const double q = (m != 0) ? r[k] / kb.pre[n] : 0.0;
+            kb.x[i] = 0;
+            kb.r[i] = r[k];
+            kb.q[i] = q;
+            kb.p[i] = q;
+            kb.hacc[i] = 0;
+            acc += r[k] * q;
+        }
+    }
+    double t = block_sum(acc);
+    if (threadIdx.x == 0) part[blockIdx.x] = t;
+}
+
+// The adjoint solve runs its Krylov loop once: the outer loop stops after it.
+__global__ void k_adj_once(SolverScalars* __restrict__ sc, cudaGraphConditionalHandle hN, int use_graph)
+{
+    sc->nit += 1;
+    if (use_graph) cudaGraphSetConditional(hN, 0u);
+}
+
 // ------------------------------------------------------------ host side --
 static NodeGeom node_geom(const Ctx* ctx)
 {
@@ -1307,6 +1344,100 @@ static int admm_impl(Ctx* ctx, const zmpm_solver& s)
     ctx->admm_iters = s.admm_iterations;
     rc = launch_admm_lastdv(ctx);
     if (rc) return rc;
+    ZMPM_CUDA(cudaGetLastError());
+    return ZMPM_OK;
+}
+
+// (M + dt^2 K) lambda = P g with CG on the Newton operator (the Hessian
+// scratch must hold the converged state); g is ctx->res on entry, lambda is
+// kv[0] on exit.  Returns the CG iteration count through stats.
+int run_adjoint_solve(Ctx* ctx, double tol, int max_iterations)
+{
+    NewtonLaunch Lc;
+    Lc.ctx = ctx;
+    Lc.ng = node_geom(ctx);
+    Lc.sc = ctx->scal.as<SolverScalars>();
+    double* part = ctx->red.as<double>();
+    Lc.pA = part + RED_A * RED_MAX_CTAS;
+    Lc.pB = part + RED_B * RED_MAX_CTAS;
+    Lc.pC = part + RED_C * RED_MAX_CTAS;
+    KrylovBufs& kb = Lc.kb;
+    kb.x = ctx->kv[0].as<double>();
+    kb.r = ctx->kv[1].as<double>();
+    kb.p = ctx->kv[2].as<double>();
+    kb.q = ctx->kv[3].as<double>();
+    kb.tmp = ctx->kv[4].as<double>();
+    for (int k = 0; k < 3; ++k) kb.Q[k] = kb.M[k] = nullptr;
+    kb.Z[0] = kb.Z[1] = nullptr;
+    kb.hacc = ctx->kv[9].as<double>();
+    kb.pre = ctx->gm.as<double>();
+    Lc.np.minres = 0;
+    Lc.np.kmax = max_iterations;
+    Lc.np.nmax = 1;
+    Lc.np.tol = 0;
+    Lc.np.abs_tol = 1e300;
+    Lc.np.tol_scale = 1;
+    Lc.np.dt = ctx->dt;
+    Lc.dt2 = ctx->dt * ctx->dt;
+    Lc.nb = Lc.ng.parts;
+    cudaStream_t st = ctx->stream;
+    ZMPM_CUDA(cudaMemsetAsync(Lc.sc, 0, sizeof(SolverScalars), st));
+    if (Lc.ng.nn == 0) return ZMPM_OK;
+    const bool l244 = ctx->layout == 1;
+    auto head = [&](cudaStream_t sm, cudaGraphConditionalHandle hK, int ug) {
+        if (l244) {
+            k_adj_cg_init<32><<<Lc.nb, ND_THREADS, 0, sm>>>(Lc.ng, ctx->gm.as<double>(), ctx->collided.as<int8_t>(), ctx->proj.as<double>(),
+                ctx->res.as<double>(), kb, tol, Lc.pB, Lc.sc);
+            k_krylov_start<32><<<Lc.nb, ND_THREADS, 0, sm>>>(Lc.ng, kb, Lc.np, Lc.pB, Lc.sc, hK, ug);
+        }
+        else {
+            k_adj_cg_init<64><<<Lc.nb, ND_THREADS, 0, sm>>>(Lc.ng, ctx->gm.as<double>(), ctx->collided.as<int8_t>(), ctx->proj.as<double>(),
+                ctx->res.as<double>(), kb, tol, Lc.pB, Lc.sc);
+            k_krylov_start<64><<<Lc.nb, ND_THREADS, 0, sm>>>(Lc.ng, kb, Lc.np, Lc.pB, Lc.sc, hK, ug);
+        }
+        g_kernel_launches += 2;
+        return (int)ZMPM_OK;
+    };
+    auto body = [&](cudaStream_t sm, cudaGraphConditionalHandle hK, int ug) {
+        return l244 ? launch_krylov_iteration<32>(Lc, sm, hK, ug, nullptr, nullptr) : launch_krylov_iteration<64>(Lc, sm, hK, ug, nullptr, nullptr);
+    };
+    auto tail = [&](cudaStream_t sm, cudaGraphConditionalHandle hN, int ug) {
+        k_adj_once<<<1, 1, 0, sm>>>(Lc.sc, hN, ug);
+        ++g_kernel_launches;
+        return (int)ZMPM_OK;
+    };
+    if (!ctx->no_graph) {
+        cudaGraphExec_t exec = nullptr;
+        const int64_t launches0 = g_kernel_launches;
+        int rc = loop_graph(
+            ctx, [&](cudaStream_t sm, cudaGraphConditionalHandle hK) { return head(sm, hK, 1); },
+            [&](cudaStream_t sm, cudaGraphConditionalHandle hK) { return body(sm, hK, 1); },
+            [&](cudaStream_t sm, cudaGraphConditionalHandle hN) { return tail(sm, hN, 1); }, &exec);
+        if (rc) return rc;
+        cudaError_t e = cudaGraphLaunch(exec, st);
+        cudaError_t e2 = cudaStreamSynchronize(st);
+        cudaGraphExecDestroy(exec);
+        ZMPM_CUDA(e);
+        ZMPM_CUDA(e2);
+        // kernels executed: head (2) and tail (1) once, 6 per Krylov body
+        SolverScalars hs;
+        ZMPM_CUDA(cudaMemcpy(&hs, Lc.sc, sizeof(hs), cudaMemcpyDeviceToHost));
+        g_kernel_launches = launches0 + 3 + 6 * (int64_t)hs.krylov_bodies;
+    }
+    else {
+        int rc = head(st, 0, 0);
+        if (rc) return rc;
+        for (int k = 0; k < max_iterations; k += 8) {
+            for (int j = 0; j < 8 && k + j < max_iterations; ++j) {
+                rc = body(st, 0, 0);
+                if (rc) return rc;
+            }
+            SolverScalars hs;
+            ZMPM_CUDA(cudaMemcpyAsync(&hs, Lc.sc, sizeof(hs), cudaMemcpyDeviceToHost, st));
+            ZMPM_CUDA(cudaStreamSynchronize(st));
+            if (!hs.kactive) break;
+        }
+    }
     ZMPM_CUDA(cudaGetLastError());
     return ZMPM_OK;
 }

@@ -560,12 +560,12 @@ static int p2g_impl(Ctx* ctx)
 int launch_p2g(Ctx* ctx) { return ctx->layout == 1 ? p2g_impl<Layout244>(ctx) : p2g_impl<Layout444>(ctx); }
 
 template <class L>
-static int update_impl(Ctx* ctx)
+static int update_impl(Ctx* ctx, bool gated)
 {
     const int64_t G = ctx->G;
     if (G == 0) return ZMPM_OK;
     DevCounters* dc = ctx->counters.as<DevCounters>();
-    const SolverScalars* sc = ctx->scal.as<SolverScalars>();
+    const SolverScalars* sc = gated ? ctx->scal.as<SolverScalars>() : nullptr;
     if (ctx->mixed) {
         k_stress<L, float, float><<<(unsigned)G, XF_THREADS, 0, ctx->stream>>>(ctx->group_start.as<int32_t>(), ctx->group_nbr.as<int32_t>(),
             ctx->pd.as<double>(), ctx->pi.as<int32_t>(), ctx->Pcap, ctx->base.as<short4>(), ctx->cfg.dx, ctx->dt, ctx->frac.as<float>(),
@@ -586,7 +586,7 @@ static int update_impl(Ctx* ctx)
     }
     return ZMPM_OK;
 }
-int launch_update(Ctx* ctx) { return ctx->layout == 1 ? update_impl<Layout244>(ctx) : update_impl<Layout444>(ctx); }
+int launch_update(Ctx* ctx, bool gated) { return ctx->layout == 1 ? update_impl<Layout244>(ctx, gated) : update_impl<Layout444>(ctx, gated); }
 
 template <class L, class TH>
 static void hvp_launch(Ctx* ctx, const double* x0, const double* x1, int alt, double* out, const SolverScalars* sc)

@@ -346,6 +346,41 @@ class MpmSimulation:
         self._call("get_damage", ptr(c))
         return c
 
+    # reverse mode and checkpoints
+    def adjointSubstep(self, dt, gx=None, gv=None, gC=None, gF=None, gE=None, tolerance=1e-12):
+        """Runs one substep forward from the current state and maps the loss
+        gradients with respect to the new state (gx, gv: [P,3]; gC, gF: [P,3,3])
+        to gradients with respect to the previous state, in place; gE [P]
+        accumulates dL/dE.  Returns the status."""
+        n = self.count
+
+        def arr(a, shape):
+            if a is None:
+                return None
+            assert a.dtype == np.float64 and a.flags.c_contiguous and a.shape == shape
+            return a
+        st = abi.Stats()
+        s = self.solver()
+        args = [arr(gx, (n, 3)), arr(gv, (n, 3)), arr(gC, (n, 3, 3)), arr(gF, (n, 3, 3)), arr(gE, (n,))]
+        rc = self.lib.adjoint_substep(self.ctx, float(dt), abi.C.byref(s), float(tolerance),
+                                      *[ptr(a) if a is not None else None for a in args], abi.C.byref(st))
+        self.last_stats = st.as_dict()
+        return rc
+
+    def checkpointSave(self, slot):
+        self._call("checkpoint_save", int(slot))
+
+    def checkpointLoad(self, slot):
+        self._call("checkpoint_load", int(slot))
+
+    def setYoungsModulus(self, E, nu, lower=0, upper=None):
+        """Per-particle E at Poisson ratio nu (mu and lambda of each particle)."""
+        upper = self.count if upper is None else upper
+        E = np.ascontiguousarray(np.broadcast_to(E, (upper - lower,)), dtype=np.float64)
+        mu = E / (2 * (1 + nu))
+        lam = E * nu / ((1 + nu) * (1 - 2 * nu))
+        self._call("set_lame", int(lower), int(upper), ptr(np.ascontiguousarray(mu)), ptr(np.ascontiguousarray(lam)))
+
     def getViscoelasticStrain(self):
         Fe = np.empty((self.count, 3, 3))
         self._call("get_viscoelastic_strain", ptr(Fe))
