@@ -172,7 +172,103 @@ def wl_damage2m(precision, lib=None, layout="auto", scale=1):
                                    "solver": "MINRES, Newton 3 x Krylov 20 (reference defaults)"}
 
 
-WORKLOADS = {"cube32k": wl_cube32k, "admm500k": wl_admm500k, "damage2m": wl_damage2m}
+def wl_rollout256k(precision, lib=None, layout="auto", scale=1):
+    """Differentiable rollout: elastic cube of 32^3 cells x 8 ppc = 262,144
+    particles (seed 0) at dx = 1/64 (side 0.5, min corner (0.25, 0.125, 0.25)),
+    fixed corotated with per-particle E ~ LogNormal(ln 1e4 - 0.3^2/2, 0.3)
+    (seed 5), nu = 0.3, initial velocities uniform in [-0.5, 0.5]^3 (seed 6),
+    sticky ground y = 0.1, gravity, Newton-CG, dt = 1e-3; loss = |com(x_100) -
+    target|^2 with the target drawn from seed 7.  scale > 1 shrinks the cube's
+    edge by that factor (CPU samples)."""
+    from ziran2019_b200 import abi, mpm
+    dx = 1.0 / 64
+    n = 32 // scale
+    x = _jitter_box((n, n, n), dx, (0.25, 0.125, 0.25), 8, 0)
+    sim = mpm.MpmSimulation(dx, gravity=(0, -9.8, 0), precision=precision, grid_log2=7, layout=layout, lib=lib)
+    V0 = dx ** 3 / 8
+    h = sim.addParticles(x, np.zeros_like(x), 1000.0 * V0, V0)
+    h.addFBasedMpmForce(mpm.FixedCorotated(1e4, 0.3))
+    sim.addCollisionObject(mpm.AnalyticCollisionObject(mpm.HalfSpace((0, 0.1, 0), (0, 1, 0)), abi.STICKY))
+    sim.switchLinearSolver(abi.CG)
+    sim.newton_tolerance = 1e-12 if precision == "fp64" else 1e-7
+    sim.newton_max_iterations = 30
+    sim.krylov_max_iterations = 500
+    sim.krylov_tolerance = 1e-30
+    return sim, 1e-3, x.shape[0], {"workload": "config4-differentiable-rollout-256k", "model": "fixed corotated, per-particle E",
+                                   "solver": "Newton-CG (FP64 tol 1e-12, mixed 1e-7), adjoint CG rel tol 1e-10",
+                                   "steps": 100, "checkpoint_every": 10}
+
+
+def run_rollout(args, world, rank):
+    """Forward + reverse sweep of the 100-substep rollout (mixed and FP64):
+    gradient rollouts per second, mixed-vs-FP64 gradient error, and a central
+    finite-difference check of the FP64 gradients in random directions."""
+    import torch
+
+    from ziran2019_b200 import build
+    from ziran2019_b200.rollout import Rollout
+    build.build()
+    steps, every, NUR = 100, 10, 0.3
+    res = {}
+    for p in ("fp64", "mixed"):
+        sim, dt, P, meta = wl_rollout256k(p, layout="444")
+        rng = np.random.default_rng(5)
+        E = np.exp(np.log(1e4) - 0.3 ** 2 / 2 + 0.3 * rng.standard_normal(P))
+        v0 = np.random.default_rng(6).uniform(-0.5, 0.5, (P, 3))
+        target = np.array([0.5, 0.3, 0.5]) + np.random.default_rng(7).uniform(-0.05, 0.05, 3)
+        m = np.full(P, 1000.0 * (1.0 / 64) ** 3 / 8)
+        ro = Rollout(sim, NUR, dt, steps, checkpoint_every=every, tolerance=1e-10)
+
+        def loss_and_grad(X):
+            com = (m[:, None] * X).sum(0) / m.sum()
+            return float(((com - target) ** 2).sum()), 2 * (com - target)[None, :] * (m / m.sum())[:, None]
+        X = ro.run(E, v0)  # warm-up (allocations, graphs)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        X = ro.run(E, v0)
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        L, gX = loss_and_grad(X)
+        gE, gv = ro.backward(gX)
+        torch.cuda.synchronize()
+        t2 = time.perf_counter()
+        res[p] = {"forward_s": t1 - t0, "backward_s": t2 - t1, "loss": L, "gE": gE, "gv": gv,
+                  "adjoint_cg_iterations": sum(s["krylov_iterations"] for s in ro.stats)}
+        if p == "fp64":
+            fd_err = []
+            drng = np.random.default_rng(11)
+            for k in range(args.fd_directions):
+                which = "E" if k % 2 == 0 else "v"
+                d = drng.standard_normal(E.shape if which == "E" else v0.shape)
+                scale_ = 1e4 if which == "E" else 0.5
+                h = 1e-4 * scale_
+                Ep, vp = (E + h * d, v0) if which == "E" else (E, v0 + h * d)
+                Em, vm = (E - h * d, v0) if which == "E" else (E, v0 - h * d)
+                fd = (loss_and_grad(ro.run(Ep, vp))[0] - loss_and_grad(ro.run(Em, vm))[0]) / (2 * h)
+                an = float(((gE if which == "E" else gv) * d).sum())
+                fd_err.append(abs(fd - an) / max(abs(an), 1e-300))
+            res[p]["fd_rel_err"] = fd_err
+        sim.close()
+    r64, rmx = res["fp64"], res["mixed"]
+    relE = float(np.linalg.norm(rmx["gE"] - r64["gE"]) / np.linalg.norm(r64["gE"]))
+    relv = float(np.linalg.norm(rmx["gv"] - r64["gv"]) / np.linalg.norm(r64["gv"]))
+    if rank == 0:
+        tot = rmx["forward_s"] + rmx["backward_s"]
+        line = {"metric": "differentiable rollouts/sec (100 implicit substeps forward + reverse), config4-differentiable-rollout-256k",
+                "value": 1.0 / tot, "unit": "rollouts/s", "n_gpus": world, "steps": steps, "warmup": 1, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "mixed forward (fp32 HVP) + fp64 adjoint vectors", "data": "synthetic",
+                "config": dict(meta, particles=P, dt=1e-3),
+                "mixed": {k: rmx[k] for k in ("forward_s", "backward_s", "loss", "adjoint_cg_iterations")},
+                "fp64": {k: r64[k] for k in ("forward_s", "backward_s", "loss", "adjoint_cg_iterations")},
+                "fp64_value": 1.0 / (r64["forward_s"] + r64["backward_s"]),
+                "grad_rel_err_mixed_vs_fp64": {"E": relE, "v0": relv},
+                "fd_check_fp64": {"directions": args.fd_directions, "h": "1e-4 x (1e4 for E, 0.5 for v0)",
+                                  "max_rel_err": max(r64["fd_rel_err"]) if r64.get("fd_rel_err") else None,
+                                  "rel_err": r64.get("fd_rel_err")}}
+        print(json.dumps(line), flush=True)
+
+
+WORKLOADS = {"cube32k": wl_cube32k, "admm500k": wl_admm500k, "damage2m": wl_damage2m, "rollout256k": wl_rollout256k}
 
 
 def run_workload(args, world, rank):
@@ -372,12 +468,16 @@ def main():
                     help="page layout of the FP64 substep: 444 = same as the mixed run (only precision differs)")
     ap.add_argument("--workload", default="config1", choices=["config1"] + sorted(WORKLOADS),
                     help="config1: the headline 1M-particle workload; others print their own line")
+    ap.add_argument("--fd-directions", type=int, default=4, help="finite-difference directions of the rollout gradient check")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     world, rank = dist_setup()
     if args.impl == "reference":
         run_reference(args, world, rank)
+        return
+    if args.workload == "rollout256k":
+        run_rollout(args, world, rank)
         return
     if args.workload != "config1":
         run_workload(args, world, rank)
