@@ -172,6 +172,9 @@ def wl_damage2m(precision, lib=None, layout="auto", scale=1):
                                    "solver": "MINRES, Newton 3 x Krylov 20 (reference defaults)"}
 
 
+MIXED_ROLLOUT_TOL = 1e-7
+
+
 def wl_rollout256k(precision, lib=None, layout="auto", scale=1):
     """Differentiable rollout: elastic cube of 32^3 cells x 8 ppc = 262,144
     particles (seed 0) at dx = 1/64 (side 0.5, min corner (0.25, 0.125, 0.25)),
@@ -190,7 +193,7 @@ def wl_rollout256k(precision, lib=None, layout="auto", scale=1):
     h.addFBasedMpmForce(mpm.FixedCorotated(1e4, 0.3))
     sim.addCollisionObject(mpm.AnalyticCollisionObject(mpm.HalfSpace((0, 0.1, 0), (0, 1, 0)), abi.STICKY))
     sim.switchLinearSolver(abi.CG)
-    sim.newton_tolerance = 1e-12 if precision == "fp64" else 1e-7
+    sim.newton_tolerance = 1e-12 if precision == "fp64" else MIXED_ROLLOUT_TOL
     sim.newton_max_iterations = 30
     sim.krylov_max_iterations = 500
     sim.krylov_tolerance = 1e-30
@@ -228,12 +231,14 @@ def run_rollout(args, world, rank):
         X = ro.run(E, v0)
         torch.cuda.synchronize()
         t1 = time.perf_counter()
+        fwd_newton = sim.last_stats["newton_iterations"]
         L, gX = loss_and_grad(X)
         gE, gv = ro.backward(gX)
         torch.cuda.synchronize()
         t2 = time.perf_counter()
         res[p] = {"forward_s": t1 - t0, "backward_s": t2 - t1, "loss": L, "gE": gE, "gv": gv,
-                  "adjoint_cg_iterations": sum(s["krylov_iterations"] for s in ro.stats)}
+                  "adjoint_cg_iterations": sum(s["krylov_iterations"] for s in ro.stats),
+                  "newton_iterations_last_substep": fwd_newton, "newton_tolerance": sim.newton_tolerance}
         if p == "fp64":
             fd_err = []
             drng = np.random.default_rng(11)
@@ -258,8 +263,8 @@ def run_rollout(args, world, rank):
                 "value": 1.0 / tot, "unit": "rollouts/s", "n_gpus": world, "steps": steps, "warmup": 1, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "mixed forward (fp32 HVP) + fp64 adjoint vectors", "data": "synthetic",
                 "config": dict(meta, particles=P, dt=1e-3),
-                "mixed": {k: rmx[k] for k in ("forward_s", "backward_s", "loss", "adjoint_cg_iterations")},
-                "fp64": {k: r64[k] for k in ("forward_s", "backward_s", "loss", "adjoint_cg_iterations")},
+                "mixed": {k: rmx[k] for k in ("forward_s", "backward_s", "loss", "adjoint_cg_iterations", "newton_iterations_last_substep", "newton_tolerance")},
+                "fp64": {k: r64[k] for k in ("forward_s", "backward_s", "loss", "adjoint_cg_iterations", "newton_iterations_last_substep", "newton_tolerance")},
                 "fp64_value": 1.0 / (r64["forward_s"] + r64["backward_s"]),
                 "grad_rel_err_mixed_vs_fp64": {"E": relE, "v0": relv},
                 "fd_check_fp64": {"directions": args.fd_directions, "h": "1e-4 x (1e4 for E, 0.5 for v0)",
@@ -469,7 +474,11 @@ def main():
     ap.add_argument("--workload", default="config1", choices=["config1"] + sorted(WORKLOADS),
                     help="config1: the headline 1M-particle workload; others print their own line")
     ap.add_argument("--fd-directions", type=int, default=4, help="finite-difference directions of the rollout gradient check")
+    ap.add_argument("--rollout-mixed-tol", type=float, default=None, help="Newton tolerance of the mixed rollout forward")
     args = ap.parse_args()
+    if args.rollout_mixed_tol is not None:
+        global MIXED_ROLLOUT_TOL
+        MIXED_ROLLOUT_TOL = args.rollout_mixed_tol
     if args.warmup < 3:
         args.warmup = 3
     world, rank = dist_setup()

@@ -50,6 +50,18 @@ def test_p2g_grid_matches_oracle(cuda_lib, oracle, kind):
     np.testing.assert_allclose(gdv, odv, rtol=1e-11, atol=1e-12)
 
 
+def test_p2g_mixed_matches_fp64_oracle(cuda_lib, oracle):
+    """MIXED P2G against the FP64 oracle, nodes matched by coordinate (4x4x4
+    against 2x4x4 pages); FP32-level agreement."""
+    g, o = pair(oracle, "hencky", precision="mixed", seed=5)
+    assert g.beginImplicit(1e-3) == o.beginImplicit(1e-3)
+    _, gm, gv, gc = by_coord(g)
+    _, om, ov, oc = by_coord(o)
+    np.testing.assert_array_equal(gc, oc)
+    np.testing.assert_allclose(gm, om, rtol=2e-6, atol=1e-6 * om.max())
+    np.testing.assert_allclose(gv, ov, rtol=0, atol=2e-6 * np.abs(ov).max())
+
+
 @pytest.mark.parametrize("kind", KINDS)
 def test_residual_and_hvp_match_oracle_fp64(cuda_lib, oracle, kind):
     g, o = pair(oracle, kind, seed=1)
