@@ -386,15 +386,6 @@ int zmpm_create(const zmpm_config* cfg, zmpm_ctx** out)
         ctx->hvp_fused = f && f[0] == '1';
         const char* ng = getenv("ZMPM_NO_GRAPH");
         ctx->no_graph = ng && ng[0] == '1';
-        const char* hm = getenv("ZMPM_HVP_MODE");
-        ctx->hvp_mode = hm ? atoi(hm) : 0;
-        const char* pm = getenv("ZMPM_P2G_MODE");
-        ctx->p2g_mode = pm ? atoi(pm) : 0;
-        const char* nc = getenv("ZMPM_NODE_CTAS");
-        if (nc) {
-            const int v = atoi(nc);
-            ctx->node_ctas = v < 1 ? 1 : (v > RED_MAX_CTAS ? RED_MAX_CTAS : v);
-        }
     }
     auto fail = [&](cudaError_t e) {
         ctx->err = cudaGetErrorString(e);

@@ -142,9 +142,6 @@ struct Ctx {
     DBuf dstress;      // [9][Pcap] dS of one Hessian-vector product (HVP precision)
     bool hvp_fused = false; // one fused HVP kernel instead of stress + scatter
     bool no_graph = false;  // host-driven Newton loop instead of the conditional graph
-    int node_ctas = RED_MAX_CTAS; // CTAs of the node kernels (each re-reduces that many partials)
-    int hvp_mode = 0;       // 2: single-pass FP32 product with dS in shared memory
-    int p2g_mode = 0;       // 1: FP32 register-accumulated P2G (mixed precision)
     cudaGraphExec_t graph_exec = nullptr; // last Newton graph, released after the next sync
     bool graph_used = false;              // the last Newton solve ran as a graph
     DBuf frac;         // [3][Pcap] fractional offsets in cells (FP32 HVP)

@@ -854,8 +854,7 @@ static NodeGeom node_geom(const Ctx* ctx)
     NodeGeom ng;
     ng.nn = ctx->B * ctx->npb();
     int64_t c = (ng.nn + ND_THREADS - 1) / ND_THREADS;
-    const int64_t cap = ctx->node_ctas;
-    ng.parts = (int)(c < 1 ? 1 : (c > cap ? cap : c));
+    ng.parts = (int)(c < 1 ? 1 : (c > RED_MAX_CTAS ? RED_MAX_CTAS : c));
     return ng;
 }
 

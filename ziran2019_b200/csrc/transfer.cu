@@ -65,79 +65,6 @@ __global__ void __launch_bounds__(XF_THREADS) k_p2g(const int32_t* __restrict__ 
     flush_window<4, 1, NPB>(acc, nbr, gm, gmv);
 }
 
-// FP32 APIC P2G of the mixed precision mode: one thread per cell of the page
-// (every (blockDim/NPB)-th particle of it) sums mass and momentum for the
-// cell's 27 stencil nodes in registers, then adds them to the shared window
-// once; the window is flushed into the FP64 grid.  x_i - x_p is formed as
-// (stencil offset - fractional offset) dx, so no large coordinates are
-// subtracted in FP32.
-template <class L>
-__global__ void __launch_bounds__(XF_THREADS) k_p2g_f32(const int32_t* __restrict__ group_start, const int32_t* __restrict__ group_nbr,
-    const double* __restrict__ pd, int64_t cap, const short4* __restrict__ base, double dx, double* __restrict__ gm, double* __restrict__ gmv,
-    float* __restrict__ frac)
-{
-    constexpr int NPB = L::NPB;
-    __shared__ __align__(16) float acc[8 * 4 * NPB];
-    __shared__ int32_t nbr[8];
-    __shared__ CellLayout<L> cl;
-    const int g = blockIdx.x;
-    if (threadIdx.x < 8) nbr[threadIdx.x] = group_nbr[8 * g + threadIdx.x];
-    zero_window<4, NPB>(acc);
-    const double inv_dx = 1.0 / dx;
-    const float fdx = (float)dx, finv_dx = (float)inv_dx;
-    const int s0 = group_start[g], s1 = group_start[g + 1];
-    build_cell_layout<L>(cl, base, s0, s1);
-    const int ce = threadIdx.x % NPB;
-    const int lx = ce >> (L::YB + L::ZB), ly = (ce >> L::ZB) & (L::BY - 1), lz = ce & (L::BZ - 1);
-    const int cnt = cl.cnt[ce], first = s0 + cl.start[ce];
-    float a[27][4];
-#pragma unroll
-    for (int n = 0; n < 27; ++n)
-#pragma unroll
-        for (int c = 0; c < 4; ++c) a[n][c] = 0.f;
-    for (int r = threadIdx.x / NPB; r < cnt; r += blockDim.x / NPB) {
-        const int s = first + r;
-        const short4 b = base[s];
-        float fr[3], w[3][3], dwr[3][3];
-#pragma unroll
-        for (int d = 0; d < 3; ++d) {
-            const double d0 = inv_dx * pd[(PD_X + d) * cap + s] - (double)((&b.x)[d]);
-            fr[d] = (float)d0;
-            frac[d * cap + s] = fr[d];
-            bspline(fr[d], w[d], dwr[d]);
-        }
-        const float mass = (float)pd[PD_M * cap + s];
-        float mom[3], Cm[9];
-#pragma unroll
-        for (int d = 0; d < 3; ++d) mom[d] = mass * (float)pd[(PD_V + d) * cap + s];
-#pragma unroll
-        for (int q = 0; q < 9; ++q) Cm[q] = mass * (float)pd[(PD_C + q) * cap + s];
-        for_stencil<L>(lx, ly, lz, w, dwr, finv_dx, [&](int, int, int i, int j, int k, float wijk, const float*) {
-            const float xi[3] = { ((float)i - fr[0]) * fdx, ((float)j - fr[1]) * fdx, ((float)k - fr[2]) * fdx };
-            const int n = 9 * i + 3 * j + k;
-            a[n][0] += mass * wijk;
-#pragma unroll
-            for (int rr = 0; rr < 3; ++rr) a[n][1 + rr] += (Cm[3 * rr] * xi[0] + Cm[3 * rr + 1] * xi[1] + Cm[3 * rr + 2] * xi[2] + mom[rr]) * wijk;
-        });
-    }
-    if (threadIdx.x / NPB < cnt) {
-#pragma unroll
-        for (int i = 0; i < 3; ++i)
-#pragma unroll
-            for (int j = 0; j < 3; ++j)
-#pragma unroll
-                for (int k = 0; k < 3; ++k) {
-                    int e;
-                    const int t = win_slot<L>(lx + i, ly + j, lz + k, e);
-                    float* dst = acc + t * 4 * NPB + e;
-#pragma unroll
-                    for (int c = 0; c < 4; ++c) atomicAdd(dst + c * NPB, a[9 * i + 3 * j + k][c]);
-                }
-    }
-    __syncthreads();
-    flush_window<4, 1, NPB>(acc, nbr, gm, gmv);
-}
-
 // -------------------------------------------------------------- damage -----
 // Largest eigenvalue of a symmetric 3x3 matrix by the trigonometric solution
 // of the characteristic cubic (O. K. Smith, "Eigenvalues of a symmetric 3x3
@@ -522,119 +449,6 @@ __global__ void __launch_bounds__(XF_THREADS) k_hvp_scatter(const int32_t* __res
     flush_window<3, 3, NPB>(acc, nbr, out, nullptr);
 }
 
-// Single-pass FP32 product: per chunk of HVP_CHUNK particles of the group,
-// phase 1 evaluates dS (slot order, as k_hvp_stress) into shared memory and
-// phase 2 adds dS grad w with the per-cell register accumulation of
-// k_hvp_scatter, reading dS from shared memory.  dS never leaves the SM; the
-// per-cell sums go to the window once per chunk (one chunk for all but the
-// densest pages), so they are not live during phase 1.
-constexpr int HVP_CHUNK = 1024;
-constexpr int HVP_DS_STRIDE = 9;
-template <int NPB>
-constexpr size_t hvp2_smem_bytes()
-{
-    return 8 * 3 * NPB * sizeof(double) + 8 * 3 * NPB * sizeof(float) + (size_t)HVP_CHUNK * HVP_DS_STRIDE * sizeof(float);
-}
-
-template <class L>
-__global__ void __launch_bounds__(XF_THREADS, 4) k_hvp2(const int32_t* __restrict__ group_start, const int32_t* __restrict__ group_nbr,
-    const int32_t* __restrict__ pi, int64_t cap, const short4* __restrict__ base, double dx, const float* __restrict__ frac,
-    const float* __restrict__ scr, const double* __restrict__ x0, const double* __restrict__ x1, int alt, double* __restrict__ out,
-    const SolverScalars* __restrict__ sc, int32_t* __restrict__ flags)
-{
-    if (sc && (sc->newton_done || !sc->kactive)) return;
-    constexpr int NPB = L::NPB;
-    extern __shared__ __align__(128) unsigned char smem_raw[];
-    double* win = reinterpret_cast<double*>(smem_raw);
-    float* acc = reinterpret_cast<float*>(smem_raw + 8 * 3 * NPB * sizeof(double));
-    float* dss = acc + 8 * 3 * NPB;
-    __shared__ int32_t nbr[8];
-    __shared__ __align__(8) uint64_t bar;
-    __shared__ CellLayout<L> cl;
-    const int g = blockIdx.x;
-    if (threadIdx.x < 8) nbr[threadIdx.x] = group_nbr[8 * g + threadIdx.x];
-    zero_window<3, NPB>(acc);
-    __syncthreads();
-    const double* x = (alt && sc && (sc->kit & 1)) ? x1 : x0;
-    stage_window<NPB>(win, x, nbr, &bar, flags);
-    const float inv_dx = float(1.0 / dx);
-    const int s0 = group_start[g], s1 = group_start[g + 1];
-    build_cell_layout<L>(cl, base, s0, s1);
-    const int ce = threadIdx.x % NPB;
-    const int lx = ce >> (L::YB + L::ZB), ly = (ce >> L::ZB) & (L::BY - 1), lz = ce & (L::BZ - 1);
-    const int cnt = cl.cnt[ce], first = s0 + cl.start[ce];
-    for (int c0 = s0; c0 < s1; c0 += HVP_CHUNK) {
-        const int c1 = min(s1, c0 + HVP_CHUNK);
-        for (int s = c0 + threadIdx.x; s < c1; s += blockDim.x) {
-            float* d = dss + (s - c0) * HVP_DS_STRIDE;
-            const int kind = pi[PI_KIND * cap + s];
-            if (kind == ZMPM_MODEL_NONE) {
-#pragma unroll
-                for (int q = 0; q < 9; ++q) d[q] = 0.f;
-                continue;
-            }
-            const short4 b = base[s];
-            float w[3][3], dwr[3][3];
-#pragma unroll
-            for (int dd = 0; dd < 3; ++dd) bspline(frac[dd * cap + s], w[dd], dwr[dd]);
-            const int px = b.x & (L::BX - 1), py = b.y & (L::BY - 1), pz = b.z & (L::BZ - 1);
-            M3<float> G = m3_zero<float>();
-            for_stencil<L>(px, py, pz, w, dwr, inv_dx, [&](int t, int e, int, int, int, float, const float* dw) {
-                const double* vv = win + t * 3 * NPB + e;
-#pragma unroll
-                for (int r = 0; r < 3; ++r) {
-                    const float vr = (float)vv[r * NPB];
-#pragma unroll
-                    for (int c = 0; c < 3; ++c) G(r, c) += vr * dw[c];
-                }
-            });
-            const M3<float> dS = model_hvp<float>(kind, scr, cap, s, G);
-#pragma unroll
-            for (int q = 0; q < 9; ++q) d[q] = dS.a[q];
-        }
-        __syncthreads();
-        float a[27][3];
-#pragma unroll
-        for (int n = 0; n < 27; ++n)
-#pragma unroll
-            for (int c = 0; c < 3; ++c) a[n][c] = 0.f;
-        bool any = false;
-        for (int r = threadIdx.x / NPB; r < cnt; r += blockDim.x / NPB) {
-            const int s = first + r;
-            if (s < c0 || s >= c1) continue;
-            any = true;
-            const float* d = dss + (s - c0) * HVP_DS_STRIDE;
-            float w[3][3], dwr[3][3];
-#pragma unroll
-            for (int dd = 0; dd < 3; ++dd) bspline(frac[dd * cap + s], w[dd], dwr[dd]);
-            float row[3][3];
-#pragma unroll
-            for (int q = 0; q < 9; ++q) row[q / 3][q % 3] = d[q];
-            for_stencil<L>(lx, ly, lz, w, dwr, inv_dx, [&](int, int, int i, int j, int k, float, const float* dw) {
-                const int n = 9 * i + 3 * j + k;
-#pragma unroll
-                for (int c = 0; c < 3; ++c) a[n][c] += row[c][0] * dw[0] + row[c][1] * dw[1] + row[c][2] * dw[2];
-            });
-        }
-        if (any) {
-#pragma unroll
-            for (int i = 0; i < 3; ++i)
-#pragma unroll
-                for (int j = 0; j < 3; ++j)
-#pragma unroll
-                    for (int k = 0; k < 3; ++k) {
-                        int e;
-                        const int t = win_slot<L>(lx + i, ly + j, lz + k, e);
-                        float* dst = acc + t * 3 * NPB + e;
-#pragma unroll
-                        for (int c = 0; c < 3; ++c) atomicAdd(dst + c * NPB, a[9 * i + 3 * j + k][c]);
-                    }
-        }
-        __syncthreads();
-    }
-    flush_window<3, 3, NPB>(acc, nbr, out, nullptr);
-}
-
 // ------------------------------------------------------------------ G2P ----
 template <class L>
 __global__ void __launch_bounds__(XF_THREADS) k_g2p(const int32_t* __restrict__ group_start, const int32_t* __restrict__ group_nbr,
@@ -734,10 +548,7 @@ static int p2g_impl(Ctx* ctx)
 {
     const int64_t G = ctx->G;
     if (G == 0) return ZMPM_OK;
-    if (ctx->mixed && ctx->p2g_mode == 1)
-        k_p2g_f32<L><<<(unsigned)G, XF_THREADS, 0, ctx->stream>>>(ctx->group_start.as<int32_t>(), ctx->group_nbr.as<int32_t>(), ctx->pd.as<double>(),
-            ctx->Pcap, ctx->base.as<short4>(), ctx->cfg.dx, ctx->gm.as<double>(), ctx->gmv.as<double>(), ctx->frac.as<float>());
-    else if (ctx->mixed)
+    if (ctx->mixed)
         k_p2g<L, float><<<(unsigned)G, XF_THREADS, 0, ctx->stream>>>(ctx->group_start.as<int32_t>(), ctx->group_nbr.as<int32_t>(), ctx->pd.as<double>(),
             ctx->Pcap, ctx->base.as<short4>(), ctx->cfg.dx, ctx->gm.as<double>(), ctx->gmv.as<double>(), ctx->frac.as<float>());
     else
@@ -782,21 +593,6 @@ static void hvp_launch(Ctx* ctx, const double* x0, const double* x1, int alt, do
 {
     const int64_t G = ctx->G;
     DevCounters* dc = ctx->counters.as<DevCounters>();
-    if constexpr (sizeof(TH) == 4) {
-        if (ctx->hvp_mode == 2) {
-            constexpr size_t smem = hvp2_smem_bytes<L::NPB>();
-            static bool attr = false; // the attribute belongs to the kernel, once per process
-            if (!attr) {
-                cudaFuncSetAttribute(k_hvp2<L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-                attr = true;
-            }
-            k_hvp2<L><<<(unsigned)G, XF_THREADS, smem, ctx->stream>>>(ctx->group_start.as<int32_t>(), ctx->group_nbr.as<int32_t>(),
-                ctx->pi.as<int32_t>(), ctx->Pcap, ctx->base.as<short4>(), ctx->cfg.dx, ctx->frac.as<float>(), ctx->scratch.as<float>(), x0, x1,
-                alt, out, sc, &dc->flags);
-            ++g_kernel_launches;
-            return;
-        }
-    }
     if (ctx->hvp_fused) {
         k_hvp<L, TH><<<(unsigned)G, XF_THREADS, 0, ctx->stream>>>(ctx->group_start.as<int32_t>(), ctx->group_nbr.as<int32_t>(),
             ctx->pi.as<int32_t>(), ctx->Pcap, ctx->base.as<short4>(), ctx->cfg.dx, ctx->frac.as<TH>(), ctx->scratch.as<TH>(), x0, x1, alt, out,
