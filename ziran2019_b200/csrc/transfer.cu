@@ -1,7 +1,7 @@
 // Particle <-> grid transfers of the implicit substep (helpers in xfer.cuh).
 //
 // Kernels
-//  k_p2g     particlesToGridHelper<APIC> (MpmSimulationBase.cpp:563-608)
+//  k_p2g_reg particlesToGridHelper<APIC> (MpmSimulationBase.cpp:563-608)
 //  k_stress  MpmForceBase::updatePositionBasedState (MpmForceBase.cpp:306-344):
 //            G2P of grad(vn+dv), F = (I + dt grad v) Fn, stress and Hessian scratch
 //  k_force   rasterizeForceToTVStack (MpmForceBase.cpp:102-152)
@@ -17,8 +17,15 @@ namespace zmpm {
 
 // ------------------------------------------------------------------ P2G ----
 // Also writes each particle's fractional cell offsets (frac) for the FP32 HVP.
-template <class L, class TH>
-__global__ void __launch_bounds__(XF_THREADS) k_p2g(const int32_t* __restrict__ group_start, const int32_t* __restrict__ group_nbr,
+// P2G with per-cell register accumulation: thread -> one cell of the page and
+// every (blockDim/NPB)-th particle of it; NCP of the four grid components
+// (mass, momentum x, y, z) are summed for the cell's 27 stencil nodes in FP64
+// registers per pass and added to the shared window once per pass, so the
+// window sees one atomic per (thread, node, component) instead of one per
+// (particle, node, component).  APIC P2G: m_i += w m_p, (mv)_i += w m_p (v_p +
+// C_p (x_i - x_p)) in FP64.
+template <class L, class TH, int NCP>
+__global__ void __launch_bounds__(XF_THREADS) k_p2g_reg(const int32_t* __restrict__ group_start, const int32_t* __restrict__ group_nbr,
     const double* __restrict__ pd, int64_t cap, const short4* __restrict__ base, double dx, double* __restrict__ gm, double* __restrict__ gmv,
     TH* __restrict__ frac)
 {
@@ -32,34 +39,64 @@ __global__ void __launch_bounds__(XF_THREADS) k_p2g(const int32_t* __restrict__ 
     const double inv_dx = 1.0 / dx;
     const int s0 = group_start[g], s1 = group_start[g + 1];
     build_cell_layout<L>(cl, base, s0, s1);
-    for (int q = threadIdx.x; q < cl.layers * NPB; q += blockDim.x) {
-        const int r = q / NPB, ce = q % NPB;
-        if (r >= cl.cnt[ce]) continue;
-        const int s = s0 + cl.start[ce] + r;
-        const short4 b = base[s];
-        double xp[3], w[3][3], dwr[3][3];
+    const int ce = threadIdx.x % NPB;
+    const int lx = ce >> (L::YB + L::ZB), ly = (ce >> L::ZB) & (L::BY - 1), lz = ce & (L::BZ - 1);
+    const int cnt = cl.cnt[ce], first = s0 + cl.start[ce];
+#pragma unroll 1
+    for (int c0 = 0; c0 < 4; c0 += NCP) {
+        double a[27][NCP];
 #pragma unroll
-        for (int d = 0; d < 3; ++d) {
-            xp[d] = pd[(PD_X + d) * cap + s];
-            double d0 = inv_dx * xp[d] - (double)((&b.x)[d]);
-            frac[d * cap + s] = (TH)d0;
-            bspline(d0, w[d], dwr[d]);
+        for (int n = 0; n < 27; ++n)
+#pragma unroll
+            for (int c = 0; c < NCP; ++c) a[n][c] = 0.0;
+        for (int r = threadIdx.x / NPB; r < cnt; r += blockDim.x / NPB) {
+            const int s = first + r;
+            const short4 b = base[s];
+            double xp[3], w[3][3], dwr[3][3];
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                xp[d] = pd[(PD_X + d) * cap + s];
+                const double d0 = inv_dx * xp[d] - (double)((&b.x)[d]);
+                if (c0 == 0) frac[d * cap + s] = (TH)d0;
+                bspline(d0, w[d], dwr[d]);
+            }
+            const double mass = pd[PD_M * cap + s];
+            double mom[NCP], Cm[NCP][3];
+#pragma unroll
+            for (int c = 0; c < NCP; ++c) {
+                const int comp = c0 + c; // 0: mass, 1..3: momentum row comp-1
+                if (comp == 0) {
+                    mom[c] = mass;
+                    Cm[c][0] = Cm[c][1] = Cm[c][2] = 0.0;
+                }
+                else {
+                    const int rr = comp - 1;
+                    mom[c] = mass * pd[(PD_V + rr) * cap + s];
+#pragma unroll
+                    for (int q = 0; q < 3; ++q) Cm[c][q] = mass * pd[(PD_C + 3 * rr + q) * cap + s];
+                }
+            }
+            for_stencil<L>(lx, ly, lz, w, dwr, inv_dx, [&](int, int, int i, int j, int k, double wijk, const double*) {
+                const double xi[3] = { (b.x + i) * dx - xp[0], (b.y + j) * dx - xp[1], (b.z + k) * dx - xp[2] };
+                const int n = 9 * i + 3 * j + k;
+#pragma unroll
+                for (int c = 0; c < NCP; ++c) a[n][c] += (Cm[c][0] * xi[0] + Cm[c][1] * xi[1] + Cm[c][2] * xi[2] + mom[c]) * wijk;
+            });
         }
-        const double mass = pd[PD_M * cap + s];
-        double mom[3], Cm[9];
+        if (threadIdx.x / NPB < cnt) {
 #pragma unroll
-        for (int d = 0; d < 3; ++d) mom[d] = mass * pd[(PD_V + d) * cap + s];
+            for (int i = 0; i < 3; ++i)
 #pragma unroll
-        for (int q = 0; q < 9; ++q) Cm[q] = mass * pd[(PD_C + q) * cap + s];
-        const int lx = b.x & (L::BX - 1), ly = b.y & (L::BY - 1), lz = b.z & (L::BZ - 1);
-        for_stencil<L>(lx, ly, lz, w, dwr, inv_dx, [&](int t, int e, int i, int j, int k, double wijk, const double*) {
-            double xi[3] = { (b.x + i) * dx - xp[0], (b.y + j) * dx - xp[1], (b.z + k) * dx - xp[2] };
-            double* a = acc + t * 4 * NPB + e;
-            atomicAdd(a, mass * wijk);
+                for (int j = 0; j < 3; ++j)
 #pragma unroll
-            for (int r = 0; r < 3; ++r)
-                atomicAdd(a + (1 + r) * NPB, (Cm[3 * r] * xi[0] + Cm[3 * r + 1] * xi[1] + Cm[3 * r + 2] * xi[2] + mom[r]) * wijk);
-        });
+                    for (int k = 0; k < 3; ++k) {
+                        int e;
+                        const int t = win_slot<L>(lx + i, ly + j, lz + k, e);
+                        double* dst = acc + t * 4 * NPB + e;
+#pragma unroll
+                        for (int c = 0; c < NCP; ++c) atomicAdd(dst + (c0 + c) * NPB, a[9 * i + 3 * j + k][c]);
+                    }
+        }
     }
     __syncthreads();
     flush_window<4, 1, NPB>(acc, nbr, gm, gmv);
@@ -549,11 +586,11 @@ static int p2g_impl(Ctx* ctx)
     const int64_t G = ctx->G;
     if (G == 0) return ZMPM_OK;
     if (ctx->mixed)
-        k_p2g<L, float><<<(unsigned)G, XF_THREADS, 0, ctx->stream>>>(ctx->group_start.as<int32_t>(), ctx->group_nbr.as<int32_t>(), ctx->pd.as<double>(),
-            ctx->Pcap, ctx->base.as<short4>(), ctx->cfg.dx, ctx->gm.as<double>(), ctx->gmv.as<double>(), ctx->frac.as<float>());
+        k_p2g_reg<L, float, 2><<<(unsigned)G, XF_THREADS, 0, ctx->stream>>>(ctx->group_start.as<int32_t>(), ctx->group_nbr.as<int32_t>(),
+            ctx->pd.as<double>(), ctx->Pcap, ctx->base.as<short4>(), ctx->cfg.dx, ctx->gm.as<double>(), ctx->gmv.as<double>(), ctx->frac.as<float>());
     else
-        k_p2g<L, double><<<(unsigned)G, XF_THREADS, 0, ctx->stream>>>(ctx->group_start.as<int32_t>(), ctx->group_nbr.as<int32_t>(), ctx->pd.as<double>(),
-            ctx->Pcap, ctx->base.as<short4>(), ctx->cfg.dx, ctx->gm.as<double>(), ctx->gmv.as<double>(), ctx->frac.as<double>());
+        k_p2g_reg<L, double, 2><<<(unsigned)G, XF_THREADS, 0, ctx->stream>>>(ctx->group_start.as<int32_t>(), ctx->group_nbr.as<int32_t>(),
+            ctx->pd.as<double>(), ctx->Pcap, ctx->base.as<short4>(), ctx->cfg.dx, ctx->gm.as<double>(), ctx->gmv.as<double>(), ctx->frac.as<double>());
     ++g_kernel_launches;
     return ZMPM_OK;
 }
