@@ -98,8 +98,15 @@ enum zmpm_linear_solver { ZMPM_MINRES = 0, ZMPM_CG = 1 };
 /* Implicit integrator of a substep.  NEWTON: MpmSimulationBase::backwardEulerStep
    (MpmSimulationBase.cpp:610-657).  ADMM: AdmmSimulation::admmStep
    (Projects/admm/AdmmSimulationFoam.h:766-801), the local (per-particle F),
-   global (MINRES on the grid) and dual steps of "Silly Rubber". */
-enum zmpm_integrator { ZMPM_NEWTON = 0, ZMPM_ADMM = 1 };
+   global (MINRES on the grid) and dual steps of "Silly Rubber".  EXPLICIT: the
+   symplectic branch of MpmSimulationBase::advanceOneTimeStep
+   (MpmSimulationBase.cpp:264-281): Kirchhoff stress at the particles
+   (forcesUpdateParticleState), P2G of mass, momentum and force
+   (particlesToGridWithForceHelper<APIC, quadratic, !MLS>, :500-560),
+   gridVelocityExplicitUpdate with collisions (:818-865), the colliders'
+   state at t + dt, trialCollision (:298-311) when `trial_collision` is set,
+   then G2P. */
+enum zmpm_integrator { ZMPM_NEWTON = 0, ZMPM_ADMM = 1, ZMPM_EXPLICIT = 2 };
 
 /* Collision objects (AnalyticCollisionObject, CollisionObject.h:42-195). */
 enum zmpm_collider_shape { ZMPM_HALF_SPACE = 0, ZMPM_SPHERE = 1, ZMPM_BOX = 2 };
@@ -134,7 +141,7 @@ typedef struct zmpm_solver {
     double admm_local_tolerance;    /* local_tolerance of the per-particle Newton, default 1e-8 */
     double admm_global_tolerance;   /* global_tolerance: absolute MINRES tolerance, default 1e-6 */
     int32_t admm_global_max_iterations; /* global_max_iteration, default 10000 */
-    int32_t pad1;
+    int32_t trial_collision;        /* EXPLICIT: useTrialCollision (MpmSimulationBase.cpp:61, default 1) */
 } zmpm_solver;
 
 typedef struct zmpm_collider {

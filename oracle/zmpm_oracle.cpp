@@ -1151,7 +1151,7 @@ struct Collider {
         dsdt = (T)d.scale_velocity;
     }
     // AnalyticLevelSet::queryInside for the three shapes (AnalyticLevelSet.cpp:111-119, 272-287, 435-451, 504-539)
-    bool queryInside(const T X[3], T N[3]) const
+    bool queryInside(const T X[3], T N[3], T* phi_out = nullptr) const
     {
         if (d.shape == ZMPM_HALF_SPACE) {
             T n[3] = { (T)d.b[0], (T)d.b[1], (T)d.b[2] };
@@ -1159,6 +1159,7 @@ struct Collider {
             for (int i = 0; i < 3; ++i) n[i] /= nn;
             T phi = n[0] * (X[0] - (T)d.a[0]) + n[1] * (X[1] - (T)d.a[1]) + n[2] * (X[2] - (T)d.a[2]);
             if (phi <= 0) {
+                if (phi_out) *phi_out = phi;
                 for (int i = 0; i < 3; ++i) N[i] = n[i];
                 return true;
             }
@@ -1170,6 +1171,7 @@ struct Collider {
             T r = (T)d.radius;
             if (d2 < r * r) {
                 T dist = std::sqrt(d2);
+                if (phi_out) *phi_out = dist - r;
                 if (dist < T(1e-7)) {
                     N[0] = 1;
                     N[1] = N[2] = 0;
@@ -1199,10 +1201,25 @@ struct Collider {
         }
         T phi = std::min(dd[imax], T(0)) + std::sqrt(q2);
         if (phi > 0) return false;
+        if (phi_out) *phi_out = phi;
         for (int i = 0; i < 3; ++i) N[i] = 0;
         N[imax] = xp[imax] >= 0 ? T(1) : T(-1);
         return true;
     }
+    // AnalyticCollisionObject::queryInside (world space), CollisionObject.cpp:232-246
+    bool queryInsideWorld(const T x[3], T& phi, T n[3]) const
+    {
+        T xb[3] = { x[0] - b[0], x[1] - b[1], x[2] - b[2] };
+        T one_over_s = 1 / s;
+        T X[3];
+        for (int i = 0; i < 3; ++i) X[i] = (R[0][i] * xb[0] + R[1][i] * xb[1] + R[2][i] * xb[2]) * one_over_s;
+        T N[3];
+        if (!queryInside(X, N, &phi)) return false;
+        for (int i = 0; i < 3; ++i) n[i] = R[i][0] * N[0] + R[i][1] * N[1] + R[i][2] * N[2];
+        phi *= s;
+        return true;
+    }
+
     // AnalyticCollisionObject::getBoundaryVelocityAndNormal, CollisionObject.cpp:313-338
     bool boundaryVelocityAndNormal(const T x[3], T vb[3], T n[3]) const
     {
@@ -2439,6 +2456,108 @@ struct Sim {
         return ZMPM_OK;
     }
 
+    // -------------------------------------------------------- explicit --
+    // The symplectic branch of advanceOneTimeStep, MpmSimulationBase.cpp:264-281.
+    const std::vector<T>* g2p_v = nullptr; // grid velocities for G2P (explicit substep)
+
+    int substepExplicit(double dt_in, const zmpm_solver& s, zmpm_stats& st)
+    {
+        dt = (T)dt_in;
+        implicit_ready = false;
+        // forcesUpdateParticleState + FBasedMpmForceHelper::updateState
+        // (MpmSimulationBase.cpp:682-700, FBasedMpmForceHelper.cpp:44-64): V0 tau(F)
+        stress.resize(P);
+        scratch.resize(P);
+#pragma omp parallel for schedule(static)
+        for (int64_t i = 0; i < P; ++i) {
+            if (model[i].kind == ZMPM_MODEL_NONE) {
+                stress[i] = M3<T>::zero();
+                continue;
+            }
+            M3<T> Fp = load9(F, i);
+            updateScratch(model[i], Fp, scratch[i]);
+            stress[i] = mulT(scaled(firstPiola(model[i], scratch[i]), vol[i]), Fp);
+            if (visco[i].on) {
+                // FElasticNonequilibratedBasedMpmForceHelper::updateState (h:39-60): + V0 tau(Fe)
+                Model<T> mv;
+                mv.kind = ZMPM_MODEL_STVK_HENCKY_ISOTROPIC;
+                mv.mu = visco[i].mu;
+                mv.lambda = visco[i].lambda;
+                Scratch<T> sv;
+                M3<T> Fe_ = load9(Fe, i);
+                updateScratch(mv, Fe_, sv);
+                stress[i] = add(stress[i], mulT(scaled(firstPiola(mv, sv), vol[i]), Fe_));
+            }
+        }
+        int rc = sortParticlesAndPolluteGrid();
+        if (rc != ZMPM_OK) return rc;
+        // particlesToGridWithForceHelper<APIC, quadratic, !MLS> (:500-560): mass,
+        // momentum, and f_i -= sum_p V0 tau_p grad w_ip, then the normalisation
+        particlesToGrid();
+        std::vector<T> f(3 * N, 0);
+        rasterize(T(1), stress, f);
+        // FractureSimulation::particlesToGrid runs the damage update after P2G
+#pragma omp parallel for schedule(static)
+        for (int64_t i = 0; i < P; ++i)
+            if (damage[i].kind == ZMPM_DAMAGE_RANKINE && model[i].kind == ZMPM_MODEL_NEOHOOKEAN_BORDEN)
+                rankineUpdate(model[i], damage[i], load9(F, i));
+        // gridVelocityExplicitUpdate (:818-865)
+        for (auto& c : colliders) c.update(time);
+        mvec.assign(N, 0);
+        vn.assign(3 * N, 0);
+        std::vector<T> vnew(3 * N, 0);
+        std::vector<uint8_t> collided_e(N, 0);
+        iterateBlocks(true, [&](const int node[3], G& g) {
+            const int64_t id = g.idx;
+            mvec[id] = g.m;
+            const T dt_over_mi = dt / g.m;
+            T xi[3], vi[3];
+            for (int d = 0; d < 3; ++d) {
+                vn[3 * id + d] = g.v[d];
+                xi[d] = node[d] * dx;
+                vi[d] = g.v[d] + gravity[d] * dt + f[3 * id + d] * dt_over_mi;
+            }
+            M3<T> K;
+            collided_e[id] = multiObjectCollision(colliders, xi, vi, K) ? 1 : 0;
+            for (int d = 0; d < 3; ++d) vnew[3 * id + d] = vi[d];
+        });
+        // the colliders move to t + dt before trialCollision (:273-279)
+        for (auto& c : colliders) c.update(time + dt_in);
+        if (s.trial_collision) {
+            // MpmSimulationBase::trialCollision (:298-311) and
+            // AnalyticCollisionObject::trialCollision (CollisionObject.cpp:48-64)
+            iterateBlocks(true, [&](const int node[3], G& g) {
+                const int64_t id = g.idx;
+                if (collided_e[id]) return;
+                T* vi = &vnew[3 * id];
+                const T xi[3] = { node[0] * dx, node[1] * dx, node[2] * dx };
+                for (const auto& o : colliders) {
+                    if (o.d.type == ZMPM_GHOST) continue;
+                    const T xt[3] = { xi[0] + dt * vi[0], xi[1] + dt * vi[1], xi[2] + dt * vi[2] };
+                    T phi, n[3];
+                    if (o.queryInsideWorld(xt, phi, n))
+                        for (int d = 0; d < 3; ++d) vi[d] -= (phi / dt) * n[d];
+                }
+            });
+        }
+        dv.assign(3 * N, 0);
+        for (int64_t i = 0; i < 3 * N; ++i) dv[i] = vnew[i] - vn[i];
+        g2p_v = &vnew;
+        int too_fast = gridToParticles();
+        g2p_v = nullptr;
+        time += dt_in;
+        st.newton_converged = 1;
+        st.cfl_violation = too_fast;
+        st.num_particles = P;
+        st.num_groups = (int64_t)group.size();
+        st.num_blocks = (int64_t)blocks.size();
+        st.num_nodes = N;
+        int64_t nc = 0;
+        for (auto c : collided_e) nc += c;
+        st.num_collision_nodes = nc;
+        return too_fast ? ZMPM_CFL_VIOLATION : ZMPM_OK;
+    }
+
     // ------------------------------------------------------------- G2P --
     // constructNewVelocityFromNewtonResult + gridToParticlesHelper<APIC,deg2,!MLS>
     // + evolveStrain + applyPlasticity, MpmSimulationBase.cpp:867-877, 906-1030
@@ -2448,7 +2567,7 @@ struct Sim {
             g.new_v[0] = g.new_v[1] = g.new_v[2] = 0;
         });
         iterateBlocks(true, [&](const int*, G& g) {
-            for (int d = 0; d < 3; ++d) g.new_v[d] = g.v[d] + dv[3 * g.idx + d];
+            for (int d = 0; d < 3; ++d) g.new_v[d] = g2p_v ? (*g2p_v)[3 * g.idx + d] : g.v[d] + dv[3 * g.idx + d];
         });
         T D_inverse = 4 / (dx * dx);
         int too_fast = 0;
@@ -2542,6 +2661,7 @@ struct Sim {
             all_models = all_models && model[i].kind != ZMPM_MODEL_NONE;
         }
         bool conv = true;
+        if (s.integrator == ZMPM_EXPLICIT) return substepExplicit(dt_in, s, st);
         if (s.integrator == ZMPM_ADMM) {
             // AdmmSimulation::advanceOneTimeStep, AdmmSimulationFoam.h:816-837
             if (!all_models) {

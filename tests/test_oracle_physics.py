@@ -273,3 +273,62 @@ def test_admm_viscoelastic_substeps(oracle):
     assert np.all(np.isfinite(Fe))
     s.integrator = abi.NEWTON
     assert s.lib.substep(s.ctx, 2e-3, C.byref(s.solver()), None) == abi.BAD_ARG
+
+
+def _explicit_cube(lib, gravity=(0, -9.8, 0), kind="fcr", v0=(0.3, -1.0, 0.2), ground=None, seed=1, lo=(0.375, 0.105, 0.375)):
+    dx = 1.0 / 64
+    s = mpm.MpmSimulation(dx, gravity=gravity, precision="fp64", lib=lib)
+    build_scene(s, kind=kind, n=6, dx=dx, v0=v0, ground=ground, seed=seed, lo=lo)
+    s.useExplicit()
+    return s
+
+
+def test_explicit_free_fall_is_exact(oracle):
+    """Symplectic substeps of an unstressed cube in free fall (F = I, no
+    colliders): every particle gains g dt per substep, C stays zero."""
+    s = _explicit_cube(oracle)
+    v0 = s.getParticles()["V"].copy()
+    dt = 1e-3
+    for _ in range(10):
+        assert s.advanceOneTimeStep(dt) == abi.OK
+    p = s.getParticles()
+    want = v0 + 10 * dt * np.array([0, -9.8, 0])
+    np.testing.assert_allclose(p["V"], want, rtol=0, atol=1e-12)
+    np.testing.assert_allclose(p["F"].reshape(-1, 9), np.tile(np.eye(3).ravel(), (len(v0), 1)), rtol=0, atol=1e-12)
+
+
+def test_explicit_conserves_momentum(oracle):
+    """Without gravity and colliders, APIC P2G/G2P with the elastic force
+    conserves total linear momentum to round-off while the cube deforms."""
+    s = _explicit_cube(oracle, gravity=(0, 0, 0), v0=(0, 0, 0))
+    p = s.getParticles()
+    rng = np.random.default_rng(4)
+    V = rng.normal(0, 0.2, p["V"].shape)
+    s.setParticles(V=V)
+    m = np.full(len(V), 1000.0 * (1 / 64) ** 3 / 8)
+    mom0 = (m[:, None] * V).sum(0)
+    for _ in range(10):
+        assert s.advanceOneTimeStep(2e-4) == abi.OK
+    p = s.getParticles()
+    assert np.abs(p["F"].reshape(-1, 3, 3) - np.eye(3)).max() > 1e-4
+    mom = (m[:, None] * p["V"]).sum(0)
+    assert np.abs(mom - mom0).max() < 1e-12 * np.abs(m[:, None] * V).sum()
+
+
+def test_explicit_trial_collision_keeps_particles_above_ground(oracle):
+    """A cube falling fast onto a sticky ground: the explicit collision at t and
+    the trial collision against the ground at t + dt keep particles from
+    crossing it; turning trial collision off changes the landing substep.  The
+    ground sits just below the grid plane y = 7 dx, where nodes that did not
+    collide at t reach it within one substep."""
+    dx = 1.0 / 64
+    ground = 7 * dx - 1e-3
+    runs = []
+    for trial in (True, False):
+        s = _explicit_cube(oracle, v0=(0, -3.0, 0), ground=ground, lo=(0.375, 8 * dx, 0.375))
+        s.useExplicit(trial_collision=trial)
+        for _ in range(40):
+            assert s.advanceOneTimeStep(5e-4) == abi.OK
+        runs.append(s.getParticles())
+    assert runs[0]["X"][:, 1].min() > ground - dx
+    assert np.abs(runs[0]["V"] - runs[1]["V"]).max() > 1e-6

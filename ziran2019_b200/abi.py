@@ -32,7 +32,7 @@ LAYOUT_AUTO, LAYOUT_244, LAYOUT_444 = 0, 1, 2
 MODEL_NONE, MODEL_NEOHOOKEAN_BORDEN, MODEL_STVK_HENCKY_ISOTROPIC, MODEL_FIXED_COROTATED = 0, 1, 2, 3
 PLASTIC_NONE, PLASTIC_VON_MISES = 0, 1
 DAMAGE_NONE, DAMAGE_RANKINE = 0, 1
-NEWTON, ADMM = 0, 1
+NEWTON, ADMM, EXPLICIT = 0, 1, 2
 MINRES, CG = 0, 1
 HALF_SPACE, SPHERE, BOX = 0, 1, 2
 STICKY, SLIP, SEPARATE, GHOST = 1, 2, 3, 4
@@ -66,7 +66,7 @@ class Solver(C.Structure):
         ("admm_local_tolerance", C.c_double),
         ("admm_global_tolerance", C.c_double),
         ("admm_global_max_iterations", C.c_int32),
-        ("pad1", C.c_int32),
+        ("trial_collision", C.c_int32),
     ]
 
 

@@ -295,7 +295,7 @@ int check_ready(Ctx* ctx)
 
 namespace zmpm {
 
-int upload_colliders(Ctx* ctx, double time)
+int upload_colliders(Ctx* ctx, double time, int slot)
 {
     const int n = (int)ctx->colliders.size();
     if (n == 0) return ZMPM_OK;
@@ -318,7 +318,8 @@ int upload_colliders(Ctx* ctx, double time)
         d.s = c.scale + time * c.scale_velocity;
         d.dsdt = c.scale_velocity;
     }
-    ZMPM_CUDA(cudaMemcpyAsync(ctx->dcolliders.p, h.data(), n * sizeof(DevCollider), cudaMemcpyHostToDevice, ctx->stream));
+    ZMPM_CUDA(cudaMemcpyAsync(ctx->dcolliders.as<DevCollider>() + (size_t)slot * MAX_COLLIDERS, h.data(), n * sizeof(DevCollider),
+        cudaMemcpyHostToDevice, ctx->stream));
     return ZMPM_OK;
 }
 
@@ -359,6 +360,7 @@ void zmpm_default_solver(zmpm_solver* s, int32_t linear_solver, int32_t precisio
     s->admm_local_tolerance = 1e-8;
     s->admm_global_tolerance = 1e-6;
     s->admm_global_max_iterations = 10000;
+    s->trial_collision = 1; // useTrialCollision, MpmSimulationBase.cpp:61
     if (linear_solver == ZMPM_MINRES)
         s->krylov_tolerance = 1;
     else
@@ -417,7 +419,8 @@ int zmpm_create(const zmpm_config* cfg, zmpm_ctx** out)
     if ((e = ctx->counters.ensure(sizeof(DevCounters))) != cudaSuccess) return fail(e);
     if ((e = ctx->scal.ensure(sizeof(SolverScalars))) != cudaSuccess) return fail(e);
     if ((e = ctx->red.ensure(RED_N * RED_MAX_CTAS * sizeof(double))) != cudaSuccess) return fail(e);
-    if ((e = ctx->dcolliders.ensure(MAX_COLLIDERS * sizeof(DevCollider))) != cudaSuccess) return fail(e);
+    // two collider states: at t, and at t + dt for the explicit substep's trial collision
+    if ((e = ctx->dcolliders.ensure(2 * MAX_COLLIDERS * sizeof(DevCollider))) != cudaSuccess) return fail(e);
     cudaMemset(ctx->counters.p, 0, sizeof(DevCounters));
     cudaMemset(ctx->scal.p, 0, sizeof(SolverScalars));
     *out = ctx;
@@ -717,8 +720,8 @@ static int begin_implicit_impl(zmpm_ctx* ctx, double dt, bool damage = true)
 int zmpm_substep(zmpm_ctx* ctx, double dt, const zmpm_solver* s, zmpm_stats* st)
 {
     if (!ctx || !s || !(dt > 0) || s->newton_max_iterations < 0 || s->krylov_max_iterations < 0) return ZMPM_BAD_ARG;
-    const bool admm = s->integrator == ZMPM_ADMM;
-    if (!admm && s->integrator != ZMPM_NEWTON) return ZMPM_BAD_ARG;
+    const bool admm = s->integrator == ZMPM_ADMM, expl = s->integrator == ZMPM_EXPLICIT;
+    if (!admm && !expl && s->integrator != ZMPM_NEWTON) return ZMPM_BAD_ARG;
     if (admm && (s->admm_iterations < 0 || s->admm_global_max_iterations < 0 || !(s->admm_rho_scale > 0))) return ZMPM_BAD_ARG;
     cudaSetDevice(ctx->device);
     if (admm) {
@@ -735,8 +738,8 @@ int zmpm_substep(zmpm_ctx* ctx, double dt, const zmpm_solver* s, zmpm_stats* st)
             ctx->pd_active = PD_FIELDS;
         }
     }
-    else if (ctx->has_visco) {
-        ctx->err = "viscoelastic particles need the ADMM integrator (StvkWithHencky has no stress differential)";
+    else if (ctx->has_visco && !expl) {
+        ctx->err = "viscoelastic particles need the ADMM or explicit integrator (StvkWithHencky has no stress differential)";
         return ZMPM_BAD_ARG;
     }
     zmpm_stats local;
@@ -744,9 +747,22 @@ int zmpm_substep(zmpm_ctx* ctx, double dt, const zmpm_solver* s, zmpm_stats* st)
     std::memset(st, 0, sizeof(*st));
     const int64_t launches0 = g_kernel_launches;
     ZMPM_CUDA(cudaEventRecord(ctx->ev0, ctx->stream));
-    int rc = begin_implicit_impl(ctx, dt, !admm);
-    if (rc) return rc;
-    rc = admm ? run_admm(ctx, *s) : run_newton(ctx, *s);
+    int rc;
+    if (expl) {
+        rc = upload(ctx);
+        if (rc) return rc;
+        ctx->dt = dt;
+        ctx->implicit_ready = false;
+        rc = run_binning(ctx);
+        if (rc) return rc;
+        ctx->graph_used = false;
+        rc = run_explicit(ctx, *s);
+    }
+    else {
+        rc = begin_implicit_impl(ctx, dt, !admm);
+        if (rc) return rc;
+        rc = admm ? run_admm(ctx, *s) : run_newton(ctx, *s);
+    }
     if (rc) return rc;
     rc = run_g2p(ctx);
     if (rc) return rc;

@@ -201,7 +201,9 @@ int run_binning(Ctx* ctx);
 int run_p2g(Ctx* ctx, bool damage = true);            // P2G (+ damage hook) + grid normalisation + Newton setup
 int run_newton(Ctx* ctx, const zmpm_solver& s);       // backward-Euler Newton
 int run_g2p(Ctx* ctx);                                 // G2P + evolveStrain + plasticity
-int upload_colliders(Ctx* ctx, double time);
+int upload_colliders(Ctx* ctx, double time, int slot = 0);    // slot 1: the state at t + dt
+int run_explicit(Ctx* ctx, const zmpm_solver& s);      // symplectic substep up to G2P
+int launch_explicit_stress(Ctx* ctx);                  // V0 tau(F) (+ V0 tau(Fe)) into the stress buffer
 int launch_update(Ctx* ctx, bool gated = true);       // G2P(vn+dv) -> stress -> force P2G
 int launch_adj_g2p(Ctx* ctx, double* vsbar);           // adjoint of G2P (adjoint.cu)
 int launch_adj_particle(Ctx* ctx, const double* lam);  // adjoint of the force term, P2G and E

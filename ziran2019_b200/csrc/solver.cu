@@ -88,13 +88,14 @@ __device__ __forceinline__ void project3(const int8_t* col, const double* P6, in
 
 // ------------------------------------------------------- collision query --
 // AnalyticLevelSet::queryInside for half space, sphere and axis-aligned box.
-__device__ bool collider_inside(const DevCollider& c, const double X[3], double N[3])
+__device__ bool collider_inside(const DevCollider& c, const double X[3], double N[3], double* phi_out = nullptr)
 {
     if (c.shape == ZMPM_HALF_SPACE) {
         double nn = sqrt(c.b[0] * c.b[0] + c.b[1] * c.b[1] + c.b[2] * c.b[2]);
         double n[3] = { c.b[0] / nn, c.b[1] / nn, c.b[2] / nn };
         double phi = n[0] * (X[0] - c.a[0]) + n[1] * (X[1] - c.a[1]) + n[2] * (X[2] - c.a[2]);
         if (phi <= 0) {
+            if (phi_out) *phi_out = phi;
             N[0] = n[0];
             N[1] = n[1];
             N[2] = n[2];
@@ -107,6 +108,7 @@ __device__ bool collider_inside(const DevCollider& c, const double X[3], double 
         double d2 = t[0] * t[0] + t[1] * t[1] + t[2] * t[2];
         if (d2 < c.radius * c.radius) {
             double d = sqrt(d2);
+            if (phi_out) *phi_out = d - c.radius;
             if (d < 1e-7) {
                 N[0] = 1;
                 N[1] = N[2] = 0;
@@ -136,6 +138,7 @@ __device__ bool collider_inside(const DevCollider& c, const double X[3], double 
     }
     double phi = fmin(dd[im], 0.0) + sqrt(q2);
     if (phi > 0) return false;
+    if (phi_out) *phi_out = phi;
     N[0] = N[1] = N[2] = 0;
     N[im] = xp[im] >= 0 ? 1.0 : -1.0;
     return true;
@@ -172,6 +175,21 @@ __device__ bool collider_resolve(const DevCollider& c, const double x[3], double
         }
     }
     for (int i = 0; i < 3; ++i) v[i] += vo[i];
+    return true;
+}
+
+// AnalyticCollisionObject::queryInside in world space (CollisionObject.cpp:232-246):
+// signed distance scaled by s, world normal.
+__device__ bool collider_query_world(const DevCollider& c, const double x[3], double& phi, double n[3])
+{
+    double xb[3] = { x[0] - c.t[0], x[1] - c.t[1], x[2] - c.t[2] };
+    double ios = 1 / c.s;
+    double X[3];
+    for (int i = 0; i < 3; ++i) X[i] = (c.R[i] * xb[0] + c.R[3 + i] * xb[1] + c.R[6 + i] * xb[2]) * ios;
+    double N[3];
+    if (!collider_inside(c, X, N, &phi)) return false;
+    for (int i = 0; i < 3; ++i) n[i] = c.R[3 * i] * N[0] + c.R[3 * i + 1] * N[1] + c.R[3 * i + 2] * N[2];
+    phi *= c.s;
     return true;
 }
 
@@ -292,6 +310,66 @@ __global__ void __launch_bounds__(ND_THREADS) k_grid_init(NodeGeom ng, const dou
         }
         col[n] = c;
         for (int k = 0; k < 6; ++k) P6[k * ng.nn + n] = P[k];
+    }
+    __shared__ int tot;
+    if (threadIdx.x == 0) tot = 0;
+    __syncthreads();
+    atomicAdd(&tot, local);
+    __syncthreads();
+    if (threadIdx.x == 0 && tot) atomicAdd(nactive, (unsigned long long)tot);
+}
+
+// ------------------------------------------------------ explicit update --
+// particlesToGrid normalisation + gridVelocityExplicitUpdate
+// (MpmSimulationBase.cpp:474-485, 818-865): vn = (mv)/m, v = vn + dt g +
+// f dt/m with the colliders at t (cols), then for nodes that did not collide
+// trialCollision with the colliders moved to t + dt (cols1;
+// MpmSimulationBase.cpp:298-311, CollisionObject.cpp:48-64):
+// v -= (phi(x_i + dt v) / dt) n.  vstar = v, dv = v - vn, facc zeroed.
+template <class L>
+__global__ void __launch_bounds__(ND_THREADS) k_grid_explicit(NodeGeom ng, const double* __restrict__ gm, const double* __restrict__ gmv,
+    double* __restrict__ facc, const int4* __restrict__ block_page, double dx, double gx, double gy, double gz, double dt,
+    const DevCollider* __restrict__ cols, const DevCollider* __restrict__ cols1, int ncols, int trial, double* __restrict__ vn,
+    double* __restrict__ dv, double* __restrict__ vstar, int8_t* __restrict__ col, unsigned long long* __restrict__ nactive)
+{
+    constexpr int NPB = L::NPB;
+    const double g[3] = { gx, gy, gz };
+    int local = 0;
+    for (int64_t n = (int64_t)blockIdx.x * ND_THREADS + threadIdx.x; n < ng.nn; n += (int64_t)gridDim.x * ND_THREADS) {
+        const int64_t b = n / NPB;
+        const int e = (int)(n - b * NPB);
+        const double m = gm[n];
+        double v[3] = { 0, 0, 0 }, vi[3] = { 0, 0, 0 };
+        int8_t c = 0;
+        if (m != 0) {
+            ++local;
+            const double dt_over_mi = dt / m;
+            for (int k = 0; k < 3; ++k) {
+                v[k] = gmv[vidx<NPB>(n, k)] / m;
+                vi[k] = v[k] + g[k] * dt + facc[vidx<NPB>(n, k)] * dt_over_mi;
+            }
+            const int4 bp = block_page[b];
+            const int lx = e >> (L::YB + L::ZB), ly = (e >> L::ZB) & (L::BY - 1), lz = e & (L::BZ - 1);
+            const double xi[3] = { (bp.x * L::BX + lx) * dx, (bp.y * L::BY + ly) * dx, (bp.z * L::BZ + lz) * dx };
+            double P[6];
+            c = multi_collide(cols, ncols, xi, vi, P, false) ? 1 : 0;
+            if (!c && trial)
+                for (int o = 0; o < ncols; ++o) {
+                    if (cols1[o].type == ZMPM_GHOST) continue;
+                    const double xt[3] = { xi[0] + dt * vi[0], xi[1] + dt * vi[1], xi[2] + dt * vi[2] };
+                    double phi, nrm[3];
+                    if (collider_query_world(cols1[o], xt, phi, nrm))
+                        for (int k = 0; k < 3; ++k) vi[k] -= (phi / dt) * nrm[k];
+                }
+        }
+        for (int k = 0; k < 3; ++k) {
+            const int64_t i = vidx<NPB>(n, k);
+            vn[i] = v[k];
+            dv[i] = vi[k] - v[k];
+            vstar[i] = vi[k];
+            facc[i] = 0;
+        }
+        col[n] = c;
     }
     __shared__ int tot;
     if (threadIdx.x == 0) tot = 0;
@@ -907,6 +985,52 @@ int run_p2g(Ctx* ctx, bool damage)
                 ctx->cfg.dx, g[0], g[1], g[2], ctx->dt, ctx->dcolliders.as<DevCollider>(), (int)ctx->colliders.size(), ctx->vn.as<double>(),
                 ctx->dv.as<double>(), ctx->vstar.as<double>(), ctx->collided.as<int8_t>(), ctx->proj.as<double>(),
                 reinterpret_cast<unsigned long long*>(&dc->N), &dc->flags);
+        ++g_kernel_launches;
+    }
+    ZMPM_CUDA(cudaGetLastError());
+    return ZMPM_OK;
+}
+
+// The symplectic substep after binning, up to G2P (MpmSimulationBase.cpp:
+// 264-281): particle stress, P2G of mass, momentum and force, the fracture
+// hook, the explicit grid update with collisions and trial collision.
+int run_explicit(Ctx* ctx, const zmpm_solver& s)
+{
+    cudaStream_t st = ctx->stream;
+    const int64_t nn = ctx->B * ctx->npb();
+    int rc = ensure_node_buffers(ctx);
+    if (rc) return rc;
+    ZMPM_CUDA(cudaMemsetAsync(ctx->scal.p, 0, sizeof(SolverScalars), st));
+    ZMPM_CUDA(cudaMemsetAsync(ctx->gm.p, 0, nn * sizeof(double), st));
+    ZMPM_CUDA(cudaMemsetAsync(ctx->gmv.p, 0, 3 * nn * sizeof(double), st));
+    ZMPM_CUDA(cudaMemsetAsync(ctx->facc.p, 0, 3 * nn * sizeof(double), st));
+    rc = launch_explicit_stress(ctx);
+    if (rc) return rc;
+    rc = launch_p2g(ctx);
+    if (rc) return rc;
+    rc = launch_force_scatter(ctx, ctx->facc.as<double>());
+    if (rc) return rc;
+    rc = launch_damage(ctx);
+    if (rc) return rc;
+    rc = upload_colliders(ctx, ctx->time, 0);
+    if (rc) return rc;
+    rc = upload_colliders(ctx, ctx->time + ctx->dt, 1);
+    if (rc) return rc;
+    if (nn > 0) {
+        NodeGeom ng = node_geom(ctx);
+        DevCounters* dc = ctx->counters.as<DevCounters>();
+        const double* g = ctx->cfg.gravity;
+        const DevCollider* c0 = ctx->dcolliders.as<DevCollider>();
+        const DevCollider* c1 = c0 + MAX_COLLIDERS;
+        const int nc = (int)ctx->colliders.size(), trial = s.trial_collision ? 1 : 0;
+        if (ctx->layout == 1)
+            k_grid_explicit<Layout244><<<ng.parts, ND_THREADS, 0, st>>>(ng, ctx->gm.as<double>(), ctx->gmv.as<double>(), ctx->facc.as<double>(),
+                ctx->block_page.as<int4>(), ctx->cfg.dx, g[0], g[1], g[2], ctx->dt, c0, c1, nc, trial, ctx->vn.as<double>(), ctx->dv.as<double>(),
+                ctx->vstar.as<double>(), ctx->collided.as<int8_t>(), reinterpret_cast<unsigned long long*>(&dc->N));
+        else
+            k_grid_explicit<Layout444><<<ng.parts, ND_THREADS, 0, st>>>(ng, ctx->gm.as<double>(), ctx->gmv.as<double>(), ctx->facc.as<double>(),
+                ctx->block_page.as<int4>(), ctx->cfg.dx, g[0], g[1], g[2], ctx->dt, c0, c1, nc, trial, ctx->vn.as<double>(), ctx->dv.as<double>(),
+                ctx->vstar.as<double>(), ctx->collided.as<int8_t>(), reinterpret_cast<unsigned long long*>(&dc->N));
         ++g_kernel_launches;
     }
     ZMPM_CUDA(cudaGetLastError());

@@ -244,6 +244,63 @@ __global__ void __launch_bounds__(XF_THREADS) k_stress(const int32_t* __restrict
     }
 }
 
+// Explicit substep: FBasedMpmForceHelper::updateState (FBasedMpmForceHelper.cpp:
+// 44-64) stores V0 tau(F) = V0 P(F) F^T per particle (slot order), plus V0
+// tau(Fe) for viscoelastic particles (FElasticNonequilibratedBasedMpmForceHelper.h:
+// 39-60).  TS precision with the FP64 re-evaluation of near-degenerate SVDs.
+template <class TS, class TH>
+__global__ void __launch_bounds__(XF_THREADS) k_explicit_stress(const double* __restrict__ pd, const int32_t* __restrict__ pi, int64_t cap,
+    int64_t P, TS* __restrict__ stress, TH* __restrict__ scr)
+{
+    const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= P) return;
+    const int kind = pi[PI_KIND * cap + s];
+    M3<TS> S = m3_zero<TS>();
+    if (kind != ZMPM_MODEL_NONE) {
+        M3<TS> F;
+#pragma unroll
+        for (int q = 0; q < 9; ++q) F.a[q] = (TS)pd[(PD_F + q) * cap + s];
+        const ModelParams mp{ pd[PD_MU * cap + s], pd[PD_LAM * cap + s], pd[PD_KAPPA * cap + s], pd[PD_G * cap + s] };
+        const double V0 = pd[PD_VOL * cap + s];
+        bool degenerate = false;
+        S = model_update<TS, TH>(kind, mp, (TS)V0, F, F, scr, cap, s, sizeof(TS) == 4 ? &degenerate : nullptr);
+        if constexpr (sizeof(TS) == 4) {
+            if (degenerate) {
+                M3<double> Fd;
+#pragma unroll
+                for (int q = 0; q < 9; ++q) Fd.a[q] = pd[(PD_F + q) * cap + s];
+                S = m3_cast<TS>(model_update<double, TH>(kind, mp, V0, Fd, Fd, scr, cap, s, nullptr));
+            }
+        }
+        if (pi[PI_VISCO * cap + s]) {
+            M3<double> Fe;
+#pragma unroll
+            for (int q = 0; q < 9; ++q) Fe.a[q] = pd[(PD_FE + q) * cap + s];
+            const ModelParams mv{ pd[PD_VMU * cap + s], pd[PD_VLAM * cap + s], 0.0, 1.0 };
+            const M3<double> Se = model_update<double, TH>(ZMPM_MODEL_STVK_HENCKY_ISOTROPIC, mv, V0, Fe, Fe, scr, cap, s, nullptr);
+#pragma unroll
+            for (int q = 0; q < 9; ++q) S.a[q] += (TS)Se.a[q];
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < 9; ++q) stress[q * cap + s] = S.a[q];
+}
+
+int launch_explicit_stress(Ctx* ctx)
+{
+    const int64_t P = ctx->P;
+    if (P == 0) return ZMPM_OK;
+    const unsigned nb = (unsigned)((P + XF_THREADS - 1) / XF_THREADS);
+    if (ctx->mixed)
+        k_explicit_stress<float, float><<<nb, XF_THREADS, 0, ctx->stream>>>(ctx->pd.as<double>(), ctx->pi.as<int32_t>(), ctx->Pcap, P,
+            ctx->stress.as<float>(), ctx->scratch.as<float>());
+    else
+        k_explicit_stress<double, double><<<nb, XF_THREADS, 0, ctx->stream>>>(ctx->pd.as<double>(), ctx->pi.as<int32_t>(), ctx->Pcap, P,
+            ctx->stress.as<double>(), ctx->scratch.as<double>());
+    ++g_kernel_launches;
+    return ZMPM_OK;
+}
+
 template <class L, class TS, class TH>
 __global__ void __launch_bounds__(XF_THREADS) k_force(const int32_t* __restrict__ group_start, const int32_t* __restrict__ group_nbr,
     int64_t cap, const short4* __restrict__ base, double dx, const TH* __restrict__ frac, const TS* __restrict__ stress,

@@ -231,6 +231,8 @@ class MpmSimulation:
         self.local_tolerance = 1e-8
         self.global_tolerance = 1e-6
         self.global_max_iteration = 10000
+        # explicit integrator (MpmSimulationBase::symplectic, useTrialCollision)
+        self.useTrialCollision = True
         self.last_stats = None
 
     # lifecycle
@@ -292,7 +294,14 @@ class MpmSimulation:
         s.admm_local_tolerance = self.local_tolerance
         s.admm_global_tolerance = self.global_tolerance
         s.admm_global_max_iterations = self.global_max_iteration
+        s.trial_collision = 1 if self.useTrialCollision else 0
         return s
+
+    def useExplicit(self, trial_collision=True):
+        """Symplectic substeps (MpmSimulationBase::symplectic = true): explicit
+        grid update instead of the implicit solve."""
+        self.integrator = abi.EXPLICIT
+        self.useTrialCollision = bool(trial_collision)
 
     def useAdmm(self, admm_max_iterations=None, rho_scale=None, local_tolerance=None, global_tolerance=None,
                 global_max_iteration=None):
