@@ -142,6 +142,9 @@ typedef struct zmpm_solver {
     double admm_global_tolerance;   /* global_tolerance: absolute MINRES tolerance, default 1e-6 */
     int32_t admm_global_max_iterations; /* global_max_iteration, default 10000 */
     int32_t trial_collision;        /* EXPLICIT: useTrialCollision (MpmSimulationBase.cpp:61, default 1) */
+    int32_t mls_mpm;                /* EXPLICIT only: MLS-MPM force and velocity gradient (MpmSimulationBase.h:66,
+                                       MpmSimulationBase.cpp:102-106, :527-541, :947-961), default 0 */
+    int32_t pad1;
 } zmpm_solver;
 
 typedef struct zmpm_collider {

@@ -2459,6 +2459,30 @@ struct Sim {
     // -------------------------------------------------------- explicit --
     // The symplectic branch of advanceOneTimeStep, MpmSimulationBase.cpp:264-281.
     const std::vector<T>* g2p_v = nullptr; // grid velocities for G2P (explicit substep)
+    bool mls = false;                      // mls_mpm: G2P velocity gradient = C
+
+    // MLS force of particlesToGridWithForceHelper<APIC, quadratic, MLS>
+    // (MpmSimulationBase.cpp:527-541): f_i -= (S_p (x_i - x_p)) w_ip D^-1
+    void rasterizeMls(const std::vector<M3<T>>& S, std::vector<T>& out)
+    {
+        const T D_inverse = 4 / (dx * dx);
+        iterateBlocks(true, [&](const int*, G& g) {
+            g.new_v[0] = g.new_v[1] = g.new_v[2] = 0;
+        });
+        coloredGroups([&](int i) {
+            const M3<T>& st = S[i];
+            const T* Xp = &X[3 * i];
+            Spline<T> sp(Xp, dx);
+            iterateKernel(sp, base_offset[i], [&](const int node[3], T w, const T*, G& g) {
+                T xm[3];
+                for (int d = 0; d < 3; ++d) xm[d] = node[d] * dx - Xp[d];
+                for (int r = 0; r < 3; ++r) g.new_v[r] -= (st.a[r][0] * xm[0] + st.a[r][1] * xm[1] + st.a[r][2] * xm[2]) * (w * D_inverse);
+            });
+        });
+        iterateBlocks(true, [&](const int*, G& g) {
+            for (int d = 0; d < 3; ++d) out[3 * g.idx + d] += g.new_v[d];
+        });
+    }
 
     int substepExplicit(double dt_in, const zmpm_solver& s, zmpm_stats& st)
     {
@@ -2495,7 +2519,10 @@ struct Sim {
         // momentum, and f_i -= sum_p V0 tau_p grad w_ip, then the normalisation
         particlesToGrid();
         std::vector<T> f(3 * N, 0);
-        rasterize(T(1), stress, f);
+        if (s.mls_mpm)
+            rasterizeMls(stress, f);
+        else
+            rasterize(T(1), stress, f);
         // FractureSimulation::particlesToGrid runs the damage update after P2G
 #pragma omp parallel for schedule(static)
         for (int64_t i = 0; i < P; ++i)
@@ -2543,8 +2570,10 @@ struct Sim {
         dv.assign(3 * N, 0);
         for (int64_t i = 0; i < 3 * N; ++i) dv[i] = vnew[i] - vn[i];
         g2p_v = &vnew;
+        mls = s.mls_mpm != 0;
         int too_fast = gridToParticles();
         g2p_v = nullptr;
+        mls = false;
         time += dt_in;
         st.newton_converged = 1;
         st.cfl_violation = too_fast;
@@ -2589,11 +2618,12 @@ struct Sim {
                     }
                 }
             });
-            gradV[i] = gr;
             for (int d = 0; d < 3; ++d) V[3 * i + d] = picV[d];
             T a = (apic_rpic_ratio + 1) * T(0.5), bcoef = (apic_rpic_ratio - 1) * T(0.5);
             for (int r = 0; r < 3; ++r)
                 for (int c = 0; c < 3; ++c) Cm[9 * i + 3 * r + c] = a * (Bp.a[r][c] * D_inverse) + bcoef * (Bp.a[c][r] * D_inverse);
+            // MLS: gradVp = C_p (MpmSimulationBase.cpp:958-961)
+            gradV[i] = mls ? load9(Cm, i) : gr;
             T inc2 = 0;
             for (int d = 0; d < 3; ++d) {
                 T inc = (T)dt * picV[d];
@@ -2661,6 +2691,10 @@ struct Sim {
             all_models = all_models && model[i].kind != ZMPM_MODEL_NONE;
         }
         bool conv = true;
+        if (s.mls_mpm && s.integrator != ZMPM_EXPLICIT) {
+            err = "mls_mpm requires the explicit integrator (MpmSimulationBase.cpp:102-106)";
+            return ZMPM_BAD_ARG;
+        }
         if (s.integrator == ZMPM_EXPLICIT) return substepExplicit(dt_in, s, st);
         if (s.integrator == ZMPM_ADMM) {
             // AdmmSimulation::advanceOneTimeStep, AdmmSimulationFoam.h:816-837

@@ -17,7 +17,7 @@ GROUND = 7 * DX - 1e-3  # just below a grid plane, so trial collision acts
 
 
 def scene(lib, kind="fcr", precision="fp64", plastic=None, visco=False, damage=False, trial=True, v0=(0.3, -2.0, 0.2),
-          gravity=(0, -9.8, 0), ground=True, sphere=True, seed=5):
+          gravity=(0, -9.8, 0), ground=True, sphere=True, seed=5, mls=False):
     kw = {"grid_log2": 8} if lib is None else {}
     s = mpm.MpmSimulation(DX, gravity=gravity, precision=precision, lib=lib, **kw)
     h, x = build_scene(s, kind=kind, n=6, dx=DX, v0=v0, plastic=plastic, ground=GROUND if ground else None,
@@ -38,7 +38,7 @@ def scene(lib, kind="fcr", precision="fp64", plastic=None, visco=False, damage=F
         c = mpm.AnalyticCollisionObject(mpm.Sphere((0, 0, 0), 0.06), abi.SLIP, friction=0.2)
         c.setTranslation((0.375 - 0.07, 0.2, 0.42), (1.5, 0.0, 0.0))
         s.addCollisionObject(c)
-    s.useExplicit(trial_collision=trial)
+    s.useExplicit(trial_collision=trial, mls_mpm=mls)
     return s
 
 
@@ -85,6 +85,32 @@ def test_explicit_matches_oracle_fp64(cuda_lib, oracle, kind, plastic, visco, da
         cg, co = sims[0].getDamage(), sims[1].getDamage()
         assert (co < 1).sum() > 0
         np.testing.assert_allclose(cg, co, rtol=1e-9, atol=0)
+
+
+@pytest.mark.parametrize("kind,plastic,visco", [("fcr", None, False), ("hencky", 150.0, False), ("hencky", None, True)])
+def test_mls_matches_oracle_fp64(cuda_lib, oracle, kind, plastic, visco):
+    """MLS-MPM force weight (S_p (x_i - x_p)) w_ip D^-1 and G2P gradV = C."""
+    sims = [scene(None, kind, plastic=plastic, visco=visco, mls=True), scene(oracle, kind, plastic=plastic, visco=visco, mls=True)]
+    run(sims, 12)
+    pg, po = sims[0].getParticles(), sims[1].getParticles()
+    assert rel(pg["X"], po["X"]) < 1e-12
+    assert rel(pg["V"], po["V"]) < 1e-9
+    assert rel(pg["F"], po["F"]) < 1e-10
+    assert rel(pg["C"], po["C"]) < 1e-8
+    if visco:
+        assert rel(sims[0].getViscoelasticStrain(), sims[1].getViscoelasticStrain()) < 1e-10
+
+
+def test_mls_mixed_and_refused_by_newton(cuda_lib, oracle):
+    sims = [scene(None, "fcr", precision="mixed", mls=True), scene(oracle, "fcr", mls=True)]
+    run(sims, 12)
+    pg, po = sims[0].getParticles(), sims[1].getParticles()
+    assert rel(pg["X"], po["X"]) < 1e-7
+    assert rel(pg["V"], po["V"]) < 1e-4
+    import ctypes as C
+    g = sims[0]
+    g.integrator = abi.NEWTON
+    assert g.lib.substep(g.ctx, 4e-4, C.byref(g.solver()), None) == abi.BAD_ARG
 
 
 def test_explicit_mixed_tracks_fp64_oracle(cuda_lib, oracle):

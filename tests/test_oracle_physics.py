@@ -332,3 +332,35 @@ def test_explicit_trial_collision_keeps_particles_above_ground(oracle):
         runs.append(s.getParticles())
     assert runs[0]["X"][:, 1].min() > ground - dx
     assert np.abs(runs[0]["V"] - runs[1]["V"]).max() > 1e-6
+
+
+def test_mls_explicit_free_fall_momentum_and_refusal(oracle):
+    """MLS-MPM (mls_mpm, MpmSimulationBase.cpp:527-541, :958-961): free fall is
+    exact, total linear momentum is conserved without gravity (sum_i w_ip
+    (x_i - x_p) = 0 for the quadratic B-spline), the result differs from the
+    APIC gradient, and the implicit integrators refuse it as the reference does
+    (MpmSimulationBase.cpp:102-106)."""
+    s = _explicit_cube(oracle)
+    s.useExplicit(mls_mpm=True)
+    v0 = s.getParticles()["V"].copy()
+    for _ in range(10):
+        assert s.advanceOneTimeStep(1e-3) == abi.OK
+    np.testing.assert_allclose(s.getParticles()["V"], v0 + 1e-2 * np.array([0, -9.8, 0]), rtol=0, atol=1e-12)
+
+    runs = []
+    for mls in (True, False):
+        s = _explicit_cube(oracle, gravity=(0, 0, 0), v0=(0, 0, 0))
+        s.useExplicit(mls_mpm=mls)
+        V = np.random.default_rng(4).normal(0, 0.2, s.getParticles()["V"].shape)
+        s.setParticles(V=V)
+        for _ in range(10):
+            assert s.advanceOneTimeStep(2e-4) == abi.OK
+        p = s.getParticles()
+        assert np.abs(p["V"].sum(0) - V.sum(0)).max() < 1e-12 * np.abs(V).sum()
+        runs.append(p)
+    assert np.abs(runs[0]["F"] - runs[1]["F"]).max() > 1e-6
+
+    s = _explicit_cube(oracle)
+    s.useExplicit(mls_mpm=True)
+    s.integrator = abi.NEWTON
+    assert s.lib.substep(s.ctx, 1e-3, C.byref(s.solver()), None) == abi.BAD_ARG

@@ -67,6 +67,8 @@ class Solver(C.Structure):
         ("admm_global_tolerance", C.c_double),
         ("admm_global_max_iterations", C.c_int32),
         ("trial_collision", C.c_int32),
+        ("mls_mpm", C.c_int32),
+        ("pad1", C.c_int32),
     ]
 
 

@@ -722,6 +722,11 @@ int zmpm_substep(zmpm_ctx* ctx, double dt, const zmpm_solver* s, zmpm_stats* st)
     if (!ctx || !s || !(dt > 0) || s->newton_max_iterations < 0 || s->krylov_max_iterations < 0) return ZMPM_BAD_ARG;
     const bool admm = s->integrator == ZMPM_ADMM, expl = s->integrator == ZMPM_EXPLICIT;
     if (!admm && !expl && s->integrator != ZMPM_NEWTON) return ZMPM_BAD_ARG;
+    if (s->mls_mpm && !expl) {
+        ctx->err = "mls_mpm requires the explicit integrator (MpmSimulationBase.cpp:102-106)";
+        return ZMPM_BAD_ARG;
+    }
+    ctx->mls = expl && s->mls_mpm;
     if (admm && (s->admm_iterations < 0 || s->admm_global_max_iterations < 0 || !(s->admm_rho_scale > 0))) return ZMPM_BAD_ARG;
     cudaSetDevice(ctx->device);
     if (admm) {
@@ -831,6 +836,7 @@ int zmpm_adjoint_substep(zmpm_ctx* ctx, double dt, const zmpm_solver* s, double 
         ctx->err = "the adjoint differentiates the Newton substep";
         return ZMPM_UNSUPPORTED;
     }
+    ctx->mls = false;
     for (int64_t i = 0; i < ctx->P; ++i)
         if (ctx->hpkind[i] != ZMPM_PLASTIC_NONE || ctx->hdamage[i] != ZMPM_DAMAGE_NONE || ctx->hvisco[i]) {
             ctx->err = "the adjoint supports elastic particles only";

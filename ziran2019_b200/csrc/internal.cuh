@@ -124,6 +124,7 @@ struct Ctx {
     std::vector<double> hFe, hvmu, hvlam, hvd, hvv, hy, homega, hlastdv; // viscoelastic + ADMM state
     bool has_damage = false;
     bool has_visco = false;
+    bool mls = false;                     // the running explicit substep uses MLS-MPM (G2P gradV = C)
     bool all_models = true;               // every particle has an F-based model
     int pd_active = PD_CORE;              // pd fields the binning permutation moves
     std::vector<zmpm_collider> colliders;
@@ -220,7 +221,7 @@ int launch_admm_local(Ctx* ctx, double rho, double local_tol); // F step + rhs s
 int launch_admm_op(Ctx* ctx, const double* x0, const double* x1, bool alt, double* out, bool gated); // out += sum (grad x B) grad w
 int launch_admm_dual(Ctx* ctx, double rho);            // y += rho omega (F - (I + dt grad v) Fn)
 int launch_admm_lastdv(Ctx* ctx);                      // last_dv = sum dv w / (dt sum w)
-int launch_force_scatter(Ctx* ctx, double* out);       // out -= sum_p stress_p grad w_ip (stress buffer)
+int launch_force_scatter(Ctx* ctx, double* out, bool mls = false);       // out -= sum_p stress_p grad w_ip (stress buffer)
 int launch_hvp_scatter(Ctx* ctx, double* out, bool gated); // out += sum_p dstress_p grad w_ip
 int finalize_multiply(Ctx* ctx, const double* x, double* q); // q = project(m x + q)
 int ensure_node_buffers(Ctx* ctx);

@@ -1008,7 +1008,7 @@ int run_explicit(Ctx* ctx, const zmpm_solver& s)
     if (rc) return rc;
     rc = launch_p2g(ctx);
     if (rc) return rc;
-    rc = launch_force_scatter(ctx, ctx->facc.as<double>());
+    rc = launch_force_scatter(ctx, ctx->facc.as<double>(), s.mls_mpm != 0);
     if (rc) return rc;
     rc = launch_damage(ctx);
     if (rc) return rc;

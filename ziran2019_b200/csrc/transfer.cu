@@ -301,7 +301,10 @@ int launch_explicit_stress(Ctx* ctx)
     return ZMPM_OK;
 }
 
-template <class L, class TS, class TH>
+// MLS = true: the MLS-MPM weight of particlesToGridWithForceHelper
+// (MpmSimulationBase.cpp:527-541), facc -= (S_p (x_i - x_p)) w_ip D^-1 with
+// D^-1 = 4 / dx^2, in place of S_p grad w_ip.
+template <class L, class TS, class TH, bool MLS = false>
 __global__ void __launch_bounds__(XF_THREADS) k_force(const int32_t* __restrict__ group_start, const int32_t* __restrict__ group_nbr,
     int64_t cap, const short4* __restrict__ base, double dx, const TH* __restrict__ frac, const TS* __restrict__ stress,
     double* __restrict__ facc, const SolverScalars* __restrict__ sc)
@@ -332,19 +335,33 @@ __global__ void __launch_bounds__(XF_THREADS) k_force(const int32_t* __restrict_
             for (int c = 0; c < NCP; ++c) a[n][c] = TS(0);
         for (int r = threadIdx.x / NPB; r < cnt; r += blockDim.x / NPB) {
             const int s = first + r;
-            TS w[3][3], dwr[3][3];
+            TS w[3][3], dwr[3][3], fr[3];
 #pragma unroll
-            for (int d = 0; d < 3; ++d) bspline((TS)frac[d * cap + s], w[d], dwr[d]);
+            for (int d = 0; d < 3; ++d) {
+                fr[d] = (TS)frac[d * cap + s];
+                bspline(fr[d], w[d], dwr[d]);
+            }
             TS row[NCP][3];
 #pragma unroll
             for (int c = 0; c < NCP; ++c)
 #pragma unroll
                 for (int q2 = 0; q2 < 3; ++q2) row[c][q2] = stress[(3 * (c0 + c) + q2) * cap + s];
-            for_stencil<L>(lx, ly, lz, w, dwr, inv_dx, [&](int, int, int i, int j, int k, TS, const TS* dw) {
-                const int n = 9 * i + 3 * j + k;
+            if constexpr (MLS) {
+                const TS tdx = (TS)dx, dinv = TS(4.0 / (dx * dx));
+                for_stencil<L>(lx, ly, lz, w, dwr, inv_dx, [&](int, int, int i, int j, int k, TS wijk, const TS*) {
+                    const int n = 9 * i + 3 * j + k;
+                    const TS xm[3] = { ((TS)i - fr[0]) * tdx, ((TS)j - fr[1]) * tdx, ((TS)k - fr[2]) * tdx };
+                    const TS q = wijk * dinv;
 #pragma unroll
-                for (int c = 0; c < NCP; ++c) a[n][c] -= row[c][0] * dw[0] + row[c][1] * dw[1] + row[c][2] * dw[2];
-            });
+                    for (int c = 0; c < NCP; ++c) a[n][c] -= (row[c][0] * xm[0] + row[c][1] * xm[1] + row[c][2] * xm[2]) * q;
+                });
+            }
+            else
+                for_stencil<L>(lx, ly, lz, w, dwr, inv_dx, [&](int, int, int i, int j, int k, TS, const TS* dw) {
+                    const int n = 9 * i + 3 * j + k;
+#pragma unroll
+                    for (int c = 0; c < NCP; ++c) a[n][c] -= row[c][0] * dw[0] + row[c][1] * dw[1] + row[c][2] * dw[2];
+                });
         }
         if (threadIdx.x / NPB < cnt) {
 #pragma unroll
@@ -547,7 +564,7 @@ __global__ void __launch_bounds__(XF_THREADS) k_hvp_scatter(const int32_t* __res
 template <class L>
 __global__ void __launch_bounds__(XF_THREADS) k_g2p(const int32_t* __restrict__ group_start, const int32_t* __restrict__ group_nbr,
     double* __restrict__ pd, int32_t* __restrict__ pi, int64_t cap, const short4* __restrict__ base, double dx, double dt,
-    double apic_rpic_ratio, const double* __restrict__ vnew, int32_t* __restrict__ flags)
+    double apic_rpic_ratio, const double* __restrict__ vnew, int32_t* __restrict__ flags, int mls)
 {
     constexpr int NPB = L::NPB;
     __shared__ __align__(128) double win[8 * 3 * NPB];
@@ -599,7 +616,11 @@ __global__ void __launch_bounds__(XF_THREADS) k_g2p(const int32_t* __restrict__ 
 #pragma unroll
         for (int r = 0; r < 3; ++r)
 #pragma unroll
-            for (int c = 0; c < 3; ++c) pd[(PD_C + 3 * r + c) * cap + s] = ca * (Bp(r, c) * D_inverse) + cb * (Bp(c, r) * D_inverse);
+            for (int c = 0; c < 3; ++c) {
+                const double cn = ca * (Bp(r, c) * D_inverse) + cb * (Bp(c, r) * D_inverse);
+                pd[(PD_C + 3 * r + c) * cap + s] = cn;
+                if (mls) gv(r, c) = cn; // MLS: gradVp = C_p (MpmSimulationBase.cpp:958-961)
+            }
         const int kind = pi[PI_KIND * cap + s];
         if (kind == ZMPM_MODEL_NONE) continue;
         // evolveStrain (FBasedMpmForceHelper.cpp:95-109) on the restored F = Fn
@@ -730,19 +751,25 @@ int launch_hvp(Ctx* ctx, const double* x, double* out, bool fp32)
 }
 
 template <class L, class TH>
-static int force_scatter_impl(Ctx* ctx, double* out)
+static int force_scatter_impl(Ctx* ctx, double* out, bool mls)
 {
-    k_force<L, TH, TH><<<(unsigned)ctx->G, XF_THREADS, 0, ctx->stream>>>(ctx->group_start.as<int32_t>(), ctx->group_nbr.as<int32_t>(), ctx->Pcap,
-        ctx->base.as<short4>(), ctx->cfg.dx, ctx->frac.as<TH>(), ctx->stress.as<TH>(), out, nullptr);
+    if (mls)
+        k_force<L, TH, TH, true><<<(unsigned)ctx->G, XF_THREADS, 0, ctx->stream>>>(ctx->group_start.as<int32_t>(), ctx->group_nbr.as<int32_t>(),
+            ctx->Pcap, ctx->base.as<short4>(), ctx->cfg.dx, ctx->frac.as<TH>(), ctx->stress.as<TH>(), out, nullptr);
+    else
+        k_force<L, TH, TH><<<(unsigned)ctx->G, XF_THREADS, 0, ctx->stream>>>(ctx->group_start.as<int32_t>(), ctx->group_nbr.as<int32_t>(), ctx->Pcap,
+            ctx->base.as<short4>(), ctx->cfg.dx, ctx->frac.as<TH>(), ctx->stress.as<TH>(), out, nullptr);
     ++g_kernel_launches;
     return ZMPM_OK;
 }
-// out -= sum_p stress_p grad w_ip with `stress` in the HVP precision.
-int launch_force_scatter(Ctx* ctx, double* out)
+// out -= sum_p stress_p grad w_ip with `stress` in the HVP precision (the MLS
+// weight when mls).
+int launch_force_scatter(Ctx* ctx, double* out, bool mls)
 {
     if (!ctx->G) return ZMPM_OK;
-    if (ctx->mixed) return ctx->layout == 1 ? force_scatter_impl<Layout244, float>(ctx, out) : force_scatter_impl<Layout444, float>(ctx, out);
-    return ctx->layout == 1 ? force_scatter_impl<Layout244, double>(ctx, out) : force_scatter_impl<Layout444, double>(ctx, out);
+    if (ctx->mixed)
+        return ctx->layout == 1 ? force_scatter_impl<Layout244, float>(ctx, out, mls) : force_scatter_impl<Layout444, float>(ctx, out, mls);
+    return ctx->layout == 1 ? force_scatter_impl<Layout244, double>(ctx, out, mls) : force_scatter_impl<Layout444, double>(ctx, out, mls);
 }
 
 template <class L, class TH>
@@ -769,7 +796,8 @@ static int g2p_impl(Ctx* ctx)
     if (G == 0) return ZMPM_OK;
     DevCounters* dc = ctx->counters.as<DevCounters>();
     k_g2p<L><<<(unsigned)G, XF_THREADS, 0, ctx->stream>>>(ctx->group_start.as<int32_t>(), ctx->group_nbr.as<int32_t>(), ctx->pd.as<double>(),
-        ctx->pi.as<int32_t>(), ctx->Pcap, ctx->base.as<short4>(), ctx->cfg.dx, ctx->dt, ctx->cfg.apic_rpic_ratio, ctx->vstar.as<double>(), &dc->flags);
+        ctx->pi.as<int32_t>(), ctx->Pcap, ctx->base.as<short4>(), ctx->cfg.dx, ctx->dt, ctx->cfg.apic_rpic_ratio, ctx->vstar.as<double>(), &dc->flags,
+        ctx->mls ? 1 : 0);
     ++g_kernel_launches;
     return ZMPM_OK;
 }

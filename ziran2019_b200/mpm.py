@@ -231,8 +231,9 @@ class MpmSimulation:
         self.local_tolerance = 1e-8
         self.global_tolerance = 1e-6
         self.global_max_iteration = 10000
-        # explicit integrator (MpmSimulationBase::symplectic, useTrialCollision)
+        # explicit integrator (MpmSimulationBase::symplectic, useTrialCollision, mls_mpm)
         self.useTrialCollision = True
+        self.mls_mpm = False
         self.last_stats = None
 
     # lifecycle
@@ -295,13 +296,16 @@ class MpmSimulation:
         s.admm_global_tolerance = self.global_tolerance
         s.admm_global_max_iterations = self.global_max_iteration
         s.trial_collision = 1 if self.useTrialCollision else 0
+        s.mls_mpm = 1 if self.mls_mpm else 0
         return s
 
-    def useExplicit(self, trial_collision=True):
+    def useExplicit(self, trial_collision=True, mls_mpm=False):
         """Symplectic substeps (MpmSimulationBase::symplectic = true): explicit
-        grid update instead of the implicit solve."""
+        grid update instead of the implicit solve; mls_mpm selects the MLS-MPM
+        force and velocity gradient (explicit only, as in the reference)."""
         self.integrator = abi.EXPLICIT
         self.useTrialCollision = bool(trial_collision)
+        self.mls_mpm = bool(mls_mpm)
 
     def useAdmm(self, admm_max_iterations=None, rho_scale=None, local_tolerance=None, global_tolerance=None,
                 global_max_iteration=None):
