@@ -89,7 +89,17 @@ enum zmpm_damage {
        sigma_max > sigma_F, g = c^2 (1 - k) + k.  sigma_max is the largest
        principal stress (the reference takes the first eigenvalue in the order
        of Eigen's general eigen-solver). */
-    ZMPM_DAMAGE_RANKINE = 1
+    ZMPM_DAMAGE_RANKINE = 1,
+    /* CD-MPM phase field, FractureSimulation::solvePhaseFieldSystem
+       (FractureSimulation.h:257-456): after P2G, c is solved on the grid from
+       the lumped-mass elliptic (or parabolic, parabolic_M > 0) phase-field
+       system by Jacobi-preconditioned CG (Projects/fracture/ConjugateGradient.h:
+       53-104), transferred back (phaseG2P, :458-507) with c <- max(min(c, c_new), 0);
+       then PhaseField::Update_Phase_Field_Fp (PhaseField.h:70-76) from the
+       positive NeoHookeanBorden energy and g = c^2 (1 - k) + k.  Every particle
+       of the scene carries the phase field (the reference indexes it for all
+       particles), added by zmpm_add_phase_field. */
+    ZMPM_DAMAGE_PHASE_FIELD = 2
 };
 
 /* Krylov solver of the Newton step (BackwardEuler.h:82-98). */
@@ -186,6 +196,9 @@ typedef struct zmpm_stats {
                                     (only with zmpm_set_profiling on) */
     int32_t hvp_timed;           /* number of products in ms_hvp */
     int32_t kernel_launches;     /* CUDA kernels this library launched for the substep */
+    int32_t phase_field_iterations; /* CG iterations of the phase-field solve (its `iterations` return) */
+    int32_t pad2;
+    double phase_field_residual; /* final |r|_2 of the phase-field CG */
 } zmpm_stats;
 
 /* Result of the binning pass (sortParticlesAndPolluteGrid,
@@ -236,6 +249,28 @@ int zmpm_add_plasticity(zmpm_ctx* ctx, int64_t lower, int64_t upper, int32_t kin
 int zmpm_add_damage(zmpm_ctx* ctx, int64_t lower, int64_t upper, int32_t kind, double sigma_f, double residual_phase);
 /* Phase-field value c per particle (1 undamaged, 0 fully damaged). */
 int zmpm_get_damage(zmpm_ctx* ctx, double* c);
+
+/* CD-MPM phase field on NeoHookeanBorden particles [lower, upper):
+   MpmParticleHandleBase::addFBasedMpmForceWithPhaseField(percentage, l0, model,
+   allow_damage) (MpmParticleHandleBase.cpp:92-118): c = 1, H = 0, l0,
+   1/sigma_c = 1 / psi((1 + percentage) I) (PhaseField::Get_Sigma_C_Based_On_Max_Deformation,
+   PhaseField.h:58-68), pf_Fp = 1, H_max = +max, vol = V0, allow_damage; residual
+   phase k (the reference fixes 0.001).  Sets the particles' damage kind to
+   ZMPM_DAMAGE_PHASE_FIELD. */
+int zmpm_add_phase_field(zmpm_ctx* ctx, int64_t lower, int64_t upper, double percentage, double l0, int32_t allow_damage,
+    double residual_phase);
+/* FractureSimulation members of the phase-field solve: parabolic_M (0: elliptic),
+   lumping (default 1), delete_particle_threshold (default 0; particles with
+   c < threshold are parked at (4, 4, 4) with V = 0, F = I, no further damage,
+   FractureSimulation.h:172-207), and the CG's max_iterations (100) and absolute
+   tolerance (1e-6), FractureSimulation.h:61-63, :444-446. */
+int zmpm_set_phase_field_solver(zmpm_ctx* ctx, double parabolic_M, int32_t lumping, double delete_threshold, int32_t cg_max_iterations,
+    double cg_tolerance);
+/* Per-particle phase-field state (particle order); any pointer may be NULL. */
+int zmpm_get_phase_field(zmpm_ctx* ctx, double* c, double* H, double* pf_Fp, double* vol);
+/* Replaces 1/sigma_c per particle (the host side of randomizePhaseFieldSigmaC /
+   voronoiSigmaC, MpmParticleHandleBase.cpp:120-200). */
+int zmpm_set_phase_field_sigma_c(zmpm_ctx* ctx, const double* one_over_sigma_c);
 
 /* MpmParticleHandleBase::addFElasticNonequilibratedBasedMpmForce
    (MpmParticleHandleBase.cpp:468-478) with the reference's only instantiated

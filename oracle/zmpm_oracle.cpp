@@ -794,7 +794,39 @@ template <class T>
 struct Damage {
     int32_t kind = ZMPM_DAMAGE_NONE;
     T c = 1, k = T(0.001), sigma_f = 0;
+    // PhaseField members (PhaseField.h:13-22) of ZMPM_DAMAGE_PHASE_FIELD
+    T H = 0, l0 = 0, one_over_sigma_c = 0, pf_Fp = 1, H_max = std::numeric_limits<T>::max(), vol = 0;
+    bool allow_damage = true;
 };
+
+// NeoHookeanBorden::get_psi_pos (NeoHookeanBorden.cpp:53-66): the part of the
+// energy that the phase field degrades.
+template <class T>
+static T neoHookeanBordenPsiPos(const Model<T>& c, const M3<T>& F)
+{
+    const T J = det(F);
+    const T a = std::pow(J, -T(1) / T(3));
+    T tr = 0;
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) tr += (a * F.a[i][j]) * (a * F.a[i][j]);
+    const T psi_dev = c.mu / 2 * (tr - 3);
+    const T psi_vol = c.kappa / 2 * ((J * J - 1) / 2 - std::log(J));
+    return (J >= 1) ? (psi_vol + psi_dev) : psi_dev;
+}
+
+// PhaseField::Get_Sigma_C_Based_On_Max_Deformation (PhaseField.h:58-68):
+// 1 / psi((1 + percentage) I) of the model (NeoHookeanBorden::psi, .cpp:38-51).
+template <class T>
+static T phaseFieldOneOverSigmaC(const Model<T>& c, T percentage)
+{
+    M3<T> F = M3<T>::identity();
+    for (int i = 0; i < 3; ++i) F.a[i][i] = 1 + percentage;
+    const T J = det(F);
+    const T psi_pos = neoHookeanBordenPsiPos(c, F);
+    const T psi_vol = c.kappa / 2 * ((J * J - 1) / 2 - std::log(J));
+    const T psi_neg = (J >= 1) ? T(0) : psi_vol;
+    return T(1) / (c.g * psi_pos + psi_neg);
+}
 
 // Largest eigenvalue of a symmetric 3x3 matrix by cyclic Jacobi rotations
 // (Golub & Van Loan, Matrix Computations, 8.5.2).
@@ -2461,6 +2493,168 @@ struct Sim {
     const std::vector<T>* g2p_v = nullptr; // grid velocities for G2P (explicit substep)
     bool mls = false;                      // mls_mpm: G2P velocity gradient = C
 
+    // ---------------------------------------------- phase-field fracture --
+    // FractureSimulation members (FractureSimulation.h:48-63)
+    T pf_M = 0, pf_delete = 0, pf_cg_tol = T(1e-6);
+    bool pf_lumping = true;
+    int pf_cg_max = 100;
+    int pf_iters = 0;
+    T pf_res = 0;
+
+    bool anyPhaseField() const
+    {
+        for (const auto& d : damage)
+            if (d.kind == ZMPM_DAMAGE_PHASE_FIELD) return true;
+        return false;
+    }
+
+    // FractureSimulation::deleteParticles (FractureSimulation.h:172-207)
+    void deletePhaseFieldParticles()
+    {
+        for (int64_t i = 0; i < P; ++i)
+            if (damage[i].kind == ZMPM_DAMAGE_PHASE_FIELD && damage[i].c < pf_delete) {
+                for (int d = 0; d < 3; ++d) {
+                    X[3 * i + d] = 4;
+                    V[3 * i + d] = 0;
+                }
+                store9(F, i, M3<T>::identity());
+                damage[i].allow_damage = false;
+            }
+    }
+
+    // FractureSimulation::solvePhaseFieldSystem (FractureSimulation.h:257-456)
+    // with phaseP2G (:208-255) and phaseG2P (:458-507), after P2G.  Node vectors
+    // are indexed by GridState::idx; nodes outside the index set are skipped as
+    // in the reference (`if (node_id < 0) return`).
+    void solvePhaseField()
+    {
+        const T M = pf_M, one_over_dt = T(1) / dt;
+        std::vector<T> phase(N, 0), mult(N, 0);
+        if (M > 0) {
+            coloredGroups([&](int i) {
+                Spline<T> sp(&X[3 * i], dx);
+                iterateKernel(sp, base_offset[i], [&](const int*, T w, const T*, G& g) {
+                    if (g.idx < 0) return;
+                    mult[g.idx] += w;
+                    phase[g.idx] += damage[i].c * w;
+                });
+            });
+            for (int64_t n = 0; n < N; ++n) phase[n] /= mult[n];
+        }
+        for (int64_t i = 0; i < P; ++i) damage[i].vol = vol[i] * det(load9(F, i));
+        // right-hand side (:318-342) and the Jacobi diagonal of the
+        // preconditioner (:409-441)
+        std::vector<T> rhs(N, 0), diag(N, 0);
+        coloredGroups([&](int i) {
+            const Damage<T>& ph = damage[i];
+            Spline<T> sp(&X[3 * i], dx);
+            iterateKernel(sp, base_offset[i], [&](const int*, T w, const T*, G& g) {
+                if (g.idx < 0) return;
+                const int64_t n = g.idx;
+                if (M > 0) {
+                    rhs[n] += (M + phase[n] / dt) * ph.vol * w;
+                    diag[n] += ph.vol * (M * ph.pf_Fp + one_over_dt) * w;
+                }
+                else {
+                    rhs[n] += ph.vol * w;
+                    diag[n] += ph.vol * ph.pf_Fp * w;
+                }
+            });
+        });
+        // the matrix-free operator (:344-407)
+        std::vector<T> cs(P), gc(3 * P);
+        auto multiply = [&](const std::vector<T>& x, std::vector<T>& b) {
+#pragma omp parallel for schedule(static)
+            for (int64_t i = 0; i < P; ++i) {
+                T c0 = 0, g0[3] = { 0, 0, 0 };
+                Spline<T> sp(&X[3 * i], dx);
+                iterateKernel(sp, base_offset[i], [&](const int*, T w, const T* dw, G& g) {
+                    if (g.idx < 0) return;
+                    if (!pf_lumping) c0 += x[g.idx] * w;
+                    for (int d = 0; d < 3; ++d) g0[d] += x[g.idx] * dw[d];
+                });
+                const Damage<T>& ph = damage[i];
+                if (!pf_lumping) c0 *= ph.vol * ph.pf_Fp;
+                cs[i] = c0;
+                for (int d = 0; d < 3; ++d) gc[3 * i + d] = g0[d] * (ph.vol * T(4) * ph.l0 * ph.l0);
+            }
+            b.assign(N, 0);
+            coloredGroups([&](int i) {
+                const Damage<T>& ph = damage[i];
+                Spline<T> sp(&X[3 * i], dx);
+                iterateKernel(sp, base_offset[i], [&](const int*, T w, const T* dw, G& g) {
+                    if (g.idx < 0) return;
+                    const int64_t n = g.idx;
+                    if (!pf_lumping)
+                        b[n] += cs[i] * w;
+                    else if (M > 0)
+                        b[n] += ph.vol * (ph.pf_Fp * M + one_over_dt) * w * x[n];
+                    else
+                        b[n] += ph.vol * ph.pf_Fp * w * x[n];
+                    const T gd = gc[3 * i] * dw[0] + gc[3 * i + 1] * dw[1] + gc[3 * i + 2] * dw[2];
+                    b[n] += (M > 0) ? gd * M : gd;
+                });
+            });
+        };
+        // Projects/fracture/ConjugateGradient.h:53-104 from x = 0 (so r = b)
+        std::vector<T> x(N, 0), r = rhs, mr(N), sdir(N, 0), q(N);
+        auto dot = [&](const std::vector<T>& a, const std::vector<T>& b) {
+            T acc = 0;
+            for (int64_t n = 0; n < N; ++n) acc += a[n] * b[n];
+            return acc;
+        };
+        T norm = std::sqrt(dot(r, r));
+        const T rel_tol = norm * (sizeof(T) == 4 ? T(1e-6) : T(1e-12));
+        T rho_old = std::numeric_limits<T>::max();
+        int it;
+        for (it = 0;; ++it) {
+            for (int64_t n = 0; n < N; ++n) mr[n] = r[n] / diag[n];
+            const T rho = dot(mr, r);
+            if (it == 0)
+                sdir = mr;
+            else
+                for (int64_t n = 0; n < N; ++n) sdir[n] = rho / rho_old * sdir[n] + mr[n];
+            multiply(sdir, q);
+            const T sq = dot(sdir, q);
+            const T alpha = sq ? rho / sq : std::numeric_limits<T>::max();
+            for (int64_t n = 0; n < N; ++n) {
+                x[n] = alpha * sdir[n] + x[n];
+                r[n] = -alpha * q[n] + r[n];
+            }
+            rho_old = rho;
+            norm = std::sqrt(dot(r, r));
+            if (norm < pf_cg_tol || norm < rel_tol || it == pf_cg_max) break;
+        }
+        pf_iters = it;
+        pf_res = norm;
+        for (int64_t n = 0; n < N; ++n) phase[n] = (M > 0) ? x[n] - phase[n] : x[n];
+        // phaseG2P
+#pragma omp parallel for schedule(static)
+        for (int64_t i = 0; i < P; ++i) {
+            Damage<T>& ph = damage[i];
+            if (!ph.allow_damage) continue;
+            T pf = 0;
+            Spline<T> sp(&X[3 * i], dx);
+            iterateKernel(sp, base_offset[i], [&](const int*, T w, const T*, G& g) {
+                if (g.idx >= 0) pf += w * phase[g.idx];
+            });
+            const T new_c = (M > 0) ? ph.c + pf : pf;
+            ph.c = std::max(std::min(ph.c, new_c), T(0));
+        }
+#pragma omp parallel for schedule(static)
+        for (int64_t i = 0; i < P; ++i) {
+            Damage<T>& ph = damage[i];
+            if (model[i].kind != ZMPM_MODEL_NEOHOOKEAN_BORDEN) continue;
+            // PhaseField::Update_Phase_Field_Fp (PhaseField.h:70-76)
+            const T psi_pos = neoHookeanBordenPsiPos(model[i], load9(F, i));
+            if (psi_pos > ph.H) {
+                ph.H = std::min(psi_pos, ph.H_max);
+                ph.pf_Fp = 4 * ph.l0 * (1 - ph.k) * ph.H * ph.one_over_sigma_c + 1;
+            }
+            model[i].g = ph.c * ph.c * (1 - ph.k) + ph.k;
+        }
+    }
+
     // MLS force of particlesToGridWithForceHelper<APIC, quadratic, MLS>
     // (MpmSimulationBase.cpp:527-541): f_i -= (S_p (x_i - x_p)) w_ip D^-1
     void rasterizeMls(const std::vector<M3<T>>& S, std::vector<T>& out)
@@ -2528,6 +2722,7 @@ struct Sim {
         for (int64_t i = 0; i < P; ++i)
             if (damage[i].kind == ZMPM_DAMAGE_RANKINE && model[i].kind == ZMPM_MODEL_NEOHOOKEAN_BORDEN)
                 rankineUpdate(model[i], damage[i], load9(F, i));
+        if (anyPhaseField()) solvePhaseField();
         // gridVelocityExplicitUpdate (:818-865)
         for (auto& c : colliders) c.update(time);
         mvec.assign(N, 0);
@@ -2577,6 +2772,8 @@ struct Sim {
         time += dt_in;
         st.newton_converged = 1;
         st.cfl_violation = too_fast;
+        st.phase_field_iterations = pf_iters;
+        st.phase_field_residual = (double)pf_res;
         st.num_particles = P;
         st.num_groups = (int64_t)group.size();
         st.num_blocks = (int64_t)blocks.size();
@@ -2676,6 +2873,7 @@ struct Sim {
         for (int64_t i = 0; i < P; ++i)
             if (damage[i].kind == ZMPM_DAMAGE_RANKINE && model[i].kind == ZMPM_MODEL_NEOHOOKEAN_BORDEN)
                 rankineUpdate(model[i], damage[i], load9(F, i));
+        if (anyPhaseField()) solvePhaseField();
         startBackwardEuler();
         return ZMPM_OK;
     }
@@ -2694,6 +2892,15 @@ struct Sim {
         if (s.mls_mpm && s.integrator != ZMPM_EXPLICIT) {
             err = "mls_mpm requires the explicit integrator (MpmSimulationBase.cpp:102-106)";
             return ZMPM_BAD_ARG;
+        }
+        pf_iters = 0;
+        pf_res = 0;
+        if (anyPhaseField()) {
+            if (s.integrator == ZMPM_ADMM) {
+                err = "the phase-field solve belongs to FractureSimulation; AdmmSimulation does not run it";
+                return ZMPM_BAD_ARG;
+            }
+            deletePhaseFieldParticles(); // FractureSimulation::reinitialize
         }
         if (s.integrator == ZMPM_EXPLICIT) return substepExplicit(dt_in, s, st);
         if (s.integrator == ZMPM_ADMM) {
@@ -2725,6 +2932,8 @@ struct Sim {
         st.newton_converged = conv ? 1 : 0;
         st.cfl_violation = too_fast;
         st.hvp_count = (int32_t)hvp_count;
+        st.phase_field_iterations = pf_iters;
+        st.phase_field_residual = (double)pf_res;
         st.num_particles = P;
         st.num_groups = (int64_t)group.size();
         st.num_blocks = (int64_t)blocks.size();
@@ -2916,6 +3125,72 @@ int zoracle_get_damage(Ctx* c, double* out)
     if (!c || !out) return ZMPM_BAD_ARG;
     DISPATCH(c, {
         for (int64_t i = 0; i < S.P; ++i) out[i] = S.damage[i].c;
+    });
+    return ZMPM_OK;
+}
+
+int zoracle_add_phase_field(Ctx* c, int64_t lo, int64_t hi, double percentage, double l0, int32_t allow_damage, double residual_phase)
+{
+    if (!c) return ZMPM_BAD_ARG;
+    DISPATCH(c, {
+        using T = typename std::remove_reference<decltype(S.dx)>::type;
+        if (lo < 0 || hi > S.P || lo > hi) return ZMPM_BAD_ARG;
+        for (int64_t i = lo; i < hi; ++i)
+            if (S.model[i].kind != ZMPM_MODEL_NEOHOOKEAN_BORDEN) {
+                S.err = "the phase field needs NeoHookeanBorden particles";
+                return ZMPM_BAD_ARG;
+            }
+        for (int64_t i = lo; i < hi; ++i) {
+            zo::Damage<T>& d = S.damage[i];
+            d = zo::Damage<T>();
+            d.kind = ZMPM_DAMAGE_PHASE_FIELD;
+            d.k = (T)residual_phase;
+            d.c = 1;
+            d.H = 0;
+            d.l0 = (T)l0;
+            d.one_over_sigma_c = phaseFieldOneOverSigmaC(S.model[i], (T)percentage);
+            d.pf_Fp = 1;
+            d.vol = S.vol[i];
+            d.allow_damage = allow_damage != 0;
+        }
+    });
+    return ZMPM_OK;
+}
+
+int zoracle_set_phase_field_solver(Ctx* c, double M, int32_t lumping, double del, int32_t cg_max, double cg_tol)
+{
+    if (!c || !(M >= 0) || cg_max < 0 || !(cg_tol >= 0)) return ZMPM_BAD_ARG;
+    DISPATCH(c, {
+        using T = typename std::remove_reference<decltype(S.dx)>::type;
+        S.pf_M = (T)M;
+        S.pf_lumping = lumping != 0;
+        S.pf_delete = (T)del;
+        S.pf_cg_max = cg_max;
+        S.pf_cg_tol = (T)cg_tol;
+    });
+    return ZMPM_OK;
+}
+
+int zoracle_get_phase_field(Ctx* c, double* cc, double* H, double* fp, double* vol)
+{
+    if (!c) return ZMPM_BAD_ARG;
+    DISPATCH(c, {
+        for (int64_t i = 0; i < S.P; ++i) {
+            if (cc) cc[i] = S.damage[i].c;
+            if (H) H[i] = S.damage[i].H;
+            if (fp) fp[i] = S.damage[i].pf_Fp;
+            if (vol) vol[i] = S.damage[i].vol;
+        }
+    });
+    return ZMPM_OK;
+}
+
+int zoracle_set_phase_field_sigma_c(Ctx* c, const double* isc)
+{
+    if (!c || !isc) return ZMPM_BAD_ARG;
+    DISPATCH(c, {
+        using T = typename std::remove_reference<decltype(S.dx)>::type;
+        for (int64_t i = 0; i < S.P; ++i) S.damage[i].one_over_sigma_c = (T)isc[i];
     });
     return ZMPM_OK;
 }

@@ -364,3 +364,92 @@ def test_mls_explicit_free_fall_momentum_and_refusal(oracle):
     s.useExplicit(mls_mpm=True)
     s.integrator = abi.NEWTON
     assert s.lib.substep(s.ctx, 1e-3, C.byref(s.solver()), None) == abi.BAD_ARG
+
+
+def _nhb_psi_pos(mu, kappa, F):
+    J = np.linalg.det(F)
+    JaF = J ** (-1.0 / 3.0) * F
+    psi_dev = mu / 2 * (np.trace(JaF.T @ JaF) - 3)
+    psi_vol = kappa / 2 * ((J * J - 1) / 2 - np.log(J))
+    return psi_vol + psi_dev if J >= 1 else psi_dev
+
+
+def _pf_cube(lib, stretch=0.3, dx=1.0 / 64, seed=2, **kw):
+    s = mpm.MpmSimulation(dx, gravity=(0, -9.8, 0), precision="fp64", lib=lib, **kw)
+    h, x = build_scene(s, kind="nh", n=6, dx=dx, seed=seed)
+    n = len(x)
+    F = np.zeros((n, 3, 3))
+    F[:, 0, 0] = 1 + stretch * (x[:, 0] - x[:, 0].min()) / np.ptp(x[:, 0])
+    F[:, 1, 1] = F[:, 2, 2] = 1
+    s.setParticles(F=F)
+    return s, h, x, F
+
+
+def test_phase_field_known_answers(oracle):
+    """CD-MPM phase field (FractureSimulation::solvePhaseFieldSystem): with
+    pf_Fp = 1 the elliptic system's solution is c = 1 exactly (the Laplacian of
+    a constant vanishes by the partition of unity), so an unstrained body stays
+    undamaged after a first CG step that lands on it; vol = V0 det F; H and
+    pf_Fp follow Update_Phase_Field_Fp (PhaseField.h:70-76) from the positive
+    NeoHookeanBorden energy (NeoHookeanBorden.cpp:53-66); 1/sigma_c follows
+    Get_Sigma_C_Based_On_Max_Deformation (PhaseField.h:58-68)."""
+    E, nu, l0, pct, k = 1e4, 0.3, 0.5 / 64, 0.05, 0.001
+    mu, lam = E / (2 * (1 + nu)), E * nu / ((1 + nu) * (1 - 2 * nu))
+    kappa = 0.666666 * mu + lam  # NeoHookeanBorden::setLameParameters (NeoHookeanBorden.cpp:20)
+    s, h, x, F = _pf_cube(oracle, stretch=0.0)
+    h.addFBasedMpmForceWithPhaseField(pct, l0)
+    s.setPhaseFieldSolver(cg_tolerance=1e-30)
+    assert s.advanceOneTimeStep(1e-3) == abi.OK
+    assert s.last_stats["phase_field_iterations"] <= 1
+    pf = s.getPhaseField()
+    np.testing.assert_allclose(pf["c"], 1.0, rtol=0, atol=1e-12)
+
+    s, h, x, F = _pf_cube(oracle, stretch=0.3)
+    h.addFBasedMpmForceWithPhaseField(pct, l0)
+    V0 = (1.0 / 64) ** 3 / 8
+    assert s.advanceOneTimeStep(1e-3) == abi.OK
+    pf = s.getPhaseField()
+    np.testing.assert_allclose(pf["vol"], V0 * np.linalg.det(F), rtol=1e-14)
+    # H and pf_Fp come from F after the substep's G2P (phaseG2P runs after P2G on
+    # the start-of-substep F; getParticles returns the end-of-substep F)
+    f = 1 + pct
+    J = f ** 3
+    isc = 1.0 / (kappa / 2 * ((J * J - 1) / 2 - np.log(J)) + mu / 2 * (3 * (J ** (-1 / 3) * f) ** 2 - 3))
+    H = np.array([_nhb_psi_pos(mu, kappa, Fi) for Fi in F])
+    np.testing.assert_allclose(pf["H"], H, rtol=1e-12, atol=1e-12)
+    np.testing.assert_allclose(pf["pf_Fp"], 4 * l0 * (1 - k) * H * isc + 1, rtol=1e-12)
+    # the first solve still saw pf_Fp = 1 (it is updated after the solve), so
+    # damage shows from the second substep on
+    np.testing.assert_allclose(pf["c"], 1.0, rtol=0, atol=1e-12)
+    assert s.advanceOneTimeStep(1e-3) == abi.OK
+    c = s.getDamage()
+    assert c.min() < 0.95 and np.all(c <= 1)
+
+
+@pytest.mark.parametrize("M,lumping", [(0.0, True), (0.0, False), (1.0, True)])
+def test_phase_field_cg_converges_and_degrades(oracle, M, lumping):
+    """The CG of the phase-field system reaches a tight tolerance, damage grows
+    where the body is stretched, and particles that may not be damaged keep c."""
+    s, h, x, F = _pf_cube(oracle, stretch=0.3)
+    lo = np.argsort(x[:, 0])[:50]
+    h.addFBasedMpmForceWithPhaseField(0.05, 0.5 / 64)
+    s.setPhaseFieldSolver(parabolic_M=M, lumping=lumping, cg_tolerance=1e-16)
+    for _ in range(3):
+        assert s.advanceOneTimeStep(1e-3) == abi.OK
+        st = s.last_stats
+        assert st["phase_field_residual"] < 1e-12 * 1e3 or st["phase_field_iterations"] > 3
+    c = s.getDamage()
+    assert np.all((c >= 0) & (c <= 1))
+    right = x[:, 0] > np.median(x[:, 0])
+    assert c[right].mean() < c[~right].mean()
+
+
+def test_phase_field_refusals(oracle):
+    s, h, x, F = _pf_cube(oracle)
+    h.addFBasedMpmForceWithPhaseField(0.05, 0.5 / 64)
+    s.useAdmm(admm_max_iterations=4)
+    assert s.lib.substep(s.ctx, 1e-3, C.byref(s.solver()), None) == abi.BAD_ARG
+    s2 = mpm.MpmSimulation(1.0 / 64, gravity=(0, -9.8, 0), precision="fp64", lib=oracle)
+    h2, _ = build_scene(s2, kind="fcr", n=4, dx=1.0 / 64)
+    with pytest.raises(abi.ZmpmError):
+        h2.addFBasedMpmForceWithPhaseField(0.05, 0.5 / 64)

@@ -31,7 +31,7 @@ NOALLOC_MAX_PARTICLES = 262144
 LAYOUT_AUTO, LAYOUT_244, LAYOUT_444 = 0, 1, 2
 MODEL_NONE, MODEL_NEOHOOKEAN_BORDEN, MODEL_STVK_HENCKY_ISOTROPIC, MODEL_FIXED_COROTATED = 0, 1, 2, 3
 PLASTIC_NONE, PLASTIC_VON_MISES = 0, 1
-DAMAGE_NONE, DAMAGE_RANKINE = 0, 1
+DAMAGE_NONE, DAMAGE_RANKINE, DAMAGE_PHASE_FIELD = 0, 1, 2
 NEWTON, ADMM, EXPLICIT = 0, 1, 2
 MINRES, CG = 0, 1
 HALF_SPACE, SPHERE, BOX = 0, 1, 2
@@ -108,6 +108,9 @@ class Stats(C.Structure):
         ("ms_hvp", C.c_double),
         ("hvp_timed", C.c_int32),
         ("kernel_launches", C.c_int32),
+        ("phase_field_iterations", C.c_int32),
+        ("pad2", C.c_int32),
+        ("phase_field_residual", C.c_double),
     ]
 
     def as_dict(self):
@@ -135,6 +138,10 @@ _SIGS = {
     "add_plasticity": (C.c_int, [C.c_void_p, C.c_int64, C.c_int64, C.c_int32, C.c_double, C.c_double, C.c_double]),
     "add_damage": (C.c_int, [C.c_void_p, C.c_int64, C.c_int64, C.c_int32, C.c_double, C.c_double]),
     "get_damage": (C.c_int, [C.c_void_p, c_double_p]),
+    "add_phase_field": (C.c_int, [C.c_void_p, C.c_int64, C.c_int64, C.c_double, C.c_double, C.c_int32, C.c_double]),
+    "set_phase_field_solver": (C.c_int, [C.c_void_p, C.c_double, C.c_int32, C.c_double, C.c_int32, C.c_double]),
+    "get_phase_field": (C.c_int, [C.c_void_p, c_double_p, c_double_p, c_double_p, c_double_p]),
+    "set_phase_field_sigma_c": (C.c_int, [C.c_void_p, c_double_p]),
     "add_viscoelastic": (C.c_int, [C.c_void_p, C.c_int64, C.c_int64, C.c_double, C.c_double, C.c_double, C.c_double]),
     "get_viscoelastic_strain": (C.c_int, [C.c_void_p, c_double_p]),
     "set_viscoelastic_strain": (C.c_int, [C.c_void_p, c_double_p]),

@@ -5,6 +5,7 @@
 #include <cmath>
 #include <cstring>
 #include <cstdlib>
+#include <limits>
 #include <new>
 
 #include "internal.cuh"
@@ -78,6 +79,13 @@ int upload(Ctx* ctx)
         hpd[PD_PF_C * cap + i] = ctx->hpfc[i];
         hpd[PD_PF_K * cap + i] = ctx->hpfk[i];
         hpd[PD_SIGMA_F * cap + i] = ctx->hsigf[i];
+        hpd[PD_PF_H * cap + i] = ctx->hpfH[i];
+        hpd[PD_PF_L0 * cap + i] = ctx->hpfl0[i];
+        hpd[PD_PF_ISC * cap + i] = ctx->hpfisc[i];
+        hpd[PD_PF_FP * cap + i] = ctx->hpffp[i];
+        hpd[PD_PF_HMAX * cap + i] = ctx->hpfhmax[i];
+        hpd[PD_PF_VOL * cap + i] = ctx->hpfvol[i];
+        hpd[PD_PF_ALLOW * cap + i] = ctx->hpfallow[i];
         hpi[PI_DAMAGE * cap + i] = ctx->hdamage[i];
         hpi[PI_KIND * cap + i] = ctx->hkind[i];
         hpi[PI_PKIND * cap + i] = ctx->hpkind[i];
@@ -100,8 +108,12 @@ int upload(Ctx* ctx)
     ctx->has_damage = false;
     ctx->has_visco = false;
     ctx->all_models = true;
+    ctx->has_pf = false;
+    ctx->all_pf = P > 0;
     for (int64_t i = 0; i < P; ++i) {
-        ctx->has_damage |= ctx->hdamage[i] != ZMPM_DAMAGE_NONE;
+        ctx->has_pf |= ctx->hdamage[i] == ZMPM_DAMAGE_PHASE_FIELD;
+        ctx->all_pf &= ctx->hdamage[i] == ZMPM_DAMAGE_PHASE_FIELD;
+        ctx->has_damage |= ctx->hdamage[i] == ZMPM_DAMAGE_RANKINE;
         ctx->has_visco |= ctx->hvisco[i] != 0;
         ctx->all_models &= ctx->hkind[i] != ZMPM_MODEL_NONE;
     }
@@ -117,7 +129,7 @@ int download(Ctx* ctx)
     if (!ctx->uploaded) return ZMPM_OK;
     const int64_t P = ctx->P, cap = ctx->Pcap;
     // fields past pd_active were not moved by the permutation: the host copy stays
-    const bool ext = ctx->pd_active == PD_FIELDS;
+    const bool ext = ctx->pd_active == PD_FIELDS, pfx = ctx->pd_active >= PD_PF_END;
     std::vector<double> hpd((size_t)ctx->pd_active * cap);
     std::vector<int32_t> hpi((size_t)PI_FIELDS * cap);
     ZMPM_CUDA(cudaStreamSynchronize(ctx->stream));
@@ -151,6 +163,15 @@ int download(Ctx* ctx)
         ctx->hpkind[i] = (uint8_t)hpi[PI_PKIND * cap + s];
         ctx->hbroken[i] = hpi[PI_BROKEN * cap + s];
         ctx->hvisco[i] = (uint8_t)hpi[PI_VISCO * cap + s];
+        if (pfx) {
+            ctx->hpfH[i] = hpd[PD_PF_H * cap + s];
+            ctx->hpfl0[i] = hpd[PD_PF_L0 * cap + s];
+            ctx->hpfisc[i] = hpd[PD_PF_ISC * cap + s];
+            ctx->hpffp[i] = hpd[PD_PF_FP * cap + s];
+            ctx->hpfhmax[i] = hpd[PD_PF_HMAX * cap + s];
+            ctx->hpfvol[i] = hpd[PD_PF_VOL * cap + s];
+            ctx->hpfallow[i] = hpd[PD_PF_ALLOW * cap + s];
+        }
         if (!ext) continue;
         for (int q = 0; q < 9; ++q) ctx->hFe[9 * i + q] = hpd[(PD_FE + q) * cap + s];
         ctx->hvmu[i] = hpd[PD_VMU * cap + s];
@@ -505,6 +526,13 @@ int zmpm_add_particles(zmpm_ctx* ctx, int64_t n, const double* x, const double* 
         ctx->homega.push_back(1.0);
         ctx->homega.push_back(1.0);
         for (int d = 0; d < 3; ++d) ctx->hlastdv.push_back(0.0);
+        ctx->hpfH.push_back(0.0);
+        ctx->hpfl0.push_back(0.0);
+        ctx->hpfisc.push_back(0.0);
+        ctx->hpffp.push_back(1.0);
+        ctx->hpfhmax.push_back(std::numeric_limits<double>::max());
+        ctx->hpfvol.push_back(vol[i]);
+        ctx->hpfallow.push_back(1.0);
     }
     ctx->P += n;
     return ZMPM_OK;
@@ -583,6 +611,86 @@ int zmpm_get_damage(zmpm_ctx* ctx, double* c)
     int rc = download(ctx);
     if (rc) return rc;
     for (int64_t i = 0; i < ctx->P; ++i) c[i] = ctx->hpfc[i];
+    return ZMPM_OK;
+}
+
+// PhaseField::Get_Sigma_C_Based_On_Max_Deformation (PhaseField.h:58-68):
+// 1 / psi((1 + percentage) I) with NeoHookeanBorden::psi (NeoHookeanBorden.cpp:38-51).
+static double pf_one_over_sigma_c(double mu, double kappa, double g, double percentage)
+{
+    const double f = 1 + percentage, J = f * (f * f);
+    const double a = std::pow(J, -1.0 / 3.0);
+    double tr = 0;
+    for (int i = 0; i < 3; ++i) tr += (a * f) * (a * f);
+    const double psi_dev = mu / 2 * (tr - 3);
+    const double psi_vol = kappa / 2 * ((J * J - 1) / 2 - std::log(J));
+    const double psi_pos = (J >= 1) ? psi_vol + psi_dev : psi_dev;
+    const double psi_neg = (J >= 1) ? 0.0 : psi_vol;
+    return 1.0 / (g * psi_pos + psi_neg);
+}
+
+int zmpm_add_phase_field(zmpm_ctx* ctx, int64_t lo, int64_t hi, double percentage, double l0, int32_t allow_damage, double residual_phase)
+{
+    if (!ctx || lo < 0 || hi > ctx->P || lo > hi || !(l0 >= 0)) return ZMPM_BAD_ARG;
+    cudaSetDevice(ctx->device);
+    int rc = begin_edit(ctx);
+    if (rc) return rc;
+    for (int64_t i = lo; i < hi; ++i)
+        if (ctx->hkind[i] != ZMPM_MODEL_NEOHOOKEAN_BORDEN) {
+            ctx->err = "the phase field needs NeoHookeanBorden particles";
+            return ZMPM_BAD_ARG;
+        }
+    for (int64_t i = lo; i < hi; ++i) {
+        ctx->hdamage[i] = ZMPM_DAMAGE_PHASE_FIELD;
+        ctx->hpfk[i] = residual_phase;
+        ctx->hpfc[i] = 1.0;
+        ctx->hpfH[i] = 0.0;
+        ctx->hpfl0[i] = l0;
+        ctx->hpfisc[i] = pf_one_over_sigma_c(ctx->hmu[i], ctx->hkappa[i], ctx->hg[i], percentage);
+        ctx->hpffp[i] = 1.0;
+        ctx->hpfhmax[i] = std::numeric_limits<double>::max();
+        ctx->hpfvol[i] = ctx->hvol[i];
+        ctx->hpfallow[i] = allow_damage ? 1.0 : 0.0;
+    }
+    if (hi > lo) ctx->pd_active = std::max(ctx->pd_active, (int)PD_PF_END);
+    return ZMPM_OK;
+}
+
+int zmpm_set_phase_field_solver(zmpm_ctx* ctx, double parabolic_M, int32_t lumping, double delete_threshold, int32_t cg_max_iterations,
+    double cg_tolerance)
+{
+    if (!ctx || !(parabolic_M >= 0) || cg_max_iterations < 0 || !(cg_tolerance >= 0) || !(delete_threshold == delete_threshold))
+        return ZMPM_BAD_ARG;
+    ctx->pf_M = parabolic_M;
+    ctx->pf_lumping = lumping != 0;
+    ctx->pf_delete = delete_threshold;
+    ctx->pf_cg_max = cg_max_iterations;
+    ctx->pf_cg_tol = cg_tolerance;
+    return ZMPM_OK;
+}
+
+int zmpm_get_phase_field(zmpm_ctx* ctx, double* c, double* H, double* pf_Fp, double* vol)
+{
+    if (!ctx) return ZMPM_BAD_ARG;
+    cudaSetDevice(ctx->device);
+    int rc = download(ctx);
+    if (rc) return rc;
+    for (int64_t i = 0; i < ctx->P; ++i) {
+        if (c) c[i] = ctx->hpfc[i];
+        if (H) H[i] = ctx->hpfH[i];
+        if (pf_Fp) pf_Fp[i] = ctx->hpffp[i];
+        if (vol) vol[i] = ctx->hpfvol[i];
+    }
+    return ZMPM_OK;
+}
+
+int zmpm_set_phase_field_sigma_c(zmpm_ctx* ctx, const double* one_over_sigma_c)
+{
+    if (!ctx || !one_over_sigma_c) return ZMPM_BAD_ARG;
+    cudaSetDevice(ctx->device);
+    int rc = begin_edit(ctx);
+    if (rc) return rc;
+    for (int64_t i = 0; i < ctx->P; ++i) ctx->hpfisc[i] = one_over_sigma_c[i];
     return ZMPM_OK;
 }
 
@@ -703,12 +811,22 @@ int zmpm_get_plastic_state(zmpm_ctx* ctx, double* ys, int32_t* broken)
 }
 
 // ---------------------------------------------------------------- substep --
+// FractureSimulation::reinitialize -> deleteParticles (FractureSimulation.h:
+// 166-207) ahead of the binning; with a threshold <= 0 no particle qualifies.
+static int delete_phase_field_particles(zmpm_ctx* ctx)
+{
+    if (!ctx->has_pf || !(ctx->pf_delete > 0)) return ZMPM_OK;
+    return launch_phase_field_delete(ctx);
+}
+
 static int begin_implicit_impl(zmpm_ctx* ctx, double dt, bool damage = true)
 {
     int rc = upload(ctx);
     if (rc) return rc;
     ctx->dt = dt;
     ctx->implicit_ready = false;
+    rc = delete_phase_field_particles(ctx);
+    if (rc) return rc;
     rc = run_binning(ctx);
     if (rc) return rc;
     rc = run_p2g(ctx, damage);
@@ -747,6 +865,20 @@ int zmpm_substep(zmpm_ctx* ctx, double dt, const zmpm_solver* s, zmpm_stats* st)
         ctx->err = "viscoelastic particles need the ADMM or explicit integrator (StvkWithHencky has no stress differential)";
         return ZMPM_BAD_ARG;
     }
+    {
+        int rc = upload(ctx);
+        if (rc) return rc;
+    }
+    if (ctx->has_pf && admm) {
+        ctx->err = "the phase-field solve belongs to FractureSimulation; AdmmSimulation does not run it";
+        return ZMPM_BAD_ARG;
+    }
+    if (ctx->has_pf && !ctx->all_pf) {
+        ctx->err = "the phase-field solve needs the phase field on every particle (FractureSimulation.h:318-342 reads it for all)";
+        return ZMPM_BAD_ARG;
+    }
+    ctx->pf_iters = 0;
+    ctx->pf_res = 0;
     zmpm_stats local;
     if (!st) st = &local;
     std::memset(st, 0, sizeof(*st));
@@ -758,6 +890,8 @@ int zmpm_substep(zmpm_ctx* ctx, double dt, const zmpm_solver* s, zmpm_stats* st)
         if (rc) return rc;
         ctx->dt = dt;
         ctx->implicit_ready = false;
+        rc = delete_phase_field_particles(ctx);
+        if (rc) return rc;
         rc = run_binning(ctx);
         if (rc) return rc;
         ctx->graph_used = false;
@@ -798,6 +932,8 @@ int zmpm_substep(zmpm_ctx* ctx, double dt, const zmpm_solver* s, zmpm_stats* st)
     st->num_blocks = ctx->B;
     st->num_nodes = hc.N;
     st->ms_total = ms;
+    st->phase_field_iterations = ctx->pf_iters;
+    st->phase_field_residual = ctx->pf_res;
     if (ctx->graph_used && admm) // ADMM iteration: 7 head + 3 tail kernels; Krylov body: 6
         g_kernel_launches += 10 * (int64_t)hs.nit + 6 * (int64_t)hs.krylov_bodies;
     else if (ctx->graph_used) // Newton body: stress, force, residual, check, start, step, advance

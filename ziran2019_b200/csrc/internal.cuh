@@ -82,11 +82,13 @@ struct SolverScalars {
 enum MinresSlot { MR_GC0, MR_GS0, MR_GC1, MR_GS1, MR_GC2, MR_GS2, MR_RHS0, MR_RHS1, MR_BETA_KP1, MR_TK, MR_DELTA, MR_EPS };
 
 // Field indices of the particle pools.
-// Fields from PD_CORE on (viscoelastic strain, ADMM state) are moved by the
-// binning permutation only once a context uses them (Ctx::pd_active).
+// Fields from PD_CORE on (phase-field state, then viscoelastic strain and ADMM
+// state) are moved by the binning permutation only once a context uses them
+// (Ctx::pd_active: PD_CORE, PD_PF_END or PD_FIELDS).
 enum PdField { PD_X = 0, PD_V = 3, PD_C = 6, PD_F = 15, PD_M = 24, PD_VOL = 25, PD_MU = 26, PD_LAM = 27, PD_KAPPA = 28,
     PD_G = 29, PD_YS = 30, PD_XI = 31, PD_FS = 32, PD_CRACK = 33, PD_PF_C = 36, PD_PF_K = 37, PD_SIGMA_F = 38, PD_CORE = 39,
-    PD_FE = 39, PD_VMU = 48, PD_VLAM = 49, PD_VD = 50, PD_VV = 51, PD_Y = 52, PD_OMEGA = 70, PD_LASTDV = 72, PD_FIELDS = 75 };
+    PD_PF_H = 39, PD_PF_L0 = 40, PD_PF_ISC = 41, PD_PF_FP = 42, PD_PF_HMAX = 43, PD_PF_VOL = 44, PD_PF_ALLOW = 45, PD_PF_END = 46,
+    PD_FE = 46, PD_VMU = 55, PD_VLAM = 56, PD_VD = 57, PD_VV = 58, PD_Y = 59, PD_OMEGA = 77, PD_LASTDV = 79, PD_FIELDS = 82 };
 enum PiField { PI_KIND = 0, PI_PKIND = 1, PI_BROKEN = 2, PI_ID = 3, PI_DAMAGE = 4, PI_VISCO = 5, PI_FIELDS = 6 };
 
 // Adjoint particle arrays [AJ_FIELDS][Pcap] (FP64, slot order): the state
@@ -122,6 +124,17 @@ struct Ctx {
     std::vector<uint8_t> hkind, hpkind, hdamage, hvisco;
     std::vector<int32_t> hbroken;
     std::vector<double> hFe, hvmu, hvlam, hvd, hvv, hy, homega, hlastdv; // viscoelastic + ADMM state
+    std::vector<double> hpfH, hpfl0, hpfisc, hpffp, hpfhmax, hpfvol, hpfallow; // phase-field state (PhaseField.h:13-22)
+    // FractureSimulation members of the phase-field solve (FractureSimulation.h:48-63)
+    double pf_M = 0, pf_delete = 0, pf_cg_tol = 1e-6;
+    bool pf_lumping = true;
+    int pf_cg_max = 100;
+    bool has_pf = false;
+    bool all_pf = false;
+    int32_t pf_iters = 0;   // CG iterations and final |r| of the last phase-field solve
+    double pf_res = 0;
+    DBuf pfn;   // phase-field node arrays [B][PN_FIELDS][NPB]
+    DBuf pfsc;  // PfScalars of the phase-field CG
     bool has_damage = false;
     bool has_visco = false;
     bool mls = false;                     // the running explicit substep uses MLS-MPM (G2P gradV = C)
@@ -204,7 +217,9 @@ int run_newton(Ctx* ctx, const zmpm_solver& s);       // backward-Euler Newton
 int run_g2p(Ctx* ctx);                                 // G2P + evolveStrain + plasticity
 int upload_colliders(Ctx* ctx, double time, int slot = 0);    // slot 1: the state at t + dt
 int run_explicit(Ctx* ctx, const zmpm_solver& s);      // symplectic substep up to G2P
-int launch_explicit_stress(Ctx* ctx);                  // V0 tau(F) (+ V0 tau(Fe)) into the stress buffer
+int launch_explicit_stress(Ctx* ctx);
+int run_phase_field(Ctx* ctx, int32_t* iterations, double* residual); // FractureSimulation::solvePhaseFieldSystem after P2G
+int launch_phase_field_delete(Ctx* ctx);                               // FractureSimulation::deleteParticles before binning                  // V0 tau(F) (+ V0 tau(Fe)) into the stress buffer
 int launch_update(Ctx* ctx, bool gated = true);       // G2P(vn+dv) -> stress -> force P2G
 int launch_adj_g2p(Ctx* ctx, double* vsbar);           // adjoint of G2P (adjoint.cu)
 int launch_adj_particle(Ctx* ctx, const double* lam);  // adjoint of the force term, P2G and E

@@ -21,60 +21,13 @@
 
 #include "internal.cuh"
 #include "mat3.cuh"
+#include "node.cuh"
 
 namespace zmpm {
-
-constexpr int ND_THREADS = 256;
 
 int launch_p2g(Ctx* ctx);
 int launch_g2p(Ctx* ctx);
 int launch_hvp_krylov(Ctx* ctx, const double* x0, const double* x1, bool alt, double* out);
-
-// ------------------------------------------------------------ reductions --
-__device__ __forceinline__ double warp_sum(double v)
-{
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-    return v;
-}
-// Block sum; result valid in every thread.
-__device__ __forceinline__ double block_sum(double v)
-{
-    __shared__ double ws[ND_THREADS / 32];
-    __shared__ double total;
-    v = warp_sum(v);
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    __syncthreads();
-    if (lane == 0) ws[w] = v;
-    __syncthreads();
-    if (w == 0) {
-        double t = (lane < ND_THREADS / 32) ? ws[lane] : 0.0;
-        t = warp_sum(t);
-        if (lane == 0) total = t;
-    }
-    __syncthreads();
-    return total;
-}
-// Sum of n partials in a fixed order (identical in every CTA).
-__device__ __forceinline__ double reduce_partials(const double* __restrict__ part, int n)
-{
-    double s = 0;
-    for (int i = threadIdx.x; i < n; i += ND_THREADS) s += part[i];
-    return block_sum(s);
-}
-
-struct NodeGeom {
-    int64_t nn;        // B * NPB
-    int parts;         // CTAs of node kernels
-};
-
-template <int NPB>
-__device__ __forceinline__ int64_t vidx(int64_t n, int d) // component d of node n in [B][3][NPB]
-{
-    int64_t b = n / NPB;
-    int e = (int)(n - b * NPB);
-    return (b * 3 + d) * NPB + e;
-}
 
 __device__ __forceinline__ void project3(const int8_t* col, const double* P6, int64_t nn, int64_t n, double v[3])
 {
@@ -968,6 +921,10 @@ int run_p2g(Ctx* ctx, bool damage)
     if (damage) {
         rc = launch_damage(ctx); // the fracture hook runs after particlesToGrid
         if (rc) return rc;
+        if (ctx->has_pf) {
+            rc = run_phase_field(ctx, &ctx->pf_iters, &ctx->pf_res);
+            if (rc) return rc;
+        }
     }
     rc = upload_colliders(ctx, ctx->time);
     if (rc) return rc;
@@ -1012,6 +969,10 @@ int run_explicit(Ctx* ctx, const zmpm_solver& s)
     if (rc) return rc;
     rc = launch_damage(ctx);
     if (rc) return rc;
+    if (ctx->has_pf) {
+        rc = run_phase_field(ctx, &ctx->pf_iters, &ctx->pf_res);
+        if (rc) return rc;
+    }
     rc = upload_colliders(ctx, ctx->time, 0);
     if (rc) return rc;
     rc = upload_colliders(ctx, ctx->time + ctx->dt, 1);

@@ -180,6 +180,16 @@ class MpmParticleHandle:
         FractureSimulation::useNaiveDamage and sigmaF); needs NeoHookeanBorden."""
         self.sim._call("add_damage", self.lower, self.upper, abi.DAMAGE_RANKINE, float(sigma_f), float(residual_phase))
 
+    def addFBasedMpmForceWithPhaseField(self, percentage, l0, model=None, allow_damage=True, residual_phase=0.001):
+        """CD-MPM phase field (MpmParticleHandleBase::addFBasedMpmForceWithPhaseField,
+        MpmParticleHandleBase.cpp:92-118) on particles that already carry a
+        NeoHookeanBorden model (pass `model` to add it here); the simulation
+        then solves the phase-field system after P2G every substep."""
+        if model is not None:
+            self.addFBasedMpmForce(model)
+        self.sim._call("add_phase_field", self.lower, self.upper, float(percentage), float(l0), 1 if allow_damage else 0,
+                       float(residual_phase))
+
     def addFElasticNonequilibratedBasedMpmForce(self, model, viscosity_d, viscosity_v):
         """MpmParticleHandleBase::addFElasticNonequilibratedBasedMpmForce
         (MpmParticleHandleBase.cpp:468-478): Fe starts at I, relaxes by the
@@ -358,6 +368,23 @@ class MpmSimulation:
         c = np.empty(self.count)
         self._call("get_damage", ptr(c))
         return c
+
+    def setPhaseFieldSolver(self, parabolic_M=0.0, lumping=True, delete_particle_threshold=0.0, cg_max_iterations=100,
+                            cg_tolerance=1e-6):
+        """FractureSimulation::parabolic_M, lumping, delete_particle_threshold and
+        its CG's max iterations and tolerance (FractureSimulation.h:48-63, 444-446)."""
+        self._call("set_phase_field_solver", float(parabolic_M), 1 if lumping else 0, float(delete_particle_threshold),
+                   int(cg_max_iterations), float(cg_tolerance))
+
+    def getPhaseField(self):
+        """Per-particle phase-field state: c, H, pf_Fp and the current volume."""
+        out = {k: np.empty(self.count) for k in ("c", "H", "pf_Fp", "vol")}
+        self._call("get_phase_field", ptr(out["c"]), ptr(out["H"]), ptr(out["pf_Fp"]), ptr(out["vol"]))
+        return out
+
+    def setPhaseFieldSigmaC(self, one_over_sigma_c):
+        a = np.ascontiguousarray(one_over_sigma_c, dtype=np.float64)
+        self._call("set_phase_field_sigma_c", ptr(a))
 
     # reverse mode and checkpoints
     def adjointSubstep(self, dt, gx=None, gv=None, gC=None, gF=None, gE=None, tolerance=1e-12):
