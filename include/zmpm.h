@@ -76,7 +76,17 @@ enum zmpm_model {
 enum zmpm_plasticity {
     ZMPM_PLASTIC_NONE = 0,
     /* VonMisesStvkHencky::projectStrain, Lib/Ziran/Physics/PlasticityApplier.cpp:462-502 */
-    ZMPM_PLASTIC_VON_MISES = 1
+    ZMPM_PLASTIC_VON_MISES = 1,
+    /* DruckerPragerStvkHencky::projectStrain (PlasticityApplier.cpp:272-317; Klar
+       et al. 2016, sand) on StvkWithHenckyIsotropic particles: Hencky strain of
+       the SVD shifted by the cohesion, projection to the cone tip when the trace
+       (with the volume-correction log Jp) is >= 0, else onto the cone. */
+    ZMPM_PLASTIC_DRUCKER_PRAGER = 2,
+    /* NonAssociativeCamClay::projectStrain (PlasticityApplier.cpp:112-227, the
+       branch it runs: Compare_With_Physbam, :35-110) on NeoHookeanBorden
+       particles: projection of (p, s) onto the Cam-Clay ellipse with tips, and
+       the "fake hardening" update of log Jp. */
+    ZMPM_PLASTIC_CAM_CLAY = 3
 };
 
 /* Damage models applied after P2G (FractureSimulation::particlesToGrid,
@@ -241,6 +251,17 @@ int zmpm_set_lame(zmpm_ctx* ctx, int64_t lower, int64_t upper, const double* mu,
 /* MpmParticleHandleBase::addPlasticity (MpmParticleHandleBase.cpp:331-348). */
 int zmpm_add_plasticity(zmpm_ctx* ctx, int64_t lower, int64_t upper, int32_t kind,
     double yield_stress, double xi, double fail_stress);
+/* DruckerPragerStvkHencky(friction_angle [degrees], beta, cohesion,
+   volume_correction) (PlasticityApplier.cpp:247-261; defaults 30, 1, 0, 1) on
+   StvkWithHenckyIsotropic particles [lower, upper); log Jp starts at 0. */
+int zmpm_add_drucker_prager(zmpm_ctx* ctx, int64_t lower, int64_t upper, double friction_angle, double beta, double cohesion,
+    int32_t volume_correction);
+/* NonAssociativeCamClay(logJp, friction_angle [degrees], beta, xi, dim = 3,
+   hardeningOn) (PlasticityApplier.cpp:10-20) on NeoHookeanBorden particles. */
+int zmpm_add_cam_clay(zmpm_ctx* ctx, int64_t lower, int64_t upper, double log_jp, double friction_angle, double beta, double xi,
+    int32_t hardening);
+/* log Jp of Drucker-Prager and Cam-Clay particles (particle order; 0 otherwise). */
+int zmpm_get_log_jp(zmpm_ctx* ctx, double* log_jp);
 
 /* Damage on particles [lower, upper) that use NeoHookeanBorden: the phase
    field of MpmParticleHandleBase::addFBasedMpmForceWithPhaseField

@@ -759,7 +759,108 @@ struct Plastic {
     T yield_stress = 0, xi = 0, fail_stress = 0;
     int32_t broken = 0;
     T crack_normal[3] = { 0, 0, 0 };
+    // Drucker-Prager (alpha, beta, cohesion, volume_correction) and Cam-Clay
+    // (M, beta, xi, hardeningOn) members, log Jp of both
+    T a = 0, beta = 0, cx = 0, logJp = 0;
+    int32_t flag = 0;
 };
+
+// sin of an angle in degrees with the reference's constant for pi
+// (PlasticityApplier.cpp:17, :255)
+template <class T>
+static T sinDegrees(T angle)
+{
+    return std::sin(angle / T(180) * T(3.141592653));
+}
+
+// DruckerPragerStvkHencky::projectStrain, PlasticityApplier.cpp:272-317
+template <class T>
+static void druckerPragerProject(const Model<T>& c, Plastic<T>& p, M3<T>& F)
+{
+    M3<T> U, V;
+    T sigma[3];
+    svd3(F, U, sigma, V);
+    T eps[3];
+    for (int d = 0; d < 3; ++d) eps[d] = std::log(std::max(std::abs(sigma[d]), T(1e-4))) - p.cx;
+    const T esum = eps[0] + eps[1] + eps[2];
+    const T tr = esum + p.logJp;
+    T hat[3];
+    for (int d = 0; d < 3; ++d) hat[d] = eps[d] - (tr / T(3)) * T(1);
+    const T hat2 = hat[0] * hat[0] + hat[1] * hat[1] + hat[2] * hat[2];
+    if (tr >= T(0)) { // case II: the tip
+        const T ec = std::exp(p.cx);
+        M3<T> Us = scaled(U, ec);
+        F = mulT(Us, V);
+        if (p.flag) p.logJp = p.beta * esum + p.logJp;
+        return;
+    }
+    else if (c.mu == 0)
+        return;
+    p.logJp = 0;
+    const T hn = std::sqrt(hat2);
+    const T dg = hn + (T(3) * c.lambda + T(2) * c.mu) / (T(2) * c.mu) * tr * p.a;
+    T H[3], eH[3];
+    for (int d = 0; d < 3; ++d) H[d] = (dg <= 0) ? eps[d] + p.cx : eps[d] - (dg / hn) * hat[d] + p.cx;
+    for (int d = 0; d < 3; ++d) eH[d] = std::exp(H[d]);
+    F = udiagvt(U, eH, V);
+}
+
+// NonAssociativeCamClay::projectStrain, PlasticityApplier.cpp:112-136, through
+// Compare_With_Physbam (:35-110), the branch the reference runs
+template <class T>
+static void camClayProject(const Model<T>& c, Plastic<T>& p, M3<T>& F)
+{
+    M3<T> U, V;
+    T Se[3];
+    svd3(F, U, Se, V);
+    const T p0 = c.kappa * (T(0.00001) + std::sinh(p.cx * std::max(-p.logJp, T(0))));
+    const T a = (T(1) + T(2) * p.beta) * (T(6) - T(3)) / T(2);
+    const T b = p.beta * p0, cc = p0, M2 = p.a * p.a;
+    T Je = 1;
+    for (int i = 0; i < 3; ++i) Je *= Se[i];
+    T Se2[3];
+    for (int i = 0; i < 3; ++i) Se2[i] = Se[i] * Se[i];
+    T mean = 0;
+    for (int i = 0; i < 3; ++i) mean += Se2[i];
+    mean /= T(3);
+    const T sc = c.mu * std::pow(Je, -T(2) / T(3));
+    T s[3];
+    for (int i = 0; i < 3; ++i) s[i] = sc * (Se2[i] - mean);
+    const T Uprime = c.kappa / T(2) * (Je - 1 / Je);
+    const T p_trial = -Uprime * Je;
+    if (p_trial > cc || p_trial < -b) { // the tips
+        const T Je_new = (p_trial > cc) ? std::sqrt(-2 * cc / c.kappa + 1) : std::sqrt(2 * b / c.kappa + 1);
+        const T r = std::pow(Je_new, T(1) / T(3));
+        for (int i = 0; i < 3; ++i) Se[i] = r;
+        p.logJp += std::log(Je / Je_new);
+        F = udiagvt(U, Se, V);
+        return;
+    }
+    const T k = std::sqrt(-M2 * (p_trial + b) * (p_trial - cc) / a);
+    const T sn = std::sqrt(s[0] * s[0] + s[1] * s[1] + s[2] * s[2]);
+    const T y = a * (sn * sn) + M2 * (p_trial + b) * (p_trial - cc);
+    if (y < T(1e-4)) { // inside: the strain is rebuilt from its SVD
+        F = udiagvt(U, Se, V);
+        return;
+    }
+    const T pc = (T(1) - p.beta) * p0 / 2;
+    if (p0 > T(1e-4) && p_trial < p0 - T(1e-4) && p_trial > -p.beta * p0 + T(1e-4)) {
+        const T aa = M2 * ((p_trial - pc) * (p_trial - pc)) / (a * (sn * sn));
+        const T dd = 1 + aa;
+        const T ff = aa * p.beta * p0 - aa * p0 - 2 * pc;
+        const T gg = pc * pc - aa * p.beta * (p0 * p0);
+        const T zz = std::sqrt(std::abs(ff * ff - 4 * dd * gg));
+        const T p1 = (-ff + zz) / (2 * dd);
+        const T p2 = (-ff - zz) / (2 * dd);
+        const T p_fake = (p_trial - pc) * (p1 - pc) > 0 ? p1 : p2;
+        const T Je_new_fake = std::sqrt(std::abs(-2 * p_fake / c.kappa + 1));
+        if (Je_new_fake > T(1e-4)) p.logJp += std::log(Je / Je_new_fake);
+    }
+    const T g = k / c.mu * std::pow(Je, T(2) / T(3));
+    const T tr = T(1) / T(3) * (Se2[0] + Se2[1] + Se2[2]);
+    for (int i = 0; i < 3; ++i) Se[i] = std::sqrt(g * s[i] / sn + tr * T(1));
+    F = udiagvt(U, Se, V);
+}
 
 // VonMisesStvkHencky::projectStrain, PlasticityApplier.cpp:462-502
 template <class T>
@@ -2837,7 +2938,12 @@ struct Sim {
             for (int r = 0; r < 3; ++r)
                 for (int c = 0; c < 3; ++c) A.a[r][c] += (T)dt * gradV[i].a[r][c];
             M3<T> Fp = mul(A, load9(F, i));
-            if (plastic[i].kind == ZMPM_PLASTIC_VON_MISES) vonMisesProject(model[i], plastic[i], Fp);
+            if (plastic[i].kind == ZMPM_PLASTIC_VON_MISES)
+                vonMisesProject(model[i], plastic[i], Fp);
+            else if (plastic[i].kind == ZMPM_PLASTIC_DRUCKER_PRAGER)
+                druckerPragerProject(model[i], plastic[i], Fp);
+            else if (plastic[i].kind == ZMPM_PLASTIC_CAM_CLAY)
+                camClayProject(model[i], plastic[i], Fp);
             store9(F, i, Fp);
             if (visco[i].on) {
                 M3<T> Fep = mul(A, load9(Fe, i));
@@ -2895,6 +3001,12 @@ struct Sim {
         }
         pf_iters = 0;
         pf_res = 0;
+        if (s.integrator == ZMPM_ADMM)
+            for (int64_t i = 0; i < P; ++i)
+                if (plastic[i].kind == ZMPM_PLASTIC_DRUCKER_PRAGER || plastic[i].kind == ZMPM_PLASTIC_CAM_CLAY) {
+                    err = "the ADMM local step has no Drucker-Prager or Cam-Clay projection here";
+                    return ZMPM_UNSUPPORTED;
+                }
         if (anyPhaseField()) {
             if (s.integrator == ZMPM_ADMM) {
                 err = "the phase-field solve belongs to FractureSimulation; AdmmSimulation does not run it";
@@ -3094,6 +3206,7 @@ int zoracle_add_plasticity(Ctx* c, int64_t lo, int64_t hi, int32_t kind, double 
     DISPATCH(c, {
         using T = typename std::remove_reference<decltype(S.dx)>::type;
         if (lo < 0 || hi > S.P || lo > hi) return ZMPM_BAD_ARG;
+        if (kind != ZMPM_PLASTIC_NONE && kind != ZMPM_PLASTIC_VON_MISES) return ZMPM_BAD_ARG;
         for (int64_t i = lo; i < hi; ++i) {
             S.plastic[i].kind = kind;
             S.plastic[i].yield_stress = (T)ys;
@@ -3101,6 +3214,111 @@ int zoracle_add_plasticity(Ctx* c, int64_t lo, int64_t hi, int32_t kind, double 
             S.plastic[i].fail_stress = (T)fs;
         }
     });
+    return ZMPM_OK;
+}
+
+int zoracle_add_drucker_prager(Ctx* c, int64_t lo, int64_t hi, double friction_angle, double beta, double cohesion, int32_t vc)
+{
+    if (!c) return ZMPM_BAD_ARG;
+    DISPATCH(c, {
+        using T = typename std::remove_reference<decltype(S.dx)>::type;
+        if (lo < 0 || hi > S.P || lo > hi) return ZMPM_BAD_ARG;
+        for (int64_t i = lo; i < hi; ++i)
+            if (S.model[i].kind != ZMPM_MODEL_STVK_HENCKY_ISOTROPIC) {
+                S.err = "Drucker-Prager needs StvkWithHenckyIsotropic particles";
+                return ZMPM_BAD_ARG;
+            }
+        // DruckerPragerStvkHencky::DruckerPragerStvkHencky, PlasticityApplier.cpp:247-255
+        const T sin_phi = zo::sinDegrees((T)friction_angle);
+        const T alpha = std::sqrt(T(2) / T(3)) * T(2) * sin_phi / (T(3) - sin_phi);
+        for (int64_t i = lo; i < hi; ++i) {
+            zo::Plastic<T>& p = S.plastic[i];
+            p = zo::Plastic<T>();
+            p.kind = ZMPM_PLASTIC_DRUCKER_PRAGER;
+            p.a = alpha;
+            p.beta = (T)beta;
+            p.cx = (T)cohesion;
+            p.flag = vc ? 1 : 0;
+            p.logJp = 0;
+            // reported by get_plastic_state in the library's per-kind layout
+            p.yield_stress = p.a;
+            p.xi = p.beta;
+            p.fail_stress = p.cx;
+            p.broken = p.flag;
+        }
+    });
+    return ZMPM_OK;
+}
+
+int zoracle_add_cam_clay(Ctx* c, int64_t lo, int64_t hi, double logJp, double friction_angle, double beta, double xi, int32_t hardening)
+{
+    if (!c) return ZMPM_BAD_ARG;
+    DISPATCH(c, {
+        using T = typename std::remove_reference<decltype(S.dx)>::type;
+        if (lo < 0 || hi > S.P || lo > hi) return ZMPM_BAD_ARG;
+        for (int64_t i = lo; i < hi; ++i)
+            if (S.model[i].kind != ZMPM_MODEL_NEOHOOKEAN_BORDEN) {
+                S.err = "Cam-Clay needs NeoHookeanBorden particles";
+                return ZMPM_BAD_ARG;
+            }
+        // NonAssociativeCamClay::NonAssociativeCamClay with dim = 3, PlasticityApplier.cpp:10-20
+        const T sin_phi = zo::sinDegrees((T)friction_angle);
+        const T mc = std::sqrt(T(2) / T(3)) * T(2) * sin_phi / (T(3) - sin_phi);
+        const T M = mc * T(3) / std::sqrt(T(2) / (T(6) - T(3)));
+        for (int64_t i = lo; i < hi; ++i) {
+            zo::Plastic<T>& p = S.plastic[i];
+            p = zo::Plastic<T>();
+            p.kind = ZMPM_PLASTIC_CAM_CLAY;
+            p.a = M;
+            p.beta = (T)beta;
+            p.cx = (T)xi;
+            p.flag = hardening ? 1 : 0;
+            p.logJp = (T)logJp;
+            p.yield_stress = p.a;
+            p.xi = p.beta;
+            p.fail_stress = p.cx;
+            p.broken = p.flag;
+        }
+    });
+    return ZMPM_OK;
+}
+
+int zoracle_get_log_jp(Ctx* c, double* out)
+{
+    if (!c || !out) return ZMPM_BAD_ARG;
+    DISPATCH(c, {
+        for (int64_t i = 0; i < S.P; ++i) out[i] = S.plastic[i].logJp;
+    });
+    return ZMPM_OK;
+}
+
+// One Drucker-Prager (kind 2) or Cam-Clay (kind 3) projection of a row-major F
+// in place, for known-answer tests: params = (alpha or M, beta, cohesion or xi),
+// model (mu, lambda, kappa).
+int zoracle_plastic_project(int32_t kind, double mu, double lambda, double kappa, const double* params, int32_t flag, double* logJp,
+    double* F)
+{
+    zo::Model<double> c;
+    c.mu = mu;
+    c.lambda = lambda;
+    c.kappa = kappa;
+    zo::Plastic<double> p;
+    p.kind = kind;
+    p.a = params[0];
+    p.beta = params[1];
+    p.cx = params[2];
+    p.flag = flag;
+    p.logJp = *logJp;
+    zo::M3<double> Fm;
+    for (int i = 0; i < 9; ++i) Fm.a[i / 3][i % 3] = F[i];
+    if (kind == ZMPM_PLASTIC_DRUCKER_PRAGER)
+        zo::druckerPragerProject(c, p, Fm);
+    else if (kind == ZMPM_PLASTIC_CAM_CLAY)
+        zo::camClayProject(c, p, Fm);
+    else
+        return ZMPM_BAD_ARG;
+    for (int i = 0; i < 9; ++i) F[i] = Fm.a[i / 3][i % 3];
+    *logJp = p.logJp;
     return ZMPM_OK;
 }
 

@@ -453,3 +453,115 @@ def test_phase_field_refusals(oracle):
     h2, _ = build_scene(s2, kind="fcr", n=4, dx=1.0 / 64)
     with pytest.raises(abi.ZmpmError):
         h2.addFBasedMpmForceWithPhaseField(0.05, 0.5 / 64)
+
+
+def _dp_numpy(F, mu, lam, alpha, beta, cohesion, vc, logJp):
+    """Drucker-Prager return map restated from Klar et al. 2016 (the reference's
+    DruckerPragerStvkHencky::projectStrain) with numpy's SVD; isotropic, so the
+    SVD's sign and order conventions do not matter for det F > 0."""
+    U, s, Vt = np.linalg.svd(F)
+    eps = np.log(np.maximum(np.abs(s), 1e-4)) - cohesion
+    tr = eps.sum() + logJp
+    hat = eps - tr / 3
+    if tr >= 0:
+        return np.exp(cohesion) * U @ Vt, (beta * eps.sum() + logJp if vc else logJp)
+    hn = np.linalg.norm(hat)
+    dg = hn + (3 * lam + 2 * mu) / (2 * mu) * tr * alpha
+    H = eps + cohesion if dg <= 0 else eps - dg / hn * hat + cohesion
+    return U @ np.diag(np.exp(H)) @ Vt, 0.0
+
+
+def _camclay_numpy(F, mu, kappa, M, beta, xi, logJp):
+    """Cam-Clay projection (the reference's Compare_With_Physbam branch of
+    NonAssociativeCamClay::projectStrain) restated with numpy's SVD."""
+    U, Se, Vt = np.linalg.svd(F)
+    p0 = kappa * (1e-5 + np.sinh(xi * max(-logJp, 0.0)))
+    a = (1 + 2 * beta) * 3 / 2
+    b, c, M2 = beta * p0, p0, M * M
+    Je = np.prod(Se)
+    Se2 = Se ** 2
+    s = mu * Je ** (-2 / 3) * (Se2 - Se2.mean())
+    p_trial = -kappa / 2 * (Je - 1 / Je) * Je
+    if p_trial > c or p_trial < -b:
+        Je_new = np.sqrt(-2 * c / kappa + 1) if p_trial > c else np.sqrt(2 * b / kappa + 1)
+        return Je_new ** (1 / 3) * U @ Vt, logJp + np.log(Je / Je_new)
+    k = np.sqrt(-M2 * (p_trial + b) * (p_trial - c) / a)
+    sn = np.linalg.norm(s)
+    if a * sn ** 2 + M2 * (p_trial + b) * (p_trial - c) < 1e-4:
+        return F.copy(), logJp
+    pc = (1 - beta) * p0 / 2
+    if p0 > 1e-4 and p0 - 1e-4 > p_trial > -beta * p0 + 1e-4:
+        aa = M2 * (p_trial - pc) ** 2 / (a * sn ** 2)
+        dd, ff, gg = 1 + aa, aa * beta * p0 - aa * p0 - 2 * pc, pc ** 2 - aa * beta * p0 ** 2
+        zz = np.sqrt(abs(ff ** 2 - 4 * dd * gg))
+        p1, p2 = (-ff + zz) / (2 * dd), (-ff - zz) / (2 * dd)
+        p_fake = p1 if (p_trial - pc) * (p1 - pc) > 0 else p2
+        Jf = np.sqrt(abs(-2 * p_fake / kappa + 1))
+        if Jf > 1e-4:
+            logJp += np.log(Je / Jf)
+    be = k / mu * Je ** (2 / 3) * s / sn + Se2.sum() / 3
+    return U @ np.diag(np.sqrt(be)) @ Vt, logJp
+
+
+def test_drucker_prager_and_cam_clay_known_answers(oracle):
+    """The oracle's Drucker-Prager and Cam-Clay return maps against numpy
+    restatements over compressed, sheared and stretched strains (every branch:
+    inside, cone / ellipse projection, tips, fake hardening)."""
+    d = oracle.dll
+    rng = np.random.default_rng(12)
+    E, nu = 1e4, 0.3
+    mu, lam = E / (2 * (1 + nu)), E * nu / ((1 + nu) * (1 - 2 * nu))
+    kappa = 0.666666 * mu + lam
+    sphi = np.sin(30 / 180 * 3.141592653)
+    alpha = np.sqrt(2 / 3) * 2 * sphi / (3 - sphi)
+    M = alpha * 3 / np.sqrt(2 / 3)
+    seen_dp, seen_cc = set(), set()
+    for trial in range(400):
+        R1, _ = np.linalg.qr(rng.standard_normal((3, 3)))
+        R2, _ = np.linalg.qr(rng.standard_normal((3, 3)))
+        R1 *= np.sign(np.linalg.det(R1))
+        R2 *= np.sign(np.linalg.det(R2))
+        vol = rng.choice([0.9, 0.97, 1.0, 1.03, 1.2])
+        s = vol * np.exp(rng.normal(0, 0.08, 3))
+        F = R1 @ np.diag(s) @ R2.T
+        for cohesion, vc, logJp in ((0.0, 1, 0.0), (0.01, 1, -0.02), (0.0, 0, 0.05)):
+            out = F.ravel().copy()
+            lj = C.c_double(logJp)
+            prm = np.array([alpha, 1.0, cohesion])
+            assert d.zoracle_plastic_project(2, mu, lam, kappa, P(prm), vc, C.byref(lj), P(out)) == 0
+            want, wl = _dp_numpy(F, mu, lam, alpha, 1.0, cohesion, vc, logJp)
+            np.testing.assert_allclose(out.reshape(3, 3), want, rtol=0, atol=1e-12)
+            assert abs(lj.value - wl) < 1e-12
+            seen_dp.add("tip" if np.allclose(want @ want.T, np.exp(2 * cohesion) * np.eye(3)) else
+                        ("in" if np.allclose(want, F) else "cone"))
+        for beta, xi, logJp in ((0.5, 2.0, -0.05), (0.2, 5.0, -0.2), (0.0, 1.0, 0.0)):
+            out = F.ravel().copy()
+            lj = C.c_double(logJp)
+            prm = np.array([M, beta, xi])
+            assert d.zoracle_plastic_project(3, mu, lam, kappa, P(prm), 1, C.byref(lj), P(out)) == 0
+            want, wl = _camclay_numpy(F, mu, kappa, M, beta, xi, logJp)
+            np.testing.assert_allclose(out.reshape(3, 3), want, rtol=0, atol=1e-11)
+            assert abs(lj.value - wl) < 1e-11
+            seen_cc.add("moved" if not np.allclose(want, F) else "in")
+    assert seen_dp == {"tip", "in", "cone"} and seen_cc == {"moved", "in"}
+
+
+@pytest.mark.parametrize("kind", ["dp", "cc"])
+def test_sand_and_clay_substeps(oracle, kind):
+    """A falling block with Drucker-Prager (sand) or Cam-Clay (clay) plasticity
+    lands on the ground: log Jp evolves and every substep is clean.  The sand
+    starts dilated (F = 1.05 I), which sends it to the cone tip (the volume
+    correction then stores the excess in log Jp)."""
+    dx = 1.0 / 64
+    s = mpm.MpmSimulation(dx, gravity=(0, -9.8, 0), precision="fp64", lib=oracle)
+    model = "hencky" if kind == "dp" else "nh"
+    h, x = build_scene(s, kind=model, n=6, dx=dx, v0=(0, -2.0, 0), lo=(0.375, 8 * dx, 0.375), ground=7 * dx)
+    if kind == "dp":
+        s.setParticles(F=np.tile(1.05 * np.eye(3), (len(x), 1, 1)))
+        h.addPlasticity(None, mpm.DruckerPragerStvkHencky(30.0, 1.0, 0.0, True))
+    else:
+        h.addPlasticity(None, mpm.NonAssociativeCamClay(-0.01, 45.0, 0.3, 3.0, True))
+    for _ in range(8):
+        assert s.advanceOneTimeStep(1e-3) == abi.OK
+    lj = s.getLogJp()
+    assert np.all(np.isfinite(lj)) and np.abs(lj).max() > 0

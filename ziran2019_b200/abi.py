@@ -30,7 +30,7 @@ MIXED = 1
 NOALLOC_MAX_PARTICLES = 262144
 LAYOUT_AUTO, LAYOUT_244, LAYOUT_444 = 0, 1, 2
 MODEL_NONE, MODEL_NEOHOOKEAN_BORDEN, MODEL_STVK_HENCKY_ISOTROPIC, MODEL_FIXED_COROTATED = 0, 1, 2, 3
-PLASTIC_NONE, PLASTIC_VON_MISES = 0, 1
+PLASTIC_NONE, PLASTIC_VON_MISES, PLASTIC_DRUCKER_PRAGER, PLASTIC_CAM_CLAY = 0, 1, 2, 3
 DAMAGE_NONE, DAMAGE_RANKINE, DAMAGE_PHASE_FIELD = 0, 1, 2
 NEWTON, ADMM, EXPLICIT = 0, 1, 2
 MINRES, CG = 0, 1
@@ -136,6 +136,9 @@ _SIGS = {
     "add_fbased_force": (C.c_int, [C.c_void_p, C.c_int64, C.c_int64, C.c_int32, C.c_double, C.c_double]),
     "set_lame": (C.c_int, [C.c_void_p, C.c_int64, C.c_int64, c_double_p, c_double_p]),
     "add_plasticity": (C.c_int, [C.c_void_p, C.c_int64, C.c_int64, C.c_int32, C.c_double, C.c_double, C.c_double]),
+    "add_drucker_prager": (C.c_int, [C.c_void_p, C.c_int64, C.c_int64, C.c_double, C.c_double, C.c_double, C.c_int32]),
+    "add_cam_clay": (C.c_int, [C.c_void_p, C.c_int64, C.c_int64, C.c_double, C.c_double, C.c_double, C.c_double, C.c_int32]),
+    "get_log_jp": (C.c_int, [C.c_void_p, c_double_p]),
     "add_damage": (C.c_int, [C.c_void_p, C.c_int64, C.c_int64, C.c_int32, C.c_double, C.c_double]),
     "get_damage": (C.c_int, [C.c_void_p, c_double_p]),
     "add_phase_field": (C.c_int, [C.c_void_p, C.c_int64, C.c_int64, C.c_double, C.c_double, C.c_int32, C.c_double]),

@@ -79,6 +79,7 @@ int upload(Ctx* ctx)
         hpd[PD_PF_C * cap + i] = ctx->hpfc[i];
         hpd[PD_PF_K * cap + i] = ctx->hpfk[i];
         hpd[PD_SIGMA_F * cap + i] = ctx->hsigf[i];
+        hpd[PD_LOGJP * cap + i] = ctx->hlogjp[i];
         hpd[PD_PF_H * cap + i] = ctx->hpfH[i];
         hpd[PD_PF_L0 * cap + i] = ctx->hpfl0[i];
         hpd[PD_PF_ISC * cap + i] = ctx->hpfisc[i];
@@ -158,6 +159,7 @@ int download(Ctx* ctx)
         ctx->hpfc[i] = hpd[PD_PF_C * cap + s];
         ctx->hpfk[i] = hpd[PD_PF_K * cap + s];
         ctx->hsigf[i] = hpd[PD_SIGMA_F * cap + s];
+        ctx->hlogjp[i] = hpd[PD_LOGJP * cap + s];
         ctx->hdamage[i] = (uint8_t)hpi[PI_DAMAGE * cap + s];
         ctx->hkind[i] = (uint8_t)hpi[PI_KIND * cap + s];
         ctx->hpkind[i] = (uint8_t)hpi[PI_PKIND * cap + s];
@@ -512,6 +514,7 @@ int zmpm_add_particles(zmpm_ctx* ctx, int64_t n, const double* x, const double* 
         ctx->hpfc.push_back(1.0);
         ctx->hpfk.push_back(0.001);
         ctx->hsigf.push_back(0.0);
+        ctx->hlogjp.push_back(0.0);
         ctx->hdamage.push_back(ZMPM_DAMAGE_NONE);
         ctx->hkind.push_back(ZMPM_MODEL_NONE);
         ctx->hpkind.push_back(ZMPM_PLASTIC_NONE);
@@ -585,6 +588,72 @@ int zmpm_add_plasticity(zmpm_ctx* ctx, int64_t lo, int64_t hi, int32_t kind, dou
         ctx->hxi[i] = xi;
         ctx->hfs[i] = fs;
     }
+    return ZMPM_OK;
+}
+
+// sin of an angle in degrees with the reference's constant for pi
+// (PlasticityApplier.cpp:17, :255)
+static double sin_degrees(double angle) { return std::sin(angle / 180.0 * 3.141592653); }
+
+int zmpm_add_drucker_prager(zmpm_ctx* ctx, int64_t lo, int64_t hi, double friction_angle, double beta, double cohesion,
+    int32_t volume_correction)
+{
+    if (!ctx || lo < 0 || hi > ctx->P || lo > hi) return ZMPM_BAD_ARG;
+    cudaSetDevice(ctx->device);
+    int rc = begin_edit(ctx);
+    if (rc) return rc;
+    for (int64_t i = lo; i < hi; ++i)
+        if (ctx->hkind[i] != ZMPM_MODEL_STVK_HENCKY_ISOTROPIC) {
+            ctx->err = "Drucker-Prager needs StvkWithHenckyIsotropic particles";
+            return ZMPM_BAD_ARG;
+        }
+    // DruckerPragerStvkHencky::DruckerPragerStvkHencky, PlasticityApplier.cpp:247-255
+    const double sin_phi = sin_degrees(friction_angle);
+    const double alpha = std::sqrt(2.0 / 3.0) * 2.0 * sin_phi / (3.0 - sin_phi);
+    for (int64_t i = lo; i < hi; ++i) {
+        ctx->hpkind[i] = ZMPM_PLASTIC_DRUCKER_PRAGER;
+        ctx->hys[i] = alpha;
+        ctx->hxi[i] = beta;
+        ctx->hfs[i] = cohesion;
+        ctx->hbroken[i] = volume_correction ? 1 : 0;
+        ctx->hlogjp[i] = 0.0;
+    }
+    return ZMPM_OK;
+}
+
+int zmpm_add_cam_clay(zmpm_ctx* ctx, int64_t lo, int64_t hi, double log_jp, double friction_angle, double beta, double xi, int32_t hardening)
+{
+    if (!ctx || lo < 0 || hi > ctx->P || lo > hi) return ZMPM_BAD_ARG;
+    cudaSetDevice(ctx->device);
+    int rc = begin_edit(ctx);
+    if (rc) return rc;
+    for (int64_t i = lo; i < hi; ++i)
+        if (ctx->hkind[i] != ZMPM_MODEL_NEOHOOKEAN_BORDEN) {
+            ctx->err = "Cam-Clay needs NeoHookeanBorden particles";
+            return ZMPM_BAD_ARG;
+        }
+    // NonAssociativeCamClay::NonAssociativeCamClay with dim = 3, PlasticityApplier.cpp:10-20
+    const double sin_phi = sin_degrees(friction_angle);
+    const double mc = std::sqrt(2.0 / 3.0) * 2.0 * sin_phi / (3.0 - sin_phi);
+    const double M = mc * 3.0 / std::sqrt(2.0 / (6.0 - 3.0));
+    for (int64_t i = lo; i < hi; ++i) {
+        ctx->hpkind[i] = ZMPM_PLASTIC_CAM_CLAY;
+        ctx->hys[i] = M;
+        ctx->hxi[i] = beta;
+        ctx->hfs[i] = xi;
+        ctx->hbroken[i] = hardening ? 1 : 0;
+        ctx->hlogjp[i] = log_jp;
+    }
+    return ZMPM_OK;
+}
+
+int zmpm_get_log_jp(zmpm_ctx* ctx, double* log_jp)
+{
+    if (!ctx || !log_jp) return ZMPM_BAD_ARG;
+    cudaSetDevice(ctx->device);
+    int rc = download(ctx);
+    if (rc) return rc;
+    std::memcpy(log_jp, ctx->hlogjp.data(), ctx->P * sizeof(double));
     return ZMPM_OK;
 }
 
@@ -869,6 +938,12 @@ int zmpm_substep(zmpm_ctx* ctx, double dt, const zmpm_solver* s, zmpm_stats* st)
         int rc = upload(ctx);
         if (rc) return rc;
     }
+    if (admm)
+        for (int64_t i = 0; i < ctx->P; ++i)
+            if (ctx->hpkind[i] == ZMPM_PLASTIC_DRUCKER_PRAGER || ctx->hpkind[i] == ZMPM_PLASTIC_CAM_CLAY) {
+                ctx->err = "the ADMM local step has no Drucker-Prager or Cam-Clay projection here";
+                return ZMPM_UNSUPPORTED;
+            }
     if (ctx->has_pf && admm) {
         ctx->err = "the phase-field solve belongs to FractureSimulation; AdmmSimulation does not run it";
         return ZMPM_BAD_ARG;

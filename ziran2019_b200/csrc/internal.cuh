@@ -85,10 +85,15 @@ enum MinresSlot { MR_GC0, MR_GS0, MR_GC1, MR_GS1, MR_GC2, MR_GS2, MR_RHS0, MR_RH
 // Fields from PD_CORE on (phase-field state, then viscoelastic strain and ADMM
 // state) are moved by the binning permutation only once a context uses them
 // (Ctx::pd_active: PD_CORE, PD_PF_END or PD_FIELDS).
+// Plasticity parameters by kind: von Mises PD_YS = yield stress, PD_XI = xi,
+// PD_FS = fail stress, PI_BROKEN = broken; Drucker-Prager PD_YS = alpha,
+// PD_XI = beta, PD_FS = cohesion, PI_BROKEN = volume_correction; Cam-Clay
+// PD_YS = M, PD_XI = beta, PD_FS = xi, PI_BROKEN = hardeningOn.  PD_LOGJP is
+// log Jp of the last two.
 enum PdField { PD_X = 0, PD_V = 3, PD_C = 6, PD_F = 15, PD_M = 24, PD_VOL = 25, PD_MU = 26, PD_LAM = 27, PD_KAPPA = 28,
-    PD_G = 29, PD_YS = 30, PD_XI = 31, PD_FS = 32, PD_CRACK = 33, PD_PF_C = 36, PD_PF_K = 37, PD_SIGMA_F = 38, PD_CORE = 39,
-    PD_PF_H = 39, PD_PF_L0 = 40, PD_PF_ISC = 41, PD_PF_FP = 42, PD_PF_HMAX = 43, PD_PF_VOL = 44, PD_PF_ALLOW = 45, PD_PF_END = 46,
-    PD_FE = 46, PD_VMU = 55, PD_VLAM = 56, PD_VD = 57, PD_VV = 58, PD_Y = 59, PD_OMEGA = 77, PD_LASTDV = 79, PD_FIELDS = 82 };
+    PD_G = 29, PD_YS = 30, PD_XI = 31, PD_FS = 32, PD_CRACK = 33, PD_PF_C = 36, PD_PF_K = 37, PD_SIGMA_F = 38, PD_LOGJP = 39, PD_CORE = 40,
+    PD_PF_H = 40, PD_PF_L0 = 41, PD_PF_ISC = 42, PD_PF_FP = 43, PD_PF_HMAX = 44, PD_PF_VOL = 45, PD_PF_ALLOW = 46, PD_PF_END = 47,
+    PD_FE = 47, PD_VMU = 56, PD_VLAM = 57, PD_VD = 58, PD_VV = 59, PD_Y = 60, PD_OMEGA = 78, PD_LASTDV = 80, PD_FIELDS = 83 };
 enum PiField { PI_KIND = 0, PI_PKIND = 1, PI_BROKEN = 2, PI_ID = 3, PI_DAMAGE = 4, PI_VISCO = 5, PI_FIELDS = 6 };
 
 // Adjoint particle arrays [AJ_FIELDS][Pcap] (FP64, slot order): the state
@@ -120,7 +125,7 @@ struct Ctx {
     // host copy of the scene until the first upload
     int64_t P = 0;
     bool uploaded = false;
-    std::vector<double> hx, hv, hC, hF, hcrack, hm, hvol, hmu, hlam, hkappa, hg, hys, hxi, hfs, hpfc, hpfk, hsigf;
+    std::vector<double> hx, hv, hC, hF, hcrack, hm, hvol, hmu, hlam, hkappa, hg, hys, hxi, hfs, hpfc, hpfk, hsigf, hlogjp;
     std::vector<uint8_t> hkind, hpkind, hdamage, hvisco;
     std::vector<int32_t> hbroken;
     std::vector<double> hFe, hvmu, hvlam, hvd, hvv, hy, homega, hlastdv; // viscoelastic + ADMM state

@@ -270,4 +270,110 @@ ZMPM_D void von_mises_project(T mu, T lambda, T& yield_stress, T xi, T fail_stre
     }
 }
 
+// DruckerPragerStvkHencky::projectStrain (PlasticityApplier.cpp:272-317):
+// Hencky strain of the SVD less the cohesion; the trace with log Jp >= 0 sends
+// F to the cone tip exp(cohesion) U V^T (and, with the volume correction, the
+// excess volume into log Jp), else log Jp = 0 and the strain is projected onto
+// the cone of friction coefficient alpha.
+template <class T>
+ZMPM_D void drucker_prager_project(T mu, T lambda, T alpha, T beta, T cohesion, int volume_correction, T& logJp, M3<T>& F)
+{
+    M3<T> U, V;
+    T sg[3];
+    svd3(F, U, sg, V);
+    T e[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        const T a = fabs(sg[d]);
+        e[d] = log(a > T(1e-4) ? a : T(1e-4)) - cohesion;
+    }
+    const T esum = e[0] + e[1] + e[2];
+    const T tr = esum + logJp;
+    T h[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) h[d] = e[d] - (tr / T(3));
+    const T h2 = h[0] * h[0] + h[1] * h[1] + h[2] * h[2];
+    if (tr >= T(0)) {
+        const T ec = exp(cohesion);
+        const T one[3] = { ec, ec, ec };
+        F = m3_udvt(U, one, V);
+        if (volume_correction) logJp = beta * esum + logJp;
+        return;
+    }
+    if (mu == T(0)) return;
+    logJp = T(0);
+    const T hn = sqrt(h2);
+    const T dg = hn + (T(3) * lambda + T(2) * mu) / (T(2) * mu) * tr * alpha;
+    T eH[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) eH[d] = exp((dg <= T(0)) ? e[d] + cohesion : e[d] - (dg / hn) * h[d] + cohesion);
+    F = m3_udvt(U, eH, V);
+}
+
+// NonAssociativeCamClay::projectStrain (PlasticityApplier.cpp:112-136) through
+// Compare_With_Physbam (:35-110), the branch the reference runs: pressure
+// p = -kappa/2 (J - 1/J) J and deviatoric s of the SVD; tips beyond p0 and
+// -beta p0; outside the ellipse a (s:s) + M^2 (p + beta p0)(p - p0) <= 1e-4 the
+// deviatoric part is scaled onto it, and log Jp takes the "fake hardening"
+// step towards the ellipse centre.  Inside, F is rebuilt from its SVD.
+template <class T>
+ZMPM_D void cam_clay_project(T mu, T kappa, T M, T beta, T xi, T& logJp, M3<T>& F)
+{
+    M3<T> U, V;
+    T Se[3];
+    svd3(F, U, Se, V);
+    const T nl = -logJp;
+    const T p0 = kappa * (T(0.00001) + sinh(xi * (nl > T(0) ? nl : T(0))));
+    const T a = (T(1) + T(2) * beta) * (T(6) - T(3)) / T(2);
+    const T b = beta * p0, c = p0, M2 = M * M;
+    T Je = T(1);
+#pragma unroll
+    for (int i = 0; i < 3; ++i) Je *= Se[i];
+    T Se2[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) Se2[i] = Se[i] * Se[i];
+    T mean = T(0);
+#pragma unroll
+    for (int i = 0; i < 3; ++i) mean += Se2[i];
+    mean /= T(3);
+    const T sc = mu * pow(Je, -T(2) / T(3));
+    T s[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) s[i] = sc * (Se2[i] - mean);
+    const T p_trial = -(kappa / T(2) * (Je - T(1) / Je)) * Je;
+    if (p_trial > c || p_trial < -b) {
+        const T Je_new = (p_trial > c) ? sqrt(-T(2) * c / kappa + T(1)) : sqrt(T(2) * b / kappa + T(1));
+        const T r = pow(Je_new, T(1) / T(3));
+        const T rr[3] = { r, r, r };
+        logJp += log(Je / Je_new);
+        F = m3_udvt(U, rr, V);
+        return;
+    }
+    const T k = sqrt(-M2 * (p_trial + b) * (p_trial - c) / a);
+    const T sn = sqrt(s[0] * s[0] + s[1] * s[1] + s[2] * s[2]);
+    const T y = a * (sn * sn) + M2 * (p_trial + b) * (p_trial - c);
+    if (y < T(1e-4)) {
+        F = m3_udvt(U, Se, V);
+        return;
+    }
+    const T pc = (T(1) - beta) * p0 / T(2);
+    if (p0 > T(1e-4) && p_trial < p0 - T(1e-4) && p_trial > -beta * p0 + T(1e-4)) {
+        const T aa = M2 * ((p_trial - pc) * (p_trial - pc)) / (a * (sn * sn));
+        const T dd = T(1) + aa;
+        const T ff = aa * beta * p0 - aa * p0 - T(2) * pc;
+        const T gg = pc * pc - aa * beta * (p0 * p0);
+        const T zz = sqrt(fabs(ff * ff - T(4) * dd * gg));
+        const T p1 = (-ff + zz) / (T(2) * dd);
+        const T p2 = (-ff - zz) / (T(2) * dd);
+        const T p_fake = (p_trial - pc) * (p1 - pc) > T(0) ? p1 : p2;
+        const T Je_new_fake = sqrt(fabs(-T(2) * p_fake / kappa + T(1)));
+        if (Je_new_fake > T(1e-4)) logJp += log(Je / Je_new_fake);
+    }
+    const T g = k / mu * pow(Je, T(2) / T(3));
+    const T tr = T(1) / T(3) * (Se2[0] + Se2[1] + Se2[2]);
+#pragma unroll
+    for (int i = 0; i < 3; ++i) Se[i] = sqrt(g * s[i] / sn + tr);
+    F = m3_udvt(U, Se, V);
+}
+
 } // namespace zmpm

@@ -631,7 +631,18 @@ __global__ void __launch_bounds__(XF_THREADS) k_g2p(const int32_t* __restrict__ 
             A.a[q] += dt * gv.a[q];
         }
         M3<double> F = m3_mul(A, F0);
-        if (pi[PI_PKIND * cap + s] == ZMPM_PLASTIC_VON_MISES) {
+        const int pkind = pi[PI_PKIND * cap + s];
+        if (pkind == ZMPM_PLASTIC_DRUCKER_PRAGER || pkind == ZMPM_PLASTIC_CAM_CLAY) {
+            double logJp = pd[PD_LOGJP * cap + s];
+            if (pkind == ZMPM_PLASTIC_DRUCKER_PRAGER)
+                drucker_prager_project<double>(pd[PD_MU * cap + s], pd[PD_LAM * cap + s], pd[PD_YS * cap + s], pd[PD_XI * cap + s],
+                    pd[PD_FS * cap + s], pi[PI_BROKEN * cap + s], logJp, F);
+            else
+                cam_clay_project<double>(pd[PD_MU * cap + s], pd[PD_KAPPA * cap + s], pd[PD_YS * cap + s], pd[PD_XI * cap + s],
+                    pd[PD_FS * cap + s], logJp, F);
+            pd[PD_LOGJP * cap + s] = logJp;
+        }
+        if (pkind == ZMPM_PLASTIC_VON_MISES) {
             double ys = pd[PD_YS * cap + s];
             int broken = pi[PI_BROKEN * cap + s];
             double crack[3] = { pd[(PD_CRACK + 0) * cap + s], pd[(PD_CRACK + 1) * cap + s], pd[(PD_CRACK + 2) * cap + s] };

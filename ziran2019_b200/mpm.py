@@ -61,6 +61,31 @@ class VonMisesStvkHencky:
         self.xi = float(xi)
 
 
+class DruckerPragerStvkHencky:
+    """DruckerPragerStvkHencky(friction_angle, beta, cohesion, volume_correction),
+    PlasticityApplier.cpp:247-261 (sand; StvkWithHenckyIsotropic particles)."""
+    kind = abi.PLASTIC_DRUCKER_PRAGER
+
+    def __init__(self, friction_angle=30.0, beta=1.0, cohesion=0.0, volume_correction=True):
+        self.friction_angle = float(friction_angle)
+        self.beta = float(beta)
+        self.cohesion = float(cohesion)
+        self.volume_correction = bool(volume_correction)
+
+
+class NonAssociativeCamClay:
+    """NonAssociativeCamClay(logJp, friction_angle, beta, xi, dim=3, hardeningOn),
+    PlasticityApplier.cpp:10-20 (snow / clay; NeoHookeanBorden particles)."""
+    kind = abi.PLASTIC_CAM_CLAY
+
+    def __init__(self, logJp=0.0, friction_angle=0.0, beta=0.0, xi=0.0, hardeningOn=True):
+        self.logJp = float(logJp)
+        self.friction_angle = float(friction_angle)
+        self.beta = float(beta)
+        self.xi = float(xi)
+        self.hardeningOn = bool(hardeningOn)
+
+
 # -------------------------------------------------------------- colliders --
 class HalfSpace:
     """HalfSpace(origin, outward_normal), AnalyticLevelSet.cpp:259-304."""
@@ -198,8 +223,15 @@ class MpmParticleHandle:
 
     def addPlasticity(self, model, plasticity):
         del model  # the model is the one attached with addFBasedMpmForce
-        self.sim._call("add_plasticity", self.lower, self.upper, plasticity.kind,
-                       plasticity.yield_stress, plasticity.xi, plasticity.fail_stress)
+        if plasticity.kind == abi.PLASTIC_DRUCKER_PRAGER:
+            self.sim._call("add_drucker_prager", self.lower, self.upper, plasticity.friction_angle, plasticity.beta,
+                           plasticity.cohesion, 1 if plasticity.volume_correction else 0)
+        elif plasticity.kind == abi.PLASTIC_CAM_CLAY:
+            self.sim._call("add_cam_clay", self.lower, self.upper, plasticity.logJp, plasticity.friction_angle, plasticity.beta,
+                           plasticity.xi, 1 if plasticity.hardeningOn else 0)
+        else:
+            self.sim._call("add_plasticity", self.lower, self.upper, plasticity.kind,
+                           plasticity.yield_stress, plasticity.xi, plasticity.fail_stress)
 
 
 # ------------------------------------------------------------ simulation --
@@ -429,6 +461,12 @@ class MpmSimulation:
     def setViscoelasticStrain(self, Fe):
         Fe = np.ascontiguousarray(Fe, dtype=np.float64).reshape(self.count, 3, 3)
         self._call("set_viscoelastic_strain", ptr(Fe))
+
+    def getLogJp(self):
+        """log Jp of Drucker-Prager and Cam-Clay particles."""
+        out = np.empty(self.count)
+        self._call("get_log_jp", ptr(out))
+        return out
 
     def getPlasticState(self):
         n = self.count
