@@ -363,6 +363,27 @@ int zmpm_adjoint_substep(zmpm_ctx* ctx, double dt, const zmpm_solver* s, double 
 int zmpm_checkpoint_save(zmpm_ctx* ctx, int32_t slot);
 int zmpm_checkpoint_load(zmpm_ctx* ctx, int32_t slot);
 
+/* Restart files: the role of SimulationBase::write / read with
+   MpmSimulationBase::writeState / readState (SimulationBase.h:146-187,
+   MpmSimulationBase.cpp:725-761).  The library's own versioned binary format
+   (every per-particle array by name, the colliders, the phase-field solver
+   settings and the time), not the reference's DataManager stream, whose
+   attribute order follows a hash map.  read_state replaces the context's
+   particles; the context must have the file's dx and grid size. */
+int zmpm_write_state(zmpm_ctx* ctx, const char* path);
+int zmpm_read_state(zmpm_ctx* ctx, const char* path);
+
+/* Particle output in Houdini's binary geometry point format (BGEO version 5,
+   uncompressed, big-endian), as the reference writes it through Partio:
+   writePartio (PartioIO.h:138-182) stores "position"; FractureSimulation's
+   frame dump (FractureSimulation.h:110-146) adds "pf" and "sigmaC". */
+enum zmpm_bgeo_fields {
+    ZMPM_BGEO_POSITION = 0,     /* position only */
+    ZMPM_BGEO_VELOCITY = 1,     /* + "v" (3 floats) */
+    ZMPM_BGEO_PHASE_FIELD = 2   /* + "pf" and "sigmaC" (1 float each; 1 without a phase field) */
+};
+int zmpm_write_bgeo(zmpm_ctx* ctx, const char* path, int32_t fields);
+
 /* Default solver settings of the reference (MpmSimulationBase.cpp:51,
    BackwardEuler.h:56-62, LinearSolver.h:24). */
 void zmpm_default_solver(zmpm_solver* s, int32_t linear_solver, int32_t precision);

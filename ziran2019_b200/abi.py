@@ -33,6 +33,7 @@ MODEL_NONE, MODEL_NEOHOOKEAN_BORDEN, MODEL_STVK_HENCKY_ISOTROPIC, MODEL_FIXED_CO
 PLASTIC_NONE, PLASTIC_VON_MISES, PLASTIC_DRUCKER_PRAGER, PLASTIC_CAM_CLAY = 0, 1, 2, 3
 DAMAGE_NONE, DAMAGE_RANKINE, DAMAGE_PHASE_FIELD = 0, 1, 2
 NEWTON, ADMM, EXPLICIT = 0, 1, 2
+BGEO_POSITION, BGEO_VELOCITY, BGEO_PHASE_FIELD = 0, 1, 2
 MINRES, CG = 0, 1
 HALF_SPACE, SPHERE, BOX = 0, 1, 2
 STICKY, SLIP, SEPARATE, GHOST = 1, 2, 3, 4
@@ -176,6 +177,9 @@ _PRODUCT_ONLY = {
     "status_string": (C.c_char_p, [C.c_int]),
     "sort_keys_noalloc": (C.c_int, [C.c_void_p, C.c_int64, C.c_double, C.c_int32, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p]),
     "default_solver": (None, [C.POINTER(Solver), C.c_int32, C.c_int32]),
+    "write_state": (C.c_int, [C.c_void_p, C.c_char_p]),
+    "read_state": (C.c_int, [C.c_void_p, C.c_char_p]),
+    "write_bgeo": (C.c_int, [C.c_void_p, C.c_char_p, C.c_int32]),
 }
 
 

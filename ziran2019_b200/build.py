@@ -12,7 +12,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT_DIR = os.path.join(HERE, "lib")
 OUT = os.path.join(OUT_DIR, "libzmpm.so")
-SOURCES = ["adjoint.cu", "admm.cu", "api.cu", "bin.cu", "noalloc.cu", "phase.cu", "prims.cu", "solver.cu", "transfer.cu"]
+SOURCES = ["adjoint.cu", "admm.cu", "api.cu", "bin.cu", "io.cu", "noalloc.cu", "phase.cu", "prims.cu", "solver.cu", "transfer.cu"]
 HEADERS = ["admm.cuh", "common.cuh", "internal.cuh", "mat3.cuh", "models.cuh", "node.cuh", "svd3.cuh", "xfer.cuh"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = [

@@ -36,6 +36,10 @@ int64_t key_bits_for(const int pages[3])
     return bitlen(hi);
 }
 
+} // namespace
+
+namespace zmpm {
+
 // Puts the host scene on the device (first use) with slot = particle index.
 int upload(Ctx* ctx)
 {
@@ -197,6 +201,10 @@ int begin_edit(Ctx* ctx)
     ctx->implicit_ready = false;
     return ZMPM_OK;
 }
+
+} // namespace zmpm
+
+namespace {
 
 void quat_to_R(const double q[4], double R[9])
 {

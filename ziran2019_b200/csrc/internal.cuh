@@ -221,6 +221,9 @@ int run_p2g(Ctx* ctx, bool damage = true);            // P2G (+ damage hook) + g
 int run_newton(Ctx* ctx, const zmpm_solver& s);       // backward-Euler Newton
 int run_g2p(Ctx* ctx);                                 // G2P + evolveStrain + plasticity
 int upload_colliders(Ctx* ctx, double time, int slot = 0);    // slot 1: the state at t + dt
+int upload(Ctx* ctx);      // host scene arrays -> device pools (once per edit)
+int download(Ctx* ctx);    // device pools -> host scene arrays (particle order)
+int begin_edit(Ctx* ctx);  // download, then mark the device copy stale
 int run_explicit(Ctx* ctx, const zmpm_solver& s);      // symplectic substep up to G2P
 int launch_explicit_stress(Ctx* ctx);
 int run_phase_field(Ctx* ctx, int32_t* iterations, double* residual); // FractureSimulation::solvePhaseFieldSystem after P2G

@@ -462,6 +462,20 @@ class MpmSimulation:
         Fe = np.ascontiguousarray(Fe, dtype=np.float64).reshape(self.count, 3, 3)
         self._call("set_viscoelastic_strain", ptr(Fe))
 
+    # files (SimulationBase::write / read, writePartio)
+    def write(self, path):
+        """Restart file of the whole scene state (library format)."""
+        self._call("write_state", str(path).encode())
+
+    def read(self, path):
+        """Replaces the scene with a restart file written by `write`."""
+        self._call("read_state", str(path).encode())
+
+    def writePartio(self, path, velocity=False, phase_field=False):
+        """BGEO point file with "position" (+ "v", + "pf" / "sigmaC")."""
+        fields = (abi.BGEO_VELOCITY if velocity else 0) | (abi.BGEO_PHASE_FIELD if phase_field else 0)
+        self._call("write_bgeo", str(path).encode(), fields)
+
     def getLogJp(self):
         """log Jp of Drucker-Prager and Cam-Clay particles."""
         out = np.empty(self.count)
