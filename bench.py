@@ -70,7 +70,7 @@ def scene(n_boxes=4, seed_pos=1, seed_vel=2, seed_jit=0, velocity="particle"):
     return x, v
 
 
-def make_sim(x, v, precision, lib=None, model="hencky", layout="auto"):
+def make_sim(x, v, precision, lib=None, model="hencky", layout="auto", plastic="von_mises"):
     from ziran2019_b200 import abi, mpm
 
     sim = mpm.MpmSimulation(DX, gravity=(0, -9.8, 0), precision=precision, grid_log2=9, layout=layout,
@@ -79,7 +79,10 @@ def make_sim(x, v, precision, lib=None, model="hencky", layout="auto"):
     h = sim.addParticles(x, v, RHO * V0, V0)
     m = mpm.StvkWithHenckyIsotropic(E, NU) if model == "hencky" else mpm.NeoHookeanBorden(E, NU)
     h.addFBasedMpmForce(m)
-    h.addPlasticity(m, mpm.VonMisesStvkHencky(YIELD, 1e30, 0.0))
+    if plastic == "von_mises":
+        h.addPlasticity(m, mpm.VonMisesStvkHencky(YIELD, 1e30, 0.0))
+    elif plastic == "drucker_prager":
+        h.addPlasticity(m, mpm.DruckerPragerStvkHencky(30.0, 1.0, 0.0, True))
     mpm.add_all_walls_in_domain(sim, 1.0, 3 * DX, abi.STICKY)
     return sim
 
@@ -170,6 +173,60 @@ def wl_damage2m(precision, lib=None, layout="auto", scale=1):
         sim.addCollisionObject(box)
     return sim, 2e-4, x.shape[0], {"workload": "config3-rankine-notched-slab-2m", "model": "neo-Hookean + Rankine damage",
                                    "solver": "MINRES, Newton 3 x Krylov 20 (reference defaults)"}
+
+
+def wl_explicit1m(precision, lib=None, layout="auto", scale=1):
+    """The headline scene (four boxes of 250,000 particles, StvkWithHencky +
+    von Mises, sticky walls) advanced by the explicit symplectic substep
+    (symplectic = true, trial collision on) at dt = 1e-4 (the p-wave speed is
+    about 9.6 m/s at dx = 1/256).  scale > 1 keeps 4 // scale boxes (CPU samples)."""
+    x, v = scene(n_boxes=max(1, 4 // scale))
+    sim = make_sim(x, v, precision, lib=lib, layout=layout)
+    sim.useExplicit()
+    return sim, 1e-4, x.shape[0], {"workload": "explicit-elastoplastic-4boxes-1m", "model": "hencky+von Mises",
+                                   "solver": "explicit symplectic substep, trial collision"}
+
+
+def wl_sand1m(precision, lib=None, layout="auto", scale=1):
+    """The headline scene with Drucker-Prager sand plasticity (friction angle 30
+    degrees, beta 1, no cohesion, volume correction) instead of von Mises;
+    implicit substep with the reference solver defaults.  scale > 1 keeps
+    4 // scale boxes (CPU samples)."""
+    x, v = scene(n_boxes=max(1, 4 // scale))
+    sim = make_sim(x, v, precision, lib=lib, layout=layout, plastic="drucker_prager")
+    return sim, DT, x.shape[0], {"workload": "sand-drucker-prager-4boxes-1m", "model": "hencky+Drucker-Prager",
+                                 "solver": "MINRES, Newton 3 x Krylov 20 (reference defaults)"}
+
+
+def wl_phasefield2m(precision, lib=None, layout="auto", scale=1):
+    """The notched slab of damage2m (about 2.05M particles, ends pulled apart at
+    +-0.5 m/s, NeoHookeanBorden E = 1e5, nu = 0.3) with the CD-MPM phase field
+    instead of Rankine damage: l0 = dx / 2, sigma_c from 1% volumetric stretch,
+    parabolic_M = 1, lumped mass, CG tolerance 1e-6 and cap 100 (the fracture
+    project's settings).  scale > 1 keeps every scale-th cell layer in z."""
+    from ziran2019_b200 import abi, mpm
+    dx = 1.0 / 216
+    nx, ny, nz = 216, 54, max(1, 22 // scale)
+    lo = np.array([0.25, 0.5, 0.5])
+    x = _jitter_box((nx, ny, nz), dx, lo, 8, 4)
+    rel = (x - lo) / dx
+    notch = (np.abs(rel[:, 0] - nx / 2) < 0.5) & (rel[:, 1] < 0.1 / dx)
+    x = x[~notch]
+    sim = mpm.MpmSimulation(dx, gravity=(0, 0, 0), precision=precision, grid_log2=9, layout=layout, lib=lib)
+    V0 = dx ** 3 / 8
+    h = sim.addParticles(x, np.zeros_like(x), 1000.0 * V0, V0)
+    h.addFBasedMpmForceWithPhaseField(0.01, 0.5 * dx, mpm.NeoHookeanBorden(1e5, 0.3))
+    sim.setPhaseFieldSolver(parabolic_M=1.0, lumping=True)
+    hi = lo + np.array([nx, ny, nz]) * dx
+    grip = 3 * dx
+    for side, vel in ((0, -0.5), (1, 0.5)):
+        a = [lo[0] - 4 * dx if side == 0 else hi[0] - grip, lo[1] - 4 * dx, lo[2] - 4 * dx]
+        b = [lo[0] + grip if side == 0 else hi[0] + 4 * dx, hi[1] + 4 * dx, hi[2] + 4 * dx]
+        box = mpm.AnalyticCollisionObject(mpm.AxisAlignedAnalyticBox(a, b), abi.STICKY)
+        box.setTranslation((0.0, 0.0, 0.0), (vel, 0.0, 0.0))
+        sim.addCollisionObject(box)
+    return sim, 2e-4, x.shape[0], {"workload": "cdmpm-phase-field-notched-slab-2m", "model": "neo-Hookean + CD-MPM phase field",
+                                   "solver": "MINRES, Newton 3 x Krylov 20; phase-field CG 1e-6 x 100"}
 
 
 MIXED_ROLLOUT_TOL = 1e-7
@@ -273,7 +330,8 @@ def run_rollout(args, world, rank):
         print(json.dumps(line), flush=True)
 
 
-WORKLOADS = {"cube32k": wl_cube32k, "admm500k": wl_admm500k, "damage2m": wl_damage2m, "rollout256k": wl_rollout256k}
+WORKLOADS = {"cube32k": wl_cube32k, "admm500k": wl_admm500k, "damage2m": wl_damage2m, "rollout256k": wl_rollout256k,
+             "explicit1m": wl_explicit1m, "sand1m": wl_sand1m, "phasefield2m": wl_phasefield2m}
 
 
 def run_workload(args, world, rank):
@@ -301,7 +359,7 @@ def run_workload(args, world, rank):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         from oracle import zoracle
-        scale = {"cube32k": 1, "admm500k": 4, "damage2m": 11}[args.workload]
+        scale = {"cube32k": 1, "admm500k": 4, "damage2m": 11, "explicit1m": 4, "sand1m": 4, "phasefield2m": 11}[args.workload]
         osim, _, Pc, _ = fn("fp64", lib=zoracle.lib(), scale=scale)
         for _ in range(args.warmup):
             osim.advanceOneTimeStep(dt)
@@ -315,7 +373,8 @@ def run_workload(args, world, rank):
     if rank == 0:
         value = world * args.steps / (ms_mx / 1e3)
         fp64_value = world * args.steps / (ms64 / 1e3)
-        line = {"metric": f"implicit MPM substeps/sec, {meta['workload']}", "value": value, "unit": "substeps/s", "n_gpus": world,
+        kind = "explicit" if args.workload == "explicit1m" else "implicit"
+        line = {"metric": f"{kind} MPM substeps/sec, {meta['workload']}", "value": value, "unit": "substeps/s", "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_mx / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "mixed (fp32 operator, fp64 state)", "data": "synthetic",
                 "config": dict(meta, particles=P, dt=dt), "particles_substeps_per_s": value * P,
@@ -323,6 +382,7 @@ def run_workload(args, world, rank):
                 "rel_pos_err_vs_fp64": float(np.linalg.norm(xmx - x64) / np.linalg.norm(x64)),
                 "accuracy_steps": args.warmup + args.steps,
                 "iterations_per_step": [st_mx[-1]["newton_iterations"], st_mx[-1]["krylov_iterations"]],
+                "phase_field_cg_iterations": st_mx[-1].get("phase_field_iterations"),
                 "gpu_launches": sum(s["kernel_launches"] for s in st_mx), "cpu_baseline": cpu, "clocks": clk}
         print(json.dumps(line), flush=True)
     for s in sims.values():

@@ -10,8 +10,8 @@
 // 53-104, Jacobi preconditioner with the lumped diagonal) keeps its scalars on
 // the device; its reductions are per-CTA partials summed in a fixed order by a
 // one-CTA kernel, so the iteration is deterministic.  The host enqueues
-// iterations in batches and reads the "active" flag between batches; kernels
-// of iterations past convergence return at once.
+// iterations in batches (1, 4, then 16) and reads the "active" flag between
+// batches; kernels of iterations past convergence return at once.
 #include <algorithm>
 #include <cfloat>
 
@@ -103,7 +103,9 @@ __device__ __forceinline__ void pf_flush(const double* acc, const int32_t* nbr, 
 // phaseP2G + the right-hand side and preconditioner sums: per particle
 // vol = V0 det F, then sum_p w, sum_p c w (normalised phase field of the
 // parabolic form), sum_p vol w and the lumped diagonal sum_p vol pf_Fp w (or
-// vol (M pf_Fp + 1/dt) w).
+// vol (M pf_Fp + 1/dt) w).  Layered scatter (as P2G): a thread takes one cell
+// and every layers-th particle of it, sums the cell's 27 node contributions in
+// FP64 registers (two fields per pass) and adds them to the window once.
 template <class L>
 __global__ void __launch_bounds__(XF_THREADS) k_pf_p2g(const int32_t* __restrict__ group_start, const int32_t* __restrict__ group_nbr,
     double* __restrict__ pd, int64_t cap, const short4* __restrict__ base, double dx, PfParams p, double* __restrict__ pfn)
@@ -111,30 +113,64 @@ __global__ void __launch_bounds__(XF_THREADS) k_pf_p2g(const int32_t* __restrict
     constexpr int NPB = L::NPB;
     __shared__ double acc[8 * 4 * NPB];
     __shared__ int32_t nbr[8];
+    __shared__ CellLayout<L> cl;
     const int g = blockIdx.x;
     if (threadIdx.x < 8) nbr[threadIdx.x] = group_nbr[8 * g + threadIdx.x];
     zero_window<4, NPB>(acc);
-    __syncthreads();
-    const double inv_dx = 1.0 / dx;
     const int s0 = group_start[g], s1 = group_start[g + 1];
-    for (int s = s0 + threadIdx.x; s < s1; s += blockDim.x) {
-        double w[3][3], dwr[3][3];
-        int lx, ly, lz;
-        pf_weights<L>(pd, cap, s, base[s], inv_dx, w, dwr, lx, ly, lz);
-        M3<double> F;
+    build_cell_layout<L>(cl, base, s0, s1);
+    const double inv_dx = 1.0 / dx;
+    const int ce = threadIdx.x % NPB, layer = threadIdx.x / NPB, layers = blockDim.x / NPB;
+    const int cnt = cl.cnt[ce], first = s0 + cl.start[ce];
+    // pass 0: sum vol w and the diagonal (fields PN_VS, PN_DIAG); pass 1 (parabolic
+    // only): sum w and sum c w (fields PN_MULT, PN_PHASE)
+#pragma unroll 1
+    for (int pass = 0; pass < ((p.M > 0) ? 2 : 1); ++pass) {
+        double a[27][2];
 #pragma unroll
-        for (int q = 0; q < 9; ++q) F.a[q] = pd[(PD_F + q) * cap + s];
-        const double vol = pd[PD_VOL * cap + s] * m3_det(F);
-        pd[PD_PF_VOL * cap + s] = vol;
-        const double c = pd[PD_PF_C * cap + s], fp = pd[PD_PF_FP * cap + s];
-        const double dterm = (p.M > 0) ? vol * (p.M * fp + p.one_over_dt) : vol * fp;
-        for_stencil<L>(lx, ly, lz, w, dwr, inv_dx, [&](int t, int e, int, int, int, double wijk, const double*) {
-            double* a = acc + t * 4 * NPB + e;
-            atomicAdd(a, wijk);
-            atomicAdd(a + NPB, c * wijk);
-            atomicAdd(a + 2 * NPB, vol * wijk);
-            atomicAdd(a + 3 * NPB, dterm * wijk);
-        });
+        for (int m = 0; m < 27; ++m) a[m][0] = a[m][1] = 0.0;
+        int lx = 0, ly = 0, lz = 0;
+        for (int r = layer; r < cnt; r += layers) {
+            const int s = first + r;
+            double w[3][3], dwr[3][3];
+            pf_weights<L>(pd, cap, s, base[s], inv_dx, w, dwr, lx, ly, lz);
+            double v0, v1;
+            if (pass == 0) {
+                M3<double> F;
+#pragma unroll
+                for (int q = 0; q < 9; ++q) F.a[q] = pd[(PD_F + q) * cap + s];
+                const double vol = pd[PD_VOL * cap + s] * m3_det(F);
+                pd[PD_PF_VOL * cap + s] = vol;
+                const double fp = pd[PD_PF_FP * cap + s];
+                v0 = vol;
+                v1 = (p.M > 0) ? vol * (p.M * fp + p.one_over_dt) : vol * fp;
+            }
+            else {
+                v0 = 1.0;
+                v1 = pd[PD_PF_C * cap + s];
+            }
+            for_stencil<L>(lx, ly, lz, w, dwr, inv_dx, [&](int, int, int i, int j, int k, double wijk, const double*) {
+                const int m = 9 * i + 3 * j + k;
+                a[m][0] += v0 * wijk;
+                a[m][1] += v1 * wijk;
+            });
+        }
+        if (layer < cnt) {
+            const int cx = ce >> (L::YB + L::ZB), cy = (ce >> L::ZB) & (L::BY - 1), cz = ce & (L::BZ - 1);
+            const int f0 = (pass == 0) ? PN_VS : PN_MULT;
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+#pragma unroll
+                for (int j = 0; j < 3; ++j)
+#pragma unroll
+                    for (int k = 0; k < 3; ++k) {
+                        int e;
+                        const int t = win_slot<L>(cx + i, cy + j, cz + k, e);
+                        double* dst = acc + t * 4 * NPB + f0 * NPB + e;
+                        atomicAdd(dst, a[9 * i + 3 * j + k][0]);
+                        atomicAdd(dst + NPB, a[9 * i + 3 * j + k][1]);
+                    }
+        }
     }
     __syncthreads();
     pf_flush<4, NPB>(acc, nbr, pfn, PN_MULT);
@@ -143,8 +179,9 @@ __global__ void __launch_bounds__(XF_THREADS) k_pf_p2g(const int32_t* __restrict
 // The operator of the CG without its lumped mass (that is diag * x, added by
 // k_pf_sq): q_i = sum_p [c_p w_ip] + M' (4 l0^2 vol_p grad c_p) . grad w_ip,
 // grad c_p = sum_j s_j grad w_jp, c_p = vol pf_Fp sum_j s_j w_jp (consistent
-// mass, lumping off only), M' = parabolic_M or 1.
-template <class L>
+// mass, lumping off only), M' = parabolic_M or 1.  Gather from the staged
+// window, layered scatter as in k_pf_p2g.
+template <class L, bool LUMP>
 __global__ void __launch_bounds__(XF_THREADS) k_pf_apply(const int32_t* __restrict__ group_start, const int32_t* __restrict__ group_nbr,
     const double* __restrict__ pd, int64_t cap, const short4* __restrict__ base, double dx, PfParams p, double* __restrict__ pfn,
     const PfScalars* __restrict__ sc)
@@ -154,36 +191,56 @@ __global__ void __launch_bounds__(XF_THREADS) k_pf_apply(const int32_t* __restri
     __shared__ double win[8 * NPB];
     __shared__ double acc[8 * NPB];
     __shared__ int32_t nbr[8];
+    __shared__ CellLayout<L> cl;
     const int g = blockIdx.x;
     if (threadIdx.x < 8) nbr[threadIdx.x] = group_nbr[8 * g + threadIdx.x];
     zero_window<1, NPB>(acc);
-    __syncthreads();
+    const int s0 = group_start[g], s1 = group_start[g + 1];
+    build_cell_layout<L>(cl, base, s0, s1);
     pf_stage<NPB>(win, pfn, nbr, PN_S);
     __syncthreads();
     const double inv_dx = 1.0 / dx;
     const double mg = (p.M > 0) ? p.M : 1.0;
-    const int s0 = group_start[g], s1 = group_start[g + 1];
-    for (int s = s0 + threadIdx.x; s < s1; s += blockDim.x) {
+    const int ce = threadIdx.x % NPB, layer = threadIdx.x / NPB, layers = blockDim.x / NPB;
+    const int cnt = cl.cnt[ce], first = s0 + cl.start[ce];
+    double a[27];
+#pragma unroll
+    for (int m = 0; m < 27; ++m) a[m] = 0.0;
+    int lx = 0, ly = 0, lz = 0;
+    for (int r = layer; r < cnt; r += layers) {
+        const int s = first + r;
         double w[3][3], dwr[3][3];
-        int lx, ly, lz;
         pf_weights<L>(pd, cap, s, base[s], inv_dx, w, dwr, lx, ly, lz);
         double c0 = 0, g0[3] = { 0, 0, 0 };
         for_stencil<L>(lx, ly, lz, w, dwr, inv_dx, [&](int t, int e, int, int, int, double wijk, const double* dw) {
             const double xv = win[t * NPB + e];
-            c0 += xv * wijk;
+            if (!LUMP) c0 += xv * wijk;
 #pragma unroll
             for (int d = 0; d < 3; ++d) g0[d] += xv * dw[d];
         });
         const double vol = pd[PD_PF_VOL * cap + s], l0 = pd[PD_PF_L0 * cap + s];
-        c0 *= vol * pd[PD_PF_FP * cap + s];
+        if (!LUMP) c0 *= vol * pd[PD_PF_FP * cap + s];
         const double gs = vol * 4.0 * l0 * l0;
 #pragma unroll
         for (int d = 0; d < 3; ++d) g0[d] *= gs;
-        for_stencil<L>(lx, ly, lz, w, dwr, inv_dx, [&](int t, int e, int, int, int, double wijk, const double* dw) {
+        for_stencil<L>(lx, ly, lz, w, dwr, inv_dx, [&](int, int, int i, int j, int k, double wijk, const double* dw) {
             double v = (g0[0] * dw[0] + g0[1] * dw[1] + g0[2] * dw[2]) * mg;
-            if (!p.lumping) v += c0 * wijk;
-            atomicAdd(acc + t * NPB + e, v);
+            if (!LUMP) v += c0 * wijk;
+            a[9 * i + 3 * j + k] += v;
         });
+    }
+    if (layer < cnt) {
+        const int cx = ce >> (L::YB + L::ZB), cy = (ce >> L::ZB) & (L::BY - 1), cz = ce & (L::BZ - 1);
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 3; ++j)
+#pragma unroll
+                for (int k = 0; k < 3; ++k) {
+                    int e;
+                    const int t = win_slot<L>(cx + i, cy + j, cz + k, e);
+                    atomicAdd(acc + t * NPB + e, a[9 * i + 3 * j + k]);
+                }
     }
     __syncthreads();
     pf_flush<1, NPB>(acc, nbr, pfn, PN_Q);
@@ -457,10 +514,15 @@ static int phase_field_impl(Ctx* ctx, int32_t* iterations, double* residual)
     PfScalars hs{};
     const int total = p.max_it + 1;
     for (int k = 0; k < total;) {
-        const int batch = std::min(k == 0 ? 4 : 16, total - k);
+        // the reference's default tolerance usually stops the CG after its first
+        // iteration: check after 1, then after 4 more, then every 16
+        const int batch = std::min(k == 0 ? 1 : (k == 1 ? 4 : 16), total - k);
         for (int j = 0; j < batch; ++j) {
             k_pf_dir<NPB><<<nb, ND_THREADS, 0, st>>>(nn, gm, pfn, sc);
-            k_pf_apply<L><<<(unsigned)G, XF_THREADS, 0, st>>>(gs, gn, pd, ctx->Pcap, base, dx, p, pfn, sc);
+            if (p.lumping)
+                k_pf_apply<L, true><<<(unsigned)G, XF_THREADS, 0, st>>>(gs, gn, pd, ctx->Pcap, base, dx, p, pfn, sc);
+            else
+                k_pf_apply<L, false><<<(unsigned)G, XF_THREADS, 0, st>>>(gs, gn, pd, ctx->Pcap, base, dx, p, pfn, sc);
             k_pf_sq<NPB><<<nb, ND_THREADS, 0, st>>>(nn, gm, pfn, p.lumping, pA, sc);
             k_pf_alpha<<<1, ND_THREADS, 0, st>>>(pA, nb, sc);
             k_pf_update<NPB><<<nb, ND_THREADS, 0, st>>>(nn, gm, pfn, pA, pB, sc);
