@@ -344,7 +344,7 @@ def run_workload(args, world, rank):
     fn = WORKLOADS[args.workload]
     sims, meta = {}, None
     for p in ("fp64", "mixed"):
-        sims[p], dt, P, meta = fn(p, layout="444")
+        sims[p], dt, P, meta = fn(p, layout="444", scale=args.scale)
     for p in sims:
         for _ in range(args.warmup):
             rc = sims[p].advanceOneTimeStep(dt)
@@ -531,6 +531,8 @@ def main():
     ap.add_argument("--boxes", type=int, default=4, help="boxes of 250k particles (profiling runs use fewer)")
     ap.add_argument("--fp64-layout", default="444", choices=["444", "auto"],
                     help="page layout of the FP64 substep: 444 = same as the mixed run (only precision differs)")
+    ap.add_argument("--scale", type=int, default=1,
+                    help="secondary workloads: the cut used for CPU samples, on the GPU too (profiling runs)")
     ap.add_argument("--workload", default="config1", choices=["config1"] + sorted(WORKLOADS),
                     help="config1: the headline 1M-particle workload; others print their own line")
     ap.add_argument("--fd-directions", type=int, default=4, help="finite-difference directions of the rollout gradient check")
