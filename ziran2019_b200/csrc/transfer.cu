@@ -25,7 +25,7 @@ namespace zmpm {
 // (particle, node, component).  APIC P2G: m_i += w m_p, (mv)_i += w m_p (v_p +
 // C_p (x_i - x_p)) in FP64.
 template <class L, class TH, int NCP>
-__global__ void __launch_bounds__(XF_THREADS) k_p2g_reg(const int32_t* __restrict__ group_start, const int32_t* __restrict__ group_nbr,
+__global__ void __launch_bounds__(XF_THREADS, 3) k_p2g_reg(const int32_t* __restrict__ group_start, const int32_t* __restrict__ group_nbr,
     const double* __restrict__ pd, int64_t cap, const short4* __restrict__ base, double dx, double* __restrict__ gm, double* __restrict__ gmv,
     TH* __restrict__ frac)
 {
@@ -561,8 +561,11 @@ __global__ void __launch_bounds__(XF_THREADS) k_hvp_scatter(const int32_t* __res
 }
 
 // ------------------------------------------------------------------ G2P ----
+// Three CTAs per SM (at most 168 registers): G2P and P2G are latency bound on
+// FP64 chains, and the third CTA outweighs the few spilled registers (about
+// 1.5% of the 1M-particle substep, same-box A/B).
 template <class L>
-__global__ void __launch_bounds__(XF_THREADS) k_g2p(const int32_t* __restrict__ group_start, const int32_t* __restrict__ group_nbr,
+__global__ void __launch_bounds__(XF_THREADS, 3) k_g2p(const int32_t* __restrict__ group_start, const int32_t* __restrict__ group_nbr,
     double* __restrict__ pd, int32_t* __restrict__ pi, int64_t cap, const short4* __restrict__ base, double dx, double dt,
     double apic_rpic_ratio, const double* __restrict__ vnew, int32_t* __restrict__ flags, int mls)
 {
