@@ -133,3 +133,44 @@ def test_bgeo_output(cuda_lib, tmp_path):
     pf = s.getPhaseField()
     np.testing.assert_array_equal(g["pf"][:, 0], pf["c"].astype(np.float32))
     assert np.all(g["sigmaC"] > 0)
+
+
+def test_restart_carries_admm_and_viscoelastic_state(cuda_lib, tmp_path):
+    """ADMM multipliers, weights, last dv and the viscoelastic Fe travel in the
+    restart file: the restarted ADMM run ends where the uninterrupted one ends."""
+    def admm_scene():
+        s = mpm.MpmSimulation(DX, gravity=(0, -9.8, 0), grid_log2=8)
+        h, x = build_scene(s, kind="hencky", n=6, dx=DX, seed=5, ground=0.1)
+        E, nu = 1e4, 0.3
+        nv = 2 * E / (2 * (1 + nu)) * 0.05
+        h.addFElasticNonequilibratedBasedMpmForce(mpm.StvkWithHencky(E, nu), nv, nv)
+        s.useAdmm(admm_max_iterations=10, rho_scale=0.8, global_tolerance=1e-12)
+        return s
+    a = admm_scene()
+    run(a, 2, 2e-3)
+    path = tmp_path / "admm.dat"
+    a.write(path)
+    run(a, 3, 2e-3)
+    b = admm_scene()
+    b.read(path)
+    run(b, 3, 2e-3)
+    pa, pb = a.getParticles(), b.getParticles()
+    for k, tol in (("X", 1e-10), ("F", 1e-8), ("V", 1e-6)):
+        assert np.abs(pb[k] - pa[k]).max() <= tol * np.abs(pa[k]).max(), k
+    np.testing.assert_allclose(b.getViscoelasticStrain(), a.getViscoelasticStrain(), rtol=0, atol=1e-10)
+
+
+def test_restart_explicit_run_is_reproduced(cuda_lib, tmp_path):
+    a = scene()
+    a.useExplicit()
+    run(a, 5, 2e-4)
+    path = tmp_path / "ex.dat"
+    a.write(path)
+    run(a, 5, 2e-4)
+    b = scene()
+    b.useExplicit()
+    b.read(path)
+    run(b, 5, 2e-4)
+    pa, pb = a.getParticles(), b.getParticles()
+    for k in ("X", "V", "F", "C"):
+        assert np.abs(pb[k] - pa[k]).max() <= 1e-12 * max(np.abs(pa[k]).max(), 1.0), k
