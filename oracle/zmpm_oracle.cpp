@@ -1142,6 +1142,67 @@ static bool vmProjectSigma(T mu, T ys, const T s[3], T out[3], T D[3][3])
     return true;
 }
 
+// DruckerPragerStvkHencky::projectSigma, PlasticityApplier.cpp:319-347 (no
+// log Jp: the ADMM local step's view of the return map).
+template <class T>
+static void dpProjectSigma(T mu, T lambda, T alpha, T cohesion, const T s[3], T out[3])
+{
+    T eps[3];
+    for (int d = 0; d < 3; ++d) eps[d] = std::log(std::max(std::abs(s[d]), T(1e-4))) - cohesion;
+    const T tr = eps[0] + eps[1] + eps[2];
+    T hat[3];
+    for (int d = 0; d < 3; ++d) hat[d] = eps[d] - (tr / T(3)) * T(1);
+    if (tr >= 0) {
+        for (int d = 0; d < 3; ++d) out[d] = std::exp(cohesion) * T(1);
+        return;
+    }
+    const T hn = std::sqrt(hat[0] * hat[0] + hat[1] * hat[1] + hat[2] * hat[2]);
+    const T dg = hn + (T(3) * lambda + T(2) * mu) / (T(2) * mu) * tr * alpha;
+    for (int d = 0; d < 3; ++d) out[d] = std::exp((dg <= 0) ? eps[d] + cohesion : eps[d] - (dg / hn) * hat[d] + cohesion);
+}
+
+// DruckerPragerStvkHencky::projectSigmaAndDerivative, PlasticityApplier.cpp:387-423.
+template <class T>
+static void dpProjectSigmaDerivative(T mu, T lambda, T alpha, T cohesion, const T s[3], T out[3], T D[3][3])
+{
+    T eps[3];
+    for (int d = 0; d < 3; ++d) eps[d] = std::log(std::max(std::abs(s[d]), T(1e-4))) - cohesion;
+    const T tr = eps[0] + eps[1] + eps[2];
+    T hat[3];
+    for (int d = 0; d < 3; ++d) hat[d] = eps[d] - (tr / T(3)) * T(1);
+    const T hn = std::sqrt(hat[0] * hat[0] + hat[1] * hat[1] + hat[2] * hat[2]);
+    const T dg = hn + (T(3) * lambda + T(2) * mu) / (T(2) * mu) * tr * alpha;
+    if (dg <= 0) { // inside the yield surface
+        for (int r = 0; r < 3; ++r) {
+            out[r] = std::exp(eps[r] + cohesion);
+            for (int c = 0; c < 3; ++c) D[r][c] = r == c ? T(1) : T(0);
+        }
+        return;
+    }
+    if (tr > 0 || hn == 0) { // the tip
+        for (int r = 0; r < 3; ++r) {
+            out[r] = std::exp(cohesion) * T(1);
+            for (int c = 0; c < 3; ++c) D[r][c] = T(0);
+        }
+        return;
+    }
+    T w[3], sv[3], sh[3];
+    for (int d = 0; d < 3; ++d) {
+        w[d] = T(1) / s[d];
+        sv[d] = eps[d] - tr / T(3) * T(1);
+    }
+    const T sn = std::sqrt(sv[0] * sv[0] + sv[1] * sv[1] + sv[2] * sv[2]);
+    for (int d = 0; d < 3; ++d) sh[d] = sv[d] / sn;
+    const T pp = alpha * tr * (T(3) * lambda + T(2) * mu) / (T(2) * mu * sn);
+    for (int d = 0; d < 3; ++d) out[d] = std::exp(eps[d] - (dg / hn) * hat[d] + cohesion);
+    for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c) {
+            const T m1 = ((T(1) + T(2) * pp) / T(3) * T(1) - pp / tr * eps[r]) * w[c];
+            const T m2 = pp * ((r == c ? T(1) : T(0)) - sh[r] * sh[c]) * w[c];
+            D[r][c] = out[r] * (m1 - m2);
+        }
+}
+
 // The viscous map in singular-value space and its derivative,
 // AdmmSimulationFoam.h:583-595.
 template <class T>
@@ -1171,10 +1232,11 @@ static M3<T> inverse3(const M3<T>& A)
 // One strain of AdmmSimulation::FStepSolve (AdmmSimulationFoam.h:507-615):
 // SVD of the target FDb, then a Newton solve in singular values for
 // argmin vol psi(P(z)) + coeff/2 |z - sigma|^2 starting from the current F.
-// mode 0: elastic, 1: von Mises projection, 2: viscous map.
+// mode 0: elastic, 1: von Mises projection, 2: viscous map, 3: Drucker-Prager
+// projection (alpha = ys, cohesion).
 template <class T>
 static M3<T> admmLocalSolve(const M3<T>& FDb, const M3<T>& Fcur, T vol, T coeff, T mu, T lambda, int mode, T ys, const Visco<T>& vis,
-    T dt, int iters, T tol)
+    T dt, int iters, T tol, T cohesion = T(0))
 {
     M3<T> U, V;
     T sigma[3];
@@ -1185,6 +1247,8 @@ static M3<T> admmLocalSolve(const M3<T>& FDb, const M3<T>& Fcur, T vol, T coeff,
         T zp[3], D[3][3];
         if (mode == 1)
             vmProjectSigma(mu, ys, zi, zp, D);
+        else if (mode == 3)
+            dpProjectSigmaDerivative(mu, lambda, ys, cohesion, zi, zp, D);
         else if (mode == 2)
             viscousSigma(vis, dt, zi, zp, D);
         else
@@ -1214,7 +1278,7 @@ static M3<T> admmLocalSolve(const M3<T>& FDb, const M3<T>& Fcur, T vol, T coeff,
 // initOmega for one strain, AdmmSimulationFoam.h:236-270:
 // omega = sqrt(vol sqrt(|makePD(d2E)|^2 + sum_ij |makePD2D(B_ij)|^2)).
 template <class T>
-static T admmOmega(const M3<T>& Fa, T vol, T mu, T lambda, bool vm, T ys)
+static T admmOmega(const M3<T>& Fa, T vol, T mu, T lambda, bool vm, T ys, bool dp = false, T alpha = T(0), T cohesion = T(0))
 {
     M3<T> U, V;
     T sigma[3];
@@ -1228,6 +1292,11 @@ static T admmOmega(const M3<T>& Fa, T vol, T mu, T lambda, bool vm, T ys)
     if (vm) {
         T sp[3], D[3][3];
         vmProjectSigma(mu, ys, sigma, sp, D);
+        for (int d = 0; d < 3; ++d) sigma[d] = sp[d];
+    }
+    else if (dp) {
+        T sp[3];
+        dpProjectSigma(mu, lambda, alpha, cohesion, sigma, sp);
         for (int d = 0; d < 3; ++d) sigma[d] = sp[d];
     }
     const int pairs[3][2] = { { 0, 1 }, { 0, 2 }, { 1, 2 } };
@@ -2411,8 +2480,9 @@ struct Sim {
             // initOmega (:222-274) and the rescaled dual variables (:355-371)
             if (!isHencky(i)) continue;
             T om0 = admm_omega[2 * i], om1 = admm_omega[2 * i + 1];
-            bool vm = plastic[i].kind == ZMPM_PLASTIC_VON_MISES;
-            admm_omega[2 * i] = admmOmega(admm_F[0][i], vol[i], model[i].mu, model[i].lambda, vm, plastic[i].yield_stress);
+            bool vm = plastic[i].kind == ZMPM_PLASTIC_VON_MISES, dp = plastic[i].kind == ZMPM_PLASTIC_DRUCKER_PRAGER;
+            admm_omega[2 * i] = admmOmega(admm_F[0][i], vol[i], model[i].mu, model[i].lambda, vm, plastic[i].yield_stress, dp, plastic[i].a,
+                plastic[i].cx);
             if (visco[i].on) admm_omega[2 * i + 1] = admmOmega(admm_F[1][i], vol[i], visco[i].mu, visco[i].lambda, false, T(0));
             for (int q = 0; q < 9; ++q) {
                 admm_y[18 * i + q] = admm_y[18 * i + q] * om0 / admm_omega[2 * i];
@@ -2491,9 +2561,10 @@ struct Sim {
                     for (int c = 0; c < 3; ++c) FDb.a[r][c] = (Sn.a[r][c] + (-y.a[r][c] / (om * rho))) + dt * t.a[r][c];
                 T coeff = rho * om * om;
                 if (k == 0) {
-                    int mode = plastic[i].kind == ZMPM_PLASTIC_VON_MISES ? 1 : 0;
+                    const bool dp = plastic[i].kind == ZMPM_PLASTIC_DRUCKER_PRAGER;
+                    int mode = plastic[i].kind == ZMPM_PLASTIC_VON_MISES ? 1 : (dp ? 3 : 0);
                     admm_F[0][i] = admmLocalSolve(FDb, admm_F[0][i], vol[i], coeff, model[i].mu, model[i].lambda, mode,
-                        plastic[i].yield_stress, visco[i], dt, 5, local_tol);
+                        dp ? plastic[i].a : plastic[i].yield_stress, visco[i], dt, 5, local_tol, dp ? plastic[i].cx : T(0));
                 }
                 else
                     admm_F[1][i] = admmLocalSolve(FDb, admm_F[1][i], vol[i], coeff, visco[i].mu, visco[i].lambda, 2, T(0), visco[i], dt, 20,
@@ -3003,8 +3074,8 @@ struct Sim {
         pf_res = 0;
         if (s.integrator == ZMPM_ADMM)
             for (int64_t i = 0; i < P; ++i)
-                if (plastic[i].kind == ZMPM_PLASTIC_DRUCKER_PRAGER || plastic[i].kind == ZMPM_PLASTIC_CAM_CLAY) {
-                    err = "the ADMM local step has no Drucker-Prager or Cam-Clay projection here";
+                if (plastic[i].kind == ZMPM_PLASTIC_CAM_CLAY) {
+                    err = "the ADMM F-step has no Cam-Clay projection (AdmmSimulationFoam.h:617-633 lists none)";
                     return ZMPM_UNSUPPORTED;
                 }
         if (anyPhaseField()) {
@@ -3319,6 +3390,22 @@ int zoracle_plastic_project(int32_t kind, double mu, double lambda, double kappa
         return ZMPM_BAD_ARG;
     for (int i = 0; i < 9; ++i) F[i] = Fm.a[i / 3][i % 3];
     *logJp = p.logJp;
+    return ZMPM_OK;
+}
+
+// Drucker-Prager in singular values for known-answer tests: projectSigma
+// (D = NULL) or projectSigmaAndDerivative.
+int zoracle_dp_project_sigma(double mu, double lambda, double alpha, double cohesion, const double* s, double* out, double* D)
+{
+    if (!s || !out) return ZMPM_BAD_ARG;
+    if (!D) {
+        zo::dpProjectSigma(mu, lambda, alpha, cohesion, s, out);
+        return ZMPM_OK;
+    }
+    double Dm[3][3];
+    zo::dpProjectSigmaDerivative(mu, lambda, alpha, cohesion, s, out, Dm);
+    for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c) D[3 * r + c] = Dm[r][c];
     return ZMPM_OK;
 }
 

@@ -37,6 +37,9 @@ def lib():
         d.zoracle_plastic_project.restype = C.c_int
         d.zoracle_plastic_project.argtypes = [C.c_int32, C.c_double, C.c_double, C.c_double, abi.c_double_p, C.c_int32,
                                               abi.c_double_p, abi.c_double_p]
+        d.zoracle_dp_project_sigma.restype = C.c_int
+        d.zoracle_dp_project_sigma.argtypes = [C.c_double, C.c_double, C.c_double, C.c_double, abi.c_double_p, abi.c_double_p,
+                                               abi.c_double_p]
         d.zoracle_linear_offset.restype = C.c_uint64
         d.zoracle_linear_offset.argtypes = [C.c_int32, C.c_int32, C.c_int32, C.c_int32]
         d.zoracle_packed_add.restype = C.c_uint64

@@ -65,8 +65,27 @@ def test_plasticity_mixed_tracks_fp64_oracle(cuda_lib, oracle, kind):
     np.testing.assert_allclose(sims[0].getLogJp(), sims[1].getLogJp(), rtol=0, atol=1e-4)
 
 
-def test_admm_refuses_sand_and_clay(cuda_lib):
+def test_admm_refuses_clay(cuda_lib):
+    """The ADMM F-step handles elastic, von Mises and Drucker-Prager particles
+    (AdmmSimulationFoam.h:617-633); Cam-Clay is refused."""
     import ctypes as C
-    s = scene(None, "dp")
+    s = scene(None, "cc")
     s.useAdmm(admm_max_iterations=4)
     assert s.lib.substep(s.ctx, 1e-3, C.byref(s.solver()), None) == abi.UNSUPPORTED
+
+
+def test_admm_sand_matches_oracle_fp64(cuda_lib, oracle):
+    """ADMM substeps of Drucker-Prager sand (StvkWithHencky + DruckerPragerStvkHencky
+    F-step with projectSigmaAndDerivative, initOmega with projectSigma)."""
+    sims = [scene(None, "dp"), scene(oracle, "dp")]
+    for s in sims:
+        s.useAdmm(admm_max_iterations=10, rho_scale=0.8, global_tolerance=1e-12)
+    for _ in range(4):
+        for k, s in enumerate(sims):
+            rc = s.advanceOneTimeStep(1e-3)
+            assert rc == abi.OK, (k, rc, s.last_stats)
+    pg, po = sims[0].getParticles(), sims[1].getParticles()
+    assert rel(pg["X"], po["X"]) < 1e-10
+    assert rel(pg["V"], po["V"]) < 1e-6
+    assert rel(pg["F"], po["F"]) < 1e-8
+    np.testing.assert_allclose(sims[0].getLogJp(), sims[1].getLogJp(), rtol=1e-7, atol=1e-10)

@@ -565,3 +565,71 @@ def test_sand_and_clay_substeps(oracle, kind):
         assert s.advanceOneTimeStep(1e-3) == abi.OK
     lj = s.getLogJp()
     assert np.all(np.isfinite(lj)) and np.abs(lj).max() > 0
+
+
+def _dp_sigma_numpy(mu, lam, alpha, cohesion, s):
+    """DruckerPragerStvkHencky::projectSigma restated (no log Jp)."""
+    eps = np.log(np.maximum(np.abs(s), 1e-4)) - cohesion
+    tr = eps.sum()
+    hat = eps - tr / 3
+    if tr >= 0:
+        return np.exp(cohesion) * np.ones(3)
+    hn = np.linalg.norm(hat)
+    dg = hn + (3 * lam + 2 * mu) / (2 * mu) * tr * alpha
+    return np.exp(eps + cohesion) if dg <= 0 else np.exp(eps - dg / hn * hat + cohesion)
+
+
+def test_admm_drucker_prager_sigma_maps(oracle):
+    """The Drucker-Prager maps of the ADMM local step: projectSigma against a
+    numpy restatement, projectSigmaAndDerivative's Jacobian against central
+    differences of its own projection inside each branch (cone, inside, tip)."""
+    d = oracle.dll
+    E, nu = 1e4, 0.3
+    mu, lam = E / (2 * (1 + nu)), E * nu / ((1 + nu) * (1 - 2 * nu))
+    sphi = np.sin(30 / 180 * 3.141592653)
+    alpha = np.sqrt(2 / 3) * 2 * sphi / (3 - sphi)
+    rng = np.random.default_rng(21)
+    seen = set()
+    for _ in range(300):
+        cohesion = rng.choice([0.0, 0.01])
+        s = rng.choice([0.9, 0.97, 1.0, 1.05]) * np.exp(rng.normal(0, 0.08, 3))
+        out = np.zeros(3)
+        assert d.zoracle_dp_project_sigma(mu, lam, alpha, cohesion, P(s), P(out), None) == 0
+        np.testing.assert_allclose(out, _dp_sigma_numpy(mu, lam, alpha, cohesion, s), rtol=1e-13, atol=0)
+        D = np.zeros(9)
+        o2 = np.zeros(3)
+        assert d.zoracle_dp_project_sigma(mu, lam, alpha, cohesion, P(s), P(o2), P(D)) == 0
+        h = 1e-6
+        J = np.zeros((3, 3))
+        for c in range(3):
+            sp, sm = s.copy(), s.copy()
+            sp[c] += h
+            sm[c] -= h
+            op, om = np.zeros(3), np.zeros(3)
+            d.zoracle_dp_project_sigma(mu, lam, alpha, cohesion, P(sp), P(op), P(np.zeros(9)))
+            d.zoracle_dp_project_sigma(mu, lam, alpha, cohesion, P(sm), P(om), P(np.zeros(9)))
+            J[:, c] = (op - om) / (2 * h)
+        branch = "tip" if not D.any() else ("inside" if np.allclose(D.reshape(3, 3), np.eye(3)) else "cone")
+        seen.add(branch)
+        np.testing.assert_allclose(D.reshape(3, 3), J, rtol=1e-5, atol=1e-6)
+    assert seen == {"tip", "inside", "cone"}
+
+
+def test_admm_sand_substeps(oracle):
+    """ADMM with Drucker-Prager sand (AdmmSimulationFoam's StvkWithHencky +
+    DruckerPragerStvkHencky F-step): substeps are clean and log Jp evolves;
+    Cam-Clay stays refused under ADMM."""
+    dx = 1.0 / 64
+    s = mpm.MpmSimulation(dx, gravity=(0, -9.8, 0), precision="fp64", lib=oracle)
+    h, x = build_scene(s, kind="hencky", n=6, dx=dx, v0=(0, -2.0, 0), lo=(0.375, 8 * dx, 0.375), ground=7 * dx)
+    s.setParticles(F=np.tile(np.diag([1.04, 1.0, 1.02]), (len(x), 1, 1)))
+    h.addPlasticity(None, mpm.DruckerPragerStvkHencky(30.0, 1.0, 0.0, True))
+    s.useAdmm(admm_max_iterations=10, rho_scale=0.8, global_tolerance=1e-10)
+    for _ in range(4):
+        assert s.advanceOneTimeStep(1e-3) == abi.OK
+    assert np.all(np.isfinite(s.getParticles()["X"])) and np.abs(s.getLogJp()).max() > 0
+    s2 = mpm.MpmSimulation(dx, gravity=(0, -9.8, 0), precision="fp64", lib=oracle)
+    h2, _ = build_scene(s2, kind="nh", n=4, dx=dx)
+    h2.addPlasticity(None, mpm.NonAssociativeCamClay(-0.01, 45.0, 0.3, 3.0, True))
+    s2.useAdmm(admm_max_iterations=4)
+    assert s2.lib.substep(s2.ctx, 1e-3, C.byref(s2.solver()), None) == abi.UNSUPPORTED

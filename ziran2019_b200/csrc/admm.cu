@@ -154,10 +154,12 @@ __global__ void __launch_bounds__(XF_THREADS) k_admm_init(const int32_t* __restr
         double om0 = pd[(PD_OMEGA + 0) * cap + s], om1 = pd[(PD_OMEGA + 1) * cap + s];
         if (pi[PI_KIND * cap + s] == ZMPM_MODEL_STVK_HENCKY_ISOTROPIC) {
             const double vol = pd[PD_VOL * cap + s];
-            const bool vm = pi[PI_PKIND * cap + s] == ZMPM_PLASTIC_VON_MISES;
-            const double n0 = admm_omega<double>(Fa0, vol, pd[PD_MU * cap + s], pd[PD_LAM * cap + s], vm, pd[PD_YS * cap + s]);
+            const int pkind = pi[PI_PKIND * cap + s];
+            // Drucker-Prager: PD_YS = alpha, PD_FS = cohesion
+            const double n0 = admm_omega<double>(Fa0, vol, pd[PD_MU * cap + s], pd[PD_LAM * cap + s], pkind, pd[PD_YS * cap + s],
+                pd[PD_YS * cap + s], pd[PD_FS * cap + s]);
             double n1 = om1;
-            if (visco) n1 = admm_omega<double>(load9(aF, cap, 9, s), vol, pd[PD_VMU * cap + s], pd[PD_VLAM * cap + s], false, 0.0);
+            if (visco) n1 = admm_omega<double>(load9(aF, cap, 9, s), vol, pd[PD_VMU * cap + s], pd[PD_VLAM * cap + s], ZMPM_PLASTIC_NONE, 0.0);
 #pragma unroll
             for (int q = 0; q < 9; ++q) {
                 pd[(PD_Y + q) * cap + s] = pd[(PD_Y + q) * cap + s] * om0 / n0;
@@ -256,12 +258,13 @@ __global__ void __launch_bounds__(XF_THREADS) k_admm_local(const int32_t* __rest
                 AdmmStrainParams p;
                 int mode, iters;
                 if (k == 0) {
-                    p = { pd[PD_MU * cap + s], pd[PD_LAM * cap + s], pd[PD_YS * cap + s], 1.0, 1.0 };
-                    mode = pi[PI_PKIND * cap + s] == ZMPM_PLASTIC_VON_MISES ? ADMM_VON_MISES : ADMM_ELASTIC;
+                    p = { pd[PD_MU * cap + s], pd[PD_LAM * cap + s], pd[PD_YS * cap + s], 1.0, 1.0, pd[PD_YS * cap + s], pd[PD_FS * cap + s] };
+                    const int pk = pi[PI_PKIND * cap + s];
+                    mode = pk == ZMPM_PLASTIC_VON_MISES ? ADMM_VON_MISES : (pk == ZMPM_PLASTIC_DRUCKER_PRAGER ? ADMM_DRUCKER_PRAGER : ADMM_ELASTIC);
                     iters = 5;
                 }
                 else {
-                    p = { pd[PD_VMU * cap + s], pd[PD_VLAM * cap + s], 0.0, pd[PD_VD * cap + s], pd[PD_VV * cap + s] };
+                    p = { pd[PD_VMU * cap + s], pd[PD_VLAM * cap + s], 0.0, pd[PD_VD * cap + s], pd[PD_VV * cap + s], 0.0, 0.0 };
                     mode = ADMM_VISCOUS;
                     iters = 20;
                 }

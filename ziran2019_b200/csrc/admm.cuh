@@ -182,6 +182,91 @@ ZMPM_HD void vm_project_sigma(T mu, T ys, const T s[3], T out[3], T D[3][3])
         }
 }
 
+// DruckerPragerStvkHencky::projectSigma (PlasticityApplier.cpp:319-347): the
+// return map in singular values without log Jp, as initOmega uses it.
+template <class T>
+ZMPM_HD void dp_project_sigma(T mu, T lambda, T alpha, T cohesion, const T s[3], T out[3])
+{
+    T eps[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        const T a = fabs(s[d]);
+        eps[d] = log(a > T(1e-4) ? a : T(1e-4)) - cohesion;
+    }
+    const T tr = eps[0] + eps[1] + eps[2];
+    T hat[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) hat[d] = eps[d] - (tr / T(3)) * T(1);
+    if (tr >= T(0)) {
+#pragma unroll
+        for (int d = 0; d < 3; ++d) out[d] = exp(cohesion) * T(1);
+        return;
+    }
+    const T hn = sqrt(hat[0] * hat[0] + hat[1] * hat[1] + hat[2] * hat[2]);
+    const T dg = hn + (T(3) * lambda + T(2) * mu) / (T(2) * mu) * tr * alpha;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) out[d] = exp((dg <= T(0)) ? eps[d] + cohesion : eps[d] - (dg / hn) * hat[d] + cohesion);
+}
+
+// DruckerPragerStvkHencky::projectSigmaAndDerivative (PlasticityApplier.cpp:
+// 387-423), the F-step's projection: inside (identity), tip (zero derivative)
+// or cone, D = diag(out) (((1 + 2p)/3 - p eps / k) w^T - p (I - s s^T) diag(w)).
+template <class T>
+ZMPM_HD void dp_project_sigma_derivative(T mu, T lambda, T alpha, T cohesion, const T s[3], T out[3], T D[3][3])
+{
+    T eps[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        const T a = fabs(s[d]);
+        eps[d] = log(a > T(1e-4) ? a : T(1e-4)) - cohesion;
+    }
+    const T tr = eps[0] + eps[1] + eps[2];
+    T hat[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) hat[d] = eps[d] - (tr / T(3)) * T(1);
+    const T hn = sqrt(hat[0] * hat[0] + hat[1] * hat[1] + hat[2] * hat[2]);
+    const T dg = hn + (T(3) * lambda + T(2) * mu) / (T(2) * mu) * tr * alpha;
+    if (dg <= T(0)) {
+#pragma unroll
+        for (int r = 0; r < 3; ++r) {
+            out[r] = exp(eps[r] + cohesion);
+#pragma unroll
+            for (int c = 0; c < 3; ++c) D[r][c] = r == c ? T(1) : T(0);
+        }
+        return;
+    }
+    if (tr > T(0) || hn == T(0)) {
+#pragma unroll
+        for (int r = 0; r < 3; ++r) {
+            out[r] = exp(cohesion) * T(1);
+#pragma unroll
+            for (int c = 0; c < 3; ++c) D[r][c] = T(0);
+        }
+        return;
+    }
+    T w[3], sv[3], sh[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        w[d] = T(1) / s[d];
+        sv[d] = eps[d] - tr / T(3) * T(1);
+    }
+    const T sn = sqrt(sv[0] * sv[0] + sv[1] * sv[1] + sv[2] * sv[2]);
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        sh[d] = sv[d] / sn;
+        out[d] = exp(eps[d] - (dg / hn) * hat[d] + cohesion);
+    }
+    const T pp = alpha * tr * (T(3) * lambda + T(2) * mu) / (T(2) * mu * sn);
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            const T m1 = ((T(1) + T(2) * pp) / T(3) * T(1) - pp / tr * eps[r]) * w[c];
+            const T m2 = pp * ((r == c ? T(1) : T(0)) - sh[r] * sh[c]) * w[c];
+            D[r][c] = out[r] * (m1 - m2);
+        }
+}
+
 // The viscous map in singular values and its derivative, AdmmSimulationFoam.h:583-595.
 template <class T>
 ZMPM_HD void viscous_sigma(T mu, T lambda, T vd, T vv, T dt, const T zi[3], T zp[3], T D[3][3])
@@ -200,10 +285,11 @@ ZMPM_HD void viscous_sigma(T mu, T lambda, T vd, T vv, T dt, const T zi[3], T zp
         for (int c = 0; c < 3; ++c) D[r][c] = zp[r] * a * ((r == c ? T(1) / zi[c] : T(0)) - b * (T(1) / zi[c]));
 }
 
-enum AdmmLocalMode { ADMM_ELASTIC = 0, ADMM_VON_MISES = 1, ADMM_VISCOUS = 2 };
+enum AdmmLocalMode { ADMM_ELASTIC = 0, ADMM_VON_MISES = 1, ADMM_VISCOUS = 2, ADMM_DRUCKER_PRAGER = 3 };
 
 struct AdmmStrainParams {
     double mu, lambda, ys, vd, vv;
+    double alpha, cohesion; // Drucker-Prager
 };
 
 // One strain of AdmmSimulation::FStepSolve (AdmmSimulationFoam.h:507-615): SVD of
@@ -223,6 +309,8 @@ ZMPM_D M3<T> admm_local_solve(const M3<T>& FDb, const M3<T>& Fcur, T vol, T coef
         T zp[3], D[3][3];
         if (mode == ADMM_VON_MISES)
             vm_project_sigma(mu, (T)p.ys, zi, zp, D);
+        else if (mode == ADMM_DRUCKER_PRAGER)
+            dp_project_sigma_derivative(mu, lambda, (T)p.alpha, (T)p.cohesion, zi, zp, D);
         else if (mode == ADMM_VISCOUS)
             viscous_sigma(mu, lambda, (T)p.vd, (T)p.vv, dt, zi, zp, D);
         else {
@@ -258,9 +346,10 @@ ZMPM_D M3<T> admm_local_solve(const M3<T>& FDb, const M3<T>& Fcur, T vol, T coef
 
 // initOmega for one strain (AdmmSimulationFoam.h:236-270):
 // omega = sqrt(vol sqrt(|makePD(d2E)|^2 + sum_ij |makePD2D(B_ij)|^2)), with
-// sigma projected onto the yield surface for the B_ij terms under von Mises.
+// sigma projected onto the yield surface for the B_ij terms under von Mises
+// and Drucker-Prager (pkind).
 template <class T>
-ZMPM_D T admm_omega(const M3<T>& Fa, T vol, T mu, T lambda, bool vm, T ys)
+ZMPM_D T admm_omega(const M3<T>& Fa, T vol, T mu, T lambda, int pkind, T ys, T alpha = T(0), T cohesion = T(0))
 {
     M3<T> U, V;
     T s[3];
@@ -268,9 +357,15 @@ ZMPM_D T admm_omega(const M3<T>& Fa, T vol, T mu, T lambda, bool vm, T ys)
     T dE[3], ddE[3][3];
     hencky_diag(mu, lambda, s, dE, ddE);
     T total = make_pd_norm2(ddE);
-    if (vm) {
+    if (pkind == ZMPM_PLASTIC_VON_MISES) {
         T sp[3], D[3][3];
         vm_project_sigma(mu, ys, s, sp, D);
+#pragma unroll
+        for (int d = 0; d < 3; ++d) s[d] = sp[d];
+    }
+    else if (pkind == ZMPM_PLASTIC_DRUCKER_PRAGER) {
+        T sp[3];
+        dp_project_sigma(mu, lambda, alpha, cohesion, s, sp);
 #pragma unroll
         for (int d = 0; d < 3; ++d) s[d] = sp[d];
     }

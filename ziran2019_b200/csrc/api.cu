@@ -948,8 +948,8 @@ int zmpm_substep(zmpm_ctx* ctx, double dt, const zmpm_solver* s, zmpm_stats* st)
     }
     if (admm)
         for (int64_t i = 0; i < ctx->P; ++i)
-            if (ctx->hpkind[i] == ZMPM_PLASTIC_DRUCKER_PRAGER || ctx->hpkind[i] == ZMPM_PLASTIC_CAM_CLAY) {
-                ctx->err = "the ADMM local step has no Drucker-Prager or Cam-Clay projection here";
+            if (ctx->hpkind[i] == ZMPM_PLASTIC_CAM_CLAY) {
+                ctx->err = "the ADMM F-step has no Cam-Clay projection (AdmmSimulationFoam.h:617-633 lists none)";
                 return ZMPM_UNSUPPORTED;
             }
     if (ctx->has_pf && admm) {
