@@ -363,6 +363,17 @@ int zmpm_adjoint_substep(zmpm_ctx* ctx, double dt, const zmpm_solver* s, double 
 int zmpm_checkpoint_save(zmpm_ctx* ctx, int32_t slot);
 int zmpm_checkpoint_load(zmpm_ctx* ctx, int32_t slot);
 
+/* MpmSimulationBase::evalMaxParticleSpeed (MpmSimulationBase.cpp:1143-1166):
+   the largest particle speed and the particles' bounding box (any pointer may
+   be NULL). */
+int zmpm_max_particle_speed(zmpm_ctx* ctx, double* speed, double* min_corner, double* max_corner);
+/* MpmSimulationBase::calculateDt (MpmSimulationBase.cpp:766-790): cfl dx / v,
+   v the larger of the particle speed and the colliders' evalMaxSpeed
+   (CollisionObject.cpp:159-196) over the particles' box grown by 4 dx; max_dt
+   when nothing moves.  cfl is the config's.  The frame-boundary clamp of
+   TimeStepping::nextDt is the caller's (the Python TimeStepping mirrors it). */
+int zmpm_calculate_dt(zmpm_ctx* ctx, double max_dt, double* dt);
+
 /* Restart files: the role of SimulationBase::write / read with
    MpmSimulationBase::writeState / readState (SimulationBase.h:146-187,
    MpmSimulationBase.cpp:725-761).  The library's own versioned binary format

@@ -27,6 +27,7 @@
 #include "../include/zmpm.h"
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -2680,6 +2681,113 @@ struct Sim {
         return false;
     }
 
+    // MpmSimulationBase::evalMaxParticleSpeed (MpmSimulationBase.cpp:1143-1166)
+    void maxParticleSpeed(T& speed, T lo[3], T hi[3]) const
+    {
+        T m[7];
+        m[0] = 0;
+        for (int k = 1; k < 7; ++k) m[k] = std::numeric_limits<float>::lowest();
+        for (int64_t i = 0; i < P; ++i) {
+            T v2 = 0;
+            for (int d = 0; d < 3; ++d) {
+                v2 += V[3 * i + d] * V[3 * i + d];
+                m[1 + d] = std::max(m[1 + d], X[3 * i + d]);
+                m[4 + d] = std::max(m[4 + d], -X[3 * i + d]);
+            }
+            m[0] = std::max(m[0], std::sqrt(v2));
+        }
+        speed = m[0];
+        for (int d = 0; d < 3; ++d) {
+            hi[d] = m[1 + d];
+            lo[d] = -m[4 + d];
+        }
+    }
+
+    // AnalyticCollisionObject::evalMaxSpeed (CollisionObject.cpp:159-196) with
+    // AnalyticLevelSet::getBounds of spheres and boxes; returns false for a
+    // rotating or scaling half space, whose bounds the reference does not have.
+    static bool colliderMaxSpeed(const zmpm_collider& c, double time, const T pmin[3], const T pmax[3], T& speed)
+    {
+        const T om[3] = { (T)c.angular_velocity[0], (T)c.angular_velocity[1], (T)c.angular_velocity[2] };
+        const T dbdt[3] = { (T)c.translation_velocity[0], (T)c.translation_velocity[1], (T)c.translation_velocity[2] };
+        const T dsdt = (T)c.scale_velocity;
+        if (!(dsdt != 0 || std::sqrt(om[0] * om[0] + om[1] * om[1] + om[2] * om[2]) != 0)) {
+            speed = std::sqrt(dbdt[0] * dbdt[0] + dbdt[1] * dbdt[1] + dbdt[2] * dbdt[2]);
+            return true;
+        }
+        T lo[3], hi[3];
+        if (c.shape == ZMPM_SPHERE)
+            for (int d = 0; d < 3; ++d) {
+                lo[d] = (T)(c.a[d] - c.radius);
+                hi[d] = (T)(c.a[d] + c.radius);
+            }
+        else if (c.shape == ZMPM_BOX)
+            for (int d = 0; d < 3; ++d) {
+                lo[d] = (T)c.a[d];
+                hi[d] = (T)c.b[d];
+            }
+        else
+            return false;
+        Collider<T> co;
+        co.d = c;
+        co.setRotation();
+        const T s_ = (T)(c.scale + time * c.scale_velocity), ios = 1 / s_;
+        T b[3];
+        for (int d = 0; d < 3; ++d) b[d] = (T)(c.translation[d] + time * c.translation_velocity[d]);
+        std::vector<std::array<T, 3>> pts;
+        for (int i = 0; i < 8; ++i) {
+            T x[3], Xm[3];
+            for (int d = 0; d < 3; ++d) x[d] = (i & (1 << d)) ? pmin[d] : pmax[d];
+            for (int r = 0; r < 3; ++r) Xm[r] = (co.R[0][r] * (x[0] - b[0]) + co.R[1][r] * (x[1] - b[1]) + co.R[2][r] * (x[2] - b[2])) * ios;
+            bool any_a = false, any_b = false;
+            for (int d = 0; d < 3; ++d) {
+                any_a = any_a || lo[d] < Xm[d];
+                any_b = any_b || Xm[d] < hi[d];
+            }
+            if (any_a && any_b) pts.push_back({ x[0], x[1], x[2] });
+        }
+        for (int i = 0; i < 8; ++i) {
+            T Xm[3], x[3];
+            for (int d = 0; d < 3; ++d) Xm[d] = (i & (1 << d)) ? lo[d] : hi[d];
+            for (int r = 0; r < 3; ++r) x[r] = (co.R[r][0] * Xm[0] + co.R[r][1] * Xm[1] + co.R[r][2] * Xm[2]) * s_ + b[r];
+            bool any_a = false, any_b = false;
+            for (int d = 0; d < 3; ++d) {
+                any_a = any_a || pmin[d] < x[d];
+                any_b = any_b || x[d] < pmax[d];
+            }
+            if (any_a && any_b) pts.push_back({ x[0], x[1], x[2] });
+        }
+        speed = 0;
+        for (const auto& x : pts) {
+            const T xb[3] = { x[0] - b[0], x[1] - b[1], x[2] - b[2] };
+            const T v[3] = { om[1] * xb[2] - om[2] * xb[1] + (dsdt * ios) * xb[0] + dbdt[0], om[2] * xb[0] - om[0] * xb[2] + (dsdt * ios) * xb[1] + dbdt[1],
+                om[0] * xb[1] - om[1] * xb[0] + (dsdt * ios) * xb[2] + dbdt[2] };
+            speed = std::max(speed, std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]));
+        }
+        return true;
+    }
+
+    // MpmSimulationBase::calculateDt (MpmSimulationBase.cpp:766-790)
+    int calculateDt(double max_dt, double& dt_out)
+    {
+        T v, lo[3], hi[3];
+        maxParticleSpeed(v, lo, hi);
+        for (int d = 0; d < 3; ++d) {
+            lo[d] -= (2 + 2) * dx;
+            hi[d] += (2 + 2) * dx;
+        }
+        for (const auto& c : colliders) {
+            T sc;
+            if (!colliderMaxSpeed(c.d, time, lo, hi, sc)) {
+                err = "a rotating or scaling half space has no bounds (AnalyticLevelSet::getBounds)";
+                return ZMPM_BAD_ARG;
+            }
+            v = std::max(v, sc);
+        }
+        dt_out = v ? (double)(cfl * dx / v) : max_dt;
+        return ZMPM_OK;
+    }
+
     // FractureSimulation::deleteParticles (FractureSimulation.h:172-207)
     void deletePhaseFieldParticles()
     {
@@ -3487,6 +3595,29 @@ int zoracle_get_phase_field(Ctx* c, double* cc, double* H, double* fp, double* v
             if (vol) vol[i] = S.damage[i].vol;
         }
     });
+    return ZMPM_OK;
+}
+
+int zoracle_max_particle_speed(Ctx* c, double* speed, double* lo, double* hi)
+{
+    if (!c) return ZMPM_BAD_ARG;
+    DISPATCH(c, {
+        using T = typename std::remove_reference<decltype(S.dx)>::type;
+        T v, l[3], h[3];
+        S.maxParticleSpeed(v, l, h);
+        if (speed) *speed = (double)v;
+        for (int d = 0; d < 3; ++d) {
+            if (lo) lo[d] = (double)l[d];
+            if (hi) hi[d] = (double)h[d];
+        }
+    });
+    return ZMPM_OK;
+}
+
+int zoracle_calculate_dt(Ctx* c, double max_dt, double* dt)
+{
+    if (!c || !dt || !(max_dt > 0)) return ZMPM_BAD_ARG;
+    DISPATCH(c, { return S.calculateDt(max_dt, *dt); });
     return ZMPM_OK;
 }
 

@@ -633,3 +633,34 @@ def test_admm_sand_substeps(oracle):
     h2.addPlasticity(None, mpm.NonAssociativeCamClay(-0.01, 45.0, 0.3, 3.0, True))
     s2.useAdmm(admm_max_iterations=4)
     assert s2.lib.substep(s2.ctx, 1e-3, C.byref(s2.solver()), None) == abi.UNSUPPORTED
+
+
+def test_calculate_dt_and_time_stepping(oracle):
+    """calculateDt (MpmSimulationBase.cpp:766-790) = cfl dx / max speed over
+    particles and colliders; TimeStepping hits frame times exactly."""
+    dx = 1.0 / 64
+    s = mpm.MpmSimulation(dx, gravity=(0, -9.8, 0), precision="fp64", lib=oracle, cfl=0.5)
+    h, x = build_scene(s, kind="fcr", n=4, dx=dx, v0=(0.3, -1.0, 0.2))
+    v, lo, hi = s.maxParticleSpeed()
+    assert abs(v - np.linalg.norm([0.3, -1.0, 0.2])) < 1e-12
+    np.testing.assert_allclose(lo, x.min(0), rtol=0, atol=1e-15)
+    np.testing.assert_allclose(hi, x.max(0), rtol=0, atol=1e-15)
+    assert abs(s.calculateDt(0.01) - 0.5 * dx / v) < 1e-15
+    fast = mpm.AnalyticCollisionObject(mpm.Sphere((0.5, 0.5, 0.5), 0.1), abi.SLIP)
+    fast.setTranslation((0.0, 0.0, 0.0), (0.0, 0.0, 5.0))
+    s.addCollisionObject(fast)
+    assert abs(s.calculateDt(0.01) - 0.5 * dx / 5.0) < 1e-15
+    spin = mpm.AnalyticCollisionObject(mpm.HalfSpace((0, 0.05, 0), (0, 1, 0)), abi.STICKY)
+    spin.setAngularVelocity((0, 1.0, 0))
+    s.addCollisionObject(spin)
+    with pytest.raises(abi.ZmpmError):
+        s.calculateDt(0.01)
+    step = mpm.TimeStepping(frame_dt=1.0 / 24)
+    step.max_dt = 0.01
+    dts = []
+    while True:
+        dt = step.nextDt(0.007)
+        dts.append(dt)
+        if step.advance(dt) == mpm.TimeStepping.FRAME:
+            break
+    assert abs(sum(dts) - 1.0 / 24) < 1e-15 and max(dts) <= 0.007 + 1e-15

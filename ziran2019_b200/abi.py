@@ -140,6 +140,8 @@ _SIGS = {
     "add_drucker_prager": (C.c_int, [C.c_void_p, C.c_int64, C.c_int64, C.c_double, C.c_double, C.c_double, C.c_int32]),
     "add_cam_clay": (C.c_int, [C.c_void_p, C.c_int64, C.c_int64, C.c_double, C.c_double, C.c_double, C.c_double, C.c_int32]),
     "get_log_jp": (C.c_int, [C.c_void_p, c_double_p]),
+    "max_particle_speed": (C.c_int, [C.c_void_p, c_double_p, c_double_p, c_double_p]),
+    "calculate_dt": (C.c_int, [C.c_void_p, C.c_double, c_double_p]),
     "add_damage": (C.c_int, [C.c_void_p, C.c_int64, C.c_int64, C.c_int32, C.c_double, C.c_double]),
     "get_damage": (C.c_int, [C.c_void_p, c_double_p]),
     "add_phase_field": (C.c_int, [C.c_void_p, C.c_int64, C.c_int64, C.c_double, C.c_double, C.c_int32, C.c_double]),

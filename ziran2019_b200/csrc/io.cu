@@ -16,6 +16,10 @@
 //   uint16 name length, name, uint16 components, int32 type (5: vector),
 //   components x int32 default (0); per point: x, y, z, w = 1, then the
 //   attribute floats; trailer bytes 0x00 0xff.
+#include <algorithm>
+#include <array>
+#include <cfloat>
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -118,6 +122,117 @@ struct File {
 };
 
 const char STATE_MAGIC[8] = { 'Z', 'M', 'P', 'M', 'S', 'T', 'A', 'T' };
+
+// Per-CTA partial maxima of |v|, x and -x (7 values per CTA).
+constexpr int SPEED_THREADS = 256;
+__global__ void __launch_bounds__(SPEED_THREADS) k_max_speed(const double* __restrict__ pd, int64_t cap, int64_t P, double* __restrict__ part)
+{
+    __shared__ double red[7][SPEED_THREADS];
+    double m[7];
+    m[0] = 0;
+    for (int k = 1; k < 7; ++k) m[k] = -(double)FLT_MAX; // numeric_limits<float>::lowest(), as the reference
+    for (int64_t s = (int64_t)blockIdx.x * SPEED_THREADS + threadIdx.x; s < P; s += (int64_t)gridDim.x * SPEED_THREADS) {
+        double v2 = 0;
+        for (int d = 0; d < 3; ++d) {
+            const double v = pd[(PD_V + d) * cap + s], x = pd[(PD_X + d) * cap + s];
+            v2 += v * v;
+            m[1 + d] = fmax(m[1 + d], x);
+            m[4 + d] = fmax(m[4 + d], -x);
+        }
+        m[0] = fmax(m[0], sqrt(v2));
+    }
+    for (int k = 0; k < 7; ++k) red[k][threadIdx.x] = m[k];
+    __syncthreads();
+    for (int o = SPEED_THREADS / 2; o > 0; o >>= 1) {
+        if (threadIdx.x < o)
+            for (int k = 0; k < 7; ++k) red[k][threadIdx.x] = fmax(red[k][threadIdx.x], red[k][threadIdx.x + o]);
+        __syncthreads();
+    }
+    if (threadIdx.x < 7) part[7 * blockIdx.x + threadIdx.x] = red[threadIdx.x][0];
+}
+
+void rotation_of(const double q[4], double R[9])
+{
+    double w = q[0], x = q[1], y = q[2], z = q[3];
+    double n = std::sqrt(w * w + x * x + y * y + z * z);
+    if (n == 0) {
+        w = 1;
+        x = y = z = 0;
+        n = 1;
+    }
+    w /= n;
+    x /= n;
+    y /= n;
+    z /= n;
+    const double r[9] = { 1 - 2 * (y * y + z * z), 2 * (x * y - w * z), 2 * (x * z + w * y), 2 * (x * y + w * z), 1 - 2 * (x * x + z * z),
+        2 * (y * z - w * x), 2 * (x * z - w * y), 2 * (y * z + w * x), 1 - 2 * (x * x + y * y) };
+    for (int i = 0; i < 9; ++i) R[i] = r[i];
+}
+
+// AnalyticCollisionObject::evalMaxSpeed (CollisionObject.cpp:159-196) at `time`
+// against the particles' box [pmin, pmax]; the level-set bounds are those of
+// AnalyticLevelSet::getBounds (sphere, box; a half space has none).
+int collider_max_speed(const zmpm_collider& c, double time, const double pmin[3], const double pmax[3], double& speed, std::string& err)
+{
+    const double* om = c.angular_velocity;
+    const double* dbdt = c.translation_velocity;
+    const double dsdt = c.scale_velocity;
+    if (!(dsdt != 0 || std::sqrt(om[0] * om[0] + om[1] * om[1] + om[2] * om[2]) != 0)) {
+        speed = std::sqrt(dbdt[0] * dbdt[0] + dbdt[1] * dbdt[1] + dbdt[2] * dbdt[2]);
+        return ZMPM_OK;
+    }
+    double lo[3], hi[3];
+    if (c.shape == ZMPM_SPHERE)
+        for (int d = 0; d < 3; ++d) {
+            lo[d] = c.a[d] - c.radius;
+            hi[d] = c.a[d] + c.radius;
+        }
+    else if (c.shape == ZMPM_BOX)
+        for (int d = 0; d < 3; ++d) {
+            lo[d] = c.a[d];
+            hi[d] = c.b[d];
+        }
+    else {
+        err = "a rotating or scaling half space has no bounds (AnalyticLevelSet::getBounds)";
+        return ZMPM_BAD_ARG;
+    }
+    double R[9], b[3];
+    rotation_of(c.rotation, R);
+    const double s = c.scale + time * dsdt, one_over_s = 1 / s;
+    for (int d = 0; d < 3; ++d) b[d] = c.translation[d] + time * dbdt[d];
+    std::vector<std::array<double, 3>> corners;
+    for (int i = 0; i < 8; ++i) {
+        double x[3], X[3];
+        for (int d = 0; d < 3; ++d) x[d] = (i & (1 << d)) ? pmin[d] : pmax[d];
+        for (int r = 0; r < 3; ++r) X[r] = (R[r] * (x[0] - b[0]) + R[3 + r] * (x[1] - b[1]) + R[6 + r] * (x[2] - b[2])) * one_over_s;
+        bool a = false, bb = false;
+        for (int d = 0; d < 3; ++d) {
+            a = a || lo[d] < X[d];
+            bb = bb || X[d] < hi[d];
+        }
+        if (a && bb) corners.push_back({ x[0], x[1], x[2] });
+    }
+    for (int i = 0; i < 8; ++i) {
+        double X[3], x[3];
+        for (int d = 0; d < 3; ++d) X[d] = (i & (1 << d)) ? lo[d] : hi[d];
+        for (int r = 0; r < 3; ++r) x[r] = (R[3 * r] * X[0] + R[3 * r + 1] * X[1] + R[3 * r + 2] * X[2]) * s + b[r];
+        bool a = false, bb = false;
+        for (int d = 0; d < 3; ++d) {
+            a = a || pmin[d] < x[d];
+            bb = bb || x[d] < pmax[d];
+        }
+        if (a && bb) corners.push_back({ x[0], x[1], x[2] });
+    }
+    speed = 0;
+    for (const auto& x : corners) {
+        const double xb[3] = { x[0] - b[0], x[1] - b[1], x[2] - b[2] };
+        const double v[3] = { om[1] * xb[2] - om[2] * xb[1] + (dsdt * one_over_s) * xb[0] + dbdt[0],
+            om[2] * xb[0] - om[0] * xb[2] + (dsdt * one_over_s) * xb[1] + dbdt[1],
+            om[0] * xb[1] - om[1] * xb[0] + (dsdt * one_over_s) * xb[2] + dbdt[2] };
+        speed = std::max(speed, std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]));
+    }
+    return ZMPM_OK;
+}
 
 } // namespace
 } // namespace zmpm
@@ -312,6 +427,64 @@ int zmpm_write_bgeo(zmpm_ctx* ctx, const char* path, int32_t fields)
         ctx->err = std::string("write failed: ") + path;
         return ZMPM_BAD_ARG;
     }
+    return ZMPM_OK;
+}
+
+int zmpm_max_particle_speed(zmpm_ctx* ctx, double* speed, double* min_corner, double* max_corner)
+{
+    if (!ctx) return ZMPM_BAD_ARG;
+    cudaSetDevice(ctx->device);
+    double m[7];
+    m[0] = 0;
+    for (int k = 1; k < 7; ++k) m[k] = -(double)FLT_MAX;
+    if (ctx->uploaded && ctx->P > 0) {
+        const int64_t P = ctx->P;
+        const int nb = (int)std::min<int64_t>(1024, (P + SPEED_THREADS - 1) / SPEED_THREADS);
+        ZMPM_CUDA(ctx->stage.ensure(7 * nb * sizeof(double)));
+        k_max_speed<<<nb, SPEED_THREADS, 0, ctx->stream>>>(ctx->pd.as<double>(), ctx->Pcap, P, ctx->stage.as<double>());
+        ++g_kernel_launches;
+        std::vector<double> part(7 * nb);
+        ZMPM_CUDA(cudaMemcpyAsync(part.data(), ctx->stage.p, part.size() * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+        ZMPM_CUDA(cudaStreamSynchronize(ctx->stream));
+        for (int b = 0; b < nb; ++b)
+            for (int k = 0; k < 7; ++k) m[k] = std::max(m[k], part[7 * b + k]);
+    }
+    else
+        for (int64_t i = 0; i < ctx->P; ++i) {
+            double v2 = 0;
+            for (int d = 0; d < 3; ++d) {
+                v2 += ctx->hv[3 * i + d] * ctx->hv[3 * i + d];
+                m[1 + d] = std::max(m[1 + d], ctx->hx[3 * i + d]);
+                m[4 + d] = std::max(m[4 + d], -ctx->hx[3 * i + d]);
+            }
+            m[0] = std::max(m[0], std::sqrt(v2));
+        }
+    if (speed) *speed = m[0];
+    for (int d = 0; d < 3; ++d) {
+        if (max_corner) max_corner[d] = m[1 + d];
+        if (min_corner) min_corner[d] = -m[4 + d];
+    }
+    return ZMPM_OK;
+}
+
+int zmpm_calculate_dt(zmpm_ctx* ctx, double max_dt, double* dt)
+{
+    if (!ctx || !dt || !(max_dt > 0)) return ZMPM_BAD_ARG;
+    double v, lo[3], hi[3];
+    int rc = zmpm_max_particle_speed(ctx, &v, lo, hi);
+    if (rc) return rc;
+    const double grow = (2 + 2) * ctx->cfg.dx; // (interpolation_degree + 2) dx
+    for (int d = 0; d < 3; ++d) {
+        lo[d] -= grow;
+        hi[d] += grow;
+    }
+    for (const auto& c : ctx->colliders) {
+        double sc = 0;
+        rc = collider_max_speed(c, ctx->time, lo, hi, sc, ctx->err);
+        if (rc) return rc;
+        v = std::max(v, sc);
+    }
+    *dt = v ? ctx->cfg.cfl * ctx->cfg.dx / v : max_dt;
     return ZMPM_OK;
 }
 

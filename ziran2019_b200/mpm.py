@@ -234,6 +234,56 @@ class MpmParticleHandle:
                            plasticity.yield_stress, plasticity.xi, plasticity.fail_stress)
 
 
+# ----------------------------------------------------------- time stepping --
+class TimeStepping:
+    """TimeStepping (Lib/Ziran/Sim/TimeStepping.h:8-91): substep sizes that hit
+    the frame times exactly.  Set `max_dt` after construction, as the
+    reference's scenes do; `nextDt` clamps it to the frame length."""
+    FRAME, SUBSTEP = 0, 1
+
+    def __init__(self, frame_dt=1.0 / 24, min_dt=1e-6):
+        self.time = 0.0
+        self.time_since_last_frame = 0.0
+        self.frame_dt = float(frame_dt)
+        self.min_dt = float(min_dt)
+        self.max_dt = self.frame_dt
+        self.max_dt_original = self.frame_dt
+
+    def nextDt(self, dt):
+        if not dt > 0:
+            raise ValueError("dt must be positive")
+        self.max_dt = min(self.max_dt, self.max_dt_original)
+        dt = self.min_dt if dt < self.min_dt else (self.max_dt if dt > self.max_dt else dt)
+        if self.time_since_last_frame + dt >= self.frame_dt:
+            dt = self.frame_dt - self.time_since_last_frame  # final substep of the frame
+        elif self.time_since_last_frame + 2 * dt > self.frame_dt:
+            dt = (self.frame_dt - self.time_since_last_frame) / 2  # no tiny last substep
+        return dt
+
+    def advance(self, dt):
+        self.time += dt
+        self.time_since_last_frame += dt
+        if self.time_since_last_frame >= self.frame_dt:
+            self.time_since_last_frame = 0.0
+            return self.FRAME
+        return self.SUBSTEP
+
+    def reset(self, frame):
+        self.time = frame * self.frame_dt
+        self.time_since_last_frame = 0.0
+
+
+class RestartRequired(RuntimeError):
+    """A substep moved a particle more than one cell: the reference throws
+    RestartException and restarts the frame with half the max dt
+    (MpmSimulationBase.cpp:983-1002).  `max_dt` is the suggested new value."""
+
+    def __init__(self, frame, max_dt):
+        super().__init__(f"CFL violation in frame {frame}; restart it with max_dt = {max_dt}")
+        self.frame = frame
+        self.max_dt = max_dt
+
+
 # ------------------------------------------------------------ simulation --
 class MpmSimulation:
     """Implicit APIC MPM on one GPU (MpmSimulationBase<T,3>, symplectic = false).
@@ -367,6 +417,36 @@ class MpmSimulation:
         self.last_stats = st.as_dict()
         self.last_status = rc
         return rc
+
+    def calculateDt(self, max_dt):
+        """MpmSimulationBase::calculateDt: cfl dx / max(particle, collider speed)."""
+        dt = abi.C.c_double()
+        self._call("calculate_dt", float(max_dt), abi.C.byref(dt))
+        return dt.value
+
+    def maxParticleSpeed(self):
+        """evalMaxParticleSpeed: (max |v|, min corner, max corner)."""
+        v = abi.C.c_double()
+        lo, hi = np.zeros(3), np.zeros(3)
+        self._call("max_particle_speed", abi.C.byref(v), ptr(lo), ptr(hi))
+        return v.value, lo, hi
+
+    def advanceOneFrame(self, step, frame=0, autorestart=True):
+        """SimulationBase::advanceOneFrame (SimulationBase.h:288-321): substeps of
+        step.nextDt(calculateDt()) until the frame ends; returns the substep
+        count.  A CFL violation raises RestartRequired (autorestart) with half
+        the max dt, as the reference's restart does."""
+        n = 0
+        while True:
+            dt = step.nextDt(self.calculateDt(step.max_dt))
+            rc = self.advanceOneTimeStep(dt)
+            n += 1
+            if rc == abi.CFL_VIOLATION and autorestart:
+                raise RestartRequired(frame, max(step.max_dt / 2, step.min_dt))
+            if rc not in (abi.OK, abi.CFL_VIOLATION):
+                raise abi.ZmpmError(rc, "substep")
+            if step.advance(dt) == TimeStepping.FRAME:
+                return n
 
     # state
     @property
