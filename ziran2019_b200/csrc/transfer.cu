@@ -535,11 +535,28 @@ __global__ void __launch_bounds__(XF_THREADS) k_hvp_scatter(const int32_t* __res
             for (int c = 0; c < NCP; ++c)
 #pragma unroll
                 for (int q2 = 0; q2 < 3; ++q2) row[c][q2] = dstress[(3 * (c0 + c) + q2) * cap + s];
-            for_stencil<L>(lx, ly, lz, w, dwr, inv_dx, [&](int, int, int i, int j, int k, TH, const TH* dw) {
-                const int n = 9 * i + 3 * j + k;
+            if constexpr (NCP == 3) {
+                // components 0 and 1 as one packed FP32 pair (same per-component
+                // rounding as the scalar fma), component 2 scalar
+                const float2 r0 = make_float2(row[0][0], row[1][0]), r1 = make_float2(row[0][1], row[1][1]),
+                             r2 = make_float2(row[0][2], row[1][2]);
+                for_stencil<L>(lx, ly, lz, w, dwr, inv_dx, [&](int, int, int i, int j, int k, TH, const TH* dw) {
+                    const int n = 9 * i + 3 * j + k;
+                    float2 t = __fmul2_rn(r0, make_float2(dw[0], dw[0]));
+                    t = __ffma2_rn(r1, make_float2(dw[1], dw[1]), t);
+                    t = __ffma2_rn(r2, make_float2(dw[2], dw[2]), t);
+                    const float2 acc = __fadd2_rn(make_float2(a[n][0], a[n][1]), t);
+                    a[n][0] = acc.x;
+                    a[n][1] = acc.y;
+                    a[n][2] += row[2][0] * dw[0] + row[2][1] * dw[1] + row[2][2] * dw[2];
+                });
+            }
+            else
+                for_stencil<L>(lx, ly, lz, w, dwr, inv_dx, [&](int, int, int i, int j, int k, TH, const TH* dw) {
+                    const int n = 9 * i + 3 * j + k;
 #pragma unroll
-                for (int c = 0; c < NCP; ++c) a[n][c] += row[c][0] * dw[0] + row[c][1] * dw[1] + row[c][2] * dw[2];
-            });
+                    for (int c = 0; c < NCP; ++c) a[n][c] += row[c][0] * dw[0] + row[c][1] * dw[1] + row[c][2] * dw[2];
+                });
         }
         if (threadIdx.x / NPB < cnt) {
 #pragma unroll
