@@ -994,10 +994,9 @@ int zmpm_substep(zmpm_ctx* ctx, double dt, const zmpm_solver* s, zmpm_stats* st)
     ZMPM_CUDA(cudaMemcpyAsync(&hs, ctx->scal.p, sizeof(hs), cudaMemcpyDeviceToHost, ctx->stream));
     ZMPM_CUDA(cudaMemcpyAsync(&hc, ctx->counters.p, sizeof(hc), cudaMemcpyDeviceToHost, ctx->stream));
     ZMPM_CUDA(cudaStreamSynchronize(ctx->stream));
-    if (ctx->graph_exec) {
-        cudaGraphExecDestroy(ctx->graph_exec);
-        ctx->graph_exec = nullptr;
-    }
+    // the solve's graph stays instantiated until the next solve replaces it
+    // (after launching its own graph) or zmpm_destroy: destroying it here sat
+    // in the GPU's idle time between substeps
     float ms = 0;
     cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
     ctx->time += dt;

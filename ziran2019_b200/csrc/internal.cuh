@@ -161,7 +161,7 @@ struct Ctx {
     DBuf dstress;      // [9][Pcap] dS of one Hessian-vector product (HVP precision)
     bool hvp_fused = false; // one fused HVP kernel instead of stress + scatter
     bool no_graph = false;  // host-driven Newton loop instead of the conditional graph
-    cudaGraphExec_t graph_exec = nullptr; // last Newton graph, released after the next sync
+    cudaGraphExec_t graph_exec = nullptr; // last solve graph, released when the next one is launched
     bool graph_used = false;              // the last Newton solve ran as a graph
     DBuf frac;         // [3][Pcap] fractional offsets in cells (FP32 HVP)
     double* pdf(int f) const { return pd.as<double>() + (int64_t)f * Pcap; }

@@ -1241,7 +1241,7 @@ static int newton_impl(Ctx* ctx, const zmpm_solver& s)
         g_kernel_launches = launches0;
         ctx->graph_used = true;
         if (ctx->graph_exec) cudaGraphExecDestroy(ctx->graph_exec);
-        ctx->graph_exec = exec; // released after the next synchronisation
+        ctx->graph_exec = exec; // released when the next solve launches its graph, or by zmpm_destroy
         ZMPM_CUDA(e);
         return ZMPM_OK;
     }
