@@ -65,7 +65,7 @@ struct SolverScalars {
     int32_t kit;               // Krylov iteration index of the current linear solve
     int32_t nit;               // Newton iteration index (= Newton loop bodies run)
     int32_t krylov_bodies;     // Krylov loop bodies run (graph launch accounting)
-    int32_t pad0;
+    uint32_t ticket;           // CTAs of the running kernel that finished (last_cta); 0 between kernels
     int32_t newton_iters;      // linear solves run
     int32_t krylov_iters;      // summed Krylov iterations
     int32_t hvp_count;
@@ -78,8 +78,12 @@ struct SolverScalars {
     double zTrk;
     // MINRES (Minres.h:16-24), double buffered by iteration parity
     double mr[2][12];
+    // delta, epsilon, gamma, t and beta of the last MINRES iteration: its
+    // search direction and x update run in the next operator pass (or at the
+    // solve's end)
+    double pend[5];
 };
-enum MinresSlot { MR_GC0, MR_GS0, MR_GC1, MR_GS1, MR_GC2, MR_GS2, MR_RHS0, MR_RHS1, MR_BETA_KP1, MR_TK, MR_DELTA, MR_EPS };
+enum MinresSlot { MR_GC0, MR_GS0, MR_GC1, MR_GS1, MR_GC2, MR_GS2, MR_RHS0, MR_RHS1, MR_BETA_KP1 };
 
 // Field indices of the particle pools.
 // Fields from PD_CORE on (phase-field state, then viscoelastic strain and ADMM

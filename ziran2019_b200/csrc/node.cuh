@@ -43,6 +43,36 @@ __device__ __forceinline__ double reduce_partials(const double* __restrict__ par
     return block_sum(s);
 }
 
+// The same sum read through L2 (ld.cg), for partials that other CTAs of the
+// running kernel wrote.
+__device__ __forceinline__ double reduce_partials_l2(const double* part, int n)
+{
+    double s = 0;
+    for (int i = threadIdx.x; i < n; i += ND_THREADS) s += __ldcg(part + i);
+    return block_sum(s);
+}
+
+// True in every thread of the CTA that finishes last among the kernel's CTAs;
+// every CTA's earlier global writes (its partial sum) are then visible to it,
+// so that CTA can run the scalar step that needs all partials inside the same
+// kernel.  It puts the ticket back to 0 for the next kernel.  No CTA waits.
+__device__ __forceinline__ bool last_cta(uint32_t* ticket)
+{
+    __shared__ bool last;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        const uint32_t t = atomicAdd(ticket, 1u);
+        last = (t == gridDim.x - 1);
+        if (last) {
+            *ticket = 0;
+            __threadfence();
+        }
+    }
+    __syncthreads();
+    return last;
+}
+
 struct NodeGeom {
     int64_t nn;        // B * NPB
     int parts;         // CTAs of node kernels

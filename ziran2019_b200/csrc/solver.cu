@@ -425,6 +425,7 @@ __global__ void __launch_bounds__(ND_THREADS) k_newton_check(NodeGeom ng, const 
                 kb.M[1][i] = 0;
                 kb.M[2][i] = 0;
                 kb.Z[0][i] = z;
+                kb.Z[1][i] = 0;
             }
             else {
                 kb.r[i] = rv;
@@ -439,8 +440,9 @@ __global__ void __launch_bounds__(ND_THREADS) k_newton_check(NodeGeom ng, const 
 }
 
 // Initial preconditioned norm and local tolerance (Minres.h:73-98,
-// ConjugateGradient.h:108-117); MINRES normalises Q0, Z0.  Sets the Krylov
-// loop condition when running as a graph.
+// ConjugateGradient.h:108-117); MINRES keeps Q0, Z0 unnormalised (beta_0 =
+// the norm divides them where they are read).  Sets the Krylov loop condition
+// when running as a graph.  One CTA.
 template <int NPB>
 __global__ void __launch_bounds__(ND_THREADS) k_krylov_start(NodeGeom ng, KrylovBufs kb, NewtonParams np, const double* __restrict__ part_in,
     SolverScalars* __restrict__ sc, cudaGraphConditionalHandle hK, int use_graph)
@@ -471,18 +473,12 @@ __global__ void __launch_bounds__(ND_THREADS) k_krylov_start(NodeGeom ng, Krylov
             sc->mr[0][0] = dotv; // CG keeps zTrk double-buffered in mr[parity][0]
         if (use_graph) cudaGraphSetConditional(hK, active ? 1u : 0u);
     }
-    if (!np.minres || !active || !(rnorm > 0)) return;
-    for (int64_t n = (int64_t)blockIdx.x * ND_THREADS + threadIdx.x; n < ng.nn; n += (int64_t)gridDim.x * ND_THREADS)
-        for (int k = 0; k < 3; ++k) {
-            int64_t i = vidx<NPB>(n, k);
-            kb.Q[0][i] /= rnorm;
-            kb.Z[0][i] /= rnorm;
-        }
 }
 
 // out = project(m x + dt^2 hacc) (BackwardEuler.h:322-351 then Minres.h:116);
 // zeroes hacc; partial dot(out, x) when part != null.
-template <int NPB>
+// SKIP: massless slots (zero in every Krylov vector) are not touched.
+template <int NPB, bool SKIP>
 __device__ __forceinline__ void apply_A_body(NodeGeom ng, const double* __restrict__ gm, const int8_t* __restrict__ col,
     const double* __restrict__ P6, double dt2, const double* __restrict__ xin, double* __restrict__ hacc, double* __restrict__ out,
     double* __restrict__ part, int project)
@@ -490,6 +486,7 @@ __device__ __forceinline__ void apply_A_body(NodeGeom ng, const double* __restri
     double acc = 0;
     for (int64_t n = (int64_t)blockIdx.x * ND_THREADS + threadIdx.x; n < ng.nn; n += (int64_t)gridDim.x * ND_THREADS) {
         const double m = gm[n];
+        if (SKIP && m == 0) continue;
         double o[3], xv[3];
         for (int k = 0; k < 3; ++k) {
             int64_t i = vidx<NPB>(n, k);
@@ -514,25 +511,71 @@ template <int NPB>
 __global__ void __launch_bounds__(ND_THREADS) k_apply_A(NodeGeom ng, const double* __restrict__ gm, const int8_t* __restrict__ col,
     const double* __restrict__ P6, double dt2, const double* __restrict__ xin, double* __restrict__ hacc, double* __restrict__ out)
 {
-    apply_A_body<NPB>(ng, gm, col, P6, dt2, xin, hacc, out, nullptr, 0);
+    apply_A_body<NPB, false>(ng, gm, col, P6, dt2, xin, hacc, out, nullptr, 0);
 }
 
-// Krylov form: MINRES qkp1 = project(A mk) with mk = Z[k&1], alpha partial
-// mk . qkp1; CG tmp = project(A p), partial tmp . p.
+// CG operator pass: tmp = project(A p), partial tmp . p.
 template <int NPB>
 __global__ void __launch_bounds__(ND_THREADS) k_apply_A_krylov(NodeGeom ng, const double* __restrict__ gm, const int8_t* __restrict__ col,
-    const double* __restrict__ P6, double dt2, KrylovBufs kb, int minres, double* __restrict__ part, const SolverScalars* __restrict__ sc)
+    const double* __restrict__ P6, double dt2, KrylovBufs kb, double* __restrict__ part, const SolverScalars* __restrict__ sc)
 {
     if (krylov_off(sc)) return;
-    const int k = sc->kit;
-    if (minres)
-        apply_A_body<NPB>(ng, gm, col, P6, dt2, sel2(kb.Z, k & 1), kb.hacc, sel3(kb.Q, (k + 1) % 3), part, 1);
-    else
-        apply_A_body<NPB>(ng, gm, col, P6, dt2, kb.p, kb.hacc, kb.tmp, part, 1);
+    apply_A_body<NPB, true>(ng, gm, col, P6, dt2, kb.p, kb.hacc, kb.tmp, part, 1);
+}
+
+// Ends a Krylov iteration (the next loop top's test, Minres.h:100,
+// ConjugateGradient.h:118): advances k, stops on the local tolerance or the
+// iteration cap; as a graph, sets the loop condition.  Run by one thread of
+// the last CTA of the iteration's last kernel, after every CTA read k.
+__device__ __forceinline__ void krylov_advance(SolverScalars* sc, int it, double rnorm, int kmax, cudaGraphConditionalHandle hK, int use_graph)
+{
+    sc->krylov_bodies += 1;
+    const int k = it + 1;
+    sc->kit = k;
+    const bool go = !(rnorm < sc->local_tol || k >= kmax);
+    if (!go) sc->kactive = 0;
+    if (use_graph) cudaGraphSetConditional(hK, go ? 1u : 0u);
+}
+
+// MINRES keeps its Lanczos vectors Q_j and preconditioned vectors Z_j
+// unnormalised (Minres.h:170-173 divides them by beta_j at the end of
+// iteration j - 1); every reader divides by beta_j, the same rounding as the
+// stored normalised vector.  beta_j = 0 leaves them as they are, as there.
+__device__ __forceinline__ double mr_norm(double v, double beta) { return beta > 0 ? v / beta : v; }
+
+// The search direction of iteration j = k - 1 (Minres.h:167-170):
+// M_j = (Z_j - delta M_{j-1} - epsilon M_{j-2}) / gamma, then x += t M_j.
+// k_mr_b computes its scalars; the vector update runs in the next operator
+// pass (k_mr_a) or, after the last iteration, where the solve's x is used.
+struct MrPending {
+    const double *z, *m1, *m2;
+    double* out;
+    double delta, eps, gamma, t, beta;
+    bool on;
+};
+__device__ __forceinline__ MrPending mr_pending(const KrylovBufs& kb, const SolverScalars* sc, int k)
+{
+    MrPending p;
+    p.on = k > 0;
+    p.z = sel2(kb.Z, (k + 1) & 1);   // Z_{k-1}, unnormalised
+    p.m1 = sel3(kb.M, (k + 1) % 3);  // M_{k-2}
+    p.m2 = sel3(kb.M, k % 3);        // M_{k-3}
+    p.out = sel3(kb.M, (k + 2) % 3); // M_{k-1}
+    p.delta = sc->pend[0];
+    p.eps = sc->pend[1];
+    p.gamma = sc->pend[2];
+    p.t = sc->pend[3];
+    p.beta = sc->pend[4];            // beta_{k-1}
+    return p;
+}
+__device__ __forceinline__ double mr_direction(const MrPending& p, int64_t i)
+{
+    return (mr_norm(p.z[i], p.beta) - p.delta * p.m1[i] - p.eps * p.m2[i]) / p.gamma;
 }
 
 // ---------------------------------------------------------------- CG ------
-// x += alpha p; r -= alpha tmp; q = r/m; partial q.r
+// x += alpha p; r -= alpha tmp; q = r/m; partial q.r.  The CG kernels skip
+// massless slots, which hold zeros in every vector from the solve's start.
 template <int NPB>
 __global__ void __launch_bounds__(ND_THREADS) k_cg_b(NodeGeom ng, const double* __restrict__ gm, KrylovBufs kb, const double* __restrict__ part_in,
     double* __restrict__ part_out, const SolverScalars* __restrict__ sc)
@@ -543,12 +586,13 @@ __global__ void __launch_bounds__(ND_THREADS) k_cg_b(NodeGeom ng, const double* 
     double acc = 0;
     for (int64_t n = (int64_t)blockIdx.x * ND_THREADS + threadIdx.x; n < ng.nn; n += (int64_t)gridDim.x * ND_THREADS) {
         const double m = gm[n];
+        if (m == 0) continue;
         for (int k = 0; k < 3; ++k) {
             int64_t i = vidx<NPB>(n, k);
             kb.x[i] += kb.p[i] * alpha;
             double r = kb.r[i] - kb.tmp[i] * alpha;
             kb.r[i] = r;
-            double q = (m != 0) ? r / kb.pre[n] : 0.0;
+            double q = r / kb.pre[n];
             kb.q[i] = q;
             acc += q * r;
         }
@@ -557,35 +601,82 @@ __global__ void __launch_bounds__(ND_THREADS) k_cg_b(NodeGeom ng, const double* 
     if (threadIdx.x == 0) part_out[blockIdx.x] = s;
 }
 
-// beta, p = q + beta p, residual norm
+// beta, p = q + beta p, residual norm; the last CTA ends the iteration.
 template <int NPB>
-__global__ void __launch_bounds__(ND_THREADS) k_cg_c(NodeGeom ng, KrylovBufs kb, const double* __restrict__ part_in, SolverScalars* __restrict__ sc)
+__global__ void __launch_bounds__(ND_THREADS) k_cg_c(NodeGeom ng, const double* __restrict__ gm, KrylovBufs kb, const double* __restrict__ part_in,
+    SolverScalars* __restrict__ sc, int kmax, cudaGraphConditionalHandle hK, int use_graph)
 {
     if (krylov_off(sc)) return;
     const int it = sc->kit, nit = sc->nit;
     const double zTrk = reduce_partials(part_in, ng.parts);
     const double beta = zTrk / sc->mr[it & 1][0];
     const double rnorm = sqrt(zTrk);
-    __syncthreads();
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        sc->mr[(it + 1) & 1][0] = zTrk;
-        sc->rnorm = rnorm;
-        sc->krylov_iters += 1;
-        sc->hvp_count += 1;
-        if (nit < 64) sc->kcount[nit] += 1;
-    }
-    for (int64_t n = (int64_t)blockIdx.x * ND_THREADS + threadIdx.x; n < ng.nn; n += (int64_t)gridDim.x * ND_THREADS)
+    for (int64_t n = (int64_t)blockIdx.x * ND_THREADS + threadIdx.x; n < ng.nn; n += (int64_t)gridDim.x * ND_THREADS) {
+        if (gm[n] == 0) continue;
         for (int k = 0; k < 3; ++k) {
             int64_t i = vidx<NPB>(n, k);
             kb.p[i] = kb.q[i] + beta * kb.p[i];
         }
+    }
+    if (!last_cta(&sc->ticket) || threadIdx.x != 0) return;
+    sc->mr[(it + 1) & 1][0] = zTrk;
+    sc->rnorm = rnorm;
+    sc->krylov_iters += 1;
+    sc->hvp_count += 1;
+    if (nit < 64) sc->kcount[nit] += 1;
+    krylov_advance(sc, it, rnorm, kmax, hK, use_graph);
 }
 
 // ------------------------------------------------------------- MINRES -----
-// qkp1 -= alpha qk + beta_k qkm1; z = qkp1/m; partial z.qkp1
+// Operator pass of iteration k: the deferred search direction and x update of
+// iteration k - 1; Z_k = Z~_k / beta_k and the Hessian product (which ran on
+// the unnormalised Z~_k, a linear map) scaled the same way; W = project(m Z_k
+// + dt^2 H Z_k) (BackwardEuler.h:322-351, Minres.h:116) into Q's slot k + 1;
+// hacc = 0; partial Z_k . W.  Massless slots hold zeros in every vector and
+// are skipped.
+template <int NPB>
+__global__ void __launch_bounds__(ND_THREADS) k_mr_a(NodeGeom ng, const double* __restrict__ gm, const int8_t* __restrict__ col,
+    const double* __restrict__ P6, double dt2, KrylovBufs kb, double* __restrict__ part, const SolverScalars* __restrict__ sc)
+{
+    if (krylov_off(sc)) return;
+    const int k = sc->kit;
+    const double* __restrict__ zk = sel2(kb.Z, k & 1);
+    double* __restrict__ w = sel3(kb.Q, (k + 1) % 3);
+    const MrPending pd = mr_pending(kb, sc, k);
+    const double beta = sc->mr[k & 1][MR_BETA_KP1];
+    double acc = 0;
+    for (int64_t n = (int64_t)blockIdx.x * ND_THREADS + threadIdx.x; n < ng.nn; n += (int64_t)gridDim.x * ND_THREADS) {
+        const double m = gm[n];
+        if (m == 0) continue;
+        double o[3], z[3];
+        for (int c = 0; c < 3; ++c) {
+            const int64_t i = vidx<NPB>(n, c);
+            if (pd.on) {
+                const double mv = mr_direction(pd, i);
+                pd.out[i] = mv;
+                kb.x[i] += pd.t * mv;
+            }
+            z[c] = mr_norm(zk[i], beta);
+            o[c] = m * z[c] + dt2 * mr_norm(kb.hacc[i], beta);
+            kb.hacc[i] = 0;
+        }
+        project3(col, P6, ng.nn, n, o);
+        for (int c = 0; c < 3; ++c) {
+            w[vidx<NPB>(n, c)] = o[c];
+            acc += o[c] * z[c];
+        }
+    }
+    const double s = block_sum(acc);
+    if (threadIdx.x == 0) part[blockIdx.x] = s;
+}
+
+// Lanczos step: Q~_{k+1} = W - alpha Q_k - beta_k Q_{k-1} (Q_j = Q~_j /
+// beta_j); Z~_{k+1} = Q~_{k+1} / pre; partial Z~_{k+1} . Q~_{k+1}.  The last
+// CTA then sums the partials, runs the Givens update of iteration k
+// (Minres.h:151-175) and ends the iteration.
 template <int NPB>
 __global__ void __launch_bounds__(ND_THREADS) k_mr_b(NodeGeom ng, const double* __restrict__ gm, KrylovBufs kb, const double* __restrict__ part_in,
-    double* __restrict__ part_out, SolverScalars* __restrict__ sc)
+    double* __restrict__ part_out, SolverScalars* __restrict__ sc, int kmax, cudaGraphConditionalHandle hK, int use_graph)
 {
     if (krylov_off(sc)) return;
     const int it = sc->kit;
@@ -595,49 +686,36 @@ __global__ void __launch_bounds__(ND_THREADS) k_mr_b(NodeGeom ng, const double* 
     double* __restrict__ zout = sel2(kb.Z, (it + 1) & 1);
     const double alpha = reduce_partials(part_in, ng.parts);
     const double beta_k = sc->mr[it & 1][MR_BETA_KP1];
+    const double beta_km1 = sc->mr[(it + 1) & 1][MR_BETA_KP1];
     double acc = 0;
     for (int64_t n = (int64_t)blockIdx.x * ND_THREADS + threadIdx.x; n < ng.nn; n += (int64_t)gridDim.x * ND_THREADS) {
         const double m = gm[n];
+        if (m == 0) continue;
+        const double pre = kb.pre[n];
         for (int k = 0; k < 3; ++k) {
             int64_t i = vidx<NPB>(n, k);
             double q = qkp1[i];
-            q -= alpha * qk[i];
-            q -= beta_k * qkm1[i];
+            q -= alpha * mr_norm(qk[i], beta_k);
+            q -= beta_k * mr_norm(qkm1[i], beta_km1);
             qkp1[i] = q;
-            double z = (m != 0) ? q / kb.pre[n] : 0.0;
+            double z = q / pre;
             zout[i] = z;
             acc += z * q;
         }
     }
     double s = block_sum(acc);
     if (threadIdx.x == 0) part_out[blockIdx.x] = s;
-    // alpha of this iteration, for the Givens update in k_mr_c
-    if (blockIdx.x == 0 && threadIdx.x == 0) sc->mr[(it + 1) & 1][MR_TK] = alpha;
-}
-
-// Givens update (Minres.h:151-175), normalisation, search direction and x.
-template <int NPB>
-__global__ void __launch_bounds__(ND_THREADS) k_mr_c(NodeGeom ng, KrylovBufs kb, const double* __restrict__ part_in, SolverScalars* __restrict__ sc)
-{
-    if (krylov_off(sc)) return;
-    const int it = sc->kit, nit = sc->nit;
-    double* __restrict__ qkp1 = sel3(kb.Q, (it + 1) % 3);
-    double* __restrict__ zout = sel2(kb.Z, (it + 1) & 1);
-    const double* __restrict__ zin = sel2(kb.Z, it & 1);
-    const double* __restrict__ mkm1 = sel3(kb.M, (it + 2) % 3);
-    const double* __restrict__ mkm2 = sel3(kb.M, (it + 1) % 3);
-    double* __restrict__ mk_out = sel3(kb.M, it % 3);
-    double* __restrict__ x = kb.x;
-    const double dz = reduce_partials(part_in, ng.parts);
+    if (!last_cta(&sc->ticket)) return;
+    const double dz = reduce_partials_l2(part_out, ng.parts);
+    if (threadIdx.x != 0) return;
+    const int nit = sc->nit;
     const double* cur = sc->mr[it & 1];
-    const double alpha_k = sc->mr[(it + 1) & 1][MR_TK];
-    const double beta_k = cur[MR_BETA_KP1];
     const double beta_kp1 = sqrt(dz > 0 ? dz : 0.0);
     // Gkm2 = Gkm1, Gkm1 = Gk
     double c2 = cur[MR_GC1], s2 = cur[MR_GS1], c1 = cur[MR_GC0], s1 = cur[MR_GS0];
     double e0 = c2 * 0 - s2 * beta_k, e1 = s2 * 0 + c2 * beta_k;
     const double epsilon = e0;
-    double d0 = c1 * e1 - s1 * alpha_k, d1 = s1 * e1 + c1 * alpha_k;
+    double d0 = c1 * e1 - s1 * alpha, d1 = s1 * e1 + c1 * alpha;
     const double delta = d0;
     double t0 = d1, t1 = beta_kp1;
     double c0 = 1, s0 = 0;
@@ -655,63 +733,44 @@ __global__ void __launch_bounds__(ND_THREADS) k_mr_c(NodeGeom ng, KrylovBufs kb,
     const double tk = c0 * r0 - s0 * r1;
     const double residual = s0 * r0 + c0 * r1;
     const double rnorm = residual < 0 ? -residual : residual;
-    __syncthreads();
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        double* nx = sc->mr[(it + 1) & 1];
-        nx[MR_GC0] = c0;
-        nx[MR_GS0] = s0;
-        nx[MR_GC1] = c1;
-        nx[MR_GS1] = s1;
-        nx[MR_GC2] = c2;
-        nx[MR_GS2] = s2;
-        nx[MR_RHS0] = residual;
-        nx[MR_RHS1] = 0;
-        nx[MR_BETA_KP1] = beta_kp1;
-        sc->rnorm = rnorm;
-        sc->krylov_iters += 1;
-        sc->hvp_count += 1;
-        if (nit < 64) sc->kcount[nit] += 1;
-    }
-    const bool norm = beta_kp1 > 0;
-    for (int64_t n = (int64_t)blockIdx.x * ND_THREADS + threadIdx.x; n < ng.nn; n += (int64_t)gridDim.x * ND_THREADS)
-        for (int k = 0; k < 3; ++k) {
-            int64_t i = vidx<NPB>(n, k);
-            if (norm) {
-                qkp1[i] /= beta_kp1;
-                zout[i] /= beta_kp1;
-            }
-            double mk = (zin[i] - delta * mkm1[i] - epsilon * mkm2[i]) / gamma;
-            mk_out[i] = mk;
-            x[i] += tk * mk;
-        }
+    double* nx = sc->mr[(it + 1) & 1];
+    nx[MR_GC0] = c0;
+    nx[MR_GS0] = s0;
+    nx[MR_GC1] = c1;
+    nx[MR_GS1] = s1;
+    nx[MR_GC2] = c2;
+    nx[MR_GS2] = s2;
+    nx[MR_RHS0] = residual;
+    nx[MR_RHS1] = 0;
+    nx[MR_BETA_KP1] = beta_kp1;
+    sc->pend[0] = delta;
+    sc->pend[1] = epsilon;
+    sc->pend[2] = gamma;
+    sc->pend[3] = tk;
+    sc->pend[4] = beta_k;
+    sc->rnorm = rnorm;
+    sc->krylov_iters += 1;
+    sc->hvp_count += 1;
+    if (nit < 64) sc->kcount[nit] += 1;
+    krylov_advance(sc, it, rnorm, kmax, hK, use_graph);
 }
 
-// Ends a Krylov iteration: advances k and applies the convergence test of the
-// next loop top (Minres.h:100, ConjugateGradient.h:118); as a graph, sets the
-// loop condition.  A separate one-thread kernel so that no kernel both reads
-// and updates k.
-__global__ void k_krylov_advance(SolverScalars* __restrict__ sc, int kmax, cudaGraphConditionalHandle hK, int use_graph)
-{
-    sc->krylov_bodies += 1;
-    if (!sc->newton_done && sc->kactive) {
-        const int k = sc->kit + 1;
-        sc->kit = k;
-        if (sc->rnorm < sc->local_tol || k >= kmax) sc->kactive = 0;
-    }
-    if (use_graph) cudaGraphSetConditional(hK, (!sc->newton_done && sc->kactive) ? 1u : 0u);
-}
-
-// dv += step; vstar = vn + dv on active nodes.
+// dv += x (the linear solve's step, with MINRES's deferred last update);
+// vstar = vn + dv on active nodes.
 template <int NPB>
-__global__ void __launch_bounds__(ND_THREADS) k_newton_step(NodeGeom ng, const double* __restrict__ gm, const double* __restrict__ step,
+__global__ void __launch_bounds__(ND_THREADS) k_newton_step(NodeGeom ng, const double* __restrict__ gm, KrylovBufs kb, int minres,
     const double* __restrict__ vn, double* __restrict__ dv, double* __restrict__ vstar, const SolverScalars* __restrict__ sc)
 {
     if (sc->newton_done) return;
+    MrPending pd = mr_pending(kb, sc, sc->kit);
+    pd.on = pd.on && minres;
     for (int64_t n = (int64_t)blockIdx.x * ND_THREADS + threadIdx.x; n < ng.nn; n += (int64_t)gridDim.x * ND_THREADS) {
         const bool act = gm[n] != 0;
         for (int k = 0; k < 3; ++k) {
             int64_t i = vidx<NPB>(n, k);
-            double d = dv[i] + step[i];
+            double step = kb.x[i];
+            if (pd.on) step += pd.t * mr_direction(pd, i);
+            double d = dv[i] + step;
             dv[i] = d;
             vstar[i] = act ? vn[i] + d : 0.0;
         }
@@ -809,6 +868,7 @@ __global__ void __launch_bounds__(ND_THREADS) k_admm_start(NodeGeom ng, const do
             kb.M[1][i] = 0;
             kb.M[2][i] = 0;
             kb.Z[0][i] = z;
+            kb.Z[1][i] = 0;
             acc += z * r[k];
         }
     }
@@ -816,16 +876,20 @@ __global__ void __launch_bounds__(ND_THREADS) k_admm_start(NodeGeom ng, const do
     if (threadIdx.x == 0) part[blockIdx.x] = t;
 }
 
-// dv += x (the MINRES correction); vstar = vn + dv on active nodes.
+// dv += x (the MINRES correction, with its deferred last update); vstar =
+// vn + dv on active nodes.
 template <int NPB>
-__global__ void __launch_bounds__(ND_THREADS) k_admm_dv_update(NodeGeom ng, const double* __restrict__ gm, const double* __restrict__ x,
-    const double* __restrict__ vn, double* __restrict__ dv, double* __restrict__ vstar)
+__global__ void __launch_bounds__(ND_THREADS) k_admm_dv_update(NodeGeom ng, const double* __restrict__ gm, KrylovBufs kb,
+    const double* __restrict__ vn, double* __restrict__ dv, double* __restrict__ vstar, const SolverScalars* __restrict__ sc)
 {
+    const MrPending pd = mr_pending(kb, sc, sc->kit);
     for (int64_t n = (int64_t)blockIdx.x * ND_THREADS + threadIdx.x; n < ng.nn; n += (int64_t)gridDim.x * ND_THREADS) {
         const bool act = gm[n] != 0;
         for (int k = 0; k < 3; ++k) {
             const int64_t i = vidx<NPB>(n, k);
-            const double d = dv[i] + x[i];
+            double x = kb.x[i];
+            if (pd.on) x += pd.t * mr_direction(pd, i);
+            const double d = dv[i] + x;
             dv[i] = d;
             vstar[i] = act ? vn[i] + d : 0.0;
         }
@@ -1054,7 +1118,7 @@ int launch_newton_head(const NewtonLaunch& L, cudaStream_t st, cudaGraphConditio
     if (rc) return rc;
     k_newton_check<NPB><<<L.nb, ND_THREADS, 0, st>>>(L.ng, ctx->gm.as<double>(), ctx->res.as<double>(), L.kb, L.np, L.pA, L.pB, L.sc);
     ++g_kernel_launches;
-    k_krylov_start<NPB><<<L.nb, ND_THREADS, 0, st>>>(L.ng, L.kb, L.np, L.pB, L.sc, hK, use_graph);
+    k_krylov_start<NPB><<<1, ND_THREADS, 0, st>>>(L.ng, L.kb, L.np, L.pB, L.sc, hK, use_graph);
     ++g_kernel_launches;
     return ZMPM_OK;
 }
@@ -1070,20 +1134,19 @@ int launch_krylov_iteration(const NewtonLaunch& L, cudaStream_t st, cudaGraphCon
     else
         launch_hvp_krylov(ctx, L.kb.p, L.kb.p, false, L.kb.hacc);
     if (e1) ZMPM_CUDA(cudaEventRecord(e1, st));
-    k_apply_A_krylov<NPB><<<L.nb, ND_THREADS, 0, st>>>(L.ng, ctx->gm.as<double>(), ctx->collided.as<int8_t>(), ctx->proj.as<double>(), L.dt2, L.kb,
-        L.np.minres, L.pA, L.sc);
-    ++g_kernel_launches;
     if (L.np.minres) {
-        k_mr_b<NPB><<<L.nb, ND_THREADS, 0, st>>>(L.ng, ctx->gm.as<double>(), L.kb, L.pA, L.pC, L.sc);
-        k_mr_c<NPB><<<L.nb, ND_THREADS, 0, st>>>(L.ng, L.kb, L.pC, L.sc);
+        k_mr_a<NPB><<<L.nb, ND_THREADS, 0, st>>>(L.ng, ctx->gm.as<double>(), ctx->collided.as<int8_t>(), ctx->proj.as<double>(), L.dt2, L.kb,
+            L.pA, L.sc);
+        k_mr_b<NPB><<<L.nb, ND_THREADS, 0, st>>>(L.ng, ctx->gm.as<double>(), L.kb, L.pA, L.pC, L.sc, L.np.kmax, hK, use_graph);
+        g_kernel_launches += 2;
     }
     else {
+        k_apply_A_krylov<NPB><<<L.nb, ND_THREADS, 0, st>>>(L.ng, ctx->gm.as<double>(), ctx->collided.as<int8_t>(), ctx->proj.as<double>(), L.dt2,
+            L.kb, L.pA, L.sc);
         k_cg_b<NPB><<<L.nb, ND_THREADS, 0, st>>>(L.ng, ctx->gm.as<double>(), L.kb, L.pA, L.pC, L.sc);
-        k_cg_c<NPB><<<L.nb, ND_THREADS, 0, st>>>(L.ng, L.kb, L.pC, L.sc);
+        k_cg_c<NPB><<<L.nb, ND_THREADS, 0, st>>>(L.ng, ctx->gm.as<double>(), L.kb, L.pC, L.sc, L.np.kmax, hK, use_graph);
+        g_kernel_launches += 3;
     }
-    g_kernel_launches += 2;
-    k_krylov_advance<<<1, 1, 0, st>>>(L.sc, L.np.kmax, hK, use_graph);
-    ++g_kernel_launches;
     return ZMPM_OK;
 }
 
@@ -1091,7 +1154,7 @@ template <int NPB>
 int launch_newton_tail(const NewtonLaunch& L, cudaStream_t st, cudaGraphConditionalHandle hN, int use_graph)
 {
     Ctx* ctx = L.ctx;
-    k_newton_step<NPB><<<L.nb, ND_THREADS, 0, st>>>(L.ng, ctx->gm.as<double>(), L.kb.x, ctx->vn.as<double>(), ctx->dv.as<double>(),
+    k_newton_step<NPB><<<L.nb, ND_THREADS, 0, st>>>(L.ng, ctx->gm.as<double>(), L.kb, L.np.minres, ctx->vn.as<double>(), ctx->dv.as<double>(),
         ctx->vstar.as<double>(), L.sc);
     k_newton_advance<<<1, 1, 0, st>>>(L.sc, L.np.nmax, hN, use_graph);
     g_kernel_launches += 2;
@@ -1363,24 +1426,22 @@ static int admm_impl(Ctx* ctx, const zmpm_solver& s)
         if (r) return r;
         k_admm_start<NPB><<<Lc.nb, ND_THREADS, 0, sm>>>(Lc.ng, ctx->gm.as<double>(), ctx->collided.as<int8_t>(), ctx->proj.as<double>(),
             ctx->adm_rhs.as<double>(), ctx->dv.as<double>(), kb, Lc.pB, Lc.sc);
-        k_krylov_start<NPB><<<Lc.nb, ND_THREADS, 0, sm>>>(Lc.ng, kb, Lc.np, Lc.pB, Lc.sc, hK, ug);
+        k_krylov_start<NPB><<<1, ND_THREADS, 0, sm>>>(Lc.ng, kb, Lc.np, Lc.pB, Lc.sc, hK, ug);
         g_kernel_launches += 2;
         return (int)ZMPM_OK;
     };
     auto body = [&](cudaStream_t sm, cudaGraphConditionalHandle hK, int ug) {
         int r = launch_admm_op(ctx, kb.Z[0], kb.Z[1], true, kb.hacc, true);
         if (r) return r;
-        k_apply_A_krylov<NPB><<<Lc.nb, ND_THREADS, 0, sm>>>(Lc.ng, ctx->gm.as<double>(), ctx->collided.as<int8_t>(), ctx->proj.as<double>(),
-            1.0, kb, 1, Lc.pA, Lc.sc);
-        k_mr_b<NPB><<<Lc.nb, ND_THREADS, 0, sm>>>(Lc.ng, ctx->gm.as<double>(), kb, Lc.pA, Lc.pC, Lc.sc);
-        k_mr_c<NPB><<<Lc.nb, ND_THREADS, 0, sm>>>(Lc.ng, kb, Lc.pC, Lc.sc);
-        k_krylov_advance<<<1, 1, 0, sm>>>(Lc.sc, Lc.np.kmax, hK, ug);
-        g_kernel_launches += 4;
+        k_mr_a<NPB><<<Lc.nb, ND_THREADS, 0, sm>>>(Lc.ng, ctx->gm.as<double>(), ctx->collided.as<int8_t>(), ctx->proj.as<double>(), 1.0, kb,
+            Lc.pA, Lc.sc);
+        k_mr_b<NPB><<<Lc.nb, ND_THREADS, 0, sm>>>(Lc.ng, ctx->gm.as<double>(), kb, Lc.pA, Lc.pC, Lc.sc, Lc.np.kmax, hK, ug);
+        g_kernel_launches += 2;
         return (int)ZMPM_OK;
     };
     auto tail = [&](cudaStream_t sm, cudaGraphConditionalHandle hN, int ug) {
-        k_admm_dv_update<NPB><<<Lc.nb, ND_THREADS, 0, sm>>>(Lc.ng, ctx->gm.as<double>(), kb.x, ctx->vn.as<double>(), ctx->dv.as<double>(),
-            ctx->vstar.as<double>());
+        k_admm_dv_update<NPB><<<Lc.nb, ND_THREADS, 0, sm>>>(Lc.ng, ctx->gm.as<double>(), kb, ctx->vn.as<double>(), ctx->dv.as<double>(),
+            ctx->vstar.as<double>(), Lc.sc);
         ++g_kernel_launches;
         int r = launch_admm_dual(ctx, rho);
         if (r) return r;
@@ -1473,12 +1534,12 @@ int run_adjoint_solve(Ctx* ctx, double tol, int max_iterations)
         if (l244) {
             k_adj_cg_init<32><<<Lc.nb, ND_THREADS, 0, sm>>>(Lc.ng, ctx->gm.as<double>(), ctx->collided.as<int8_t>(), ctx->proj.as<double>(),
                 ctx->res.as<double>(), kb, tol, Lc.pB, Lc.sc);
-            k_krylov_start<32><<<Lc.nb, ND_THREADS, 0, sm>>>(Lc.ng, kb, Lc.np, Lc.pB, Lc.sc, hK, ug);
+            k_krylov_start<32><<<1, ND_THREADS, 0, sm>>>(Lc.ng, kb, Lc.np, Lc.pB, Lc.sc, hK, ug);
         }
         else {
             k_adj_cg_init<64><<<Lc.nb, ND_THREADS, 0, sm>>>(Lc.ng, ctx->gm.as<double>(), ctx->collided.as<int8_t>(), ctx->proj.as<double>(),
                 ctx->res.as<double>(), kb, tol, Lc.pB, Lc.sc);
-            k_krylov_start<64><<<Lc.nb, ND_THREADS, 0, sm>>>(Lc.ng, kb, Lc.np, Lc.pB, Lc.sc, hK, ug);
+            k_krylov_start<64><<<1, ND_THREADS, 0, sm>>>(Lc.ng, kb, Lc.np, Lc.pB, Lc.sc, hK, ug);
         }
         g_kernel_launches += 2;
         return (int)ZMPM_OK;
@@ -1504,10 +1565,10 @@ int run_adjoint_solve(Ctx* ctx, double tol, int max_iterations)
         cudaGraphExecDestroy(exec);
         ZMPM_CUDA(e);
         ZMPM_CUDA(e2);
-        // kernels executed: head (2) and tail (1) once, 6 per Krylov body
+        // kernels executed: head (2) and tail (1) once, 5 per Krylov body (CG)
         SolverScalars hs;
         ZMPM_CUDA(cudaMemcpy(&hs, Lc.sc, sizeof(hs), cudaMemcpyDeviceToHost));
-        g_kernel_launches = launches0 + 3 + 6 * (int64_t)hs.krylov_bodies;
+        g_kernel_launches = launches0 + 3 + 5 * (int64_t)hs.krylov_bodies;
     }
     else {
         int rc = head(st, 0, 0);
