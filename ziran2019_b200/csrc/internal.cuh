@@ -183,6 +183,7 @@ struct Ctx {
     DBuf gm, gmv, vn, dv, vstar, facc, res, proj, collided, node_idx;
     // Krylov vectors
     DBuf kv[10];
+    DBuf kvf;                             // FP32 copies of MINRES's two Z vectors ([2][B][3][NPB]), read by the FP32 product
     DBuf red;                             // reduction partials [4][RED_MAX_CTAS]
     DBuf scal;                            // SolverScalars
     DBuf counters;                        // DevCounters
@@ -238,6 +239,8 @@ int launch_adj_particle(Ctx* ctx, const double* lam);  // adjoint of the force t
 int run_adjoint_solve(Ctx* ctx, double tol, int max_iterations); // (M + dt^2 K) lambda = P dL/dv*
 int launch_residual(Ctx* ctx);                         // r = dt m g + dt f - m dv (projected), norm partials
 int launch_hvp(Ctx* ctx, const double* x, double* out, bool fp32); // out += dt^2 K x (no inertia)
+// FP32 product inside the MINRES loop of a MIXED context, on the FP32 copies x0 / x1 (even / odd iterations)
+int launch_hvp_krylov_f32(Ctx* ctx, const float* x0, const float* x1, double* out);
 int launch_damage(Ctx* ctx);                           // Rankine damage after P2G
 int run_admm(Ctx* ctx, const zmpm_solver& s);         // AdmmSimulation::admmStep
 // particle kernels of the ADMM substep (admm.cu)

@@ -368,6 +368,7 @@ __global__ void __launch_bounds__(ND_THREADS) k_residual(NodeGeom ng, const doub
 struct KrylovBufs {
     double *x, *r, *p, *q, *tmp;      // CG
     double *Q[3], *M[3], *Z[2];       // MINRES
+    float* Zf[2];                     // FP32 copies of Z for the FP32 product (MIXED MINRES), or null
     double* hacc;                     // Hessian accumulator
     const double* pre;                // diagonal preconditioner per node (the mass for Newton)
 };
@@ -382,7 +383,8 @@ __device__ __forceinline__ bool krylov_off(const SolverScalars* sc) { return sc-
 // Role selection by iteration index without indexing the parameter arrays at
 // run time (which would copy the kernel parameters to local memory).
 __device__ __forceinline__ double* sel3(double* const (&a)[3], int i) { return i == 0 ? a[0] : (i == 1 ? a[1] : a[2]); }
-__device__ __forceinline__ double* sel2(double* const (&a)[2], int i) { return i == 0 ? a[0] : a[1]; }
+template <class T>
+__device__ __forceinline__ T* sel2(T* const (&a)[2], int i) { return i == 0 ? a[0] : a[1]; }
 
 // Newton check (NewtonsMethod.h:48-61) + start of the linear solve: x = 0,
 // CG: r = res, q = r/m, p = q, partial r.q;  MINRES: Q0 = res, Z0 = res/m,
@@ -426,6 +428,10 @@ __global__ void __launch_bounds__(ND_THREADS) k_newton_check(NodeGeom ng, const 
                 kb.M[2][i] = 0;
                 kb.Z[0][i] = z;
                 kb.Z[1][i] = 0;
+                if (kb.Zf[0]) {
+                    kb.Zf[0][i] = (float)z;
+                    kb.Zf[1][i] = 0;
+                }
             }
             else {
                 kb.r[i] = rv;
@@ -671,7 +677,8 @@ __global__ void __launch_bounds__(ND_THREADS) k_mr_a(NodeGeom ng, const double* 
 }
 
 // Lanczos step: Q~_{k+1} = W - alpha Q_k - beta_k Q_{k-1} (Q_j = Q~_j /
-// beta_j); Z~_{k+1} = Q~_{k+1} / pre; partial Z~_{k+1} . Q~_{k+1}.  The last
+// beta_j); Z~_{k+1} = Q~_{k+1} / pre (and its FP32 copy for the MIXED
+// product); partial Z~_{k+1} . Q~_{k+1}.  The last
 // CTA then sums the partials, runs the Givens update of iteration k
 // (Minres.h:151-175) and ends the iteration.
 template <int NPB>
@@ -684,6 +691,7 @@ __global__ void __launch_bounds__(ND_THREADS) k_mr_b(NodeGeom ng, const double* 
     const double* __restrict__ qk = sel3(kb.Q, it % 3);
     const double* __restrict__ qkm1 = sel3(kb.Q, (it + 2) % 3);
     double* __restrict__ zout = sel2(kb.Z, (it + 1) & 1);
+    float* __restrict__ zfout = sel2(kb.Zf, (it + 1) & 1);
     const double alpha = reduce_partials(part_in, ng.parts);
     const double beta_k = sc->mr[it & 1][MR_BETA_KP1];
     const double beta_km1 = sc->mr[(it + 1) & 1][MR_BETA_KP1];
@@ -700,6 +708,7 @@ __global__ void __launch_bounds__(ND_THREADS) k_mr_b(NodeGeom ng, const double* 
             qkp1[i] = q;
             double z = q / pre;
             zout[i] = z;
+            if (zfout) zfout[i] = (float)z;
             acc += z * q;
         }
     }
@@ -967,6 +976,7 @@ int ensure_node_buffers(Ctx* ctx)
     ZMPM_CUDA(ctx->proj.ensure(6 * nn * sizeof(double)));
     ZMPM_CUDA(ctx->collided.ensure(nn));
     for (int i = 0; i < 10; ++i) ZMPM_CUDA(ctx->kv[i].ensure(vec));
+    ZMPM_CUDA(ctx->kvf.ensure((size_t)(6 * nn) * sizeof(float)));
     return ZMPM_OK;
 }
 
@@ -1129,7 +1139,9 @@ int launch_krylov_iteration(const NewtonLaunch& L, cudaStream_t st, cudaGraphCon
 {
     Ctx* ctx = L.ctx;
     if (e0) ZMPM_CUDA(cudaEventRecord(e0, st));
-    if (L.np.minres)
+    if (L.np.minres && L.kb.Zf[0])
+        launch_hvp_krylov_f32(ctx, L.kb.Zf[0], L.kb.Zf[1], L.kb.hacc);
+    else if (L.np.minres)
         launch_hvp_krylov(ctx, L.kb.Z[0], L.kb.Z[1], true, L.kb.hacc);
     else
         launch_hvp_krylov(ctx, L.kb.p, L.kb.p, false, L.kb.hacc);
@@ -1279,6 +1291,10 @@ static int newton_impl(Ctx* ctx, const zmpm_solver& s)
     L.kb.hacc = ctx->kv[9].as<double>();
     L.kb.pre = ctx->gm.as<double>();
     L.np.minres = s.linear_solver == ZMPM_MINRES ? 1 : 0;
+    // MIXED MINRES runs its split FP32 product on FP32 copies of Z
+    const bool zf = ctx->mixed && L.np.minres && !ctx->hvp_fused;
+    L.kb.Zf[0] = zf ? ctx->kvf.as<float>() : nullptr;
+    L.kb.Zf[1] = zf ? ctx->kvf.as<float>() + 3 * L.ng.nn : nullptr;
     L.np.kmax = s.krylov_max_iterations;
     L.np.nmax = s.newton_max_iterations;
     L.np.tol = s.newton_tolerance;
@@ -1377,6 +1393,7 @@ static int admm_impl(Ctx* ctx, const zmpm_solver& s)
     kb.M[2] = ctx->kv[6].as<double>();
     kb.Z[0] = ctx->kv[7].as<double>();
     kb.Z[1] = ctx->kv[8].as<double>();
+    kb.Zf[0] = kb.Zf[1] = nullptr;
     kb.hacc = ctx->kv[9].as<double>();
     kb.pre = ctx->adm_pre.as<double>();
     Lc.np.minres = 1;
@@ -1515,6 +1532,7 @@ int run_adjoint_solve(Ctx* ctx, double tol, int max_iterations)
     kb.tmp = ctx->kv[4].as<double>();
     for (int k = 0; k < 3; ++k) kb.Q[k] = kb.M[k] = nullptr;
     kb.Z[0] = kb.Z[1] = nullptr;
+    kb.Zf[0] = kb.Zf[1] = nullptr;
     kb.hacc = ctx->kv[9].as<double>();
     kb.pre = ctx->gm.as<double>();
     Lc.np.minres = 0;

@@ -447,22 +447,24 @@ __global__ void __launch_bounds__(XF_THREADS, sizeof(TH) == 4 ? 4 : 2) k_hvp(con
 // the HVP precision): k_hvp_stress gathers grad(x) and evaluates dS in slot
 // order; k_hvp_scatter adds dS grad w with the layered scatter.  Each half
 // holds far fewer live registers than the fused kernel.
-template <class L, class TH>
+// TX: the input vector's type (FP64, or the FP32 copy MINRES keeps for MIXED
+// products, which halves the staged window and needs no conversions).
+template <class L, class TH, class TX = double>
 __global__ void __launch_bounds__(XF_THREADS) k_hvp_stress(const int32_t* __restrict__ group_start, const int32_t* __restrict__ group_nbr,
     const int32_t* __restrict__ pi, int64_t cap, const short4* __restrict__ base, double dx, const TH* __restrict__ frac,
-    const TH* __restrict__ scr, const double* __restrict__ x0, const double* __restrict__ x1, int alt, TH* __restrict__ dstress,
+    const TH* __restrict__ scr, const TX* __restrict__ x0, const TX* __restrict__ x1, int alt, TH* __restrict__ dstress,
     const SolverScalars* __restrict__ sc, int32_t* __restrict__ flags)
 {
     if (sc && (sc->newton_done || !sc->kactive)) return;
     constexpr int NPB = L::NPB;
-    __shared__ __align__(128) double win[8 * 3 * NPB];
+    __shared__ __align__(128) TX win[8 * 3 * NPB];
     __shared__ int32_t nbr[8];
     __shared__ __align__(8) uint64_t bar;
     const int g = blockIdx.x;
     if (threadIdx.x < 8) nbr[threadIdx.x] = group_nbr[8 * g + threadIdx.x];
     __syncthreads();
     // the input alternates between x0 and x1 with the Krylov iteration (MINRES)
-    const double* x = (alt && sc && (sc->kit & 1)) ? x1 : x0;
+    const TX* x = (alt && sc && (sc->kit & 1)) ? x1 : x0;
     stage_window<NPB>(win, x, nbr, &bar, flags);
     const TH inv_dx = TH(1.0 / dx);
     const int s0 = group_start[g], s1 = group_start[g + 1];
@@ -480,7 +482,7 @@ __global__ void __launch_bounds__(XF_THREADS) k_hvp_stress(const int32_t* __rest
         const int lx = b.x & (L::BX - 1), ly = b.y & (L::BY - 1), lz = b.z & (L::BZ - 1);
         M3<TH> G = m3_zero<TH>();
         for_stencil<L>(lx, ly, lz, w, dwr, inv_dx, [&](int t, int e, int, int, int, TH, const TH* dw) {
-            const double* vv = win + t * 3 * NPB + e;
+            const TX* vv = win + t * 3 * NPB + e;
 #pragma unroll
             for (int r = 0; r < 3; ++r) {
                 TH vr = (TH)vv[r * NPB];
@@ -764,6 +766,27 @@ static int hvp_impl(Ctx* ctx, const double* x0, const double* x1, int alt, doubl
     else
         hvp_launch<L, double>(ctx, x0, x1, alt, out, sc);
     return ZMPM_OK;
+}
+
+template <class L>
+static int hvp_f32_impl(Ctx* ctx, const float* x0, const float* x1, double* out)
+{
+    const int64_t G = ctx->G;
+    if (G == 0) return ZMPM_OK;
+    const SolverScalars* sc = ctx->scal.as<SolverScalars>();
+    DevCounters* dc = ctx->counters.as<DevCounters>();
+    k_hvp_stress<L, float, float><<<(unsigned)G, XF_THREADS, 0, ctx->stream>>>(ctx->group_start.as<int32_t>(), ctx->group_nbr.as<int32_t>(),
+        ctx->pi.as<int32_t>(), ctx->Pcap, ctx->base.as<short4>(), ctx->cfg.dx, ctx->frac.as<float>(), ctx->scratch.as<float>(), x0, x1, 1,
+        ctx->dstress.as<float>(), sc, &dc->flags);
+    ++g_kernel_launches;
+    k_hvp_scatter<L, float><<<(unsigned)G, XF_THREADS, 0, ctx->stream>>>(ctx->group_start.as<int32_t>(), ctx->group_nbr.as<int32_t>(), ctx->Pcap,
+        ctx->base.as<short4>(), ctx->cfg.dx, ctx->frac.as<float>(), ctx->dstress.as<float>(), out, sc);
+    ++g_kernel_launches;
+    return ZMPM_OK;
+}
+int launch_hvp_krylov_f32(Ctx* ctx, const float* x0, const float* x1, double* out)
+{
+    return ctx->layout == 1 ? hvp_f32_impl<Layout244>(ctx, x0, x1, out) : hvp_f32_impl<Layout444>(ctx, x0, x1, out);
 }
 
 // Product inside the Newton solve: gated by the solver scalars; with alt the

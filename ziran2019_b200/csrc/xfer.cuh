@@ -60,12 +60,15 @@ __device__ __forceinline__ void mbar_wait_bounded(uint64_t* bar, uint32_t parity
     }
 }
 
-// Stages the 8 page slabs ([3][NPB] doubles each) of vector `vec` into win.
-// Must be called by all threads of the CTA; nbr is in shared memory.
-template <int NPB>
-__device__ __forceinline__ void stage_window(double* win, const double* __restrict__ vec, const int32_t* nbr, uint64_t* bar, int32_t* flags)
+// Stages the 8 page slabs ([3][NPB] values each) of vector `vec` into win.
+// Must be called by all threads of the CTA; nbr is in shared memory.  A slab
+// is 3 NPB doubles or floats: a multiple of 16 bytes at a 16-byte aligned
+// offset for NPB = 32 or 64.
+template <int NPB, class T>
+__device__ __forceinline__ void stage_window(T* win, const T* __restrict__ vec, const int32_t* nbr, uint64_t* bar, int32_t* flags)
 {
-    constexpr uint32_t SLAB = 3 * NPB * sizeof(double);
+    constexpr uint32_t SLAB = 3 * NPB * sizeof(T);
+    static_assert(SLAB % 16 == 0, "bulk copies move multiples of 16 bytes");
     if (threadIdx.x == 0) {
         mbar_init(bar, 1);
         mbar_expect_tx(bar, 8 * SLAB);
