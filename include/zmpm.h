@@ -207,7 +207,7 @@ typedef struct zmpm_stats {
     int32_t hvp_timed;           /* number of products in ms_hvp */
     int32_t kernel_launches;     /* CUDA kernels this library launched for the substep */
     int32_t phase_field_iterations; /* CG iterations of the phase-field solve (its `iterations` return) */
-    int32_t pad2;
+    int32_t fp64_residual;       /* MIXED: 1 if the Newton residual went to FP64 after the FP32 one stalled */
     double phase_field_residual; /* final |r|_2 of the phase-field CG */
 } zmpm_stats;
 

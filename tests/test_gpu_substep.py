@@ -65,6 +65,23 @@ def test_mixed_precision_tracks_fp64_oracle(cuda_lib, oracle, kind):
     assert rel(pg["V"], po["V"]) < 1e-3
 
 
+@pytest.mark.parametrize("kind", ["fcr", "hencky"])
+@pytest.mark.parametrize("solver", ["minres", "cg"])
+def test_mixed_reaches_tolerance_below_fp32_floor(cuda_lib, oracle, kind, solver):
+    """MIXED with a Newton tolerance below the FP32 round-off of the force: the
+    FP32-evaluated residual stops falling, the solve switches to the FP64
+    residual (the Hessian products stay FP32) and converges, so the state
+    agrees with the FP64 oracle to the tolerance rather than to FP32 noise."""
+    (g, o), (sg, so) = run_pair(oracle, kind, solver, steps=4, precision="mixed", tol=1e-11, newton_max=20, kmax=200)
+    assert all(st["newton_converged"] == 1 for st in sg), [st["newton_residual_final"] for st in sg]
+    assert all(st["newton_residual_final"] < 1e-11 for st in sg)
+    assert all(st["newton_converged"] == 1 for st in so)
+    assert any(st["fp64_residual"] == 1 for st in sg)
+    pg, po = g.getParticles(), o.getParticles()
+    assert rel(pg["X"], po["X"]) < 1e-11
+    assert rel(pg["V"], po["V"]) < 1e-7
+
+
 def test_walls_and_free_particles(cuda_lib, oracle):
     dx = 1.0 / 64
     sims = [mpm.MpmSimulation(dx, gravity=(0, -9.8, 0), precision="fp64", grid_log2=8),

@@ -110,7 +110,7 @@ class Stats(C.Structure):
         ("hvp_timed", C.c_int32),
         ("kernel_launches", C.c_int32),
         ("phase_field_iterations", C.c_int32),
-        ("pad2", C.c_int32),
+        ("fp64_residual", C.c_int32),
         ("phase_field_residual", C.c_double),
     ]
 

@@ -903,6 +903,11 @@ static int64_t krylov_body_launches(const zmpm_ctx* ctx, const zmpm_solver& s)
     return (ctx->hvp_fused ? 1 : 2) + (s.linear_solver == ZMPM_MINRES ? 2 : 3);
 }
 
+// Kernels of one Newton loop body outside the Krylov loop: stress and force
+// (MIXED: an FP32 and an FP64 pair, one of which returns at once), residual,
+// check, Krylov start, step, advance.
+static int64_t newton_body_launches(const zmpm_ctx* ctx) { return ctx->mixed ? 9 : 7; }
+
 static int begin_implicit_impl(zmpm_ctx* ctx, double dt, bool damage = true)
 {
     int rc = upload(ctx);
@@ -1023,10 +1028,11 @@ int zmpm_substep(zmpm_ctx* ctx, double dt, const zmpm_solver* s, zmpm_stats* st)
     st->ms_total = ms;
     st->phase_field_iterations = ctx->pf_iters;
     st->phase_field_residual = ctx->pf_res;
+    st->fp64_residual = hs.fp64_res;
     if (ctx->graph_used && admm) // ADMM iteration: 7 head + 3 tail kernels; Krylov body: operator (2), k_mr_a, k_mr_b
         g_kernel_launches += 10 * (int64_t)hs.nit + 4 * (int64_t)hs.krylov_bodies;
-    else if (ctx->graph_used) // Newton body: stress, force, residual, check, start, step, advance
-        g_kernel_launches += 7 * (int64_t)hs.nit + krylov_body_launches(ctx, *s) * (int64_t)hs.krylov_bodies;
+    else if (ctx->graph_used)
+        g_kernel_launches += newton_body_launches(ctx) * (int64_t)hs.nit + krylov_body_launches(ctx, *s) * (int64_t)hs.krylov_bodies;
     st->kernel_launches = (int32_t)(g_kernel_launches - launches0);
     ctx->N = hc.N;
     if (ctx->prof_newton > 0) {
@@ -1116,9 +1122,11 @@ int zmpm_adjoint_substep(zmpm_ctx* ctx, double dt, const zmpm_solver* s, double 
         cudaGraphExecDestroy(ctx->graph_exec);
         ctx->graph_exec = nullptr;
     }
-    if (ctx->graph_used) g_kernel_launches += 7 * (int64_t)hs.nit + krylov_body_launches(ctx, *s) * (int64_t)hs.krylov_bodies;
+    if (ctx->graph_used)
+        g_kernel_launches += newton_body_launches(ctx) * (int64_t)hs.nit + krylov_body_launches(ctx, *s) * (int64_t)hs.krylov_bodies;
     st->newton_iterations = hs.newton_iters;
     st->newton_converged = hs.converged;
+    st->fp64_residual = hs.fp64_res;
     st->newton_residual_initial = hs.res_initial;
     st->newton_residual_final = hs.res_final;
     // reverse: G2P, the adjoint solve, force / P2G / E

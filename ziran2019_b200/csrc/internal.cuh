@@ -70,6 +70,8 @@ struct SolverScalars {
     int32_t krylov_iters;      // summed Krylov iterations
     int32_t hvp_count;
     int32_t converged;
+    int32_t fp64_res;          // MIXED: 1 once the Newton residual is evaluated in FP64 (its FP32 form stalled)
+    int32_t skip_step;         // 1: this Newton iteration takes no step (the residual is re-evaluated first)
     int32_t kcount[64];        // Krylov iterations of each Newton iteration
     double res_initial, res_final;
     double rel_tol, local_tol;

@@ -374,7 +374,8 @@ struct KrylovBufs {
 };
 
 struct NewtonParams {
-    int32_t minres, kmax, nmax, pad;
+    int32_t minres, kmax, nmax;
+    int32_t escalate;                 // MIXED: FP64 residual once the FP32 one stalls
     double tol, abs_tol, tol_scale, dt;
 };
 
@@ -398,6 +399,12 @@ __global__ void __launch_bounds__(ND_THREADS) k_newton_check(NodeGeom ng, const 
     const bool done = (norm < np.tol) || !(norm == norm);
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         if (sc->nit == 0) sc->res_initial = norm;
+        // MIXED: a norm that did not halve means FP32 stress round-off now
+        // dominates the residual; the rest of the solve evaluates it in FP64,
+        // and this iteration takes no step (the residual is re-evaluated first)
+        const bool stall = np.escalate && !done && !sc->fp64_res && sc->nit > 0 && !(norm <= 0.5 * sc->res_final);
+        if (stall) sc->fp64_res = 1;
+        sc->skip_step = stall ? 1 : 0;
         sc->res_final = norm;
         if (done) {
             sc->newton_done = 1;
@@ -461,7 +468,7 @@ __global__ void __launch_bounds__(ND_THREADS) k_krylov_start(NodeGeom ng, Krylov
     const double rnorm = sqrt(dotv);
     const double rel = sc->rel_tol;
     const double lt = fmin(rel * rnorm, np.abs_tol);
-    const bool active = !(rnorm < lt) && np.kmax > 0;
+    const bool active = !(rnorm < lt) && np.kmax > 0 && !sc->skip_step;
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         sc->rnorm = rnorm;
         sc->local_tol = lt;
@@ -1291,6 +1298,7 @@ static int newton_impl(Ctx* ctx, const zmpm_solver& s)
     L.kb.hacc = ctx->kv[9].as<double>();
     L.kb.pre = ctx->gm.as<double>();
     L.np.minres = s.linear_solver == ZMPM_MINRES ? 1 : 0;
+    L.np.escalate = ctx->mixed ? 1 : 0;
     // MIXED MINRES runs its split FP32 product on FP32 copies of Z
     const bool zf = ctx->mixed && L.np.minres && !ctx->hvp_fused;
     L.kb.Zf[0] = zf ? ctx->kvf.as<float>() : nullptr;
@@ -1397,6 +1405,7 @@ static int admm_impl(Ctx* ctx, const zmpm_solver& s)
     kb.hacc = ctx->kv[9].as<double>();
     kb.pre = ctx->adm_pre.as<double>();
     Lc.np.minres = 1;
+    Lc.np.escalate = 0;
     Lc.np.kmax = s.admm_global_max_iterations;
     Lc.np.nmax = s.admm_iterations;
     Lc.np.tol = 0;
@@ -1536,6 +1545,7 @@ int run_adjoint_solve(Ctx* ctx, double tol, int max_iterations)
     kb.hacc = ctx->kv[9].as<double>();
     kb.pre = ctx->gm.as<double>();
     Lc.np.minres = 0;
+    Lc.np.escalate = 0;
     Lc.np.kmax = max_iterations;
     Lc.np.nmax = 1;
     Lc.np.tol = 0;

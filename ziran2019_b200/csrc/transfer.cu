@@ -177,13 +177,22 @@ int launch_damage(Ctx* ctx)
 //            S = V0 P(F) Fn^T (to `stress`) and the Hessian scratch; particles in
 //            slot order so every particle array is read coalesced.
 //  k_force : facc -= sum_p S_p grad w_ip, layered conflict-free scatter.
+// gate (MIXED contexts, which launch an FP32 and an FP64 pair of k_stress /
+// k_force per Newton iteration): 0 always runs, 1 runs while the solve's
+// residual is FP32, 2 once it is FP64.  frac_x: B-spline weights from the FP64
+// positions instead of the stored fractions (the FP64 residual of MIXED).
+__device__ __forceinline__ bool gated_off(const SolverScalars* sc, int gate)
+{
+    return sc && (sc->newton_done || (gate != 0 && (gate == 1) == (sc->fp64_res != 0)));
+}
+
 template <class L, class TS, class TH>
 __global__ void __launch_bounds__(XF_THREADS) k_stress(const int32_t* __restrict__ group_start, const int32_t* __restrict__ group_nbr,
     const double* __restrict__ pd, const int32_t* __restrict__ pi, int64_t cap, const short4* __restrict__ base, double dx, double dt,
     const TH* __restrict__ frac, const double* __restrict__ vstar, TS* __restrict__ stress, TH* __restrict__ scr,
-    const SolverScalars* __restrict__ sc, int32_t* __restrict__ flags)
+    const SolverScalars* __restrict__ sc, int32_t* __restrict__ flags, int gate, int frac_x)
 {
-    if (sc && sc->newton_done) return;
+    if (gated_off(sc, gate)) return;
     constexpr int NPB = L::NPB;
     __shared__ __align__(128) double win[8 * 3 * NPB];
     __shared__ int32_t nbr[8];
@@ -205,7 +214,8 @@ __global__ void __launch_bounds__(XF_THREADS) k_stress(const int32_t* __restrict
         const short4 b = base[s];
         TS w[3][3], dwr[3][3];
 #pragma unroll
-        for (int d = 0; d < 3; ++d) bspline((TS)frac[d * cap + s], w[d], dwr[d]);
+        for (int d = 0; d < 3; ++d)
+            bspline(frac_x ? (TS)((1.0 / dx) * pd[(PD_X + d) * cap + s] - (double)((&b.x)[d])) : (TS)frac[d * cap + s], w[d], dwr[d]);
         const int lx = b.x & (L::BX - 1), ly = b.y & (L::BY - 1), lz = b.z & (L::BZ - 1);
         M3<TS> gv = m3_zero<TS>();
         for_stencil<L>(lx, ly, lz, w, dwr, inv_dx, [&](int t, int e, int, int, int, TS, const TS* dw) {
@@ -307,9 +317,9 @@ int launch_explicit_stress(Ctx* ctx)
 template <class L, class TS, class TH, bool MLS = false>
 __global__ void __launch_bounds__(XF_THREADS) k_force(const int32_t* __restrict__ group_start, const int32_t* __restrict__ group_nbr,
     int64_t cap, const short4* __restrict__ base, double dx, const TH* __restrict__ frac, const TS* __restrict__ stress,
-    double* __restrict__ facc, const SolverScalars* __restrict__ sc)
+    double* __restrict__ facc, const SolverScalars* __restrict__ sc, int gate = 0, const double* __restrict__ xpos = nullptr)
 {
-    if (sc && sc->newton_done) return;
+    if (gated_off(sc, gate)) return;
     constexpr int NPB = L::NPB;
     __shared__ __align__(16) TS acc[8 * 3 * NPB];
     __shared__ int32_t nbr[8];
@@ -336,11 +346,16 @@ __global__ void __launch_bounds__(XF_THREADS) k_force(const int32_t* __restrict_
         for (int r = threadIdx.x / NPB; r < cnt; r += blockDim.x / NPB) {
             const int s = first + r;
             TS w[3][3], dwr[3][3], fr[3];
+            if (xpos) {
+                const short4 b = base[s];
 #pragma unroll
-            for (int d = 0; d < 3; ++d) {
-                fr[d] = (TS)frac[d * cap + s];
-                bspline(fr[d], w[d], dwr[d]);
+                for (int d = 0; d < 3; ++d) fr[d] = (TS)((1.0 / dx) * xpos[d * cap + s] - (double)((&b.x)[d]));
             }
+            else
+#pragma unroll
+                for (int d = 0; d < 3; ++d) fr[d] = (TS)frac[d * cap + s];
+#pragma unroll
+            for (int d = 0; d < 3; ++d) bspline(fr[d], w[d], dwr[d]);
             TS row[NCP][3];
 #pragma unroll
             for (int c = 0; c < NCP; ++c)
@@ -715,18 +730,32 @@ static int update_impl(Ctx* ctx, bool gated)
     DevCounters* dc = ctx->counters.as<DevCounters>();
     const SolverScalars* sc = gated ? ctx->scal.as<SolverScalars>() : nullptr;
     if (ctx->mixed) {
+        // FP32 stress and force; inside a solve also the FP64 pair, which runs
+        // instead once the FP32 residual stalled (FP32 Hessian scratch either way)
+        const int gate = sc ? 1 : 0;
         k_stress<L, float, float><<<(unsigned)G, XF_THREADS, 0, ctx->stream>>>(ctx->group_start.as<int32_t>(), ctx->group_nbr.as<int32_t>(),
             ctx->pd.as<double>(), ctx->pi.as<int32_t>(), ctx->Pcap, ctx->base.as<short4>(), ctx->cfg.dx, ctx->dt, ctx->frac.as<float>(),
-            ctx->vstar.as<double>(), ctx->stress.as<float>(), ctx->scratch.as<float>(), sc, &dc->flags);
+            ctx->vstar.as<double>(), ctx->stress.as<float>(), ctx->scratch.as<float>(), sc, &dc->flags, gate, 0);
         ++g_kernel_launches;
         k_force<L, float, float><<<(unsigned)G, XF_THREADS, 0, ctx->stream>>>(ctx->group_start.as<int32_t>(), ctx->group_nbr.as<int32_t>(),
-            ctx->Pcap, ctx->base.as<short4>(), ctx->cfg.dx, ctx->frac.as<float>(), ctx->stress.as<float>(), ctx->facc.as<double>(), sc);
+            ctx->Pcap, ctx->base.as<short4>(), ctx->cfg.dx, ctx->frac.as<float>(), ctx->stress.as<float>(), ctx->facc.as<double>(), sc, gate);
         ++g_kernel_launches;
+        if (sc) {
+            k_stress<L, double, float><<<(unsigned)G, XF_THREADS, 0, ctx->stream>>>(ctx->group_start.as<int32_t>(),
+                ctx->group_nbr.as<int32_t>(), ctx->pd.as<double>(), ctx->pi.as<int32_t>(), ctx->Pcap, ctx->base.as<short4>(), ctx->cfg.dx,
+                ctx->dt, ctx->frac.as<float>(), ctx->vstar.as<double>(), ctx->stress.as<double>(), ctx->scratch.as<float>(), sc, &dc->flags, 2,
+                1);
+            ++g_kernel_launches;
+            k_force<L, double, float><<<(unsigned)G, XF_THREADS, 0, ctx->stream>>>(ctx->group_start.as<int32_t>(), ctx->group_nbr.as<int32_t>(),
+                ctx->Pcap, ctx->base.as<short4>(), ctx->cfg.dx, ctx->frac.as<float>(), ctx->stress.as<double>(), ctx->facc.as<double>(), sc, 2,
+                ctx->pd.as<double>() + PD_X * ctx->Pcap);
+            ++g_kernel_launches;
+        }
     }
     else {
         k_stress<L, double, double><<<(unsigned)G, XF_THREADS, 0, ctx->stream>>>(ctx->group_start.as<int32_t>(), ctx->group_nbr.as<int32_t>(),
             ctx->pd.as<double>(), ctx->pi.as<int32_t>(), ctx->Pcap, ctx->base.as<short4>(), ctx->cfg.dx, ctx->dt, ctx->frac.as<double>(),
-            ctx->vstar.as<double>(), ctx->stress.as<double>(), ctx->scratch.as<double>(), sc, &dc->flags);
+            ctx->vstar.as<double>(), ctx->stress.as<double>(), ctx->scratch.as<double>(), sc, &dc->flags, 0, 0);
         ++g_kernel_launches;
         k_force<L, double, double><<<(unsigned)G, XF_THREADS, 0, ctx->stream>>>(ctx->group_start.as<int32_t>(), ctx->group_nbr.as<int32_t>(),
             ctx->Pcap, ctx->base.as<short4>(), ctx->cfg.dx, ctx->frac.as<double>(), ctx->stress.as<double>(), ctx->facc.as<double>(), sc);
