@@ -229,7 +229,7 @@ def wl_phasefield2m(precision, lib=None, layout="auto", scale=1):
                                    "solver": "MINRES, Newton 3 x Krylov 20; phase-field CG 1e-6 x 100"}
 
 
-MIXED_ROLLOUT_TOL = 1e-7
+MIXED_ROLLOUT_TOL = 1e-12
 
 
 def wl_rollout256k(precision, lib=None, layout="auto", scale=1):
@@ -255,7 +255,7 @@ def wl_rollout256k(precision, lib=None, layout="auto", scale=1):
     sim.krylov_max_iterations = 500
     sim.krylov_tolerance = 1e-30
     return sim, 1e-3, x.shape[0], {"workload": "config4-differentiable-rollout-256k", "model": "fixed corotated, per-particle E",
-                                   "solver": "Newton-CG (FP64 tol 1e-12, mixed 1e-7), adjoint CG rel tol 1e-10",
+                                   "solver": "Newton-CG tol 1e-12, adjoint CG rel tol 1e-10",
                                    "steps": 100, "checkpoint_every": 10}
 
 

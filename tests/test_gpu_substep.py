@@ -76,7 +76,9 @@ def test_mixed_reaches_tolerance_below_fp32_floor(cuda_lib, oracle, kind, solver
     assert all(st["newton_converged"] == 1 for st in sg), [st["newton_residual_final"] for st in sg]
     assert all(st["newton_residual_final"] < 1e-11 for st in sg)
     assert all(st["newton_converged"] == 1 for st in so)
-    assert any(st["fp64_residual"] == 1 for st in sg)
+    # the first solve escalates; the context then starts later solves in FP64
+    first = [st["fp64_residual"] for st in sg].index(1)
+    assert all(st["fp64_residual"] == 1 for st in sg[first:])
     pg, po = g.getParticles(), o.getParticles()
     assert rel(pg["X"], po["X"]) < 1e-11
     assert rel(pg["V"], po["V"]) < 1e-7

@@ -1029,6 +1029,7 @@ int zmpm_substep(zmpm_ctx* ctx, double dt, const zmpm_solver* s, zmpm_stats* st)
     st->phase_field_iterations = ctx->pf_iters;
     st->phase_field_residual = ctx->pf_res;
     st->fp64_residual = hs.fp64_res;
+    if (!admm && !expl) ctx->fp64_res_run = hs.fp64_res ? ctx->fp64_res_run + 1 : 0;
     if (ctx->graph_used && admm) // ADMM iteration: 7 head + 3 tail kernels; Krylov body: operator (2), k_mr_a, k_mr_b
         g_kernel_launches += 10 * (int64_t)hs.nit + 4 * (int64_t)hs.krylov_bodies;
     else if (ctx->graph_used)
@@ -1127,6 +1128,7 @@ int zmpm_adjoint_substep(zmpm_ctx* ctx, double dt, const zmpm_solver* s, double 
     st->newton_iterations = hs.newton_iters;
     st->newton_converged = hs.converged;
     st->fp64_residual = hs.fp64_res;
+    ctx->fp64_res_run = hs.fp64_res ? ctx->fp64_res_run + 1 : 0;
     st->newton_residual_initial = hs.res_initial;
     st->newton_residual_final = hs.res_final;
     // reverse: G2P, the adjoint solve, force / P2G / E

@@ -149,6 +149,8 @@ struct Ctx {
     bool has_damage = false;
     bool has_visco = false;
     bool mls = false;                     // the running explicit substep uses MLS-MPM (G2P gradV = C)
+    int fp64_res_run = 0;                 // MIXED: consecutive Newton solves that needed the FP64 residual; while
+                                          // nonzero the next solve starts with it, except every 16th (an FP32 retry)
     bool all_models = true;               // every particle has an F-based model
     int pd_active = PD_CORE;              // pd fields the binning permutation moves
     std::vector<zmpm_collider> colliders;

@@ -1312,6 +1312,10 @@ static int newton_impl(Ctx* ctx, const zmpm_solver& s)
     L.dt2 = ctx->dt * ctx->dt;
     L.nb = L.ng.parts;
     ZMPM_CUDA(cudaMemsetAsync(L.sc, 0, sizeof(SolverScalars), st));
+    // MIXED: start with the FP64 residual when the last solves needed it (any
+    // nonzero byte sets the flag)
+    if (ctx->mixed && ctx->fp64_res_run > 0 && ctx->fp64_res_run % 16 != 0)
+        ZMPM_CUDA(cudaMemsetAsync(&L.sc->fp64_res, 1, 1, st));
     ctx->prof_newton = 0;
     ctx->graph_used = false;
     if (L.ng.nn == 0 || s.newton_max_iterations == 0) return ZMPM_OK;
