@@ -468,7 +468,7 @@ int zmpm_destroy(zmpm_ctx* ctx)
         &ctx->group_page, &ctx->group_nbr, &ctx->emit_flag, &ctx->emit_scan, &ctx->page_first, &ctx->page_block, &ctx->block_page,
         &ctx->block_index, &ctx->gm, &ctx->gmv, &ctx->vn, &ctx->dv, &ctx->vstar, &ctx->facc, &ctx->res, &ctx->proj, &ctx->collided,
         &ctx->node_idx, &ctx->red, &ctx->scal, &ctx->counters, &ctx->dcolliders, &ctx->adm_F, &ctx->adm_gvn, &ctx->adm_B, &ctx->adm_pre,
-        &ctx->adm_rhs, &ctx->adm_w, &ctx->adj };
+        &ctx->adm_rhs, &ctx->adm_w, &ctx->adj, &ctx->kvf, &ctx->pfn, &ctx->pfsc };
     for (DBuf* b : bufs) b->release();
     for (auto& b : ctx->kv) b.release();
     for (auto* v : { &ctx->ckpt_pd, &ctx->ckpt_pi, &ctx->ckpt_sid })
