@@ -363,12 +363,9 @@ def run_workload(args, world, rank):
         osim, _, Pc, _ = fn("fp64", lib=zoracle.lib(), scale=scale)
         for _ in range(args.warmup):
             osim.advanceOneTimeStep(dt)
-        t0 = time.perf_counter()
-        for _ in range(args.cpu_steps):
-            osim.advanceOneTimeStep(dt)
-        secs = time.perf_counter() - t0
-        cpu = {"value": args.cpu_steps / secs * Pc / P, "unit": "substeps/s", "cores": os.cpu_count(), "kind": "port",
-               "sample": f"{args.cpu_steps} substep(s) of a {Pc}-particle cut of the workload after {args.warmup} warm-up, oracle port, "
+        n, secs = timed_cpu_steps(osim, dt, args.cpu_steps, args.cpu_seconds)
+        cpu = {"value": n / secs * Pc / P, "unit": "substeps/s", "cores": os.cpu_count(), "kind": "port",
+               "sample": f"{n} substep(s) of a {Pc}-particle cut of the workload after {args.warmup} warm-up, oracle port, "
                          f"{secs:.1f} s, scaled by {Pc}/{P}"}
     if rank == 0:
         value = world * args.steps / (ms_mx / 1e3)
@@ -484,27 +481,36 @@ def timed_steps(sim, steps, world, profile=False, dt=None):
     return barrier_max(ms, world), stats
 
 
-def cpu_oracle_rate(steps, warmup, velocity="particle"):
+def timed_cpu_steps(sim, dt, steps, min_seconds, max_steps=400):
+    """Runs at least `steps` oracle substeps and keeps going until `min_seconds`
+    of CPU work (at most max_steps); returns (substeps run, seconds)."""
+    t0 = time.perf_counter()
+    n = 0
+    while n < max_steps and (n < steps or time.perf_counter() - t0 < min_seconds):
+        sim.advanceOneTimeStep(dt)
+        n += 1
+    return n, time.perf_counter() - t0
+
+
+def cpu_oracle_rate(steps, warmup, velocity="particle", min_seconds=0.0):
     """The oracle (CPU restatement of the reference substep) on one 250k-particle
-    box of the same scene, all host threads; returns 1M-equivalent substeps/s."""
+    box of the same scene, all host threads; returns 1M-equivalent substeps/s,
+    the sample's particles, seconds and substeps."""
     from oracle import zoracle
     x, v = scene(n_boxes=1, velocity=velocity)
     sim = make_sim(x, v, "fp64", lib=zoracle.lib())
     for _ in range(warmup):
         sim.advanceOneTimeStep(DT)
-    t0 = time.perf_counter()
-    for _ in range(steps):
-        sim.advanceOneTimeStep(DT)
-    dt = time.perf_counter() - t0
+    n, dt = timed_cpu_steps(sim, DT, steps, min_seconds)
     P = x.shape[0]
-    return steps / dt * P / 1_000_000, P, dt
+    return n / dt * P / 1_000_000, P, dt, n
 
 
 def run_reference(args, world, rank):
     if rank != 0:
         return
     cores = os.cpu_count()
-    rate, P, secs = cpu_oracle_rate(args.steps, args.warmup, args.velocity)
+    rate, P, secs, _ = cpu_oracle_rate(args.steps, args.warmup, args.velocity)
     sample = f"{args.steps} substeps of one {P}-particle box of the workload (oracle port, {cores} threads), scaled by {P}/1e6"
     line = {"metric": METRIC, "value": rate, "unit": "substeps/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1e3 * secs / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
@@ -522,7 +528,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--accuracy-steps", type=int, default=100)
-    ap.add_argument("--cpu-steps", type=int, default=1)
+    ap.add_argument("--cpu-steps", type=int, default=1, help="minimum oracle substeps of the CPU baseline sample")
+    ap.add_argument("--cpu-seconds", type=float, default=10.0, help="the CPU baseline sample runs substeps until this much CPU work")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--model", default="hencky", choices=["hencky", "nh"])
@@ -652,9 +659,9 @@ def main():
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        rate, Pc, secs = cpu_oracle_rate(args.cpu_steps, 0, args.velocity)
+        rate, Pc, secs, n = cpu_oracle_rate(args.cpu_steps, 0, args.velocity, args.cpu_seconds)
         cpu = {"value": rate, "unit": "substeps/s", "cores": os.cpu_count(), "kind": "port",
-               "sample": f"{args.cpu_steps} substep(s) of one {Pc}-particle box of the workload, oracle port, {secs:.1f} s, scaled by {Pc}/1e6"}
+               "sample": f"{n} substep(s) of one {Pc}-particle box of the workload, oracle port, {secs:.1f} s, scaled by {Pc}/1e6"}
 
     launches = sum(s["kernel_launches"] for s in st_mx)
     if rank == 0:
