@@ -37,9 +37,9 @@ E, NU, YIELD = 5e4, 0.35, 150.0
 METRIC = "implicit MPM substeps/sec at 1M particles, mixed vs FP64 GPU, at <=1e-6 rel err"
 HVP_WORDS = 22  # compulsory words per particle of one Hessian-vector product: X(3), Fn(9), F(9), V0(1)
 # DRAM bytes of one product (k_hvp_stress + k_hvp_scatter) per particle, from an
-# ncu capture at 250k particles (52.9 MB; profiles/k_hvp_stress_k_hvp_scatter_250k_mixed.md),
-# scaled by the particle count: traffic grows in proportion to particles.
-HVP_DRAM_BYTES_PER_PARTICLE = 52.9e6 / 250_000
+# ncu capture of this workload at 1M particles (228.7 MB;
+# profiles/k_hvp_stress_k_hvp_scatter_1M_mixed.md).
+HVP_DRAM_BYTES_PER_PARTICLE = 228.7e6 / 1_000_000
 
 
 def scene(n_boxes=4, seed_pos=1, seed_vel=2, seed_jit=0, velocity="particle"):
@@ -620,7 +620,7 @@ def main():
     achieved = hvp_bytes / (hvp_ms / hvp_n / 1e3) / 1e9 if hvp_n else None
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak if achieved else None, "traffic": HVP_DRAM_BYTES_PER_PARTICLE * P,
-                "traffic_source": "ncu dram__bytes_read+write at 250k particles, scaled by particles",
+                "traffic_source": "ncu dram__bytes_read+write of both kernels at 1M particles",
                 "kernel": "k_hvp (FP32 Hessian-vector product)", "bytes_per_launch": hvp_bytes,
                 "avg_launch_ms": hvp_ms / hvp_n if hvp_n else None, "peak_source": "measured" if peaks else "fallback"}
 
