@@ -53,3 +53,32 @@ def test_single_particle_with_phase_field_and_sand(cuda_lib, oracle, integrator)
         np.testing.assert_allclose(pg[k], po[k], rtol=1e-10, atol=1e-12)
     np.testing.assert_allclose(sims[0].getPhaseField()["c"], sims[1].getPhaseField()["c"], rtol=0, atol=1e-12)
     np.testing.assert_allclose(sims[0].getLogJp(), sims[1].getLogJp(), rtol=0, atol=1e-12)
+
+
+def test_destroy_releases_device_memory(cuda_lib):
+    """zmpm_destroy frees every device array a context allocated: MIXED Newton
+    (with MINRES's FP32 Krylov copies), the phase-field solve and ADMM, each
+    created, stepped and destroyed repeatedly, leave the device's free memory
+    where it was."""
+    import torch
+    from tests.scenes import build_scene
+
+    def cycle():
+        for kind in ("mixed", "phase_field", "admm"):
+            s = mpm.MpmSimulation(DX, gravity=(0, -9.8, 0), precision="mixed" if kind == "mixed" else "fp64", grid_log2=8)
+            h, _ = build_scene(s, kind="nh" if kind == "phase_field" else "hencky", n=16, dx=DX)
+            if kind == "phase_field":
+                h.addFBasedMpmForceWithPhaseField(0.05, 0.5 * DX)
+            if kind == "admm":
+                s.useAdmm(admm_max_iterations=2)
+            assert s.advanceOneTimeStep(1e-3) == abi.OK, (kind, s.last_stats)
+            s.close()
+
+    cycle()  # first use: the library's one-time allocations
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    for _ in range(3):
+        cycle()
+    torch.cuda.synchronize()
+    free1 = torch.cuda.mem_get_info()[0]
+    assert free1 >= free0 - (4 << 20), (free0 - free1) / 2**20
