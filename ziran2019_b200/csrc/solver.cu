@@ -391,7 +391,7 @@ __device__ __forceinline__ T* sel2(T* const (&a)[2], int i) { return i == 0 ? a[
 // CG: r = res, q = r/m, p = q, partial r.q;  MINRES: Q0 = res, Z0 = res/m,
 // Q1 = Q2 = M* = 0, partial z.q.
 template <int NPB>
-__global__ void __launch_bounds__(ND_THREADS) k_newton_check(NodeGeom ng, const double* __restrict__ gm, const double* __restrict__ res,
+__global__ void __launch_bounds__(ND_THREADS, 4) k_newton_check(NodeGeom ng, const double* __restrict__ gm, const double* __restrict__ res,
     KrylovBufs kb, NewtonParams np, double* __restrict__ part_in, double* __restrict__ part_out, SolverScalars* __restrict__ sc)
 {
     if (sc->newton_done) return;
@@ -648,7 +648,7 @@ __global__ void __launch_bounds__(ND_THREADS) k_cg_c(NodeGeom ng, const double* 
 // hacc = 0; partial Z_k . W.  Massless slots hold zeros in every vector and
 // are skipped.
 template <int NPB>
-__global__ void __launch_bounds__(ND_THREADS) k_mr_a(NodeGeom ng, const double* __restrict__ gm, const int8_t* __restrict__ col,
+__global__ void __launch_bounds__(ND_THREADS, 4) k_mr_a(NodeGeom ng, const double* __restrict__ gm, const int8_t* __restrict__ col,
     const double* __restrict__ P6, double dt2, KrylovBufs kb, double* __restrict__ part, const SolverScalars* __restrict__ sc)
 {
     if (krylov_off(sc)) return;
