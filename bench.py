@@ -360,13 +360,12 @@ def run_workload(args, world, rank):
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         from oracle import zoracle
         scale = {"cube32k": 1, "admm500k": 4, "damage2m": 11, "explicit1m": 4, "sand1m": 4, "phasefield2m": 11}[args.workload]
-        osim, _, Pc, _ = fn("fp64", lib=zoracle.lib(), scale=scale)
-        for _ in range(args.warmup):
-            osim.advanceOneTimeStep(dt)
-        n, secs = timed_cpu_steps(osim, dt, args.cpu_steps, args.cpu_seconds)
+        Pc = fn("fp64", lib=zoracle.lib(), scale=scale)[2]
+        n, secs, reps = timed_cpu_window(lambda: fn("fp64", lib=zoracle.lib(), scale=scale)[0], dt, args.warmup, args.steps,
+                                         args.cpu_seconds)
         cpu = {"value": n / secs * Pc / P, "unit": "substeps/s", "cores": os.cpu_count(), "kind": "port",
-               "sample": f"{n} substep(s) of a {Pc}-particle cut of the workload after {args.warmup} warm-up, oracle port, "
-                         f"{secs:.1f} s, scaled by {Pc}/{P}"}
+               "sample": f"the timed window ({args.warmup} warm-up + {args.steps} timed substeps) on a {Pc}-particle cut of the "
+                         f"workload, {reps}x, oracle port, {secs:.1f} s timed, scaled by {Pc}/{P}"}
     if rank == 0:
         value = world * args.steps / (ms_mx / 1e3)
         fp64_value = world * args.steps / (ms64 / 1e3)
@@ -481,36 +480,43 @@ def timed_steps(sim, steps, world, profile=False, dt=None):
     return barrier_max(ms, world), stats
 
 
-def timed_cpu_steps(sim, dt, steps, min_seconds, max_steps=400):
-    """Runs at least `steps` oracle substeps and keeps going until `min_seconds`
-    of CPU work (at most max_steps); returns (substeps run, seconds)."""
-    t0 = time.perf_counter()
-    n = 0
-    while n < max_steps and (n < steps or time.perf_counter() - t0 < min_seconds):
-        sim.advanceOneTimeStep(dt)
-        n += 1
-    return n, time.perf_counter() - t0
+def timed_cpu_window(make, dt, warmup, steps, min_seconds, max_repeats=50):
+    """The GPU's timed window on the oracle: a fresh scene from make(), `warmup`
+    untimed substeps, then `steps` timed ones; repeated until `min_seconds` of
+    timed CPU work (at most max_repeats).  Returns (timed substeps, seconds,
+    repeats)."""
+    secs, n, reps = 0.0, 0, 0
+    while reps < max_repeats and (reps == 0 or secs < min_seconds):
+        sim = make()
+        for _ in range(warmup):
+            sim.advanceOneTimeStep(dt)
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            sim.advanceOneTimeStep(dt)
+        secs += time.perf_counter() - t0
+        n += steps
+        reps += 1
+        sim.close()
+    return n, secs, reps
 
 
 def cpu_oracle_rate(steps, warmup, velocity="particle", min_seconds=0.0):
     """The oracle (CPU restatement of the reference substep) on one 250k-particle
-    box of the same scene, all host threads; returns 1M-equivalent substeps/s,
-    the sample's particles, seconds and substeps."""
+    box of the same scene, all host threads, over the GPU's timed window;
+    returns 1M-equivalent substeps/s, the sample's particles, seconds, timed
+    substeps and repeats of the window."""
     from oracle import zoracle
     x, v = scene(n_boxes=1, velocity=velocity)
-    sim = make_sim(x, v, "fp64", lib=zoracle.lib())
-    for _ in range(warmup):
-        sim.advanceOneTimeStep(DT)
-    n, dt = timed_cpu_steps(sim, DT, steps, min_seconds)
+    n, dt, reps = timed_cpu_window(lambda: make_sim(x, v, "fp64", lib=zoracle.lib()), DT, warmup, steps, min_seconds)
     P = x.shape[0]
-    return n / dt * P / 1_000_000, P, dt, n
+    return n / dt * P / 1_000_000, P, dt, n, reps
 
 
 def run_reference(args, world, rank):
     if rank != 0:
         return
     cores = os.cpu_count()
-    rate, P, secs, _ = cpu_oracle_rate(args.steps, args.warmup, args.velocity)
+    rate, P, secs, _, _ = cpu_oracle_rate(args.steps, args.warmup, args.velocity)
     sample = f"{args.steps} substeps of one {P}-particle box of the workload (oracle port, {cores} threads), scaled by {P}/1e6"
     line = {"metric": METRIC, "value": rate, "unit": "substeps/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1e3 * secs / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
@@ -528,8 +534,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--accuracy-steps", type=int, default=100)
-    ap.add_argument("--cpu-steps", type=int, default=1, help="minimum oracle substeps of the CPU baseline sample")
-    ap.add_argument("--cpu-seconds", type=float, default=10.0, help="the CPU baseline sample runs substeps until this much CPU work")
+    ap.add_argument("--cpu-seconds", type=float, default=10.0,
+                    help="the CPU baseline repeats the timed window on the oracle until this much timed CPU work")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--model", default="hencky", choices=["hencky", "nh"])
@@ -659,9 +665,10 @@ def main():
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        rate, Pc, secs, n = cpu_oracle_rate(args.cpu_steps, 0, args.velocity, args.cpu_seconds)
+        rate, Pc, secs, n, reps = cpu_oracle_rate(args.steps, args.warmup, args.velocity, args.cpu_seconds)
         cpu = {"value": rate, "unit": "substeps/s", "cores": os.cpu_count(), "kind": "port",
-               "sample": f"{n} substep(s) of one {Pc}-particle box of the workload, oracle port, {secs:.1f} s, scaled by {Pc}/1e6"}
+               "sample": f"the timed window ({args.warmup} warm-up + {args.steps} timed substeps) on one {Pc}-particle box of the workload, "
+                         f"{reps}x, oracle port, {secs:.1f} s timed, scaled by {Pc}/1e6"}
 
     launches = sum(s["kernel_launches"] for s in st_mx)
     if rank == 0:
