@@ -904,9 +904,10 @@ static int64_t krylov_body_launches(const zmpm_ctx* ctx, const zmpm_solver& s)
 }
 
 // Kernels of one Newton loop body outside the Krylov loop: stress and force
-// (MIXED: an FP32 and an FP64 pair, one of which returns at once), residual,
-// check, Krylov start, step, advance.
-static int64_t newton_body_launches(const zmpm_ctx* ctx) { return ctx->mixed ? 9 : 7; }
+// (MIXED: an FP32 and an FP64 pair, one of which returns at once), residual
+// with the Krylov start vectors, Newton check with the Krylov start, step,
+// advance.
+static int64_t newton_body_launches(const zmpm_ctx* ctx) { return ctx->mixed ? 8 : 6; }
 
 static int begin_implicit_impl(zmpm_ctx* ctx, double dt, bool damage = true)
 {

@@ -387,46 +387,38 @@ __device__ __forceinline__ double* sel3(double* const (&a)[3], int i) { return i
 template <class T>
 __device__ __forceinline__ T* sel2(T* const (&a)[2], int i) { return i == 0 ? a[0] : a[1]; }
 
-// Newton check (NewtonsMethod.h:48-61) + start of the linear solve: x = 0,
-// CG: r = res, q = r/m, p = q, partial r.q;  MINRES: Q0 = res, Z0 = res/m,
-// Q1 = Q2 = M* = 0, partial z.q.
+// The Newton residual of k_residual fused with the operands of the linear
+// solve's start, in one node pass: r = project(dt m g + dt f - m dv), facc
+// zeroed, x = 0, and from r the Krylov start vectors (CG: r, q = p = r/pre;
+// MINRES: Q0 = r, Z0 = r/pre and its FP32 copy, Q1 = Q2 = M* = Z1 = 0);
+// partials of |r|^2/m (computeNorm, BackwardEuler.h:101-140) and of z.r.
+// When k_newton_start then finds the norm converged these vectors go unused.
 template <int NPB>
-__global__ void __launch_bounds__(ND_THREADS, 4) k_newton_check(NodeGeom ng, const double* __restrict__ gm, const double* __restrict__ res,
-    KrylovBufs kb, NewtonParams np, double* __restrict__ part_in, double* __restrict__ part_out, SolverScalars* __restrict__ sc)
+__global__ void __launch_bounds__(ND_THREADS, 4) k_residual_start(NodeGeom ng, const double* __restrict__ gm, double* __restrict__ facc,
+    const double* __restrict__ dv, const int8_t* __restrict__ col, const double* __restrict__ P6, double gx, double gy, double gz, double dt,
+    KrylovBufs kb, int minres, double* __restrict__ part_norm, double* __restrict__ part_zr, const SolverScalars* __restrict__ sc)
 {
     if (sc->newton_done) return;
-    const double norm = sqrt(reduce_partials(part_in, ng.parts));
-    const bool done = (norm < np.tol) || !(norm == norm);
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        if (sc->nit == 0) sc->res_initial = norm;
-        // MIXED: a norm that did not halve means FP32 stress round-off now
-        // dominates the residual; the rest of the solve evaluates it in FP64,
-        // and this iteration takes no step (the residual is re-evaluated first)
-        const bool stall = np.escalate && !done && !sc->fp64_res && sc->nit > 0 && !(norm <= 0.5 * sc->res_final);
-        if (stall) sc->fp64_res = 1;
-        sc->skip_step = stall ? 1 : 0;
-        sc->res_final = norm;
-        if (done) {
-            sc->newton_done = 1;
-            sc->converged = (norm == norm) ? 1 : 0;
-            sc->kactive = 0;
-        }
-        else {
-            double mx = norm > np.tol ? norm : np.tol;
-            double rel = np.tol_scale * sqrt(mx);
-            sc->rel_tol = rel < 0.5 ? rel : 0.5;
-        }
-    }
-    if (done) return;
-    double acc = 0;
+    double acc = 0, zr = 0;
+    const double g[3] = { gx, gy, gz };
     for (int64_t n = (int64_t)blockIdx.x * ND_THREADS + threadIdx.x; n < ng.nn; n += (int64_t)gridDim.x * ND_THREADS) {
         const double m = gm[n];
+        double r[3] = { 0, 0, 0 };
         for (int k = 0; k < 3; ++k) {
-            int64_t i = vidx<NPB>(n, k);
-            double rv = res[i];
-            double z = (m != 0) ? rv / kb.pre[n] : 0.0;
+            const int64_t i = vidx<NPB>(n, k);
+            if (m != 0) r[k] = dt * g[k] * m + dt * facc[i] - (dt / dt) * m * dv[i];
+            facc[i] = 0;
+        }
+        if (m != 0) {
+            project3(col, P6, ng.nn, n, r);
+            acc += (r[0] * r[0] + r[1] * r[1] + r[2] * r[2]) / m;
+        }
+        for (int k = 0; k < 3; ++k) {
+            const int64_t i = vidx<NPB>(n, k);
+            const double rv = r[k];
+            const double z = (m != 0) ? rv / kb.pre[n] : 0.0;
             kb.x[i] = 0;
-            if (np.minres) {
+            if (minres) {
                 kb.Q[0][i] = rv;
                 kb.Q[1][i] = 0;
                 kb.Q[2][i] = 0;
@@ -445,11 +437,70 @@ __global__ void __launch_bounds__(ND_THREADS, 4) k_newton_check(NodeGeom ng, con
                 kb.q[i] = z;
                 kb.p[i] = z;
             }
-            acc += z * rv;
+            zr += z * rv;
         }
     }
-    double s = block_sum(acc);
-    if (threadIdx.x == 0) part_out[blockIdx.x] = s;
+    const double s0 = block_sum(acc);
+    const double s1 = block_sum(zr);
+    if (threadIdx.x == 0) {
+        part_norm[blockIdx.x] = s0;
+        part_zr[blockIdx.x] = s1;
+    }
+}
+
+// Newton check (NewtonsMethod.h:48-61) and, unless converged, the start of
+// the linear solve (k_krylov_start's scalars); sets the Krylov loop condition
+// when running as a graph.  One CTA.
+template <int NPB>
+__global__ void __launch_bounds__(ND_THREADS) k_newton_start(NodeGeom ng, NewtonParams np, const double* __restrict__ part_norm,
+    const double* __restrict__ part_zr, SolverScalars* __restrict__ sc, cudaGraphConditionalHandle hK, int use_graph)
+{
+    if (sc->newton_done) {
+        if (use_graph && threadIdx.x == 0) cudaGraphSetConditional(hK, 0u);
+        return;
+    }
+    const double norm = sqrt(reduce_partials(part_norm, ng.parts));
+    const bool done = (norm < np.tol) || !(norm == norm);
+    const double dotv = reduce_partials(part_zr, ng.parts);
+    if (threadIdx.x != 0) return;
+    if (sc->nit == 0) sc->res_initial = norm;
+    // MIXED: a norm that did not halve means FP32 stress round-off now
+    // dominates the residual; the rest of the solve evaluates it in FP64, and
+    // this iteration takes no step (the residual is re-evaluated first)
+    const bool stall = np.escalate && !done && !sc->fp64_res && sc->nit > 0 && !(norm <= 0.5 * sc->res_final);
+    if (stall) sc->fp64_res = 1;
+    sc->skip_step = stall ? 1 : 0;
+    sc->res_final = norm;
+    if (done) {
+        sc->newton_done = 1;
+        sc->converged = (norm == norm) ? 1 : 0;
+        sc->kactive = 0;
+        if (use_graph) cudaGraphSetConditional(hK, 0u);
+        return;
+    }
+    const double mx = norm > np.tol ? norm : np.tol;
+    const double rel0 = np.tol_scale * sqrt(mx);
+    const double rel = rel0 < 0.5 ? rel0 : 0.5;
+    sc->rel_tol = rel;
+    // Minres.h:73-98, ConjugateGradient.h:108-117
+    const double rnorm = sqrt(dotv);
+    const double lt = fmin(rel * rnorm, np.abs_tol);
+    const bool active = !(rnorm < lt) && np.kmax > 0 && !stall;
+    sc->rnorm = rnorm;
+    sc->local_tol = lt;
+    sc->kit = 0;
+    sc->kactive = active ? 1 : 0;
+    if (np.minres) {
+        double* mr = sc->mr[0];
+        mr[MR_GC0] = mr[MR_GC1] = mr[MR_GC2] = 1;
+        mr[MR_GS0] = mr[MR_GS1] = mr[MR_GS2] = 0;
+        mr[MR_RHS0] = rnorm;
+        mr[MR_RHS1] = 0;
+        mr[MR_BETA_KP1] = rnorm;
+    }
+    else
+        sc->mr[0][0] = dotv; // CG keeps zTrk double-buffered in mr[parity][0]
+    if (use_graph) cudaGraphSetConditional(hK, active ? 1u : 0u);
 }
 
 // Initial preconditioned norm and local tolerance (Minres.h:73-98,
@@ -1124,19 +1175,19 @@ struct NewtonLaunch {
     int nb;
 };
 
-// First part of a Newton iteration: update, residual, check, Krylov start.
+// First part of a Newton iteration: update, residual with the Krylov start
+// vectors, check and Krylov start.
 template <int NPB>
 int launch_newton_head(const NewtonLaunch& L, cudaStream_t st, cudaGraphConditionalHandle hK, int use_graph)
 {
     Ctx* ctx = L.ctx;
     int rc = launch_update(ctx);
     if (rc) return rc;
-    rc = launch_residual(ctx);
-    if (rc) return rc;
-    k_newton_check<NPB><<<L.nb, ND_THREADS, 0, st>>>(L.ng, ctx->gm.as<double>(), ctx->res.as<double>(), L.kb, L.np, L.pA, L.pB, L.sc);
-    ++g_kernel_launches;
-    k_krylov_start<NPB><<<1, ND_THREADS, 0, st>>>(L.ng, L.kb, L.np, L.pB, L.sc, hK, use_graph);
-    ++g_kernel_launches;
+    const double* g = ctx->cfg.gravity;
+    k_residual_start<NPB><<<L.nb, ND_THREADS, 0, st>>>(L.ng, ctx->gm.as<double>(), ctx->facc.as<double>(), ctx->dv.as<double>(),
+        ctx->collided.as<int8_t>(), ctx->proj.as<double>(), g[0], g[1], g[2], ctx->dt, L.kb, L.np.minres, L.pA, L.pB, L.sc);
+    k_newton_start<NPB><<<1, ND_THREADS, 0, st>>>(L.ng, L.np, L.pA, L.pB, L.sc, hK, use_graph);
+    g_kernel_launches += 2;
     return ZMPM_OK;
 }
 
