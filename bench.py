@@ -480,6 +480,22 @@ def timed_steps(sim, steps, world, profile=False, dt=None):
     return barrier_max(ms, world), stats
 
 
+def substep_algorithmic_bytes(st, P, hvp_word_bytes):
+    """Compulsory DRAM bytes of one implicit substep from its data flow, with
+    the Newton and Krylov counts the substep took.  Per particle: binning (X
+    read; key, index, offset written: 5.5 words), P2G (X, V, C, m: 16), per
+    Newton head the update (X, Fn, V0 read, F written: 22) and the force (X,
+    stress: 12), per Hessian product 22 words (X, Fn, F, V0) in the product's
+    precision, G2P (33) and the return map (21).  Per active grid node: P2G 4,
+    per head 9, per product 27 (operator input / output and the MINRES
+    vectors), G2P 3 words.  FP64 words unless stated."""
+    heads = st["newton_iterations"] + 1
+    nh = st["hvp_count"]
+    pw = 5.5 + 16 + heads * (22 + 12) + 33 + 21
+    nw = 4 + heads * 9 + nh * 27 + 3
+    return (P * pw + st["num_nodes"] * nw) * 8 + P * nh * 22 * hvp_word_bytes
+
+
 def timed_cpu_window(make, dt, warmup, steps, min_seconds, max_repeats=50):
     """The GPU's timed window on the oracle: a fresh scene from make(), `warmup`
     untimed substeps, then `steps` timed ones; repeated until `min_seconds` of
@@ -671,6 +687,12 @@ def main():
                          f"{reps}x, oracle port, {secs:.1f} s timed, scaled by {Pc}/1e6"}
 
     launches = sum(s["kernel_launches"] for s in st_mx)
+    sub_bytes = sum(substep_algorithmic_bytes(s_, P, 4) for s_ in st_mx) / len(st_mx)
+    sub_achieved = sub_bytes / (ms_mx / args.steps / 1e3) / 1e9
+    substep_roofline = {"bound": "hbm", "algorithmic_bytes": sub_bytes, "achieved": sub_achieved, "peak": peak, "unit": "GB/s",
+                        "frac": sub_achieved / peak, "peak_source": roofline["peak_source"],
+                        "model": "compulsory particle and node words of binning, P2G, each Newton head, each Hessian product, G2P "
+                                 "and the return map, at the substeps' own Newton / Krylov counts"}
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "substeps/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -683,7 +705,8 @@ def main():
             "fp64_value": fp64_value, "mixed_over_fp64": value / fp64_value,
             "rel_pos_err_vs_fp64": rel_err, "max_abs_err_over_dx": max_abs_dx, "accuracy_steps": total,
             "newton_krylov_per_step": [st_mx[-1]["newton_iterations"], st_mx[-1]["krylov_iterations"]],
-            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk,
+            "roofline": roofline, "substep_roofline": substep_roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
+            "clocks": clk,
         }
         print(json.dumps(line), flush=True)
     for s in sims.values():
