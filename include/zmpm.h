@@ -332,6 +332,37 @@ double zmpm_time(const zmpm_ctx* ctx);
    evolveStrain -> plasticity.  stats may be NULL. */
 int zmpm_substep(zmpm_ctx* ctx, double dt, const zmpm_solver* solver, zmpm_stats* stats);
 
+/* The implicit substep in the phases a reference subclass can override
+   (MpmSimulationBase virtuals, Lib/MPM/MpmSimulationBase.h:133-229; the
+   sequence of advanceOneTimeStep's implicit branch, MpmSimulationBase.cpp:
+   282-295).  zmpm_substep(ctx, dt, s, st) equals
+     zmpm_particles_to_grid(ctx, dt, s); zmpm_backward_euler_step(ctx, st);
+     zmpm_grid_to_particles(ctx, 1, st);
+   and a caller may run its own work between the calls (a fracture hook after
+   particlesToGrid, its own plasticity after gridToParticles).  Newton and ADMM
+   integrators only (ZMPM_UNSUPPORTED for ZMPM_EXPLICIT); a call out of order
+   returns ZMPM_NOT_READY, and a particle or plugin edit between the calls ends
+   the sequence.
+
+   reinitialize + particlesToGrid (MpmSimulationBase.cpp:146-230, 437-486): the
+   sort and page map, APIC P2G, the registered damage hook
+   (FractureSimulation::particlesToGrid, FractureSimulation.h:149-160) and the
+   Newton start (startBackwardEuler, :610-633) for step dt. */
+int zmpm_particles_to_grid(zmpm_ctx* ctx, double dt, const zmpm_solver* solver);
+/* backwardEulerStep (MpmSimulationBase.cpp:635-657), or AdmmSimulation's ADMM
+   solve when solver->integrator is ZMPM_ADMM, on the grid of the last
+   zmpm_particles_to_grid; fills the Newton fields of stats (may be NULL). */
+int zmpm_backward_euler_step(zmpm_ctx* ctx, zmpm_stats* stats);
+/* gridToParticles(dt) (MpmSimulationBase.cpp:879-1016): G2P, the particle
+   advection and CFL check, evolveStrain, and with apply_plasticity != 0 the
+   return maps of applyPlasticity (:1018-1030) in the same pass.  Ends the
+   substep: the context's time advances by dt; ZMPM_CFL_VIOLATION as
+   zmpm_substep. */
+int zmpm_grid_to_particles(zmpm_ctx* ctx, int32_t apply_plasticity, zmpm_stats* stats);
+/* MpmSimulationBase::applyPlasticity (MpmSimulationBase.cpp:1018-1030) alone:
+   every particle's plasticity return map on its current F. */
+int zmpm_apply_plasticity(zmpm_ctx* ctx);
+
 /* The CUDA stream (cudaStream_t) every kernel of this context runs on, so a
    caller can order its own work or CUDA events against the substep. */
 int zmpm_get_stream(zmpm_ctx* ctx, void** stream);
@@ -439,10 +470,13 @@ int zmpm_multiply(zmpm_ctx* ctx, const double* x, double* b, int32_t fp32);
    Scratch memory is one fixed device array inside the library (about 2.2 MB on
    every GPU that loads it, kept until exit); n above
    ZMPM_NOALLOC_MAX_PARTICLES is rejected with ZMPM_BAD_ARG.  The first call
-   on each device looks up that array's device address, so make it before any
-   stream capture.  Calls share the array: calls that overlap on the GPU race.
-   Returns ZMPM_OUT_OF_GRID if a particle's stencil leaves the grid.  The call
-   synchronises `stream` before it returns. */
+   on each device looks up that array's device address and keeps it for the
+   life of the process, so do not use this call after resetting the device
+   (cudaDeviceReset).  Calls share the array: calls that overlap on the GPU
+   race.  Returns ZMPM_OUT_OF_GRID if a particle's stencil leaves the grid or a
+   coordinate is not finite.  The call synchronises `stream` and reads a status
+   word back to the host before it returns, so it cannot be made inside a
+   stream capture. */
 int zmpm_sort_keys_noalloc(const double* x, int64_t n, double dx, int32_t precision, int32_t layout, int32_t grid_log2,
     uint64_t* keys, void* stream);
 

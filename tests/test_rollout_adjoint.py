@@ -86,3 +86,19 @@ def test_torch_autograd_wrapper(oracle):
     gE, gv = ro.backward(gX)
     np.testing.assert_allclose(Et.grad.numpy(), gE, rtol=1e-10)
     np.testing.assert_allclose(vt.grad.numpy(), gv, rtol=1e-10)
+
+
+def test_torch_wrapper_refuses_stale_backward(oracle):
+    """Two forward calls before a backward: the first call's backward raises
+    (the checkpoints hold the second call's states); the second one's gradient
+    keeps the shape of its input (a flat v0 stays flat)."""
+    s, E, v0, m = scene(oracle, n=2)
+    ro = Rollout(s, NU, 1e-3, 2, checkpoint_every=1)
+    Et = torch.tensor(E, requires_grad=True)
+    vt = torch.tensor(v0.reshape(-1), requires_grad=True)
+    X1 = DifferentiableRollout.apply(Et, vt, ro)
+    X2 = DifferentiableRollout.apply(Et, vt, ro)
+    with pytest.raises(RuntimeError, match="ran forward again"):
+        X1.sum().backward()
+    X2.sum().backward()
+    assert vt.grad.shape == vt.shape and Et.grad.shape == Et.shape

@@ -51,8 +51,9 @@ def test_noalloc_rejects_oversize_and_bad_input(cuda_lib):
     kd = torch.empty(n, dtype=torch.int64, device="cuda")
     rc = cuda_lib.sort_keys_noalloc(xd.data_ptr(), n, 1.0 / 64, abi.FP64, abi.LAYOUT_AUTO, 9, kd.data_ptr(), None)
     assert rc == abi.BAD_ARG
-    x = np.array([[0.5, 0.5, 0.5], [-0.5, 0.5, 0.5]])
-    xd = torch.tensor(x, device="cuda")
-    kd = torch.empty(2, dtype=torch.int64, device="cuda")
-    rc = cuda_lib.sort_keys_noalloc(xd.data_ptr(), 2, 1.0 / 64, abi.FP64, abi.LAYOUT_AUTO, 9, kd.data_ptr(), None)
-    assert rc == abi.OUT_OF_GRID
+    for bad in ([-0.5, 0.5, 0.5], [0.5, np.nan, 0.5], [np.inf, 0.5, 0.5]):
+        x = np.array([[0.5, 0.5, 0.5], bad])
+        xd = torch.tensor(x, device="cuda")
+        kd = torch.empty(2, dtype=torch.int64, device="cuda")
+        rc = cuda_lib.sort_keys_noalloc(xd.data_ptr(), 2, 1.0 / 64, abi.FP64, abi.LAYOUT_AUTO, 9, kd.data_ptr(), None)
+        assert rc == abi.OUT_OF_GRID, bad

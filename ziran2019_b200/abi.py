@@ -182,6 +182,10 @@ _PRODUCT_ONLY = {
     "write_state": (C.c_int, [C.c_void_p, C.c_char_p]),
     "read_state": (C.c_int, [C.c_void_p, C.c_char_p]),
     "write_bgeo": (C.c_int, [C.c_void_p, C.c_char_p, C.c_int32]),
+    "particles_to_grid": (C.c_int, [C.c_void_p, C.c_double, C.POINTER(Solver)]),
+    "backward_euler_step": (C.c_int, [C.c_void_p, C.POINTER(Stats)]),
+    "grid_to_particles": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(Stats)]),
+    "apply_plasticity": (C.c_int, [C.c_void_p]),
 }
 
 

@@ -199,6 +199,7 @@ int begin_edit(Ctx* ctx)
     ctx->uploaded = false;
     ctx->binned = false;
     ctx->implicit_ready = false;
+    ctx->phase = 0; // an edit ends a substep split into phases
     return ZMPM_OK;
 }
 
@@ -414,12 +415,6 @@ int zmpm_create(const zmpm_config* cfg, zmpm_ctx** out)
     }
     ctx->device = cfg->device;
     ctx->grid_log2 = cfg->grid_log2;
-    {
-        const char* f = getenv("ZMPM_HVP_FUSED");
-        ctx->hvp_fused = f && f[0] == '1';
-        const char* ng = getenv("ZMPM_NO_GRAPH");
-        ctx->no_graph = ng && ng[0] == '1';
-    }
     auto fail = [&](cudaError_t e) {
         ctx->err = cudaGetErrorString(e);
         delete ctx;
@@ -900,7 +895,7 @@ static int delete_phase_field_particles(zmpm_ctx* ctx)
 // k_mr_a + k_mr_b (MINRES) or k_apply_A_krylov + k_cg_b + k_cg_c (CG).
 static int64_t krylov_body_launches(const zmpm_ctx* ctx, const zmpm_solver& s)
 {
-    return (ctx->hvp_fused ? 1 : 2) + (s.linear_solver == ZMPM_MINRES ? 2 : 3);
+    return 2 + (s.linear_solver == ZMPM_MINRES ? 2 : 3);
 }
 
 // Kernels of one Newton loop body outside the Krylov loop: stress and force
@@ -925,7 +920,8 @@ static int begin_implicit_impl(zmpm_ctx* ctx, double dt, bool damage = true)
     return ZMPM_OK;
 }
 
-int zmpm_substep(zmpm_ctx* ctx, double dt, const zmpm_solver* s, zmpm_stats* st)
+// Argument checks and uploads shared by zmpm_substep and the phase entry points.
+static int substep_prepare(zmpm_ctx* ctx, double dt, const zmpm_solver* s)
 {
     if (!ctx || !s || !(dt > 0) || s->newton_max_iterations < 0 || s->krylov_max_iterations < 0) return ZMPM_BAD_ARG;
     const bool admm = s->integrator == ZMPM_ADMM, expl = s->integrator == ZMPM_EXPLICIT;
@@ -975,14 +971,17 @@ int zmpm_substep(zmpm_ctx* ctx, double dt, const zmpm_solver* s, zmpm_stats* st)
     }
     ctx->pf_iters = 0;
     ctx->pf_res = 0;
-    zmpm_stats local;
-    if (!st) st = &local;
-    std::memset(st, 0, sizeof(*st));
-    const int64_t launches0 = g_kernel_launches;
+    return ZMPM_OK;
+}
+
+// Phase 1 of a substep: reinitialize + particlesToGrid (+ the fracture hook and
+// the Newton start), or the explicit substep up to the grid update.
+static int substep_to_grid(zmpm_ctx* ctx, double dt, const zmpm_solver& s)
+{
+    const bool admm = s.integrator == ZMPM_ADMM, expl = s.integrator == ZMPM_EXPLICIT;
     ZMPM_CUDA(cudaEventRecord(ctx->ev0, ctx->stream));
-    int rc;
     if (expl) {
-        rc = upload(ctx);
+        int rc = upload(ctx);
         if (rc) return rc;
         ctx->dt = dt;
         ctx->implicit_ready = false;
@@ -991,17 +990,18 @@ int zmpm_substep(zmpm_ctx* ctx, double dt, const zmpm_solver* s, zmpm_stats* st)
         rc = run_binning(ctx);
         if (rc) return rc;
         ctx->graph_used = false;
-        rc = run_explicit(ctx, *s);
+        return run_explicit(ctx, s);
     }
-    else {
-        rc = begin_implicit_impl(ctx, dt, !admm);
-        if (rc) return rc;
-        rc = admm ? run_admm(ctx, *s) : run_newton(ctx, *s);
-    }
-    if (rc) return rc;
-    rc = run_g2p(ctx);
-    if (rc) return rc;
-    ZMPM_CUDA(cudaEventRecord(ctx->ev1, ctx->stream));
+    return begin_implicit_impl(ctx, dt, !admm);
+}
+
+// Reads the substep's device counters and scalars back (synchronises the
+// stream) and fills the statistics; `g2p_done`: the substep ended with G2P
+// (the time advances, and the CFL flag and the device time are final).
+static int substep_finish(zmpm_ctx* ctx, double dt, const zmpm_solver& s, zmpm_stats* st, int64_t launches0, bool g2p_done)
+{
+    const bool admm = s.integrator == ZMPM_ADMM, expl = s.integrator == ZMPM_EXPLICIT;
+    if (g2p_done) ZMPM_CUDA(cudaEventRecord(ctx->ev1, ctx->stream));
     SolverScalars hs;
     DevCounters hc;
     ZMPM_CUDA(cudaMemcpyAsync(&hs, ctx->scal.p, sizeof(hs), cudaMemcpyDeviceToHost, ctx->stream));
@@ -1011,16 +1011,18 @@ int zmpm_substep(zmpm_ctx* ctx, double dt, const zmpm_solver* s, zmpm_stats* st)
     // (after launching its own graph) or zmpm_destroy: destroying it here sat
     // in the GPU's idle time between substeps
     float ms = 0;
-    cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
-    ctx->time += dt;
-    ctx->implicit_ready = false;
+    if (g2p_done) {
+        cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+        ctx->time += dt;
+        ctx->implicit_ready = false;
+    }
     st->newton_iterations = hs.newton_iters;
     st->krylov_iterations = hs.krylov_iters;
     st->hvp_count = hs.hvp_count;
     st->newton_converged = hs.converged;
     st->newton_residual_initial = hs.res_initial;
     st->newton_residual_final = hs.res_final;
-    st->cfl_violation = (hc.flags & FLAG_CFL) ? 1 : 0;
+    st->cfl_violation = (g2p_done && (hc.flags & FLAG_CFL)) ? 1 : 0;
     st->status_flags = ((hc.flags & FLAG_NAN) || !(hs.res_final == hs.res_final) ? 1 : 0) | ((hc.flags & FLAG_TIMEOUT) ? 2 : 0);
     st->num_particles = ctx->P;
     st->num_groups = ctx->G;
@@ -1034,7 +1036,8 @@ int zmpm_substep(zmpm_ctx* ctx, double dt, const zmpm_solver* s, zmpm_stats* st)
     if (ctx->graph_used && admm) // ADMM iteration: 7 head + 3 tail kernels; Krylov body: operator (2), k_mr_a, k_mr_b
         g_kernel_launches += 10 * (int64_t)hs.nit + 4 * (int64_t)hs.krylov_bodies;
     else if (ctx->graph_used)
-        g_kernel_launches += newton_body_launches(ctx) * (int64_t)hs.nit + krylov_body_launches(ctx, *s) * (int64_t)hs.krylov_bodies;
+        g_kernel_launches += newton_body_launches(ctx) * (int64_t)hs.nit + krylov_body_launches(ctx, s) * (int64_t)hs.krylov_bodies;
+    ctx->graph_used = false;
     st->kernel_launches = (int32_t)(g_kernel_launches - launches0);
     ctx->N = hc.N;
     if (ctx->prof_newton > 0) {
@@ -1058,6 +1061,94 @@ int zmpm_substep(zmpm_ctx* ctx, double dt, const zmpm_solver* s, zmpm_stats* st)
     }
     if (st->status_flags & 1) return ZMPM_NAN_DETECTED;
     return st->cfl_violation ? ZMPM_CFL_VIOLATION : ZMPM_OK;
+}
+
+int zmpm_substep(zmpm_ctx* ctx, double dt, const zmpm_solver* s, zmpm_stats* st)
+{
+    int rc = substep_prepare(ctx, dt, s);
+    if (rc) return rc;
+    const bool admm = s->integrator == ZMPM_ADMM, expl = s->integrator == ZMPM_EXPLICIT;
+    zmpm_stats local;
+    if (!st) st = &local;
+    std::memset(st, 0, sizeof(*st));
+    const int64_t launches0 = g_kernel_launches;
+    ctx->phase = 0;
+    rc = substep_to_grid(ctx, dt, *s);
+    if (rc) return rc;
+    if (!expl) {
+        rc = admm ? run_admm(ctx, *s) : run_newton(ctx, *s);
+        if (rc) return rc;
+    }
+    rc = run_g2p(ctx);
+    if (rc) return rc;
+    return substep_finish(ctx, dt, *s, st, launches0, true);
+}
+
+// ------------------------------------------------------------ substep phases --
+int zmpm_particles_to_grid(zmpm_ctx* ctx, double dt, const zmpm_solver* s)
+{
+    int rc = substep_prepare(ctx, dt, s);
+    if (rc) return rc;
+    if (s->integrator == ZMPM_EXPLICIT) {
+        ctx->err = "the phase entry points run the implicit (Newton or ADMM) substep";
+        return ZMPM_UNSUPPORTED;
+    }
+    ctx->phase = 0;
+    rc = substep_to_grid(ctx, dt, *s);
+    if (rc) return rc;
+    ctx->phase = 1;
+    ctx->phase_solver = *s;
+    ctx->phase_launches0 = g_kernel_launches;
+    return ZMPM_OK;
+}
+
+int zmpm_backward_euler_step(zmpm_ctx* ctx, zmpm_stats* st)
+{
+    if (!ctx) return ZMPM_BAD_ARG;
+    if (ctx->phase != 1 || !ctx->implicit_ready) {
+        ctx->err = "zmpm_backward_euler_step follows zmpm_particles_to_grid";
+        return ZMPM_NOT_READY;
+    }
+    cudaSetDevice(ctx->device);
+    const zmpm_solver& s = ctx->phase_solver;
+    zmpm_stats local;
+    if (!st) st = &local;
+    std::memset(st, 0, sizeof(*st));
+    int rc = s.integrator == ZMPM_ADMM ? run_admm(ctx, s) : run_newton(ctx, s);
+    if (rc) return rc;
+    ctx->phase = 2;
+    return substep_finish(ctx, ctx->dt, s, st, ctx->phase_launches0, false);
+}
+
+int zmpm_grid_to_particles(zmpm_ctx* ctx, int32_t apply_plasticity, zmpm_stats* st)
+{
+    if (!ctx) return ZMPM_BAD_ARG;
+    if (ctx->phase != 2) {
+        ctx->err = "zmpm_grid_to_particles follows zmpm_backward_euler_step";
+        return ZMPM_NOT_READY;
+    }
+    cudaSetDevice(ctx->device);
+    zmpm_stats local;
+    if (!st) st = &local;
+    std::memset(st, 0, sizeof(*st));
+    const int64_t launches0 = g_kernel_launches;
+    int rc = run_g2p(ctx, apply_plasticity != 0);
+    if (rc) return rc;
+    ctx->phase = 0;
+    return substep_finish(ctx, ctx->dt, ctx->phase_solver, st, launches0, true);
+}
+
+int zmpm_apply_plasticity(zmpm_ctx* ctx)
+{
+    if (!ctx) return ZMPM_BAD_ARG;
+    cudaSetDevice(ctx->device);
+    int rc = upload(ctx);
+    if (rc) return rc;
+    rc = launch_plasticity(ctx);
+    if (rc) return rc;
+    ZMPM_CUDA(cudaGetLastError());
+    ZMPM_CUDA(cudaStreamSynchronize(ctx->stream));
+    return ZMPM_OK;
 }
 
 // ---------------------------------------------------------------- adjoint --
@@ -1287,6 +1378,7 @@ int zmpm_begin_implicit(zmpm_ctx* ctx, double dt, int64_t* num_nodes)
 {
     if (!ctx || !(dt > 0)) return ZMPM_BAD_ARG;
     cudaSetDevice(ctx->device);
+    ctx->phase = 0;
     int rc = begin_implicit_impl(ctx, dt);
     if (rc) return rc;
     std::vector<int64_t> idx;

@@ -47,8 +47,10 @@ __global__ void k_keys(const double* __restrict__ x, int64_t cap, int64_t P, dou
     int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= P) return;
     int b[3];
+    bool finite = true;
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
+        finite = finite && isfinite(x[d * cap + s]);
         if constexpr (sizeof(KT) == 8) {
             double t = __dmul_rn(x[d * cap + s], inv_dx_d);
             b[d] = int_floor_d(__dsub_rn(t, 0.5));
@@ -59,7 +61,8 @@ __global__ void k_keys(const double* __restrict__ x, int64_t cap, int64_t P, dou
         }
     }
     int p0 = b[0] >> L::XB, p1 = b[1] >> L::YB, p2 = b[2] >> L::ZB;
-    bool bad = b[0] < 0 || b[1] < 0 || b[2] < 0 || p0 + 1 >= pd.px || p1 + 1 >= pd.py || p2 + 1 >= pd.pz;
+    // a non-finite position converts to an arbitrary integer: it is out of the grid
+    bool bad = !finite || b[0] < 0 || b[1] < 0 || b[2] < 0 || p0 + 1 >= pd.px || p1 + 1 >= pd.py || p2 + 1 >= pd.pz;
     if (bad) {
         atomicOr(flags, (int32_t)FLAG_OUT_OF_GRID);
         b[0] = b[1] = b[2] = 0;

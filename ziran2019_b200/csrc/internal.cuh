@@ -167,8 +167,6 @@ struct Ctx {
     DBuf scratch;      // Hessian scratch [NS][Pcap] in the HVP precision
     DBuf stress;       // [9][Pcap] V0 P(F) Fn^T of the current Newton iterate
     DBuf dstress;      // [9][Pcap] dS of one Hessian-vector product (HVP precision)
-    bool hvp_fused = false; // one fused HVP kernel instead of stress + scatter
-    bool no_graph = false;  // host-driven Newton loop instead of the conditional graph
     cudaGraphExec_t graph_exec = nullptr; // last solve graph, released when the next one is launched
     bool graph_used = false;              // the last Newton solve ran as a graph
     DBuf frac;         // [3][Pcap] fractional offsets in cells (FP32 HVP)
@@ -210,6 +208,10 @@ struct Ctx {
     std::vector<double> ckpt_time;
     std::vector<int64_t> ckpt_P;
     bool admm_used = false;               // the last substep ran ADMM (launch accounting)
+    // substep phases: 1 after zmpm_particles_to_grid, 2 after zmpm_backward_euler_step
+    int phase = 0;
+    zmpm_solver phase_solver{};
+    int64_t phase_launches0 = 0;
     int admm_iters = 0;
 
     int npb() const { return layout == 1 ? 32 : 64; }
@@ -228,7 +230,8 @@ struct Ctx {
 int run_binning(Ctx* ctx);
 int run_p2g(Ctx* ctx, bool damage = true);            // P2G (+ damage hook) + grid normalisation + Newton setup
 int run_newton(Ctx* ctx, const zmpm_solver& s);       // backward-Euler Newton
-int run_g2p(Ctx* ctx);                                 // G2P + evolveStrain + plasticity
+int run_g2p(Ctx* ctx, bool plastic = true);            // G2P + evolveStrain (+ applyPlasticity)
+int launch_plasticity(Ctx* ctx);                       // applyPlasticity alone
 int upload_colliders(Ctx* ctx, double time, int slot = 0);    // slot 1: the state at t + dt
 int upload(Ctx* ctx);      // host scene arrays -> device pools (once per edit)
 int download(Ctx* ctx);    // device pools -> host scene arrays (particle order)

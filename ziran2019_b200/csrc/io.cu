@@ -22,6 +22,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <exception>
 #include <string>
 #include <vector>
 
@@ -314,6 +315,22 @@ int zmpm_read_state(zmpm_ctx* ctx, const char* path)
         ctx->err = "corrupt restart header";
         return ZMPM_BAD_ARG;
     }
+    // the particle index must fit the binning key, as zmpm_add_particles requires
+    if (P >= ((int64_t)1 << (ctx->layout == 1 ? Layout244::INDEX_BITS : Layout444::INDEX_BITS))) {
+        ctx->err = "particle count exceeds the key's index bits (MpmSimulationBase.cpp:1037-1038)";
+        return ZMPM_BAD_ARG;
+    }
+    // every particle holds at least one byte of every field: P cannot exceed the bytes left
+    const long here = std::ftell(f.f);
+    if (here < 0 || std::fseek(f.f, 0, SEEK_END) != 0) {
+        ctx->err = "restart file is not seekable";
+        return ZMPM_BAD_ARG;
+    }
+    const long end = std::ftell(f.f);
+    if (end < here || std::fseek(f.f, here, SEEK_SET) != 0 || P > (int64_t)(end - here)) {
+        ctx->err = "restart file is shorter than its particle count";
+        return ZMPM_BAD_ARG;
+    }
     std::vector<zmpm_collider> cols(ncol);
     for (auto& c : cols) c = f.get<zmpm_collider>();
     // stage the arrays as bytes so that a failed read leaves ctx intact
@@ -335,7 +352,18 @@ int zmpm_read_state(zmpm_ctx* ctx, const char* path)
             return ZMPM_BAD_ARG;
         }
         seen[idx] = true;
-        staged[idx].resize((size_t)P * comps * type_size(type));
+        const size_t bytes = (size_t)P * comps * type_size(type);
+        if (bytes > (size_t)(end - here)) {
+            ctx->err = "restart file is shorter than its field " + name;
+            return ZMPM_BAD_ARG;
+        }
+        try {
+            staged[idx].resize(bytes);
+        }
+        catch (const std::exception&) {
+            ctx->err = "no host memory to stage the restart file";
+            return ZMPM_NO_MEMORY;
+        }
         f.get(staged[idx].data(), staged[idx].size());
     }
     for (size_t i = 0; i < fields.size(); ++i)
@@ -349,9 +377,15 @@ int zmpm_read_state(zmpm_ctx* ctx, const char* path)
     }
     int rc = begin_edit(ctx);
     if (rc) return rc;
-    for (size_t i = 0; i < fields.size(); ++i) {
-        field_resize(fields[i], (size_t)P * fields[i].comps);
-        if (!staged[i].empty()) std::memcpy(field_data(fields[i]), staged[i].data(), staged[i].size());
+    try {
+        for (size_t i = 0; i < fields.size(); ++i) {
+            field_resize(fields[i], (size_t)P * fields[i].comps);
+            if (!staged[i].empty()) std::memcpy(field_data(fields[i]), staged[i].data(), staged[i].size());
+        }
+    }
+    catch (const std::exception&) {
+        ctx->err = "no host memory for the restart file's particles";
+        return ZMPM_NO_MEMORY;
     }
     ctx->P = P;
     ctx->time = time;

@@ -13,7 +13,11 @@
 // the array's name is only a host-side stand-in, never a device address: the
 // device address is looked up once per device with cudaGetSymbolAddress (with
 // that device current) and passed to the kernels.  The first call on a device
-// performs that lookup, so make the first call before any stream capture.
+// performs that lookup and caches the address for the life of the process; a
+// caller that resets the device (cudaDeviceReset) invalidates that cached
+// address, so this entry point must not be used after such a reset.  Each call
+// synchronises its stream and copies a status word to host memory, so no call
+// can be made inside a stream capture.
 // Every call reuses the same array and it keeps the previous call's contents:
 // the out-of-grid flag is cleared at the start of each call, and everything
 // else is fully written before it is read.  Calls whose work overlaps on the
@@ -74,15 +78,19 @@ __global__ void k_noalloc_keys(const double* __restrict__ x, int64_t n, double i
     int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     int b[3];
+    bool finite = true;
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
+        const double xd = x[3 * i + d];
+        finite = finite && isfinite(xd);
         if constexpr (sizeof(KT) == 8)
-            b[d] = floor_d(__dsub_rn(__dmul_rn(x[3 * i + d], inv_dx_d), 0.5));
+            b[d] = floor_d(__dsub_rn(__dmul_rn(xd, inv_dx_d), 0.5));
         else
-            b[d] = floor_f(__fsub_rn(__fmul_rn((float)x[3 * i + d], inv_dx_f), 0.5f));
+            b[d] = floor_f(__fsub_rn(__fmul_rn((float)xd, inv_dx_f), 0.5f));
     }
     int p0 = b[0] >> L::XB, p1 = b[1] >> L::YB, p2 = b[2] >> L::ZB;
-    if (b[0] < 0 || b[1] < 0 || b[2] < 0 || p0 + 1 >= px || p1 + 1 >= py || p2 + 1 >= pz) {
+    // a non-finite coordinate converts to an arbitrary integer: it is out of the grid
+    if (!finite || b[0] < 0 || b[1] < 0 || b[2] < 0 || p0 + 1 >= px || p1 + 1 >= py || p2 + 1 >= pz) {
         atomicOr(flags, 1);
         b[0] = b[1] = b[2] = 0;
         p0 = p1 = p2 = 0;
@@ -113,12 +121,13 @@ int sort_keys(const double* x, int64_t n, double dx, int grid_log2, uint64_t* ke
     if (cudaMemsetAsync(flags, 0, sizeof(int32_t), st) != cudaSuccess) return ZMPM_CUDA_ERROR;
     k_noalloc_keys<L, KT><<<(unsigned)((n + 255) / 256), 256, 0, st>>>(x, n, 1.0 / dx, 1.0f / (float)dx, px, py, pz, keys, flags);
     ++g_kernel_launches;
+    // a launch failure of this call (peeked, so an error the caller left pending is not cleared)
+    if (cudaPeekAtLastError() != cudaSuccess) return ZMPM_CUDA_ERROR;
     uint64_t* out = radix_sort(keys, alt, n, L::INDEX_BITS, key_bits, radix, st);
     if (out != keys && cudaMemcpyAsync(keys, out, n * sizeof(uint64_t), cudaMemcpyDeviceToDevice, st) != cudaSuccess) return ZMPM_CUDA_ERROR;
     int32_t hflag = 0;
     if (cudaMemcpyAsync(&hflag, flags, sizeof(int32_t), cudaMemcpyDeviceToHost, st) != cudaSuccess) return ZMPM_CUDA_ERROR;
     if (cudaStreamSynchronize(st) != cudaSuccess) return ZMPM_CUDA_ERROR;
-    if (cudaGetLastError() != cudaSuccess) return ZMPM_CUDA_ERROR;
     return hflag ? ZMPM_OUT_OF_GRID : ZMPM_OK;
 }
 

@@ -26,7 +26,7 @@
 namespace zmpm {
 
 int launch_p2g(Ctx* ctx);
-int launch_g2p(Ctx* ctx);
+int launch_g2p(Ctx* ctx, bool plastic);
 int launch_hvp_krylov(Ctx* ctx, const double* x0, const double* x1, bool alt, double* out);
 
 __device__ __forceinline__ void project3(const int8_t* col, const double* P6, int64_t nn, int64_t n, double v[3])
@@ -1351,7 +1351,7 @@ static int newton_impl(Ctx* ctx, const zmpm_solver& s)
     L.np.minres = s.linear_solver == ZMPM_MINRES ? 1 : 0;
     L.np.escalate = ctx->mixed ? 1 : 0;
     // MIXED MINRES runs its split FP32 product on FP32 copies of Z
-    const bool zf = ctx->mixed && L.np.minres && !ctx->hvp_fused;
+    const bool zf = ctx->mixed && L.np.minres;
     L.kb.Zf[0] = zf ? ctx->kvf.as<float>() : nullptr;
     L.kb.Zf[1] = zf ? ctx->kvf.as<float>() + 3 * L.ng.nn : nullptr;
     L.np.kmax = s.krylov_max_iterations;
@@ -1371,7 +1371,7 @@ static int newton_impl(Ctx* ctx, const zmpm_solver& s)
     ctx->graph_used = false;
     if (L.ng.nn == 0 || s.newton_max_iterations == 0) return ZMPM_OK;
     const bool prof = ctx->profiling && s.newton_max_iterations <= 64;
-    if (!prof && !ctx->no_graph) {
+    if (!prof) {
         // whole solve as one graph with device-side loop conditions
         cudaGraphExec_t exec = nullptr;
         const int64_t launches0 = g_kernel_launches;
@@ -1532,7 +1532,7 @@ static int admm_impl(Ctx* ctx, const zmpm_solver& s)
     };
 
     if (s.admm_iterations > 0) {
-        if (!ctx->profiling && !ctx->no_graph) {
+        if (!ctx->profiling) {
             cudaGraphExec_t exec = nullptr;
             const int64_t launches0 = g_kernel_launches;
             rc = loop_graph(
@@ -1635,7 +1635,7 @@ int run_adjoint_solve(Ctx* ctx, double tol, int max_iterations)
         ++g_kernel_launches;
         return (int)ZMPM_OK;
     };
-    if (!ctx->no_graph) {
+    if (!ctx->profiling) {
         cudaGraphExec_t exec = nullptr;
         const int64_t launches0 = g_kernel_launches;
         int rc = loop_graph(
@@ -1676,9 +1676,9 @@ int run_admm(Ctx* ctx, const zmpm_solver& s)
     return ctx->layout == 1 ? admm_impl<Layout244>(ctx, s) : admm_impl<Layout444>(ctx, s);
 }
 
-int run_g2p(Ctx* ctx)
+int run_g2p(Ctx* ctx, bool plastic)
 {
-    int rc = launch_g2p(ctx);
+    int rc = launch_g2p(ctx, plastic);
     if (rc) return rc;
     ZMPM_CUDA(cudaGetLastError());
     return ZMPM_OK;

@@ -5,9 +5,9 @@
 //  k_stress  MpmForceBase::updatePositionBasedState (MpmForceBase.cpp:306-344):
 //            G2P of grad(vn+dv), F = (I + dt grad v) Fn, stress and Hessian scratch
 //  k_force   rasterizeForceToTVStack (MpmForceBase.cpp:102-152)
-//  k_hvp     MpmForceBase::addScaledForceDifferential (MpmForceBase.cpp:259-302)
-//            fused: G2P of grad(dv), dS = V0 dP Fn^T, P2G of dS grad w
-//            (k_hvp_stress + k_hvp_scatter: the split form)
+//  k_hvp_stress + k_hvp_scatter
+//            MpmForceBase::addScaledForceDifferential (MpmForceBase.cpp:259-302):
+//            G2P of grad(dv), dS = V0 dP Fn^T, P2G of dS grad w
 //  k_g2p     gridToParticlesHelper<APIC> (MpmSimulationBase.cpp:906-1016) +
 //            evolveStrain + applyPlasticity (:1018-1030)
 #include "admm.cuh"
@@ -397,71 +397,10 @@ __global__ void __launch_bounds__(XF_THREADS) k_force(const int32_t* __restrict_
 }
 
 // ------------------------------------------------------------------ HVP ----
-// out += sum_p dS_p grad w_ip with dS = V0 dP(grad(x) Fn) Fn^T; TH is the
-// arithmetic precision (float in mixed runs).  Skipped when the linear solve
-// is inactive.
-template <class L, class TH>
-__global__ void __launch_bounds__(XF_THREADS, sizeof(TH) == 4 ? 4 : 2) k_hvp(const int32_t* __restrict__ group_start, const int32_t* __restrict__ group_nbr,
-    const int32_t* __restrict__ pi, int64_t cap, const short4* __restrict__ base, double dx, const TH* __restrict__ frac,
-    const TH* __restrict__ scr, const double* __restrict__ x0, const double* __restrict__ x1, int alt, double* __restrict__ out,
-    const SolverScalars* __restrict__ sc, int32_t* __restrict__ flags)
-{
-    if (sc && (sc->newton_done || !sc->kactive)) return;
-    constexpr int NPB = L::NPB;
-    __shared__ __align__(128) double win[8 * 3 * NPB];
-    __shared__ __align__(16) TH acc[8 * 3 * NPB];
-    __shared__ int32_t nbr[8];
-    __shared__ __align__(8) uint64_t bar;
-    __shared__ CellLayout<L> cl;
-    const int g = blockIdx.x;
-    if (threadIdx.x < 8) nbr[threadIdx.x] = group_nbr[8 * g + threadIdx.x];
-    zero_window<3, NPB>(acc);
-    __syncthreads();
-    // the input alternates between x0 and x1 with the Krylov iteration (MINRES)
-    const double* x = (alt && sc && (sc->kit & 1)) ? x1 : x0;
-    stage_window<NPB>(win, x, nbr, &bar, flags);
-    const TH inv_dx = TH(1.0 / dx);
-    const int s0 = group_start[g], s1 = group_start[g + 1];
-    build_cell_layout<L>(cl, base, s0, s1);
-    for (int q = threadIdx.x; q < cl.layers * NPB; q += blockDim.x) {
-        const int r = q / NPB, ce = q % NPB;
-        if (r >= cl.cnt[ce]) continue;
-        const int s = s0 + cl.start[ce] + r;
-        const int kind = pi[PI_KIND * cap + s];
-        if (kind == ZMPM_MODEL_NONE) continue;
-        const short4 b = base[s];
-        TH w[3][3], dwr[3][3];
-#pragma unroll
-        for (int d = 0; d < 3; ++d) bspline(frac[d * cap + s], w[d], dwr[d]);
-        const int lx = b.x & (L::BX - 1), ly = b.y & (L::BY - 1), lz = b.z & (L::BZ - 1);
-        M3<TH> G = m3_zero<TH>();
-        for_stencil<L>(lx, ly, lz, w, dwr, inv_dx, [&](int t, int e, int, int, int, TH, const TH* dw) {
-            const double* vv = win + t * 3 * NPB + e;
-#pragma unroll
-            for (int r = 0; r < 3; ++r) {
-                TH vr = (TH)vv[r * NPB];
-#pragma unroll
-                for (int c = 0; c < 3; ++c) G(r, c) += vr * dw[c];
-            }
-        });
-        M3<TH> dS = model_hvp<TH>(kind, scr, cap, s, G);
-        // recomputed rather than kept live across the constitutive step
-#pragma unroll
-        for (int d = 0; d < 3; ++d) bspline(frac[d * cap + s], w[d], dwr[d]);
-        for_stencil<L>(lx, ly, lz, w, dwr, inv_dx, [&](int t, int e, int, int, int, TH, const TH* dw) {
-            TH* a = acc + t * 3 * NPB + e;
-#pragma unroll
-            for (int r = 0; r < 3; ++r) atomicAdd(a + r * NPB, dS(r, 0) * dw[0] + dS(r, 1) * dw[1] + dS(r, 2) * dw[2]);
-        });
-    }
-    __syncthreads();
-    flush_window<3, 3, NPB>(acc, nbr, out, nullptr);
-}
-
-// Split form of the same product (two kernels, dS round-trips through HBM in
-// the HVP precision): k_hvp_stress gathers grad(x) and evaluates dS in slot
-// order; k_hvp_scatter adds dS grad w with the layered scatter.  Each half
-// holds far fewer live registers than the fused kernel.
+// out += sum_p dS_p grad w_ip with dS = V0 dP(grad(x) Fn) Fn^T, as two kernels
+// (dS round-trips through HBM in the HVP precision): k_hvp_stress gathers
+// grad(x) and evaluates dS in slot order; k_hvp_scatter adds dS grad w with the
+// layered scatter.
 // TX: the input vector's type (FP64, or the FP32 copy MINRES keeps for MIXED
 // products, which halves the staged window and needs no conversions).  FP32:
 // eight CTAs per SM (64 registers, a few bytes spilled; product 1.6% faster
@@ -597,13 +536,64 @@ __global__ void __launch_bounds__(XF_THREADS) k_hvp_scatter(const int32_t* __res
 }
 
 // ------------------------------------------------------------------ G2P ----
+// MpmSimulationBase::applyPlasticity (MpmSimulationBase.cpp:1018-1030) on one
+// particle (slot s): the return map of its plasticity kind applied to F, with
+// the kind's state (log Jp; yield stress, broken flag and crack normal) updated
+// in the pools.
+__device__ __forceinline__ void apply_return_map(double* __restrict__ pd, int32_t* __restrict__ pi, int64_t cap, int64_t s, M3<double>& F)
+{
+    const int pkind = pi[PI_PKIND * cap + s];
+    if (pkind == ZMPM_PLASTIC_DRUCKER_PRAGER || pkind == ZMPM_PLASTIC_CAM_CLAY) {
+        double logJp = pd[PD_LOGJP * cap + s];
+        if (pkind == ZMPM_PLASTIC_DRUCKER_PRAGER)
+            drucker_prager_project<double>(pd[PD_MU * cap + s], pd[PD_LAM * cap + s], pd[PD_YS * cap + s], pd[PD_XI * cap + s],
+                pd[PD_FS * cap + s], pi[PI_BROKEN * cap + s], logJp, F);
+        else
+            cam_clay_project<double>(pd[PD_MU * cap + s], pd[PD_KAPPA * cap + s], pd[PD_YS * cap + s], pd[PD_XI * cap + s],
+                pd[PD_FS * cap + s], logJp, F);
+        pd[PD_LOGJP * cap + s] = logJp;
+    }
+    if (pkind == ZMPM_PLASTIC_VON_MISES) {
+        double ys = pd[PD_YS * cap + s];
+        int broken = pi[PI_BROKEN * cap + s];
+        double crack[3] = { pd[(PD_CRACK + 0) * cap + s], pd[(PD_CRACK + 1) * cap + s], pd[(PD_CRACK + 2) * cap + s] };
+        von_mises_project<double>(pd[PD_MU * cap + s], pd[PD_LAM * cap + s], ys, pd[PD_XI * cap + s], pd[PD_FS * cap + s], broken, crack, F);
+        pd[PD_YS * cap + s] = ys;
+        pi[PI_BROKEN * cap + s] = broken;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) pd[(PD_CRACK + d) * cap + s] = crack[d];
+    }
+}
+
+// applyPlasticity as its own pass (slot order), for callers that run
+// gridToParticles without it.
+__global__ void k_plasticity(double* __restrict__ pd, int32_t* __restrict__ pi, int64_t cap, int64_t P)
+{
+    const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= P || pi[PI_KIND * cap + s] == ZMPM_MODEL_NONE || pi[PI_PKIND * cap + s] == ZMPM_PLASTIC_NONE) return;
+    M3<double> F;
+#pragma unroll
+    for (int q = 0; q < 9; ++q) F.a[q] = pd[(PD_F + q) * cap + s];
+    apply_return_map(pd, pi, cap, s, F);
+#pragma unroll
+    for (int q = 0; q < 9; ++q) pd[(PD_F + q) * cap + s] = F.a[q];
+}
+
+int launch_plasticity(Ctx* ctx)
+{
+    if (ctx->P == 0) return ZMPM_OK;
+    k_plasticity<<<(unsigned)((ctx->P + 127) / 128), 128, 0, ctx->stream>>>(ctx->pd.as<double>(), ctx->pi.as<int32_t>(), ctx->Pcap, ctx->P);
+    ++g_kernel_launches;
+    return ZMPM_OK;
+}
+
 // Three CTAs per SM (at most 168 registers): G2P and P2G are latency bound on
 // FP64 chains, and the third CTA outweighs the few spilled registers (about
 // 1.5% of the 1M-particle substep, same-box A/B).
 template <class L>
 __global__ void __launch_bounds__(XF_THREADS, 3) k_g2p(const int32_t* __restrict__ group_start, const int32_t* __restrict__ group_nbr,
     double* __restrict__ pd, int32_t* __restrict__ pi, int64_t cap, const short4* __restrict__ base, double dx, double dt,
-    double apic_rpic_ratio, const double* __restrict__ vnew, int32_t* __restrict__ flags, int mls)
+    double apic_rpic_ratio, const double* __restrict__ vnew, int32_t* __restrict__ flags, int mls, int plastic)
 {
     constexpr int NPB = L::NPB;
     __shared__ __align__(128) double win[8 * 3 * NPB];
@@ -670,27 +660,7 @@ __global__ void __launch_bounds__(XF_THREADS, 3) k_g2p(const int32_t* __restrict
             A.a[q] += dt * gv.a[q];
         }
         M3<double> F = m3_mul(A, F0);
-        const int pkind = pi[PI_PKIND * cap + s];
-        if (pkind == ZMPM_PLASTIC_DRUCKER_PRAGER || pkind == ZMPM_PLASTIC_CAM_CLAY) {
-            double logJp = pd[PD_LOGJP * cap + s];
-            if (pkind == ZMPM_PLASTIC_DRUCKER_PRAGER)
-                drucker_prager_project<double>(pd[PD_MU * cap + s], pd[PD_LAM * cap + s], pd[PD_YS * cap + s], pd[PD_XI * cap + s],
-                    pd[PD_FS * cap + s], pi[PI_BROKEN * cap + s], logJp, F);
-            else
-                cam_clay_project<double>(pd[PD_MU * cap + s], pd[PD_KAPPA * cap + s], pd[PD_YS * cap + s], pd[PD_XI * cap + s],
-                    pd[PD_FS * cap + s], logJp, F);
-            pd[PD_LOGJP * cap + s] = logJp;
-        }
-        if (pkind == ZMPM_PLASTIC_VON_MISES) {
-            double ys = pd[PD_YS * cap + s];
-            int broken = pi[PI_BROKEN * cap + s];
-            double crack[3] = { pd[(PD_CRACK + 0) * cap + s], pd[(PD_CRACK + 1) * cap + s], pd[(PD_CRACK + 2) * cap + s] };
-            von_mises_project<double>(pd[PD_MU * cap + s], pd[PD_LAM * cap + s], ys, pd[PD_XI * cap + s], pd[PD_FS * cap + s], broken, crack, F);
-            pd[PD_YS * cap + s] = ys;
-            pi[PI_BROKEN * cap + s] = broken;
-#pragma unroll
-            for (int d = 0; d < 3; ++d) pd[(PD_CRACK + d) * cap + s] = crack[d];
-        }
+        if (plastic) apply_return_map(pd, pi, cap, s, F);
 #pragma unroll
         for (int q = 0; q < 9; ++q) pd[(PD_F + q) * cap + s] = F.a[q];
         if (pi[PI_VISCO * cap + s]) {
@@ -772,13 +742,6 @@ static void hvp_launch(Ctx* ctx, const double* x0, const double* x1, int alt, do
 {
     const int64_t G = ctx->G;
     DevCounters* dc = ctx->counters.as<DevCounters>();
-    if (ctx->hvp_fused) {
-        k_hvp<L, TH><<<(unsigned)G, XF_THREADS, 0, ctx->stream>>>(ctx->group_start.as<int32_t>(), ctx->group_nbr.as<int32_t>(),
-            ctx->pi.as<int32_t>(), ctx->Pcap, ctx->base.as<short4>(), ctx->cfg.dx, ctx->frac.as<TH>(), ctx->scratch.as<TH>(), x0, x1, alt, out,
-            sc, &dc->flags);
-        ++g_kernel_launches;
-        return;
-    }
     k_hvp_stress<L, TH><<<(unsigned)G, XF_THREADS, 0, ctx->stream>>>(ctx->group_start.as<int32_t>(), ctx->group_nbr.as<int32_t>(),
         ctx->pi.as<int32_t>(), ctx->Pcap, ctx->base.as<short4>(), ctx->cfg.dx, ctx->frac.as<TH>(), ctx->scratch.as<TH>(), x0, x1, alt,
         ctx->dstress.as<TH>(), sc, &dc->flags);
@@ -875,17 +838,17 @@ int launch_hvp_scatter(Ctx* ctx, double* out, bool gated)
 }
 
 template <class L>
-static int g2p_impl(Ctx* ctx)
+static int g2p_impl(Ctx* ctx, bool plastic)
 {
     const int64_t G = ctx->G;
     if (G == 0) return ZMPM_OK;
     DevCounters* dc = ctx->counters.as<DevCounters>();
     k_g2p<L><<<(unsigned)G, XF_THREADS, 0, ctx->stream>>>(ctx->group_start.as<int32_t>(), ctx->group_nbr.as<int32_t>(), ctx->pd.as<double>(),
         ctx->pi.as<int32_t>(), ctx->Pcap, ctx->base.as<short4>(), ctx->cfg.dx, ctx->dt, ctx->cfg.apic_rpic_ratio, ctx->vstar.as<double>(), &dc->flags,
-        ctx->mls ? 1 : 0);
+        ctx->mls ? 1 : 0, plastic ? 1 : 0);
     ++g_kernel_launches;
     return ZMPM_OK;
 }
-int launch_g2p(Ctx* ctx) { return ctx->layout == 1 ? g2p_impl<Layout244>(ctx) : g2p_impl<Layout444>(ctx); }
+int launch_g2p(Ctx* ctx, bool plastic) { return ctx->layout == 1 ? g2p_impl<Layout244>(ctx, plastic) : g2p_impl<Layout444>(ctx, plastic); }
 
 } // namespace zmpm

@@ -418,6 +418,29 @@ class MpmSimulation:
         self.last_status = rc
         return rc
 
+    # the implicit substep in the phases of MpmSimulationBase's virtuals
+    # (MpmSimulationBase.h:133-229), for callers that run their own work between them
+    def particlesToGrid(self, dt):
+        """reinitialize + particlesToGrid (+ the damage hook and the Newton start)."""
+        s = self.solver()
+        return self._call("particles_to_grid", float(dt), abi.C.byref(s))
+
+    def backwardEulerStep(self):
+        st = abi.Stats()
+        rc = self._call("backward_euler_step", abi.C.byref(st))
+        self.last_stats = st.as_dict()
+        return rc
+
+    def gridToParticles(self, apply_plasticity=True):
+        """gridToParticles(dt): G2P, evolveStrain and (by default) applyPlasticity; ends the substep."""
+        st = abi.Stats()
+        rc = self._call("grid_to_particles", 1 if apply_plasticity else 0, abi.C.byref(st))
+        self.last_status = rc
+        return rc
+
+    def applyPlasticity(self):
+        return self._call("apply_plasticity")
+
     def calculateDt(self, max_dt):
         """MpmSimulationBase::calculateDt: cfl dx / max(particle, collider speed)."""
         dt = abi.C.c_double()

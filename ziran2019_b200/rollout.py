@@ -30,6 +30,8 @@ class Rollout:
         self.nseg = (self.steps + self.every - 1) // self.every
         sim.checkpointSave(self._base_slot())
         self.stats = []
+        # forward calls so far: the checkpoints belong to the last one only
+        self.generation = 0
 
     # slots: 0 .. nseg-1 segment checkpoints, nseg .. nseg+every-1 segment
     # states, the last one the untouched initial state
@@ -38,6 +40,7 @@ class Rollout:
 
     def run(self, E, v0):
         sim = self.sim
+        self.generation += 1
         sim.checkpointLoad(self._base_slot())
         sim.setYoungsModulus(np.asarray(E, dtype=np.float64), self.nu)
         sim.setParticles(V=np.asarray(v0, dtype=np.float64).reshape(-1, 3))
@@ -78,16 +81,26 @@ class Rollout:
 
 
 class DifferentiableRollout(torch.autograd.Function):
-    """X_final = rollout(E, v0) with the reverse sweep of `Rollout` as backward."""
+    """X_final = rollout(E, v0) with the reverse sweep of `Rollout` as backward.
+
+    The rollout's checkpoints hold the state of its latest forward call only, so
+    the backward of an earlier forward call (a second forward ran in between)
+    raises instead of returning the later call's gradients."""
 
     @staticmethod
     def forward(ctx, E, v0, rollout):
         X = rollout.run(E.detach().cpu().double().numpy(), v0.detach().cpu().double().numpy())
         ctx.rollout = rollout
+        ctx.generation = rollout.generation
         ctx.dev = E.device
+        ctx.shapes = (E.shape, v0.shape)
         return torch.from_numpy(np.ascontiguousarray(X)).to(device=E.device, dtype=torch.float64)
 
     @staticmethod
     def backward(ctx, gX):
+        if ctx.rollout.generation != ctx.generation:
+            raise RuntimeError("DifferentiableRollout: the rollout ran forward again after this call; "
+                               "its checkpoints no longer hold this call's states")
         gE, gv0 = ctx.rollout.backward(gX.detach().cpu().double().numpy())
-        return torch.from_numpy(gE).to(ctx.dev), torch.from_numpy(gv0).to(ctx.dev), None
+        sE, sv = ctx.shapes
+        return (torch.from_numpy(gE).reshape(sE).to(ctx.dev), torch.from_numpy(gv0).reshape(sv).to(ctx.dev), None)
