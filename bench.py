@@ -28,235 +28,12 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-DX = 1.0 / 256
-DT = 5e-4
-CELLS = (25, 25, 50)
-PPC = 8
-RHO = 1000.0
-E, NU, YIELD = 5e4, 0.35, 150.0
+from ziran2019_b200.workloads import CELLS, DT, DX, PPC, RHO, WORKLOADS, make_sim, scene  # noqa: E402,F401
+from ziran2019_b200 import workloads  # noqa: E402
+
 METRIC = "implicit MPM substeps/sec at 1M particles, mixed vs FP64 GPU, at <=1e-6 rel err"
 HVP_WORDS = 22  # compulsory words per particle of one Hessian-vector product: X(3), Fn(9), F(9), V0(1)
-# DRAM bytes of one product (k_hvp_stress + k_hvp_scatter) per particle, from an
-# ncu capture of this workload at 1M particles (228.7 MB;
-# profiles/k_hvp_stress_k_hvp_scatter_1M_mixed.md).
-HVP_DRAM_BYTES_PER_PARTICLE = 228.7e6 / 1_000_000
-
-
-def scene(n_boxes=4, seed_pos=1, seed_vel=2, seed_jit=0, velocity="particle"):
-    """Seeded synthetic scene (the benchmark has no dataset; shapes follow the workload).
-
-    velocity="particle": every particle draws its velocity uniformly from [-1,1]^3,
-    so the Newton solve works from the first substep.  velocity="box": one rigid
-    velocity per box; the boxes then fly undeformed (Newton converges at its first
-    residual check, no Hessian products) until they reach a wall."""
-    size = np.array(CELLS) * DX
-    rng = np.random.default_rng(seed_pos)
-    corners = []
-    while len(corners) < 4:
-        c = rng.uniform(4 * DX, 1 - size - 4 * DX)
-        if all(np.any((c + size + 2 * DX <= o) | (o + size + 2 * DX <= c)) for o in corners):
-            corners.append(c)
-    vel = np.random.default_rng(seed_vel).uniform(-1, 1, size=(4, 3))
-    jr = np.random.default_rng(seed_jit)
-    grid = np.stack(np.meshgrid(*[np.arange(c) for c in CELLS], indexing="ij"), -1).reshape(-1, 3)
-    xs, vs = [], []
-    for b in range(n_boxes):
-        x = (np.repeat(grid, PPC, 0) + jr.random((grid.shape[0] * PPC, 3))) * DX + corners[b]
-        xs.append(x)
-        vs.append(np.tile(vel[b], (x.shape[0], 1)))
-    x, v = np.concatenate(xs), np.concatenate(vs)
-    if velocity == "particle":
-        v = np.random.default_rng(seed_vel).uniform(-1, 1, size=x.shape)
-    return x, v
-
-
-def make_sim(x, v, precision, lib=None, model="hencky", layout="auto", plastic="von_mises"):
-    from ziran2019_b200 import abi, mpm
-
-    sim = mpm.MpmSimulation(DX, gravity=(0, -9.8, 0), precision=precision, grid_log2=9, layout=layout,
-                            device=int(os.environ.get("LOCAL_RANK", "0")) if lib is None else 0, lib=lib)
-    V0 = DX ** 3 / PPC
-    h = sim.addParticles(x, v, RHO * V0, V0)
-    m = mpm.StvkWithHenckyIsotropic(E, NU) if model == "hencky" else mpm.NeoHookeanBorden(E, NU)
-    h.addFBasedMpmForce(m)
-    if plastic == "von_mises":
-        h.addPlasticity(m, mpm.VonMisesStvkHencky(YIELD, 1e30, 0.0))
-    elif plastic == "drucker_prager":
-        h.addPlasticity(m, mpm.DruckerPragerStvkHencky(30.0, 1.0, 0.0, True))
-    mpm.add_all_walls_in_domain(sim, 1.0, 3 * DX, abi.STICKY)
-    return sim
-
-
-# ----------------------------------------------------------------------------
-# Secondary workloads (the other benchmark configurations; `--workload`).  Each
-# prints its own JSON line; the default workload is the headline above.
-def _jitter_box(cells, dx, lo, ppc, seed):
-    rng = np.random.default_rng(seed)
-    grid = np.stack(np.meshgrid(*[np.arange(c) for c in cells], indexing="ij"), -1).reshape(-1, 3)
-    return (np.repeat(grid, ppc, 0) + rng.random((grid.shape[0] * ppc, 3))) * dx + np.asarray(lo, dtype=np.float64)
-
-
-def wl_cube32k(precision, lib=None, layout="auto", scale=1):
-    """Elastic cube: 16^3 cells x 8 ppc = 32,768 particles (seed 0), dx = 1/64,
-    min corner (0.375, 0.125, 0.375), fixed corotated E = 1e4, nu = 0.3,
-    rho = 1000, gravity, sticky ground y = 0.1, Newton-CG rel. tol 1e-7, dt = 1e-3."""
-    from ziran2019_b200 import abi, mpm
-    dx = 1.0 / 64
-    x = _jitter_box((16, 16, 16), dx, (0.375, 0.125, 0.375), 8, 0)
-    sim = mpm.MpmSimulation(dx, gravity=(0, -9.8, 0), precision=precision, grid_log2=7, layout=layout, lib=lib)
-    V0 = dx ** 3 / 8
-    h = sim.addParticles(x, np.zeros_like(x), 1000.0 * V0, V0)
-    h.addFBasedMpmForce(mpm.FixedCorotated(1e4, 0.3))
-    sim.addCollisionObject(mpm.AnalyticCollisionObject(mpm.HalfSpace((0, 0.1, 0), (0, 1, 0)), abi.STICKY))
-    sim.switchLinearSolver(abi.CG)
-    sim.newton_tolerance = 1e-7
-    sim.newton_max_iterations = 10
-    sim.krylov_max_iterations = 100
-    return sim, 1e-3, x.shape[0], {"workload": "config0-elastic-cube-32k", "model": "fixed corotated", "solver": "Newton-CG tol 1e-7"}
-
-
-def wl_admm500k(precision, lib=None, layout="auto", scale=1):
-    """Viscoelastic ADMM slab: 0.6 x 0.1 x 0.6 at dx = 1/120, 72 x 12 x 72 cells x 8
-    ppc = 497,664 particles (seed 3) over a static sticky sphere of radius 0.2;
-    StvkWithHenckyIsotropic E = 2e4, nu = 0.4 plus the non-equilibrated
-    StvkWithHencky with nu_d = nu_v = 2 mu tau, tau = 0.05 s; 20 ADMM
-    iterations, rho_scale 0.8, dt = 2e-3.  The slab starts touching the sphere
-    with the speed of a 0.3 m drop (sqrt(2 g 0.3) = 2.42 m/s) so every timed
-    substep deforms it.  scale > 1 takes every scale-th cell column in x and z
-    (CPU samples)."""
-    from ziran2019_b200 import abi, mpm
-    dx = 1.0 / 120
-    nx = 72 // scale
-    x = _jitter_box((nx, 12, nx), dx, (0.5 - nx * dx / 2, 0.5 + 2 * dx, 0.5 - nx * dx / 2), 8, 3)
-    sim = mpm.MpmSimulation(dx, gravity=(0, -9.8, 0), precision=precision, grid_log2=8, layout=layout, lib=lib)
-    V0 = dx ** 3 / 8
-    v = np.tile([0.0, -np.sqrt(2 * 9.8 * 0.3), 0.0], (x.shape[0], 1))
-    h = sim.addParticles(x, v, 1000.0 * V0, V0)
-    E, nu, tau = 2e4, 0.4, 0.05
-    h.addFBasedMpmForce(mpm.StvkWithHenckyIsotropic(E, nu))
-    nvis = 2 * E / (2 * (1 + nu)) * tau
-    h.addFElasticNonequilibratedBasedMpmForce(mpm.StvkWithHencky(E, nu), nvis, nvis)
-    sim.addCollisionObject(mpm.AnalyticCollisionObject(mpm.Sphere((0.5, 0.3, 0.5), 0.2), abi.STICKY))
-    sim.addCollisionObject(mpm.AnalyticCollisionObject(mpm.HalfSpace((0, 3 * dx, 0), (0, 1, 0)), abi.STICKY))
-    sim.useAdmm(admm_max_iterations=20, rho_scale=0.8, global_tolerance=1e-8, local_tolerance=1e-8)
-    return sim, 2e-3, x.shape[0], {"workload": "config2-viscoelastic-admm-500k", "model": "hencky + viscoelastic Fe",
-                                   "solver": "ADMM 20 iterations, MINRES abs tol 1e-8"}
-
-
-def wl_damage2m(precision, lib=None, layout="auto", scale=1):
-    """Notched slab 1.0 x 0.25 x 0.1 with a 0.1-long, one-cell-wide edge notch at
-    mid-length, 8 ppc at dx = 1/216 (216 x 54 x 22 cells, about 2.05M
-    particles, seed 4); the end faces are held by sticky boxes moving apart at
-    +-0.5 m/s; NeoHookeanBorden E = 1e5, nu = 0.3 with Rankine damage sigma_F =
-    1e3 Pa, k = 1e-3; dt = 2e-4, no gravity.  scale > 1 keeps every scale-th
-    cell layer in z (CPU samples)."""
-    from ziran2019_b200 import abi, mpm
-    dx = 1.0 / 216
-    nx, ny, nz = 216, 54, max(1, 22 // scale)
-    lo = np.array([0.25, 0.5, 0.5])
-    x = _jitter_box((nx, ny, nz), dx, lo, 8, 4)
-    rel = (x - lo) / dx
-    notch = (np.abs(rel[:, 0] - nx / 2) < 0.5) & (rel[:, 1] < 0.1 / dx)
-    x = x[~notch]
-    sim = mpm.MpmSimulation(dx, gravity=(0, 0, 0), precision=precision, grid_log2=9, layout=layout, lib=lib)
-    V0 = dx ** 3 / 8
-    h = sim.addParticles(x, np.zeros_like(x), 1000.0 * V0, V0)
-    h.addFBasedMpmForce(mpm.NeoHookeanBorden(1e5, 0.3))
-    h.addRankineDamage(1e3, residual_phase=1e-3)
-    hi = lo + np.array([nx, ny, nz]) * dx
-    grip = 3 * dx
-    for side, vel in ((0, -0.5), (1, 0.5)):
-        a = [lo[0] - 4 * dx if side == 0 else hi[0] - grip, lo[1] - 4 * dx, lo[2] - 4 * dx]
-        b = [lo[0] + grip if side == 0 else hi[0] + 4 * dx, hi[1] + 4 * dx, hi[2] + 4 * dx]
-        box = mpm.AnalyticCollisionObject(mpm.AxisAlignedAnalyticBox(a, b), abi.STICKY)
-        box.setTranslation((0.0, 0.0, 0.0), (vel, 0.0, 0.0))
-        sim.addCollisionObject(box)
-    return sim, 2e-4, x.shape[0], {"workload": "config3-rankine-notched-slab-2m", "model": "neo-Hookean + Rankine damage",
-                                   "solver": "MINRES, Newton 3 x Krylov 20 (reference defaults)"}
-
-
-def wl_explicit1m(precision, lib=None, layout="auto", scale=1):
-    """The headline scene (four boxes of 250,000 particles, StvkWithHencky +
-    von Mises, sticky walls) advanced by the explicit symplectic substep
-    (symplectic = true, trial collision on) at dt = 1e-4 (the p-wave speed is
-    about 9.6 m/s at dx = 1/256).  scale > 1 keeps 4 // scale boxes (CPU samples)."""
-    x, v = scene(n_boxes=max(1, 4 // scale))
-    sim = make_sim(x, v, precision, lib=lib, layout=layout)
-    sim.useExplicit()
-    return sim, 1e-4, x.shape[0], {"workload": "explicit-elastoplastic-4boxes-1m", "model": "hencky+von Mises",
-                                   "solver": "explicit symplectic substep, trial collision"}
-
-
-def wl_sand1m(precision, lib=None, layout="auto", scale=1):
-    """The headline scene with Drucker-Prager sand plasticity (friction angle 30
-    degrees, beta 1, no cohesion, volume correction) instead of von Mises;
-    implicit substep with the reference solver defaults.  scale > 1 keeps
-    4 // scale boxes (CPU samples)."""
-    x, v = scene(n_boxes=max(1, 4 // scale))
-    sim = make_sim(x, v, precision, lib=lib, layout=layout, plastic="drucker_prager")
-    return sim, DT, x.shape[0], {"workload": "sand-drucker-prager-4boxes-1m", "model": "hencky+Drucker-Prager",
-                                 "solver": "MINRES, Newton 3 x Krylov 20 (reference defaults)"}
-
-
-def wl_phasefield2m(precision, lib=None, layout="auto", scale=1):
-    """The notched slab of damage2m (about 2.05M particles, ends pulled apart at
-    +-0.5 m/s, NeoHookeanBorden E = 1e5, nu = 0.3) with the CD-MPM phase field
-    instead of Rankine damage: l0 = dx / 2, sigma_c from 1% volumetric stretch,
-    parabolic_M = 1, lumped mass, CG tolerance 1e-6 and cap 100 (the fracture
-    project's settings).  scale > 1 keeps every scale-th cell layer in z."""
-    from ziran2019_b200 import abi, mpm
-    dx = 1.0 / 216
-    nx, ny, nz = 216, 54, max(1, 22 // scale)
-    lo = np.array([0.25, 0.5, 0.5])
-    x = _jitter_box((nx, ny, nz), dx, lo, 8, 4)
-    rel = (x - lo) / dx
-    notch = (np.abs(rel[:, 0] - nx / 2) < 0.5) & (rel[:, 1] < 0.1 / dx)
-    x = x[~notch]
-    sim = mpm.MpmSimulation(dx, gravity=(0, 0, 0), precision=precision, grid_log2=9, layout=layout, lib=lib)
-    V0 = dx ** 3 / 8
-    h = sim.addParticles(x, np.zeros_like(x), 1000.0 * V0, V0)
-    h.addFBasedMpmForceWithPhaseField(0.01, 0.5 * dx, mpm.NeoHookeanBorden(1e5, 0.3))
-    sim.setPhaseFieldSolver(parabolic_M=1.0, lumping=True)
-    hi = lo + np.array([nx, ny, nz]) * dx
-    grip = 3 * dx
-    for side, vel in ((0, -0.5), (1, 0.5)):
-        a = [lo[0] - 4 * dx if side == 0 else hi[0] - grip, lo[1] - 4 * dx, lo[2] - 4 * dx]
-        b = [lo[0] + grip if side == 0 else hi[0] + 4 * dx, hi[1] + 4 * dx, hi[2] + 4 * dx]
-        box = mpm.AnalyticCollisionObject(mpm.AxisAlignedAnalyticBox(a, b), abi.STICKY)
-        box.setTranslation((0.0, 0.0, 0.0), (vel, 0.0, 0.0))
-        sim.addCollisionObject(box)
-    return sim, 2e-4, x.shape[0], {"workload": "cdmpm-phase-field-notched-slab-2m", "model": "neo-Hookean + CD-MPM phase field",
-                                   "solver": "MINRES, Newton 3 x Krylov 20; phase-field CG 1e-6 x 100"}
-
-
-MIXED_ROLLOUT_TOL = 1e-12
-
-
-def wl_rollout256k(precision, lib=None, layout="auto", scale=1):
-    """Differentiable rollout: elastic cube of 32^3 cells x 8 ppc = 262,144
-    particles (seed 0) at dx = 1/64 (side 0.5, min corner (0.25, 0.125, 0.25)),
-    fixed corotated with per-particle E ~ LogNormal(ln 1e4 - 0.3^2/2, 0.3)
-    (seed 5), nu = 0.3, initial velocities uniform in [-0.5, 0.5]^3 (seed 6),
-    sticky ground y = 0.1, gravity, Newton-CG, dt = 1e-3; loss = |com(x_100) -
-    target|^2 with the target drawn from seed 7.  scale > 1 shrinks the cube's
-    edge by that factor (CPU samples)."""
-    from ziran2019_b200 import abi, mpm
-    dx = 1.0 / 64
-    n = 32 // scale
-    x = _jitter_box((n, n, n), dx, (0.25, 0.125, 0.25), 8, 0)
-    sim = mpm.MpmSimulation(dx, gravity=(0, -9.8, 0), precision=precision, grid_log2=7, layout=layout, lib=lib)
-    V0 = dx ** 3 / 8
-    h = sim.addParticles(x, np.zeros_like(x), 1000.0 * V0, V0)
-    h.addFBasedMpmForce(mpm.FixedCorotated(1e4, 0.3))
-    sim.addCollisionObject(mpm.AnalyticCollisionObject(mpm.HalfSpace((0, 0.1, 0), (0, 1, 0)), abi.STICKY))
-    sim.switchLinearSolver(abi.CG)
-    sim.newton_tolerance = 1e-12 if precision == "fp64" else MIXED_ROLLOUT_TOL
-    sim.newton_max_iterations = 30
-    sim.krylov_max_iterations = 500
-    sim.krylov_tolerance = 1e-30
-    return sim, 1e-3, x.shape[0], {"workload": "config4-differentiable-rollout-256k", "model": "fixed corotated, per-particle E",
-                                   "solver": "Newton-CG tol 1e-12, adjoint CG rel tol 1e-10",
-                                   "steps": 100, "checkpoint_every": 10}
+HVP_KERNELS = ("k_hvp_stress", "k_hvp_scatter")  # the kernels of one Hessian-vector product
 
 
 def run_rollout(args, world, rank):
@@ -271,7 +48,7 @@ def run_rollout(args, world, rank):
     steps, every, NUR = 100, 10, 0.3
     res = {}
     for p in ("fp64", "mixed"):
-        sim, dt, P, meta = wl_rollout256k(p, layout="444")
+        sim, dt, P, meta = workloads.wl_rollout256k(p, layout="444", mixed_tol=args.rollout_mixed_tol)
         rng = np.random.default_rng(5)
         E = np.exp(np.log(1e4) - 0.3 ** 2 / 2 + 0.3 * rng.standard_normal(P))
         v0 = np.random.default_rng(6).uniform(-0.5, 0.5, (P, 3))
@@ -328,10 +105,6 @@ def run_rollout(args, world, rank):
                                   "max_rel_err": max(r64["fd_rel_err"]) if r64.get("fd_rel_err") else None,
                                   "rel_err": r64.get("fd_rel_err")}}
         print(json.dumps(line), flush=True)
-
-
-WORKLOADS = {"cube32k": wl_cube32k, "admm500k": wl_admm500k, "damage2m": wl_damage2m, "rollout256k": wl_rollout256k,
-             "explicit1m": wl_explicit1m, "sand1m": wl_sand1m, "phasefield2m": wl_phasefield2m}
 
 
 def run_workload(args, world, rank):
@@ -516,31 +289,108 @@ def timed_cpu_window(make, dt, warmup, steps, min_seconds, max_repeats=50):
     return n, secs, reps
 
 
-def cpu_oracle_rate(steps, warmup, velocity="particle", min_seconds=0.0):
-    """The oracle (CPU restatement of the reference substep) on one 250k-particle
-    box of the same scene, all host threads, over the GPU's timed window;
-    returns 1M-equivalent substeps/s, the sample's particles, seconds, timed
-    substeps and repeats of the window."""
+def oracle_lib_native(wait_for=None):
+    """The oracle built for this host (-march=native), waiting for its build."""
     from oracle import zoracle
-    x, v = scene(n_boxes=1, velocity=velocity)
-    n, dt, reps = timed_cpu_window(lambda: make_sim(x, v, "fp64", lib=zoracle.lib()), DT, warmup, steps, min_seconds)
-    P = x.shape[0]
-    return n / dt * P / 1_000_000, P, dt, n, reps
+    if wait_for is not None:
+        wait_for.wait()
+    return zoracle.lib(native=True)
+
+
+def oracle_run(x, v, steps, warmup, model, lib):
+    """The full workload on the oracle (FP64, all host threads): `steps`
+    substeps from the initial state (x, v), the ones after the first `warmup`
+    timed.  Returns (final state, timed substeps, seconds)."""
+    sim = make_sim(x, v, "fp64", lib=lib, model=model)
+    for _ in range(warmup):
+        sim.advanceOneTimeStep(DT)
+    t0 = time.perf_counter()
+    for _ in range(steps - warmup):
+        sim.advanceOneTimeStep(DT)
+    secs = time.perf_counter() - t0
+    st = sim.getParticles()
+    st["yield_active"] = yield_active(st["F"], model)
+    sim.close()
+    return st, steps - warmup, secs
+
+
+def yield_active(F, model):
+    """Particles on the von Mises yield surface: |dev Hencky strain| >= tau_Y / (2 mu)
+    up to 1e-9 relative (VonMisesStvkHencky::projectStrain, PlasticityApplier.cpp:
+    462-502, projected them in their last substep)."""
+    if model != "hencky":
+        return None
+    s = np.linalg.svd(F, compute_uv=False)
+    eps = np.log(np.maximum(np.abs(s), 1e-4))
+    dev = eps - eps.mean(1, keepdims=True)
+    mu = workloads.E / (2 * (1 + workloads.NU))
+    return np.linalg.norm(dev, axis=1) >= (workloads.YIELD / (2 * mu)) * (1 - 1e-9)
+
+
+def accuracy_vs_oracle(states, ref):
+    """Relative L2 errors of positions and velocities against the FP64 oracle,
+    the largest position error in cells, and the particles whose von Mises
+    branch (projected or not in the last substep) differs from the oracle's."""
+    out = {}
+    for p, st in states.items():
+        row = {"rel_pos_err": float(np.linalg.norm(st["X"] - ref["X"]) / np.linalg.norm(ref["X"])),
+               "rel_vel_err": float(np.linalg.norm(st["V"] - ref["V"]) / np.linalg.norm(ref["V"])),
+               "max_abs_pos_err_over_dx": float(np.abs(st["X"] - ref["X"]).max() / DX)}
+        if ref.get("yield_active") is not None and st.get("yield_active") is not None:
+            row["yield_branch_disagreements"] = int(np.count_nonzero(st["yield_active"] != ref["yield_active"]))
+            row["yield_active_particles_oracle"] = int(np.count_nonzero(ref["yield_active"]))
+        out[p] = row
+    return out
+
+
+def ncu_traffic(path, kernels):
+    """DRAM bytes (read + write) per launch of `kernels`, summed, from an ncu CSV
+    (--metrics dram__bytes_read.sum,dram__bytes_write.sum --csv) of the same
+    workload: the mean over the captured launches of each kernel."""
+    import csv
+    per = {}
+    with open(path) as f:
+        rows = [r for r in csv.reader(f) if len(r) > 5]
+    head = rows[0]
+    ik, im, iv, iu = head.index("Kernel Name"), head.index("Metric Name"), head.index("Metric Value"), head.index("Metric Unit")
+    scale = {"byte": 1, "Kbyte": 1e3, "Mbyte": 1e6, "Gbyte": 1e9, "KB": 1e3, "MB": 1e6, "GB": 1e9, "B": 1}
+    for r in rows[1:]:
+        name = r[ik].split("<")[0].split("(")[0].strip()
+        if name in kernels and r[im] in ("dram__bytes_read.sum", "dram__bytes_write.sum"):
+            per.setdefault(name, []).append(float(r[iv].replace(",", "")) * scale.get(r[iu], 1))
+    if not per:
+        return None
+    # read and write rows alternate per launch: sum per kernel, divide by launches
+    return sum(sum(v) / (len(v) / 2) for v in per.values())
 
 
 def run_reference(args, world, rank):
+    """The reference's CPU path on the host cores: the oracle (the CPU
+    restatement of the reference substep, built for this host) on the full
+    1M-particle workload, all threads; `warmup` untimed then `steps` timed
+    substeps.  Rank 0 only."""
     if rank != 0:
         return
     cores = os.cpu_count()
-    rate, P, secs, _, _ = cpu_oracle_rate(args.steps, args.warmup, args.velocity)
-    sample = f"{args.steps} substeps of one {P}-particle box of the workload (oracle port, {cores} threads), scaled by {P}/1e6"
+    lib = oracle_lib_native(oracle_build_process())
+    x, v = scene(n_boxes=args.boxes, velocity=args.velocity)
+    P = x.shape[0]
+    _, n, secs = oracle_run(x, v, args.warmup + args.steps, args.warmup, args.model, lib)
+    rate = n / secs
+    sample = (f"{args.steps} timed substeps (after {args.warmup} warm-up) of the full {P}-particle workload, oracle port "
+              f"({'-march=native' if lib.native else 'portable build'}), {cores} threads")
     line = {"metric": METRIC, "value": rate, "unit": "substeps/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": 1e3 * secs / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "ms_per_step": 1e3 * secs / n, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic", "impl": "reference",
-            "config": {"workload": "config1-elastoplastic-4boxes", "particles": 1_000_000, "sample_particles": P},
+            "config": {"workload": "config1-elastoplastic-4boxes", "particles": P, "model": f"{args.model}+von Mises"},
             "cpu_baseline": {"value": rate, "unit": "substeps/s", "cores": cores, "kind": "port", "sample": sample},
             "e2e": {"value": rate, "unit": "substeps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+def oracle_build_process():
+    from oracle import zoracle
+    return zoracle.build_native_async()
 
 
 def main():
@@ -551,12 +401,15 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--accuracy-steps", type=int, default=100)
     ap.add_argument("--cpu-seconds", type=float, default=10.0,
-                    help="the CPU baseline repeats the timed window on the oracle until this much timed CPU work")
-    ap.add_argument("--no-cpu-baseline", action="store_true")
+                    help="secondary workloads: the CPU baseline repeats the timed window on the oracle until this much timed CPU work")
+    ap.add_argument("--no-cpu-baseline", action="store_true",
+                    help="skip the FP64 oracle run (accuracy against the oracle and the CPU baseline)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--model", default="hencky", choices=["hencky", "nh"])
     ap.add_argument("--velocity", default="particle", choices=["particle", "box"])
     ap.add_argument("--only", default=None, choices=["fp64", "mixed"], help="time one precision (profiling runs)")
+    ap.add_argument("--host-loop", action="store_true",
+                    help="with --only: host-driven solver loops (every kernel a plain launch, for ncu launch lists)")
     ap.add_argument("--boxes", type=int, default=4, help="boxes of 250k particles (profiling runs use fewer)")
     ap.add_argument("--fp64-layout", default="444", choices=["444", "auto"],
                     help="page layout of the FP64 substep: 444 = same as the mixed run (only precision differs)")
@@ -565,11 +418,13 @@ def main():
     ap.add_argument("--workload", default="config1", choices=["config1"] + sorted(WORKLOADS),
                     help="config1: the headline 1M-particle workload; others print their own line")
     ap.add_argument("--fd-directions", type=int, default=4, help="finite-difference directions of the rollout gradient check")
-    ap.add_argument("--rollout-mixed-tol", type=float, default=None, help="Newton tolerance of the mixed rollout forward")
+    ap.add_argument("--rollout-mixed-tol", type=float, default=1e-12, help="Newton tolerance of the mixed rollout forward")
+    ap.add_argument("--ncu-csv", default=None,
+                    help="ncu CSV (dram__bytes_read.sum, dram__bytes_write.sum) of the product kernels of this workload: "
+                         "fills roofline.traffic")
+    ap.add_argument("--ncu-particles", type=int, default=None,
+                    help="particles of the workload that --ncu-csv captured (its traffic is scaled to this run by particle count)")
     args = ap.parse_args()
-    if args.rollout_mixed_tol is not None:
-        global MIXED_ROLLOUT_TOL
-        MIXED_ROLLOUT_TOL = args.rollout_mixed_tol
     if args.warmup < 3:
         args.warmup = 3
     world, rank = dist_setup()
@@ -587,6 +442,8 @@ def main():
 
     from ziran2019_b200 import build
     build.build()
+    want_oracle = rank == 0 and world == 1 and not args.no_cpu_baseline and not args.only
+    oracle_build = oracle_build_process() if want_oracle else None
     dev = int(os.environ.get("LOCAL_RANK", "0"))
     x, v = scene(n_boxes=args.boxes, velocity=args.velocity)
     P = x.shape[0]
@@ -596,10 +453,10 @@ def main():
         for _ in range(args.warmup):
             sims[p].advanceOneTimeStep(DT)
     if args.only:
-        ms, st = timed_steps(sims[args.only], args.steps, world)
+        ms, st = timed_steps(sims[args.only], args.steps, world, profile=args.host_loop)
         _, stp = timed_steps(sims[args.only], 2, world, profile=True)
         if rank == 0:
-            print(json.dumps({"only": args.only, "particles": P, "ms_per_step": ms / args.steps,
+            print(json.dumps({"only": args.only, "particles": P, "ms_per_step": ms / args.steps, "host_loop": args.host_loop,
                               "hvp_ms": sum(s["ms_hvp"] for s in stp) / max(1, sum(s["hvp_timed"] for s in stp)),
                               "launches_per_step": st[-1]["kernel_launches"], "newton_krylov": [st[-1]["newton_iterations"], st[-1]["krylov_iterations"]]}),
                   flush=True)
@@ -616,23 +473,11 @@ def main():
     value = world * args.steps / (ms_mx / 1e3)
     fp64_value = world * args.steps / (ms64 / 1e3)
 
-    # position error of the mixed substep against the FP64 substep after
-    # `accuracy-steps` substeps from the same initial state
-    done = {"fp64": args.warmup + args.steps, "mixed": args.warmup + args.steps + nprof}
-    total = max(args.accuracy_steps, max(done.values()))
-    for p in ("fp64", "mixed"):
-        for _ in range(total - done[p]):
-            sims[p].advanceOneTimeStep(DT)
-    x64 = sims["fp64"].getParticles()["X"]
-    xmx = sims["mixed"].getParticles()["X"]
-    rel_err = float(np.linalg.norm(xmx - x64) / np.linalg.norm(x64))
-    max_abs_dx = float(np.abs(xmx - x64).max() / DX)
-
     # dominant kernel: the Hessian-vector product
     hvp_ms = sum(s["ms_hvp"] for s in st_prof)
     hvp_n = sum(s["hvp_timed"] for s in st_prof)
     nodes = st_prof[-1]["num_blocks"] * 64
-    hvp_bytes = P * HVP_WORDS * 4 + nodes * 3 * 8 * 2
+    hvp_bytes = P * HVP_WORDS * 4 + nodes * 3 * 4 * 2
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
@@ -640,10 +485,13 @@ def main():
         pass
     peak = float(peaks.get("hbm_gbs", 6650.0))
     achieved = hvp_bytes / (hvp_ms / hvp_n / 1e3) / 1e9 if hvp_n else None
+    traffic = ncu_traffic(args.ncu_csv, HVP_KERNELS) if args.ncu_csv else None
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": achieved / peak if achieved else None, "traffic": HVP_DRAM_BYTES_PER_PARTICLE * P,
-                "traffic_source": "ncu dram__bytes_read+write of both kernels at 1M particles",
-                "kernel": "k_hvp (FP32 Hessian-vector product)", "bytes_per_launch": hvp_bytes,
+                "frac": achieved / peak if achieved else None,
+                "traffic": traffic * P / args.ncu_particles if traffic is not None and args.ncu_particles else traffic,
+                "traffic_source": (f"ncu dram__bytes_read+write per product, {args.ncu_csv}" if traffic is not None
+                                   else "no ncu capture in this run"),
+                "kernel": "Hessian-vector product (" + " + ".join(HVP_KERNELS) + ")", "bytes_per_launch": hvp_bytes,
                 "avg_launch_ms": hvp_ms / hvp_n if hvp_n else None, "peak_source": "measured" if peaks else "fallback"}
 
     e2e = None
@@ -679,12 +527,29 @@ def main():
         e2e = {"value": world * args.steps / (ms_e2e / 1e3), "unit": "substeps/s", "h2d_bytes_per_step": P * 24 * 8,
                "d2h_bytes_per_step": P * 24 * 8}
 
-    cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        rate, Pc, secs, n, reps = cpu_oracle_rate(args.steps, args.warmup, args.velocity, args.cpu_seconds)
-        cpu = {"value": rate, "unit": "substeps/s", "cores": os.cpu_count(), "kind": "port",
-               "sample": f"the timed window ({args.warmup} warm-up + {args.steps} timed substeps) on one {Pc}-particle box of the workload, "
-                         f"{reps}x, oracle port, {secs:.1f} s timed, scaled by {Pc}/1e6"}
+    # accuracy after `accuracy-steps` substeps from the initial state: both GPU
+    # runs against each other and (rank 0, one GPU) against the FP64 oracle
+    sims_acc = {p: make_sim(x, v, p, model=args.model, layout=args.fp64_layout if p == "fp64" else "auto") for p in ("fp64", "mixed")}
+    states = {}
+    for p, s_ in sims_acc.items():
+        for _ in range(args.accuracy_steps):
+            rc = s_.advanceOneTimeStep(DT)
+            if rc not in (0, 1):
+                raise RuntimeError(f"accuracy run ({p}): substep status {rc}")
+        states[p] = s_.getParticles()
+        states[p]["yield_active"] = yield_active(states[p]["F"], args.model)
+        s_.close()
+    rel_err = float(np.linalg.norm(states["mixed"]["X"] - states["fp64"]["X"]) / np.linalg.norm(states["fp64"]["X"]))
+    max_abs_dx = float(np.abs(states["mixed"]["X"] - states["fp64"]["X"]).max() / DX)
+    cpu, vs_oracle = None, None
+    if want_oracle:
+        lib = oracle_lib_native(oracle_build)
+        ref, n, secs = oracle_run(x, v, args.accuracy_steps, args.warmup, args.model, lib)
+        vs_oracle = accuracy_vs_oracle(states, ref)
+        cpu = {"value": n / secs, "unit": "substeps/s", "cores": os.cpu_count(), "kind": "port",
+               "sample": f"substeps {args.warmup + 1}..{args.accuracy_steps} of the {args.accuracy_steps}-substep accuracy run of the "
+                         f"full {P}-particle workload on the oracle ({'-march=native' if lib.native else 'portable build'}, "
+                         f"{os.cpu_count()} threads), {secs:.1f} s"}
 
     launches = sum(s["kernel_launches"] for s in st_mx)
     sub_bytes = sum(substep_algorithmic_bytes(s_, P, 4) for s_ in st_mx) / len(st_mx)
@@ -697,14 +562,19 @@ def main():
         line = {
             "metric": METRIC, "value": value, "unit": "substeps/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": ms_mx / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "fp32 Hessian products, fp64 state/residual/reductions", "data": "synthetic",
+            "dtype": "mixed: fp32 particle/grid/Hessian arithmetic, fp64 positions, residual and reductions", "data": "synthetic",
             "config": {"workload": "config1-elastoplastic-4boxes", "particles": P, "dx": DX, "dt": DT,
                        "model": f"{args.model}+von Mises", "velocity": args.velocity, "fp64_layout": args.fp64_layout, "solver": "MINRES, Newton 3 x Krylov 20 (reference defaults)",
                        "parallelism": f"replicas x{world}", "l2": "inputs larger than L2 (particle state ~300 MB)"},
             "particles_substeps_per_s": value * P,
             "fp64_value": fp64_value, "mixed_over_fp64": value / fp64_value,
-            "rel_pos_err_vs_fp64": rel_err, "max_abs_err_over_dx": max_abs_dx, "accuracy_steps": total,
+            "ms_per_step_fp64": ms64 / args.steps,
+            "rel_pos_err_vs_fp64": rel_err, "max_abs_err_over_dx": max_abs_dx, "accuracy_steps": args.accuracy_steps,
+            "vs_oracle": vs_oracle,
+            "rel_pos_err_vs_oracle": vs_oracle["mixed"]["rel_pos_err"] if vs_oracle else None,
+            "rel_vel_err_vs_oracle": vs_oracle["mixed"]["rel_vel_err"] if vs_oracle else None,
             "newton_krylov_per_step": [st_mx[-1]["newton_iterations"], st_mx[-1]["krylov_iterations"]],
+            "newton_krylov_per_step_fp64": [st64[-1]["newton_iterations"], st64[-1]["krylov_iterations"]],
             "roofline": roofline, "substep_roofline": substep_roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
             "clocks": clk,
         }
