@@ -8,9 +8,10 @@ relative L2 errors over all particles, for the FP64 and the mixed substep.
 
 FP64 against FP64 differs only in the order of floating-point sums (atomic
 scatters and tree reductions on the GPU, the 8-colour schedule and OpenMP
-reductions in the oracle); the Newton and Krylov stopping tests see those
-rounding differences too, so a solve may stop one iteration apart, which bounds
-the agreement by the solver tolerances rather than by round-off."""
+reductions in the oracle): measured 1e-17 to 3e-16 in positions and 1e-15 to
+4e-14 in velocities, bounded here at 1e-13 and 1e-11.  The mixed substep
+(FP32 particle, grid and Hessian arithmetic) is bounded by the benchmark's
+1e-6 relative position error and 1e-4 in velocities."""
 import numpy as np
 import pytest
 
@@ -48,7 +49,7 @@ def compare(build, dt, steps, oracle, tol):
 def test_config0_cube_32k_50_substeps(cuda_lib, oracle):
     def build(p, lib):
         return workloads.wl_cube32k(p, lib=lib, layout="444" if lib is None else "auto")[0]
-    compare(build, 1e-3, 50, oracle, {"fp64": (1e-11, 1e-8), "mixed": (1e-8, 1e-5)})
+    compare(build, 1e-3, 50, oracle, {"fp64": (1e-13, 1e-11), "mixed": (1e-6, 1e-4)})
 
 
 def test_config1_box_250k_50_substeps(cuda_lib, oracle):
@@ -56,16 +57,16 @@ def test_config1_box_250k_50_substeps(cuda_lib, oracle):
 
     def build(p, lib):
         return workloads.make_sim(x, v, p, lib=lib, layout="444" if lib is None else "auto")
-    compare(build, workloads.DT, 50, oracle, {"fp64": (1e-9, 1e-6), "mixed": (1e-6, 1e-4)})
+    compare(build, workloads.DT, 50, oracle, {"fp64": (1e-13, 1e-11), "mixed": (1e-6, 1e-4)})
 
 
 def test_config2_admm_slab_cut_10_substeps(cuda_lib, oracle):
     def build(p, lib):
         return workloads.wl_admm500k(p, lib=lib, layout="444" if lib is None else "auto", scale=4)[0]
-    compare(build, 2e-3, 10, oracle, {"fp64": (1e-9, 1e-6), "mixed": (1e-6, 1e-4)})
+    compare(build, 2e-3, 10, oracle, {"fp64": (1e-13, 1e-11), "mixed": (1e-6, 1e-4)})
 
 
 def test_config3_damage_slab_layer_20_substeps(cuda_lib, oracle):
     def build(p, lib):
         return workloads.wl_damage2m(p, lib=lib, layout="444" if lib is None else "auto", scale=22)[0]
-    compare(build, 2e-4, 20, oracle, {"fp64": (1e-9, 1e-6), "mixed": (1e-6, 1e-4)})
+    compare(build, 2e-4, 20, oracle, {"fp64": (1e-13, 1e-11), "mixed": (1e-6, 1e-4)})

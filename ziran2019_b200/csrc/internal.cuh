@@ -185,7 +185,7 @@ struct Ctx {
     DBuf gm, gmv, vn, dv, vstar, facc, res, proj, collided, node_idx;
     // Krylov vectors
     DBuf kv[10];
-    DBuf kvf;                             // FP32 copies of MINRES's two Z vectors ([2][B][3][NPB]), read by the FP32 product
+    DBuf kvf;                             // FP32 node-major copies of MINRES's two Z vectors ([2][B][NPB][4]), read by the FP32 product
     DBuf red;                             // reduction partials [4][RED_MAX_CTAS]
     DBuf scal;                            // SolverScalars
     DBuf counters;                        // DevCounters

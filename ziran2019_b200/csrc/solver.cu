@@ -368,7 +368,7 @@ __global__ void __launch_bounds__(ND_THREADS) k_residual(NodeGeom ng, const doub
 struct KrylovBufs {
     double *x, *r, *p, *q, *tmp;      // CG
     double *Q[3], *M[3], *Z[2];       // MINRES
-    float* Zf[2];                     // FP32 copies of Z for the FP32 product (MIXED MINRES), or null
+    float* Zf[2];                     // FP32 node-major copies of Z ([B][NPB][4]) for the FP32 product (MIXED MINRES), or null
     double* hacc;                     // Hessian accumulator
     const double* pre;                // diagonal preconditioner per node (the mass for Newton)
 };
@@ -428,8 +428,8 @@ __global__ void __launch_bounds__(ND_THREADS, 4) k_residual_start(NodeGeom ng, c
                 kb.Z[0][i] = z;
                 kb.Z[1][i] = 0;
                 if (kb.Zf[0]) {
-                    kb.Zf[0][i] = (float)z;
-                    kb.Zf[1][i] = 0;
+                    kb.Zf[0][4 * n + k] = (float)z;
+                    kb.Zf[1][4 * n + k] = 0;
                 }
             }
             else {
@@ -758,6 +758,7 @@ __global__ void __launch_bounds__(ND_THREADS) k_mr_b(NodeGeom ng, const double* 
         const double m = gm[n];
         if (m == 0) continue;
         const double pre = kb.pre[n];
+        float zf[3];
         for (int k = 0; k < 3; ++k) {
             int64_t i = vidx<NPB>(n, k);
             double q = qkp1[i];
@@ -766,9 +767,10 @@ __global__ void __launch_bounds__(ND_THREADS) k_mr_b(NodeGeom ng, const double* 
             qkp1[i] = q;
             double z = q / pre;
             zout[i] = z;
-            if (zfout) zfout[i] = (float)z;
+            zf[k] = (float)z;
             acc += z * q;
         }
+        if (zfout) reinterpret_cast<float4*>(zfout)[n] = make_float4(zf[0], zf[1], zf[2], 0.f);
     }
     double s = block_sum(acc);
     if (threadIdx.x == 0) part_out[blockIdx.x] = s;
@@ -1034,7 +1036,7 @@ int ensure_node_buffers(Ctx* ctx)
     ZMPM_CUDA(ctx->proj.ensure(6 * nn * sizeof(double)));
     ZMPM_CUDA(ctx->collided.ensure(nn));
     for (int i = 0; i < 10; ++i) ZMPM_CUDA(ctx->kv[i].ensure(vec));
-    ZMPM_CUDA(ctx->kvf.ensure((size_t)(6 * nn) * sizeof(float)));
+    ZMPM_CUDA(ctx->kvf.ensure((size_t)(8 * nn) * sizeof(float)));
     return ZMPM_OK;
 }
 
@@ -1353,7 +1355,7 @@ static int newton_impl(Ctx* ctx, const zmpm_solver& s)
     // MIXED MINRES runs its split FP32 product on FP32 copies of Z
     const bool zf = ctx->mixed && L.np.minres;
     L.kb.Zf[0] = zf ? ctx->kvf.as<float>() : nullptr;
-    L.kb.Zf[1] = zf ? ctx->kvf.as<float>() + 3 * L.ng.nn : nullptr;
+    L.kb.Zf[1] = zf ? ctx->kvf.as<float>() + 4 * L.ng.nn : nullptr;
     L.np.kmax = s.krylov_max_iterations;
     L.np.nmax = s.newton_max_iterations;
     L.np.tol = s.newton_tolerance;

@@ -4,13 +4,18 @@
 //  k_p2g_reg particlesToGridHelper<APIC> (MpmSimulationBase.cpp:563-608)
 //  k_stress  MpmForceBase::updatePositionBasedState (MpmForceBase.cpp:306-344):
 //            G2P of grad(vn+dv), F = (I + dt grad v) Fn, stress and Hessian scratch
-//  k_force   rasterizeForceToTVStack (MpmForceBase.cpp:102-152)
-//  k_hvp_stress + k_hvp_scatter
-//            MpmForceBase::addScaledForceDifferential (MpmForceBase.cpp:259-302):
-//            G2P of grad(dv), dS = V0 dP Fn^T, P2G of dS grad w
+//            (the FP64 evaluation of a MIXED solve whose FP32 residual stalled)
+//  k_force   rasterizeForceToTVStack (MpmForceBase.cpp:102-152); also the
+//            explicit substep's and ADMM's force scatter
+//  k_update_fused  updatePositionBasedState + rasterizeForceToTVStack in one
+//            pass (gather of grad v, F, stress and Hessian scratch, force scatter)
+//  k_hvp_fused  MpmForceBase::addScaledForceDifferential (MpmForceBase.cpp:259-302):
+//            G2P of grad(dv), dS = V0 dP Fn^T, P2G of dS grad w in one pass
+//  k_hvp_scatter  the scatter half alone (ADMM's global operator)
 //  k_g2p     gridToParticlesHelper<APIC> (MpmSimulationBase.cpp:906-1016) +
 //            evolveStrain + applyPlasticity (:1018-1030)
 #include "admm.cuh"
+#include "fused.cuh"
 #include "xfer.cuh"
 
 namespace zmpm {
@@ -397,61 +402,8 @@ __global__ void __launch_bounds__(XF_THREADS) k_force(const int32_t* __restrict_
 }
 
 // ------------------------------------------------------------------ HVP ----
-// out += sum_p dS_p grad w_ip with dS = V0 dP(grad(x) Fn) Fn^T, as two kernels
-// (dS round-trips through HBM in the HVP precision): k_hvp_stress gathers
-// grad(x) and evaluates dS in slot order; k_hvp_scatter adds dS grad w with the
-// layered scatter.
-// TX: the input vector's type (FP64, or the FP32 copy MINRES keeps for MIXED
-// products, which halves the staged window and needs no conversions).  FP32:
-// eight CTAs per SM (64 registers, a few bytes spilled; product 1.6% faster
-// than seven CTAs at 72 registers).
-template <class L, class TH, class TX = double>
-__global__ void __launch_bounds__(XF_THREADS, sizeof(TH) == 4 ? 8 : 1) k_hvp_stress(const int32_t* __restrict__ group_start, const int32_t* __restrict__ group_nbr,
-    const int32_t* __restrict__ pi, int64_t cap, const short4* __restrict__ base, double dx, const TH* __restrict__ frac,
-    const TH* __restrict__ scr, const TX* __restrict__ x0, const TX* __restrict__ x1, int alt, TH* __restrict__ dstress,
-    const SolverScalars* __restrict__ sc, int32_t* __restrict__ flags)
-{
-    if (sc && (sc->newton_done || !sc->kactive)) return;
-    constexpr int NPB = L::NPB;
-    __shared__ __align__(128) TX win[8 * 3 * NPB];
-    __shared__ int32_t nbr[8];
-    __shared__ __align__(8) uint64_t bar;
-    const int g = blockIdx.x;
-    if (threadIdx.x < 8) nbr[threadIdx.x] = group_nbr[8 * g + threadIdx.x];
-    __syncthreads();
-    // the input alternates between x0 and x1 with the Krylov iteration (MINRES)
-    const TX* x = (alt && sc && (sc->kit & 1)) ? x1 : x0;
-    stage_window<NPB>(win, x, nbr, &bar, flags);
-    const TH inv_dx = TH(1.0 / dx);
-    const int s0 = group_start[g], s1 = group_start[g + 1];
-    for (int s = s0 + threadIdx.x; s < s1; s += blockDim.x) {
-        const int kind = pi[PI_KIND * cap + s];
-        if (kind == ZMPM_MODEL_NONE) {
-#pragma unroll
-            for (int q = 0; q < 9; ++q) dstress[q * cap + s] = TH(0);
-            continue;
-        }
-        const short4 b = base[s];
-        TH w[3][3], dwr[3][3];
-#pragma unroll
-        for (int d = 0; d < 3; ++d) bspline(frac[d * cap + s], w[d], dwr[d]);
-        const int lx = b.x & (L::BX - 1), ly = b.y & (L::BY - 1), lz = b.z & (L::BZ - 1);
-        M3<TH> G = m3_zero<TH>();
-        for_stencil<L>(lx, ly, lz, w, dwr, inv_dx, [&](int t, int e, int, int, int, TH, const TH* dw) {
-            const TX* vv = win + t * 3 * NPB + e;
-#pragma unroll
-            for (int r = 0; r < 3; ++r) {
-                TH vr = (TH)vv[r * NPB];
-#pragma unroll
-                for (int c = 0; c < 3; ++c) G(r, c) += vr * dw[c];
-            }
-        });
-        M3<TH> dS = model_hvp<TH>(kind, scr, cap, s, G);
-#pragma unroll
-        for (int q = 0; q < 9; ++q) dstress[q * cap + s] = dS.a[q];
-    }
-}
-
+// out += sum_p dstress_p grad w_ip with the layered per-cell scatter (the ADMM
+// global operator, whose per-particle products k_admm_op writes to dstress).
 template <class L, class TH>
 __global__ void __launch_bounds__(XF_THREADS) k_hvp_scatter(const int32_t* __restrict__ group_start, const int32_t* __restrict__ group_nbr,
     int64_t cap, const short4* __restrict__ base, double dx, const TH* __restrict__ frac, const TH* __restrict__ dstress,
@@ -534,6 +486,166 @@ __global__ void __launch_bounds__(XF_THREADS) k_hvp_scatter(const int32_t* __res
     __syncthreads();
     flush_window<3, 3, NPB>(acc, nbr, out, nullptr);
 }
+
+// ------------------------------------------------------- fused products ----
+// MpmForceBase::addScaledForceDifferential (MpmForceBase.cpp:259-302) in one
+// kernel (fused.cuh): phase 1 gathers grad(x) at each particle from the staged
+// window of the input vector and evaluates dS = V0 dP(grad(x) Fn) Fn^T from the
+// Hessian scratch (computeStressDifferential, FBasedMpmForceHelper.cpp:132-
+// 154); phase 2 adds dS grad w_ip to the nodes (rasterizeForceToTVStack with
+// the differential, :102-152), out += sum_p dS_p grad w_ip.  T: arithmetic
+// precision; TX: the input vector (FP32 node-major copy or FP64 vector).  The
+// input alternates between x0 and x1 with the Krylov iteration when `alt`.
+template <class L, class T, class TX, int CH>
+__global__ void __launch_bounds__(FUSED_THREADS) k_hvp_fused(const int32_t* __restrict__ group_start, const int32_t* __restrict__ group_nbr,
+    const int32_t* __restrict__ pi, int64_t cap, const short4* __restrict__ base, double dx, const T* __restrict__ frac,
+    const T* __restrict__ scr, const TX* __restrict__ x0, const TX* __restrict__ x1, int alt, double* __restrict__ out,
+    const SolverScalars* __restrict__ sc, int32_t* __restrict__ flags)
+{
+    if (sc && (sc->newton_done || !sc->kactive)) return;
+    constexpr int NPB = L::NPB;
+    __shared__ __align__(128) TX win[VecWindow<NPB, TX>::ELEMS];
+    __shared__ ScatterSmem<L, T, CH> sm;
+    __shared__ __align__(8) uint64_t bar;
+    const int g = blockIdx.x;
+    if (threadIdx.x < 8) sm.nbr[threadIdx.x] = group_nbr[8 * g + threadIdx.x];
+    zero_window<3, NPB>(sm.acc);
+    __syncthreads();
+    const TX* x = (alt && sc && (sc->kit & 1)) ? x1 : x0;
+    stage_vec_window<NPB, TX>(win, x, sm.nbr, &bar, flags);
+    const int s0 = group_start[g], n = group_start[g + 1] - s0;
+    build_cell_layout<L>(sm.cl, base, s0, s0 + n);
+    list_occupied(sm);
+    const T inv_dx = T(1.0 / dx);
+    for (int c0 = 0; c0 < n; c0 += CH) {
+        const int c1 = c0 + CH < n ? c0 + CH : n;
+        __syncthreads();
+        for (int p = c0 + threadIdx.x; p < c1; p += blockDim.x) {
+            const int64_t s = s0 + p;
+            T* rc = sm.rec + (p - c0);
+            T fr[3];
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                fr[d] = frac[d * cap + s];
+                rc[d * sm.FS] = fr[d];
+            }
+            const int kind = pi[PI_KIND * cap + s];
+            M3<T> dS = m3_zero<T>();
+            if (kind != ZMPM_MODEL_NONE) {
+                const short4 b = base[s];
+                T w[3][3], dw[3][3];
+#pragma unroll
+                for (int d = 0; d < 3; ++d) bspline_all(fr[d], w[d], dw[d]);
+                const StencilOffsets<L> so(b.x & (L::BX - 1), b.y & (L::BY - 1), b.z & (L::BZ - 1));
+                M3<T> G;
+                if constexpr (sizeof(T) == 4 && sizeof(TX) == 4)
+                    gather_gradient_f32<L>(win, so, w, dw, G.a);
+                else
+                    gather_gradient<L, T, TX>(win, so, w, dw, G.a);
+#pragma unroll
+                for (int q = 0; q < 9; ++q) G.a[q] *= inv_dx;
+                dS = model_hvp<T>(kind, scr, cap, s, G);
+            }
+#pragma unroll
+            for (int r = 0; r < 3; ++r)
+#pragma unroll
+                for (int c = 0; c < 3; ++c) rc[(3 + 3 * r + c) * sm.FS] = dS(r, c) * inv_dx;
+        }
+        __syncthreads();
+        scatter_rows(sm, c0, c1);
+    }
+    __syncthreads();
+    flush_window<3, 3, NPB>(sm.acc, sm.nbr, out, nullptr);
+}
+
+// MpmForceBase::updatePositionBasedState + rasterizeForceToTVStack
+// (MpmForceBase.cpp:306-344, 102-152) in one kernel: phase 1 gathers grad(v)
+// of vstar = vn + dv at each particle, F = (I + dt grad v) Fn (evolveStrain on
+// the restored Fn, FBasedMpmForceHelper.cpp:95-109), S = V0 P(F) Fn^T and the
+// Hessian scratch (updateImplicitState, :68-92); FP32 evaluations of
+// near-degenerate SVDs are redone in FP64.  Phase 2 adds -S_p grad w_ip to
+// facc.  gate as k_stress / k_force.
+template <class L, class T, class TX, int CH>
+__global__ void __launch_bounds__(FUSED_THREADS) k_update_fused(const int32_t* __restrict__ group_start, const int32_t* __restrict__ group_nbr,
+    const double* __restrict__ pd, const int32_t* __restrict__ pi, int64_t cap, const short4* __restrict__ base, double dx, double dt,
+    const T* __restrict__ frac, const TX* __restrict__ vstar, T* __restrict__ scr, double* __restrict__ facc,
+    const SolverScalars* __restrict__ sc, int32_t* __restrict__ flags, int gate)
+{
+    if (gated_off(sc, gate)) return;
+    constexpr int NPB = L::NPB;
+    __shared__ __align__(128) TX win[VecWindow<NPB, TX>::ELEMS];
+    __shared__ ScatterSmem<L, T, CH> sm;
+    __shared__ __align__(8) uint64_t bar;
+    const int g = blockIdx.x;
+    if (threadIdx.x < 8) sm.nbr[threadIdx.x] = group_nbr[8 * g + threadIdx.x];
+    zero_window<3, NPB>(sm.acc);
+    __syncthreads();
+    stage_vec_window<NPB, TX>(win, vstar, sm.nbr, &bar, flags);
+    const int s0 = group_start[g], n = group_start[g + 1] - s0;
+    build_cell_layout<L>(sm.cl, base, s0, s0 + n);
+    list_occupied(sm);
+    const T inv_dx = T(1.0 / dx);
+    const T tdt = T(dt);
+    for (int c0 = 0; c0 < n; c0 += CH) {
+        const int c1 = c0 + CH < n ? c0 + CH : n;
+        __syncthreads();
+        for (int p = c0 + threadIdx.x; p < c1; p += blockDim.x) {
+            const int64_t s = s0 + p;
+            T* rc = sm.rec + (p - c0);
+            T fr[3];
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                fr[d] = frac[d * cap + s];
+                rc[d * sm.FS] = fr[d];
+            }
+            const int kind = pi[PI_KIND * cap + s];
+            M3<T> S = m3_zero<T>();
+            if (kind != ZMPM_MODEL_NONE) {
+                const short4 b = base[s];
+                T w[3][3], dw[3][3];
+#pragma unroll
+                for (int d = 0; d < 3; ++d) bspline_all(fr[d], w[d], dw[d]);
+                const StencilOffsets<L> so(b.x & (L::BX - 1), b.y & (L::BY - 1), b.z & (L::BZ - 1));
+                M3<T> gv;
+                gather_gradient<L, T, TX>(win, so, w, dw, gv.a);
+                M3<T> Fn, A = m3_identity<T>();
+#pragma unroll
+                for (int q = 0; q < 9; ++q) {
+                    Fn.a[q] = (T)pd[(PD_F + q) * cap + s];
+                    A.a[q] += tdt * (gv.a[q] * inv_dx);
+                }
+                const ModelParams mp{ pd[PD_MU * cap + s], pd[PD_LAM * cap + s], pd[PD_KAPPA * cap + s], pd[PD_G * cap + s] };
+                const double V0 = pd[PD_VOL * cap + s];
+                bool degenerate = false;
+                S = model_update<T, T>(kind, mp, (T)V0, m3_mul(A, Fn), Fn, scr, cap, s, sizeof(T) == 4 ? &degenerate : nullptr);
+                if constexpr (sizeof(T) == 4) {
+                    if (degenerate) { // FP64 re-evaluation of near-degenerate particles
+                        M3<double> Fnd, Ad = m3_identity<double>();
+#pragma unroll
+                        for (int q = 0; q < 9; ++q) {
+                            Fnd.a[q] = pd[(PD_F + q) * cap + s];
+                            Ad.a[q] += dt * ((double)gv.a[q] * (1.0 / dx));
+                        }
+                        S = m3_cast<T>(model_update<double, T>(kind, mp, V0, m3_mul(Ad, Fnd), Fnd, scr, cap, s, nullptr));
+                    }
+                }
+            }
+#pragma unroll
+            for (int r = 0; r < 3; ++r)
+#pragma unroll
+                for (int c = 0; c < 3; ++c) rc[(3 + 3 * r + c) * sm.FS] = -S(r, c) * inv_dx;
+        }
+        __syncthreads();
+        scatter_rows(sm, c0, c1);
+    }
+    __syncthreads();
+    flush_window<3, 3, NPB>(sm.acc, sm.nbr, facc, nullptr);
+}
+
+// chunk sizes: the particle records of a chunk fill 24 KB (FP32) / 18 KB (FP64), which keeps
+// the static shared memory of a CTA below 48 KB
+template <class T>
+constexpr int fused_chunk() { return sizeof(T) == 4 ? 512 : 192; }
 
 // ------------------------------------------------------------------ G2P ----
 // MpmSimulationBase::applyPlasticity (MpmSimulationBase.cpp:1018-1030) on one
@@ -705,12 +817,9 @@ static int update_impl(Ctx* ctx, bool gated)
         // FP32 stress and force; inside a solve also the FP64 pair, which runs
         // instead once the FP32 residual stalled (FP32 Hessian scratch either way)
         const int gate = sc ? 1 : 0;
-        k_stress<L, float, float><<<(unsigned)G, XF_THREADS, 0, ctx->stream>>>(ctx->group_start.as<int32_t>(), ctx->group_nbr.as<int32_t>(),
-            ctx->pd.as<double>(), ctx->pi.as<int32_t>(), ctx->Pcap, ctx->base.as<short4>(), ctx->cfg.dx, ctx->dt, ctx->frac.as<float>(),
-            ctx->vstar.as<double>(), ctx->stress.as<float>(), ctx->scratch.as<float>(), sc, &dc->flags, gate, 0);
-        ++g_kernel_launches;
-        k_force<L, float, float><<<(unsigned)G, XF_THREADS, 0, ctx->stream>>>(ctx->group_start.as<int32_t>(), ctx->group_nbr.as<int32_t>(),
-            ctx->Pcap, ctx->base.as<short4>(), ctx->cfg.dx, ctx->frac.as<float>(), ctx->stress.as<float>(), ctx->facc.as<double>(), sc, gate);
+        k_update_fused<L, float, double, fused_chunk<float>()><<<(unsigned)G, FUSED_THREADS, 0, ctx->stream>>>(ctx->group_start.as<int32_t>(),
+            ctx->group_nbr.as<int32_t>(), ctx->pd.as<double>(), ctx->pi.as<int32_t>(), ctx->Pcap, ctx->base.as<short4>(), ctx->cfg.dx, ctx->dt,
+            ctx->frac.as<float>(), ctx->vstar.as<double>(), ctx->scratch.as<float>(), ctx->facc.as<double>(), sc, &dc->flags, gate);
         ++g_kernel_launches;
         if (sc) {
             k_stress<L, double, float><<<(unsigned)G, XF_THREADS, 0, ctx->stream>>>(ctx->group_start.as<int32_t>(),
@@ -725,43 +834,36 @@ static int update_impl(Ctx* ctx, bool gated)
         }
     }
     else {
-        k_stress<L, double, double><<<(unsigned)G, XF_THREADS, 0, ctx->stream>>>(ctx->group_start.as<int32_t>(), ctx->group_nbr.as<int32_t>(),
-            ctx->pd.as<double>(), ctx->pi.as<int32_t>(), ctx->Pcap, ctx->base.as<short4>(), ctx->cfg.dx, ctx->dt, ctx->frac.as<double>(),
-            ctx->vstar.as<double>(), ctx->stress.as<double>(), ctx->scratch.as<double>(), sc, &dc->flags, 0, 0);
-        ++g_kernel_launches;
-        k_force<L, double, double><<<(unsigned)G, XF_THREADS, 0, ctx->stream>>>(ctx->group_start.as<int32_t>(), ctx->group_nbr.as<int32_t>(),
-            ctx->Pcap, ctx->base.as<short4>(), ctx->cfg.dx, ctx->frac.as<double>(), ctx->stress.as<double>(), ctx->facc.as<double>(), sc);
+        k_update_fused<L, double, double, fused_chunk<double>()><<<(unsigned)G, FUSED_THREADS, 0, ctx->stream>>>(ctx->group_start.as<int32_t>(),
+            ctx->group_nbr.as<int32_t>(), ctx->pd.as<double>(), ctx->pi.as<int32_t>(), ctx->Pcap, ctx->base.as<short4>(), ctx->cfg.dx, ctx->dt,
+            ctx->frac.as<double>(), ctx->vstar.as<double>(), ctx->scratch.as<double>(), ctx->facc.as<double>(), sc, &dc->flags, 0);
         ++g_kernel_launches;
     }
     return ZMPM_OK;
 }
 int launch_update(Ctx* ctx, bool gated) { return ctx->layout == 1 ? update_impl<Layout244>(ctx, gated) : update_impl<Layout444>(ctx, gated); }
 
-template <class L, class TH>
-static void hvp_launch(Ctx* ctx, const double* x0, const double* x1, int alt, double* out, const SolverScalars* sc)
+// out += dt^-2 (Hessian part of A) x: the fused product, T the context's HVP
+// precision, on an FP64 input vector
+template <class L>
+static int hvp_impl(Ctx* ctx, const double* x0, const double* x1, int alt, double* out, const SolverScalars* sc)
 {
     const int64_t G = ctx->G;
+    if (G == 0) return ZMPM_OK;
     DevCounters* dc = ctx->counters.as<DevCounters>();
-    k_hvp_stress<L, TH><<<(unsigned)G, XF_THREADS, 0, ctx->stream>>>(ctx->group_start.as<int32_t>(), ctx->group_nbr.as<int32_t>(),
-        ctx->pi.as<int32_t>(), ctx->Pcap, ctx->base.as<short4>(), ctx->cfg.dx, ctx->frac.as<TH>(), ctx->scratch.as<TH>(), x0, x1, alt,
-        ctx->dstress.as<TH>(), sc, &dc->flags);
-    ++g_kernel_launches;
-    k_hvp_scatter<L, TH><<<(unsigned)G, XF_THREADS, 0, ctx->stream>>>(ctx->group_start.as<int32_t>(), ctx->group_nbr.as<int32_t>(), ctx->Pcap,
-        ctx->base.as<short4>(), ctx->cfg.dx, ctx->frac.as<TH>(), ctx->dstress.as<TH>(), out, sc);
-    ++g_kernel_launches;
-}
-
-template <class L>
-static int hvp_impl(Ctx* ctx, const double* x0, const double* x1, int alt, double* out, bool fp32, const SolverScalars* sc)
-{
-    if (ctx->G == 0) return ZMPM_OK;
-    if (fp32)
-        hvp_launch<L, float>(ctx, x0, x1, alt, out, sc);
+    if (ctx->mixed)
+        k_hvp_fused<L, float, double, fused_chunk<float>()><<<(unsigned)G, FUSED_THREADS, 0, ctx->stream>>>(ctx->group_start.as<int32_t>(),
+            ctx->group_nbr.as<int32_t>(), ctx->pi.as<int32_t>(), ctx->Pcap, ctx->base.as<short4>(), ctx->cfg.dx, ctx->frac.as<float>(),
+            ctx->scratch.as<float>(), x0, x1, alt, out, sc, &dc->flags);
     else
-        hvp_launch<L, double>(ctx, x0, x1, alt, out, sc);
+        k_hvp_fused<L, double, double, fused_chunk<double>()><<<(unsigned)G, FUSED_THREADS, 0, ctx->stream>>>(ctx->group_start.as<int32_t>(),
+            ctx->group_nbr.as<int32_t>(), ctx->pi.as<int32_t>(), ctx->Pcap, ctx->base.as<short4>(), ctx->cfg.dx, ctx->frac.as<double>(),
+            ctx->scratch.as<double>(), x0, x1, alt, out, sc, &dc->flags);
+    ++g_kernel_launches;
     return ZMPM_OK;
 }
 
+// The FP32 product inside MINRES on the node-major FP32 copies of Z.
 template <class L>
 static int hvp_f32_impl(Ctx* ctx, const float* x0, const float* x1, double* out)
 {
@@ -769,12 +871,9 @@ static int hvp_f32_impl(Ctx* ctx, const float* x0, const float* x1, double* out)
     if (G == 0) return ZMPM_OK;
     const SolverScalars* sc = ctx->scal.as<SolverScalars>();
     DevCounters* dc = ctx->counters.as<DevCounters>();
-    k_hvp_stress<L, float, float><<<(unsigned)G, XF_THREADS, 0, ctx->stream>>>(ctx->group_start.as<int32_t>(), ctx->group_nbr.as<int32_t>(),
-        ctx->pi.as<int32_t>(), ctx->Pcap, ctx->base.as<short4>(), ctx->cfg.dx, ctx->frac.as<float>(), ctx->scratch.as<float>(), x0, x1, 1,
-        ctx->dstress.as<float>(), sc, &dc->flags);
-    ++g_kernel_launches;
-    k_hvp_scatter<L, float><<<(unsigned)G, XF_THREADS, 0, ctx->stream>>>(ctx->group_start.as<int32_t>(), ctx->group_nbr.as<int32_t>(), ctx->Pcap,
-        ctx->base.as<short4>(), ctx->cfg.dx, ctx->frac.as<float>(), ctx->dstress.as<float>(), out, sc);
+    k_hvp_fused<L, float, float, fused_chunk<float>()><<<(unsigned)G, FUSED_THREADS, 0, ctx->stream>>>(ctx->group_start.as<int32_t>(),
+        ctx->group_nbr.as<int32_t>(), ctx->pi.as<int32_t>(), ctx->Pcap, ctx->base.as<short4>(), ctx->cfg.dx, ctx->frac.as<float>(),
+        ctx->scratch.as<float>(), x0, x1, 1, out, sc, &dc->flags);
     ++g_kernel_launches;
     return ZMPM_OK;
 }
@@ -788,14 +887,13 @@ int launch_hvp_krylov_f32(Ctx* ctx, const float* x0, const float* x1, double* ou
 int launch_hvp_krylov(Ctx* ctx, const double* x0, const double* x1, bool alt, double* out)
 {
     const SolverScalars* sc = ctx->scal.as<SolverScalars>();
-    return ctx->layout == 1 ? hvp_impl<Layout244>(ctx, x0, x1, alt ? 1 : 0, out, ctx->mixed, sc)
-                            : hvp_impl<Layout444>(ctx, x0, x1, alt ? 1 : 0, out, ctx->mixed, sc);
+    return ctx->layout == 1 ? hvp_impl<Layout244>(ctx, x0, x1, alt ? 1 : 0, out, sc) : hvp_impl<Layout444>(ctx, x0, x1, alt ? 1 : 0, out, sc);
 }
 
 int launch_hvp(Ctx* ctx, const double* x, double* out, bool fp32)
 {
-    if (fp32 && !ctx->mixed) return ZMPM_UNSUPPORTED;
-    return ctx->layout == 1 ? hvp_impl<Layout244>(ctx, x, x, 0, out, ctx->mixed, nullptr) : hvp_impl<Layout444>(ctx, x, x, 0, out, ctx->mixed, nullptr);
+    if (fp32 != ctx->mixed) return ZMPM_UNSUPPORTED;
+    return ctx->layout == 1 ? hvp_impl<Layout244>(ctx, x, x, 0, out, nullptr) : hvp_impl<Layout444>(ctx, x, x, 0, out, nullptr);
 }
 
 template <class L, class TH>
