@@ -24,5 +24,6 @@ def test_cpp_phase_adapter_matches_substep(tmp_path, cuda_lib, precision):
     assert out.returncode == 0, out.stdout + out.stderr
     fields = out.stdout.split()
     assert fields[0] == "max_rel_dx", out.stdout
-    # the two runs differ only in the order of floating-point atomics
-    assert float(fields[1]) < 1e-9, out.stdout
+    # the two runs differ only in the order of floating-point atomics (FP32
+    # sums in the mixed substep's transfers and products)
+    assert float(fields[1]) < (1e-9 if precision == "fp64" else 1e-5), out.stdout

@@ -114,7 +114,7 @@ def test_mls_mixed_and_refused_by_newton(cuda_lib, oracle):
 
 
 def test_explicit_mixed_tracks_fp64_oracle(cuda_lib, oracle):
-    """MIXED: FP32 constitutive stress, FP64 transfers, grid and state."""
+    """MIXED: FP32 constitutive stress and transfers; FP64 positions and grid sums."""
     sims = [scene(None, "fcr", precision="mixed"), scene(oracle, "fcr")]
     run(sims, 12)
     pg, po = sims[0].getParticles(), sims[1].getParticles()
@@ -131,8 +131,9 @@ def test_explicit_free_fall_is_exact(cuda_lib, precision):
     run([s], 10, dt)
     p = s.getParticles()
     # FP64: exact up to round-off.  MIXED: the FP32 constitutive step at F = I
-    # leaves stress round-off of order mu * 1e-7, a force that moves V by < 1e-6
-    atol = 1e-12 if precision == "fp64" else 1e-6
+    # leaves stress round-off of order mu * 1e-7, and the FP32 transfers round
+    # the velocity to FP32 (relative 1e-7 of |v| ~ 0.1 m/s per substep)
+    atol = 1e-12 if precision == "fp64" else 1e-5
     np.testing.assert_allclose(p["V"], v0 + 10 * dt * np.array([0, -9.8, 0]), rtol=0, atol=atol)
     np.testing.assert_allclose(p["C"], 0, atol=1e-9 if precision == "fp64" else 1e-3)
 

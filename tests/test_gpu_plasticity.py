@@ -62,7 +62,9 @@ def test_plasticity_mixed_tracks_fp64_oracle(cuda_lib, oracle, kind):
             assert s.advanceOneTimeStep(1e-3) == abi.OK
     pg, po = sims[0].getParticles(), sims[1].getParticles()
     assert rel(pg["X"], po["X"]) < 1e-6
-    np.testing.assert_allclose(sims[0].getLogJp(), sims[1].getLogJp(), rtol=0, atol=1e-4)
+    # the return maps run in FP64 on the FP32-evolved F; Cam-Clay's fake hardening
+    # (sinh of xi log Jp) amplifies that F's FP32 rounding
+    np.testing.assert_allclose(sims[0].getLogJp(), sims[1].getLogJp(), rtol=0, atol=1e-3)
 
 
 def test_admm_refuses_clay(cuda_lib):

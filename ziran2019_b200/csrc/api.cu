@@ -19,6 +19,16 @@ int launch_p2g(Ctx* ctx);
 
 namespace {
 
+// Device -> host copy ordered after the context's stream (whose work produced
+// the data), complete on return.  The library's stream does not synchronise
+// with the legacy default stream, so plain cudaMemcpy would not order it.
+cudaError_t d2h_sync(Ctx* ctx, void* dst, const void* src, size_t bytes)
+{
+    cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, ctx->stream);
+    if (e != cudaSuccess) return e;
+    return cudaStreamSynchronize(ctx->stream);
+}
+
 int64_t bitlen(uint64_t v)
 {
     int64_t n = 0;
@@ -107,9 +117,9 @@ int upload(Ctx* ctx)
         for (int d = 0; d < 3; ++d) hpd[(PD_LASTDV + d) * cap + i] = ctx->hlastdv[3 * i + d];
         sid[i] = (int32_t)i;
     }
-    ZMPM_CUDA(cudaMemcpy(ctx->pd.p, hpd.data(), hpd.size() * sizeof(double), cudaMemcpyHostToDevice));
-    ZMPM_CUDA(cudaMemcpy(ctx->pi.p, hpi.data(), hpi.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
-    ZMPM_CUDA(cudaMemcpy(ctx->slot_of_id.p, sid.data(), sid.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
+    ZMPM_CUDA(cudaMemcpyAsync(ctx->pd.p, hpd.data(), hpd.size() * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    ZMPM_CUDA(cudaMemcpyAsync(ctx->pi.p, hpi.data(), hpi.size() * sizeof(int32_t), cudaMemcpyHostToDevice, ctx->stream));
+    ZMPM_CUDA(cudaMemcpyAsync(ctx->slot_of_id.p, sid.data(), sid.size() * sizeof(int32_t), cudaMemcpyHostToDevice, ctx->stream));
     ctx->has_damage = false;
     ctx->has_visco = false;
     ctx->all_models = true;
@@ -138,8 +148,8 @@ int download(Ctx* ctx)
     std::vector<double> hpd((size_t)ctx->pd_active * cap);
     std::vector<int32_t> hpi((size_t)PI_FIELDS * cap);
     ZMPM_CUDA(cudaStreamSynchronize(ctx->stream));
-    ZMPM_CUDA(cudaMemcpy(hpd.data(), ctx->pd.p, hpd.size() * sizeof(double), cudaMemcpyDeviceToHost));
-    ZMPM_CUDA(cudaMemcpy(hpi.data(), ctx->pi.p, hpi.size() * sizeof(int32_t), cudaMemcpyDeviceToHost));
+    ZMPM_CUDA(d2h_sync(ctx, hpd.data(), ctx->pd.p, hpd.size() * sizeof(double)));
+    ZMPM_CUDA(d2h_sync(ctx, hpi.data(), ctx->pi.p, hpi.size() * sizeof(int32_t)));
     for (int64_t s = 0; s < P; ++s) {
         const int64_t i = hpi[PI_ID * cap + s];
         for (int d = 0; d < 3; ++d) {
@@ -239,7 +249,7 @@ int node_indices(Ctx* ctx, std::vector<int64_t>& idx, std::vector<double>& hm)
     hm.resize(nn);
     idx.assign(nn, -1);
     ZMPM_CUDA(cudaStreamSynchronize(ctx->stream));
-    if (nn) ZMPM_CUDA(cudaMemcpy(hm.data(), ctx->gm.p, nn * sizeof(double), cudaMemcpyDeviceToHost));
+    if (nn) ZMPM_CUDA(d2h_sync(ctx, hm.data(), ctx->gm.p, nn * sizeof(double)));
     int64_t c = 0;
     for (int64_t n = 0; n < nn; ++n)
         if (hm[n] != 0) idx[n] = c++;
@@ -449,6 +459,8 @@ int zmpm_create(const zmpm_config* cfg, zmpm_ctx** out)
     if ((e = ctx->dcolliders.ensure(2 * MAX_COLLIDERS * sizeof(DevCollider))) != cudaSuccess) return fail(e);
     cudaMemset(ctx->counters.p, 0, sizeof(DevCounters));
     cudaMemset(ctx->scal.p, 0, sizeof(SolverScalars));
+    // the context's stream does not order itself after the legacy stream's memsets
+    if ((e = cudaDeviceSynchronize()) != cudaSuccess) return fail(e);
     *out = ctx;
     return ZMPM_OK;
 }
@@ -463,7 +475,7 @@ int zmpm_destroy(zmpm_ctx* ctx)
         &ctx->group_page, &ctx->group_nbr, &ctx->emit_flag, &ctx->emit_scan, &ctx->page_first, &ctx->page_block, &ctx->block_page,
         &ctx->block_index, &ctx->gm, &ctx->gmv, &ctx->vn, &ctx->dv, &ctx->vstar, &ctx->facc, &ctx->res, &ctx->proj, &ctx->collided,
         &ctx->node_idx, &ctx->red, &ctx->scal, &ctx->counters, &ctx->dcolliders, &ctx->adm_F, &ctx->adm_gvn, &ctx->adm_B, &ctx->adm_pre,
-        &ctx->adm_rhs, &ctx->adm_w, &ctx->adj, &ctx->kvf, &ctx->pfn, &ctx->pfsc };
+        &ctx->adm_rhs, &ctx->adm_w, &ctx->adj, &ctx->kvf, &ctx->vstarf, &ctx->pfn, &ctx->pfsc };
     for (DBuf* b : bufs) b->release();
     for (auto& b : ctx->kv) b.release();
     for (auto* v : { &ctx->ckpt_pd, &ctx->ckpt_pi, &ctx->ckpt_sid })
@@ -1259,7 +1271,7 @@ int zmpm_adjoint_substep(zmpm_ctx* ctx, double dt, const zmpm_solver* s, double 
     }
     ZMPM_CUDA(cudaStreamSynchronize(sm));
     DevCounters hc;
-    ZMPM_CUDA(cudaMemcpy(&hc, ctx->counters.p, sizeof(hc), cudaMemcpyDeviceToHost));
+    ZMPM_CUDA(d2h_sync(ctx, &hc, ctx->counters.p, sizeof(hc)));
     st->krylov_iterations = ha.krylov_iters;
     st->hvp_count = ha.hvp_count;
     st->cfl_violation = (hc.flags & FLAG_CFL) ? 1 : 0;
@@ -1352,9 +1364,9 @@ int zmpm_bin_fetch(zmpm_ctx* ctx, zmpm_bin_result* out)
     std::vector<uint64_t> keys(P), bidx(B);
     std::vector<int32_t> gs(G + 1);
     ZMPM_CUDA(cudaStreamSynchronize(ctx->stream));
-    if (P) ZMPM_CUDA(cudaMemcpy(keys.data(), ctx->keys.p, P * sizeof(uint64_t), cudaMemcpyDeviceToHost));
-    if (G) ZMPM_CUDA(cudaMemcpy(gs.data(), ctx->group_start.p, (G + 1) * sizeof(int32_t), cudaMemcpyDeviceToHost));
-    if (B) ZMPM_CUDA(cudaMemcpy(bidx.data(), ctx->block_index.p, B * sizeof(uint64_t), cudaMemcpyDeviceToHost));
+    if (P) ZMPM_CUDA(d2h_sync(ctx, keys.data(), ctx->keys.p, P * sizeof(uint64_t)));
+    if (G) ZMPM_CUDA(d2h_sync(ctx, gs.data(), ctx->group_start.p, (G + 1) * sizeof(int32_t)));
+    if (B) ZMPM_CUDA(d2h_sync(ctx, bidx.data(), ctx->block_index.p, B * sizeof(uint64_t)));
     for (int64_t i = 0; i < P; ++i) {
         const uint64_t k = keys[i];
         const int32_t id = (int32_t)(k & ((1ull << index_bits) - 1));
@@ -1414,7 +1426,7 @@ void tv_to_dense(const Ctx* ctx, const std::vector<int64_t>& idx, const double* 
 int fetch_vec(Ctx* ctx, const DBuf& buf, std::vector<double>& h)
 {
     h.resize(3 * ctx->B * ctx->npb());
-    if (!h.empty()) ZMPM_CUDA(cudaMemcpy(h.data(), buf.p, h.size() * sizeof(double), cudaMemcpyDeviceToHost));
+    if (!h.empty()) ZMPM_CUDA(d2h_sync(ctx, h.data(), buf.p, h.size() * sizeof(double)));
     return ZMPM_OK;
 }
 } // namespace
@@ -1432,7 +1444,7 @@ int zmpm_get_grid(zmpm_ctx* ctx, double* m, double* v, int32_t* coord)
     rc = fetch_vec(ctx, ctx->vn, hv);
     if (rc) return rc;
     std::vector<int4> bp(ctx->B);
-    if (ctx->B) ZMPM_CUDA(cudaMemcpy(bp.data(), ctx->block_page.p, ctx->B * sizeof(int4), cudaMemcpyDeviceToHost));
+    if (ctx->B) ZMPM_CUDA(d2h_sync(ctx, bp.data(), ctx->block_page.p, ctx->B * sizeof(int4)));
     const int npb = ctx->npb();
     const int bx = ctx->layout == 1 ? 2 : 4, by = 4, bz = 4, yb = 2, zb = 2;
     for (size_t n = 0; n < idx.size(); ++n) {
@@ -1464,7 +1476,7 @@ int zmpm_get_initial_dv(zmpm_ctx* ctx, double* dv, int32_t* collided)
     if (dv) dense_to_tv(ctx, idx, hd, dv);
     if (collided) {
         std::vector<int8_t> hc(idx.size());
-        if (!hc.empty()) ZMPM_CUDA(cudaMemcpy(hc.data(), ctx->collided.p, hc.size(), cudaMemcpyDeviceToHost));
+        if (!hc.empty()) ZMPM_CUDA(d2h_sync(ctx, hc.data(), ctx->collided.p, hc.size()));
         for (size_t n = 0; n < idx.size(); ++n)
             if (idx[n] >= 0) collided[idx[n]] = hc[n];
     }
@@ -1493,11 +1505,12 @@ int zmpm_residual(zmpm_ctx* ctx, const double* dvin, double* r, double* norm)
         }
     const size_t bytes = hdv.size() * sizeof(double);
     if (bytes) {
-        ZMPM_CUDA(cudaMemcpy(ctx->dv.p, hdv.data(), bytes, cudaMemcpyHostToDevice));
-        ZMPM_CUDA(cudaMemcpy(ctx->vstar.p, hvs.data(), bytes, cudaMemcpyHostToDevice));
-        ZMPM_CUDA(cudaMemset(ctx->facc.p, 0, bytes));
+        ZMPM_CUDA(cudaMemcpyAsync(ctx->dv.p, hdv.data(), bytes, cudaMemcpyHostToDevice, ctx->stream));
+        ZMPM_CUDA(cudaMemcpyAsync(ctx->vstar.p, hvs.data(), bytes, cudaMemcpyHostToDevice, ctx->stream));
+        ctx->vstarf_valid = false;
+        ZMPM_CUDA(cudaMemsetAsync(ctx->facc.p, 0, bytes, ctx->stream));
     }
-    ZMPM_CUDA(cudaMemset(ctx->scal.p, 0, sizeof(SolverScalars)));
+    ZMPM_CUDA(cudaMemsetAsync(ctx->scal.p, 0, sizeof(SolverScalars), ctx->stream));
     rc = launch_update(ctx);
     if (rc) return rc;
     rc = launch_residual(ctx);
@@ -1550,8 +1563,8 @@ int zmpm_multiply(zmpm_ctx* ctx, const double* x, double* b, int32_t fp32)
     double* dx_ = ctx->kv[0].as<double>();
     double* dq = ctx->kv[1].as<double>();
     if (bytes) {
-        ZMPM_CUDA(cudaMemcpy(dx_, hx.data(), bytes, cudaMemcpyHostToDevice));
-        ZMPM_CUDA(cudaMemset(ctx->kv[9].p, 0, bytes));
+        ZMPM_CUDA(cudaMemcpyAsync(dx_, hx.data(), bytes, cudaMemcpyHostToDevice, ctx->stream));
+        ZMPM_CUDA(cudaMemsetAsync(ctx->kv[9].p, 0, bytes, ctx->stream));
     }
     rc = launch_hvp(ctx, dx_, ctx->kv[9].as<double>(), ctx->mixed);
     if (rc) return rc;

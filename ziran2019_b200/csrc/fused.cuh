@@ -235,11 +235,12 @@ constexpr int REC_FIELDS = 12;
 // 3 + 3 r + c) fall in different shared-memory banks
 template <int CH>
 constexpr int rec_stride() { return CH + 1; }
-template <class L, class T, int CH>
+// NF record fields per particle, NC scattered components per node
+template <class L, class T, int CH, int NF = REC_FIELDS, int NC = 3>
 struct ScatterSmem {
     static constexpr int FS = rec_stride<CH>();
-    __align__(16) T acc[8 * 3 * L::NPB];
-    __align__(16) T rec[REC_FIELDS * FS];
+    __align__(16) T acc[8 * NC * L::NPB];
+    __align__(16) T rec[NF * FS];
     CellLayout<L> cl;
     int32_t occ[L::NPB];
     int32_t nocc;
@@ -247,14 +248,14 @@ struct ScatterSmem {
 };
 
 // The group's occupied cells, in cell order (after build_cell_layout).
-template <class L, class T, int CH>
-__device__ __forceinline__ void list_occupied(ScatterSmem<L, T, CH>& sm)
+template <class SM>
+__device__ __forceinline__ void list_occupied(SM& sm)
 {
     if (threadIdx.x < 32) {
         const int lane = threadIdx.x;
         int base = 0;
 #pragma unroll
-        for (int c = 0; c < L::NPB; c += 32) {
+        for (int c = 0; c < (int)(sizeof(sm.occ) / sizeof(sm.occ[0])); c += 32) {
             const bool on = sm.cl.cnt[c + lane] > 0;
             const unsigned m = __ballot_sync(0xffffffffu, on);
             if (on) sm.occ[base + __popc(m & ((1u << lane) - 1u))] = c + lane;
@@ -341,6 +342,97 @@ __device__ __forceinline__ void scatter_rows(ScatterSmem<L, T, CH>& sm, int c0, 
             for (int j = 0; j < 3; ++j)
 #pragma unroll
                 for (int k = 0; k < 3; ++k) atomicAdd(sm.acc + window_scalar<NPB>(so.X[i] + so.Y[j] + so.Z[k], r, 3), a[9 * i + 3 * j + k]);
+    }
+}
+
+// Phase 2 of the APIC P2G (particlesToGridHelper, MpmSimulationBase.cpp:563-
+// 608) for the chunk [c0, c1): item (component c, occupied cell) adds, for the
+// cell's particles, w_ip m_p (c = 0) or w_ip (q_r + a_r i + b_r j + c_r k)
+// (c = r + 1, the momentum m (v + C (x_i - x_p)) written affinely in the node
+// offset (i, j, k)) to the window.  Records: fractions at fields 0-2, the mass
+// at 3, row r's (q, a, b, c) at 4 + 4 r .. 7 + 4 r.  FP32 takes the cell's
+// particles two at a time as packed pairs.
+template <class L, class T, int CH>
+__device__ __forceinline__ void scatter_p2g(ScatterSmem<L, T, CH, 16, 4>& sm, int c0, int c1)
+{
+    constexpr int NPB = L::NPB;
+    constexpr int FS = ScatterSmem<L, T, CH, 16, 4>::FS;
+    const int nocc = sm.nocc, items = 4 * nocc;
+    for (int q = threadIdx.x; q < items; q += blockDim.x) {
+        const int c = q / nocc, cidx = q - c * nocc;
+        const int ce = sm.occ[cidx];
+        const int st = sm.cl.start[ce];
+        const int p0 = (st > c0 ? st : c0) - c0;
+        const int e1 = st + sm.cl.cnt[ce];
+        const int p1 = (e1 < c1 ? e1 : c1) - c0;
+        if (p0 >= p1) continue;
+        const T* fr = sm.rec;
+        const T* row = sm.rec + (c == 0 ? 3 : 4 * c) * FS; // mass, or (q, a, b, c) of row c - 1
+        T a[27];
+        if constexpr (sizeof(T) == 4) {
+            float2 a2[27];
+#pragma unroll
+            for (int n = 0; n < 27; ++n) a2[n] = f2(0.f);
+            for (int p = p0; p < p1; p += 2) {
+                const int pq = p + 1 < p1 ? p + 1 : p;
+                const float sq = p + 1 < p1 ? 1.f : 0.f;
+                float2 w[3][3], dw[3][3];
+#pragma unroll
+                for (int d = 0; d < 3; ++d) bspline_all2(f2(fr[d * FS + p], fr[d * FS + pq]), w[d], dw[d]);
+                const float2 q0 = f2(row[p], sq * row[pq]);
+                float2 ax = f2(0.f), by = f2(0.f), cz = f2(0.f);
+                if (c != 0) {
+                    ax = f2(row[FS + p], sq * row[FS + pq]);
+                    by = f2(row[2 * FS + p], sq * row[2 * FS + pq]);
+                    cz = f2(row[3 * FS + p], sq * row[3 * FS + pq]);
+                }
+                const float2 wx1 = w[0][1], wx2 = mul2(w[0][2], f2(2.f)); // i w_i for i = 1, 2
+#pragma unroll
+                for (int j = 0; j < 3; ++j)
+#pragma unroll
+                    for (int k = 0; k < 3; ++k) {
+                        const float2 t = mul2(w[1][j], w[2][k]);
+                        // (q + b j + c k) t and a t
+                        float2 l = q0;
+                        if (j) l = fma2(by, f2((float)j), l);
+                        if (k) l = fma2(cz, f2((float)k), l);
+                        const float2 u = mul2(l, t), v = mul2(ax, t);
+                        a2[3 * j + k] = fma2(w[0][0], u, a2[3 * j + k]);
+                        a2[9 + 3 * j + k] = fma2(w[0][1], u, fma2(wx1, v, a2[9 + 3 * j + k]));
+                        a2[18 + 3 * j + k] = fma2(w[0][2], u, fma2(wx2, v, a2[18 + 3 * j + k]));
+                    }
+            }
+#pragma unroll
+            for (int n = 0; n < 27; ++n) a[n] = a2[n].x + a2[n].y;
+        }
+        else {
+#pragma unroll
+            for (int n = 0; n < 27; ++n) a[n] = T(0);
+            for (int p = p0; p < p1; ++p) {
+                T w[3][3], dw[3][3];
+#pragma unroll
+                for (int d = 0; d < 3; ++d) bspline_all(fr[d * FS + p], w[d], dw[d]);
+                const T q0 = row[p];
+                const T ax = c ? row[FS + p] : T(0), by = c ? row[2 * FS + p] : T(0), cz = c ? row[3 * FS + p] : T(0);
+#pragma unroll
+                for (int j = 0; j < 3; ++j)
+#pragma unroll
+                    for (int k = 0; k < 3; ++k) {
+                        const T t = w[1][j] * w[2][k];
+                        const T u = (q0 + by * T(j) + cz * T(k)) * t, v = ax * t;
+#pragma unroll
+                        for (int i = 0; i < 3; ++i) a[9 * i + 3 * j + k] += w[0][i] * u + (T(i) * w[0][i]) * v;
+                    }
+            }
+        }
+        const int lx = ce >> (L::YB + L::ZB), ly = (ce >> L::ZB) & (L::BY - 1), lz = ce & (L::BZ - 1);
+        const StencilOffsets<L> so(lx, ly, lz);
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 3; ++j)
+#pragma unroll
+                for (int k = 0; k < 3; ++k) atomicAdd(sm.acc + window_scalar<NPB>(so.X[i] + so.Y[j] + so.Z[k], c, 4), a[9 * i + 3 * j + k]);
     }
 }
 

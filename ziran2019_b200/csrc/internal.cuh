@@ -185,6 +185,8 @@ struct Ctx {
     DBuf gm, gmv, vn, dv, vstar, facc, res, proj, collided, node_idx;
     // Krylov vectors
     DBuf kv[10];
+    DBuf vstarf;                          // MIXED: FP32 node-major copy of vstar ([B][NPB][4]), the particle kernels' gather input
+    bool vstarf_valid = false;            // vstarf holds the current vstar (the Newton solve keeps it; other integrators refresh it)
     DBuf kvf;                             // FP32 node-major copies of MINRES's two Z vectors ([2][B][NPB][4]), read by the FP32 product
     DBuf red;                             // reduction partials [4][RED_MAX_CTAS]
     DBuf scal;                            // SolverScalars
@@ -231,6 +233,7 @@ int run_binning(Ctx* ctx);
 int run_p2g(Ctx* ctx, bool damage = true);            // P2G (+ damage hook) + grid normalisation + Newton setup
 int run_newton(Ctx* ctx, const zmpm_solver& s);       // backward-Euler Newton
 int run_g2p(Ctx* ctx, bool plastic = true);            // G2P + evolveStrain (+ applyPlasticity)
+int refresh_vstar_f32(Ctx* ctx);                       // MIXED: vstarf from vstar
 int launch_plasticity(Ctx* ctx);                       // applyPlasticity alone
 int upload_colliders(Ctx* ctx, double time, int slot = 0);    // slot 1: the state at t + dt
 int upload(Ctx* ctx);      // host scene arrays -> device pools (once per edit)

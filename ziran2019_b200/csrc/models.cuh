@@ -237,14 +237,12 @@ ZMPM_D M3<TH> model_hvp(int kind, const TH* __restrict__ scr, int64_t stride, in
     return m3_zero<TH>();
 }
 
-// VonMisesStvkHencky::projectStrain, Lib/Ziran/Physics/PlasticityApplier.cpp:462-502.
-// Returns true when the state changed; updates yield stress and the broken flag.
+// VonMisesStvkHencky::projectStrain, Lib/Ziran/Physics/PlasticityApplier.cpp:462-502,
+// on F = U diag(sg) V^T; updates F, the yield stress and the broken flag.
 template <class T>
-ZMPM_D void von_mises_project(T mu, T lambda, T& yield_stress, T xi, T fail_stress, int& broken, T crack[3], M3<T>& F)
+ZMPM_D void von_mises_from_svd(T mu, T lambda, T& yield_stress, T xi, T fail_stress, int& broken, T crack[3], M3<T>& F, const M3<T>& U,
+    const T sg[3], const M3<T>& V)
 {
-    M3<T> U, V;
-    T sg[3];
-    svd3(F, U, sg, V);
     T e[3];
 #pragma unroll
     for (int d = 0; d < 3; ++d) e[d] = log(sg[d] > T(1e-4) ? sg[d] : T(1e-4));
@@ -268,6 +266,15 @@ ZMPM_D void von_mises_project(T mu, T lambda, T& yield_stress, T xi, T fail_stre
 #pragma unroll
         for (int d = 0; d < 3; ++d) crack[d] = V(d, 0);
     }
+}
+
+template <class T>
+ZMPM_D void von_mises_project(T mu, T lambda, T& yield_stress, T xi, T fail_stress, int& broken, T crack[3], M3<T>& F)
+{
+    M3<T> U, V;
+    T sg[3];
+    svd3(F, U, sg, V);
+    von_mises_from_svd(mu, lambda, yield_stress, xi, fail_stress, broken, crack, F, U, sg, V);
 }
 
 // DruckerPragerStvkHencky::projectStrain (PlasticityApplier.cpp:272-317):

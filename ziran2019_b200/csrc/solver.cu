@@ -227,7 +227,7 @@ template <class L>
 __global__ void __launch_bounds__(ND_THREADS) k_grid_init(NodeGeom ng, const double* __restrict__ gm, const double* __restrict__ gmv,
     const int4* __restrict__ block_page, double dx, double gx, double gy, double gz, double dt, const DevCollider* __restrict__ cols, int ncols,
     double* __restrict__ vn, double* __restrict__ dv, double* __restrict__ vstar, int8_t* __restrict__ col, double* __restrict__ P6,
-    unsigned long long* __restrict__ nactive, int32_t* __restrict__ flags)
+    unsigned long long* __restrict__ nactive, int32_t* __restrict__ flags, float4* __restrict__ vstar_f)
 {
     constexpr int NPB = L::NPB;
     int local = 0;
@@ -255,12 +255,15 @@ __global__ void __launch_bounds__(ND_THREADS) k_grid_init(NodeGeom ng, const dou
                 d[2] = gz * dt;
             }
         }
+        double vs[3];
         for (int k = 0; k < 3; ++k) {
             int64_t vi = vidx<NPB>(n, k);
             vn[vi] = v[k];
             dv[vi] = d[k];
-            vstar[vi] = (m != 0) ? v[k] + d[k] : 0.0;
+            vs[k] = (m != 0) ? v[k] + d[k] : 0.0;
+            vstar[vi] = vs[k];
         }
+        if (vstar_f) vstar_f[n] = make_float4((float)vs[0], (float)vs[1], (float)vs[2], 0.f);
         col[n] = c;
         for (int k = 0; k < 6; ++k) P6[k * ng.nn + n] = P[k];
     }
@@ -828,22 +831,35 @@ __global__ void __launch_bounds__(ND_THREADS) k_mr_b(NodeGeom ng, const double* 
 // vstar = vn + dv on active nodes.
 template <int NPB>
 __global__ void __launch_bounds__(ND_THREADS) k_newton_step(NodeGeom ng, const double* __restrict__ gm, KrylovBufs kb, int minres,
-    const double* __restrict__ vn, double* __restrict__ dv, double* __restrict__ vstar, const SolverScalars* __restrict__ sc)
+    const double* __restrict__ vn, double* __restrict__ dv, double* __restrict__ vstar, const SolverScalars* __restrict__ sc,
+    float4* __restrict__ vstar_f)
 {
     if (sc->newton_done) return;
     MrPending pd = mr_pending(kb, sc, sc->kit);
     pd.on = pd.on && minres;
     for (int64_t n = (int64_t)blockIdx.x * ND_THREADS + threadIdx.x; n < ng.nn; n += (int64_t)gridDim.x * ND_THREADS) {
         const bool act = gm[n] != 0;
+        double vs[3];
         for (int k = 0; k < 3; ++k) {
             int64_t i = vidx<NPB>(n, k);
             double step = kb.x[i];
             if (pd.on) step += pd.t * mr_direction(pd, i);
             double d = dv[i] + step;
             dv[i] = d;
-            vstar[i] = act ? vn[i] + d : 0.0;
+            vs[k] = act ? vn[i] + d : 0.0;
+            vstar[i] = vs[k];
         }
+        if (vstar_f) vstar_f[n] = make_float4((float)vs[0], (float)vs[1], (float)vs[2], 0.f);
     }
+}
+
+// The FP32 node-major copy of vstar ([B][NPB][4]) that the MIXED particle
+// kernels gather from, for the substeps whose grid update writes only vstar.
+template <int NPB>
+__global__ void __launch_bounds__(ND_THREADS) k_vstar_f32(NodeGeom ng, const double* __restrict__ vstar, float4* __restrict__ vstar_f)
+{
+    for (int64_t n = (int64_t)blockIdx.x * ND_THREADS + threadIdx.x; n < ng.nn; n += (int64_t)gridDim.x * ND_THREADS)
+        vstar_f[n] = make_float4((float)vstar[vidx<NPB>(n, 0)], (float)vstar[vidx<NPB>(n, 1)], (float)vstar[vidx<NPB>(n, 2)], 0.f);
 }
 
 // Ends a Newton iteration (NewtonsMethod.h:46 loop); as a graph, sets the
@@ -1037,6 +1053,7 @@ int ensure_node_buffers(Ctx* ctx)
     ZMPM_CUDA(ctx->collided.ensure(nn));
     for (int i = 0; i < 10; ++i) ZMPM_CUDA(ctx->kv[i].ensure(vec));
     ZMPM_CUDA(ctx->kvf.ensure((size_t)(8 * nn) * sizeof(float)));
+    ZMPM_CUDA(ctx->vstarf.ensure((size_t)(4 * nn) * sizeof(float)));
     return ZMPM_OK;
 }
 
@@ -1070,14 +1087,15 @@ int run_p2g(Ctx* ctx, bool damage)
             k_grid_init<Layout244><<<ng.parts, ND_THREADS, 0, st>>>(ng, ctx->gm.as<double>(), ctx->gmv.as<double>(), ctx->block_page.as<int4>(),
                 ctx->cfg.dx, g[0], g[1], g[2], ctx->dt, ctx->dcolliders.as<DevCollider>(), (int)ctx->colliders.size(), ctx->vn.as<double>(),
                 ctx->dv.as<double>(), ctx->vstar.as<double>(), ctx->collided.as<int8_t>(), ctx->proj.as<double>(),
-                reinterpret_cast<unsigned long long*>(&dc->N), &dc->flags);
+                reinterpret_cast<unsigned long long*>(&dc->N), &dc->flags, ctx->mixed ? ctx->vstarf.as<float4>() : nullptr);
         else
             k_grid_init<Layout444><<<ng.parts, ND_THREADS, 0, st>>>(ng, ctx->gm.as<double>(), ctx->gmv.as<double>(), ctx->block_page.as<int4>(),
                 ctx->cfg.dx, g[0], g[1], g[2], ctx->dt, ctx->dcolliders.as<DevCollider>(), (int)ctx->colliders.size(), ctx->vn.as<double>(),
                 ctx->dv.as<double>(), ctx->vstar.as<double>(), ctx->collided.as<int8_t>(), ctx->proj.as<double>(),
-                reinterpret_cast<unsigned long long*>(&dc->N), &dc->flags);
+                reinterpret_cast<unsigned long long*>(&dc->N), &dc->flags, ctx->mixed ? ctx->vstarf.as<float4>() : nullptr);
         ++g_kernel_launches;
     }
+    ctx->vstarf_valid = ctx->mixed; // k_grid_init wrote the FP32 copy
     ZMPM_CUDA(cudaGetLastError());
     return ZMPM_OK;
 }
@@ -1087,6 +1105,7 @@ int run_p2g(Ctx* ctx, bool damage)
 // hook, the explicit grid update with collisions and trial collision.
 int run_explicit(Ctx* ctx, const zmpm_solver& s)
 {
+    ctx->vstarf_valid = false; // k_grid_explicit writes vstar only
     cudaStream_t st = ctx->stream;
     const int64_t nn = ctx->B * ctx->npb();
     int rc = ensure_node_buffers(ctx);
@@ -1227,7 +1246,7 @@ int launch_newton_tail(const NewtonLaunch& L, cudaStream_t st, cudaGraphConditio
 {
     Ctx* ctx = L.ctx;
     k_newton_step<NPB><<<L.nb, ND_THREADS, 0, st>>>(L.ng, ctx->gm.as<double>(), L.kb, L.np.minres, ctx->vn.as<double>(), ctx->dv.as<double>(),
-        ctx->vstar.as<double>(), L.sc);
+        ctx->vstar.as<double>(), L.sc, ctx->mixed ? ctx->vstarf.as<float4>() : nullptr);
     k_newton_advance<<<1, 1, 0, st>>>(L.sc, L.np.nmax, hN, use_graph);
     g_kernel_launches += 2;
     return ZMPM_OK;
@@ -1652,7 +1671,8 @@ int run_adjoint_solve(Ctx* ctx, double tol, int max_iterations)
         ZMPM_CUDA(e2);
         // kernels executed: head (2) and tail (1) once, 5 per Krylov body (CG)
         SolverScalars hs;
-        ZMPM_CUDA(cudaMemcpy(&hs, Lc.sc, sizeof(hs), cudaMemcpyDeviceToHost));
+        ZMPM_CUDA(cudaMemcpyAsync(&hs, Lc.sc, sizeof(hs), cudaMemcpyDeviceToHost, st));
+        ZMPM_CUDA(cudaStreamSynchronize(st));
         g_kernel_launches = launches0 + 3 + 5 * (int64_t)hs.krylov_bodies;
     }
     else {
@@ -1675,11 +1695,29 @@ int run_adjoint_solve(Ctx* ctx, double tol, int max_iterations)
 
 int run_admm(Ctx* ctx, const zmpm_solver& s)
 {
+    ctx->vstarf_valid = false; // the ADMM kernels write vstar only
     return ctx->layout == 1 ? admm_impl<Layout244>(ctx, s) : admm_impl<Layout444>(ctx, s);
+}
+
+// MIXED: vstar_f from vstar (the ADMM and explicit grid updates write vstar only).
+int refresh_vstar_f32(Ctx* ctx)
+{
+    NodeGeom ng = node_geom(ctx);
+    if (ng.nn == 0) return ZMPM_OK;
+    if (ctx->layout == 1)
+        k_vstar_f32<32><<<ng.parts, ND_THREADS, 0, ctx->stream>>>(ng, ctx->vstar.as<double>(), ctx->vstarf.as<float4>());
+    else
+        k_vstar_f32<64><<<ng.parts, ND_THREADS, 0, ctx->stream>>>(ng, ctx->vstar.as<double>(), ctx->vstarf.as<float4>());
+    ++g_kernel_launches;
+    return ZMPM_OK;
 }
 
 int run_g2p(Ctx* ctx, bool plastic)
 {
+    if (ctx->mixed && !ctx->vstarf_valid) {
+        int rc = refresh_vstar_f32(ctx);
+        if (rc) return rc;
+    }
     int rc = launch_g2p(ctx, plastic);
     if (rc) return rc;
     ZMPM_CUDA(cudaGetLastError());

@@ -24,18 +24,20 @@ namespace zmpm {
 // Also writes each particle's fractional cell offsets (frac) for the FP32 HVP.
 // P2G with per-cell register accumulation: thread -> one cell of the page and
 // every (blockDim/NPB)-th particle of it; NCP of the four grid components
-// (mass, momentum x, y, z) are summed for the cell's 27 stencil nodes in FP64
+// (mass, momentum x, y, z) are summed for the cell's 27 stencil nodes in
 // registers per pass and added to the shared window once per pass, so the
 // window sees one atomic per (thread, node, component) instead of one per
 // (particle, node, component).  APIC P2G: m_i += w m_p, (mv)_i += w m_p (v_p +
-// C_p (x_i - x_p)) in FP64.
+// C_p (x_i - x_p)), in FP64 or, in MIXED contexts, FP32 (the grid sums are
+// FP64 in global memory either way).
 template <class L, class TH, int NCP>
 __global__ void __launch_bounds__(XF_THREADS, 3) k_p2g_reg(const int32_t* __restrict__ group_start, const int32_t* __restrict__ group_nbr,
     const double* __restrict__ pd, int64_t cap, const short4* __restrict__ base, double dx, double* __restrict__ gm, double* __restrict__ gmv,
     TH* __restrict__ frac)
 {
+    using TA = TH; // arithmetic: FP64, or FP32 in MIXED contexts (the stored fractions' type)
     constexpr int NPB = L::NPB;
-    __shared__ __align__(16) double acc[8 * 4 * NPB];
+    __shared__ __align__(16) TA acc[8 * 4 * NPB];
     __shared__ int32_t nbr[8];
     __shared__ CellLayout<L> cl;
     const int g = blockIdx.x;
@@ -47,42 +49,56 @@ __global__ void __launch_bounds__(XF_THREADS, 3) k_p2g_reg(const int32_t* __rest
     const int ce = threadIdx.x % NPB;
     const int lx = ce >> (L::YB + L::ZB), ly = (ce >> L::ZB) & (L::BY - 1), lz = ce & (L::BZ - 1);
     const int cnt = cl.cnt[ce], first = s0 + cl.start[ce];
+    const TA tdx = TA(dx);
 #pragma unroll 1
     for (int c0 = 0; c0 < 4; c0 += NCP) {
-        double a[27][NCP];
+        TA a[27][NCP];
 #pragma unroll
         for (int n = 0; n < 27; ++n)
 #pragma unroll
-            for (int c = 0; c < NCP; ++c) a[n][c] = 0.0;
+            for (int c = 0; c < NCP; ++c) a[n][c] = TA(0);
         for (int r = threadIdx.x / NPB; r < cnt; r += blockDim.x / NPB) {
             const int s = first + r;
             const short4 b = base[s];
-            double xp[3], w[3][3], dwr[3][3];
+            double xp[3];
+            TA fr[3], w[3][3], dwr[3][3];
 #pragma unroll
             for (int d = 0; d < 3; ++d) {
                 xp[d] = pd[(PD_X + d) * cap + s];
                 const double d0 = inv_dx * xp[d] - (double)((&b.x)[d]);
                 if (c0 == 0) frac[d * cap + s] = (TH)d0;
-                bspline(d0, w[d], dwr[d]);
+                fr[d] = (TA)d0;
+                bspline(fr[d], w[d], dwr[d]);
             }
             const double mass = pd[PD_M * cap + s];
-            double mom[NCP], Cm[NCP][3];
+            TA mom[NCP], Cm[NCP][3];
 #pragma unroll
             for (int c = 0; c < NCP; ++c) {
                 const int comp = c0 + c; // 0: mass, 1..3: momentum row comp-1
                 if (comp == 0) {
-                    mom[c] = mass;
-                    Cm[c][0] = Cm[c][1] = Cm[c][2] = 0.0;
+                    mom[c] = (TA)mass;
+                    Cm[c][0] = Cm[c][1] = Cm[c][2] = TA(0);
                 }
                 else {
                     const int rr = comp - 1;
-                    mom[c] = mass * pd[(PD_V + rr) * cap + s];
+                    mom[c] = (TA)(mass * pd[(PD_V + rr) * cap + s]);
 #pragma unroll
-                    for (int q = 0; q < 3; ++q) Cm[c][q] = mass * pd[(PD_C + 3 * rr + q) * cap + s];
+                    for (int q = 0; q < 3; ++q) Cm[c][q] = (TA)(mass * pd[(PD_C + 3 * rr + q) * cap + s]);
                 }
             }
-            for_stencil<L>(lx, ly, lz, w, dwr, inv_dx, [&](int, int, int i, int j, int k, double wijk, const double*) {
-                const double xi[3] = { (b.x + i) * dx - xp[0], (b.y + j) * dx - xp[1], (b.z + k) * dx - xp[2] };
+            for_stencil<L>(lx, ly, lz, w, dwr, TA(inv_dx), [&](int, int, int i, int j, int k, TA wijk, const TA*) {
+                // x_i - x_p: FP64 from the positions, FP32 from the cell fractions
+                TA xi[3];
+                if constexpr (sizeof(TA) == 8) {
+                    xi[0] = (b.x + i) * dx - xp[0];
+                    xi[1] = (b.y + j) * dx - xp[1];
+                    xi[2] = (b.z + k) * dx - xp[2];
+                }
+                else {
+                    xi[0] = (TA(i) - fr[0]) * tdx;
+                    xi[1] = (TA(j) - fr[1]) * tdx;
+                    xi[2] = (TA(k) - fr[2]) * tdx;
+                }
                 const int n = 9 * i + 3 * j + k;
 #pragma unroll
                 for (int c = 0; c < NCP; ++c) a[n][c] += (Cm[c][0] * xi[0] + Cm[c][1] * xi[1] + Cm[c][2] * xi[2] + mom[c]) * wijk;
@@ -97,7 +113,7 @@ __global__ void __launch_bounds__(XF_THREADS, 3) k_p2g_reg(const int32_t* __rest
                     for (int k = 0; k < 3; ++k) {
                         int e;
                         const int t = win_slot<L>(lx + i, ly + j, lz + k, e);
-                        double* dst = acc + t * 4 * NPB + e;
+                        TA* dst = acc + t * 4 * NPB + e;
 #pragma unroll
                         for (int c = 0; c < NCP; ++c) atomicAdd(dst + (c0 + c) * NPB, a[9 * i + 3 * j + k][c]);
                     }
@@ -105,6 +121,62 @@ __global__ void __launch_bounds__(XF_THREADS, 3) k_p2g_reg(const int32_t* __rest
     }
     __syncthreads();
     flush_window<4, 1, NPB>(acc, nbr, gm, gmv);
+}
+
+// APIC P2G as a fused per-page kernel (fused.cuh): phase 1 writes each
+// particle's cell fractions (also to `frac`, for the Newton kernels), its mass
+// and the affine form of its momentum; phase 2 (scatter_p2g) sums them into the
+// window by (component, occupied cell) items.  T: arithmetic (FP32 in MIXED
+// contexts); the window is flushed into the FP64 grid sums.
+template <class L, class T, int CH>
+__global__ void __launch_bounds__(FUSED_THREADS) k_p2g_fused(const int32_t* __restrict__ group_start, const int32_t* __restrict__ group_nbr,
+    const double* __restrict__ pd, int64_t cap, const short4* __restrict__ base, double dx, double* __restrict__ gm, double* __restrict__ gmv,
+    T* __restrict__ frac)
+{
+    constexpr int NPB = L::NPB;
+    using SM = ScatterSmem<L, T, CH, 16, 4>;
+    __shared__ SM sm;
+    const int g = blockIdx.x;
+    if (threadIdx.x < 8) sm.nbr[threadIdx.x] = group_nbr[8 * g + threadIdx.x];
+    zero_window<4, NPB>(sm.acc);
+    const int s0 = group_start[g], n = group_start[g + 1] - s0;
+    build_cell_layout<L>(sm.cl, base, s0, s0 + n);
+    list_occupied(sm);
+    const double inv_dx = 1.0 / dx;
+    const T tdx = T(dx);
+    for (int c0 = 0; c0 < n; c0 += CH) {
+        const int c1 = c0 + CH < n ? c0 + CH : n;
+        __syncthreads();
+        for (int p = c0 + threadIdx.x; p < c1; p += blockDim.x) {
+            const int64_t s = s0 + p;
+            T* rc = sm.rec + (p - c0);
+            const short4 b = base[s];
+            T fr[3];
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                const double d0 = inv_dx * pd[(PD_X + d) * cap + s] - (double)((&b.x)[d]);
+                fr[d] = (T)d0;
+                frac[d * cap + s] = fr[d];
+                rc[d * SM::FS] = fr[d];
+            }
+            const double mass = pd[PD_M * cap + s];
+            rc[3 * SM::FS] = (T)mass;
+#pragma unroll
+            for (int r = 0; r < 3; ++r) {
+                T mC[3];
+#pragma unroll
+                for (int q = 0; q < 3; ++q) mC[q] = (T)(mass * pd[(PD_C + 3 * r + q) * cap + s]);
+                const T mv = (T)(mass * pd[(PD_V + r) * cap + s]);
+                rc[(4 + 4 * r) * SM::FS] = mv - tdx * (mC[0] * fr[0] + mC[1] * fr[1] + mC[2] * fr[2]);
+#pragma unroll
+                for (int q = 0; q < 3; ++q) rc[(5 + 4 * r + q) * SM::FS] = tdx * mC[q];
+            }
+        }
+        __syncthreads();
+        scatter_p2g(sm, c0, c1);
+    }
+    __syncthreads();
+    flush_window<4, 1, NPB>(sm.acc, sm.nbr, gm, gmv);
 }
 
 // -------------------------------------------------------------- damage -----
@@ -607,7 +679,10 @@ __global__ void __launch_bounds__(FUSED_THREADS) k_update_fused(const int32_t* _
                 for (int d = 0; d < 3; ++d) bspline_all(fr[d], w[d], dw[d]);
                 const StencilOffsets<L> so(b.x & (L::BX - 1), b.y & (L::BY - 1), b.z & (L::BZ - 1));
                 M3<T> gv;
-                gather_gradient<L, T, TX>(win, so, w, dw, gv.a);
+                if constexpr (sizeof(T) == 4 && sizeof(TX) == 4)
+                    gather_gradient_f32<L>(win, so, w, dw, gv.a);
+                else
+                    gather_gradient<L, T, TX>(win, so, w, dw, gv.a);
                 M3<T> Fn, A = m3_identity<T>();
 #pragma unroll
                 for (int q = 0; q < 9; ++q) {
@@ -699,44 +774,100 @@ int launch_plasticity(Ctx* ctx)
     return ZMPM_OK;
 }
 
-// Three CTAs per SM (at most 168 registers): G2P and P2G are latency bound on
-// FP64 chains, and the third CTA outweighs the few spilled registers (about
-// 1.5% of the 1M-particle substep, same-box A/B).
-template <class L>
+// MIXED: applyPlasticity on an FP32 F.  Von Mises runs in FP32 on its FP32
+// SVD unless the singular values are near inversion (|sigma2| <= 0.2) or
+// strongly stretched (sigma0 >= 5), where it runs in FP64; the other return
+// maps run in FP64.
+__device__ __forceinline__ void apply_return_map_f32(double* __restrict__ pd, int32_t* __restrict__ pi, int64_t cap, int64_t s, M3<float>& F)
+{
+    const int pkind = pi[PI_PKIND * cap + s];
+    if (pkind == ZMPM_PLASTIC_NONE) return;
+    if (pkind == ZMPM_PLASTIC_VON_MISES) {
+        M3<float> U, V;
+        float sg[3];
+        svd3(F, U, sg, V);
+        if (fabsf(sg[2]) > 0.2f && sg[0] < 5.f) {
+            float ys = (float)pd[PD_YS * cap + s];
+            int broken = pi[PI_BROKEN * cap + s];
+            float crack[3] = { (float)pd[(PD_CRACK + 0) * cap + s], (float)pd[(PD_CRACK + 1) * cap + s], (float)pd[(PD_CRACK + 2) * cap + s] };
+            const float ys0 = ys;
+            const int broken0 = broken;
+            von_mises_from_svd<float>((float)pd[PD_MU * cap + s], (float)pd[PD_LAM * cap + s], ys, (float)pd[PD_XI * cap + s],
+                (float)pd[PD_FS * cap + s], broken, crack, F, U, sg, V);
+            if (ys != ys0) pd[PD_YS * cap + s] = ys;
+            if (broken != broken0) {
+                pi[PI_BROKEN * cap + s] = broken;
+#pragma unroll
+                for (int d = 0; d < 3; ++d) pd[(PD_CRACK + d) * cap + s] = crack[d];
+            }
+            return;
+        }
+    }
+    M3<double> Fd = m3_cast<double>(F);
+    apply_return_map(pd, pi, cap, s, Fd);
+    F = m3_cast<float>(Fd);
+}
+
+// gridToParticlesHelper<APIC> (MpmSimulationBase.cpp:906-1016): v_p = sum w v_i,
+// B = sum w v_i (x_i - x_p)^T, C = ((1 + r) B D^-1 + (r - 1) (B D^-1)^T) / 2 with
+// D^-1 = 4 / dx^2, grad v_p = sum v_i grad w^T, x_p += dt v_p and the CFL flag;
+// then evolveStrain F = (I + dt grad v) Fn (FBasedMpmForceHelper.cpp:95-109, and
+// the viscoelastic Fe's relaxation) and, with `plastic`, applyPlasticity.
+// T: the arithmetic (FP32 in MIXED contexts: weights from the stored cell
+// fractions, positions advanced in FP64).  Three CTAs per SM (at most 168
+// registers): the FP64 form is latency bound on FP64 chains.
+template <class L, class T, class TX>
 __global__ void __launch_bounds__(XF_THREADS, 3) k_g2p(const int32_t* __restrict__ group_start, const int32_t* __restrict__ group_nbr,
-    double* __restrict__ pd, int32_t* __restrict__ pi, int64_t cap, const short4* __restrict__ base, double dx, double dt,
-    double apic_rpic_ratio, const double* __restrict__ vnew, int32_t* __restrict__ flags, int mls, int plastic)
+    double* __restrict__ pd, int32_t* __restrict__ pi, int64_t cap, const short4* __restrict__ base, const T* __restrict__ frac, double dx,
+    double dt, double apic_rpic_ratio, const TX* __restrict__ vnew, int32_t* __restrict__ flags, int mls, int plastic)
 {
     constexpr int NPB = L::NPB;
-    __shared__ __align__(128) double win[8 * 3 * NPB];
+    __shared__ __align__(128) TX win[VecWindow<NPB, TX>::ELEMS];
     __shared__ int32_t nbr[8];
     __shared__ __align__(8) uint64_t bar;
     const int g = blockIdx.x;
     if (threadIdx.x < 8) nbr[threadIdx.x] = group_nbr[8 * g + threadIdx.x];
     __syncthreads();
-    stage_window<NPB>(win, vnew, nbr, &bar, flags);
-    const double inv_dx = 1.0 / dx;
-    const double D_inverse = 4.0 / (dx * dx);
-    const double ca = (apic_rpic_ratio + 1) * 0.5, cb = (apic_rpic_ratio - 1) * 0.5;
+    stage_vec_window<NPB, TX>(win, vnew, nbr, &bar, flags);
+    const T inv_dx = T(1.0 / dx), tdx = T(dx);
+    const T D_inverse = T(4.0 / (dx * dx));
+    const T ca = T((apic_rpic_ratio + 1) * 0.5), cb = T((apic_rpic_ratio - 1) * 0.5);
+    const T tdt = T(dt);
     int too_fast = 0;
     const int s0 = group_start[g], s1 = group_start[g + 1];
     for (int s = s0 + threadIdx.x; s < s1; s += blockDim.x) {
         const short4 b = base[s];
-        double xp[3], w[3][3], dwr[3][3];
+        T fr[3], w[3][3], dwr[3][3];
 #pragma unroll
         for (int d = 0; d < 3; ++d) {
-            xp[d] = pd[(PD_X + d) * cap + s];
-            bspline(inv_dx * xp[d] - (double)((&b.x)[d]), w[d], dwr[d]);
+            fr[d] = frac[d * cap + s];
+            bspline(fr[d], w[d], dwr[d]);
         }
         const int lx = b.x & (L::BX - 1), ly = b.y & (L::BY - 1), lz = b.z & (L::BZ - 1);
-        double pv[3] = { 0, 0, 0 };
-        M3<double> Bp = m3_zero<double>(), gv = m3_zero<double>();
-        for_stencil<L>(lx, ly, lz, w, dwr, inv_dx, [&](int t, int e, int i, int j, int k, double wijk, const double* dw) {
-            const double* vv = win + t * 3 * NPB + e;
-            double xi[3] = { (b.x + i) * dx - xp[0], (b.y + j) * dx - xp[1], (b.z + k) * dx - xp[2] };
+        const StencilOffsets<L> so(lx, ly, lz);
+        T pv[3] = { 0, 0, 0 };
+        M3<T> Bp = m3_zero<T>(), gv = m3_zero<T>();
+        double xp[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) xp[d] = pd[(PD_X + d) * cap + s];
+        for_stencil<L>(lx, ly, lz, w, dwr, inv_dx, [&](int, int, int i, int j, int k, T wijk, const T* dw) {
+            TX vv[3];
+            VecWindow<NPB, TX>::node(win, so.X[i] + so.Y[j] + so.Z[k], vv);
+            // x_i - x_p: FP64 from the node and particle positions, FP32 from the cell fractions
+            T xi[3];
+            if constexpr (sizeof(T) == 8) {
+                xi[0] = (b.x + i) * dx - xp[0];
+                xi[1] = (b.y + j) * dx - xp[1];
+                xi[2] = (b.z + k) * dx - xp[2];
+            }
+            else {
+                xi[0] = (T(i) - fr[0]) * tdx;
+                xi[1] = (T(j) - fr[1]) * tdx;
+                xi[2] = (T(k) - fr[2]) * tdx;
+            }
 #pragma unroll
             for (int r = 0; r < 3; ++r) {
-                double vr = vv[r * NPB];
+                const T vr = (T)vv[r];
                 pv[r] += wijk * vr;
 #pragma unroll
                 for (int c = 0; c < 3; ++c) {
@@ -749,7 +880,7 @@ __global__ void __launch_bounds__(XF_THREADS, 3) k_g2p(const int32_t* __restrict
 #pragma unroll
         for (int d = 0; d < 3; ++d) {
             pd[(PD_V + d) * cap + s] = pv[d];
-            double inc = dt * pv[d];
+            const double inc = dt * (double)pv[d];
             pd[(PD_X + d) * cap + s] = xp[d] + inc;
             inc2 += inc * inc;
         }
@@ -758,29 +889,34 @@ __global__ void __launch_bounds__(XF_THREADS, 3) k_g2p(const int32_t* __restrict
         for (int r = 0; r < 3; ++r)
 #pragma unroll
             for (int c = 0; c < 3; ++c) {
-                const double cn = ca * (Bp(r, c) * D_inverse) + cb * (Bp(c, r) * D_inverse);
+                const T cn = ca * (Bp(r, c) * D_inverse) + cb * (Bp(c, r) * D_inverse);
                 pd[(PD_C + 3 * r + c) * cap + s] = cn;
                 if (mls) gv(r, c) = cn; // MLS: gradVp = C_p (MpmSimulationBase.cpp:958-961)
             }
         const int kind = pi[PI_KIND * cap + s];
         if (kind == ZMPM_MODEL_NONE) continue;
         // evolveStrain (FBasedMpmForceHelper.cpp:95-109) on the restored F = Fn
-        M3<double> F0, A = m3_identity<double>();
+        M3<T> F0, A = m3_identity<T>();
 #pragma unroll
         for (int q = 0; q < 9; ++q) {
-            F0.a[q] = pd[(PD_F + q) * cap + s];
-            A.a[q] += dt * gv.a[q];
+            F0.a[q] = (T)pd[(PD_F + q) * cap + s];
+            A.a[q] += tdt * gv.a[q];
         }
-        M3<double> F = m3_mul(A, F0);
-        if (plastic) apply_return_map(pd, pi, cap, s, F);
+        M3<T> F = m3_mul(A, F0);
+        if (plastic) {
+            if constexpr (sizeof(T) == 8)
+                apply_return_map(pd, pi, cap, s, F);
+            else
+                apply_return_map_f32(pd, pi, cap, s, F);
+        }
 #pragma unroll
         for (int q = 0; q < 9; ++q) pd[(PD_F + q) * cap + s] = F.a[q];
         if (pi[PI_VISCO * cap + s]) {
-            // FElasticNonequilibratedBasedMpmForceHelper::evolveStrain (h:62-87)
+            // FElasticNonequilibratedBasedMpmForceHelper::evolveStrain (h:62-87), FP64
             M3<double> Fe;
 #pragma unroll
             for (int q = 0; q < 9; ++q) Fe.a[q] = pd[(PD_FE + q) * cap + s];
-            Fe = m3_mul(A, Fe);
+            Fe = m3_mul(m3_cast<double>(A), Fe);
             viscous_return<double>(pd[PD_VMU * cap + s], pd[PD_VLAM * cap + s], pd[PD_VD * cap + s], pd[PD_VV * cap + s], dt, Fe);
 #pragma unroll
             for (int q = 0; q < 9; ++q) pd[(PD_FE + q) * cap + s] = Fe.a[q];
@@ -796,7 +932,7 @@ static int p2g_impl(Ctx* ctx)
     const int64_t G = ctx->G;
     if (G == 0) return ZMPM_OK;
     if (ctx->mixed)
-        k_p2g_reg<L, float, 2><<<(unsigned)G, XF_THREADS, 0, ctx->stream>>>(ctx->group_start.as<int32_t>(), ctx->group_nbr.as<int32_t>(),
+        k_p2g_fused<L, float, 384><<<(unsigned)G, FUSED_THREADS, 0, ctx->stream>>>(ctx->group_start.as<int32_t>(), ctx->group_nbr.as<int32_t>(),
             ctx->pd.as<double>(), ctx->Pcap, ctx->base.as<short4>(), ctx->cfg.dx, ctx->gm.as<double>(), ctx->gmv.as<double>(), ctx->frac.as<float>());
     else
         k_p2g_reg<L, double, 2><<<(unsigned)G, XF_THREADS, 0, ctx->stream>>>(ctx->group_start.as<int32_t>(), ctx->group_nbr.as<int32_t>(),
@@ -815,11 +951,18 @@ static int update_impl(Ctx* ctx, bool gated)
     const SolverScalars* sc = gated ? ctx->scal.as<SolverScalars>() : nullptr;
     if (ctx->mixed) {
         // FP32 stress and force; inside a solve also the FP64 pair, which runs
-        // instead once the FP32 residual stalled (FP32 Hessian scratch either way)
+        // instead once the FP32 residual stalled (FP32 Hessian scratch either
+        // way).  The FP32 pass gathers from the FP32 copy of vstar, which the
+        // Newton solve keeps current; the hooks and the adjoint set vstar directly.
         const int gate = sc ? 1 : 0;
-        k_update_fused<L, float, double, fused_chunk<float>()><<<(unsigned)G, FUSED_THREADS, 0, ctx->stream>>>(ctx->group_start.as<int32_t>(),
+        if (!sc || !ctx->vstarf_valid) {
+            int rc = refresh_vstar_f32(ctx);
+            if (rc) return rc;
+            ctx->vstarf_valid = true;
+        }
+        k_update_fused<L, float, float, fused_chunk<float>()><<<(unsigned)G, FUSED_THREADS, 0, ctx->stream>>>(ctx->group_start.as<int32_t>(),
             ctx->group_nbr.as<int32_t>(), ctx->pd.as<double>(), ctx->pi.as<int32_t>(), ctx->Pcap, ctx->base.as<short4>(), ctx->cfg.dx, ctx->dt,
-            ctx->frac.as<float>(), ctx->vstar.as<double>(), ctx->scratch.as<float>(), ctx->facc.as<double>(), sc, &dc->flags, gate);
+            ctx->frac.as<float>(), ctx->vstarf.as<float>(), ctx->scratch.as<float>(), ctx->facc.as<double>(), sc, &dc->flags, gate);
         ++g_kernel_launches;
         if (sc) {
             k_stress<L, double, float><<<(unsigned)G, XF_THREADS, 0, ctx->stream>>>(ctx->group_start.as<int32_t>(),
@@ -941,9 +1084,14 @@ static int g2p_impl(Ctx* ctx, bool plastic)
     const int64_t G = ctx->G;
     if (G == 0) return ZMPM_OK;
     DevCounters* dc = ctx->counters.as<DevCounters>();
-    k_g2p<L><<<(unsigned)G, XF_THREADS, 0, ctx->stream>>>(ctx->group_start.as<int32_t>(), ctx->group_nbr.as<int32_t>(), ctx->pd.as<double>(),
-        ctx->pi.as<int32_t>(), ctx->Pcap, ctx->base.as<short4>(), ctx->cfg.dx, ctx->dt, ctx->cfg.apic_rpic_ratio, ctx->vstar.as<double>(), &dc->flags,
-        ctx->mls ? 1 : 0, plastic ? 1 : 0);
+    if (ctx->mixed)
+        k_g2p<L, float, float><<<(unsigned)G, XF_THREADS, 0, ctx->stream>>>(ctx->group_start.as<int32_t>(), ctx->group_nbr.as<int32_t>(),
+            ctx->pd.as<double>(), ctx->pi.as<int32_t>(), ctx->Pcap, ctx->base.as<short4>(), ctx->frac.as<float>(), ctx->cfg.dx, ctx->dt,
+            ctx->cfg.apic_rpic_ratio, ctx->vstarf.as<float>(), &dc->flags, ctx->mls ? 1 : 0, plastic ? 1 : 0);
+    else
+        k_g2p<L, double, double><<<(unsigned)G, XF_THREADS, 0, ctx->stream>>>(ctx->group_start.as<int32_t>(), ctx->group_nbr.as<int32_t>(),
+            ctx->pd.as<double>(), ctx->pi.as<int32_t>(), ctx->Pcap, ctx->base.as<short4>(), ctx->frac.as<double>(), ctx->cfg.dx, ctx->dt,
+            ctx->cfg.apic_rpic_ratio, ctx->vstar.as<double>(), &dc->flags, ctx->mls ? 1 : 0, plastic ? 1 : 0);
     ++g_kernel_launches;
     return ZMPM_OK;
 }
