@@ -152,6 +152,8 @@ def run_workload(args, world, rank):
                 "accuracy_steps": args.warmup + args.steps,
                 "iterations_per_step": [st_mx[-1]["newton_iterations"], st_mx[-1]["krylov_iterations"]],
                 "phase_field_cg_iterations": st_mx[-1].get("phase_field_iterations"),
+                "rankine_first_not_max": st_mx[-1].get("rankine_first_not_max"),
+                "svd_fp64_reevaluations": st_mx[-1].get("svd_fp64_reevaluations"),
                 "gpu_launches": sum(s["kernel_launches"] for s in st_mx), "cpu_baseline": cpu, "clocks": clk}
         print(json.dumps(line), flush=True)
     for s in sims.values():

@@ -96,9 +96,9 @@ enum zmpm_damage {
     /* Rankine ("naive") damage, FractureSimulation::solvePhaseFieldSystemNaive
        (FractureSimulation.h:509-554): principal Cauchy stress of the undegraded
        NeoHookeanBorden stress, c <- min(c, sigma_F / sigma_max) when
-       sigma_max > sigma_F, g = c^2 (1 - k) + k.  sigma_max is the largest
-       principal stress (the reference takes the first eigenvalue in the order
-       of Eigen's general eigen-solver). */
+       sigma_max > sigma_F, g = c^2 (1 - k) + k, with sigma_max the largest
+       principal stress (what the criterion and the variable's name call for;
+       ZMPM_DAMAGE_RANKINE_REFERENCE follows the reference's eigenvalue order). */
     ZMPM_DAMAGE_RANKINE = 1,
     /* CD-MPM phase field, FractureSimulation::solvePhaseFieldSystem
        (FractureSimulation.h:257-456): after P2G, c is solved on the grid from
@@ -109,7 +109,13 @@ enum zmpm_damage {
        positive NeoHookeanBorden energy and g = c^2 (1 - k) + k.  Every particle
        of the scene carries the phase field (the reference indexes it for all
        particles), added by zmpm_add_phase_field. */
-    ZMPM_DAMAGE_PHASE_FIELD = 2
+    ZMPM_DAMAGE_PHASE_FIELD = 2,
+    /* Rankine damage as the reference computes it: sigma_max is
+       cauchy.eigenvalues()[0].real() of Eigen's general eigensolver
+       (FractureSimulation.h:539-543), the first eigenvalue in the order of the
+       real Schur form (Householder-Hessenberg reduction and Francis
+       double-shift QR), which need not be the largest. */
+    ZMPM_DAMAGE_RANKINE_REFERENCE = 3
 };
 
 /* Krylov solver of the Newton step (BackwardEuler.h:82-98). */
@@ -209,6 +215,11 @@ typedef struct zmpm_stats {
     int32_t phase_field_iterations; /* CG iterations of the phase-field solve (its `iterations` return) */
     int32_t fp64_residual;       /* MIXED: 1 if the Newton residual went to FP64 after the FP32 one stalled */
     double phase_field_residual; /* final |r|_2 of the phase-field CG */
+    int64_t rankine_first_not_max; /* ZMPM_DAMAGE_RANKINE_REFERENCE particles whose first eigenvalue
+                                      (the reference's sigma_max) is not the largest one */
+    int64_t svd_fp64_reevaluations; /* MIXED: particle constitutive updates of the Newton solve redone in
+                                       FP64 because their FP32 singular values were near inversion
+                                       (|sigma2| <= 0.2) or strongly stretched (sigma0 >= 5) */
 } zmpm_stats;
 
 /* Result of the binning pass (sortParticlesAndPolluteGrid,

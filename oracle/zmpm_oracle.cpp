@@ -959,8 +959,212 @@ static T sym3_max_eig_jacobi(M3<T> A)
     return std::max(A.a[0][0], std::max(A.a[1][1], A.a[2][2]));
 }
 
+// ---- the first eigenvalue of Eigen's general (real, non-symmetric) eigensolver
+// FractureSimulation.h:539-543 takes sigma_max = cauchy.eigenvalues()[0].real()
+// from Eigen::EigenSolver, i.e. the first diagonal entry (or 2x2 block) of the
+// real Schur form that its RealSchur produces.  Eigen is not part of the
+// reference tree (find_package(Eigen3), version unpinned; 3.3 on the
+// reference's platform), so this restates its published method for a 3x3
+// matrix: scaling by the largest |a_ij|, Householder reduction to upper
+// Hessenberg form, and the Francis double-shift QR iteration of EISPACK hqr /
+// JAMA hqr2 (Golub & Van Loan, Matrix Computations, 7.5) with deflation when a
+// subdiagonal entry falls below eps (|t_kk| + |t_k-1,k-1|), exceptional shifts
+// at iterations 10 and 30 of one eigenvalue, and a 2x2 block with real
+// eigenvalues split by the rotation that keeps each diagonal entry with its
+// nearer eigenvalue.  Returns the real part of the first eigenvalue in that
+// order.  Parity unpinned (no Eigen here); checked by known answers.
+
+// Householder vector of (x0, x1[, x2]) in the form I - tau (1, e)(1, e)^T with
+// (I - tau ...) x = (beta, 0, 0).
+static void householder(const double* x, int n, double& tau, double& beta, double* ess)
+{
+    double tail = 0;
+    for (int i = 1; i < n; ++i) tail += x[i] * x[i];
+    const double c0 = x[0];
+    if (tail <= std::numeric_limits<double>::min()) {
+        tau = 0;
+        beta = c0;
+        for (int i = 1; i < n; ++i) ess[i - 1] = 0;
+        return;
+    }
+    beta = std::sqrt(c0 * c0 + tail);
+    if (c0 >= 0) beta = -beta;
+    for (int i = 1; i < n; ++i) ess[i - 1] = x[i] / (c0 - beta);
+    tau = (beta - c0) / beta;
+}
+// T[r0..r0+n)[c0..c1) <- H T with H = I - tau v v^T, v = (1, ess)
+static void reflect_left(double T[3][3], int r0, int n, int c0, int c1, double tau, const double* ess)
+{
+    for (int c = c0; c < c1; ++c) {
+        double d = T[r0][c];
+        for (int i = 1; i < n; ++i) d += ess[i - 1] * T[r0 + i][c];
+        T[r0][c] -= tau * d;
+        for (int i = 1; i < n; ++i) T[r0 + i][c] -= tau * ess[i - 1] * d;
+    }
+}
+// T[r0..r1)[c0..c0+n) <- T H
+static void reflect_right(double T[3][3], int r0, int r1, int c0, int n, double tau, const double* ess)
+{
+    for (int r = r0; r < r1; ++r) {
+        double d = T[r][c0];
+        for (int i = 1; i < n; ++i) d += ess[i - 1] * T[r][c0 + i];
+        T[r][c0] -= tau * d;
+        for (int i = 1; i < n; ++i) T[r][c0 + i] -= tau * ess[i - 1] * d;
+    }
+}
+
+static double eigen_first_eigenvalue(const double A[3][3])
+{
+    const int n = 3;
+    const double eps = std::numeric_limits<double>::epsilon();
+    double scale = 0;
+    for (int i = 0; i < n; ++i)
+        for (int j = 0; j < n; ++j) scale = std::max(scale, std::fabs(A[i][j]));
+    if (scale < std::numeric_limits<double>::min()) return 0;
+    double T[3][3];
+    for (int i = 0; i < n; ++i)
+        for (int j = 0; j < n; ++j) T[i][j] = A[i][j] / scale;
+    { // Hessenberg: one reflection of column 0 below the subdiagonal
+        double x[2] = { T[1][0], T[2][0] }, tau, beta, ess[1];
+        householder(x, 2, tau, beta, ess);
+        T[1][0] = beta;
+        T[2][0] = 0;
+        reflect_left(T, 1, 2, 1, 3, tau, ess);
+        reflect_right(T, 0, 3, 1, 2, tau, ess);
+    }
+    double norm = 0; // of the upper Hessenberg part
+    for (int j = 0; j < n; ++j)
+        for (int i = 0; i <= std::min(j + 1, n - 1); ++i) norm += std::fabs(T[i][j]);
+    if (norm == 0) return 0;
+    int iu = n - 1, iter = 0, total = 0;
+    double exshift = 0;
+    while (iu >= 0) {
+        int il = iu; // the lowest row of the active block (small subdiagonal above it)
+        while (il > 0) {
+            double s = std::fabs(T[il - 1][il - 1]) + std::fabs(T[il][il]);
+            if (s == 0) s = norm;
+            if (std::fabs(T[il][il - 1]) < eps * s) break;
+            --il;
+        }
+        if (il == iu) { // one eigenvalue
+            T[iu][iu] += exshift;
+            if (iu > 0) T[iu][iu - 1] = 0;
+            --iu;
+            iter = 0;
+        }
+        else if (il == iu - 1) { // a 2x2 block
+            const double p = 0.5 * (T[iu - 1][iu - 1] - T[iu][iu]);
+            const double q = p * p + T[iu][iu - 1] * T[iu - 1][iu];
+            T[iu][iu] += exshift;
+            T[iu - 1][iu - 1] += exshift;
+            if (q >= 0) { // two real eigenvalues: rotate the block upper triangular
+                const double z = std::sqrt(std::fabs(q));
+                const double a = p >= 0 ? p + z : p - z, b = T[iu][iu - 1];
+                const double r = std::hypot(a, b);
+                const double c = r == 0 ? 1.0 : a / r, sn = r == 0 ? 0.0 : b / r;
+                for (int k = iu - 1; k < n; ++k) { // left: rows iu-1, iu
+                    const double t0 = T[iu - 1][k], t1 = T[iu][k];
+                    T[iu - 1][k] = c * t0 + sn * t1;
+                    T[iu][k] = -sn * t0 + c * t1;
+                }
+                for (int k = 0; k <= iu; ++k) { // right: columns iu-1, iu
+                    const double t0 = T[k][iu - 1], t1 = T[k][iu];
+                    T[k][iu - 1] = c * t0 + sn * t1;
+                    T[k][iu] = -sn * t0 + c * t1;
+                }
+                T[iu][iu - 1] = 0;
+            }
+            if (iu > 1) T[iu - 1][iu - 2] = 0;
+            iu -= 2;
+            iter = 0;
+        }
+        else { // Francis double-shift step on rows il..iu
+            double x = T[iu][iu], y = T[iu - 1][iu - 1], w = T[iu][iu - 1] * T[iu - 1][iu];
+            if (iter == 10) { // exceptional shift
+                exshift += x;
+                for (int i = 0; i <= iu; ++i) T[i][i] -= x;
+                const double s = std::fabs(T[iu][iu - 1]) + std::fabs(T[iu - 1][iu - 2]);
+                x = y = 0.75 * s;
+                w = -0.4375 * s * s;
+            }
+            if (iter == 30) {
+                double s = 0.5 * (y - x);
+                s = s * s + w;
+                if (s > 0) {
+                    s = std::sqrt(s);
+                    if (y < x) s = -s;
+                    s = x - w / (0.5 * (y - x) + s);
+                    for (int i = 0; i <= iu; ++i) T[i][i] -= s;
+                    exshift += s;
+                    x = y = w = 0.964;
+                }
+            }
+            ++iter;
+            if (++total > 40 * n) break;
+            int im = iu - 2;
+            double v[3];
+            for (;; --im) {
+                const double tmm = T[im][im], r = x - tmm, s = y - tmm;
+                v[0] = (r * s - w) / T[im + 1][im] + T[im][im + 1];
+                v[1] = T[im + 1][im + 1] - tmm - r - s;
+                v[2] = T[im + 2][im + 1];
+                if (im == il) break;
+                const double lhs = T[im][im - 1] * (std::fabs(v[1]) + std::fabs(v[2]));
+                const double rhs = v[0] * (std::fabs(T[im - 1][im - 1]) + std::fabs(tmm) + std::fabs(T[im + 1][im + 1]));
+                if (std::fabs(lhs) < eps * rhs) break;
+            }
+            for (int k = im; k <= iu - 2; ++k) {
+                const bool first = k == im;
+                if (!first) {
+                    v[0] = T[k][k - 1];
+                    v[1] = T[k + 1][k - 1];
+                    v[2] = T[k + 2][k - 1];
+                }
+                double tau, beta, ess[2];
+                householder(v, 3, tau, beta, ess);
+                if (beta != 0) {
+                    if (first && k > il)
+                        T[k][k - 1] = -T[k][k - 1];
+                    else if (!first)
+                        T[k][k - 1] = beta;
+                    reflect_left(T, k, 3, k, n, tau, ess);
+                    reflect_right(T, 0, std::min(iu, k + 3) + 1, k, 3, tau, ess);
+                }
+            }
+            {
+                double v2[2] = { T[iu - 1][iu - 2], T[iu][iu - 2] }, tau, beta, ess[1];
+                householder(v2, 2, tau, beta, ess);
+                if (beta != 0) {
+                    T[iu - 1][iu - 2] = beta;
+                    reflect_left(T, iu - 1, 2, iu - 1, n, tau, ess);
+                    reflect_right(T, 0, iu + 1, iu - 1, 2, tau, ess);
+                }
+            }
+            for (int i = im + 2; i <= iu; ++i) {
+                T[i][i - 2] = 0;
+                if (i > im + 2) T[i][i - 3] = 0;
+            }
+        }
+    }
+    // EigenSolver: a real eigenvalue where the subdiagonal is zero, else a
+    // complex pair whose real part is the block's mean
+    if (T[1][0] == 0) return T[0][0] * scale;
+    return 0.5 * (T[0][0] + T[1][1]) * scale;
+}
+
+template <class T>
+static T rankine_first_eigenvalue(const M3<T>& A)
+{
+    double a[3][3];
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) a[i][j] = (double)A.a[i][j];
+    return (T)eigen_first_eigenvalue(a);
+}
+
 // FractureSimulation::solvePhaseFieldSystemNaive, FractureSimulation.h:509-554
-// (largest principal Cauchy stress of the undegraded NeoHookeanBorden stress).
+// (principal Cauchy stress of the undegraded NeoHookeanBorden stress): the
+// largest eigenvalue (ZMPM_DAMAGE_RANKINE) or, as the reference computes it,
+// the first eigenvalue of Eigen's general eigensolver (ZMPM_DAMAGE_RANKINE_REFERENCE).
 template <class T>
 static void rankineUpdate(Model<T>& c, Damage<T>& d, const M3<T>& F)
 {
@@ -975,7 +1179,7 @@ static void rankineUpdate(Model<T>& c, Damage<T>& d, const M3<T>& F)
             T dv = (i == j) ? B.a[i][j] - T(1) / 3 * tr : B.a[i][j];
             cauchy.a[i][j] = ((i == j) ? sdev * dv + vol : sdev * dv) / J;
         }
-    T smax = sym3_max_eig_jacobi(cauchy);
+    T smax = d.kind == ZMPM_DAMAGE_RANKINE_REFERENCE ? rankine_first_eigenvalue(cauchy) : sym3_max_eig_jacobi(cauchy);
     T newC = d.c;
     if (smax > d.sigma_f) newC = std::min(d.c, d.sigma_f / smax);
     d.c = newC;
@@ -3000,7 +3204,8 @@ struct Sim {
         // FractureSimulation::particlesToGrid runs the damage update after P2G
 #pragma omp parallel for schedule(static)
         for (int64_t i = 0; i < P; ++i)
-            if (damage[i].kind == ZMPM_DAMAGE_RANKINE && model[i].kind == ZMPM_MODEL_NEOHOOKEAN_BORDEN)
+            if ((damage[i].kind == ZMPM_DAMAGE_RANKINE || damage[i].kind == ZMPM_DAMAGE_RANKINE_REFERENCE) &&
+                model[i].kind == ZMPM_MODEL_NEOHOOKEAN_BORDEN)
                 rankineUpdate(model[i], damage[i], load9(F, i));
         if (anyPhaseField()) solvePhaseField();
         // gridVelocityExplicitUpdate (:818-865)
@@ -3156,7 +3361,8 @@ struct Sim {
         // FractureSimulation::particlesToGrid runs the damage update after P2G
 #pragma omp parallel for schedule(static)
         for (int64_t i = 0; i < P; ++i)
-            if (damage[i].kind == ZMPM_DAMAGE_RANKINE && model[i].kind == ZMPM_MODEL_NEOHOOKEAN_BORDEN)
+            if ((damage[i].kind == ZMPM_DAMAGE_RANKINE || damage[i].kind == ZMPM_DAMAGE_RANKINE_REFERENCE) &&
+                model[i].kind == ZMPM_MODEL_NEOHOOKEAN_BORDEN)
                 rankineUpdate(model[i], damage[i], load9(F, i));
         if (anyPhaseField()) solvePhaseField();
         startBackwardEuler();
@@ -4001,6 +4207,15 @@ int zoracle_svd3(const double* F, double* U, double* sigma, double* V, int32_t f
 }
 
 // Von Mises return map on one F (row-major, in place); returns the new yield stress.
+// The first eigenvalue of Eigen's general eigensolver for a 3x3 matrix (row-major).
+double zoracle_eigen_first_eigenvalue(const double* A)
+{
+    double a[3][3];
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) a[i][j] = A[3 * i + j];
+    return zo::eigen_first_eigenvalue(a);
+}
+
 int zoracle_von_mises(int32_t kind, double E, double nu, double yield_stress, double xi, double* F, double* ys_out)
 {
     zo::Model<double> c;

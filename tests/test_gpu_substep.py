@@ -138,11 +138,14 @@ def test_free_fall_is_exact(cuda_lib):
         np.testing.assert_allclose(p["F"], np.broadcast_to(np.eye(3), p["F"].shape), atol=tol)
 
 
-@pytest.mark.parametrize("precision", ["fp64", "mixed"])
-def test_rankine_damage_matches_oracle(cuda_lib, oracle, precision):
+@pytest.mark.parametrize("precision,axis,reference_order", [("fp64", 0, False), ("mixed", 0, False), ("fp64", 1, True), ("mixed", 1, True),
+                                                             ("fp64", 0, True)])
+def test_rankine_damage_matches_oracle(cuda_lib, oracle, precision, axis, reference_order):
     """NeoHookeanBorden with naive Rankine damage (FractureSimulation.h:509-554):
     a pre-stretched block softens where its principal stress passed sigma_F;
-    phase field c and the degraded dynamics follow the oracle."""
+    phase field c and the degraded dynamics follow the oracle.  With the
+    reference's eigenvalue order (the first eigenvalue of Eigen's general
+    eigensolver) a stretch along y takes sigma_xx, which is not the largest."""
     dx = 1.0 / 64
     sims = [mpm.MpmSimulation(dx, gravity=(0, -9.8, 0), precision=precision, grid_log2=8),
             mpm.MpmSimulation(dx, gravity=(0, -9.8, 0), precision="fp64", lib=oracle)]
@@ -152,10 +155,12 @@ def test_rankine_damage_matches_oracle(cuda_lib, oracle, precision):
         n = x.shape[0]
         stretch = 1.0 + 0.2 * (x[:, 0] - x[:, 0].min()) / np.ptp(x[:, 0])
         F = np.zeros((n, 3, 3))
-        F[:, 0, 0] = stretch
-        F[:, 1, 1] = F[:, 2, 2] = 1.0
+        F[:, 0, 0] = F[:, 1, 1] = F[:, 2, 2] = 1.0
+        F[:, axis, axis] = stretch
         s.setParticles(F=F)
-        h.addRankineDamage(2000.0, residual_phase=0.01)
+        # y-stretch: sigma_xx is negative where the block compresses laterally, so a
+        # lower sigma_F for the reference order still damages part of the block
+        h.addRankineDamage(2000.0 if axis == 0 else 300.0, residual_phase=0.01, reference_order=reference_order)
         s.newton_tolerance = 1e-7
         s.newton_max_iterations = 12
         s.krylov_max_iterations = 60
@@ -165,6 +170,12 @@ def test_rankine_damage_matches_oracle(cuda_lib, oracle, precision):
             assert rc == abi.OK, (k, rc, s.last_stats)
     cg, co = sims[0].getDamage(), sims[1].getDamage()
     assert (co < 1).sum() > 0 and (co == 1).sum() > 0
+    if reference_order:
+        # the substep reports how many particles' first eigenvalue was not the
+        # largest: most of them under the y stretch (the first is sigma_xx), a few
+        # under the x stretch (where the evolved stress is no longer diagonal)
+        nfm, P = sims[0].last_stats["rankine_first_not_max"], sims[0].count
+        assert (nfm > P // 2) if axis == 1 else (nfm < P // 20), (nfm, P)
     pg, po = sims[0].getParticles(), sims[1].getParticles()
     if precision == "fp64":
         np.testing.assert_allclose(cg, co, rtol=1e-9, atol=0)

@@ -191,6 +191,82 @@ def test_rankine_damage_known_answer(oracle):
     assert np.all(c[n // 2:] == 1.0)
 
 
+def _eigen_first(oracle, A):
+    import ctypes as C
+    f = oracle.dll.zoracle_eigen_first_eigenvalue
+    f.restype = C.c_double
+    f.argtypes = [C.POINTER(C.c_double)]
+    A = np.ascontiguousarray(A, dtype=np.float64)
+    return f(A.ctypes.data_as(C.POINTER(C.c_double)))
+
+
+def test_eigen_first_eigenvalue_known_answers(oracle):
+    """The reference's Rankine sigma_max is cauchy.eigenvalues()[0].real() of
+    Eigen's general eigensolver (FractureSimulation.h:539-543): the first entry
+    of the real Schur form.  Known answers of that order: a diagonal matrix is
+    already in Schur form (first = a_00, not the largest); a symmetric 2x2
+    block [[a, b], [b, d]] over a decoupled third row deflates at the bottom
+    and rotates the block so that each diagonal entry keeps its nearer
+    eigenvalue (a < d: the smaller one first); a rotation block gives the real
+    part of its complex pair; any symmetric matrix gives one of its
+    eigenvalues."""
+    assert _eigen_first(oracle, np.diag([1.0, 5.0, 3.0])) == 1.0
+    assert _eigen_first(oracle, np.diag([7.0, -2.0, 3.0])) == 7.0
+    a, b, d = 1.0, 1.0, 2.0
+    lam_minus = 0.5 * (a + d) - np.sqrt(0.25 * (a - d) ** 2 + b * b)
+    lam_plus = 0.5 * (a + d) + np.sqrt(0.25 * (a - d) ** 2 + b * b)
+    A = np.array([[a, b, 0.0], [b, d, 0.0], [0.0, 0.0, 10.0]])
+    assert abs(_eigen_first(oracle, A) - lam_minus) < 1e-14
+    A = np.array([[d, b, 0.0], [b, a, 0.0], [0.0, 0.0, 10.0]])
+    assert abs(_eigen_first(oracle, A) - lam_plus) < 1e-14
+    R = np.array([[0.0, -1.0, 0.0], [1.0, 0.0, 0.0], [0.0, 0.0, 2.0]])
+    assert abs(_eigen_first(oracle, R)) < 1e-15
+    rng = np.random.default_rng(0)
+    first_is_max = 0
+    for _ in range(2000):
+        M = rng.standard_normal((3, 3))
+        A = M + M.T
+        e = np.linalg.eigvalsh(A)
+        v = _eigen_first(oracle, A)
+        assert np.min(np.abs(e - v)) < 1e-12 * np.abs(e).max()
+        first_is_max += abs(v - e.max()) < 1e-12 * np.abs(e).max()
+    # the first eigenvalue is the largest in only part of the cases
+    assert 200 < first_is_max < 1800
+
+
+def test_rankine_reference_order_known_answer(oracle):
+    """With the reference's order a stretch along y (diagonal Cauchy stress)
+    takes sigma_xx, the first diagonal entry, as sigma_max: the particles damage
+    only where sigma_xx passes sigma_F, whereas the largest-eigenvalue rule
+    damages where sigma_yy does."""
+    E, nu, dx = 1e4, 0.3, 1.0 / 64
+    mu, lam = E / (2 * (1 + nu)), E * nu / ((1 + nu) * (1 - 2 * nu))
+    kappa = 0.666666 * mu + lam
+    x = jittered_box(4, dx, (0.4, 0.4, 0.4), 8, seed=3)
+    n = x.shape[0]
+    stretch = np.random.default_rng(5).uniform(0.8, 1.3, n)
+    J = stretch
+    sxx = (mu * J ** (-2.0 / 3.0) * (1.0 - (stretch ** 2 + 2) / 3) + J * kappa / 2 * (J - 1 / J)) / J
+    syy = (mu * J ** (-2.0 / 3.0) * (stretch ** 2 - (stretch ** 2 + 2) / 3) + J * kappa / 2 * (J - 1 / J)) / J
+    sigma_f = float(np.median(np.abs(sxx)))
+    out = {}
+    for ref in (False, True):
+        sim = mpm.MpmSimulation(dx, gravity=(0, 0, 0), precision="fp64", lib=oracle)
+        h = sim.addParticles(x, np.zeros_like(x), 1e-3, dx ** 3 / 8)
+        h.addFBasedMpmForce(mpm.NeoHookeanBorden(E, nu))
+        F = np.zeros((n, 3, 3))
+        F[:, 0, 0] = F[:, 2, 2] = 1.0
+        F[:, 1, 1] = stretch
+        sim.setParticles(F=F)
+        h.addRankineDamage(sigma_f, residual_phase=0.001, reference_order=ref)
+        assert sim.advanceOneTimeStep(1e-4) == abi.OK
+        out[ref] = sim.getDamage()
+    smax = np.maximum(syy, sxx)
+    np.testing.assert_allclose(out[False], np.where(smax > sigma_f, np.minimum(1.0, sigma_f / smax), 1.0), rtol=1e-12)
+    np.testing.assert_allclose(out[True], np.where(sxx > sigma_f, np.minimum(1.0, sigma_f / sxx), 1.0), rtol=1e-12)
+    assert (out[True] != out[False]).sum() > n // 8
+
+
 def _admm_scene(lib, integrator, visco=False, iters=20, precision="fp64", E=2e4, nu=0.4, dx=1.0 / 64, seed=3,
                 grid_log2=None):
     """Slab dropped on a sticky sphere over a sticky ground (the ADMM benchmark's

@@ -31,7 +31,7 @@ NOALLOC_MAX_PARTICLES = 262144
 LAYOUT_AUTO, LAYOUT_244, LAYOUT_444 = 0, 1, 2
 MODEL_NONE, MODEL_NEOHOOKEAN_BORDEN, MODEL_STVK_HENCKY_ISOTROPIC, MODEL_FIXED_COROTATED = 0, 1, 2, 3
 PLASTIC_NONE, PLASTIC_VON_MISES, PLASTIC_DRUCKER_PRAGER, PLASTIC_CAM_CLAY = 0, 1, 2, 3
-DAMAGE_NONE, DAMAGE_RANKINE, DAMAGE_PHASE_FIELD = 0, 1, 2
+DAMAGE_NONE, DAMAGE_RANKINE, DAMAGE_PHASE_FIELD, DAMAGE_RANKINE_REFERENCE = 0, 1, 2, 3
 NEWTON, ADMM, EXPLICIT = 0, 1, 2
 BGEO_POSITION, BGEO_VELOCITY, BGEO_PHASE_FIELD = 0, 1, 2
 MINRES, CG = 0, 1
@@ -112,6 +112,8 @@ class Stats(C.Structure):
         ("phase_field_iterations", C.c_int32),
         ("fp64_residual", C.c_int32),
         ("phase_field_residual", C.c_double),
+        ("rankine_first_not_max", C.c_int64),
+        ("svd_fp64_reevaluations", C.c_int64),
     ]
 
     def as_dict(self):

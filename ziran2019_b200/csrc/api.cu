@@ -128,7 +128,7 @@ int upload(Ctx* ctx)
     for (int64_t i = 0; i < P; ++i) {
         ctx->has_pf |= ctx->hdamage[i] == ZMPM_DAMAGE_PHASE_FIELD;
         ctx->all_pf &= ctx->hdamage[i] == ZMPM_DAMAGE_PHASE_FIELD;
-        ctx->has_damage |= ctx->hdamage[i] == ZMPM_DAMAGE_RANKINE;
+        ctx->has_damage |= ctx->hdamage[i] == ZMPM_DAMAGE_RANKINE || ctx->hdamage[i] == ZMPM_DAMAGE_RANKINE_REFERENCE;
         ctx->has_visco |= ctx->hvisco[i] != 0;
         ctx->all_models &= ctx->hkind[i] != ZMPM_MODEL_NONE;
     }
@@ -675,7 +675,7 @@ int zmpm_get_log_jp(zmpm_ctx* ctx, double* log_jp)
 int zmpm_add_damage(zmpm_ctx* ctx, int64_t lo, int64_t hi, int32_t kind, double sigma_f, double residual_phase)
 {
     if (!ctx || lo < 0 || hi > ctx->P || lo > hi) return ZMPM_BAD_ARG;
-    if (kind != ZMPM_DAMAGE_NONE && kind != ZMPM_DAMAGE_RANKINE) return ZMPM_BAD_ARG;
+    if (kind != ZMPM_DAMAGE_NONE && kind != ZMPM_DAMAGE_RANKINE && kind != ZMPM_DAMAGE_RANKINE_REFERENCE) return ZMPM_BAD_ARG;
     cudaSetDevice(ctx->device);
     int rc = begin_edit(ctx);
     if (rc) return rc;
@@ -1044,6 +1044,8 @@ static int substep_finish(zmpm_ctx* ctx, double dt, const zmpm_solver& s, zmpm_s
     st->phase_field_iterations = ctx->pf_iters;
     st->phase_field_residual = ctx->pf_res;
     st->fp64_residual = hs.fp64_res;
+    st->rankine_first_not_max = hc.first_not_max;
+    st->svd_fp64_reevaluations = hc.svd_fp64;
     if (!admm && !expl) ctx->fp64_res_run = hs.fp64_res ? ctx->fp64_res_run + 1 : 0;
     if (ctx->graph_used && admm) // ADMM iteration: 7 head + 3 tail kernels; Krylov body: operator (2), k_mr_a, k_mr_b
         g_kernel_launches += 10 * (int64_t)hs.nit + 4 * (int64_t)hs.krylov_bodies;

@@ -54,6 +54,8 @@ struct DevCounters {
     int64_t G, B, N;           // groups, pages, active nodes
     int32_t flags;             // FLAG_*
     int32_t pad;
+    int64_t first_not_max;     // Rankine (reference order): particles whose first eigenvalue is not the largest
+    int64_t svd_fp64;          // MIXED: FP32 constitutive updates redone in FP64 (near-degenerate singular values)
 };
 
 // Scalar state of the Newton / Krylov loop, kept on the device so no host

@@ -15,6 +15,7 @@
 //  k_g2p     gridToParticlesHelper<APIC> (MpmSimulationBase.cpp:906-1016) +
 //            evolveStrain + applyPlasticity (:1018-1030)
 #include "admm.cuh"
+#include "eig3.cuh"
 #include "fused.cuh"
 #include "xfer.cuh"
 
@@ -206,12 +207,17 @@ __device__ __forceinline__ double sym3_max_eig(const M3<double>& A)
 // FractureSimulation::solvePhaseFieldSystemNaive (FractureSimulation.h:509-554)
 // for particles with Rankine damage and NeoHookeanBorden: Cauchy stress of the
 // undegraded (g = 1) Kirchhoff stress, c <- min(c, sigma_F / sigma_max) when
-// sigma_max > sigma_F, g = c^2 (1 - k) + k.
-__global__ void k_rankine(double* __restrict__ pd, const int32_t* __restrict__ pi, int64_t cap, int64_t P)
+// sigma_max > sigma_F, g = c^2 (1 - k) + k.  sigma_max: the largest eigenvalue
+// (ZMPM_DAMAGE_RANKINE) or the reference's first eigenvalue of Eigen's general
+// eigensolver (ZMPM_DAMAGE_RANKINE_REFERENCE, eig3.cuh); first_not_max counts
+// the particles of the latter whose first eigenvalue is not the largest.
+__global__ void k_rankine(double* __restrict__ pd, const int32_t* __restrict__ pi, int64_t cap, int64_t P,
+    unsigned long long* __restrict__ first_not_max)
 {
     const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= P) return;
-    if (pi[PI_DAMAGE * cap + s] != ZMPM_DAMAGE_RANKINE || pi[PI_KIND * cap + s] != ZMPM_MODEL_NEOHOOKEAN_BORDEN) return;
+    const int dkind = pi[PI_DAMAGE * cap + s];
+    if ((dkind != ZMPM_DAMAGE_RANKINE && dkind != ZMPM_DAMAGE_RANKINE_REFERENCE) || pi[PI_KIND * cap + s] != ZMPM_MODEL_NEOHOOKEAN_BORDEN) return;
     M3<double> F;
 #pragma unroll
     for (int q = 0; q < 9; ++q) F.a[q] = pd[(PD_F + q) * cap + s];
@@ -230,7 +236,13 @@ __global__ void k_rankine(double* __restrict__ pd, const int32_t* __restrict__ p
             const double dv = (i == j) ? B(i, j) - 1.0 / 3.0 * tr : B(i, j);
             cauchy(i, j) = ((i == j) ? sdev * dv + vol : sdev * dv) / J;
         }
-    const double sigma_max = sym3_max_eig(cauchy);
+    double sigma_max = sym3_max_eig(cauchy);
+    if (dkind == ZMPM_DAMAGE_RANKINE_REFERENCE) {
+        Eig3 eig;
+        const double first = eig.first_eigenvalue(cauchy.a);
+        if (!(fabs(first - sigma_max) <= 1e-9 * fabs(sigma_max))) atomicAdd(first_not_max, 1ull);
+        sigma_max = first;
+    }
     const double sigma_f = pd[PD_SIGMA_F * cap + s];
     double c = pd[PD_PF_C * cap + s];
     const double k = pd[PD_PF_K * cap + s];
@@ -242,7 +254,9 @@ __global__ void k_rankine(double* __restrict__ pd, const int32_t* __restrict__ p
 int launch_damage(Ctx* ctx)
 {
     if (!ctx->has_damage || ctx->P == 0) return ZMPM_OK;
-    k_rankine<<<(unsigned)((ctx->P + 255) / 256), 256, 0, ctx->stream>>>(ctx->pd.as<double>(), ctx->pi.as<int32_t>(), ctx->Pcap, ctx->P);
+    DevCounters* dc = ctx->counters.as<DevCounters>();
+    k_rankine<<<(unsigned)((ctx->P + 255) / 256), 256, 0, ctx->stream>>>(ctx->pd.as<double>(), ctx->pi.as<int32_t>(), ctx->Pcap, ctx->P,
+        reinterpret_cast<unsigned long long*>(&dc->first_not_max));
     ++g_kernel_launches;
     return ZMPM_OK;
 }
@@ -641,7 +655,7 @@ template <class L, class T, class TX, int CH>
 __global__ void __launch_bounds__(FUSED_THREADS) k_update_fused(const int32_t* __restrict__ group_start, const int32_t* __restrict__ group_nbr,
     const double* __restrict__ pd, const int32_t* __restrict__ pi, int64_t cap, const short4* __restrict__ base, double dx, double dt,
     const T* __restrict__ frac, const TX* __restrict__ vstar, T* __restrict__ scr, double* __restrict__ facc,
-    const SolverScalars* __restrict__ sc, int32_t* __restrict__ flags, int gate)
+    const SolverScalars* __restrict__ sc, int32_t* __restrict__ flags, int gate, unsigned long long* __restrict__ svd64)
 {
     if (gated_off(sc, gate)) return;
     constexpr int NPB = L::NPB;
@@ -695,6 +709,7 @@ __global__ void __launch_bounds__(FUSED_THREADS) k_update_fused(const int32_t* _
                 S = model_update<T, T>(kind, mp, (T)V0, m3_mul(A, Fn), Fn, scr, cap, s, sizeof(T) == 4 ? &degenerate : nullptr);
                 if constexpr (sizeof(T) == 4) {
                     if (degenerate) { // FP64 re-evaluation of near-degenerate particles
+                        atomicAdd(svd64, 1ull);
                         M3<double> Fnd, Ad = m3_identity<double>();
 #pragma unroll
                         for (int q = 0; q < 9; ++q) {
@@ -962,7 +977,8 @@ static int update_impl(Ctx* ctx, bool gated)
         }
         k_update_fused<L, float, float, fused_chunk<float>()><<<(unsigned)G, FUSED_THREADS, 0, ctx->stream>>>(ctx->group_start.as<int32_t>(),
             ctx->group_nbr.as<int32_t>(), ctx->pd.as<double>(), ctx->pi.as<int32_t>(), ctx->Pcap, ctx->base.as<short4>(), ctx->cfg.dx, ctx->dt,
-            ctx->frac.as<float>(), ctx->vstarf.as<float>(), ctx->scratch.as<float>(), ctx->facc.as<double>(), sc, &dc->flags, gate);
+            ctx->frac.as<float>(), ctx->vstarf.as<float>(), ctx->scratch.as<float>(), ctx->facc.as<double>(), sc, &dc->flags, gate,
+            reinterpret_cast<unsigned long long*>(&dc->svd_fp64));
         ++g_kernel_launches;
         if (sc) {
             k_stress<L, double, float><<<(unsigned)G, XF_THREADS, 0, ctx->stream>>>(ctx->group_start.as<int32_t>(),
@@ -979,7 +995,8 @@ static int update_impl(Ctx* ctx, bool gated)
     else {
         k_update_fused<L, double, double, fused_chunk<double>()><<<(unsigned)G, FUSED_THREADS, 0, ctx->stream>>>(ctx->group_start.as<int32_t>(),
             ctx->group_nbr.as<int32_t>(), ctx->pd.as<double>(), ctx->pi.as<int32_t>(), ctx->Pcap, ctx->base.as<short4>(), ctx->cfg.dx, ctx->dt,
-            ctx->frac.as<double>(), ctx->vstar.as<double>(), ctx->scratch.as<double>(), ctx->facc.as<double>(), sc, &dc->flags, 0);
+            ctx->frac.as<double>(), ctx->vstar.as<double>(), ctx->scratch.as<double>(), ctx->facc.as<double>(), sc, &dc->flags, 0,
+            reinterpret_cast<unsigned long long*>(&dc->svd_fp64));
         ++g_kernel_launches;
     }
     return ZMPM_OK;

@@ -200,10 +200,14 @@ class MpmParticleHandle:
         lam = np.ascontiguousarray(lam, dtype=np.float64)
         self.sim._call("set_lame", self.lower, self.upper, ptr(mu), ptr(lam))
 
-    def addRankineDamage(self, sigma_f, residual_phase=0.001):
+    def addRankineDamage(self, sigma_f, residual_phase=0.001, reference_order=False):
         """Phase field + Rankine damage (addFBasedMpmForceWithPhaseField with
-        FractureSimulation::useNaiveDamage and sigmaF); needs NeoHookeanBorden."""
-        self.sim._call("add_damage", self.lower, self.upper, abi.DAMAGE_RANKINE, float(sigma_f), float(residual_phase))
+        FractureSimulation::useNaiveDamage and sigmaF); needs NeoHookeanBorden.
+        reference_order: sigma_max is the first eigenvalue of Eigen's general
+        eigensolver, as FractureSimulation.h:539-543 takes it, instead of the
+        largest eigenvalue."""
+        kind = abi.DAMAGE_RANKINE_REFERENCE if reference_order else abi.DAMAGE_RANKINE
+        self.sim._call("add_damage", self.lower, self.upper, kind, float(sigma_f), float(residual_phase))
 
     def addFBasedMpmForceWithPhaseField(self, percentage, l0, model=None, allow_damage=True, residual_phase=0.001):
         """CD-MPM phase field (MpmParticleHandleBase::addFBasedMpmForceWithPhaseField,

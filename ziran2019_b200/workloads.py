@@ -120,13 +120,15 @@ def wl_admm500k(precision, lib=None, layout="auto", scale=1):
                                    "solver": "ADMM 20 iterations, MINRES abs tol 1e-8"}
 
 
-def wl_damage2m(precision, lib=None, layout="auto", scale=1):
+def wl_damage2m(precision, lib=None, layout="auto", scale=1, reference_order=True):
     """Notched slab 1.0 x 0.25 x 0.1 with a 0.1-long, one-cell-wide edge notch at
     mid-length, 8 ppc at dx = 1/216 (216 x 54 x 22 cells, about 2.05M
     particles, seed 4); the end faces are held by sticky boxes moving apart at
     +-0.5 m/s; NeoHookeanBorden E = 1e5, nu = 0.3 with Rankine damage sigma_F =
-    1e3 Pa, k = 1e-3; dt = 2e-4, no gravity.  scale > 1 keeps every scale-th
-    cell layer in z (CPU samples)."""
+    1e3 Pa, k = 1e-3; dt = 2e-4, no gravity.  reference_order: sigma_max is the
+    first eigenvalue of Eigen's general eigensolver, as the reference takes it
+    (default), else the largest.  scale > 1 keeps every scale-th cell layer in
+    z (CPU samples)."""
     from . import abi, mpm
     dx = 1.0 / 216
     nx, ny, nz = 216, 54, max(1, 22 // scale)
@@ -139,7 +141,7 @@ def wl_damage2m(precision, lib=None, layout="auto", scale=1):
     V0 = dx ** 3 / 8
     h = sim.addParticles(x, np.zeros_like(x), 1000.0 * V0, V0)
     h.addFBasedMpmForce(mpm.NeoHookeanBorden(1e5, 0.3))
-    h.addRankineDamage(1e3, residual_phase=1e-3)
+    h.addRankineDamage(1e3, residual_phase=1e-3, reference_order=reference_order)
     hi = lo + np.array([nx, ny, nz]) * dx
     grip = 3 * dx
     for side, vel in ((0, -0.5), (1, 0.5)):
