@@ -34,6 +34,7 @@ from ziran2019_b200 import workloads  # noqa: E402
 METRIC = "implicit MPM substeps/sec at 1M particles, mixed vs FP64 GPU, at <=1e-6 rel err"
 HVP_WORDS = 22  # compulsory words per particle of one Hessian-vector product: X(3), Fn(9), F(9), V0(1)
 HVP_KERNELS = ("k_hvp_fused",)  # the kernel of one Hessian-vector product
+FD_STEPS = (1e-3, 1e-4, 1e-5)  # finite-difference steps of the rollout gradient check, relative to the parameter scale
 
 
 def run_rollout(args, world, rank):
@@ -74,18 +75,21 @@ def run_rollout(args, world, rank):
                   "adjoint_cg_iterations": sum(s["krylov_iterations"] for s in ro.stats),
                   "newton_iterations_last_substep": fwd_newton, "newton_tolerance": sim.newton_tolerance}
         if p == "fp64":
-            fd_err = []
+            # central differences in random directions (alternately of E and of
+            # v0) at three step sizes relative to the parameter's scale
+            fd_err = {h: [] for h in FD_STEPS}
             drng = np.random.default_rng(11)
             for k in range(args.fd_directions):
                 which = "E" if k % 2 == 0 else "v"
                 d = drng.standard_normal(E.shape if which == "E" else v0.shape)
                 scale_ = 1e4 if which == "E" else 0.5
-                h = 1e-4 * scale_
-                Ep, vp = (E + h * d, v0) if which == "E" else (E, v0 + h * d)
-                Em, vm = (E - h * d, v0) if which == "E" else (E, v0 - h * d)
-                fd = (loss_and_grad(ro.run(Ep, vp))[0] - loss_and_grad(ro.run(Em, vm))[0]) / (2 * h)
                 an = float(((gE if which == "E" else gv) * d).sum())
-                fd_err.append(abs(fd - an) / max(abs(an), 1e-300))
+                for hrel in FD_STEPS:
+                    h = hrel * scale_
+                    Ep, vp = (E + h * d, v0) if which == "E" else (E, v0 + h * d)
+                    Em, vm = (E - h * d, v0) if which == "E" else (E, v0 - h * d)
+                    fd = (loss_and_grad(ro.run(Ep, vp))[0] - loss_and_grad(ro.run(Em, vm))[0]) / (2 * h)
+                    fd_err[hrel].append(abs(fd - an) / max(abs(an), 1e-300))
             res[p]["fd_rel_err"] = fd_err
         sim.close()
     r64, rmx = res["fp64"], res["mixed"]
@@ -101,9 +105,11 @@ def run_rollout(args, world, rank):
                 "fp64": {k: r64[k] for k in ("forward_s", "backward_s", "loss", "adjoint_cg_iterations", "newton_iterations_last_substep", "newton_tolerance")},
                 "fp64_value": 1.0 / (r64["forward_s"] + r64["backward_s"]),
                 "grad_rel_err_mixed_vs_fp64": {"E": relE, "v0": relv},
-                "fd_check_fp64": {"directions": args.fd_directions, "h": "1e-4 x (1e4 for E, 0.5 for v0)",
-                                  "max_rel_err": max(r64["fd_rel_err"]) if r64.get("fd_rel_err") else None,
-                                  "rel_err": r64.get("fd_rel_err")}}
+                "fd_check_fp64": {"directions": args.fd_directions, "h": f"{list(FD_STEPS)} x (1e4 for E, 0.5 for v0)",
+                                  "max_rel_err_per_h": {str(h): max(v) for h, v in r64["fd_rel_err"].items()} if args.fd_directions else None,
+                                  "max_rel_err_best_h": max(min(v[k] for v in r64["fd_rel_err"].values()) for k in range(args.fd_directions))
+                                  if args.fd_directions else None,
+                                  "rel_err": {str(h): v for h, v in r64["fd_rel_err"].items()}}}
         print(json.dumps(line), flush=True)
 
 
@@ -423,7 +429,7 @@ def main():
                     help="secondary workloads: the cut used for CPU samples, on the GPU too (profiling runs)")
     ap.add_argument("--workload", default="config1", choices=["config1"] + sorted(WORKLOADS),
                     help="config1: the headline 1M-particle workload; others print their own line")
-    ap.add_argument("--fd-directions", type=int, default=4, help="finite-difference directions of the rollout gradient check")
+    ap.add_argument("--fd-directions", type=int, default=16, help="finite-difference directions of the rollout gradient check")
     ap.add_argument("--rollout-mixed-tol", type=float, default=1e-12, help="Newton tolerance of the mixed rollout forward")
     ap.add_argument("--ncu-csv", default=None,
                     help="ncu CSV (dram__bytes_read.sum, dram__bytes_write.sum) of the product kernels of this workload: "

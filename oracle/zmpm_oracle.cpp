@@ -891,6 +891,53 @@ static void vonMisesProject(const Model<T>& c, Plastic<T>& p, M3<T>& F)
     }
 }
 
+// Reverse mode of vonMisesProject with a constant yield stress (xi = 0): F =
+// Pi(Fp) = U diag(f(sigma)) V^T with f_i = exp(tr(eps)/3 + r n_i), r =
+// yield / (2 mu), n the unit deviatoric Hencky strain, an isotropic map of Fp.
+// Given Gb = dL/dF returns dL/dFp and adds dL/dE (r ~ 1/E at fixed nu) to gE.
+// The derivative of an isotropic matrix function: with A = U^T dFp V the
+// output's U^T dF V has diagonal J diag(A) (J = df/dsigma) and off-diagonal
+// entries (f_i - f_j)/(s_i - s_j) sym(A)_ij + (f_i + f_j)/(s_i + s_j) skew(A)_ij;
+// its transpose swaps J for J^T and keeps the off-diagonal part.
+template <class T>
+static M3<T> vonMisesAdjoint(const Model<T>& c, const Plastic<T>& p, const M3<T>& Fp, const M3<T>& Gb, T& gE)
+{
+    M3<T> U, V;
+    T s[3];
+    svd3(Fp, U, s, V);
+    T eps[3];
+    for (int d = 0; d < 3; ++d) eps[d] = std::log(std::max(s[d], T(1e-4)));
+    const T tr = eps[0] + eps[1] + eps[2];
+    T hat[3];
+    for (int d = 0; d < 3; ++d) hat[d] = eps[d] - tr / T(3);
+    const T hn = std::sqrt(hat[0] * hat[0] + hat[1] * hat[1] + hat[2] * hat[2]);
+    const T r = p.yield_stress / (2 * c.mu);
+    if (!(hn - r > 0)) return Gb;
+    T n[3], f[3], J[3][3];
+    for (int d = 0; d < 3; ++d) {
+        n[d] = hat[d] / hn;
+        f[d] = std::exp(tr / 3 + r * n[d]);
+    }
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) {
+            // d eps_j / d s_j = 1/s_j; d n_i / d eps_j = (delta_ij - 1/3 - n_i n_j) / |hat|
+            T dn = (T(i == j) - T(1) / 3 - n[i] * n[j]) / hn;
+            J[i][j] = s[j] > T(1e-4) ? f[i] * (T(1) / 3 + r * dn) / s[j] : T(0);
+        }
+    M3<T> A = mul(Tmul(U, Gb), V), Ab;
+    for (int j = 0; j < 3; ++j) Ab.a[j][j] = J[0][j] * A.a[0][0] + J[1][j] * A.a[1][1] + J[2][j] * A.a[2][2];
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) {
+            if (i == j) continue;
+            T a = std::fabs(s[i] - s[j]) > T(1e-12) * std::fabs(s[0]) ? (f[i] - f[j]) / (s[i] - s[j]) : J[i][i] - J[i][j];
+            T b = (f[i] + f[j]) / (s[i] + s[j]);
+            Ab.a[i][j] = a * (A.a[i][j] + A.a[j][i]) / 2 + b * (A.a[i][j] - A.a[j][i]) / 2;
+        }
+    const T E = c.mu * (3 * c.lambda + 2 * c.mu) / (c.lambda + c.mu);
+    gE += -(r / E) * (A.a[0][0] * f[0] * n[0] + A.a[1][1] * f[1] * n[1] + A.a[2][2] * f[2] * n[2]);
+    return mulT(mul(U, Ab), V);
+}
+
 // ---------------------------------------------------------------- damage --
 template <class T>
 struct Damage {
@@ -2376,11 +2423,13 @@ struct Sim {
     int adjointSubstep(double dt_in, const zmpm_solver& s, double tol, double* gx, double* gv, double* gC, double* gF, double* gE,
         zmpm_stats& st)
     {
-        for (int64_t i = 0; i < P; ++i)
-            if (plastic[i].kind != ZMPM_PLASTIC_NONE || damage[i].kind != ZMPM_DAMAGE_NONE || visco[i].on) {
-                err = "the adjoint supports elastic particles only";
+        for (int64_t i = 0; i < P; ++i) {
+            const bool vm = plastic[i].kind == ZMPM_PLASTIC_VON_MISES && plastic[i].xi == 0 && model[i].kind == ZMPM_MODEL_STVK_HENCKY_ISOTROPIC;
+            if ((plastic[i].kind != ZMPM_PLASTIC_NONE && !vm) || damage[i].kind != ZMPM_DAMAGE_NONE || visco[i].on) {
+                err = "the adjoint supports elastic particles and von Mises (StvkWithHenckyIsotropic, xi = 0) only";
                 return ZMPM_UNSUPPORTED;
             }
+        }
         if (s.integrator != ZMPM_NEWTON) {
             err = "the adjoint differentiates the Newton substep";
             return ZMPM_UNSUPPORTED;
@@ -2417,9 +2466,21 @@ struct Sim {
                 xb[d] = in3(gx, i, d);
             }
             M3<T> Cb = in9(gC, i), Fb = in9(gF, i), Fn_ = load9(F0, i);
+            Spline<T> sp(xp, dx);
+            if (plastic[i].kind == ZMPM_PLASTIC_VON_MISES) {
+                // the projection's input Fp = (I + dt grad v*) Fn
+                M3<T> Ap = M3<T>::identity();
+                iterateKernel2(sp, base_offset[i], [&](const int*, T, const T* dw, const T (*)[3], G& g) {
+                    if (g.idx < 0) return;
+                    for (int r = 0; r < 3; ++r)
+                        for (int c = 0; c < 3; ++c) Ap.a[r][c] += dtt * vstar[3 * g.idx + r] * dw[c];
+                });
+                T gEp = 0;
+                Fb = vonMisesAdjoint(model[i], plastic[i], mul(Ap, Fn_), Fb, gEp);
+                if (gE) gE[i] += (double)gEp;
+            }
             M3<T> FnFbT = mulT(Fn_, Fb); // Fn gF^T
             M3<T> gvs = M3<T>::zero();
-            Spline<T> sp(xp, dx);
             iterateKernel2(sp, base_offset[i], [&](const int node[3], T w, const T* dw, const T H[3][3], G& g) {
                 const int64_t id = g.idx;
                 if (id < 0) return;

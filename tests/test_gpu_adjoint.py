@@ -147,3 +147,63 @@ def test_gpu_rollout_finite_differences(cuda_lib):
         fd = (com_loss(ro.run(*args_p), m, target)[0] - com_loss(ro.run(*args_m), m, target)[0]) / (2 * h)
         an = float(((gE if which == "E" else gv) * d).sum())
         assert abs(fd - an) <= 1e-5 * abs(an) + 1e-14, (which, fd, an)
+
+
+def test_gpu_plastic_rollout_matches_oracle_and_finite_differences(cuda_lib, oracle):
+    """The adjoint through the von Mises return map (xi = 0) on the GPU: a
+    rollout whose particles yield, against the oracle's adjoint and against
+    central differences of the GPU's own forward rollout."""
+    from ziran2019_b200.rollout import Rollout
+    from tests.test_rollout_adjoint import NU, com_loss, plastic_scene
+    target = np.array([0.5, 0.2, 0.45])
+    out = []
+    for lib, kw in ((None, {}), (oracle, {})):
+        s, E, v0, m = plastic_scene(lib, n=3)
+        ro = Rollout(s, NU, 1e-3, 6, checkpoint_every=3)
+        X = ro.run(E, v0)
+        _, gX = com_loss(X, m, target)
+        out.append((X,) + ro.backward(gX) + (ro, s, E, v0, m))
+    assert rel(out[0][0], out[1][0]) < 1e-11
+    assert rel(out[0][1], out[1][1]) < 1e-6
+    assert rel(out[0][2], out[1][2]) < 1e-6
+    _, gE, gv, ro, s, E, v0, m = out[0]
+    rng = np.random.default_rng(4)
+    for which, h in (("E", 1.0), ("v", 1e-6)):
+        d = rng.standard_normal(E.shape if which == "E" else v0.shape)
+        args_p = (E + h * d, v0) if which == "E" else (E, v0 + h * d)
+        args_m = (E - h * d, v0) if which == "E" else (E, v0 - h * d)
+        fd = (com_loss(ro.run(*args_p), m, target)[0] - com_loss(ro.run(*args_m), m, target)[0]) / (2 * h)
+        an = float(((gE if which == "E" else gv) * d).sum())
+        assert abs(fd - an) <= 1e-5 * abs(an) + 1e-14, (which, fd, an)
+
+
+def test_torch_autograd_wrapper_over_cuda_library(cuda_lib):
+    """DifferentiableRollout (the torch.autograd.Function over the C ABI) on
+    the CUDA library: a loss written in torch backpropagates to E and v0, and
+    the gradients equal the rollout's own reverse sweep and central
+    differences of the forward."""
+    import torch
+
+    from ziran2019_b200.rollout import DifferentiableRollout, Rollout
+    from tests.test_rollout_adjoint import NU, com_loss, scene
+    s, E, v0, m = scene(None, n=4, grid_log2=8)
+    ro = Rollout(s, NU, 1e-3, 8, checkpoint_every=4)
+    dev = "cuda"
+    Et = torch.tensor(E, device=dev, requires_grad=True)
+    vt = torch.tensor(v0, device=dev, requires_grad=True)
+    target = torch.tensor([0.5, 0.2, 0.45], dtype=torch.float64, device=dev)
+    X = DifferentiableRollout.apply(Et, vt, ro)
+    assert X.device.type == "cuda" and X.shape == (s.count, 3)
+    mt = torch.tensor(m, device=dev)
+    loss = (((mt[:, None] * X).sum(0) / mt.sum() - target) ** 2).sum()
+    loss.backward()
+    _, gX = com_loss(X.detach().cpu().numpy(), m, target.cpu().numpy())
+    gE, gv = ro.backward(gX)
+    np.testing.assert_allclose(Et.grad.cpu().numpy(), gE, rtol=1e-10)
+    np.testing.assert_allclose(vt.grad.cpu().numpy(), gv, rtol=1e-10)
+    rng = np.random.default_rng(8)
+    d = rng.standard_normal(v0.shape)
+    h = 1e-5
+    fd = (com_loss(ro.run(E, v0 + h * d), m, target.cpu().numpy())[0] - com_loss(ro.run(E, v0 - h * d), m, target.cpu().numpy())[0]) / (2 * h)
+    an = float((vt.grad.cpu().numpy() * d).sum())
+    assert abs(fd - an) <= 1e-5 * abs(an) + 1e-14, (fd, an)

@@ -61,10 +61,14 @@ __device__ __forceinline__ M3<double> ld9(const double* __restrict__ a, int64_t 
 } // namespace
 
 // ---------------------------------------------------------------- G2P -----
+// With von Mises plasticity the G2P output is F' = Pi((I + dt grad v*) Fn), so
+// dL/dF of the projection's input replaces dL/dF' first (von_mises_adjoint),
+// and the yield radius' dependence on E starts dL/dE (AJ_OE; k_adj_particle
+// adds the force term's).
 template <class L>
 __global__ void __launch_bounds__(XF_THREADS) k_adj_g2p(const int32_t* __restrict__ group_start, const int32_t* __restrict__ group_nbr,
-    double* __restrict__ aj, int64_t cap, const short4* __restrict__ base, double dx, double dt, const double* __restrict__ vstar,
-    double* __restrict__ vsbar, int32_t* __restrict__ flags)
+    const double* __restrict__ pd, const int32_t* __restrict__ pi, double* __restrict__ aj, int64_t cap, const short4* __restrict__ base,
+    double dx, double dt, const double* __restrict__ vstar, double* __restrict__ vsbar, int32_t* __restrict__ flags)
 {
     constexpr int NPB = L::NPB;
     __shared__ __align__(128) double win[8 * 3 * NPB];
@@ -97,10 +101,27 @@ __global__ void __launch_bounds__(XF_THREADS) k_adj_g2p(const int32_t* __restric
             xb[d] = aj[(AJ_GX + d) * cap + s];
             vt[d] = aj[(AJ_GV + d) * cap + s] + dt * xb[d];
         }
-        const M3<double> Cb = ld9(aj, cap, AJ_GC, s), Fb = ld9(aj, cap, AJ_GF, s), Fn = ld9(aj, cap, AJ_F0, s);
+        const M3<double> Cb = ld9(aj, cap, AJ_GC, s), Fn = ld9(aj, cap, AJ_F0, s);
+        M3<double> Fb = ld9(aj, cap, AJ_GF, s);
+        const int lx = b.x & (L::BX - 1), ly = b.y & (L::BY - 1), lz = b.z & (L::BZ - 1);
+        double gE = 0;
+        if (pi[PI_PKIND * cap + s] == ZMPM_PLASTIC_VON_MISES && pi[PI_KIND * cap + s] != ZMPM_MODEL_NONE) {
+            // the projection's input F' = (I + dt grad v*) Fn
+            M3<double> A = m3_identity<double>();
+            for_stencil<L>(lx, ly, lz, w, dwr, inv_dx, [&](int t, int e, int, int, int, double, const double* dw) {
+                const double* vv = win + t * 3 * NPB + e;
+#pragma unroll
+                for (int rr = 0; rr < 3; ++rr)
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) A(rr, c) += dt * vv[rr * NPB] * dw[c];
+            });
+            const double mu = pd[PD_MU * cap + s], lm = pd[PD_LAM * cap + s];
+            const double E = mu * (3 * lm + 2 * mu) / (lm + mu);
+            Fb = von_mises_adjoint<double>(mu, pd[PD_YS * cap + s], E, m3_mul(A, Fn), Fb, &gE);
+        }
+        aj[AJ_OE * cap + s] = gE;
         const M3<double> FbFnT = m3_mulT(Fb, Fn), FnFbT = m3_mulT(Fn, Fb);
         M3<double> gvs = m3_zero<double>();
-        const int lx = b.x & (L::BX - 1), ly = b.y & (L::BY - 1), lz = b.z & (L::BZ - 1);
         for_stencil_h<L>(lx, ly, lz, w, dwr, inv_dx, [&](int t, int e, int i, int j, int k, double wt, const double* dw, const double (*H)[3]) {
             const double* vv = win + t * 3 * NPB + e;
             const double v[3] = { vv[0], vv[NPB], vv[2 * NPB] };
@@ -259,7 +280,7 @@ __global__ void __launch_bounds__(XF_THREADS) k_adj_particle(const int32_t* __re
             aj[(int64_t)(AJ_OC + k2) * cap + s] = Cb.a[k2];
             aj[(int64_t)(AJ_OF + k2) * cap + s] = Fb.a[k2];
         }
-        aj[AJ_OE * cap + s] = gE;
+        aj[AJ_OE * cap + s] += gE;
     }
 }
 
@@ -270,10 +291,12 @@ int launch_adj_g2p(Ctx* ctx, double* vsbar)
     DevCounters* dc = ctx->counters.as<DevCounters>();
     if (ctx->layout == 1)
         k_adj_g2p<Layout244><<<(unsigned)ctx->G, XF_THREADS, 0, ctx->stream>>>(ctx->group_start.as<int32_t>(), ctx->group_nbr.as<int32_t>(),
-            ctx->adj.as<double>(), ctx->Pcap, ctx->base.as<short4>(), ctx->cfg.dx, ctx->dt, ctx->vstar.as<double>(), vsbar, &dc->flags);
+            ctx->pd.as<double>(), ctx->pi.as<int32_t>(), ctx->adj.as<double>(), ctx->Pcap, ctx->base.as<short4>(), ctx->cfg.dx, ctx->dt,
+            ctx->vstar.as<double>(), vsbar, &dc->flags);
     else
         k_adj_g2p<Layout444><<<(unsigned)ctx->G, XF_THREADS, 0, ctx->stream>>>(ctx->group_start.as<int32_t>(), ctx->group_nbr.as<int32_t>(),
-            ctx->adj.as<double>(), ctx->Pcap, ctx->base.as<short4>(), ctx->cfg.dx, ctx->dt, ctx->vstar.as<double>(), vsbar, &dc->flags);
+            ctx->pd.as<double>(), ctx->pi.as<int32_t>(), ctx->adj.as<double>(), ctx->Pcap, ctx->base.as<short4>(), ctx->cfg.dx, ctx->dt,
+            ctx->vstar.as<double>(), vsbar, &dc->flags);
     ++g_kernel_launches;
     return ZMPM_OK;
 }

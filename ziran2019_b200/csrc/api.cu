@@ -1175,11 +1175,16 @@ int zmpm_adjoint_substep(zmpm_ctx* ctx, double dt, const zmpm_solver* s, double 
         return ZMPM_UNSUPPORTED;
     }
     ctx->mls = false;
-    for (int64_t i = 0; i < ctx->P; ++i)
-        if (ctx->hpkind[i] != ZMPM_PLASTIC_NONE || ctx->hdamage[i] != ZMPM_DAMAGE_NONE || ctx->hvisco[i]) {
-            ctx->err = "the adjoint supports elastic particles only";
+    for (int64_t i = 0; i < ctx->P; ++i) {
+        // von Mises with a constant yield stress (xi = 0) has an adjoint; hardening
+        // would need the yield stress as adjoint state, the other return maps,
+        // damage and the viscoelastic strain have none
+        const bool vm = ctx->hpkind[i] == ZMPM_PLASTIC_VON_MISES && ctx->hxi[i] == 0.0 && ctx->hkind[i] == ZMPM_MODEL_STVK_HENCKY_ISOTROPIC;
+        if ((ctx->hpkind[i] != ZMPM_PLASTIC_NONE && !vm) || ctx->hdamage[i] != ZMPM_DAMAGE_NONE || ctx->hvisco[i]) {
+            ctx->err = "the adjoint supports elastic particles and von Mises (StvkWithHenckyIsotropic, xi = 0) only";
             return ZMPM_UNSUPPORTED;
         }
+    }
     cudaSetDevice(ctx->device);
     zmpm_stats local;
     if (!st) st = &local;

@@ -277,6 +277,67 @@ ZMPM_D void von_mises_project(T mu, T lambda, T& yield_stress, T xi, T fail_stre
     von_mises_from_svd(mu, lambda, yield_stress, xi, fail_stress, broken, crack, F, U, sg, V);
 }
 
+// Adjoint of von_mises_project (perfect plasticity, xi = 0) at the trial
+// strain Fp: given Gb = dL/dF of the projected F, returns dL/dFp, and adds
+// dL/dE to *gE (the yield radius r = yield_stress / (2 mu) scales as 1/E at
+// fixed Poisson ratio).  Inside the yield surface the map is the identity.
+// Outside, the projected singular values are f_i = exp(tr(eps)/3 + r n_i)
+// with eps_i = log max(sigma_i, 1e-4) and n the unit deviatoric direction, an
+// isotropic function of Fp: with A = U^T Gb V the adjoint is
+// U Abar V^T, Abar_jj = sum_i (df_i/dsigma_j) A_ii and, off the diagonal,
+// (f_i - f_j)/(sigma_i - sigma_j) on the symmetric part and (f_i + f_j) /
+// (sigma_i + sigma_j) on the antisymmetric part of A (both self-adjoint; the
+// first taken at its limit for equal singular values).  The map is not
+// differentiable on the yield surface itself (dgamma = 0).
+template <class T>
+ZMPM_D M3<T> von_mises_adjoint(T mu, T yield_stress, T E, const M3<T>& Fp, const M3<T>& Gb, T* gE)
+{
+    M3<T> U, V;
+    T sg[3];
+    svd3(Fp, U, sg, V);
+    T e[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) e[d] = log(sg[d] > T(1e-4) ? sg[d] : T(1e-4));
+    const T tr = e[0] + e[1] + e[2];
+    T h[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) h[d] = e[d] - tr / T(3);
+    const T hn = sqrt(h[0] * h[0] + h[1] * h[1] + h[2] * h[2]);
+    const T r = yield_stress / (T(2) * mu);
+    if (!(hn - r > T(0))) return Gb;
+    T n[3], f[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        n[d] = h[d] / hn;
+        f[d] = exp(tr / T(3) + r * n[d]);
+    }
+    T J[3][3]; // df_i / dsigma_j
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            const T dn = ((i == j ? T(1) : T(0)) - T(1) / T(3) - n[i] * n[j]) / hn;
+            J[i][j] = sg[j] > T(1e-4) ? f[i] * (T(1) / T(3) + r * dn) / sg[j] : T(0);
+        }
+    const M3<T> A = m3_mul(m3_Tmul(U, Gb), V);
+    M3<T> Ab;
+#pragma unroll
+    for (int j = 0; j < 3; ++j) Ab(j, j) = J[0][j] * A(0, 0) + J[1][j] * A(1, 1) + J[2][j] * A(2, 2);
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            if (i == j) continue;
+            const T ds = sg[i] - sg[j];
+            const T a = fabs(ds) > T(1e-12) * fabs(sg[0]) ? (f[i] - f[j]) / ds : J[i][i] - J[i][j];
+            const T b = (f[i] + f[j]) / (sg[i] + sg[j]);
+            Ab(i, j) = a * (A(i, j) + A(j, i)) / T(2) + b * (A(i, j) - A(j, i)) / T(2);
+        }
+    // dL/dr = sum_i A_ii f_i n_i, dr/dE = -r / E
+    *gE += -(r / E) * (A(0, 0) * f[0] * n[0] + A(1, 1) * f[1] * n[1] + A(2, 2) * f[2] * n[2]);
+    return m3_mulT(m3_mul(U, Ab), V);
+}
+
 // DruckerPragerStvkHencky::projectStrain (PlasticityApplier.cpp:272-317):
 // Hencky strain of the SVD less the cohesion; the trace with log Jp >= 0 sends
 // F to the cone tip exp(cohesion) U V^T (and, with the volume correction, the
