@@ -377,6 +377,13 @@ int zmpm_apply_plasticity(zmpm_ctx* ctx);
 /* The CUDA stream (cudaStream_t) every kernel of this context runs on, so a
    caller can order its own work or CUDA events against the substep. */
 int zmpm_get_stream(zmpm_ctx* ctx, void** stream);
+/* Polls of a grid-wide barrier of the persistent Krylov kernel before the wait
+   gives up (0: the default, 2^22, about a second).  A wait that gives up makes
+   every CTA of the kernel return and the substep report ZMPM_TIMEOUT; the
+   context stays usable.  (The reference runs on one host thread and has no
+   device waits.) */
+int zmpm_set_spin_limit(zmpm_ctx* ctx, int64_t polls);
+
 /* on != 0: bracket each Hessian-vector product with CUDA events and report
    their summed device time in zmpm_stats.ms_hvp (the reference's ZIRAN_TIMER
    scopes, Lib/Ziran/CS/Util/Timer.h:34-58, as device timers). */

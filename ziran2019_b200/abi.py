@@ -188,6 +188,7 @@ _PRODUCT_ONLY = {
     "backward_euler_step": (C.c_int, [C.c_void_p, C.POINTER(Stats)]),
     "grid_to_particles": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(Stats)]),
     "apply_plasticity": (C.c_int, [C.c_void_p]),
+    "set_spin_limit": (C.c_int, [C.c_void_p, C.c_int64]),
 }
 
 

@@ -454,6 +454,7 @@ int zmpm_create(const zmpm_config* cfg, zmpm_ctx** out)
     if ((e = cudaMemset(ctx->page_first.p, 0x7f, ctx->table_size * sizeof(int32_t))) != cudaSuccess) return fail(e);
     if ((e = ctx->counters.ensure(sizeof(DevCounters))) != cudaSuccess) return fail(e);
     if ((e = ctx->scal.ensure(sizeof(SolverScalars))) != cudaSuccess) return fail(e);
+    if ((e = ctx->gsync.ensure(sizeof(GridSync))) != cudaSuccess) return fail(e);
     if ((e = ctx->red.ensure(RED_N * RED_MAX_CTAS * sizeof(double))) != cudaSuccess) return fail(e);
     // two collider states: at t, and at t + dt for the explicit substep's trial collision
     if ((e = ctx->dcolliders.ensure(2 * MAX_COLLIDERS * sizeof(DevCollider))) != cudaSuccess) return fail(e);
@@ -475,7 +476,7 @@ int zmpm_destroy(zmpm_ctx* ctx)
         &ctx->group_page, &ctx->group_nbr, &ctx->emit_flag, &ctx->emit_scan, &ctx->page_first, &ctx->page_block, &ctx->block_page,
         &ctx->block_index, &ctx->gm, &ctx->gmv, &ctx->vn, &ctx->dv, &ctx->vstar, &ctx->facc, &ctx->res, &ctx->proj, &ctx->collided,
         &ctx->node_idx, &ctx->red, &ctx->scal, &ctx->counters, &ctx->dcolliders, &ctx->adm_F, &ctx->adm_gvn, &ctx->adm_B, &ctx->adm_pre,
-        &ctx->adm_rhs, &ctx->adm_w, &ctx->adj, &ctx->kvf, &ctx->vstarf, &ctx->pfn, &ctx->pfsc };
+        &ctx->adm_rhs, &ctx->adm_w, &ctx->adj, &ctx->kvf, &ctx->vstarf, &ctx->pfn, &ctx->pfsc, &ctx->gsync };
     for (DBuf* b : bufs) b->release();
     for (auto& b : ctx->kv) b.release();
     for (auto* v : { &ctx->ckpt_pd, &ctx->ckpt_pi, &ctx->ckpt_sid })
@@ -848,6 +849,13 @@ int zmpm_get_stream(zmpm_ctx* ctx, void** stream)
     return ZMPM_OK;
 }
 
+int zmpm_set_spin_limit(zmpm_ctx* ctx, int64_t polls)
+{
+    if (!ctx || polls < 0) return ZMPM_BAD_ARG;
+    ctx->spin_limit = polls == 0 ? (1ll << 22) : polls;
+    return ZMPM_OK;
+}
+
 int zmpm_set_profiling(zmpm_ctx* ctx, int32_t on)
 {
     if (!ctx) return ZMPM_BAD_ARG;
@@ -903,18 +911,21 @@ static int delete_phase_field_particles(zmpm_ctx* ctx)
     return launch_phase_field_delete(ctx);
 }
 
-// Kernels of one Newton Krylov-loop body: the Hessian product (1 or 2), then
-// k_mr_a + k_mr_b (MINRES) or k_apply_A_krylov + k_cg_b + k_cg_c (CG).
-static int64_t krylov_body_launches(const zmpm_ctx* ctx, const zmpm_solver& s)
-{
-    return 2 + (s.linear_solver == ZMPM_MINRES ? 2 : 3);
-}
+// Kernels of one Newton Krylov-loop body: MINRES runs the Hessian product,
+// k_mr_a and k_mr_b per iteration; CG runs its whole solve in one persistent
+// kernel (counted with the Newton body).
+static int64_t krylov_body_launches(const zmpm_ctx*, const zmpm_solver& s) { return s.linear_solver == ZMPM_MINRES ? 3 : 0; }
 
 // Kernels of one Newton loop body outside the Krylov loop: stress and force
 // (MIXED: an FP32 and an FP64 pair, one of which returns at once), residual
 // with the Krylov start vectors, Newton check with the Krylov start, step,
 // advance.
-static int64_t newton_body_launches(const zmpm_ctx* ctx) { return ctx->mixed ? 8 : 6; }
+static int64_t newton_body_launches(const zmpm_ctx* ctx, const zmpm_solver& s)
+{
+    // update (MIXED: the FP32 pass and the gated FP64 pair), residual, Newton
+    // check, step, advance; CG adds its persistent solve
+    return (ctx->mixed ? 7 : 5) + (s.linear_solver == ZMPM_MINRES ? 0 : 1);
+}
 
 static int begin_implicit_impl(zmpm_ctx* ctx, double dt, bool damage = true)
 {
@@ -1050,7 +1061,7 @@ static int substep_finish(zmpm_ctx* ctx, double dt, const zmpm_solver& s, zmpm_s
     if (ctx->graph_used && admm) // ADMM iteration: 7 head + 3 tail kernels; Krylov body: operator (2), k_mr_a, k_mr_b
         g_kernel_launches += 10 * (int64_t)hs.nit + 4 * (int64_t)hs.krylov_bodies;
     else if (ctx->graph_used)
-        g_kernel_launches += newton_body_launches(ctx) * (int64_t)hs.nit + krylov_body_launches(ctx, s) * (int64_t)hs.krylov_bodies;
+        g_kernel_launches += newton_body_launches(ctx, s) * (int64_t)hs.nit + krylov_body_launches(ctx, s) * (int64_t)hs.krylov_bodies;
     ctx->graph_used = false;
     st->kernel_launches = (int32_t)(g_kernel_launches - launches0);
     ctx->N = hc.N;
@@ -1235,7 +1246,7 @@ int zmpm_adjoint_substep(zmpm_ctx* ctx, double dt, const zmpm_solver* s, double 
         ctx->graph_exec = nullptr;
     }
     if (ctx->graph_used)
-        g_kernel_launches += newton_body_launches(ctx) * (int64_t)hs.nit + krylov_body_launches(ctx, *s) * (int64_t)hs.krylov_bodies;
+        g_kernel_launches += newton_body_launches(ctx, *s) * (int64_t)hs.nit + krylov_body_launches(ctx, *s) * (int64_t)hs.krylov_bodies;
     st->newton_iterations = hs.newton_iters;
     st->newton_converged = hs.converged;
     st->fp64_residual = hs.fp64_res;

@@ -120,20 +120,27 @@ struct VecWindow<NPB, double> {
     }
 };
 
-// Stages the 8 page slabs of `vec` for the window; all threads call it.
+// Stages the 8 page slabs of `vec` for the window; all threads call it.  The
+// mbarrier is initialised once per kernel (by the caller, or here when
+// `phase` < 0); a CTA that stages several windows in turn waits on the
+// alternating phase parity.
 template <int NPB, class TX>
-__device__ __forceinline__ void stage_vec_window(TX* win, const TX* __restrict__ vec, const int32_t* nbr, uint64_t* bar, int32_t* flags)
+__device__ __forceinline__ void stage_vec_window(TX* win, const TX* __restrict__ vec, const int32_t* nbr, uint64_t* bar, int32_t* flags,
+    int phase = -1)
 {
     using W = VecWindow<NPB, TX>;
     static_assert(W::SLAB % 16 == 0, "bulk copies move multiples of 16 bytes");
     if (threadIdx.x == 0) {
-        mbar_init(bar, 1);
+        if (phase < 0)
+            mbar_init(bar, 1);
+        else // a persistent kernel: order the vector's generic-proxy writes (other CTAs, before a grid barrier) before the bulk reads
+            asm volatile("fence.proxy.async.global;" ::: "memory");
         mbar_expect_tx(bar, 8 * W::SLAB);
 #pragma unroll
         for (int t = 0; t < 8; ++t) bulk_g2s(win + t * W::PAGE, vec + (int64_t)nbr[t] * W::PAGE, W::SLAB, bar);
     }
     __syncthreads();
-    mbar_wait_bounded(bar, 0, flags);
+    mbar_wait_bounded(bar, phase < 0 ? 0u : (uint32_t)(phase & 1), flags);
 }
 
 // G(r, c) = sum over the 27 stencil nodes of x_r(node) d_c w(node) * dx (the

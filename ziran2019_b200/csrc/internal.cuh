@@ -89,6 +89,15 @@ struct SolverScalars {
 };
 enum MinresSlot { MR_GC0, MR_GS0, MR_GC1, MR_GS1, MR_GC2, MR_GS2, MR_RHS0, MR_RHS1, MR_BETA_KP1 };
 
+// State of the bounded grid-wide barrier of a persistent (cooperative) kernel,
+// zeroed before each launch.
+struct GridSync {
+    unsigned count;  // CTAs arrived at the current barrier
+    unsigned gen;    // barriers completed
+    unsigned work;   // next particle group of the running product
+    unsigned abort;  // 1 once a CTA's wait gave up
+};
+
 // Field indices of the particle pools.
 // Fields from PD_CORE on (phase-field state, then viscoelastic strain and ADMM
 // state) are moved by the binning permutation only once a context uses them
@@ -212,6 +221,9 @@ struct Ctx {
     std::vector<double> ckpt_time;
     std::vector<int64_t> ckpt_P;
     bool admm_used = false;               // the last substep ran ADMM (launch accounting)
+    DBuf gsync;                           // GridSync of the persistent Krylov kernel
+    int coop_blocks = 0;                  // its cooperative grid size (all CTAs co-resident)
+    long long spin_limit = 1ll << 22;     // polls before a grid-barrier wait gives up (zmpm_set_spin_limit)
     // substep phases: 1 after zmpm_particles_to_grid, 2 after zmpm_backward_euler_step
     int phase = 0;
     zmpm_solver phase_solver{};

@@ -19,6 +19,7 @@
 // (MpmSimulationBase.cpp:617-623) and the collision projection.
 #include <algorithm>
 
+#include "hvp.cuh"
 #include "internal.cuh"
 #include "mat3.cuh"
 #include "node.cuh"
@@ -581,15 +582,6 @@ __global__ void __launch_bounds__(ND_THREADS) k_apply_A(NodeGeom ng, const doubl
     apply_A_body<NPB, false>(ng, gm, col, P6, dt2, xin, hacc, out, nullptr, 0);
 }
 
-// CG operator pass: tmp = project(A p), partial tmp . p.
-template <int NPB>
-__global__ void __launch_bounds__(ND_THREADS) k_apply_A_krylov(NodeGeom ng, const double* __restrict__ gm, const int8_t* __restrict__ col,
-    const double* __restrict__ P6, double dt2, KrylovBufs kb, double* __restrict__ part, const SolverScalars* __restrict__ sc)
-{
-    if (krylov_off(sc)) return;
-    apply_A_body<NPB, true>(ng, gm, col, P6, dt2, kb.p, kb.hacc, kb.tmp, part, 1);
-}
-
 // Ends a Krylov iteration (the next loop top's test, Minres.h:100,
 // ConjugateGradient.h:118): advances k, stops on the local tolerance or the
 // iteration cap; as a graph, sets the loop condition.  Run by one thread of
@@ -638,60 +630,6 @@ __device__ __forceinline__ MrPending mr_pending(const KrylovBufs& kb, const Solv
 __device__ __forceinline__ double mr_direction(const MrPending& p, int64_t i)
 {
     return (mr_norm(p.z[i], p.beta) - p.delta * p.m1[i] - p.eps * p.m2[i]) / p.gamma;
-}
-
-// ---------------------------------------------------------------- CG ------
-// x += alpha p; r -= alpha tmp; q = r/m; partial q.r.  The CG kernels skip
-// massless slots, which hold zeros in every vector from the solve's start.
-template <int NPB>
-__global__ void __launch_bounds__(ND_THREADS) k_cg_b(NodeGeom ng, const double* __restrict__ gm, KrylovBufs kb, const double* __restrict__ part_in,
-    double* __restrict__ part_out, const SolverScalars* __restrict__ sc)
-{
-    if (krylov_off(sc)) return;
-    const int it = sc->kit;
-    const double alpha = sc->mr[it & 1][0] / reduce_partials(part_in, ng.parts);
-    double acc = 0;
-    for (int64_t n = (int64_t)blockIdx.x * ND_THREADS + threadIdx.x; n < ng.nn; n += (int64_t)gridDim.x * ND_THREADS) {
-        const double m = gm[n];
-        if (m == 0) continue;
-        for (int k = 0; k < 3; ++k) {
-            int64_t i = vidx<NPB>(n, k);
-            kb.x[i] += kb.p[i] * alpha;
-            double r = kb.r[i] - kb.tmp[i] * alpha;
-            kb.r[i] = r;
-            double q = r / kb.pre[n];
-            kb.q[i] = q;
-            acc += q * r;
-        }
-    }
-    double s = block_sum(acc);
-    if (threadIdx.x == 0) part_out[blockIdx.x] = s;
-}
-
-// beta, p = q + beta p, residual norm; the last CTA ends the iteration.
-template <int NPB>
-__global__ void __launch_bounds__(ND_THREADS) k_cg_c(NodeGeom ng, const double* __restrict__ gm, KrylovBufs kb, const double* __restrict__ part_in,
-    SolverScalars* __restrict__ sc, int kmax, cudaGraphConditionalHandle hK, int use_graph)
-{
-    if (krylov_off(sc)) return;
-    const int it = sc->kit, nit = sc->nit;
-    const double zTrk = reduce_partials(part_in, ng.parts);
-    const double beta = zTrk / sc->mr[it & 1][0];
-    const double rnorm = sqrt(zTrk);
-    for (int64_t n = (int64_t)blockIdx.x * ND_THREADS + threadIdx.x; n < ng.nn; n += (int64_t)gridDim.x * ND_THREADS) {
-        if (gm[n] == 0) continue;
-        for (int k = 0; k < 3; ++k) {
-            int64_t i = vidx<NPB>(n, k);
-            kb.p[i] = kb.q[i] + beta * kb.p[i];
-        }
-    }
-    if (!last_cta(&sc->ticket) || threadIdx.x != 0) return;
-    sc->mr[(it + 1) & 1][0] = zTrk;
-    sc->rnorm = rnorm;
-    sc->krylov_iters += 1;
-    sc->hvp_count += 1;
-    if (nit < 64) sc->kcount[nit] += 1;
-    krylov_advance(sc, it, rnorm, kmax, hK, use_graph);
 }
 
 // ------------------------------------------------------------- MINRES -----
@@ -827,6 +765,188 @@ __global__ void __launch_bounds__(ND_THREADS) k_mr_b(NodeGeom ng, const double* 
     krylov_advance(sc, it, rnorm, kmax, hK, use_graph);
 }
 
+// ------------------------------------------------ persistent Krylov -----
+// One cooperative launch runs a whole linear solve of the Newton iteration
+// (ConjugateGradient::solve, ConjugateGradient.h:99-147, on the Newton
+// operator): per iteration the Hessian-vector product of p (hvp_group over
+// the particle groups, taken in turn from a shared counter), A p with its
+// partial dot, the x / r / q update with its partial dot and p = q + beta p,
+// separated by grid-wide barriers.  Every CTA reduces the per-CTA partials in
+// the same fixed order, so all hold bit-identical scalars and take the same
+// loop decision.  The barrier waits are bounded: a CTA that gives up raises
+// FLAG_TIMEOUT and the abort flag, and every CTA returns at its next barrier.
+
+// Block sum for FUSED_THREADS threads; the result in every thread.
+__device__ __forceinline__ double block_sum_fused(double v)
+{
+    __shared__ double ws[FUSED_THREADS / 32];
+    v = warp_sum(v);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    __syncthreads();
+    if (lane == 0) ws[w] = v;
+    __syncthreads();
+    double t = 0;
+#pragma unroll
+    for (int i = 0; i < FUSED_THREADS / 32; ++i) t += ws[i];
+    return t;
+}
+// Sum of n partials written by other CTAs of this kernel (read through L2), in
+// a fixed order identical in every CTA.
+__device__ __forceinline__ double reduce_partials_fused(const double* part, int n)
+{
+    double s = 0;
+    for (int i = threadIdx.x; i < n; i += FUSED_THREADS) s += __ldcg(part + i);
+    return block_sum_fused(s);
+}
+
+// Bounded grid-wide barrier (sense by generation count).  Returns false in
+// every thread of the CTA when this CTA gave up after `limit` polls or another
+// CTA did; the caller then returns.
+__device__ __forceinline__ bool grid_sync(GridSync* gs, long long limit, int32_t* flags)
+{
+    __shared__ int ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        volatile unsigned* vgen = &gs->gen;
+        volatile unsigned* vabort = &gs->abort;
+        int good = 1;
+        const unsigned g = *vgen;
+        __threadfence();
+        if (atomicAdd(&gs->count, 1u) == gridDim.x - 1) {
+            gs->count = 0;
+            __threadfence();
+            atomicAdd(&gs->gen, 1u);
+        }
+        else {
+            long long it = 0;
+            while (*vgen == g) {
+                if (*vabort) {
+                    good = 0;
+                    break;
+                }
+                if (++it > limit) {
+                    atomicOr(flags, (int32_t)FLAG_TIMEOUT);
+                    atomicExch(&gs->abort, 1u);
+                    good = 0;
+                    break;
+                }
+            }
+        }
+        __threadfence();
+        if (*vabort) good = 0;
+        ok = good;
+    }
+    __syncthreads();
+    return ok != 0;
+}
+
+struct HvpArgs {
+    const int32_t *group_start, *group_nbr, *pi;
+    const short4* base;
+    const void *frac, *scr; // in the product's precision
+    int64_t cap;
+    double dx;
+    int G;
+};
+
+template <class L, class T>
+__global__ void __launch_bounds__(FUSED_THREADS) k_cg_persistent(NodeGeom ng, HvpArgs ha, const double* __restrict__ gm,
+    const int8_t* __restrict__ col, const double* __restrict__ P6, double dt2, KrylovBufs kb, double* __restrict__ part_a,
+    double* __restrict__ part_b, SolverScalars* __restrict__ sc, int kmax, GridSync* __restrict__ gs, long long limit, int32_t* __restrict__ flags)
+{
+    if (sc->newton_done || !sc->kactive) return;
+    constexpr int NPB = L::NPB;
+    constexpr int CH = sizeof(T) == 4 ? 512 : 192;
+    __shared__ HvpSmem<L, T, double, CH> hs;
+    __shared__ int gsh;
+    if (threadIdx.x == 0) mbar_init(&hs.bar, 1);
+    __syncthreads();
+    int phase = 0;
+    const int nit = sc->nit;
+    int k = sc->kit;
+    double zTr = sc->mr[k & 1][0];
+    const double local_tol = sc->local_tol;
+    const int64_t t0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x, nt = (int64_t)gridDim.x * blockDim.x;
+    for (;;) {
+        // the Hessian-vector product of p into hacc
+        for (;;) {
+            if (threadIdx.x == 0) gsh = atomicAdd(&gs->work, 1);
+            __syncthreads();
+            const int g = gsh;
+            if (g >= ha.G) break;
+            hvp_group<L, T, double, CH>(hs, g, ha.group_start, ha.group_nbr, ha.pi, ha.cap, ha.base, ha.dx, static_cast<const T*>(ha.frac),
+                static_cast<const T*>(ha.scr), kb.p, kb.hacc, flags, phase++);
+        }
+        if (!grid_sync(gs, limit, flags)) return;
+        if (blockIdx.x == 0 && threadIdx.x == 0) gs->work = 0; // read again only after two more barriers
+        // tmp = project(m p + dt^2 hacc), hacc = 0; partial p . tmp (BackwardEuler.h:322-351)
+        double acc = 0;
+        for (int64_t n = t0; n < ng.nn; n += nt) {
+            const double m = gm[n];
+            if (m == 0) continue;
+            double o[3], pv[3];
+            for (int c = 0; c < 3; ++c) {
+                const int64_t i = vidx<NPB>(n, c);
+                pv[c] = kb.p[i];
+                o[c] = m * pv[c] + dt2 * kb.hacc[i];
+                kb.hacc[i] = 0;
+            }
+            project3(col, P6, ng.nn, n, o);
+            for (int c = 0; c < 3; ++c) {
+                kb.tmp[vidx<NPB>(n, c)] = o[c];
+                acc += o[c] * pv[c];
+            }
+        }
+        acc = block_sum_fused(acc);
+        if (threadIdx.x == 0) part_a[blockIdx.x] = acc;
+        if (!grid_sync(gs, limit, flags)) return;
+        // x += alpha p; r -= alpha tmp; q = r / m; partial q . r
+        const double alpha = zTr / reduce_partials_fused(part_a, gridDim.x);
+        acc = 0;
+        for (int64_t n = t0; n < ng.nn; n += nt) {
+            const double m = gm[n];
+            if (m == 0) continue;
+            for (int c = 0; c < 3; ++c) {
+                const int64_t i = vidx<NPB>(n, c);
+                kb.x[i] += kb.p[i] * alpha;
+                const double r = kb.r[i] - kb.tmp[i] * alpha;
+                kb.r[i] = r;
+                const double q = r / kb.pre[n];
+                kb.q[i] = q;
+                acc += q * r;
+            }
+        }
+        acc = block_sum_fused(acc);
+        if (threadIdx.x == 0) part_b[blockIdx.x] = acc;
+        if (!grid_sync(gs, limit, flags)) return;
+        // beta, p = q + beta p; the loop test of the next iteration
+        const double zTr1 = reduce_partials_fused(part_b, gridDim.x);
+        const double beta = zTr1 / zTr, rnorm = sqrt(zTr1);
+        for (int64_t n = t0; n < ng.nn; n += nt) {
+            if (gm[n] == 0) continue;
+            for (int c = 0; c < 3; ++c) {
+                const int64_t i = vidx<NPB>(n, c);
+                kb.p[i] = kb.q[i] + beta * kb.p[i];
+            }
+        }
+        ++k;
+        zTr = zTr1;
+        const bool go = !(rnorm < local_tol || k >= kmax);
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+            sc->mr[k & 1][0] = zTr1;
+            sc->rnorm = rnorm;
+            sc->krylov_iters += 1;
+            sc->hvp_count += 1;
+            sc->krylov_bodies += 1;
+            if (nit < 64) sc->kcount[nit] += 1;
+            sc->kit = k;
+            if (!go) sc->kactive = 0;
+        }
+        if (!go) return;
+        if (!grid_sync(gs, limit, flags)) return; // p complete before the next product
+    }
+}
+
 // dv += x (the linear solve's step, with MINRES's deferred last update);
 // vstar = vn + dv on active nodes.
 template <int NPB>
@@ -864,8 +984,9 @@ __global__ void __launch_bounds__(ND_THREADS) k_vstar_f32(NodeGeom ng, const dou
 
 // Ends a Newton iteration (NewtonsMethod.h:46 loop); as a graph, sets the
 // Newton loop condition.
-__global__ void k_newton_advance(SolverScalars* __restrict__ sc, int nmax, cudaGraphConditionalHandle hN, int use_graph)
+__global__ void k_newton_advance(SolverScalars* __restrict__ sc, int nmax, cudaGraphConditionalHandle hN, int use_graph, GridSync* __restrict__ gs)
 {
+    if (gs) *gs = GridSync{}; // the next persistent solve starts from a clean barrier
     if (!sc->newton_done) sc->newton_iters += 1;
     const int n = sc->nit + 1;
     sc->nit = n;
@@ -1212,32 +1333,22 @@ int launch_newton_head(const NewtonLaunch& L, cudaStream_t st, cudaGraphConditio
     return ZMPM_OK;
 }
 
-// One Krylov iteration: Hessian-vector product, A x, and the solver updates.
+// One MINRES iteration: Hessian-vector product, the operator pass and the
+// Lanczos / Givens step (CG runs its whole solve in k_cg_persistent).
 template <int NPB>
 int launch_krylov_iteration(const NewtonLaunch& L, cudaStream_t st, cudaGraphConditionalHandle hK, int use_graph, cudaEvent_t e0, cudaEvent_t e1)
 {
     Ctx* ctx = L.ctx;
     if (e0) ZMPM_CUDA(cudaEventRecord(e0, st));
-    if (L.np.minres && L.kb.Zf[0])
+    if (L.kb.Zf[0])
         launch_hvp_krylov_f32(ctx, L.kb.Zf[0], L.kb.Zf[1], L.kb.hacc);
-    else if (L.np.minres)
-        launch_hvp_krylov(ctx, L.kb.Z[0], L.kb.Z[1], true, L.kb.hacc);
     else
-        launch_hvp_krylov(ctx, L.kb.p, L.kb.p, false, L.kb.hacc);
+        launch_hvp_krylov(ctx, L.kb.Z[0], L.kb.Z[1], true, L.kb.hacc);
     if (e1) ZMPM_CUDA(cudaEventRecord(e1, st));
-    if (L.np.minres) {
-        k_mr_a<NPB><<<L.nb, ND_THREADS, 0, st>>>(L.ng, ctx->gm.as<double>(), ctx->collided.as<int8_t>(), ctx->proj.as<double>(), L.dt2, L.kb,
-            L.pA, L.sc);
-        k_mr_b<NPB><<<L.nb, ND_THREADS, 0, st>>>(L.ng, ctx->gm.as<double>(), L.kb, L.pA, L.pC, L.sc, L.np.kmax, hK, use_graph);
-        g_kernel_launches += 2;
-    }
-    else {
-        k_apply_A_krylov<NPB><<<L.nb, ND_THREADS, 0, st>>>(L.ng, ctx->gm.as<double>(), ctx->collided.as<int8_t>(), ctx->proj.as<double>(), L.dt2,
-            L.kb, L.pA, L.sc);
-        k_cg_b<NPB><<<L.nb, ND_THREADS, 0, st>>>(L.ng, ctx->gm.as<double>(), L.kb, L.pA, L.pC, L.sc);
-        k_cg_c<NPB><<<L.nb, ND_THREADS, 0, st>>>(L.ng, ctx->gm.as<double>(), L.kb, L.pC, L.sc, L.np.kmax, hK, use_graph);
-        g_kernel_launches += 3;
-    }
+    k_mr_a<NPB><<<L.nb, ND_THREADS, 0, st>>>(L.ng, ctx->gm.as<double>(), ctx->collided.as<int8_t>(), ctx->proj.as<double>(), L.dt2, L.kb, L.pA,
+        L.sc);
+    k_mr_b<NPB><<<L.nb, ND_THREADS, 0, st>>>(L.ng, ctx->gm.as<double>(), L.kb, L.pA, L.pC, L.sc, L.np.kmax, hK, use_graph);
+    g_kernel_launches += 2;
     return ZMPM_OK;
 }
 
@@ -1247,9 +1358,59 @@ int launch_newton_tail(const NewtonLaunch& L, cudaStream_t st, cudaGraphConditio
     Ctx* ctx = L.ctx;
     k_newton_step<NPB><<<L.nb, ND_THREADS, 0, st>>>(L.ng, ctx->gm.as<double>(), L.kb, L.np.minres, ctx->vn.as<double>(), ctx->dv.as<double>(),
         ctx->vstar.as<double>(), L.sc, ctx->mixed ? ctx->vstarf.as<float4>() : nullptr);
-    k_newton_advance<<<1, 1, 0, st>>>(L.sc, L.np.nmax, hN, use_graph);
+    k_newton_advance<<<1, 1, 0, st>>>(L.sc, L.np.nmax, hN, use_graph, L.np.minres ? nullptr : L.ctx->gsync.as<GridSync>());
     g_kernel_launches += 2;
     return ZMPM_OK;
+}
+
+// The persistent CG solve (k_cg_persistent) as one cooperative launch of as
+// many CTAs as fit on the device at once (all co-resident, which the grid
+// barrier needs; the launch fails rather than oversubscribes).  GridSync must
+// be zero.
+template <int NPB>
+int launch_cg_persistent(const NewtonLaunch& L, cudaStream_t st)
+{
+    Ctx* ctx = L.ctx;
+    using Lay = typename std::conditional<NPB == 32, Layout244, Layout444>::type;
+    HvpArgs ha;
+    ha.group_start = ctx->group_start.as<int32_t>();
+    ha.group_nbr = ctx->group_nbr.as<int32_t>();
+    ha.pi = ctx->pi.as<int32_t>();
+    ha.base = ctx->base.as<short4>();
+    ha.frac = ctx->frac.p;
+    ha.scr = ctx->scratch.p;
+    ha.cap = ctx->Pcap;
+    ha.dx = ctx->cfg.dx;
+    ha.G = (int)ctx->G;
+    DevCounters* dc = ctx->counters.as<DevCounters>();
+    auto launch = [&](auto kern) -> int {
+        if (ctx->coop_blocks <= 0) {
+            int per_sm = 0, sms = 0;
+            ZMPM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, FUSED_THREADS, 0));
+            ZMPM_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device));
+            ctx->coop_blocks = std::min(per_sm * sms, RED_MAX_CTAS);
+            if (ctx->coop_blocks <= 0) {
+                ctx->err = "the persistent Krylov kernel does not fit on this device";
+                return ZMPM_CUDA_ERROR;
+            }
+        }
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3((unsigned)ctx->coop_blocks);
+        cfg.blockDim = dim3(FUSED_THREADS);
+        cfg.stream = st;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeCooperative;
+        attr[0].val.cooperative = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        ZMPM_CUDA(cudaLaunchKernelEx(&cfg, kern, L.ng, ha, (const double*)ctx->gm.as<double>(), (const int8_t*)ctx->collided.as<int8_t>(),
+            (const double*)ctx->proj.as<double>(), L.dt2, L.kb, L.pA, L.pC, L.sc, L.np.kmax, ctx->gsync.as<GridSync>(), ctx->spin_limit,
+            &dc->flags));
+        ++g_kernel_launches;
+        return ZMPM_OK;
+    };
+    if (ctx->mixed) return launch(k_cg_persistent<Lay, float>);
+    return launch(k_cg_persistent<Lay, double>);
 }
 
 #define ZMPM_CAP(expr)                                                                                                 \
@@ -1330,10 +1491,55 @@ int loop_graph(Ctx* ctx, Head&& head, Body&& body, Tail&& tail, cudaGraphExec_t*
     return ZMPM_OK;
 }
 
+// A solver loop as one CUDA graph: WHILE(outer){ body(st, hN) }, its
+// condition set on the device.
+template <class Body>
+int while_graph(Ctx* ctx, Body&& body, cudaGraphExec_t* exec_out)
+{
+    cudaStream_t st = ctx->stream;
+    cudaGraph_t g = nullptr;
+    ZMPM_CAP(cudaGraphCreate(&g, 0));
+    cudaGraphConditionalHandle hN;
+    ZMPM_CAP(cudaGraphConditionalHandleCreate(&hN, g, 1, cudaGraphCondAssignDefault));
+    cudaGraphNodeParams pN = {};
+    pN.type = cudaGraphNodeTypeConditional;
+    pN.conditional.handle = hN;
+    pN.conditional.type = cudaGraphCondTypeWhile;
+    pN.conditional.size = 1;
+    cudaGraphNode_t nN;
+    ZMPM_CAP(cudaGraphAddNode(&nN, g, nullptr, 0, &pN));
+    ZMPM_CAP(cudaStreamBeginCaptureToGraph(st, pN.conditional.phGraph_out[0], nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    int rc = body(st, hN);
+    cudaGraph_t tmp = nullptr;
+    ZMPM_CAP(cudaStreamEndCapture(st, &tmp));
+    if (rc) {
+        cudaGraphDestroy(g);
+        return rc;
+    }
+    ZMPM_CAP(cudaGraphInstantiate(exec_out, g, 0));
+    cudaGraphDestroy(g);
+    return ZMPM_OK;
+}
+
+// One Newton iteration with the CG solve as one persistent kernel: update,
+// residual and Krylov start, Newton check, the solve, step and advance.
+template <int NPB>
+int launch_newton_iteration_cg(const NewtonLaunch& L, cudaStream_t st, cudaGraphConditionalHandle hN, int use_graph)
+{
+    int rc = launch_newton_head<NPB>(L, st, 0, 0);
+    if (rc) return rc;
+    rc = launch_cg_persistent<NPB>(L, st);
+    if (rc) return rc;
+    return launch_newton_tail<NPB>(L, st, hN, use_graph);
+}
+
 // The Newton solve as one graph.
 template <int NPB>
 int newton_graph(const NewtonLaunch& L, cudaGraphExec_t* exec_out)
 {
+    if (!L.np.minres)
+        return while_graph(L.ctx, [&](cudaStream_t st, cudaGraphConditionalHandle hN) { return launch_newton_iteration_cg<NPB>(L, st, hN, 1); },
+            exec_out);
     return loop_graph(
         L.ctx, [&](cudaStream_t st, cudaGraphConditionalHandle hK) { return launch_newton_head<NPB>(L, st, hK, 1); },
         [&](cudaStream_t st, cudaGraphConditionalHandle hK) { return launch_krylov_iteration<NPB>(L, st, hK, 1, nullptr, nullptr); },
@@ -1391,7 +1597,9 @@ static int newton_impl(Ctx* ctx, const zmpm_solver& s)
     ctx->prof_newton = 0;
     ctx->graph_used = false;
     if (L.ng.nn == 0 || s.newton_max_iterations == 0) return ZMPM_OK;
-    const bool prof = ctx->profiling && s.newton_max_iterations <= 64;
+    if (!L.np.minres) ZMPM_CUDA(cudaMemsetAsync(ctx->gsync.p, 0, sizeof(GridSync), st));
+    // profiling (per-product events) applies to MINRES, whose products are separate launches
+    const bool prof = ctx->profiling && s.newton_max_iterations <= 64 && L.np.minres;
     if (!prof) {
         // whole solve as one graph with device-side loop conditions
         cudaGraphExec_t exec = nullptr;
@@ -1633,62 +1841,21 @@ int run_adjoint_solve(Ctx* ctx, double tol, int max_iterations)
     cudaStream_t st = ctx->stream;
     ZMPM_CUDA(cudaMemsetAsync(Lc.sc, 0, sizeof(SolverScalars), st));
     if (Lc.ng.nn == 0) return ZMPM_OK;
-    const bool l244 = ctx->layout == 1;
-    auto head = [&](cudaStream_t sm, cudaGraphConditionalHandle hK, int ug) {
-        if (l244) {
-            k_adj_cg_init<32><<<Lc.nb, ND_THREADS, 0, sm>>>(Lc.ng, ctx->gm.as<double>(), ctx->collided.as<int8_t>(), ctx->proj.as<double>(),
-                ctx->res.as<double>(), kb, tol, Lc.pB, Lc.sc);
-            k_krylov_start<32><<<1, ND_THREADS, 0, sm>>>(Lc.ng, kb, Lc.np, Lc.pB, Lc.sc, hK, ug);
-        }
-        else {
-            k_adj_cg_init<64><<<Lc.nb, ND_THREADS, 0, sm>>>(Lc.ng, ctx->gm.as<double>(), ctx->collided.as<int8_t>(), ctx->proj.as<double>(),
-                ctx->res.as<double>(), kb, tol, Lc.pB, Lc.sc);
-            k_krylov_start<64><<<1, ND_THREADS, 0, sm>>>(Lc.ng, kb, Lc.np, Lc.pB, Lc.sc, hK, ug);
-        }
-        g_kernel_launches += 2;
-        return (int)ZMPM_OK;
-    };
-    auto body = [&](cudaStream_t sm, cudaGraphConditionalHandle hK, int ug) {
-        return l244 ? launch_krylov_iteration<32>(Lc, sm, hK, ug, nullptr, nullptr) : launch_krylov_iteration<64>(Lc, sm, hK, ug, nullptr, nullptr);
-    };
-    auto tail = [&](cudaStream_t sm, cudaGraphConditionalHandle hN, int ug) {
-        k_adj_once<<<1, 1, 0, sm>>>(Lc.sc, hN, ug);
-        ++g_kernel_launches;
-        return (int)ZMPM_OK;
-    };
-    if (!ctx->profiling) {
-        cudaGraphExec_t exec = nullptr;
-        const int64_t launches0 = g_kernel_launches;
-        int rc = loop_graph(
-            ctx, [&](cudaStream_t sm, cudaGraphConditionalHandle hK) { return head(sm, hK, 1); },
-            [&](cudaStream_t sm, cudaGraphConditionalHandle hK) { return body(sm, hK, 1); },
-            [&](cudaStream_t sm, cudaGraphConditionalHandle hN) { return tail(sm, hN, 1); }, &exec);
-        if (rc) return rc;
-        cudaError_t e = cudaGraphLaunch(exec, st);
-        cudaError_t e2 = cudaStreamSynchronize(st);
-        cudaGraphExecDestroy(exec);
-        ZMPM_CUDA(e);
-        ZMPM_CUDA(e2);
-        // kernels executed: head (2) and tail (1) once, 5 per Krylov body (CG)
-        SolverScalars hs;
-        ZMPM_CUDA(cudaMemcpyAsync(&hs, Lc.sc, sizeof(hs), cudaMemcpyDeviceToHost, st));
-        ZMPM_CUDA(cudaStreamSynchronize(st));
-        g_kernel_launches = launches0 + 3 + 5 * (int64_t)hs.krylov_bodies;
+    if (ctx->layout == 1) {
+        k_adj_cg_init<32><<<Lc.nb, ND_THREADS, 0, st>>>(Lc.ng, ctx->gm.as<double>(), ctx->collided.as<int8_t>(), ctx->proj.as<double>(),
+            ctx->res.as<double>(), kb, tol, Lc.pB, Lc.sc);
+        k_krylov_start<32><<<1, ND_THREADS, 0, st>>>(Lc.ng, kb, Lc.np, Lc.pB, Lc.sc, 0, 0);
     }
     else {
-        int rc = head(st, 0, 0);
-        if (rc) return rc;
-        for (int k = 0; k < max_iterations; k += 8) {
-            for (int j = 0; j < 8 && k + j < max_iterations; ++j) {
-                rc = body(st, 0, 0);
-                if (rc) return rc;
-            }
-            SolverScalars hs;
-            ZMPM_CUDA(cudaMemcpyAsync(&hs, Lc.sc, sizeof(hs), cudaMemcpyDeviceToHost, st));
-            ZMPM_CUDA(cudaStreamSynchronize(st));
-            if (!hs.kactive) break;
-        }
+        k_adj_cg_init<64><<<Lc.nb, ND_THREADS, 0, st>>>(Lc.ng, ctx->gm.as<double>(), ctx->collided.as<int8_t>(), ctx->proj.as<double>(),
+            ctx->res.as<double>(), kb, tol, Lc.pB, Lc.sc);
+        k_krylov_start<64><<<1, ND_THREADS, 0, st>>>(Lc.ng, kb, Lc.np, Lc.pB, Lc.sc, 0, 0);
     }
+    g_kernel_launches += 2;
+    ZMPM_CUDA(cudaMemsetAsync(ctx->gsync.p, 0, sizeof(GridSync), st));
+    int rc = ctx->layout == 1 ? launch_cg_persistent<32>(Lc, st) : launch_cg_persistent<64>(Lc, st);
+    if (rc) return rc;
+    ZMPM_CUDA(cudaStreamSynchronize(st));
     ZMPM_CUDA(cudaGetLastError());
     return ZMPM_OK;
 }

@@ -17,6 +17,7 @@
 #include "admm.cuh"
 #include "eig3.cuh"
 #include "fused.cuh"
+#include "hvp.cuh"
 #include "xfer.cuh"
 
 namespace zmpm {
@@ -574,14 +575,7 @@ __global__ void __launch_bounds__(XF_THREADS) k_hvp_scatter(const int32_t* __res
 }
 
 // ------------------------------------------------------- fused products ----
-// MpmForceBase::addScaledForceDifferential (MpmForceBase.cpp:259-302) in one
-// kernel (fused.cuh): phase 1 gathers grad(x) at each particle from the staged
-// window of the input vector and evaluates dS = V0 dP(grad(x) Fn) Fn^T from the
-// Hessian scratch (computeStressDifferential, FBasedMpmForceHelper.cpp:132-
-// 154); phase 2 adds dS grad w_ip to the nodes (rasterizeForceToTVStack with
-// the differential, :102-152), out += sum_p dS_p grad w_ip.  T: arithmetic
-// precision; TX: the input vector (FP32 node-major copy or FP64 vector).  The
-// input alternates between x0 and x1 with the Krylov iteration when `alt`.
+// The Hessian-vector product (hvp.cuh) as one CTA per particle group.
 template <class L, class T, class TX, int CH>
 __global__ void __launch_bounds__(FUSED_THREADS) k_hvp_fused(const int32_t* __restrict__ group_start, const int32_t* __restrict__ group_nbr,
     const int32_t* __restrict__ pi, int64_t cap, const short4* __restrict__ base, double dx, const T* __restrict__ frac,
@@ -589,59 +583,9 @@ __global__ void __launch_bounds__(FUSED_THREADS) k_hvp_fused(const int32_t* __re
     const SolverScalars* __restrict__ sc, int32_t* __restrict__ flags)
 {
     if (sc && (sc->newton_done || !sc->kactive)) return;
-    constexpr int NPB = L::NPB;
-    __shared__ __align__(128) TX win[VecWindow<NPB, TX>::ELEMS];
-    __shared__ ScatterSmem<L, T, CH> sm;
-    __shared__ __align__(8) uint64_t bar;
-    const int g = blockIdx.x;
-    if (threadIdx.x < 8) sm.nbr[threadIdx.x] = group_nbr[8 * g + threadIdx.x];
-    zero_window<3, NPB>(sm.acc);
-    __syncthreads();
+    __shared__ HvpSmem<L, T, TX, CH> hs;
     const TX* x = (alt && sc && (sc->kit & 1)) ? x1 : x0;
-    stage_vec_window<NPB, TX>(win, x, sm.nbr, &bar, flags);
-    const int s0 = group_start[g], n = group_start[g + 1] - s0;
-    build_cell_layout<L>(sm.cl, base, s0, s0 + n);
-    list_occupied(sm);
-    const T inv_dx = T(1.0 / dx);
-    for (int c0 = 0; c0 < n; c0 += CH) {
-        const int c1 = c0 + CH < n ? c0 + CH : n;
-        __syncthreads();
-        for (int p = c0 + threadIdx.x; p < c1; p += blockDim.x) {
-            const int64_t s = s0 + p;
-            T* rc = sm.rec + (p - c0);
-            T fr[3];
-#pragma unroll
-            for (int d = 0; d < 3; ++d) {
-                fr[d] = frac[d * cap + s];
-                rc[d * sm.FS] = fr[d];
-            }
-            const int kind = pi[PI_KIND * cap + s];
-            M3<T> dS = m3_zero<T>();
-            if (kind != ZMPM_MODEL_NONE) {
-                const short4 b = base[s];
-                T w[3][3], dw[3][3];
-#pragma unroll
-                for (int d = 0; d < 3; ++d) bspline_all(fr[d], w[d], dw[d]);
-                const StencilOffsets<L> so(b.x & (L::BX - 1), b.y & (L::BY - 1), b.z & (L::BZ - 1));
-                M3<T> G;
-                if constexpr (sizeof(T) == 4 && sizeof(TX) == 4)
-                    gather_gradient_f32<L>(win, so, w, dw, G.a);
-                else
-                    gather_gradient<L, T, TX>(win, so, w, dw, G.a);
-#pragma unroll
-                for (int q = 0; q < 9; ++q) G.a[q] *= inv_dx;
-                dS = model_hvp<T>(kind, scr, cap, s, G);
-            }
-#pragma unroll
-            for (int r = 0; r < 3; ++r)
-#pragma unroll
-                for (int c = 0; c < 3; ++c) rc[(3 + 3 * r + c) * sm.FS] = dS(r, c) * inv_dx;
-        }
-        __syncthreads();
-        scatter_rows(sm, c0, c1);
-    }
-    __syncthreads();
-    flush_window<3, 3, NPB>(sm.acc, sm.nbr, out, nullptr);
+    hvp_group<L, T, TX, CH>(hs, blockIdx.x, group_start, group_nbr, pi, cap, base, dx, frac, scr, x, out, flags);
 }
 
 // MpmForceBase::updatePositionBasedState + rasterizeForceToTVStack
