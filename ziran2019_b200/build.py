@@ -13,7 +13,8 @@ CSRC = os.path.join(HERE, "csrc")
 OUT_DIR = os.path.join(HERE, "lib")
 OUT = os.path.join(OUT_DIR, "libzmpm.so")
 SOURCES = ["adjoint.cu", "admm.cu", "api.cu", "bin.cu", "io.cu", "noalloc.cu", "phase.cu", "prims.cu", "solver.cu", "transfer.cu"]
-HEADERS = ["admm.cuh", "common.cuh", "internal.cuh", "mat3.cuh", "models.cuh", "node.cuh", "svd3.cuh", "xfer.cuh"]
+HEADERS = ["admm.cuh", "common.cuh", "eig3.cuh", "fused.cuh", "hvp.cuh", "internal.cuh", "mat3.cuh", "models.cuh", "node.cuh", "svd3.cuh",
+           "xfer.cuh"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

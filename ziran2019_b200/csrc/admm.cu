@@ -8,8 +8,10 @@
 // omega_1^2 Fe Fe^T) (6 numbers per particle),
 //     (A x)_i = m_i x_i + sum_p (grad x_p B_p) grad w_ip,  grad x_p = sum_j x_j grad w_jp^T,
 // the same gather -> 3x3 -> scatter shape as the Newton Hessian product, so it
-// reuses that scatter kernel.  Per product that is 6 numbers per particle
-// instead of 125 values + 125 indices per node.
+// runs through the same per-group product (hvp.cuh, AdmmOpModel): k_op_fused
+// for the right-hand side's product, the persistent MINRES for the solve.
+// Per product that is 6 numbers per particle instead of 125 values + 125
+// indices per node.
 //
 // Kernels
 //  k_admm_dvinit   dv_i = sum_p last_dv_p w_ip, w_i = sum_p w_ip (initStep :304-320)
@@ -18,7 +20,6 @@
 //  k_admm_pre      preconditioner m_i + sum_p grad w^T B grad w (:477-503)
 //  k_admm_local    FStepSolve (:507-615) for F and Fe, then the dvStep
 //                  right-hand side stress dt rho omega^2 bFu Fn^T (:163-205)
-//  k_admm_op       grad x B for the matrix-free global operator
 //  k_admm_dual     uStep (:638-671)
 //  k_admm_lastdv   last_dv = sum dv w / (dt sum w) (:788-800)
 #include "admm.cuh"
@@ -289,52 +290,6 @@ __global__ void __launch_bounds__(XF_THREADS) k_admm_local(const int32_t* __rest
     }
 }
 
-// ----------------------------------------------------------- operator -----
-template <class L, class TH>
-__global__ void __launch_bounds__(XF_THREADS) k_admm_op(const int32_t* __restrict__ group_start, const int32_t* __restrict__ group_nbr,
-    int64_t cap, const short4* __restrict__ base, double dx, const TH* __restrict__ frac, const TH* __restrict__ B,
-    const double* __restrict__ x0, const double* __restrict__ x1, int alt, TH* __restrict__ dstress, const SolverScalars* __restrict__ sc,
-    int32_t* __restrict__ flags)
-{
-    if (sc && (sc->newton_done || !sc->kactive)) return;
-    constexpr int NPB = L::NPB;
-    __shared__ __align__(128) double win[8 * 3 * NPB];
-    __shared__ int32_t nbr[8];
-    __shared__ __align__(8) uint64_t bar;
-    const int g = blockIdx.x;
-    if (threadIdx.x < 8) nbr[threadIdx.x] = group_nbr[8 * g + threadIdx.x];
-    __syncthreads();
-    const double* x = (alt && sc && (sc->kit & 1)) ? x1 : x0;
-    stage_window<NPB>(win, x, nbr, &bar, flags);
-    const TH inv_dx = TH(1.0 / dx);
-    const int s0 = group_start[g], s1 = group_start[g + 1];
-    for (int s = s0 + threadIdx.x; s < s1; s += blockDim.x) {
-        const short4 b = base[s];
-        TH w[3][3], dwr[3][3];
-#pragma unroll
-        for (int d = 0; d < 3; ++d) bspline(frac[d * cap + s], w[d], dwr[d]);
-        const int lx = b.x & (L::BX - 1), ly = b.y & (L::BY - 1), lz = b.z & (L::BZ - 1);
-        M3<TH> G = m3_zero<TH>();
-        for_stencil<L>(lx, ly, lz, w, dwr, inv_dx, [&](int t, int e, int, int, int, TH, const TH* dw) {
-            const double* vv = win + t * 3 * NPB + e;
-#pragma unroll
-            for (int r = 0; r < 3; ++r) {
-                const TH vr = (TH)vv[r * NPB];
-#pragma unroll
-                for (int c = 0; c < 3; ++c) G(r, c) += vr * dw[c];
-            }
-        });
-        const TH b00 = B[0 * cap + s], b01 = B[1 * cap + s], b02 = B[2 * cap + s], b11 = B[3 * cap + s], b12 = B[4 * cap + s],
-                 b22 = B[5 * cap + s];
-#pragma unroll
-        for (int r = 0; r < 3; ++r) {
-            dstress[(int64_t)(3 * r + 0) * cap + s] = G(r, 0) * b00 + G(r, 1) * b01 + G(r, 2) * b02;
-            dstress[(int64_t)(3 * r + 1) * cap + s] = G(r, 0) * b01 + G(r, 1) * b11 + G(r, 2) * b12;
-            dstress[(int64_t)(3 * r + 2) * cap + s] = G(r, 0) * b02 + G(r, 1) * b12 + G(r, 2) * b22;
-        }
-    }
-}
-
 // ------------------------------------------------------------ dual step ---
 template <class L>
 __global__ void __launch_bounds__(XF_THREADS) k_admm_dual(const int32_t* __restrict__ group_start, const int32_t* __restrict__ group_nbr,
@@ -448,17 +403,6 @@ int local_impl(Ctx* ctx, double rho, double local_tol)
     return ZMPM_OK;
 }
 
-template <class L, class TH>
-int op_impl(Ctx* ctx, const double* x0, const double* x1, bool alt, bool gated)
-{
-    DevCounters* dc = ctx->counters.as<DevCounters>();
-    k_admm_op<L, TH><<<(unsigned)ctx->G, XF_THREADS, 0, ctx->stream>>>(ctx->group_start.as<int32_t>(), ctx->group_nbr.as<int32_t>(), ctx->Pcap,
-        ctx->base.as<short4>(), ctx->cfg.dx, ctx->frac.as<TH>(), ctx->adm_B.as<TH>(), x0, x1, alt ? 1 : 0, ctx->dstress.as<TH>(),
-        gated ? ctx->scal.as<SolverScalars>() : nullptr, &dc->flags);
-    ++g_kernel_launches;
-    return ZMPM_OK;
-}
-
 template <class L>
 int dual_impl(Ctx* ctx, double rho)
 {
@@ -493,13 +437,5 @@ int launch_admm_pre(Ctx* ctx) { return ctx->G ? ZMPM_BY_LAYOUT_TH(pre_impl, ctx)
 int launch_admm_local(Ctx* ctx, double rho, double local_tol) { return ctx->G ? ZMPM_BY_LAYOUT_TH(local_impl, ctx, rho, local_tol) : ZMPM_OK; }
 int launch_admm_dual(Ctx* ctx, double rho) { return ctx->G ? ZMPM_BY_LAYOUT(dual_impl, ctx, rho) : ZMPM_OK; }
 int launch_admm_lastdv(Ctx* ctx) { return ctx->G ? ZMPM_BY_LAYOUT(lastdv_impl, ctx) : ZMPM_OK; }
-
-int launch_admm_op(Ctx* ctx, const double* x0, const double* x1, bool alt, double* out, bool gated)
-{
-    if (!ctx->G) return ZMPM_OK;
-    int rc = ZMPM_BY_LAYOUT_TH(op_impl, ctx, x0, x1, alt, gated);
-    if (rc) return rc;
-    return launch_hvp_scatter(ctx, out, gated);
-}
 
 } // namespace zmpm

@@ -68,7 +68,6 @@ int upload(Ctx* ctx)
     ZMPM_CUDA(ctx->scratch.ensure(NS * cap * TH));
     ZMPM_CUDA(ctx->frac.ensure(3 * cap * TH));
     ZMPM_CUDA(ctx->stress.ensure(9 * cap * sizeof(double)));
-    ZMPM_CUDA(ctx->dstress.ensure(9 * cap * TH));
     std::vector<double> hpd((size_t)PD_FIELDS * cap, 0.0);
     std::vector<int32_t> hpi((size_t)PI_FIELDS * cap, 0), sid(cap);
     for (int64_t i = 0; i < P; ++i) {
@@ -472,7 +471,7 @@ int zmpm_destroy(zmpm_ctx* ctx)
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     DBuf* bufs[] = { &ctx->pd, &ctx->pd_alt, &ctx->pi, &ctx->pi_alt, &ctx->slot_of_id, &ctx->base_by_id, &ctx->base, &ctx->Fn, &ctx->scratch,
-        &ctx->frac, &ctx->stress, &ctx->dstress, &ctx->keys, &ctx->keys_alt, &ctx->flags_i32, &ctx->scan_i32, &ctx->scan_scr, &ctx->radix_scr, &ctx->group_start,
+        &ctx->frac, &ctx->stress, &ctx->keys, &ctx->keys_alt, &ctx->flags_i32, &ctx->scan_i32, &ctx->scan_scr, &ctx->radix_scr, &ctx->group_start,
         &ctx->group_page, &ctx->group_nbr, &ctx->emit_flag, &ctx->emit_scan, &ctx->page_first, &ctx->page_block, &ctx->block_page,
         &ctx->block_index, &ctx->gm, &ctx->gmv, &ctx->vn, &ctx->dv, &ctx->vstar, &ctx->facc, &ctx->res, &ctx->proj, &ctx->collided,
         &ctx->node_idx, &ctx->red, &ctx->scal, &ctx->counters, &ctx->dcolliders, &ctx->adm_F, &ctx->adm_gvn, &ctx->adm_B, &ctx->adm_pre,
@@ -911,21 +910,11 @@ static int delete_phase_field_particles(zmpm_ctx* ctx)
     return launch_phase_field_delete(ctx);
 }
 
-// Kernels of one Newton Krylov-loop body: MINRES runs the Hessian product,
-// k_mr_a and k_mr_b per iteration; CG runs its whole solve in one persistent
-// kernel (counted with the Newton body).
-static int64_t krylov_body_launches(const zmpm_ctx*, const zmpm_solver& s) { return s.linear_solver == ZMPM_MINRES ? 3 : 0; }
-
-// Kernels of one Newton loop body outside the Krylov loop: stress and force
-// (MIXED: an FP32 and an FP64 pair, one of which returns at once), residual
-// with the Krylov start vectors, Newton check with the Krylov start, step,
-// advance.
-static int64_t newton_body_launches(const zmpm_ctx* ctx, const zmpm_solver& s)
-{
-    // update (MIXED: the FP32 pass and the gated FP64 pair), residual, Newton
-    // check, step, advance; CG adds its persistent solve
-    return (ctx->mixed ? 7 : 5) + (s.linear_solver == ZMPM_MINRES ? 0 : 1);
-}
+// Kernels of one Newton loop body when the solve runs as a graph: the update
+// (MIXED: the FP32 pass and the gated FP64 stress / force pair, one of which
+// returns at once), residual with the Krylov start vectors, Newton check with
+// the Krylov start, the persistent linear solve, step, advance.
+static int64_t newton_body_launches(const zmpm_ctx* ctx) { return ctx->mixed ? 8 : 6; }
 
 static int begin_implicit_impl(zmpm_ctx* ctx, double dt, bool damage = true)
 {
@@ -1058,10 +1047,12 @@ static int substep_finish(zmpm_ctx* ctx, double dt, const zmpm_solver& s, zmpm_s
     st->rankine_first_not_max = hc.first_not_max;
     st->svd_fp64_reevaluations = hc.svd_fp64;
     if (!admm && !expl) ctx->fp64_res_run = hs.fp64_res ? ctx->fp64_res_run + 1 : 0;
-    if (ctx->graph_used && admm) // ADMM iteration: 7 head + 3 tail kernels; Krylov body: operator (2), k_mr_a, k_mr_b
-        g_kernel_launches += 10 * (int64_t)hs.nit + 4 * (int64_t)hs.krylov_bodies;
+    // ADMM iteration: collision, local step, force scatter, operator, start,
+    // Krylov start, persistent MINRES, dv update, dual update, advance
+    if (ctx->graph_used && admm)
+        g_kernel_launches += 10 * (int64_t)hs.nit;
     else if (ctx->graph_used)
-        g_kernel_launches += newton_body_launches(ctx, s) * (int64_t)hs.nit + krylov_body_launches(ctx, s) * (int64_t)hs.krylov_bodies;
+        g_kernel_launches += newton_body_launches(ctx) * (int64_t)hs.nit;
     ctx->graph_used = false;
     st->kernel_launches = (int32_t)(g_kernel_launches - launches0);
     ctx->N = hc.N;
@@ -1246,7 +1237,7 @@ int zmpm_adjoint_substep(zmpm_ctx* ctx, double dt, const zmpm_solver* s, double 
         ctx->graph_exec = nullptr;
     }
     if (ctx->graph_used)
-        g_kernel_launches += newton_body_launches(ctx, *s) * (int64_t)hs.nit + krylov_body_launches(ctx, *s) * (int64_t)hs.krylov_bodies;
+        g_kernel_launches += newton_body_launches(ctx) * (int64_t)hs.nit;
     st->newton_iterations = hs.newton_iters;
     st->newton_converged = hs.converged;
     st->fp64_residual = hs.fp64_res;

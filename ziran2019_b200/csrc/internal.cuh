@@ -3,6 +3,7 @@
 
 #include <cstdint>
 #include <cstdio>
+#include <map>
 #include <string>
 #include <vector>
 
@@ -93,9 +94,10 @@ enum MinresSlot { MR_GC0, MR_GS0, MR_GC1, MR_GS1, MR_GC2, MR_GS2, MR_RHS0, MR_RH
 // zeroed before each launch.
 struct GridSync {
     unsigned count;  // CTAs arrived at the current barrier
-    unsigned gen;    // barriers completed
-    unsigned work;   // next particle group of the running product
+    unsigned pad0[31];
+    unsigned gen;    // barriers completed (polled by the waiting CTAs, on its own 128-byte line)
     unsigned abort;  // 1 once a CTA's wait gave up
+    unsigned pad1[30];
 };
 
 // Field indices of the particle pools.
@@ -177,7 +179,6 @@ struct Ctx {
     DBuf Fn;           // [9][Pcap] F at the start of the Newton solve
     DBuf scratch;      // Hessian scratch [NS][Pcap] in the HVP precision
     DBuf stress;       // [9][Pcap] V0 P(F) Fn^T of the current Newton iterate
-    DBuf dstress;      // [9][Pcap] dS of one Hessian-vector product (HVP precision)
     cudaGraphExec_t graph_exec = nullptr; // last solve graph, released when the next one is launched
     bool graph_used = false;              // the last Newton solve ran as a graph
     DBuf frac;         // [3][Pcap] fractional offsets in cells (FP32 HVP)
@@ -221,8 +222,8 @@ struct Ctx {
     std::vector<double> ckpt_time;
     std::vector<int64_t> ckpt_P;
     bool admm_used = false;               // the last substep ran ADMM (launch accounting)
-    DBuf gsync;                           // GridSync of the persistent Krylov kernel
-    int coop_blocks = 0;                  // its cooperative grid size (all CTAs co-resident)
+    DBuf gsync;                           // GridSync of the persistent Krylov kernels
+    std::map<const void*, int> coop_blocks; // cooperative grid size of each persistent kernel (all CTAs co-resident)
     long long spin_limit = 1ll << 22;     // polls before a grid-barrier wait gives up (zmpm_set_spin_limit)
     // substep phases: 1 after zmpm_particles_to_grid, 2 after zmpm_backward_euler_step
     int phase = 0;
@@ -272,11 +273,10 @@ int launch_admm_dvinit(Ctx* ctx);                      // scatter last_dv w and 
 int launch_admm_init(Ctx* ctx, double rho);            // local variables, omega, y rescale, B
 int launch_admm_pre(Ctx* ctx);                         // preconditioner += grad w^T B grad w
 int launch_admm_local(Ctx* ctx, double rho, double local_tol); // F step + rhs stress
-int launch_admm_op(Ctx* ctx, const double* x0, const double* x1, bool alt, double* out, bool gated); // out += sum (grad x B) grad w
+int launch_admm_op(Ctx* ctx, const double* x, double* out); // out += sum (grad x B) grad w
 int launch_admm_dual(Ctx* ctx, double rho);            // y += rho omega (F - (I + dt grad v) Fn)
 int launch_admm_lastdv(Ctx* ctx);                      // last_dv = sum dv w / (dt sum w)
 int launch_force_scatter(Ctx* ctx, double* out, bool mls = false);       // out -= sum_p stress_p grad w_ip (stress buffer)
-int launch_hvp_scatter(Ctx* ctx, double* out, bool gated); // out += sum_p dstress_p grad w_ip
 int finalize_multiply(Ctx* ctx, const double* x, double* q); // q = project(m x + q)
 int ensure_node_buffers(Ctx* ctx);
 int compute_node_indices(Ctx* ctx);                    // getNumNodes numbering (hooks)

@@ -612,7 +612,7 @@ struct MrPending {
     double delta, eps, gamma, t, beta;
     bool on;
 };
-__device__ __forceinline__ MrPending mr_pending(const KrylovBufs& kb, const SolverScalars* sc, int k)
+__device__ __forceinline__ MrPending mr_pending(const KrylovBufs& kb, const double* pend, int k)
 {
     MrPending p;
     p.on = k > 0;
@@ -620,11 +620,11 @@ __device__ __forceinline__ MrPending mr_pending(const KrylovBufs& kb, const Solv
     p.m1 = sel3(kb.M, (k + 1) % 3);  // M_{k-2}
     p.m2 = sel3(kb.M, k % 3);        // M_{k-3}
     p.out = sel3(kb.M, (k + 2) % 3); // M_{k-1}
-    p.delta = sc->pend[0];
-    p.eps = sc->pend[1];
-    p.gamma = sc->pend[2];
-    p.t = sc->pend[3];
-    p.beta = sc->pend[4];            // beta_{k-1}
+    p.delta = pend[0];
+    p.eps = pend[1];
+    p.gamma = pend[2];
+    p.t = pend[3];
+    p.beta = pend[4];                // beta_{k-1}
     return p;
 }
 __device__ __forceinline__ double mr_direction(const MrPending& p, int64_t i)
@@ -647,7 +647,7 @@ __global__ void __launch_bounds__(ND_THREADS, 4) k_mr_a(NodeGeom ng, const doubl
     const int k = sc->kit;
     const double* __restrict__ zk = sel2(kb.Z, k & 1);
     double* __restrict__ w = sel3(kb.Q, (k + 1) % 3);
-    const MrPending pd = mr_pending(kb, sc, k);
+    const MrPending pd = mr_pending(kb, sc->pend, k);
     const double beta = sc->mr[k & 1][MR_BETA_KP1];
     double acc = 0;
     for (int64_t n = (int64_t)blockIdx.x * ND_THREADS + threadIdx.x; n < ng.nn; n += (int64_t)gridDim.x * ND_THREADS) {
@@ -673,6 +673,52 @@ __global__ void __launch_bounds__(ND_THREADS, 4) k_mr_a(NodeGeom ng, const doubl
     }
     const double s = block_sum(acc);
     if (threadIdx.x == 0) part[blockIdx.x] = s;
+}
+
+// The Givens update of MINRES iteration k (Minres.h:151-175): from the state
+// cur of iteration k (Minres.h:16-24), alpha = Z_k . W, beta_k and dz =
+// Z~_{k+1} . Q~_{k+1}, the state of iteration k + 1 into nx and the deferred
+// search direction's delta, epsilon, gamma, t and beta into pend; returns the
+// preconditioned residual norm.
+__device__ __forceinline__ double mr_givens(const double* cur, double alpha, double beta_k, double dz, double* nx, double* pend)
+{
+    const double beta_kp1 = sqrt(dz > 0 ? dz : 0.0);
+    // Gkm2 = Gkm1, Gkm1 = Gk
+    double c2 = cur[MR_GC1], s2 = cur[MR_GS1], c1 = cur[MR_GC0], s1 = cur[MR_GS0];
+    double e0 = c2 * 0 - s2 * beta_k, e1 = s2 * 0 + c2 * beta_k;
+    const double epsilon = e0;
+    double d0 = c1 * e1 - s1 * alpha, d1 = s1 * e1 + c1 * alpha;
+    const double delta = d0;
+    double t0 = d1, t1 = beta_kp1;
+    double c0 = 1, s0 = 0;
+    {
+        double dd = t0 * t0 + t1 * t1;
+        double sd = sqrt(dd);
+        if (sd != 0) {
+            double tt = 1 / sd;
+            c0 = t0 * tt;
+            s0 = -t1 * tt;
+        }
+    }
+    const double gamma = c0 * t0 - s0 * t1;
+    const double r0 = cur[MR_RHS0], r1 = cur[MR_RHS1];
+    const double tk = c0 * r0 - s0 * r1;
+    const double residual = s0 * r0 + c0 * r1;
+    nx[MR_GC0] = c0;
+    nx[MR_GS0] = s0;
+    nx[MR_GC1] = c1;
+    nx[MR_GS1] = s1;
+    nx[MR_GC2] = c2;
+    nx[MR_GS2] = s2;
+    nx[MR_RHS0] = residual;
+    nx[MR_RHS1] = 0;
+    nx[MR_BETA_KP1] = beta_kp1;
+    pend[0] = delta;
+    pend[1] = epsilon;
+    pend[2] = gamma;
+    pend[3] = tk;
+    pend[4] = beta_k;
+    return residual < 0 ? -residual : residual;
 }
 
 // Lanczos step: Q~_{k+1} = W - alpha Q_k - beta_k Q_{k-1} (Q_j = Q~_j /
@@ -719,45 +765,7 @@ __global__ void __launch_bounds__(ND_THREADS) k_mr_b(NodeGeom ng, const double* 
     const double dz = reduce_partials_l2(part_out, ng.parts);
     if (threadIdx.x != 0) return;
     const int nit = sc->nit;
-    const double* cur = sc->mr[it & 1];
-    const double beta_kp1 = sqrt(dz > 0 ? dz : 0.0);
-    // Gkm2 = Gkm1, Gkm1 = Gk
-    double c2 = cur[MR_GC1], s2 = cur[MR_GS1], c1 = cur[MR_GC0], s1 = cur[MR_GS0];
-    double e0 = c2 * 0 - s2 * beta_k, e1 = s2 * 0 + c2 * beta_k;
-    const double epsilon = e0;
-    double d0 = c1 * e1 - s1 * alpha, d1 = s1 * e1 + c1 * alpha;
-    const double delta = d0;
-    double t0 = d1, t1 = beta_kp1;
-    double c0 = 1, s0 = 0;
-    {
-        double dd = t0 * t0 + t1 * t1;
-        double sd = sqrt(dd);
-        if (sd != 0) {
-            double tt = 1 / sd;
-            c0 = t0 * tt;
-            s0 = -t1 * tt;
-        }
-    }
-    const double gamma = c0 * t0 - s0 * t1;
-    const double r0 = cur[MR_RHS0], r1 = cur[MR_RHS1];
-    const double tk = c0 * r0 - s0 * r1;
-    const double residual = s0 * r0 + c0 * r1;
-    const double rnorm = residual < 0 ? -residual : residual;
-    double* nx = sc->mr[(it + 1) & 1];
-    nx[MR_GC0] = c0;
-    nx[MR_GS0] = s0;
-    nx[MR_GC1] = c1;
-    nx[MR_GS1] = s1;
-    nx[MR_GC2] = c2;
-    nx[MR_GS2] = s2;
-    nx[MR_RHS0] = residual;
-    nx[MR_RHS1] = 0;
-    nx[MR_BETA_KP1] = beta_kp1;
-    sc->pend[0] = delta;
-    sc->pend[1] = epsilon;
-    sc->pend[2] = gamma;
-    sc->pend[3] = tk;
-    sc->pend[4] = beta_k;
+    const double rnorm = mr_givens(sc->mr[it & 1], alpha, beta_k, dz, sc->mr[(it + 1) & 1], sc->pend);
     sc->rnorm = rnorm;
     sc->krylov_iters += 1;
     sc->hvp_count += 1;
@@ -768,8 +776,8 @@ __global__ void __launch_bounds__(ND_THREADS) k_mr_b(NodeGeom ng, const double* 
 // ------------------------------------------------ persistent Krylov -----
 // One cooperative launch runs a whole linear solve of the Newton iteration
 // (ConjugateGradient::solve, ConjugateGradient.h:99-147, on the Newton
-// operator): per iteration the Hessian-vector product of p (hvp_group over
-// the particle groups, taken in turn from a shared counter), A p with its
+// operator): per iteration the Hessian-vector product of p (hvp_share over
+// each CTA's even share of the particle groups), A p with its
 // partial dot, the x / r / q update with its partial dot and p = q + beta p,
 // separated by grid-wide barriers.  Every CTA reduces the per-CTA partials in
 // the same fixed order, so all hold bit-identical scalars and take the same
@@ -849,8 +857,46 @@ struct HvpArgs {
     int G;
 };
 
+// The product of x into out over this CTA's share of the particle groups.  A
+// group's cost is about K particles' worth of fixed work (staging the window,
+// the cell layout, the flush) plus its particles, so group g spans the
+// weights [W(g), W(g + 1)), W(g) = group_start[g] + K g; the total weight is
+// split evenly over the grid and a group whose weight range a share boundary
+// cuts is split into two pieces at the matching particle (pieces of one group
+// add to the same nodes).  K measured on B200 at 1M particles: about 192
+// FP32 particles, 128 FP64 ones (the per-particle work costs more in FP64).
+template <class L, class T, class TX, int CH, class Model>
+__device__ __forceinline__ void hvp_share(HvpSmem<L, T, TX, CH>& hs, const HvpArgs& ha, const Model& model, const TX* x, double* out,
+    int32_t* flags, int& phase)
+{
+    constexpr int PIECE_COST = sizeof(T) == 4 ? 192 : 128;
+    if (ha.G <= 0) return;
+    const int32_t* __restrict__ gs = ha.group_start;
+    const int64_t total = (int64_t)gs[ha.G] + (int64_t)PIECE_COST * ha.G;
+    const int64_t w0 = total * blockIdx.x / gridDim.x, w1 = total * (blockIdx.x + 1) / gridDim.x;
+    if (w0 >= w1) return;
+    int a = 0, b = ha.G - 1; // the last group whose weight range starts at or before w0
+    while (a < b) {
+        const int m = (a + b + 1) >> 1;
+        if ((int64_t)gs[m] + (int64_t)PIECE_COST * m <= w0)
+            a = m;
+        else
+            b = m - 1;
+    }
+    for (int g = a; g < ha.G; ++g) {
+        const int g0 = gs[g], n = gs[g + 1] - g0;
+        const int64_t wp = (int64_t)g0 + (int64_t)PIECE_COST * g + PIECE_COST; // weight of the group's first particle
+        if (wp - PIECE_COST >= w1) break;
+        const int64_t lo = w0 - wp, hi = w1 - wp;
+        const int s0 = g0 + (int)(lo < 0 ? 0 : (lo > n ? n : lo)), s1 = g0 + (int)(hi < 0 ? 0 : (hi > n ? n : hi));
+        if (s0 < s1)
+            hvp_group<L, T, TX, CH>(hs, g, s0, s1, ha.group_nbr, model, ha.cap, ha.base, ha.dx, static_cast<const T*>(ha.frac), x, out, flags,
+                phase++);
+    }
+}
+
 template <class L, class T>
-__global__ void __launch_bounds__(FUSED_THREADS) k_cg_persistent(NodeGeom ng, HvpArgs ha, const double* __restrict__ gm,
+__global__ void __launch_bounds__(FUSED_THREADS, 4) k_cg_persistent(NodeGeom ng, HvpArgs ha, const double* __restrict__ gm,
     const int8_t* __restrict__ col, const double* __restrict__ P6, double dt2, KrylovBufs kb, double* __restrict__ part_a,
     double* __restrict__ part_b, SolverScalars* __restrict__ sc, int kmax, GridSync* __restrict__ gs, long long limit, int32_t* __restrict__ flags)
 {
@@ -858,7 +904,6 @@ __global__ void __launch_bounds__(FUSED_THREADS) k_cg_persistent(NodeGeom ng, Hv
     constexpr int NPB = L::NPB;
     constexpr int CH = sizeof(T) == 4 ? 512 : 192;
     __shared__ HvpSmem<L, T, double, CH> hs;
-    __shared__ int gsh;
     if (threadIdx.x == 0) mbar_init(&hs.bar, 1);
     __syncthreads();
     int phase = 0;
@@ -869,16 +914,8 @@ __global__ void __launch_bounds__(FUSED_THREADS) k_cg_persistent(NodeGeom ng, Hv
     const int64_t t0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x, nt = (int64_t)gridDim.x * blockDim.x;
     for (;;) {
         // the Hessian-vector product of p into hacc
-        for (;;) {
-            if (threadIdx.x == 0) gsh = atomicAdd(&gs->work, 1);
-            __syncthreads();
-            const int g = gsh;
-            if (g >= ha.G) break;
-            hvp_group<L, T, double, CH>(hs, g, ha.group_start, ha.group_nbr, ha.pi, ha.cap, ha.base, ha.dx, static_cast<const T*>(ha.frac),
-                static_cast<const T*>(ha.scr), kb.p, kb.hacc, flags, phase++);
-        }
+        hvp_share<L, T, double, CH>(hs, ha, HvpModel<T>{ ha.pi, static_cast<const T*>(ha.scr), ha.cap }, kb.p, kb.hacc, flags, phase);
         if (!grid_sync(gs, limit, flags)) return;
-        if (blockIdx.x == 0 && threadIdx.x == 0) gs->work = 0; // read again only after two more barriers
         // tmp = project(m p + dt^2 hacc), hacc = 0; partial p . tmp (BackwardEuler.h:322-351)
         double acc = 0;
         for (int64_t n = t0; n < ng.nn; n += nt) {
@@ -947,6 +984,145 @@ __global__ void __launch_bounds__(FUSED_THREADS) k_cg_persistent(NodeGeom ng, Hv
     }
 }
 
+// ------------------------------------------------ persistent MINRES -----
+// One cooperative launch runs a whole MINRES solve (Minres.h:69-175) on the
+// Newton operator (HvpModel; dt2 = dt^2, pre = m) or on ADMM's global operator
+// (AdmmOpModel; dt2 = 1, pre = its preconditioner).  Per iteration k: the
+// product of Z~_k (its FP32 node-major copy when TX is float) over each CTA's
+// even share of the particle groups (hvp_share); the operator pass of k_mr_a; the
+// Lanczos step of k_mr_b; the Givens update, which thread 0 of every CTA runs
+// on the same fixed-order reductions, so every CTA holds the same MINRES state
+// (in shared memory) and takes the same loop decision.  CTA 0 stores the state
+// after each iteration (the Newton step applies the last deferred direction
+// from it).  Three bounded grid barriers per iteration: the product is
+// complete before the operator pass reads hacc, W before the Lanczos step, and
+// Z~_{k+1} before the next product and the reduction of its norm.
+template <class L, class T, class TX, class Model>
+__global__ void __launch_bounds__(FUSED_THREADS, 4) k_mr_persistent(NodeGeom ng, HvpArgs ha, Model model, const double* __restrict__ gm,
+    const int8_t* __restrict__ col, const double* __restrict__ P6, double dt2, KrylovBufs kb, double* __restrict__ part_a,
+    double* __restrict__ part_b, SolverScalars* __restrict__ sc, int kmax, GridSync* __restrict__ gs, long long limit, int32_t* __restrict__ flags)
+{
+    if (sc->newton_done || !sc->kactive) return;
+    constexpr int NPB = L::NPB;
+    constexpr int CH = sizeof(T) == 4 ? 512 : 192;
+    __shared__ HvpSmem<L, T, TX, CH> hs;
+    // the MINRES state of iteration k (Minres.h:16-24), then the deferred
+    // direction's scalars, beta_{k-1} and the residual norm
+    __shared__ double mst[12 + 5 + 2];
+    double* const pend = mst + 12;
+    int k = sc->kit;
+    if (threadIdx.x == 0) {
+        mbar_init(&hs.bar, 1);
+        for (int i = 0; i < 12; ++i) mst[i] = sc->mr[k & 1][i];
+        for (int i = 0; i < 5; ++i) pend[i] = sc->pend[i];
+        mst[17] = sc->mr[(k + 1) & 1][MR_BETA_KP1];
+    }
+    __syncthreads();
+    int phase = 0;
+    const int nit = sc->nit;
+    const double local_tol = sc->local_tol;
+    const int64_t t0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x, nt = (int64_t)gridDim.x * blockDim.x;
+    for (;;) {
+        // the product of Z~_k into hacc
+        const TX* zin;
+        if constexpr (sizeof(TX) == 4)
+            zin = reinterpret_cast<const TX*>(sel2(kb.Zf, k & 1));
+        else
+            zin = reinterpret_cast<const TX*>(sel2(kb.Z, k & 1));
+        hvp_share<L, T, TX, CH>(hs, ha, model, zin, kb.hacc, flags, phase);
+        if (!grid_sync(gs, limit, flags)) return;
+        // operator pass (k_mr_a): the deferred direction of iteration k - 1;
+        // W = project(m Z_k + dt2 H Z_k) into Q's slot k + 1; partial Z_k . W
+        {
+            const double* __restrict__ zk = sel2(kb.Z, k & 1);
+            double* __restrict__ w = sel3(kb.Q, (k + 1) % 3);
+            const MrPending pd = mr_pending(kb, pend, k);
+            const double beta = mst[MR_BETA_KP1];
+            double acc = 0;
+            for (int64_t n = t0; n < ng.nn; n += nt) {
+                const double m = gm[n];
+                if (m == 0) continue;
+                double o[3], z[3];
+                for (int c = 0; c < 3; ++c) {
+                    const int64_t i = vidx<NPB>(n, c);
+                    if (pd.on) {
+                        const double mv = mr_direction(pd, i);
+                        pd.out[i] = mv;
+                        kb.x[i] += pd.t * mv;
+                    }
+                    z[c] = mr_norm(zk[i], beta);
+                    o[c] = m * z[c] + dt2 * mr_norm(kb.hacc[i], beta);
+                    kb.hacc[i] = 0;
+                }
+                project3(col, P6, ng.nn, n, o);
+                for (int c = 0; c < 3; ++c) {
+                    w[vidx<NPB>(n, c)] = o[c];
+                    acc += o[c] * z[c];
+                }
+            }
+            acc = block_sum_fused(acc);
+            if (threadIdx.x == 0) part_a[blockIdx.x] = acc;
+        }
+        if (!grid_sync(gs, limit, flags)) return;
+        // Lanczos step (k_mr_b): Q~_{k+1} = W - alpha Q_k - beta_k Q_{k-1},
+        // Z~_{k+1} = Q~_{k+1} / pre (and its FP32 copy); partial Z~_{k+1} . Q~_{k+1}
+        const double alpha = reduce_partials_fused(part_a, gridDim.x);
+        const double beta_k = mst[MR_BETA_KP1], beta_km1 = mst[17];
+        {
+            double* __restrict__ qkp1 = sel3(kb.Q, (k + 1) % 3);
+            const double* __restrict__ qk = sel3(kb.Q, k % 3);
+            const double* __restrict__ qkm1 = sel3(kb.Q, (k + 2) % 3);
+            double* __restrict__ zout = sel2(kb.Z, (k + 1) & 1);
+            float* __restrict__ zfout = sel2(kb.Zf, (k + 1) & 1);
+            double acc = 0;
+            for (int64_t n = t0; n < ng.nn; n += nt) {
+                const double m = gm[n];
+                if (m == 0) continue;
+                const double pre = kb.pre[n];
+                float zf[3];
+                for (int c = 0; c < 3; ++c) {
+                    const int64_t i = vidx<NPB>(n, c);
+                    double q = qkp1[i];
+                    q -= alpha * mr_norm(qk[i], beta_k);
+                    q -= beta_k * mr_norm(qkm1[i], beta_km1);
+                    qkp1[i] = q;
+                    const double z = q / pre;
+                    zout[i] = z;
+                    zf[c] = (float)z;
+                    acc += z * q;
+                }
+                if (zfout) reinterpret_cast<float4*>(zfout)[n] = make_float4(zf[0], zf[1], zf[2], 0.f);
+            }
+            acc = block_sum_fused(acc);
+            if (threadIdx.x == 0) part_b[blockIdx.x] = acc;
+        }
+        if (!grid_sync(gs, limit, flags)) return;
+        const double dz = reduce_partials_fused(part_b, gridDim.x);
+        if (threadIdx.x == 0) {
+            double nx[12] = {};
+            mst[18] = mr_givens(mst, alpha, beta_k, dz, nx, pend);
+            for (int i = 0; i < 12; ++i) mst[i] = nx[i];
+            mst[17] = beta_k;
+        }
+        __syncthreads();
+        const double rnorm = mst[18];
+        ++k;
+        const bool go = !(rnorm < local_tol || k >= kmax);
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+            for (int i = 0; i < 12; ++i) sc->mr[k & 1][i] = mst[i];
+            for (int i = 0; i < 5; ++i) sc->pend[i] = pend[i];
+            sc->rnorm = rnorm;
+            sc->krylov_iters += 1;
+            sc->hvp_count += 1;
+            sc->krylov_bodies += 1;
+            if (nit < 64) sc->kcount[nit] += 1;
+            sc->kit = k;
+            if (!go) sc->kactive = 0;
+        }
+        if (!go) return;
+    }
+}
+
 // dv += x (the linear solve's step, with MINRES's deferred last update);
 // vstar = vn + dv on active nodes.
 template <int NPB>
@@ -955,7 +1131,7 @@ __global__ void __launch_bounds__(ND_THREADS) k_newton_step(NodeGeom ng, const d
     float4* __restrict__ vstar_f)
 {
     if (sc->newton_done) return;
-    MrPending pd = mr_pending(kb, sc, sc->kit);
+    MrPending pd = mr_pending(kb, sc->pend, sc->kit);
     pd.on = pd.on && minres;
     for (int64_t n = (int64_t)blockIdx.x * ND_THREADS + threadIdx.x; n < ng.nn; n += (int64_t)gridDim.x * ND_THREADS) {
         const bool act = gm[n] != 0;
@@ -1088,7 +1264,7 @@ template <int NPB>
 __global__ void __launch_bounds__(ND_THREADS) k_admm_dv_update(NodeGeom ng, const double* __restrict__ gm, KrylovBufs kb,
     const double* __restrict__ vn, double* __restrict__ dv, double* __restrict__ vstar, const SolverScalars* __restrict__ sc)
 {
-    const MrPending pd = mr_pending(kb, sc, sc->kit);
+    const MrPending pd = mr_pending(kb, sc->pend, sc->kit);
     for (int64_t n = (int64_t)blockIdx.x * ND_THREADS + threadIdx.x; n < ng.nn; n += (int64_t)gridDim.x * ND_THREADS) {
         const bool act = gm[n] != 0;
         for (int k = 0; k < 3; ++k) {
@@ -1103,8 +1279,9 @@ __global__ void __launch_bounds__(ND_THREADS) k_admm_dv_update(NodeGeom ng, cons
 }
 
 // Ends an ADMM iteration (admmStep loop, AdmmSimulationFoam.h:776-784).
-__global__ void k_admm_advance(SolverScalars* __restrict__ sc, int nmax, cudaGraphConditionalHandle hN, int use_graph)
+__global__ void k_admm_advance(SolverScalars* __restrict__ sc, int nmax, cudaGraphConditionalHandle hN, int use_graph, GridSync* __restrict__ gs)
 {
+    *gs = GridSync{}; // the next persistent solve starts from a clean barrier
     sc->newton_iters += 1;
     const int n = sc->nit + 1;
     sc->nit = n;
@@ -1358,20 +1535,45 @@ int launch_newton_tail(const NewtonLaunch& L, cudaStream_t st, cudaGraphConditio
     Ctx* ctx = L.ctx;
     k_newton_step<NPB><<<L.nb, ND_THREADS, 0, st>>>(L.ng, ctx->gm.as<double>(), L.kb, L.np.minres, ctx->vn.as<double>(), ctx->dv.as<double>(),
         ctx->vstar.as<double>(), L.sc, ctx->mixed ? ctx->vstarf.as<float4>() : nullptr);
-    k_newton_advance<<<1, 1, 0, st>>>(L.sc, L.np.nmax, hN, use_graph, L.np.minres ? nullptr : L.ctx->gsync.as<GridSync>());
+    k_newton_advance<<<1, 1, 0, st>>>(L.sc, L.np.nmax, hN, use_graph, L.ctx->gsync.as<GridSync>());
     g_kernel_launches += 2;
     return ZMPM_OK;
 }
 
-// The persistent CG solve (k_cg_persistent) as one cooperative launch of as
-// many CTAs as fit on the device at once (all co-resident, which the grid
-// barrier needs; the launch fails rather than oversubscribes).  GridSync must
-// be zero.
-template <int NPB>
-int launch_cg_persistent(const NewtonLaunch& L, cudaStream_t st)
+// A persistent Krylov kernel as one cooperative launch of as many CTAs as fit
+// on the device at once (all co-resident, which the grid barrier needs; the
+// launch fails rather than oversubscribes), the grid size found once per
+// kernel.  GridSync must be zero.
+template <class... P, class... A>
+int launch_coop(Ctx* ctx, cudaStream_t st, void (*kern)(P...), A&&... args)
 {
-    Ctx* ctx = L.ctx;
-    using Lay = typename std::conditional<NPB == 32, Layout244, Layout444>::type;
+    int& blocks = ctx->coop_blocks[reinterpret_cast<const void*>(kern)];
+    if (blocks <= 0) {
+        int per_sm = 0, sms = 0;
+        ZMPM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, FUSED_THREADS, 0));
+        ZMPM_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device));
+        blocks = std::min(per_sm * sms, RED_MAX_CTAS);
+        if (blocks <= 0) {
+            ctx->err = "the persistent Krylov kernel does not fit on this device";
+            return ZMPM_CUDA_ERROR;
+        }
+    }
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)blocks);
+    cfg.blockDim = dim3(FUSED_THREADS);
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    ZMPM_CUDA(cudaLaunchKernelEx(&cfg, kern, std::forward<A>(args)...));
+    ++g_kernel_launches;
+    return ZMPM_OK;
+}
+
+static HvpArgs hvp_args(const Ctx* ctx)
+{
     HvpArgs ha;
     ha.group_start = ctx->group_start.as<int32_t>();
     ha.group_nbr = ctx->group_nbr.as<int32_t>();
@@ -1382,35 +1584,61 @@ int launch_cg_persistent(const NewtonLaunch& L, cudaStream_t st)
     ha.cap = ctx->Pcap;
     ha.dx = ctx->cfg.dx;
     ha.G = (int)ctx->G;
-    DevCounters* dc = ctx->counters.as<DevCounters>();
-    auto launch = [&](auto kern) -> int {
-        if (ctx->coop_blocks <= 0) {
-            int per_sm = 0, sms = 0;
-            ZMPM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, FUSED_THREADS, 0));
-            ZMPM_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device));
-            ctx->coop_blocks = std::min(per_sm * sms, RED_MAX_CTAS);
-            if (ctx->coop_blocks <= 0) {
-                ctx->err = "the persistent Krylov kernel does not fit on this device";
-                return ZMPM_CUDA_ERROR;
-            }
+    return ha;
+}
+
+// The persistent CG solve (k_cg_persistent) on the Newton operator.
+template <int NPB>
+int launch_cg_persistent(const NewtonLaunch& L, cudaStream_t st)
+{
+    Ctx* ctx = L.ctx;
+    using Lay = typename std::conditional<NPB == 32, Layout244, Layout444>::type;
+    const HvpArgs ha = hvp_args(ctx);
+    int32_t* flags = &ctx->counters.as<DevCounters>()->flags;
+    const double* gm = ctx->gm.as<double>();
+    const int8_t* col = ctx->collided.as<int8_t>();
+    const double* P6 = ctx->proj.as<double>();
+    GridSync* gs = ctx->gsync.as<GridSync>();
+    if (ctx->mixed)
+        return launch_coop(ctx, st, k_cg_persistent<Lay, float>, L.ng, ha, gm, col, P6, L.dt2, L.kb, L.pA, L.pC, L.sc, L.np.kmax, gs,
+            ctx->spin_limit, flags);
+    return launch_coop(ctx, st, k_cg_persistent<Lay, double>, L.ng, ha, gm, col, P6, L.dt2, L.kb, L.pA, L.pC, L.sc, L.np.kmax, gs,
+        ctx->spin_limit, flags);
+}
+
+// The persistent MINRES solve (k_mr_persistent) on the Newton operator
+// (MIXED: FP32 products on the FP32 copies of Z) or, admm = true, on ADMM's
+// global operator.
+template <int NPB>
+int launch_mr_persistent(const NewtonLaunch& L, cudaStream_t st, bool admm)
+{
+    Ctx* ctx = L.ctx;
+    using Lay = typename std::conditional<NPB == 32, Layout244, Layout444>::type;
+    const HvpArgs ha = hvp_args(ctx);
+    int32_t* flags = &ctx->counters.as<DevCounters>()->flags;
+    const double* gm = ctx->gm.as<double>();
+    const int8_t* col = ctx->collided.as<int8_t>();
+    const double* P6 = ctx->proj.as<double>();
+    GridSync* gs = ctx->gsync.as<GridSync>();
+    const long long lim = ctx->spin_limit;
+    if (admm) {
+        if (ctx->mixed)
+            return launch_coop(ctx, st, k_mr_persistent<Lay, float, double, AdmmOpModel<float>>, L.ng, ha,
+                AdmmOpModel<float>{ ctx->adm_B.as<float>(), ctx->Pcap }, gm, col, P6, L.dt2, L.kb, L.pA, L.pC, L.sc, L.np.kmax, gs, lim, flags);
+        return launch_coop(ctx, st, k_mr_persistent<Lay, double, double, AdmmOpModel<double>>, L.ng, ha,
+            AdmmOpModel<double>{ ctx->adm_B.as<double>(), ctx->Pcap }, gm, col, P6, L.dt2, L.kb, L.pA, L.pC, L.sc, L.np.kmax, gs, lim, flags);
+    }
+    if (ctx->mixed) {
+        if (!L.kb.Zf[0]) {
+            ctx->err = "MIXED MINRES needs the FP32 copies of Z";
+            return ZMPM_BAD_ARG;
         }
-        cudaLaunchConfig_t cfg = {};
-        cfg.gridDim = dim3((unsigned)ctx->coop_blocks);
-        cfg.blockDim = dim3(FUSED_THREADS);
-        cfg.stream = st;
-        cudaLaunchAttribute attr[1];
-        attr[0].id = cudaLaunchAttributeCooperative;
-        attr[0].val.cooperative = 1;
-        cfg.attrs = attr;
-        cfg.numAttrs = 1;
-        ZMPM_CUDA(cudaLaunchKernelEx(&cfg, kern, L.ng, ha, (const double*)ctx->gm.as<double>(), (const int8_t*)ctx->collided.as<int8_t>(),
-            (const double*)ctx->proj.as<double>(), L.dt2, L.kb, L.pA, L.pC, L.sc, L.np.kmax, ctx->gsync.as<GridSync>(), ctx->spin_limit,
-            &dc->flags));
-        ++g_kernel_launches;
-        return ZMPM_OK;
-    };
-    if (ctx->mixed) return launch(k_cg_persistent<Lay, float>);
-    return launch(k_cg_persistent<Lay, double>);
+        return launch_coop(ctx, st, k_mr_persistent<Lay, float, float, HvpModel<float>>, L.ng, ha,
+            HvpModel<float>{ ha.pi, ctx->scratch.as<float>(), ctx->Pcap }, gm, col, P6, L.dt2, L.kb, L.pA, L.pC, L.sc, L.np.kmax, gs, lim,
+            flags);
+    }
+    return launch_coop(ctx, st, k_mr_persistent<Lay, double, double, HvpModel<double>>, L.ng, ha,
+        HvpModel<double>{ ha.pi, ctx->scratch.as<double>(), ctx->Pcap }, gm, col, P6, L.dt2, L.kb, L.pA, L.pC, L.sc, L.np.kmax, gs, lim, flags);
 }
 
 #define ZMPM_CAP(expr)                                                                                                 \
@@ -1427,69 +1655,6 @@ int launch_cg_persistent(const NewtonLaunch& L, cudaStream_t st)
             return ZMPM_CUDA_ERROR;                                                                                    \
         }                                                                                                              \
     } while (0)
-
-// An outer solver loop as one CUDA graph: WHILE(outer){ head; WHILE(Krylov){
-// body }; tail }.  Both loop conditions are set on the device, so the host
-// launches the whole solve once and no Krylov slot is launched idle.
-// head(st, hK), body(st, hK) and tail(st, hN) launch with use_graph = 1.
-template <class Head, class Body, class Tail>
-int loop_graph(Ctx* ctx, Head&& head, Body&& body, Tail&& tail, cudaGraphExec_t* exec_out)
-{
-    cudaStream_t st = ctx->stream;
-    cudaGraph_t g = nullptr;
-    ZMPM_CAP(cudaGraphCreate(&g, 0));
-    cudaGraphConditionalHandle hN, hK;
-    ZMPM_CAP(cudaGraphConditionalHandleCreate(&hN, g, 1, cudaGraphCondAssignDefault));
-    ZMPM_CAP(cudaGraphConditionalHandleCreate(&hK, g, 0, cudaGraphCondAssignDefault));
-    cudaGraphNodeParams pN = {};
-    pN.type = cudaGraphNodeTypeConditional;
-    pN.conditional.handle = hN;
-    pN.conditional.type = cudaGraphCondTypeWhile;
-    pN.conditional.size = 1;
-    cudaGraphNode_t nN;
-    ZMPM_CAP(cudaGraphAddNode(&nN, g, nullptr, 0, &pN));
-    cudaGraph_t bodyN = pN.conditional.phGraph_out[0];
-
-    ZMPM_CAP(cudaStreamBeginCaptureToGraph(st, bodyN, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
-    int rc = head(st, hK);
-    if (rc) {
-        cudaGraph_t tmp;
-        cudaStreamEndCapture(st, &tmp);
-        cudaGraphDestroy(g);
-        return rc;
-    }
-    cudaStreamCaptureStatus cst;
-    const cudaGraphNode_t* deps = nullptr;
-    size_t ndeps = 0;
-    cudaGraph_t capg = nullptr;
-    ZMPM_CAP(cudaStreamGetCaptureInfo(st, &cst, nullptr, &capg, &deps, &ndeps));
-    cudaGraphNodeParams pK = {};
-    pK.type = cudaGraphNodeTypeConditional;
-    pK.conditional.handle = hK;
-    pK.conditional.type = cudaGraphCondTypeWhile;
-    pK.conditional.size = 1;
-    cudaGraphNode_t nK;
-    ZMPM_CAP(cudaGraphAddNode(&nK, capg, deps, ndeps, &pK));
-    ZMPM_CAP(cudaStreamUpdateCaptureDependencies(st, &nK, 1, cudaStreamSetCaptureDependencies));
-    cudaGraph_t bodyK = pK.conditional.phGraph_out[0];
-    rc = tail(st, hN);
-    cudaGraph_t tmp = nullptr;
-    ZMPM_CAP(cudaStreamEndCapture(st, &tmp));
-    if (rc) {
-        cudaGraphDestroy(g);
-        return rc;
-    }
-    ZMPM_CAP(cudaStreamBeginCaptureToGraph(st, bodyK, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
-    rc = body(st, hK);
-    ZMPM_CAP(cudaStreamEndCapture(st, &tmp));
-    if (rc) {
-        cudaGraphDestroy(g);
-        return rc;
-    }
-    ZMPM_CAP(cudaGraphInstantiate(exec_out, g, 0));
-    cudaGraphDestroy(g);
-    return ZMPM_OK;
-}
 
 // A solver loop as one CUDA graph: WHILE(outer){ body(st, hN) }, its
 // condition set on the device.
@@ -1521,29 +1686,25 @@ int while_graph(Ctx* ctx, Body&& body, cudaGraphExec_t* exec_out)
     return ZMPM_OK;
 }
 
-// One Newton iteration with the CG solve as one persistent kernel: update,
-// residual and Krylov start, Newton check, the solve, step and advance.
+// One Newton iteration with its linear solve as one persistent kernel
+// (k_mr_persistent or k_cg_persistent): update, residual and Krylov start,
+// Newton check, the solve, step and advance.
 template <int NPB>
-int launch_newton_iteration_cg(const NewtonLaunch& L, cudaStream_t st, cudaGraphConditionalHandle hN, int use_graph)
+int launch_newton_iteration(const NewtonLaunch& L, cudaStream_t st, cudaGraphConditionalHandle hN, int use_graph)
 {
     int rc = launch_newton_head<NPB>(L, st, 0, 0);
     if (rc) return rc;
-    rc = launch_cg_persistent<NPB>(L, st);
+    rc = L.np.minres ? launch_mr_persistent<NPB>(L, st, false) : launch_cg_persistent<NPB>(L, st);
     if (rc) return rc;
     return launch_newton_tail<NPB>(L, st, hN, use_graph);
 }
 
-// The Newton solve as one graph.
+// The Newton solve as one graph: WHILE(Newton){ iteration }.
 template <int NPB>
 int newton_graph(const NewtonLaunch& L, cudaGraphExec_t* exec_out)
 {
-    if (!L.np.minres)
-        return while_graph(L.ctx, [&](cudaStream_t st, cudaGraphConditionalHandle hN) { return launch_newton_iteration_cg<NPB>(L, st, hN, 1); },
-            exec_out);
-    return loop_graph(
-        L.ctx, [&](cudaStream_t st, cudaGraphConditionalHandle hK) { return launch_newton_head<NPB>(L, st, hK, 1); },
-        [&](cudaStream_t st, cudaGraphConditionalHandle hK) { return launch_krylov_iteration<NPB>(L, st, hK, 1, nullptr, nullptr); },
-        [&](cudaStream_t st, cudaGraphConditionalHandle hN) { return launch_newton_tail<NPB>(L, st, hN, 1); }, exec_out);
+    return while_graph(L.ctx, [&](cudaStream_t st, cudaGraphConditionalHandle hN) { return launch_newton_iteration<NPB>(L, st, hN, 1); },
+        exec_out);
 }
 
 } // namespace
@@ -1597,8 +1758,8 @@ static int newton_impl(Ctx* ctx, const zmpm_solver& s)
     ctx->prof_newton = 0;
     ctx->graph_used = false;
     if (L.ng.nn == 0 || s.newton_max_iterations == 0) return ZMPM_OK;
-    if (!L.np.minres) ZMPM_CUDA(cudaMemsetAsync(ctx->gsync.p, 0, sizeof(GridSync), st));
-    // profiling (per-product events) applies to MINRES, whose products are separate launches
+    ZMPM_CUDA(cudaMemsetAsync(ctx->gsync.p, 0, sizeof(GridSync), st));
+    // profiling: MINRES as separate launches, each product bracketed by events
     const bool prof = ctx->profiling && s.newton_max_iterations <= 64 && L.np.minres;
     if (!prof) {
         // whole solve as one graph with device-side loop conditions
@@ -1726,72 +1887,50 @@ static int admm_impl(Ctx* ctx, const zmpm_solver& s)
     rc = launch_admm_pre(ctx);
     if (rc) return rc;
 
-    auto head = [&](cudaStream_t sm, cudaGraphConditionalHandle hK, int ug) {
+    // one ADMM iteration: collision update, local step and the right-hand
+    // side, the MINRES solve as one persistent kernel, dv / vstar and the dual
+    // update
+    auto iteration = [&](cudaStream_t sm, cudaGraphConditionalHandle hN, int ug) {
         collide(sm, nullptr);
         int r = launch_admm_local(ctx, rho, local_tol);
         if (r) return r;
         r = launch_force_scatter(ctx, ctx->adm_rhs.as<double>());
         if (r) return r;
-        r = launch_admm_op(ctx, ctx->dv.as<double>(), ctx->dv.as<double>(), false, kb.hacc, false);
+        r = launch_admm_op(ctx, ctx->dv.as<double>(), kb.hacc);
         if (r) return r;
         k_admm_start<NPB><<<Lc.nb, ND_THREADS, 0, sm>>>(Lc.ng, ctx->gm.as<double>(), ctx->collided.as<int8_t>(), ctx->proj.as<double>(),
             ctx->adm_rhs.as<double>(), ctx->dv.as<double>(), kb, Lc.pB, Lc.sc);
-        k_krylov_start<NPB><<<1, ND_THREADS, 0, sm>>>(Lc.ng, kb, Lc.np, Lc.pB, Lc.sc, hK, ug);
+        k_krylov_start<NPB><<<1, ND_THREADS, 0, sm>>>(Lc.ng, kb, Lc.np, Lc.pB, Lc.sc, 0, 0);
         g_kernel_launches += 2;
-        return (int)ZMPM_OK;
-    };
-    auto body = [&](cudaStream_t sm, cudaGraphConditionalHandle hK, int ug) {
-        int r = launch_admm_op(ctx, kb.Z[0], kb.Z[1], true, kb.hacc, true);
+        r = launch_mr_persistent<NPB>(Lc, sm, true);
         if (r) return r;
-        k_mr_a<NPB><<<Lc.nb, ND_THREADS, 0, sm>>>(Lc.ng, ctx->gm.as<double>(), ctx->collided.as<int8_t>(), ctx->proj.as<double>(), 1.0, kb,
-            Lc.pA, Lc.sc);
-        k_mr_b<NPB><<<Lc.nb, ND_THREADS, 0, sm>>>(Lc.ng, ctx->gm.as<double>(), kb, Lc.pA, Lc.pC, Lc.sc, Lc.np.kmax, hK, ug);
-        g_kernel_launches += 2;
-        return (int)ZMPM_OK;
-    };
-    auto tail = [&](cudaStream_t sm, cudaGraphConditionalHandle hN, int ug) {
         k_admm_dv_update<NPB><<<Lc.nb, ND_THREADS, 0, sm>>>(Lc.ng, ctx->gm.as<double>(), kb, ctx->vn.as<double>(), ctx->dv.as<double>(),
             ctx->vstar.as<double>(), Lc.sc);
         ++g_kernel_launches;
-        int r = launch_admm_dual(ctx, rho);
+        r = launch_admm_dual(ctx, rho);
         if (r) return r;
-        k_admm_advance<<<1, 1, 0, sm>>>(Lc.sc, Lc.np.nmax, hN, ug);
+        k_admm_advance<<<1, 1, 0, sm>>>(Lc.sc, Lc.np.nmax, hN, ug, ctx->gsync.as<GridSync>());
         ++g_kernel_launches;
         return (int)ZMPM_OK;
     };
 
     if (s.admm_iterations > 0) {
+        ZMPM_CUDA(cudaMemsetAsync(ctx->gsync.p, 0, sizeof(GridSync), st));
         if (!ctx->profiling) {
             cudaGraphExec_t exec = nullptr;
             const int64_t launches0 = g_kernel_launches;
-            rc = loop_graph(
-                ctx, [&](cudaStream_t sm, cudaGraphConditionalHandle hK) { return head(sm, hK, 1); },
-                [&](cudaStream_t sm, cudaGraphConditionalHandle hK) { return body(sm, hK, 1); },
-                [&](cudaStream_t sm, cudaGraphConditionalHandle hN) { return tail(sm, hN, 1); }, &exec);
+            rc = while_graph(ctx, [&](cudaStream_t sm, cudaGraphConditionalHandle hN) { return iteration(sm, hN, 1); }, &exec);
             if (rc) return rc;
             cudaError_t e = cudaGraphLaunch(exec, st);
-            g_kernel_launches = launches0; // counted per executed body after the substep
+            g_kernel_launches = launches0; // counted per executed iteration after the substep
             ctx->graph_used = true;
             if (ctx->graph_exec) cudaGraphExecDestroy(ctx->graph_exec);
             ctx->graph_exec = exec;
             ZMPM_CUDA(e);
         }
         else {
-            // host-driven: the Krylov loop polls the active flag every 8 iterations
             for (int it = 0; it < s.admm_iterations; ++it) {
-                rc = head(st, 0, 0);
-                if (rc) return rc;
-                for (int k = 0; k < Lc.np.kmax; k += 8) {
-                    for (int j = 0; j < 8 && k + j < Lc.np.kmax; ++j) {
-                        rc = body(st, 0, 0);
-                        if (rc) return rc;
-                    }
-                    SolverScalars hs;
-                    ZMPM_CUDA(cudaMemcpyAsync(&hs, Lc.sc, sizeof(hs), cudaMemcpyDeviceToHost, st));
-                    ZMPM_CUDA(cudaStreamSynchronize(st));
-                    if (!hs.kactive) break;
-                }
-                rc = tail(st, 0, 0);
+                rc = iteration(st, 0, 0);
                 if (rc) return rc;
                 ZMPM_CUDA(cudaGetLastError());
             }

@@ -11,7 +11,7 @@
 //            pass (gather of grad v, F, stress and Hessian scratch, force scatter)
 //  k_hvp_fused  MpmForceBase::addScaledForceDifferential (MpmForceBase.cpp:259-302):
 //            G2P of grad(dv), dS = V0 dP Fn^T, P2G of dS grad w in one pass
-//  k_hvp_scatter  the scatter half alone (ADMM's global operator)
+//  k_op_fused  ADMM's global operator in the same one-pass form
 //  k_g2p     gridToParticlesHelper<APIC> (MpmSimulationBase.cpp:906-1016) +
 //            evolveStrain + applyPlasticity (:1018-1030)
 #include "admm.cuh"
@@ -422,8 +422,10 @@ __global__ void __launch_bounds__(XF_THREADS) k_force(const int32_t* __restrict_
     const TS inv_dx = TS(1.0 / dx);
     const int s0 = group_start[g], s1 = group_start[g + 1];
     build_cell_layout<L>(cl, base, s0, s1);
-    // One cell per thread (see k_hvp_scatter): FP32 keeps all 81 sums in
-    // registers, FP64 one force component per pass.
+    // Thread -> one cell of the page and every (blockDim/NPB)-th particle of
+    // it; the cell's particles share one 27-node stencil, so their terms are
+    // summed in registers and added to the shared window once per thread (FP32
+    // keeps all 81 sums in registers, FP64 one force component per pass).
     const int ce = threadIdx.x % NPB;
     const int lx = ce >> (L::YB + L::ZB), ly = (ce >> L::ZB) & (L::BY - 1), lz = ce & (L::BZ - 1);
     const int cnt = cl.cnt[ce], first = s0 + cl.start[ce];
@@ -488,92 +490,6 @@ __global__ void __launch_bounds__(XF_THREADS) k_force(const int32_t* __restrict_
     flush_window<3, 3, NPB>(acc, nbr, facc, nullptr);
 }
 
-// ------------------------------------------------------------------ HVP ----
-// out += sum_p dstress_p grad w_ip with the layered per-cell scatter (the ADMM
-// global operator, whose per-particle products k_admm_op writes to dstress).
-template <class L, class TH>
-__global__ void __launch_bounds__(XF_THREADS) k_hvp_scatter(const int32_t* __restrict__ group_start, const int32_t* __restrict__ group_nbr,
-    int64_t cap, const short4* __restrict__ base, double dx, const TH* __restrict__ frac, const TH* __restrict__ dstress,
-    double* __restrict__ out, const SolverScalars* __restrict__ sc)
-{
-    if (sc && (sc->newton_done || !sc->kactive)) return;
-    constexpr int NPB = L::NPB;
-    __shared__ __align__(16) TH acc[8 * 3 * NPB];
-    __shared__ int32_t nbr[8];
-    __shared__ CellLayout<L> cl;
-    const int g = blockIdx.x;
-    if (threadIdx.x < 8) nbr[threadIdx.x] = group_nbr[8 * g + threadIdx.x];
-    zero_window<3, NPB>(acc);
-    const TH inv_dx = TH(1.0 / dx);
-    const int s0 = group_start[g], s1 = group_start[g + 1];
-    build_cell_layout<L>(cl, base, s0, s1);
-    // Thread -> one cell (ce) and every (blockDim/NPB)-th particle of it: all of
-    // its particles share the cell's 27 nodes, so their contributions are summed
-    // in registers and added to the window once.
-    const int ce = threadIdx.x % NPB;
-    const int lx = ce >> (L::YB + L::ZB), ly = (ce >> L::ZB) & (L::BY - 1), lz = ce & (L::BZ - 1);
-    const int cnt = cl.cnt[ce], first = s0 + cl.start[ce];
-    // FP32 keeps all 81 sums in registers (one pass); FP64 one component per pass.
-    constexpr int NCP = sizeof(TH) == 4 ? 3 : 1;
-#pragma unroll 1
-    for (int c0 = 0; c0 < 3; c0 += NCP) {
-        TH a[27][NCP];
-#pragma unroll
-        for (int n = 0; n < 27; ++n)
-#pragma unroll
-            for (int c = 0; c < NCP; ++c) a[n][c] = TH(0);
-        for (int r = threadIdx.x / NPB; r < cnt; r += blockDim.x / NPB) {
-            const int s = first + r;
-            TH w[3][3], dwr[3][3];
-#pragma unroll
-            for (int d = 0; d < 3; ++d) bspline(frac[d * cap + s], w[d], dwr[d]);
-            TH row[NCP][3];
-#pragma unroll
-            for (int c = 0; c < NCP; ++c)
-#pragma unroll
-                for (int q2 = 0; q2 < 3; ++q2) row[c][q2] = dstress[(3 * (c0 + c) + q2) * cap + s];
-            if constexpr (NCP == 3) {
-                // components 0 and 1 as one packed FP32 pair (same per-component
-                // rounding as the scalar fma), component 2 scalar
-                const float2 r0 = make_float2(row[0][0], row[1][0]), r1 = make_float2(row[0][1], row[1][1]),
-                             r2 = make_float2(row[0][2], row[1][2]);
-                for_stencil<L>(lx, ly, lz, w, dwr, inv_dx, [&](int, int, int i, int j, int k, TH, const TH* dw) {
-                    const int n = 9 * i + 3 * j + k;
-                    float2 t = __fmul2_rn(r0, make_float2(dw[0], dw[0]));
-                    t = __ffma2_rn(r1, make_float2(dw[1], dw[1]), t);
-                    t = __ffma2_rn(r2, make_float2(dw[2], dw[2]), t);
-                    const float2 acc = __fadd2_rn(make_float2(a[n][0], a[n][1]), t);
-                    a[n][0] = acc.x;
-                    a[n][1] = acc.y;
-                    a[n][2] += row[2][0] * dw[0] + row[2][1] * dw[1] + row[2][2] * dw[2];
-                });
-            }
-            else
-                for_stencil<L>(lx, ly, lz, w, dwr, inv_dx, [&](int, int, int i, int j, int k, TH, const TH* dw) {
-                    const int n = 9 * i + 3 * j + k;
-#pragma unroll
-                    for (int c = 0; c < NCP; ++c) a[n][c] += row[c][0] * dw[0] + row[c][1] * dw[1] + row[c][2] * dw[2];
-                });
-        }
-        if (threadIdx.x / NPB < cnt) {
-#pragma unroll
-            for (int i = 0; i < 3; ++i)
-#pragma unroll
-                for (int j = 0; j < 3; ++j)
-#pragma unroll
-                    for (int k = 0; k < 3; ++k) {
-                        int e;
-                        const int t = win_slot<L>(lx + i, ly + j, lz + k, e);
-                        TH* dst = acc + t * 3 * NPB + e;
-#pragma unroll
-                        for (int c = 0; c < NCP; ++c) atomicAdd(dst + (c0 + c) * NPB, a[9 * i + 3 * j + k][c]);
-                    }
-        }
-    }
-    __syncthreads();
-    flush_window<3, 3, NPB>(acc, nbr, out, nullptr);
-}
-
 // ------------------------------------------------------- fused products ----
 // The Hessian-vector product (hvp.cuh) as one CTA per particle group.
 template <class L, class T, class TX, int CH>
@@ -585,7 +501,23 @@ __global__ void __launch_bounds__(FUSED_THREADS) k_hvp_fused(const int32_t* __re
     if (sc && (sc->newton_done || !sc->kactive)) return;
     __shared__ HvpSmem<L, T, TX, CH> hs;
     const TX* x = (alt && sc && (sc->kit & 1)) ? x1 : x0;
-    hvp_group<L, T, TX, CH>(hs, blockIdx.x, group_start, group_nbr, pi, cap, base, dx, frac, scr, x, out, flags);
+    const int g = blockIdx.x;
+    hvp_group<L, T, TX, CH>(hs, g, group_start[g], group_start[g + 1], group_nbr, HvpModel<T>{ pi, scr, cap }, cap, base, dx, frac, x, out,
+        flags);
+}
+
+// ADMM's global operator (the matrix-free product of dvStep's MINRES,
+// AdmmSimulationFoam.h:167-170 with the B of initMultiplierAndPreconditioner):
+// out += sum_p (grad(x)_p B_p) grad w_ip, one CTA per particle group.
+template <class L, class T, int CH>
+__global__ void __launch_bounds__(FUSED_THREADS) k_op_fused(const int32_t* __restrict__ group_start, const int32_t* __restrict__ group_nbr,
+    int64_t cap, const short4* __restrict__ base, double dx, const T* __restrict__ frac, const T* __restrict__ B, const double* __restrict__ x,
+    double* __restrict__ out, int32_t* __restrict__ flags)
+{
+    __shared__ HvpSmem<L, T, double, CH> hs;
+    const int g = blockIdx.x;
+    hvp_group<L, T, double, CH>(hs, g, group_start[g], group_start[g + 1], group_nbr, AdmmOpModel<T>{ B, cap }, cap, base, dx, frac, x, out,
+        flags);
 }
 
 // MpmForceBase::updatePositionBasedState + rasterizeForceToTVStack
@@ -1022,21 +954,26 @@ int launch_force_scatter(Ctx* ctx, double* out, bool mls)
     return ctx->layout == 1 ? force_scatter_impl<Layout244, double>(ctx, out, mls) : force_scatter_impl<Layout444, double>(ctx, out, mls);
 }
 
-template <class L, class TH>
-static int hvp_scatter_impl(Ctx* ctx, double* out, bool gated)
+// out += sum_p (grad(x)_p B_p) grad w_ip (ADMM's global operator).
+template <class L>
+static int admm_op_impl(Ctx* ctx, const double* x, double* out)
 {
-    k_hvp_scatter<L, TH><<<(unsigned)ctx->G, XF_THREADS, 0, ctx->stream>>>(ctx->group_start.as<int32_t>(), ctx->group_nbr.as<int32_t>(), ctx->Pcap,
-        ctx->base.as<short4>(), ctx->cfg.dx, ctx->frac.as<TH>(), ctx->dstress.as<TH>(), out, gated ? ctx->scal.as<SolverScalars>() : nullptr);
+    DevCounters* dc = ctx->counters.as<DevCounters>();
+    if (ctx->mixed)
+        k_op_fused<L, float, fused_chunk<float>()><<<(unsigned)ctx->G, FUSED_THREADS, 0, ctx->stream>>>(ctx->group_start.as<int32_t>(),
+            ctx->group_nbr.as<int32_t>(), ctx->Pcap, ctx->base.as<short4>(), ctx->cfg.dx, ctx->frac.as<float>(), ctx->adm_B.as<float>(), x, out,
+            &dc->flags);
+    else
+        k_op_fused<L, double, fused_chunk<double>()><<<(unsigned)ctx->G, FUSED_THREADS, 0, ctx->stream>>>(ctx->group_start.as<int32_t>(),
+            ctx->group_nbr.as<int32_t>(), ctx->Pcap, ctx->base.as<short4>(), ctx->cfg.dx, ctx->frac.as<double>(), ctx->adm_B.as<double>(), x,
+            out, &dc->flags);
     ++g_kernel_launches;
     return ZMPM_OK;
 }
-// out += sum_p dstress_p grad w_ip; gated: skipped while the linear solve is inactive.
-int launch_hvp_scatter(Ctx* ctx, double* out, bool gated)
+int launch_admm_op(Ctx* ctx, const double* x, double* out)
 {
     if (!ctx->G) return ZMPM_OK;
-    if (ctx->mixed)
-        return ctx->layout == 1 ? hvp_scatter_impl<Layout244, float>(ctx, out, gated) : hvp_scatter_impl<Layout444, float>(ctx, out, gated);
-    return ctx->layout == 1 ? hvp_scatter_impl<Layout244, double>(ctx, out, gated) : hvp_scatter_impl<Layout444, double>(ctx, out, gated);
+    return ctx->layout == 1 ? admm_op_impl<Layout244>(ctx, x, out) : admm_op_impl<Layout444>(ctx, x, out);
 }
 
 template <class L>
