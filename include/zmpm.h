@@ -433,6 +433,20 @@ int zmpm_calculate_dt(zmpm_ctx* ctx, double max_dt, double* dt);
 int zmpm_write_state(zmpm_ctx* ctx, const char* path);
 int zmpm_read_state(zmpm_ctx* ctx, const char* path);
 
+/* The reference's restart directory (SimulationBase::write, read and
+   outputFileName, SimulationBase.h:146-199).  write_restart creates
+   output_dir if needed and writes there restart_<frame>.dat
+   (restart_<frame>_<substep>.dat when substep > 0; zmpm_write_state's
+   format), then last_written.txt holding the frame and binary_ver.txt
+   holding ZMPM_BINARY_VER.  read_restart reads binary_ver.txt (0 when it is
+   missing) and fails with ZMPM_BAD_ARG when it is newer than
+   ZMPM_BINARY_VER, stores last_written.txt's frame in *last_written_frame
+   (-1 when missing; the reference warns when it is below `frame`, stale
+   data), then reads the state file.  last_written_frame may be NULL. */
+#define ZMPM_BINARY_VER 1
+int zmpm_write_restart(zmpm_ctx* ctx, const char* output_dir, int32_t frame, int32_t substep);
+int zmpm_read_restart(zmpm_ctx* ctx, const char* output_dir, int32_t frame, int32_t substep, int32_t* last_written_frame);
+
 /* Particle output in Houdini's binary geometry point format (BGEO version 5,
    uncompressed, big-endian), as the reference writes it through Partio:
    writePartio (PartioIO.h:138-182) stores "position"; FractureSimulation's

@@ -34,3 +34,12 @@ def test_status_strings_need_no_device():
     lib = abi.Lib(build.build(), "zmpm_")
     assert lib.status_string(0) == b"ok"
     assert b"CFL" in lib.status_string(1)
+
+
+def test_restart_file_names_follow_the_reference():
+    """SimulationBase::outputFileName (SimulationBase.h:192-199)."""
+    from ziran2019_b200 import mpm
+    assert mpm.MpmSimulation.outputFileName(7) == "restart_7.dat"
+    assert mpm.MpmSimulation.outputFileName(7, 0) == "restart_7.dat"
+    assert mpm.MpmSimulation.outputFileName(7, 3) == "restart_7_3.dat"
+    assert mpm.MpmSimulation.outputFileName(0, 1, name="state", suffix=".bin") == "state_0_1.bin"

@@ -81,6 +81,39 @@ def test_restart_rejects_mismatch_and_garbage(cuda_lib, tmp_path):
     np.testing.assert_array_equal(b.getParticles()["X"], x0)  # a failed read leaves the scene
 
 
+def test_restart_directory_layout(cuda_lib, tmp_path):
+    """SimulationBase::write / read (SimulationBase.h:146-199): the state file
+    restart_<frame>[_<substep>].dat beside last_written.txt and binary_ver.txt;
+    a newer binary version is refused, a stale last frame warns."""
+    a = scene()
+    run(a, 2)
+    out = tmp_path / "out"
+    a.writeRestart(out, 2)
+    a.writeRestart(out, 3, substep=4)
+    assert sorted(p.name for p in out.iterdir()) == ["binary_ver.txt", "last_written.txt", "restart_2.dat", "restart_3_4.dat"]
+    assert (out / "last_written.txt").read_text().strip() == "3"
+    assert (out / "binary_ver.txt").read_text().strip() == str(abi.BINARY_VER)
+    assert mpm.MpmSimulation.outputFileName(3, 4) == "restart_3_4.dat"
+    assert mpm.MpmSimulation.outputFileName(2) == "restart_2.dat"
+    b = scene()
+    assert b.readRestart(out, 2) == 3
+    for k in ("X", "V", "C", "F"):
+        np.testing.assert_array_equal(b.getParticles()[k], a.getParticles()[k])
+    # the last written frame (3) is before frame 5: stale data warns
+    (out / "restart_5.dat").write_bytes((out / "restart_2.dat").read_bytes())
+    with pytest.warns(UserWarning, match="stale"):
+        b.readRestart(out, 5)
+    # data of a newer binary version is refused, the scene kept
+    (out / "binary_ver.txt").write_text(str(abi.BINARY_VER + 1))
+    x0 = b.getParticles()["X"].copy()
+    with pytest.raises(abi.ZmpmError, match="newer"):
+        b.readRestart(out, 2)
+    np.testing.assert_array_equal(b.getParticles()["X"], x0)
+    # a missing version file reads as version 0 (accepted)
+    (out / "binary_ver.txt").unlink()
+    assert b.readRestart(out, 2) == 3
+
+
 def read_bgeo(path):
     """Reader of the uncompressed BGEO v5 point files the library writes."""
     data = open(path, "rb").read()

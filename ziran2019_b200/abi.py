@@ -183,6 +183,8 @@ _PRODUCT_ONLY = {
     "default_solver": (None, [C.POINTER(Solver), C.c_int32, C.c_int32]),
     "write_state": (C.c_int, [C.c_void_p, C.c_char_p]),
     "read_state": (C.c_int, [C.c_void_p, C.c_char_p]),
+    "write_restart": (C.c_int, [C.c_void_p, C.c_char_p, C.c_int32, C.c_int32]),
+    "read_restart": (C.c_int, [C.c_void_p, C.c_char_p, C.c_int32, C.c_int32, C.POINTER(C.c_int32)]),
     "write_bgeo": (C.c_int, [C.c_void_p, C.c_char_p, C.c_int32]),
     "particles_to_grid": (C.c_int, [C.c_void_p, C.c_double, C.POINTER(Solver)]),
     "backward_euler_step": (C.c_int, [C.c_void_p, C.POINTER(Stats)]),
@@ -235,6 +237,8 @@ def ptr(a, ctype=C.c_double):
         return None
     return a.ctypes.data_as(C.POINTER(ctype))
 
+
+BINARY_VER = 1  # ZMPM_BINARY_VER: the restart format version in binary_ver.txt
 
 _PKG_DIR = os.path.dirname(os.path.abspath(__file__))
 PRODUCT_LIB_PATH = os.path.join(_PKG_DIR, "lib", "libzmpm.so")

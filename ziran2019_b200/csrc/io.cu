@@ -9,6 +9,11 @@
 //   (0 f64, 1 u8, 2 i32), int32 components, P * components values.
 // Reading matches fields by name and requires every field the library knows.
 //
+// Restart directory (the reference's layout, SimulationBase.h:146-199): the
+// state file restart_<frame>.dat (restart_<frame>_<substep>.dat for
+// substep > 0), last_written.txt holding the frame, binary_ver.txt holding
+// ZMPM_BINARY_VER.
+//
 // BGEO (Houdini binary geometry, version 5, big-endian) with points only:
 //   int32 magic 'Bgeo', char 'V', int32 5, int32 points, primitives (0), point
 //   groups (0), primitive groups (0), point attributes, vertex attributes (0),
@@ -21,9 +26,11 @@
 #include <cfloat>
 #include <cmath>
 #include <cstdio>
+#include <cerrno>
 #include <cstring>
 #include <exception>
 #include <string>
+#include <sys/stat.h>
 #include <vector>
 
 #include "internal.cuh"
@@ -520,6 +527,72 @@ int zmpm_calculate_dt(zmpm_ctx* ctx, double max_dt, double* dt)
     }
     *dt = v ? ctx->cfg.cfl * ctx->cfg.dx / v : max_dt;
     return ZMPM_OK;
+}
+
+// SimulationBase::outputFileName (SimulationBase.h:192-199).
+static std::string restart_path(const char* dir, int32_t frame, int32_t substep)
+{
+    std::string p = std::string(dir) + "/restart_" + std::to_string(frame);
+    if (substep > 0) p += "_" + std::to_string(substep);
+    return p + ".dat";
+}
+
+static bool write_text(const std::string& path, long long v)
+{
+    FILE* f = std::fopen(path.c_str(), "w");
+    if (!f) return false;
+    const bool ok = std::fprintf(f, "%lld", v) > 0;
+    return (std::fclose(f) == 0) && ok;
+}
+
+// The integer in a text file; false when the file is missing or holds none.
+static bool read_text(const std::string& path, long long& v)
+{
+    FILE* f = std::fopen(path.c_str(), "r");
+    if (!f) return false;
+    const bool ok = std::fscanf(f, "%lld", &v) == 1;
+    std::fclose(f);
+    return ok;
+}
+
+int zmpm_write_restart(zmpm_ctx* ctx, const char* output_dir, int32_t frame, int32_t substep)
+{
+    if (!ctx || !output_dir || frame < 0 || substep < 0) return ZMPM_BAD_ARG;
+    struct stat sb;
+    if (stat(output_dir, &sb) != 0) {
+        if (mkdir(output_dir, 0755) != 0 && errno != EEXIST) {
+            ctx->err = std::string("cannot create ") + output_dir;
+            return ZMPM_BAD_ARG;
+        }
+    }
+    else if (!S_ISDIR(sb.st_mode)) {
+        ctx->err = std::string(output_dir) + " is not a directory";
+        return ZMPM_BAD_ARG;
+    }
+    int rc = zmpm_write_state(ctx, restart_path(output_dir, frame, substep).c_str());
+    if (rc) return rc;
+    const std::string d(output_dir);
+    if (!write_text(d + "/last_written.txt", frame) || !write_text(d + "/binary_ver.txt", ZMPM_BINARY_VER)) {
+        ctx->err = "cannot write last_written.txt / binary_ver.txt in " + d;
+        return ZMPM_BAD_ARG;
+    }
+    return ZMPM_OK;
+}
+
+int zmpm_read_restart(zmpm_ctx* ctx, const char* output_dir, int32_t frame, int32_t substep, int32_t* last_written_frame)
+{
+    if (!ctx || !output_dir || frame < 0 || substep < 0) return ZMPM_BAD_ARG;
+    const std::string d(output_dir);
+    long long ver = 0, last = -1;
+    if (!read_text(d + "/binary_ver.txt", ver)) ver = 0; // as the reference: a missing version file reads as 0
+    if (ver > ZMPM_BINARY_VER) {
+        ctx->err = "the restart data is of binary version " + std::to_string(ver) + ", newer than this library's " +
+                   std::to_string(ZMPM_BINARY_VER);
+        return ZMPM_BAD_ARG;
+    }
+    if (!read_text(d + "/last_written.txt", last)) last = -1;
+    if (last_written_frame) *last_written_frame = (int32_t)last;
+    return zmpm_read_state(ctx, restart_path(output_dir, frame, substep).c_str());
 }
 
 } // extern "C"

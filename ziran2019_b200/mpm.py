@@ -13,6 +13,8 @@ Names follow the reference so that scene code reads the same:
 Every call goes through the CUDA library (`abi.product_lib()`); a missing
 library raises instead of falling back to anything else.
 """
+import warnings
+
 import numpy as np
 
 from . import abi
@@ -577,6 +579,27 @@ class MpmSimulation:
     def read(self, path):
         """Replaces the scene with a restart file written by `write`."""
         self._call("read_state", str(path).encode())
+
+    @staticmethod
+    def outputFileName(frame, substep=0, name="restart", suffix=".dat"):
+        """SimulationBase::outputFileName (SimulationBase.h:192-199)."""
+        return f"{name}_{frame}" + (f"_{substep}" if substep > 0 else "") + suffix
+
+    def writeRestart(self, output_dir, frame, substep=0):
+        """SimulationBase::write in the reference's restart layout:
+        output_dir/restart_<frame>[_<substep>].dat, last_written.txt (the frame)
+        and binary_ver.txt (BINARY_VER)."""
+        self._call("write_restart", str(output_dir).encode(), int(frame), int(substep))
+
+    def readRestart(self, output_dir, frame, substep=0):
+        """SimulationBase::read: fails on restart data of a newer binary version;
+        warns, as the reference does, when last_written.txt holds a frame before
+        `frame` (stale data).  Returns that last written frame (-1 if missing)."""
+        last = abi.C.c_int32(-1)
+        self._call("read_restart", str(output_dir).encode(), int(frame), int(substep), abi.C.byref(last))
+        if last.value < frame:
+            warnings.warn(f"Frame {frame} is after the last written frame {last.value}. Could be reading stale data")
+        return last.value
 
     def writePartio(self, path, velocity=False, phase_field=False):
         """BGEO point file with "position" (+ "v", + "pf" / "sigmaC")."""
