@@ -33,7 +33,8 @@ from ziran2019_b200 import workloads  # noqa: E402
 
 METRIC = "implicit MPM substeps/sec at 1M particles, mixed vs FP64 GPU, at <=1e-6 rel err"
 HVP_WORDS = 22  # compulsory words per particle of one Hessian-vector product: X(3), Fn(9), F(9), V0(1)
-HVP_KERNELS = ("k_hvp_fused",)  # the kernel of one Hessian-vector product
+KRYLOV_NODE_WORDS = 27  # compulsory FP64 words per active node of one MINRES iteration's node passes
+SOLVE_KERNELS = ("k_mr_persistent",)  # the persistent linear solve (one launch per Newton iteration)
 FD_STEPS = (1e-3, 1e-4, 1e-5)  # finite-difference steps of the rollout gradient check, relative to the parameter scale
 
 
@@ -128,9 +129,10 @@ def run_workload(args, world, rank):
         for _ in range(args.warmup):
             rc = sims[p].advanceOneTimeStep(dt)
             assert rc == 0, (p, rc, sims[p].last_stats)
-    ms64, st64 = timed_steps(sims["fp64"], args.steps, world, dt=dt)
     clocks = Clocks(int(os.environ.get("LOCAL_RANK", "0")))
     clocks.start()
+    time.sleep(1.0)
+    ms64, st64 = timed_steps(sims["fp64"], args.steps, world, dt=dt)
     ms_mx, st_mx = timed_steps(sims["mixed"], args.steps, world, dt=dt)
     clk = clocks.stop()
     x64 = sims["fp64"].getParticles()["X"]
@@ -356,9 +358,8 @@ def accuracy_vs_oracle(states, ref):
 
 
 def ncu_traffic(path, kernels):
-    """DRAM bytes (read + write) per launch of `kernels`, summed, from an ncu CSV
-    (--metrics dram__bytes_read.sum,dram__bytes_write.sum --csv) of the same
-    workload: the mean over the captured launches of each kernel."""
+    """DRAM bytes (read + write) of `kernels` summed over every captured launch,
+    from an ncu CSV (--metrics dram__bytes_read.sum,dram__bytes_write.sum --csv)."""
     import csv
     per = {}
     with open(path) as f:
@@ -367,13 +368,12 @@ def ncu_traffic(path, kernels):
     ik, im, iv, iu = head.index("Kernel Name"), head.index("Metric Name"), head.index("Metric Value"), head.index("Metric Unit")
     scale = {"byte": 1, "Kbyte": 1e3, "Mbyte": 1e6, "Gbyte": 1e9, "KB": 1e3, "MB": 1e6, "GB": 1e9, "B": 1}
     for r in rows[1:]:
-        name = r[ik].split("<")[0].split("(")[0].strip()
+        name = r[ik].split("<")[0].split("(")[0].replace("void ", "").strip().split("::")[-1]
         if name in kernels and r[im] in ("dram__bytes_read.sum", "dram__bytes_write.sum"):
             per.setdefault(name, []).append(float(r[iv].replace(",", "")) * scale.get(r[iu], 1))
     if not per:
         return None
-    # read and write rows alternate per launch: sum per kernel, divide by launches
-    return sum(sum(v) / (len(v) / 2) for v in per.values())
+    return sum(sum(v) for v in per.values())
 
 
 def run_reference(args, world, rank):
@@ -432,8 +432,10 @@ def main():
     ap.add_argument("--fd-directions", type=int, default=16, help="finite-difference directions of the rollout gradient check")
     ap.add_argument("--rollout-mixed-tol", type=float, default=1e-12, help="Newton tolerance of the mixed rollout forward")
     ap.add_argument("--ncu-csv", default=None,
-                    help="ncu CSV (dram__bytes_read.sum, dram__bytes_write.sum) of the product kernels of this workload: "
-                         "fills roofline.traffic")
+                    help="ncu CSV (dram__bytes_read.sum, dram__bytes_write.sum) of every persistent-solve launch of a run of "
+                         "this workload: fills roofline.traffic (per Krylov iteration)")
+    ap.add_argument("--ncu-iterations", type=int, default=None,
+                    help="Krylov iterations the launches in --ncu-csv ran")
     ap.add_argument("--ncu-particles", type=int, default=None,
                     help="particles of the workload that --ncu-csv captured (its traffic is scaled to this run by particle count)")
     args = ap.parse_args()
@@ -473,13 +475,16 @@ def main():
         _, stp = timed_steps(sims[args.only], 2, world, profile=True)
         if rank == 0:
             print(json.dumps({"only": args.only, "particles": P, "ms_per_step": ms / args.steps, "host_loop": args.host_loop,
-                              "hvp_ms": sum(s["ms_hvp"] for s in stp) / max(1, sum(s["hvp_timed"] for s in stp)),
+                              "iteration_ms": sum(s["ms_hvp"] for s in stp) / max(1, sum(s["hvp_timed"] for s in stp)),
                               "launches_per_step": st[-1]["kernel_launches"], "newton_krylov": [st[-1]["newton_iterations"], st[-1]["krylov_iterations"]]}),
                   flush=True)
         return
-    ms64, st64 = timed_steps(sims["fp64"], args.steps, world)
+    # nvidia-smi samples through both timed regions; it starts a second ahead
+    # so that its start-up is outside them
     clocks = Clocks(dev)
     clocks.start()
+    time.sleep(1.0)
+    ms64, st64 = timed_steps(sims["fp64"], args.steps, world)
     ms_mx, st_mx = timed_steps(sims["mixed"], args.steps, world)
     clk = clocks.stop()
     # second timed region with each Hessian-vector product bracketed by CUDA
@@ -489,26 +494,35 @@ def main():
     value = world * args.steps / (ms_mx / 1e3)
     fp64_value = world * args.steps / (ms64 / 1e3)
 
-    # dominant kernel: the Hessian-vector product
-    hvp_ms = sum(s["ms_hvp"] for s in st_prof)
-    hvp_n = sum(s["hvp_timed"] for s in st_prof)
-    nodes = st_prof[-1]["num_blocks"] * 64
-    hvp_bytes = P * HVP_WORDS * 4 + nodes * 3 * 4 * 2
+    # dominant kernel: the persistent MINRES solve (one launch per Newton
+    # iteration), measured per Krylov iteration: one Hessian-vector product
+    # (HVP_WORDS per particle in FP32) and the node passes (KRYLOV_NODE_WORDS
+    # FP64 words per active node)
+    solve_ms = sum(s["ms_hvp"] for s in st_prof)
+    iters = sum(s["hvp_timed"] for s in st_prof)
+    nodes = st_prof[-1]["num_nodes"]
+    iter_bytes = P * HVP_WORDS * 4 + nodes * KRYLOV_NODE_WORDS * 8
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
     except OSError:
         pass
     peak = float(peaks.get("hbm_gbs", 6650.0))
-    achieved = hvp_bytes / (hvp_ms / hvp_n / 1e3) / 1e9 if hvp_n else None
-    traffic = ncu_traffic(args.ncu_csv, HVP_KERNELS) if args.ncu_csv else None
+    achieved = iter_bytes / (solve_ms / iters / 1e3) / 1e9 if iters else None
+    traffic = None
+    if args.ncu_csv and args.ncu_iterations:
+        t = ncu_traffic(args.ncu_csv, SOLVE_KERNELS)
+        if t is not None:
+            traffic = t / args.ncu_iterations * (P / args.ncu_particles if args.ncu_particles else 1.0)
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": achieved / peak if achieved else None,
-                "traffic": traffic * P / args.ncu_particles if traffic is not None and args.ncu_particles else traffic,
-                "traffic_source": (f"ncu dram__bytes_read+write per product, {args.ncu_csv}" if traffic is not None
-                                   else "no ncu capture in this run"),
-                "kernel": "Hessian-vector product (" + " + ".join(HVP_KERNELS) + ")", "bytes_per_launch": hvp_bytes,
-                "avg_launch_ms": hvp_ms / hvp_n if hvp_n else None, "peak_source": "measured" if peaks else "fallback"}
+                "frac": achieved / peak if achieved else None, "traffic": traffic,
+                "traffic_source": (f"ncu dram__bytes_read+write of every k_mr_persistent launch in {args.ncu_csv}, per Krylov "
+                                   f"iteration ({args.ncu_iterations} iterations), scaled by particle count"
+                                   if traffic is not None else "no ncu capture in this run"),
+                "kernel": "persistent MINRES solve (k_mr_persistent), per Krylov iteration: Hessian-vector product, "
+                          "operator pass, Lanczos step",
+                "bytes_per_iteration": iter_bytes, "avg_iteration_ms": solve_ms / iters if iters else None,
+                "iterations_timed": iters, "peak_source": "measured" if peaks else "fallback"}
 
     e2e = None
     if not args.no_e2e:

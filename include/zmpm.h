@@ -208,9 +208,11 @@ typedef struct zmpm_stats {
     double newton_residual_initial;
     double newton_residual_final;
     double ms_total;             /* device time of the substep */
-    double ms_hvp;               /* summed device time of the Hessian-vector products that ran
-                                    (only with zmpm_set_profiling on) */
-    int32_t hvp_timed;           /* number of products in ms_hvp */
+    double ms_hvp;               /* summed device time of the persistent linear-solve kernels
+                                    that iterated (only with zmpm_set_profiling on); each
+                                    Krylov iteration there is one Hessian-vector product
+                                    with its node passes */
+    int32_t hvp_timed;           /* Krylov iterations (= products) in ms_hvp */
     int32_t kernel_launches;     /* CUDA kernels this library launched for the substep */
     int32_t phase_field_iterations; /* CG iterations of the phase-field solve (its `iterations` return) */
     int32_t fp64_residual;       /* MIXED: 1 if the Newton residual went to FP64 after the FP32 one stalled */
@@ -384,9 +386,12 @@ int zmpm_get_stream(zmpm_ctx* ctx, void** stream);
    device waits.) */
 int zmpm_set_spin_limit(zmpm_ctx* ctx, int64_t polls);
 
-/* on != 0: bracket each Hessian-vector product with CUDA events and report
-   their summed device time in zmpm_stats.ms_hvp (the reference's ZIRAN_TIMER
-   scopes, Lib/Ziran/CS/Util/Timer.h:34-58, as device timers). */
+/* on != 0: run the Newton loop host-driven (every kernel a plain launch, no
+   CUDA graph) and bracket each linear solve's persistent kernel with CUDA
+   events; zmpm_stats.ms_hvp reports their summed device time and hvp_timed
+   the Krylov iterations they ran (the reference's ZIRAN_TIMER scopes,
+   Lib/Ziran/CS/Util/Timer.h:34-58, as device timers).  ADMM substeps run
+   their iteration loop host-driven too. */
 int zmpm_set_profiling(zmpm_ctx* ctx, int32_t on);
 
 /* ------------------------------------------------------------ adjoint ------ */

@@ -185,3 +185,34 @@ def test_rankine_damage_matches_oracle(cuda_lib, oracle, precision, axis, refere
         np.testing.assert_allclose(cg, co, rtol=1e-4, atol=0)
         assert rel(pg["X"], po["X"]) < 1e-7
         assert rel(pg["V"], po["V"]) < 1e-3
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("solver", ["minres", "cg"])
+def test_profiling_loop_matches_graph(cuda_lib, precision, solver):
+    """The profiling mode (host-driven Newton loop, each persistent solve timed
+    by events) runs the same kernels as the graph: same iteration counts, the
+    same state up to the atomics' summation order, the solves' time and
+    Krylov iterations reported."""
+    dx = 1.0 / 64
+    sims = []
+    for prof in (0, 1):
+        s = mpm.MpmSimulation(dx, gravity=(0, -9.8, 0), precision=precision, grid_log2=8)
+        build_scene(s, kind="hencky", n=6, dx=dx, plastic=150.0, seed=2)
+        if solver == "cg":
+            s.switchLinearSolver(abi.CG)
+        s.newton_tolerance = 1e-7
+        s.lib.set_profiling(s.ctx, prof)
+        sims.append(s)
+    for _ in range(3):
+        st = []
+        for s in sims:
+            assert s.advanceOneTimeStep(1e-3) == abi.OK
+            st.append(s.last_stats)
+        assert st[0]["newton_iterations"] == st[1]["newton_iterations"]
+        assert abs(st[0]["krylov_iterations"] - st[1]["krylov_iterations"]) <= 1
+        assert st[0]["hvp_timed"] == 0
+        assert st[1]["hvp_timed"] == st[1]["krylov_iterations"] and st[1]["ms_hvp"] > 0
+    a, b = sims[0].getParticles(), sims[1].getParticles()
+    assert rel(b["X"], a["X"]) < 1e-10
+    assert rel(b["F"], a["F"]) < 1e-7

@@ -209,7 +209,7 @@ struct Ctx {
     bool scratch_valid = false;
     bool profiling = false;
     std::vector<cudaEvent_t> hvp_ev;      // [newton][krylov][2] when profiling
-    int prof_newton = 0, prof_krylov = 0;
+    int prof_newton = 0;
     DBuf stage;                           // host <-> device particle transfers
     double dt = 0;
 
@@ -265,7 +265,6 @@ int run_adjoint_solve(Ctx* ctx, double tol, int max_iterations); // (M + dt^2 K)
 int launch_residual(Ctx* ctx);                         // r = dt m g + dt f - m dv (projected), norm partials
 int launch_hvp(Ctx* ctx, const double* x, double* out, bool fp32); // out += dt^2 K x (no inertia)
 // FP32 product inside the MINRES loop of a MIXED context, on the FP32 copies x0 / x1 (even / odd iterations)
-int launch_hvp_krylov_f32(Ctx* ctx, const float* x0, const float* x1, double* out);
 int launch_damage(Ctx* ctx);                           // Rankine damage after P2G
 int run_admm(Ctx* ctx, const zmpm_solver& s);         // AdmmSimulation::admmStep
 // particle kernels of the ADMM substep (admm.cu)

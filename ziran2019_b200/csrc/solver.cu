@@ -28,7 +28,6 @@ namespace zmpm {
 
 int launch_p2g(Ctx* ctx);
 int launch_g2p(Ctx* ctx, bool plastic);
-int launch_hvp_krylov(Ctx* ctx, const double* x0, const double* x1, bool alt, double* out);
 
 __device__ __forceinline__ void project3(const int8_t* col, const double* P6, int64_t nn, int64_t n, double v[3])
 {
@@ -453,16 +452,12 @@ __global__ void __launch_bounds__(ND_THREADS, 4) k_residual_start(NodeGeom ng, c
 }
 
 // Newton check (NewtonsMethod.h:48-61) and, unless converged, the start of
-// the linear solve (k_krylov_start's scalars); sets the Krylov loop condition
-// when running as a graph.  One CTA.
+// the linear solve (k_krylov_start's scalars).  One CTA.
 template <int NPB>
 __global__ void __launch_bounds__(ND_THREADS) k_newton_start(NodeGeom ng, NewtonParams np, const double* __restrict__ part_norm,
-    const double* __restrict__ part_zr, SolverScalars* __restrict__ sc, cudaGraphConditionalHandle hK, int use_graph)
+    const double* __restrict__ part_zr, SolverScalars* __restrict__ sc)
 {
-    if (sc->newton_done) {
-        if (use_graph && threadIdx.x == 0) cudaGraphSetConditional(hK, 0u);
-        return;
-    }
+    if (sc->newton_done) return;
     const double norm = sqrt(reduce_partials(part_norm, ng.parts));
     const bool done = (norm < np.tol) || !(norm == norm);
     const double dotv = reduce_partials(part_zr, ng.parts);
@@ -479,7 +474,6 @@ __global__ void __launch_bounds__(ND_THREADS) k_newton_start(NodeGeom ng, Newton
         sc->newton_done = 1;
         sc->converged = (norm == norm) ? 1 : 0;
         sc->kactive = 0;
-        if (use_graph) cudaGraphSetConditional(hK, 0u);
         return;
     }
     const double mx = norm > np.tol ? norm : np.tol;
@@ -504,21 +498,16 @@ __global__ void __launch_bounds__(ND_THREADS) k_newton_start(NodeGeom ng, Newton
     }
     else
         sc->mr[0][0] = dotv; // CG keeps zTrk double-buffered in mr[parity][0]
-    if (use_graph) cudaGraphSetConditional(hK, active ? 1u : 0u);
 }
 
 // Initial preconditioned norm and local tolerance (Minres.h:73-98,
 // ConjugateGradient.h:108-117); MINRES keeps Q0, Z0 unnormalised (beta_0 =
-// the norm divides them where they are read).  Sets the Krylov loop condition
-// when running as a graph.  One CTA.
+// the norm divides them where they are read).  One CTA.
 template <int NPB>
 __global__ void __launch_bounds__(ND_THREADS) k_krylov_start(NodeGeom ng, KrylovBufs kb, NewtonParams np, const double* __restrict__ part_in,
-    SolverScalars* __restrict__ sc, cudaGraphConditionalHandle hK, int use_graph)
+    SolverScalars* __restrict__ sc)
 {
-    if (sc->newton_done) {
-        if (use_graph && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(hK, 0u);
-        return;
-    }
+    if (sc->newton_done) return;
     const double dotv = reduce_partials(part_in, ng.parts);
     const double rnorm = sqrt(dotv);
     const double rel = sc->rel_tol;
@@ -539,7 +528,6 @@ __global__ void __launch_bounds__(ND_THREADS) k_krylov_start(NodeGeom ng, Krylov
         }
         else
             sc->mr[0][0] = dotv; // CG keeps zTrk double-buffered in mr[parity][0]
-        if (use_graph) cudaGraphSetConditional(hK, active ? 1u : 0u);
     }
 }
 
@@ -582,20 +570,6 @@ __global__ void __launch_bounds__(ND_THREADS) k_apply_A(NodeGeom ng, const doubl
     apply_A_body<NPB, false>(ng, gm, col, P6, dt2, xin, hacc, out, nullptr, 0);
 }
 
-// Ends a Krylov iteration (the next loop top's test, Minres.h:100,
-// ConjugateGradient.h:118): advances k, stops on the local tolerance or the
-// iteration cap; as a graph, sets the loop condition.  Run by one thread of
-// the last CTA of the iteration's last kernel, after every CTA read k.
-__device__ __forceinline__ void krylov_advance(SolverScalars* sc, int it, double rnorm, int kmax, cudaGraphConditionalHandle hK, int use_graph)
-{
-    sc->krylov_bodies += 1;
-    const int k = it + 1;
-    sc->kit = k;
-    const bool go = !(rnorm < sc->local_tol || k >= kmax);
-    if (!go) sc->kactive = 0;
-    if (use_graph) cudaGraphSetConditional(hK, go ? 1u : 0u);
-}
-
 // MINRES keeps its Lanczos vectors Q_j and preconditioned vectors Z_j
 // unnormalised (Minres.h:170-173 divides them by beta_j at the end of
 // iteration j - 1); every reader divides by beta_j, the same rounding as the
@@ -604,8 +578,9 @@ __device__ __forceinline__ double mr_norm(double v, double beta) { return beta >
 
 // The search direction of iteration j = k - 1 (Minres.h:167-170):
 // M_j = (Z_j - delta M_{j-1} - epsilon M_{j-2}) / gamma, then x += t M_j.
-// k_mr_b computes its scalars; the vector update runs in the next operator
-// pass (k_mr_a) or, after the last iteration, where the solve's x is used.
+// The Lanczos step computes its scalars; the vector update runs in the next
+// iteration's operator pass or, after the last iteration, where the solve's x
+// is used (k_newton_step, k_admm_dv_update).
 struct MrPending {
     const double *z, *m1, *m2;
     double* out;
@@ -630,49 +605,6 @@ __device__ __forceinline__ MrPending mr_pending(const KrylovBufs& kb, const doub
 __device__ __forceinline__ double mr_direction(const MrPending& p, int64_t i)
 {
     return (mr_norm(p.z[i], p.beta) - p.delta * p.m1[i] - p.eps * p.m2[i]) / p.gamma;
-}
-
-// ------------------------------------------------------------- MINRES -----
-// Operator pass of iteration k: the deferred search direction and x update of
-// iteration k - 1; Z_k = Z~_k / beta_k and the Hessian product (which ran on
-// the unnormalised Z~_k, a linear map) scaled the same way; W = project(m Z_k
-// + dt^2 H Z_k) (BackwardEuler.h:322-351, Minres.h:116) into Q's slot k + 1;
-// hacc = 0; partial Z_k . W.  Massless slots hold zeros in every vector and
-// are skipped.
-template <int NPB>
-__global__ void __launch_bounds__(ND_THREADS, 4) k_mr_a(NodeGeom ng, const double* __restrict__ gm, const int8_t* __restrict__ col,
-    const double* __restrict__ P6, double dt2, KrylovBufs kb, double* __restrict__ part, const SolverScalars* __restrict__ sc)
-{
-    if (krylov_off(sc)) return;
-    const int k = sc->kit;
-    const double* __restrict__ zk = sel2(kb.Z, k & 1);
-    double* __restrict__ w = sel3(kb.Q, (k + 1) % 3);
-    const MrPending pd = mr_pending(kb, sc->pend, k);
-    const double beta = sc->mr[k & 1][MR_BETA_KP1];
-    double acc = 0;
-    for (int64_t n = (int64_t)blockIdx.x * ND_THREADS + threadIdx.x; n < ng.nn; n += (int64_t)gridDim.x * ND_THREADS) {
-        const double m = gm[n];
-        if (m == 0) continue;
-        double o[3], z[3];
-        for (int c = 0; c < 3; ++c) {
-            const int64_t i = vidx<NPB>(n, c);
-            if (pd.on) {
-                const double mv = mr_direction(pd, i);
-                pd.out[i] = mv;
-                kb.x[i] += pd.t * mv;
-            }
-            z[c] = mr_norm(zk[i], beta);
-            o[c] = m * z[c] + dt2 * mr_norm(kb.hacc[i], beta);
-            kb.hacc[i] = 0;
-        }
-        project3(col, P6, ng.nn, n, o);
-        for (int c = 0; c < 3; ++c) {
-            w[vidx<NPB>(n, c)] = o[c];
-            acc += o[c] * z[c];
-        }
-    }
-    const double s = block_sum(acc);
-    if (threadIdx.x == 0) part[blockIdx.x] = s;
 }
 
 // The Givens update of MINRES iteration k (Minres.h:151-175): from the state
@@ -719,58 +651,6 @@ __device__ __forceinline__ double mr_givens(const double* cur, double alpha, dou
     pend[3] = tk;
     pend[4] = beta_k;
     return residual < 0 ? -residual : residual;
-}
-
-// Lanczos step: Q~_{k+1} = W - alpha Q_k - beta_k Q_{k-1} (Q_j = Q~_j /
-// beta_j); Z~_{k+1} = Q~_{k+1} / pre (and its FP32 copy for the MIXED
-// product); partial Z~_{k+1} . Q~_{k+1}.  The last
-// CTA then sums the partials, runs the Givens update of iteration k
-// (Minres.h:151-175) and ends the iteration.
-template <int NPB>
-__global__ void __launch_bounds__(ND_THREADS) k_mr_b(NodeGeom ng, const double* __restrict__ gm, KrylovBufs kb, const double* __restrict__ part_in,
-    double* __restrict__ part_out, SolverScalars* __restrict__ sc, int kmax, cudaGraphConditionalHandle hK, int use_graph)
-{
-    if (krylov_off(sc)) return;
-    const int it = sc->kit;
-    double* __restrict__ qkp1 = sel3(kb.Q, (it + 1) % 3);
-    const double* __restrict__ qk = sel3(kb.Q, it % 3);
-    const double* __restrict__ qkm1 = sel3(kb.Q, (it + 2) % 3);
-    double* __restrict__ zout = sel2(kb.Z, (it + 1) & 1);
-    float* __restrict__ zfout = sel2(kb.Zf, (it + 1) & 1);
-    const double alpha = reduce_partials(part_in, ng.parts);
-    const double beta_k = sc->mr[it & 1][MR_BETA_KP1];
-    const double beta_km1 = sc->mr[(it + 1) & 1][MR_BETA_KP1];
-    double acc = 0;
-    for (int64_t n = (int64_t)blockIdx.x * ND_THREADS + threadIdx.x; n < ng.nn; n += (int64_t)gridDim.x * ND_THREADS) {
-        const double m = gm[n];
-        if (m == 0) continue;
-        const double pre = kb.pre[n];
-        float zf[3];
-        for (int k = 0; k < 3; ++k) {
-            int64_t i = vidx<NPB>(n, k);
-            double q = qkp1[i];
-            q -= alpha * mr_norm(qk[i], beta_k);
-            q -= beta_k * mr_norm(qkm1[i], beta_km1);
-            qkp1[i] = q;
-            double z = q / pre;
-            zout[i] = z;
-            zf[k] = (float)z;
-            acc += z * q;
-        }
-        if (zfout) reinterpret_cast<float4*>(zfout)[n] = make_float4(zf[0], zf[1], zf[2], 0.f);
-    }
-    double s = block_sum(acc);
-    if (threadIdx.x == 0) part_out[blockIdx.x] = s;
-    if (!last_cta(&sc->ticket)) return;
-    const double dz = reduce_partials_l2(part_out, ng.parts);
-    if (threadIdx.x != 0) return;
-    const int nit = sc->nit;
-    const double rnorm = mr_givens(sc->mr[it & 1], alpha, beta_k, dz, sc->mr[(it + 1) & 1], sc->pend);
-    sc->rnorm = rnorm;
-    sc->krylov_iters += 1;
-    sc->hvp_count += 1;
-    if (nit < 64) sc->kcount[nit] += 1;
-    krylov_advance(sc, it, rnorm, kmax, hK, use_graph);
 }
 
 // ------------------------------------------------ persistent Krylov -----
@@ -989,8 +869,11 @@ __global__ void __launch_bounds__(FUSED_THREADS, 4) k_cg_persistent(NodeGeom ng,
 // Newton operator (HvpModel; dt2 = dt^2, pre = m) or on ADMM's global operator
 // (AdmmOpModel; dt2 = 1, pre = its preconditioner).  Per iteration k: the
 // product of Z~_k (its FP32 node-major copy when TX is float) over each CTA's
-// even share of the particle groups (hvp_share); the operator pass of k_mr_a; the
-// Lanczos step of k_mr_b; the Givens update, which thread 0 of every CTA runs
+// even share of the particle groups (hvp_share); the operator pass (the
+// deferred direction of iteration k - 1, W = project(m Z_k + dt2 H Z_k),
+// Minres.h:116, 167-170); the Lanczos step (Q~_{k+1} = W - alpha Q_k -
+// beta_k Q_{k-1}, Z~_{k+1} = Q~_{k+1} / pre); the Givens update
+// (Minres.h:151-175), which thread 0 of every CTA runs
 // on the same fixed-order reductions, so every CTA holds the same MINRES state
 // (in shared memory) and takes the same loop decision.  CTA 0 stores the state
 // after each iteration (the Newton step applies the last deferred direction
@@ -1031,7 +914,7 @@ __global__ void __launch_bounds__(FUSED_THREADS, 4) k_mr_persistent(NodeGeom ng,
             zin = reinterpret_cast<const TX*>(sel2(kb.Z, k & 1));
         hvp_share<L, T, TX, CH>(hs, ha, model, zin, kb.hacc, flags, phase);
         if (!grid_sync(gs, limit, flags)) return;
-        // operator pass (k_mr_a): the deferred direction of iteration k - 1;
+        // operator pass: the deferred direction of iteration k - 1;
         // W = project(m Z_k + dt2 H Z_k) into Q's slot k + 1; partial Z_k . W
         {
             const double* __restrict__ zk = sel2(kb.Z, k & 1);
@@ -1064,7 +947,7 @@ __global__ void __launch_bounds__(FUSED_THREADS, 4) k_mr_persistent(NodeGeom ng,
             if (threadIdx.x == 0) part_a[blockIdx.x] = acc;
         }
         if (!grid_sync(gs, limit, flags)) return;
-        // Lanczos step (k_mr_b): Q~_{k+1} = W - alpha Q_k - beta_k Q_{k-1},
+        // Lanczos step: Q~_{k+1} = W - alpha Q_k - beta_k Q_{k-1},
         // Z~_{k+1} = Q~_{k+1} / pre (and its FP32 copy); partial Z~_{k+1} . Q~_{k+1}
         const double alpha = reduce_partials_fused(part_a, gridDim.x);
         const double beta_k = mst[MR_BETA_KP1], beta_km1 = mst[17];
@@ -1319,12 +1202,6 @@ __global__ void __launch_bounds__(ND_THREADS) k_adj_cg_init(NodeGeom ng, const d
     if (threadIdx.x == 0) part[blockIdx.x] = t;
 }
 
-// The adjoint solve runs its Krylov loop once: the outer loop stops after it.
-__global__ void k_adj_once(SolverScalars* __restrict__ sc, cudaGraphConditionalHandle hN, int use_graph)
-{
-    sc->nit += 1;
-    if (use_graph) cudaGraphSetConditional(hN, 0u);
-}
 
 // ------------------------------------------------------------ host side --
 static NodeGeom node_geom(const Ctx* ctx)
@@ -1497,7 +1374,7 @@ struct NewtonLaunch {
 // First part of a Newton iteration: update, residual with the Krylov start
 // vectors, check and Krylov start.
 template <int NPB>
-int launch_newton_head(const NewtonLaunch& L, cudaStream_t st, cudaGraphConditionalHandle hK, int use_graph)
+int launch_newton_head(const NewtonLaunch& L, cudaStream_t st)
 {
     Ctx* ctx = L.ctx;
     int rc = launch_update(ctx);
@@ -1505,26 +1382,7 @@ int launch_newton_head(const NewtonLaunch& L, cudaStream_t st, cudaGraphConditio
     const double* g = ctx->cfg.gravity;
     k_residual_start<NPB><<<L.nb, ND_THREADS, 0, st>>>(L.ng, ctx->gm.as<double>(), ctx->facc.as<double>(), ctx->dv.as<double>(),
         ctx->collided.as<int8_t>(), ctx->proj.as<double>(), g[0], g[1], g[2], ctx->dt, L.kb, L.np.minres, L.pA, L.pB, L.sc);
-    k_newton_start<NPB><<<1, ND_THREADS, 0, st>>>(L.ng, L.np, L.pA, L.pB, L.sc, hK, use_graph);
-    g_kernel_launches += 2;
-    return ZMPM_OK;
-}
-
-// One MINRES iteration: Hessian-vector product, the operator pass and the
-// Lanczos / Givens step (CG runs its whole solve in k_cg_persistent).
-template <int NPB>
-int launch_krylov_iteration(const NewtonLaunch& L, cudaStream_t st, cudaGraphConditionalHandle hK, int use_graph, cudaEvent_t e0, cudaEvent_t e1)
-{
-    Ctx* ctx = L.ctx;
-    if (e0) ZMPM_CUDA(cudaEventRecord(e0, st));
-    if (L.kb.Zf[0])
-        launch_hvp_krylov_f32(ctx, L.kb.Zf[0], L.kb.Zf[1], L.kb.hacc);
-    else
-        launch_hvp_krylov(ctx, L.kb.Z[0], L.kb.Z[1], true, L.kb.hacc);
-    if (e1) ZMPM_CUDA(cudaEventRecord(e1, st));
-    k_mr_a<NPB><<<L.nb, ND_THREADS, 0, st>>>(L.ng, ctx->gm.as<double>(), ctx->collided.as<int8_t>(), ctx->proj.as<double>(), L.dt2, L.kb, L.pA,
-        L.sc);
-    k_mr_b<NPB><<<L.nb, ND_THREADS, 0, st>>>(L.ng, ctx->gm.as<double>(), L.kb, L.pA, L.pC, L.sc, L.np.kmax, hK, use_graph);
+    k_newton_start<NPB><<<1, ND_THREADS, 0, st>>>(L.ng, L.np, L.pA, L.pB, L.sc);
     g_kernel_launches += 2;
     return ZMPM_OK;
 }
@@ -1692,7 +1550,7 @@ int while_graph(Ctx* ctx, Body&& body, cudaGraphExec_t* exec_out)
 template <int NPB>
 int launch_newton_iteration(const NewtonLaunch& L, cudaStream_t st, cudaGraphConditionalHandle hN, int use_graph)
 {
-    int rc = launch_newton_head<NPB>(L, st, 0, 0);
+    int rc = launch_newton_head<NPB>(L, st);
     if (rc) return rc;
     rc = L.np.minres ? launch_mr_persistent<NPB>(L, st, false) : launch_cg_persistent<NPB>(L, st);
     if (rc) return rc;
@@ -1759,8 +1617,7 @@ static int newton_impl(Ctx* ctx, const zmpm_solver& s)
     ctx->graph_used = false;
     if (L.ng.nn == 0 || s.newton_max_iterations == 0) return ZMPM_OK;
     ZMPM_CUDA(cudaMemsetAsync(ctx->gsync.p, 0, sizeof(GridSync), st));
-    // profiling: MINRES as separate launches, each product bracketed by events
-    const bool prof = ctx->profiling && s.newton_max_iterations <= 64 && L.np.minres;
+    const bool prof = ctx->profiling && s.newton_max_iterations <= 64;
     if (!prof) {
         // whole solve as one graph with device-side loop conditions
         cudaGraphExec_t exec = nullptr;
@@ -1777,26 +1634,21 @@ static int newton_impl(Ctx* ctx, const zmpm_solver& s)
         ZMPM_CUDA(e);
         return ZMPM_OK;
     }
-    // host-driven loop (profiling: each product bracketed by events)
-    ctx->prof_newton = prof ? s.newton_max_iterations : 0;
-    ctx->prof_krylov = s.krylov_max_iterations;
-    if (prof) {
-        size_t need = 2 * (size_t)s.newton_max_iterations * s.krylov_max_iterations;
-        while (ctx->hvp_ev.size() < need) {
-            cudaEvent_t e;
-            ZMPM_CUDA(cudaEventCreate(&e));
-            ctx->hvp_ev.push_back(e);
-        }
+    // profiling: a host-driven Newton loop (every kernel a plain launch), each
+    // linear solve's persistent kernel bracketed by events
+    ctx->prof_newton = s.newton_max_iterations;
+    while (ctx->hvp_ev.size() < 2 * (size_t)s.newton_max_iterations) {
+        cudaEvent_t e;
+        ZMPM_CUDA(cudaEventCreate(&e));
+        ctx->hvp_ev.push_back(e);
     }
     for (int it = 0; it < s.newton_max_iterations; ++it) {
-        int rc = launch_newton_head<NPB>(L, st, 0, 0);
+        int rc = launch_newton_head<NPB>(L, st);
         if (rc) return rc;
-        for (int k = 0; k < s.krylov_max_iterations; ++k) {
-            cudaEvent_t e0 = prof ? ctx->hvp_ev[2 * (it * s.krylov_max_iterations + k)] : nullptr;
-            cudaEvent_t e1 = prof ? ctx->hvp_ev[2 * (it * s.krylov_max_iterations + k) + 1] : nullptr;
-            rc = launch_krylov_iteration<NPB>(L, st, 0, 0, e0, e1);
-            if (rc) return rc;
-        }
+        ZMPM_CUDA(cudaEventRecord(ctx->hvp_ev[2 * it], st));
+        rc = L.np.minres ? launch_mr_persistent<NPB>(L, st, false) : launch_cg_persistent<NPB>(L, st);
+        if (rc) return rc;
+        ZMPM_CUDA(cudaEventRecord(ctx->hvp_ev[2 * it + 1], st));
         rc = launch_newton_tail<NPB>(L, st, 0, 0);
         if (rc) return rc;
         ZMPM_CUDA(cudaGetLastError());
@@ -1900,7 +1752,7 @@ static int admm_impl(Ctx* ctx, const zmpm_solver& s)
         if (r) return r;
         k_admm_start<NPB><<<Lc.nb, ND_THREADS, 0, sm>>>(Lc.ng, ctx->gm.as<double>(), ctx->collided.as<int8_t>(), ctx->proj.as<double>(),
             ctx->adm_rhs.as<double>(), ctx->dv.as<double>(), kb, Lc.pB, Lc.sc);
-        k_krylov_start<NPB><<<1, ND_THREADS, 0, sm>>>(Lc.ng, kb, Lc.np, Lc.pB, Lc.sc, 0, 0);
+        k_krylov_start<NPB><<<1, ND_THREADS, 0, sm>>>(Lc.ng, kb, Lc.np, Lc.pB, Lc.sc);
         g_kernel_launches += 2;
         r = launch_mr_persistent<NPB>(Lc, sm, true);
         if (r) return r;
@@ -1983,12 +1835,12 @@ int run_adjoint_solve(Ctx* ctx, double tol, int max_iterations)
     if (ctx->layout == 1) {
         k_adj_cg_init<32><<<Lc.nb, ND_THREADS, 0, st>>>(Lc.ng, ctx->gm.as<double>(), ctx->collided.as<int8_t>(), ctx->proj.as<double>(),
             ctx->res.as<double>(), kb, tol, Lc.pB, Lc.sc);
-        k_krylov_start<32><<<1, ND_THREADS, 0, st>>>(Lc.ng, kb, Lc.np, Lc.pB, Lc.sc, 0, 0);
+        k_krylov_start<32><<<1, ND_THREADS, 0, st>>>(Lc.ng, kb, Lc.np, Lc.pB, Lc.sc);
     }
     else {
         k_adj_cg_init<64><<<Lc.nb, ND_THREADS, 0, st>>>(Lc.ng, ctx->gm.as<double>(), ctx->collided.as<int8_t>(), ctx->proj.as<double>(),
             ctx->res.as<double>(), kb, tol, Lc.pB, Lc.sc);
-        k_krylov_start<64><<<1, ND_THREADS, 0, st>>>(Lc.ng, kb, Lc.np, Lc.pB, Lc.sc, 0, 0);
+        k_krylov_start<64><<<1, ND_THREADS, 0, st>>>(Lc.ng, kb, Lc.np, Lc.pB, Lc.sc);
     }
     g_kernel_launches += 2;
     ZMPM_CUDA(cudaMemsetAsync(ctx->gsync.p, 0, sizeof(GridSync), st));

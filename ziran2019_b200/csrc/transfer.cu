@@ -491,16 +491,14 @@ __global__ void __launch_bounds__(XF_THREADS) k_force(const int32_t* __restrict_
 }
 
 // ------------------------------------------------------- fused products ----
-// The Hessian-vector product (hvp.cuh) as one CTA per particle group.
+// The Hessian-vector product (hvp.cuh) as one CTA per particle group (the
+// zmpm_multiply hook; the solves run it inside their persistent kernels).
 template <class L, class T, class TX, int CH>
 __global__ void __launch_bounds__(FUSED_THREADS) k_hvp_fused(const int32_t* __restrict__ group_start, const int32_t* __restrict__ group_nbr,
     const int32_t* __restrict__ pi, int64_t cap, const short4* __restrict__ base, double dx, const T* __restrict__ frac,
-    const T* __restrict__ scr, const TX* __restrict__ x0, const TX* __restrict__ x1, int alt, double* __restrict__ out,
-    const SolverScalars* __restrict__ sc, int32_t* __restrict__ flags)
+    const T* __restrict__ scr, const TX* __restrict__ x, double* __restrict__ out, int32_t* __restrict__ flags)
 {
-    if (sc && (sc->newton_done || !sc->kactive)) return;
     __shared__ HvpSmem<L, T, TX, CH> hs;
-    const TX* x = (alt && sc && (sc->kit & 1)) ? x1 : x0;
     const int g = blockIdx.x;
     hvp_group<L, T, TX, CH>(hs, g, group_start[g], group_start[g + 1], group_nbr, HvpModel<T>{ pi, scr, cap }, cap, base, dx, frac, x, out,
         flags);
@@ -882,7 +880,7 @@ int launch_update(Ctx* ctx, bool gated) { return ctx->layout == 1 ? update_impl<
 // out += dt^-2 (Hessian part of A) x: the fused product, T the context's HVP
 // precision, on an FP64 input vector
 template <class L>
-static int hvp_impl(Ctx* ctx, const double* x0, const double* x1, int alt, double* out, const SolverScalars* sc)
+static int hvp_impl(Ctx* ctx, const double* x, double* out)
 {
     const int64_t G = ctx->G;
     if (G == 0) return ZMPM_OK;
@@ -890,46 +888,19 @@ static int hvp_impl(Ctx* ctx, const double* x0, const double* x1, int alt, doubl
     if (ctx->mixed)
         k_hvp_fused<L, float, double, fused_chunk<float>()><<<(unsigned)G, FUSED_THREADS, 0, ctx->stream>>>(ctx->group_start.as<int32_t>(),
             ctx->group_nbr.as<int32_t>(), ctx->pi.as<int32_t>(), ctx->Pcap, ctx->base.as<short4>(), ctx->cfg.dx, ctx->frac.as<float>(),
-            ctx->scratch.as<float>(), x0, x1, alt, out, sc, &dc->flags);
+            ctx->scratch.as<float>(), x, out, &dc->flags);
     else
         k_hvp_fused<L, double, double, fused_chunk<double>()><<<(unsigned)G, FUSED_THREADS, 0, ctx->stream>>>(ctx->group_start.as<int32_t>(),
             ctx->group_nbr.as<int32_t>(), ctx->pi.as<int32_t>(), ctx->Pcap, ctx->base.as<short4>(), ctx->cfg.dx, ctx->frac.as<double>(),
-            ctx->scratch.as<double>(), x0, x1, alt, out, sc, &dc->flags);
+            ctx->scratch.as<double>(), x, out, &dc->flags);
     ++g_kernel_launches;
     return ZMPM_OK;
-}
-
-// The FP32 product inside MINRES on the node-major FP32 copies of Z.
-template <class L>
-static int hvp_f32_impl(Ctx* ctx, const float* x0, const float* x1, double* out)
-{
-    const int64_t G = ctx->G;
-    if (G == 0) return ZMPM_OK;
-    const SolverScalars* sc = ctx->scal.as<SolverScalars>();
-    DevCounters* dc = ctx->counters.as<DevCounters>();
-    k_hvp_fused<L, float, float, fused_chunk<float>()><<<(unsigned)G, FUSED_THREADS, 0, ctx->stream>>>(ctx->group_start.as<int32_t>(),
-        ctx->group_nbr.as<int32_t>(), ctx->pi.as<int32_t>(), ctx->Pcap, ctx->base.as<short4>(), ctx->cfg.dx, ctx->frac.as<float>(),
-        ctx->scratch.as<float>(), x0, x1, 1, out, sc, &dc->flags);
-    ++g_kernel_launches;
-    return ZMPM_OK;
-}
-int launch_hvp_krylov_f32(Ctx* ctx, const float* x0, const float* x1, double* out)
-{
-    return ctx->layout == 1 ? hvp_f32_impl<Layout244>(ctx, x0, x1, out) : hvp_f32_impl<Layout444>(ctx, x0, x1, out);
-}
-
-// Product inside the Newton solve: gated by the solver scalars; with alt the
-// input is x0 on even and x1 on odd Krylov iterations.
-int launch_hvp_krylov(Ctx* ctx, const double* x0, const double* x1, bool alt, double* out)
-{
-    const SolverScalars* sc = ctx->scal.as<SolverScalars>();
-    return ctx->layout == 1 ? hvp_impl<Layout244>(ctx, x0, x1, alt ? 1 : 0, out, sc) : hvp_impl<Layout444>(ctx, x0, x1, alt ? 1 : 0, out, sc);
 }
 
 int launch_hvp(Ctx* ctx, const double* x, double* out, bool fp32)
 {
     if (fp32 != ctx->mixed) return ZMPM_UNSUPPORTED;
-    return ctx->layout == 1 ? hvp_impl<Layout244>(ctx, x, x, 0, out, nullptr) : hvp_impl<Layout444>(ctx, x, x, 0, out, nullptr);
+    return ctx->layout == 1 ? hvp_impl<Layout244>(ctx, x, out) : hvp_impl<Layout444>(ctx, x, out);
 }
 
 template <class L, class TH>
