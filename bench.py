@@ -476,7 +476,8 @@ def main():
         if rank == 0:
             print(json.dumps({"only": args.only, "particles": P, "ms_per_step": ms / args.steps, "host_loop": args.host_loop,
                               "iteration_ms": sum(s["ms_hvp"] for s in stp) / max(1, sum(s["hvp_timed"] for s in stp)),
-                              "launches_per_step": st[-1]["kernel_launches"], "newton_krylov": [st[-1]["newton_iterations"], st[-1]["krylov_iterations"]]}),
+                              "launches_per_step": st[-1]["kernel_launches"], "newton_krylov": [st[-1]["newton_iterations"], st[-1]["krylov_iterations"]],
+                              "krylov_iterations_host_loop": sum(x["krylov_iterations"] for x in (st if args.host_loop else []) + stp)}),
                   flush=True)
         return
     # nvidia-smi samples through both timed regions; it starts a second ahead

@@ -526,7 +526,7 @@ __global__ void __launch_bounds__(FUSED_THREADS) k_op_fused(const int32_t* __res
 // near-degenerate SVDs are redone in FP64.  Phase 2 adds -S_p grad w_ip to
 // facc.  gate as k_stress / k_force.
 template <class L, class T, class TX, int CH>
-__global__ void __launch_bounds__(FUSED_THREADS) k_update_fused(const int32_t* __restrict__ group_start, const int32_t* __restrict__ group_nbr,
+__global__ void __launch_bounds__(FUSED_THREADS, 4) k_update_fused(const int32_t* __restrict__ group_start, const int32_t* __restrict__ group_nbr,
     const double* __restrict__ pd, const int32_t* __restrict__ pi, int64_t cap, const short4* __restrict__ base, double dx, double dt,
     const T* __restrict__ frac, const TX* __restrict__ vstar, T* __restrict__ scr, double* __restrict__ facc,
     const SolverScalars* __restrict__ sc, int32_t* __restrict__ flags, int gate, unsigned long long* __restrict__ svd64)
