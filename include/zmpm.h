@@ -403,11 +403,15 @@ int zmpm_set_profiling(zmpm_ctx* ctx, int32_t on);
    (NULL means zero).  gE [P] accumulates dL/dE_p, the Young's modulus at fixed
    Poisson ratio (mu and lambda scale with E).  The derivative is the hand-written
    adjoint of P2G, of the converged Newton solution through the implicit
-   function theorem, and of G2P (quadratic B-spline weights, their gradients and
-   Hessians): the adjoint system (M + dt^2 K) lambda = g uses the substep's own
-   symmetric Hessian, solved in FP64 by CG to the relative `adjoint_tolerance`.
-   Binning is held fixed (piecewise constant in x).  Returns ZMPM_UNSUPPORTED
-   for plasticity, damage, viscoelastic particles or the ADMM integrator. */
+   function theorem, of G2P (quadratic B-spline weights, their gradients and
+   Hessians) and of the von Mises return map (VonMisesStvkHencky with xi = 0 on
+   StvkWithHenckyIsotropic particles; the projection is differentiated as an
+   isotropic function of the trial F, and dL/dE includes the yield radius'
+   dependence on mu): the adjoint system (M + dt^2 K) lambda = g uses the
+   substep's own symmetric Hessian, solved in FP64 by CG to the relative
+   `adjoint_tolerance`.  Binning is held fixed (piecewise constant in x).
+   Returns ZMPM_UNSUPPORTED for other plasticity (hardening, Drucker-Prager,
+   Cam-Clay), damage, viscoelastic particles or the ADMM integrator. */
 int zmpm_adjoint_substep(zmpm_ctx* ctx, double dt, const zmpm_solver* s, double adjoint_tolerance, double* gx, double* gv, double* gC,
     double* gF, double* gE, zmpm_stats* stats);
 
