@@ -703,10 +703,11 @@ __device__ __forceinline__ void apply_return_map_f32(double* __restrict__ pd, in
 // then evolveStrain F = (I + dt grad v) Fn (FBasedMpmForceHelper.cpp:95-109, and
 // the viscoelastic Fe's relaxation) and, with `plastic`, applyPlasticity.
 // T: the arithmetic (FP32 in MIXED contexts: weights from the stored cell
-// fractions, positions advanced in FP64).  Three CTAs per SM (at most 168
-// registers): the FP64 form is latency bound on FP64 chains.
+// fractions, positions advanced in FP64).  FP64: three CTAs per SM (at most
+// 168 registers; the form is latency bound on FP64 chains).  FP32: four (128
+// registers, a few spilled words).
 template <class L, class T, class TX>
-__global__ void __launch_bounds__(XF_THREADS, 3) k_g2p(const int32_t* __restrict__ group_start, const int32_t* __restrict__ group_nbr,
+__global__ void __launch_bounds__(XF_THREADS, sizeof(T) == 4 ? 4 : 3) k_g2p(const int32_t* __restrict__ group_start, const int32_t* __restrict__ group_nbr,
     double* __restrict__ pd, int32_t* __restrict__ pi, int64_t cap, const short4* __restrict__ base, const T* __restrict__ frac, double dx,
     double dt, double apic_rpic_ratio, const TX* __restrict__ vnew, int32_t* __restrict__ flags, int mls, int plastic)
 {
