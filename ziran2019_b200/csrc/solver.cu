@@ -880,6 +880,9 @@ __global__ void __launch_bounds__(FUSED_THREADS, 4) k_cg_persistent(NodeGeom ng,
 // from it).  Three bounded grid barriers per iteration: the product is
 // complete before the operator pass reads hacc, W before the Lanczos step, and
 // Z~_{k+1} before the next product and the reduction of its norm.
+// Nodes per thread and step in the node passes of k_mr_persistent (their
+// loads all issue before the arithmetic: the passes are latency-bound).
+constexpr int MR_UNROLL = 2;
 template <class L, class T, class TX, class Model>
 __global__ void __launch_bounds__(FUSED_THREADS, 4) k_mr_persistent(NodeGeom ng, HvpArgs ha, Model model, const double* __restrict__ gm,
     const int8_t* __restrict__ col, const double* __restrict__ P6, double dt2, KrylovBufs kb, double* __restrict__ part_a,
@@ -922,25 +925,50 @@ __global__ void __launch_bounds__(FUSED_THREADS, 4) k_mr_persistent(NodeGeom ng,
             const MrPending pd = mr_pending(kb, pend, k);
             const double beta = mst[MR_BETA_KP1];
             double acc = 0;
-            for (int64_t n = t0; n < ng.nn; n += nt) {
-                const double m = gm[n];
-                if (m == 0) continue;
-                double o[3], z[3];
-                for (int c = 0; c < 3; ++c) {
-                    const int64_t i = vidx<NPB>(n, c);
-                    if (pd.on) {
-                        const double mv = mr_direction(pd, i);
-                        pd.out[i] = mv;
-                        kb.x[i] += pd.t * mv;
-                    }
-                    z[c] = mr_norm(zk[i], beta);
-                    o[c] = m * z[c] + dt2 * mr_norm(kb.hacc[i], beta);
-                    kb.hacc[i] = 0;
+            // MR_UNROLL nodes per step, every load issued before the arithmetic
+            // (massless nodes hold zeros in every vector and are not written)
+            for (int64_t n = t0; n < ng.nn; n += MR_UNROLL * nt) {
+                int64_t nn2[MR_UNROLL];
+                double mm[MR_UNROLL];
+#pragma unroll
+                for (int u = 0; u < MR_UNROLL; ++u) {
+                    const bool in = n + u * nt < ng.nn;
+                    nn2[u] = in ? n + u * nt : n;
+                    mm[u] = in ? gm[nn2[u]] : 0.0;
                 }
-                project3(col, P6, ng.nn, n, o);
-                for (int c = 0; c < 3; ++c) {
-                    w[vidx<NPB>(n, c)] = o[c];
-                    acc += o[c] * z[c];
+                double zv[MR_UNROLL][3], hv[MR_UNROLL][3], mv[MR_UNROLL][3], xv[MR_UNROLL][3];
+#pragma unroll
+                for (int u = 0; u < MR_UNROLL; ++u)
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) {
+                        const int64_t i = vidx<NPB>(nn2[u], c);
+                        zv[u][c] = zk[i];
+                        hv[u][c] = kb.hacc[i];
+                        mv[u][c] = pd.on ? mr_direction(pd, i) : 0.0;
+                        xv[u][c] = pd.on ? kb.x[i] : 0.0;
+                    }
+#pragma unroll
+                for (int u = 0; u < MR_UNROLL; ++u) {
+                    const double m = mm[u];
+                    if (m == 0) continue;
+                    double o[3], z[3];
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) {
+                        const int64_t i = vidx<NPB>(nn2[u], c);
+                        if (pd.on) {
+                            pd.out[i] = mv[u][c];
+                            kb.x[i] = xv[u][c] + pd.t * mv[u][c];
+                        }
+                        z[c] = mr_norm(zv[u][c], beta);
+                        o[c] = m * z[c] + dt2 * mr_norm(hv[u][c], beta);
+                        kb.hacc[i] = 0;
+                    }
+                    project3(col, P6, ng.nn, nn2[u], o);
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) {
+                        w[vidx<NPB>(nn2[u], c)] = o[c];
+                        acc += o[c] * z[c];
+                    }
                 }
             }
             acc = block_sum_fused(acc);
@@ -958,23 +986,45 @@ __global__ void __launch_bounds__(FUSED_THREADS, 4) k_mr_persistent(NodeGeom ng,
             double* __restrict__ zout = sel2(kb.Z, (k + 1) & 1);
             float* __restrict__ zfout = sel2(kb.Zf, (k + 1) & 1);
             double acc = 0;
-            for (int64_t n = t0; n < ng.nn; n += nt) {
-                const double m = gm[n];
-                if (m == 0) continue;
-                const double pre = kb.pre[n];
-                float zf[3];
-                for (int c = 0; c < 3; ++c) {
-                    const int64_t i = vidx<NPB>(n, c);
-                    double q = qkp1[i];
-                    q -= alpha * mr_norm(qk[i], beta_k);
-                    q -= beta_k * mr_norm(qkm1[i], beta_km1);
-                    qkp1[i] = q;
-                    const double z = q / pre;
-                    zout[i] = z;
-                    zf[c] = (float)z;
-                    acc += z * q;
+            for (int64_t n = t0; n < ng.nn; n += MR_UNROLL * nt) {
+                int64_t nn2[MR_UNROLL];
+                double mm[MR_UNROLL];
+#pragma unroll
+                for (int u = 0; u < MR_UNROLL; ++u) {
+                    const bool in = n + u * nt < ng.nn;
+                    nn2[u] = in ? n + u * nt : n;
+                    mm[u] = in ? gm[nn2[u]] : 0.0;
                 }
-                if (zfout) reinterpret_cast<float4*>(zfout)[n] = make_float4(zf[0], zf[1], zf[2], 0.f);
+                double pre[MR_UNROLL], qa[MR_UNROLL][3], qb[MR_UNROLL][3], qc[MR_UNROLL][3];
+#pragma unroll
+                for (int u = 0; u < MR_UNROLL; ++u) {
+                    pre[u] = kb.pre[nn2[u]];
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) {
+                        const int64_t i = vidx<NPB>(nn2[u], c);
+                        qa[u][c] = qkp1[i];
+                        qb[u][c] = qk[i];
+                        qc[u][c] = qkm1[i];
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < MR_UNROLL; ++u) {
+                    if (mm[u] == 0) continue;
+                    float zf[3];
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) {
+                        const int64_t i = vidx<NPB>(nn2[u], c);
+                        double q = qa[u][c];
+                        q -= alpha * mr_norm(qb[u][c], beta_k);
+                        q -= beta_k * mr_norm(qc[u][c], beta_km1);
+                        qkp1[i] = q;
+                        const double z = q / pre[u];
+                        zout[i] = z;
+                        zf[c] = (float)z;
+                        acc += z * q;
+                    }
+                    if (zfout) reinterpret_cast<float4*>(zfout)[nn2[u]] = make_float4(zf[0], zf[1], zf[2], 0.f);
+                }
             }
             acc = block_sum_fused(acc);
             if (threadIdx.x == 0) part_b[blockIdx.x] = acc;
