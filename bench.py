@@ -61,7 +61,8 @@ def run_rollout(args, world, rank):
         def loss_and_grad(X):
             com = (m[:, None] * X).sum(0) / m.sum()
             return float(((com - target) ** 2).sum()), 2 * (com - target)[None, :] * (m / m.sum())[:, None]
-        X = ro.run(E, v0)  # warm-up (allocations, graphs)
+        X = ro.run(E, v0)  # warm-up forward and reverse (allocations, graphs, first launches)
+        ro.backward(loss_and_grad(X)[1])
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         X = ro.run(E, v0)

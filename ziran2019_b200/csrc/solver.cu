@@ -797,21 +797,38 @@ __global__ void __launch_bounds__(FUSED_THREADS, 4) k_cg_persistent(NodeGeom ng,
         hvp_share<L, T, double, CH>(hs, ha, HvpModel<T>{ ha.pi, static_cast<const T*>(ha.scr), ha.cap }, kb.p, kb.hacc, flags, phase);
         if (!grid_sync(gs, limit, flags)) return;
         // tmp = project(m p + dt^2 hacc), hacc = 0; partial p . tmp (BackwardEuler.h:322-351)
+        // (two nodes per step, every load issued before the arithmetic, as in
+        // k_mr_persistent; massless nodes hold zeros and are not written)
         double acc = 0;
-        for (int64_t n = t0; n < ng.nn; n += nt) {
-            const double m = gm[n];
-            if (m == 0) continue;
-            double o[3], pv[3];
-            for (int c = 0; c < 3; ++c) {
-                const int64_t i = vidx<NPB>(n, c);
-                pv[c] = kb.p[i];
-                o[c] = m * pv[c] + dt2 * kb.hacc[i];
-                kb.hacc[i] = 0;
-            }
-            project3(col, P6, ng.nn, n, o);
-            for (int c = 0; c < 3; ++c) {
-                kb.tmp[vidx<NPB>(n, c)] = o[c];
-                acc += o[c] * pv[c];
+        for (int64_t n = t0; n < ng.nn; n += 2 * nt) {
+            const bool in1 = n + nt < ng.nn;
+            const int64_t nu[2] = { n, in1 ? n + nt : n };
+            const double mm[2] = { gm[nu[0]], in1 ? gm[nu[1]] : 0.0 };
+            double pv[2][3], hv[2][3];
+#pragma unroll
+            for (int u = 0; u < 2; ++u)
+#pragma unroll
+                for (int c = 0; c < 3; ++c) {
+                    const int64_t i = vidx<NPB>(nu[u], c);
+                    pv[u][c] = kb.p[i];
+                    hv[u][c] = kb.hacc[i];
+                }
+#pragma unroll
+            for (int u = 0; u < 2; ++u) {
+                const double m = mm[u];
+                if (m == 0) continue;
+                double o[3];
+#pragma unroll
+                for (int c = 0; c < 3; ++c) {
+                    o[c] = m * pv[u][c] + dt2 * hv[u][c];
+                    kb.hacc[vidx<NPB>(nu[u], c)] = 0;
+                }
+                project3(col, P6, ng.nn, nu[u], o);
+#pragma unroll
+                for (int c = 0; c < 3; ++c) {
+                    kb.tmp[vidx<NPB>(nu[u], c)] = o[c];
+                    acc += o[c] * pv[u][c];
+                }
             }
         }
         acc = block_sum_fused(acc);
@@ -820,17 +837,36 @@ __global__ void __launch_bounds__(FUSED_THREADS, 4) k_cg_persistent(NodeGeom ng,
         // x += alpha p; r -= alpha tmp; q = r / m; partial q . r
         const double alpha = zTr / reduce_partials_fused(part_a, gridDim.x);
         acc = 0;
-        for (int64_t n = t0; n < ng.nn; n += nt) {
-            const double m = gm[n];
-            if (m == 0) continue;
-            for (int c = 0; c < 3; ++c) {
-                const int64_t i = vidx<NPB>(n, c);
-                kb.x[i] += kb.p[i] * alpha;
-                const double r = kb.r[i] - kb.tmp[i] * alpha;
-                kb.r[i] = r;
-                const double q = r / kb.pre[n];
-                kb.q[i] = q;
-                acc += q * r;
+        for (int64_t n = t0; n < ng.nn; n += 2 * nt) {
+            const bool in1 = n + nt < ng.nn;
+            const int64_t nu[2] = { n, in1 ? n + nt : n };
+            const double mm[2] = { gm[nu[0]], in1 ? gm[nu[1]] : 0.0 };
+            double xv[2][3], pv[2][3], rv[2][3], tv[2][3], pre[2];
+#pragma unroll
+            for (int u = 0; u < 2; ++u) {
+                pre[u] = kb.pre[nu[u]];
+#pragma unroll
+                for (int c = 0; c < 3; ++c) {
+                    const int64_t i = vidx<NPB>(nu[u], c);
+                    xv[u][c] = kb.x[i];
+                    pv[u][c] = kb.p[i];
+                    rv[u][c] = kb.r[i];
+                    tv[u][c] = kb.tmp[i];
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < 2; ++u) {
+                if (mm[u] == 0) continue;
+#pragma unroll
+                for (int c = 0; c < 3; ++c) {
+                    const int64_t i = vidx<NPB>(nu[u], c);
+                    kb.x[i] = xv[u][c] + pv[u][c] * alpha;
+                    const double r = rv[u][c] - tv[u][c] * alpha;
+                    kb.r[i] = r;
+                    const double q = r / pre[u];
+                    kb.q[i] = q;
+                    acc += q * r;
+                }
             }
         }
         acc = block_sum_fused(acc);
@@ -839,11 +875,24 @@ __global__ void __launch_bounds__(FUSED_THREADS, 4) k_cg_persistent(NodeGeom ng,
         // beta, p = q + beta p; the loop test of the next iteration
         const double zTr1 = reduce_partials_fused(part_b, gridDim.x);
         const double beta = zTr1 / zTr, rnorm = sqrt(zTr1);
-        for (int64_t n = t0; n < ng.nn; n += nt) {
-            if (gm[n] == 0) continue;
-            for (int c = 0; c < 3; ++c) {
-                const int64_t i = vidx<NPB>(n, c);
-                kb.p[i] = kb.q[i] + beta * kb.p[i];
+        for (int64_t n = t0; n < ng.nn; n += 2 * nt) {
+            const bool in1 = n + nt < ng.nn;
+            const int64_t nu[2] = { n, in1 ? n + nt : n };
+            const double mm[2] = { gm[nu[0]], in1 ? gm[nu[1]] : 0.0 };
+            double qv[2][3], pv[2][3];
+#pragma unroll
+            for (int u = 0; u < 2; ++u)
+#pragma unroll
+                for (int c = 0; c < 3; ++c) {
+                    const int64_t i = vidx<NPB>(nu[u], c);
+                    qv[u][c] = kb.q[i];
+                    pv[u][c] = kb.p[i];
+                }
+#pragma unroll
+            for (int u = 0; u < 2; ++u) {
+                if (mm[u] == 0) continue;
+#pragma unroll
+                for (int c = 0; c < 3; ++c) kb.p[vidx<NPB>(nu[u], c)] = qv[u][c] + beta * pv[u][c];
             }
         }
         ++k;
