@@ -372,6 +372,7 @@ struct KrylovBufs {
     double *x, *r, *p, *q, *tmp;      // CG
     double *Q[3], *M[3], *Z[2];       // MINRES
     float* Zf[2];                     // FP32 node-major copies of Z ([B][NPB][4]) for the FP32 product (MIXED MINRES), or null
+    float* pf;                        // FP32 node-major copy of p for the FP32 product (MIXED CG), or null
     double* hacc;                     // Hessian accumulator
     const double* pre;                // diagonal preconditioner per node (the mass for Newton)
 };
@@ -439,6 +440,7 @@ __global__ void __launch_bounds__(ND_THREADS, 4) k_residual_start(NodeGeom ng, c
                 kb.r[i] = rv;
                 kb.q[i] = z;
                 kb.p[i] = z;
+                if (kb.pf) kb.pf[4 * n + k] = (float)z;
             }
             zr += z * rv;
         }
@@ -775,7 +777,7 @@ __device__ __forceinline__ void hvp_share(HvpSmem<L, T, TX, CH>& hs, const HvpAr
     }
 }
 
-template <class L, class T>
+template <class L, class T, class TX>
 __global__ void __launch_bounds__(FUSED_THREADS, 4) k_cg_persistent(NodeGeom ng, HvpArgs ha, const double* __restrict__ gm,
     const int8_t* __restrict__ col, const double* __restrict__ P6, double dt2, KrylovBufs kb, double* __restrict__ part_a,
     double* __restrict__ part_b, SolverScalars* __restrict__ sc, int kmax, GridSync* __restrict__ gs, long long limit, int32_t* __restrict__ flags)
@@ -783,18 +785,24 @@ __global__ void __launch_bounds__(FUSED_THREADS, 4) k_cg_persistent(NodeGeom ng,
     if (sc->newton_done || !sc->kactive) return;
     constexpr int NPB = L::NPB;
     constexpr int CH = sizeof(T) == 4 ? 512 : 192;
-    __shared__ HvpSmem<L, T, double, CH> hs;
+    __shared__ HvpSmem<L, T, TX, CH> hs;
     if (threadIdx.x == 0) mbar_init(&hs.bar, 1);
     __syncthreads();
     int phase = 0;
     const int nit = sc->nit;
     int k = sc->kit;
     double zTr = sc->mr[k & 1][0];
+    // the product's input: p, or its FP32 node-major copy when TX is float
+    const TX* pin;
+    if constexpr (sizeof(TX) == 4)
+        pin = reinterpret_cast<const TX*>(kb.pf);
+    else
+        pin = reinterpret_cast<const TX*>(kb.p);
     const double local_tol = sc->local_tol;
     const int64_t t0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x, nt = (int64_t)gridDim.x * blockDim.x;
     for (;;) {
         // the Hessian-vector product of p into hacc
-        hvp_share<L, T, double, CH>(hs, ha, HvpModel<T>{ ha.pi, static_cast<const T*>(ha.scr), ha.cap }, kb.p, kb.hacc, flags, phase);
+        hvp_share<L, T, TX, CH>(hs, ha, HvpModel<T>{ ha.pi, static_cast<const T*>(ha.scr), ha.cap }, pin, kb.hacc, flags, phase);
         if (!grid_sync(gs, limit, flags)) return;
         // tmp = project(m p + dt^2 hacc), hacc = 0; partial p . tmp (BackwardEuler.h:322-351)
         // (two nodes per step, every load issued before the arithmetic, as in
@@ -891,8 +899,13 @@ __global__ void __launch_bounds__(FUSED_THREADS, 4) k_cg_persistent(NodeGeom ng,
 #pragma unroll
             for (int u = 0; u < 2; ++u) {
                 if (mm[u] == 0) continue;
+                double pn[3];
 #pragma unroll
-                for (int c = 0; c < 3; ++c) kb.p[vidx<NPB>(nu[u], c)] = qv[u][c] + beta * pv[u][c];
+                for (int c = 0; c < 3; ++c) {
+                    pn[c] = qv[u][c] + beta * pv[u][c];
+                    kb.p[vidx<NPB>(nu[u], c)] = pn[c];
+                }
+                if (kb.pf) reinterpret_cast<float4*>(kb.pf)[nu[u]] = make_float4((float)pn[0], (float)pn[1], (float)pn[2], 0.f);
             }
         }
         ++k;
@@ -1293,6 +1306,7 @@ __global__ void __launch_bounds__(ND_THREADS) k_adj_cg_init(NodeGeom ng, const d
             kb.r[i] = r[k];
             kb.q[i] = q;
             kb.p[i] = q;
+            if (kb.pf) kb.pf[4 * n + k] = (float)q;
             kb.hacc[i] = 0;
             acc += r[k] * q;
         }
@@ -1556,10 +1570,15 @@ int launch_cg_persistent(const NewtonLaunch& L, cudaStream_t st)
     const int8_t* col = ctx->collided.as<int8_t>();
     const double* P6 = ctx->proj.as<double>();
     GridSync* gs = ctx->gsync.as<GridSync>();
-    if (ctx->mixed)
-        return launch_coop(ctx, st, k_cg_persistent<Lay, float>, L.ng, ha, gm, col, P6, L.dt2, L.kb, L.pA, L.pC, L.sc, L.np.kmax, gs,
+    if (ctx->mixed) {
+        if (!L.kb.pf) {
+            ctx->err = "MIXED CG needs the FP32 copy of p";
+            return ZMPM_BAD_ARG;
+        }
+        return launch_coop(ctx, st, k_cg_persistent<Lay, float, float>, L.ng, ha, gm, col, P6, L.dt2, L.kb, L.pA, L.pC, L.sc, L.np.kmax, gs,
             ctx->spin_limit, flags);
-    return launch_coop(ctx, st, k_cg_persistent<Lay, double>, L.ng, ha, gm, col, P6, L.dt2, L.kb, L.pA, L.pC, L.sc, L.np.kmax, gs,
+    }
+    return launch_coop(ctx, st, k_cg_persistent<Lay, double, double>, L.ng, ha, gm, col, P6, L.dt2, L.kb, L.pA, L.pC, L.sc, L.np.kmax, gs,
         ctx->spin_limit, flags);
 }
 
@@ -1699,6 +1718,8 @@ static int newton_impl(Ctx* ctx, const zmpm_solver& s)
     const bool zf = ctx->mixed && L.np.minres;
     L.kb.Zf[0] = zf ? ctx->kvf.as<float>() : nullptr;
     L.kb.Zf[1] = zf ? ctx->kvf.as<float>() + 4 * L.ng.nn : nullptr;
+    // MIXED CG runs its FP32 product on an FP32 copy of p
+    L.kb.pf = (ctx->mixed && !L.np.minres) ? ctx->kvf.as<float>() : nullptr;
     L.np.kmax = s.krylov_max_iterations;
     L.np.nmax = s.newton_max_iterations;
     L.np.tol = s.newton_tolerance;
@@ -1798,6 +1819,7 @@ static int admm_impl(Ctx* ctx, const zmpm_solver& s)
     kb.Z[0] = ctx->kv[7].as<double>();
     kb.Z[1] = ctx->kv[8].as<double>();
     kb.Zf[0] = kb.Zf[1] = nullptr;
+    kb.pf = nullptr;
     kb.hacc = ctx->kv[9].as<double>();
     kb.pre = ctx->adm_pre.as<double>();
     Lc.np.minres = 1;
@@ -1916,6 +1938,7 @@ int run_adjoint_solve(Ctx* ctx, double tol, int max_iterations)
     for (int k = 0; k < 3; ++k) kb.Q[k] = kb.M[k] = nullptr;
     kb.Z[0] = kb.Z[1] = nullptr;
     kb.Zf[0] = kb.Zf[1] = nullptr;
+    kb.pf = ctx->mixed ? ctx->kvf.as<float>() : nullptr; // the FP32 product of a MIXED context runs on an FP32 copy of p
     kb.hacc = ctx->kv[9].as<double>();
     kb.pre = ctx->gm.as<double>();
     Lc.np.minres = 0;
