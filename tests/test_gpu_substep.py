@@ -218,8 +218,12 @@ def test_profiling_loop_matches_graph(cuda_lib, precision, solver):
         assert st[0]["hvp_timed"] == 0
         assert st[1]["hvp_timed"] == st[1]["krylov_iterations"] and st[1]["ms_hvp"] > 0
     a, b = sims[0].getParticles(), sims[1].getParticles()
-    assert rel(b["X"], a["X"]) < 1e-10
-    assert rel(b["F"], a["F"]) < 1e-7
+    # the two runs differ only in the order of the scatters' atomic sums:
+    # FP64 round-off, or in MIXED FP32 round-off carried by the Newton solve
+    # (measured up to 1e-9 in positions)
+    tx, tf = (1e-10, 1e-7) if precision == "fp64" else (1e-7, 1e-5)
+    assert rel(b["X"], a["X"]) < tx
+    assert rel(b["F"], a["F"]) < tf
 
 
 @pytest.mark.parametrize("kind,plastic", [("fcr", None), ("hencky", 150.0)])
