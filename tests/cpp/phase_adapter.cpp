@@ -1,27 +1,19 @@
-// A C++ caller of include/zmpm.h, compiled with g++ against the header alone
-// and linked with the CUDA library.  It drives the implicit substep the way a
+// A C++ caller of the library through its C++ host wrapper (include/zmpm.hpp
+// over include/zmpm.h), compiled with g++ against the headers alone and linked
+// with the CUDA library.  It drives the implicit substep the way a
 // reference-side adapter does (an MpmSimulationBase subclass that overrides
 // advanceOneTimeStep and keeps one phase for itself): particlesToGrid,
 // backwardEulerStep, gridToParticles without plasticity, then applyPlasticity
-// as the subclass's own step.  The same scene advanced by zmpm_substep is the
-// comparison.  Prints one line "max_rel_dx <value> substeps <n>" and exits 0,
-// or prints the failing call and exits 1.
+// as the subclass's own step.  The same scene advanced by whole substeps is
+// the comparison.  Prints one line "max_rel_dx <value> substeps <n>" and
+// exits 0, or prints the failing call and exits 1.
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <random>
 #include <vector>
 
-#include "zmpm.h"
-
-#define CHECK(call)                                                                                   \
-    do {                                                                                              \
-        int rc_ = (call);                                                                             \
-        if (rc_ < 0) {                                                                                \
-            std::printf("FAILED %s -> %d (%s)\n", #call, rc_, zmpm_status_string(rc_));               \
-            std::exit(1);                                                                             \
-        }                                                                                             \
-    } while (0)
+#include "zmpm.hpp"
 
 namespace {
 
@@ -50,26 +42,14 @@ Scene make_scene(double dx)
     return s;
 }
 
-// The adapter: one context, the reference's registration calls, and a
-// substep in phases with plasticity applied as a separate step.
+// The adapter: a GpuMpmSimulation (include/zmpm.hpp) set up through the
+// registration calls, and a substep either whole or in phases with
+// plasticity applied as a separate step.
 class PhaseAdapter {
 public:
-    PhaseAdapter(const Scene& sc, double dx, int precision, bool phases) : phases_(phases)
+    PhaseAdapter(const Scene& sc, double dx, int precision, bool phases) : sim_(options(dx, precision)), phases_(phases)
     {
-        zmpm_config cfg{};
-        cfg.precision = precision;
-        cfg.layout = ZMPM_LAYOUT_AUTO;
-        cfg.grid_log2 = 7;
-        cfg.dx = dx;
-        cfg.gravity[1] = -9.8;
-        cfg.apic_rpic_ratio = 1;
-        cfg.cfl = 0.6;
-        CHECK(zmpm_create(&cfg, &ctx_));
-        const int64_t n = (int64_t)sc.m.size();
-        int64_t lower = 0;
-        CHECK(zmpm_add_particles(ctx_, n, sc.x.data(), sc.v.data(), sc.m.data(), sc.vol.data(), &lower));
-        CHECK(zmpm_add_fbased_force(ctx_, lower, lower + n, ZMPM_MODEL_STVK_HENCKY_ISOTROPIC, 1e4, 0.3));
-        CHECK(zmpm_add_plasticity(ctx_, lower, lower + n, ZMPM_PLASTIC_VON_MISES, 60.0, 0.0, 1e30));
+        sim_.addParticles(sc.x, sc.v, sc.m, sc.vol).addFBasedMpmForce(ZMPM_MODEL_STVK_HENCKY_ISOTROPIC, 1e4, 0.3).addVonMises(60.0, 0.0, 1e30);
         zmpm_collider floor{};
         floor.shape = ZMPM_HALF_SPACE;
         floor.type = ZMPM_STICKY;
@@ -77,36 +57,40 @@ public:
         floor.b[1] = 1.0;
         floor.rotation[0] = 1.0;
         floor.scale = 1.0;
-        int32_t id = 0;
-        CHECK(zmpm_add_collision_object(ctx_, &floor, &id));
-        zmpm_default_solver(&solver_, ZMPM_MINRES, precision);
-        solver_.newton_tolerance = 1e-9;
-        solver_.newton_max_iterations = 8;
+        sim_.addCollisionObject(floor);
+        sim_.solver().newton_tolerance = 1e-9;
+        sim_.solver().newton_max_iterations = 8;
     }
-    ~PhaseAdapter() { zmpm_destroy(ctx_); }
 
-    int advanceOneTimeStep(double dt)
+    void advanceOneTimeStep(double dt)
     {
-        if (!phases_) return zmpm_substep(ctx_, dt, &solver_, nullptr);
-        CHECK(zmpm_particles_to_grid(ctx_, dt, &solver_));
-        zmpm_stats st;
-        CHECK(zmpm_backward_euler_step(ctx_, &st));
-        const int rc = zmpm_grid_to_particles(ctx_, 0, nullptr);
-        CHECK(rc);
-        CHECK(zmpm_apply_plasticity(ctx_));
-        return rc;
+        if (!phases_) {
+            sim_.advanceOneTimeStep(dt);
+            return;
+        }
+        sim_.particlesToGrid(dt);
+        sim_.backwardEulerStep();
+        sim_.gridToParticles(false);
+        sim_.applyPlasticity();
     }
 
     std::vector<double> positions()
     {
-        std::vector<double> x(3 * zmpm_num_particles(ctx_));
-        CHECK(zmpm_get_particles(ctx_, x.data(), nullptr, nullptr, nullptr));
+        std::vector<double> x;
+        sim_.getParticles(&x);
         return x;
     }
 
 private:
-    zmpm_ctx* ctx_ = nullptr;
-    zmpm_solver solver_;
+    static zmpm::GpuMpmSimulation::Options options(double dx, int precision)
+    {
+        zmpm::GpuMpmSimulation::Options o;
+        o.dx = dx;
+        o.precision = precision;
+        o.grid_log2 = 7;
+        return o;
+    }
+    zmpm::GpuMpmSimulation sim_;
     bool phases_;
 };
 
@@ -119,9 +103,15 @@ int main(int argc, char** argv)
     const Scene sc = make_scene(dx);
     PhaseAdapter whole(sc, dx, precision, false), split(sc, dx, precision, true);
     const int steps = 4;
-    for (int n = 0; n < steps; ++n) {
-        CHECK(whole.advanceOneTimeStep(1e-3));
-        CHECK(split.advanceOneTimeStep(1e-3));
+    try {
+        for (int n = 0; n < steps; ++n) {
+            whole.advanceOneTimeStep(1e-3);
+            split.advanceOneTimeStep(1e-3);
+        }
+    }
+    catch (const std::exception& e) {
+        std::printf("FAILED %s\n", e.what());
+        return 1;
     }
     const std::vector<double> a = whole.positions(), b = split.positions();
     double err = 0;

@@ -43,3 +43,12 @@ def test_restart_file_names_follow_the_reference():
     assert mpm.MpmSimulation.outputFileName(7, 0) == "restart_7.dat"
     assert mpm.MpmSimulation.outputFileName(7, 3) == "restart_7_3.dat"
     assert mpm.MpmSimulation.outputFileName(0, 1, name="state", suffix=".bin") == "state_0_1.bin"
+
+
+def test_cpp_wrapper_compiles_without_a_gpu():
+    """include/zmpm.hpp (the GpuMpmSimulation host wrapper) and the C++ adapter
+    built on it compile with g++ -Wall -Wextra -Werror against the headers."""
+    import subprocess
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    subprocess.run(["g++", "-std=c++17", "-fsyntax-only", "-Wall", "-Wextra", "-Werror", "-I", os.path.join(root, "include"),
+                    os.path.join(root, "tests", "cpp", "phase_adapter.cpp")], check=True)

@@ -1,6 +1,7 @@
-"""A C++ program that includes only include/zmpm.h (compiled here with g++ and
-linked with the CUDA library) drives the implicit substep in phases, as a
-reference-side MpmSimulationBase subclass would, and matches zmpm_substep."""
+"""A C++ program built on the library's C++ host wrapper (include/zmpm.hpp
+over include/zmpm.h; compiled here with g++ and linked with the CUDA library)
+drives the implicit substep in phases, as a reference-side MpmSimulationBase
+subclass would, and matches whole substeps."""
 import os
 import subprocess
 
